@@ -1,0 +1,427 @@
+#!/usr/bin/env python3
+"""Benchmark: the mixed-precision CG-style level-1 chain on a 48^3x96
+DiracFermion field through the QLA C-ABI of libqla_b200.so.
+
+Workload (one "step"): 50 iterations of
+    QLA_F3_D_vpeq_r_times_D(x, &a_k, p)     x += a_k p   (a_k ~ U[-1,1], seeded)
+    QLA_DF3_r_veq_norm2_D(&nrm_k, x)        |x|^2, FP64 compensated reduction
+    QLA_DF3_c_veq_D_dot_D(&dot_k, x, p)     <x, p>, FP64 compensated reduction
+on 10,616,832 sites (x, p: 1.02 GB each in F3, resident in HBM; inputs are far
+larger than the 126 MB L2, so no flush is needed between iterations).
+
+metric: site-updates/s, one site-update = one lattice site through one chain
+iteration (axpy + norm2 + dot), next to the same chain in plain FP64
+(QLA_D3_*) on the same GPU.  Algorithmic bytes per site-update: 576 (F3) and
+1152 (D3) (288 axpy + 96 norm2 + 192 dot, x2 for D3).
+
+--impl reference runs the reference's own CPU implementation of the chain
+(oracle/_ref/libqla_ref.so, the generated QLA C built with OpenMP) on the
+host's cores on a bounded sample of the same field.
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N>1 under
+torchrun each rank runs an independent replica (QLA is single-node data:
+nothing to exchange), value = all ranks' site-updates / max rank time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+DIMS = (48, 48, 48, 96)
+NSITES = 48 * 48 * 48 * 96
+ITERS = 50
+BYTES_F3 = {"axpy": 288, "norm2": 96, "dot": 192}
+BYTES_D3 = {k: 2 * v for k, v in BYTES_F3.items()}
+METRIC = "site-updates/s & % B200 HBM peak: FP32+FP64-reduce vs plain FP64, same GPU"
+UNIT = "site-updates/s"
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------------------
+# clock sampling during the timed region
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = []
+        smax = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                smax = float(s[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, s[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_lib():
+    """(ctypes lib, kind): the reference build when present, else the oracle port."""
+    ref = os.path.join(REPO, "oracle", "_ref", "libqla_ref.so")
+    if os.path.exists(ref):
+        return ctypes.CDLL(ref), "reference"
+    return ctypes.CDLL(os.path.join(REPO, "oracle", "liboracle.so")), "port"
+
+
+def cpu_chain_rate(x, p, a_vals, budget_s=15.0, max_iters=None):
+    """Time the chain on the host cores: returns (site-updates/s, iterations, seconds, kind, threads)."""
+    import numpy as np
+    lib, kind = cpu_reference_lib()
+    n = x.shape[0]
+    xp = ctypes.c_void_p(x.ctypes.data)
+    pp = ctypes.c_void_p(p.ctypes.data)
+    nrm = ctypes.c_double(0.0)
+    dot = (ctypes.c_double * 2)()
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if kind == "reference":
+        axpy, n2, dt = lib.QLA_F3_D_vpeq_r_times_D, lib.QLA_DF3_r_veq_norm2_D, lib.QLA_DF3_c_veq_D_dot_D
+
+        def one(a):
+            af = ctypes.c_float(a)
+            axpy(xp, ctypes.byref(af), pp, n)
+            n2(ctypes.byref(nrm), xp, n)
+            dt(dot, xp, pp, n)
+    else:
+        threads = 1
+        lib.ora_rtimes_f.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_long, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ora_norm2_ref_f.restype = ctypes.c_double
+
+        def one(a):
+            lib.ora_rtimes_f(xp, a, pp, n, 12, 1, None, None)
+            lib.ora_norm2_ref_f(xp, ctypes.c_long(n), 12, None, None)
+            lib.ora_dot_ref_f(dot, xp, pp, ctypes.c_long(n), 12, None, None, None)
+    one(float(a_vals[0]))  # warm-up (page faults, thread pool)
+    t0 = time.perf_counter()
+    it = 0
+    while True:
+        one(float(a_vals[(it + 1) % len(a_vals)]))
+        it += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_iters and it >= max_iters):
+            break
+    return n * it / el, it, el, kind, threads
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args):
+    import numpy as np
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    rng = np.random.default_rng(7)
+    n = NSITES
+    x = rng.standard_normal((n, 24), dtype=np.float32)
+    p = rng.standard_normal((n, 24), dtype=np.float32)
+    a_vals = rng.uniform(-1, 1, ITERS).astype(np.float32)
+    per_step_iters = 2  # bounded sample per step
+    lib, kind = cpu_reference_lib()
+    for _ in range(args.warmup):
+        cpu_chain_rate(x, p, a_vals, budget_s=0.0, max_iters=1)
+    times = []
+    its = 0
+    for _ in range(args.steps):
+        r, it, el, kind, threads = cpu_chain_rate(x, p, a_vals, budget_s=0.0, max_iters=per_step_iters)
+        times.append(el)
+        its += it
+    tot = sum(times)
+    value = n * its / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 sites, f64 reductions",
+        "data": "synthetic (seeded N(0,1) DiracFermions, a_k ~ U[-1,1])",
+        "config": {"workload": "cg_chain_48^3x96", "sites": n, "iterations_per_step": per_step_iters,
+                   "ops": ["QLA_F3_D_vpeq_r_times_D", "QLA_DF3_r_veq_norm2_D", "QLA_DF3_c_veq_D_dot_D"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{per_step_iters} chain iterations on the full 48^3x96 field per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_gpu_arm(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import qla_b200 as qla
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    qla.set_stream(stream)
+    n = NSITES
+    g = torch.Generator(device=dev)
+    g.manual_seed(1000 + rank)
+    rng = np.random.default_rng(7)
+    a_vals = rng.uniform(-1, 1, ITERS).astype(np.float32)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------- FP32 sites + FP64 reductions chain (F3 / DF3)
+    x = torch.randn(n, 24, device=dev, dtype=torch.float32, generator=g)
+    p = torch.randn(n, 24, device=dev, dtype=torch.float32, generator=g)
+    nrm = torch.zeros(ITERS, dtype=torch.float64, device=dev)
+    dot = torch.zeros(ITERS, 2, dtype=torch.float64, device=dev)
+    L = qla.lib()
+    f_axpy, f_n2, f_dot = L.QLA_F3_D_vpeq_r_times_D, L.QLA_DF3_r_veq_norm2_D, L.QLA_DF3_c_veq_D_dot_D
+    d_axpy, d_n2, d_dot = L.QLA_D3_D_vpeq_r_times_D, L.QLA_D3_r_veq_norm2_D, L.QLA_D3_c_veq_D_dot_D
+    for f in (f_axpy, f_n2, f_dot, d_axpy, d_n2, d_dot):
+        f.restype = None
+    a_f = [ctypes.c_float(float(v)) for v in a_vals]
+    a_d = [ctypes.c_double(float(v)) for v in a_vals]
+
+    def chain(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t, ev=None):
+        xp, pp = ctypes.c_void_p(xa.data_ptr()), ctypes.c_void_p(pa.data_ptr())
+        nb, db = nrm_t.data_ptr(), dot_t.data_ptr()
+        for k in range(ITERS):
+            if ev is not None:
+                ev[k][0].record(stream)
+            axpy(xp, ctypes.byref(avals[k]), pp, n)
+            if ev is not None:
+                ev[k][1].record(stream)
+            n2(ctypes.c_void_p(nb + 8 * k), xp, n)
+            if ev is not None:
+                ev[k][2].record(stream)
+            dt(ctypes.c_void_p(db + 16 * k), xp, pp, n)
+            if ev is not None:
+                ev[k][3].record(stream)
+
+    def timed(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t, steps, warmup, per_kernel):
+        for _ in range(warmup):
+            chain(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t)
+        qla.check("warm-up")
+        evs = []
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(ITERS)] \
+                if per_kernel else None
+            chain(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t, ev)
+            if ev:
+                evs.append(ev)
+        t1.record(stream)
+        barrier()
+        ms = t0.elapsed_time(t1)
+        kern = {"axpy": 0.0, "norm2": 0.0, "dot": 0.0}
+        for ev in evs:
+            for k in range(ITERS):
+                kern["axpy"] += ev[k][0].elapsed_time(ev[k][1])
+                kern["norm2"] += ev[k][1].elapsed_time(ev[k][2])
+                kern["dot"] += ev[k][2].elapsed_time(ev[k][3])
+        nl = max(1, len(evs) * ITERS)
+        kern = {k: v / nl for k, v in kern.items()}  # ms per launch
+        qla.check("timed region")
+        return ms, kern
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms_f, kern_f = timed(x, p, f_axpy, f_n2, f_dot, a_f, nrm, dot, args.steps, args.warmup, True)
+    clocks = clk.stop()
+    ms_f = max_over_ranks(ms_f)
+    value = world * n * ITERS * args.steps / (ms_f / 1e3)
+    nrm_host = nrm.cpu().numpy()
+    assert np.all(np.isfinite(nrm_host))
+
+    # ---------------- end to end through the C-ABI with host buffers:
+    # per step: pinned host -> device copy of x and p, the 50-iteration chain,
+    # device -> host read of the 100 reduction results.
+    xh = torch.empty((n, 24), dtype=torch.float32, pin_memory=True)
+    ph = torch.empty((n, 24), dtype=torch.float32, pin_memory=True)
+    xh.copy_(x)
+    ph.copy_(p)
+    nrm_h = torch.empty(ITERS, dtype=torch.float64, pin_memory=True)
+    dot_h = torch.empty((ITERS, 2), dtype=torch.float64, pin_memory=True)
+    e_steps = max(1, min(args.steps, 5))
+    for _ in range(1):
+        x.copy_(xh, non_blocking=True)
+        p.copy_(ph, non_blocking=True)
+        chain(x, p, f_axpy, f_n2, f_dot, a_f, nrm, dot)
+        nrm_h.copy_(nrm, non_blocking=True)
+        dot_h.copy_(dot, non_blocking=True)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        x.copy_(xh, non_blocking=True)
+        p.copy_(ph, non_blocking=True)
+        chain(x, p, f_axpy, f_n2, f_dot, a_f, nrm, dot)
+        nrm_h.copy_(nrm, non_blocking=True)
+        dot_h.copy_(dot, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    ms_e = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": world * n * ITERS * e_steps / (ms_e / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(xh.numel() * 4 + ph.numel() * 4),
+           "d2h_bytes_per_step": int(nrm_h.numel() * 8 + dot_h.numel() * 8), "steps": e_steps}
+    del xh, ph
+
+    # ---------------- plain FP64 chain (D3) on the same GPU
+    del x, p
+    torch.cuda.empty_cache()
+    xd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
+    pd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
+    ms_d, kern_d = timed(xd, pd, d_axpy, d_n2, d_dot, a_d, nrm, dot, args.steps, args.warmup, True)
+    ms_d = max_over_ranks(ms_d)
+    value_d = world * n * ITERS * args.steps / (ms_d / 1e3)
+    del xd, pd
+    torch.cuda.empty_cache()
+
+    # ---------------- roofline of the dominant kernel (axpy) and of all three
+    peak, peak_kind = peaks()
+    rl = {}
+    for nm, ms in kern_f.items():
+        ach = BYTES_F3[nm] * n / (ms / 1e3) / 1e9
+        rl[nm] = {"achieved": ach, "frac": ach / peak, "us_per_launch": 1e3 * ms}
+    rl_d = {}
+    for nm, ms in kern_d.items():
+        ach = BYTES_D3[nm] * n / (ms / 1e3) / 1e9
+        rl_d[nm] = {"achieved": ach, "frac": ach / peak, "us_per_launch": 1e3 * ms}
+    dom = max(kern_f, key=lambda k: kern_f[k])
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("F3_" + dom)
+    chain_bytes = sum(BYTES_F3.values())
+    launches = 3 * ITERS * args.steps
+
+    # ---------------- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        xs = np.random.default_rng(3).standard_normal((n, 24), dtype=np.float32)
+        ps = np.random.default_rng(4).standard_normal((n, 24), dtype=np.float32)
+        os.environ.setdefault("OMP_PROC_BIND", "close")
+        r, it, el, kind, threads = cpu_chain_rate(xs, ps, a_vals, budget_s=args.cpu_seconds)
+        cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{it} chain iterations on the full 48^3x96 field ({el:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_f / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 sites, f64 reductions",
+            "data": "synthetic (seeded N(0,1) DiracFermions, a_k ~ U[-1,1])",
+            "config": {"workload": "cg_chain_48^3x96", "sites": n, "iterations_per_step": ITERS,
+                       "ops": ["QLA_F3_D_vpeq_r_times_D", "QLA_DF3_r_veq_norm2_D", "QLA_DF3_c_veq_D_dot_D"],
+                       "bytes_per_site_update": chain_bytes, "l2": "inputs (2 x 1.02 GB) larger than L2",
+                       "parallelism": f"replicas x{world}"},
+            "hbm_frac_chain": value / world * chain_bytes / 1e9 / peak,
+            "fp64_chain": {"value": value_d, "ms_per_step": ms_d / args.steps,
+                           "hbm_frac": value_d / world * 2 * chain_bytes / 1e9 / peak,
+                           "ops": ["QLA_D3_D_vpeq_r_times_D", "QLA_D3_r_veq_norm2_D", "QLA_D3_c_veq_D_dot_D"],
+                           "kernels": rl_d},
+            "speedup_vs_fp64": value / value_d,
+            "roofline": {"bound": "hbm", "kernel": f"QLA_F3_D_vpeq_r_times_D" if dom == "axpy" else dom,
+                         "achieved": rl[dom]["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": rl[dom]["frac"], "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": BYTES_F3[dom] * n},
+            "kernels": rl,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("bench.py: warm-up raised to 3 steps", file=sys.stderr)
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1458 @@
+/*
+ * qla_b200_f3.h -- GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+ *
+ * QLA F3 level-1 entry points implemented by libqla_b200.so (sm_100a).
+ * Each declaration replaces the reference function of the same name, whose
+ * C loop the reference generator emits from the cited section.  Array
+ * arguments are device pointers; see qla_b200_runtime.h for scalars,
+ * reduction outputs, streams and errors.
+ */
+#ifndef QLA_B200_F3_H
+#define QLA_B200_F3_H
+#include "qla_b200_types.h"
+
+#ifdef __cplusplus
+#define QLA_B200_RESTRICT __restrict__
+extern "C" {
+#else
+#define QLA_B200_RESTRICT restrict
+#endif
+
+/* ---- lmult: replaces the F3 functions emitted by lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix) */
+/* replaces QLA_F3_V_veq_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veq_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vpeq_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_vmeq_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_veqm_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_xeq_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeq_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xpeq_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xmeq_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_M_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_M_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_M_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_M_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_Ma_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_Ma_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_Ma_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_Ma_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pM_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_pM_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pM_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_pM_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pMa_times_V (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_pMa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pMa_times_pV (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_V_xeqm_pMa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_eq_M_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_eq_M_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_eq_Ma_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_eq_Ma_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_peq_M_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_peq_M_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_peq_Ma_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_peq_Ma_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_meq_M_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_meq_M_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_meq_Ma_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_meq_Ma_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_eqm_M_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_eqm_M_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_V_eqm_Ma_times_xV (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_eqm_Ma_times_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_veq_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veq_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vpeq_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_vmeq_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_veqm_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_xeq_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeq_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xpeq_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xmeq_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_M_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_M_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_M_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_M_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_Ma_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_Ma_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_Ma_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_Ma_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pM_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_pM_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pM_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_pM_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pMa_times_H (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_pMa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pMa_times_pH (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_H_xeqm_pMa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_eq_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_eq_M_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_eq_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_eq_Ma_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_peq_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_peq_M_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_peq_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_peq_Ma_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_meq_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_meq_M_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_meq_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_meq_Ma_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_eqm_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_eqm_M_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_H_eqm_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_eqm_Ma_times_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_veq_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veq_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vpeq_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_vmeq_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_veqm_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_xeq_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeq_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xpeq_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xmeq_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_M_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_M_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_Ma_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_Ma_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pM_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pM_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pMa_times_D (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pMa_times_pD (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_D_xeqm_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_eq_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_eq_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_eq_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_eq_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_peq_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_peq_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_peq_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_peq_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_meq_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_meq_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_meq_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_meq_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_eqm_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_eqm_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_D_eqm_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_eqm_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_veq_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veq_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vpeq_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_vmeq_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_veqm_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_xeq_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeq_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xpeq_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xmeq_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_M_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_M_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_M_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_M_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_M_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_M_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_M_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_M_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ma_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_Ma_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ma_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_Ma_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ma_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_Ma_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ma_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_Ma_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pM_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pM_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pM_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pM_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pM_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pM_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pM_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pM_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pMa_times_M (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pMa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pMa_times_pM (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pMa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pMa_times_Ma (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pMa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pMa_times_pMa (lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), expressions_tensor.pl:766) */
+void QLA_F3_M_xeqm_pMa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_eq_M_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_eq_M_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_eq_Ma_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_eq_Ma_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_peq_M_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_peq_M_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_peq_Ma_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_peq_Ma_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_meq_M_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_meq_M_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_meq_Ma_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_meq_Ma_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_eqm_M_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_eqm_M_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* replaces QLA_F3_M_eqm_Ma_times_xM (doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_eqm_Ma_times_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * jb, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_veq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_veq_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_veq_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_veq_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_veq_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_veq_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_vpeq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_vpeq_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_vpeq_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_vpeq_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_vpeq_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_vpeq_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_vmeq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_vmeq_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_vmeq_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_vmeq_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_vmeq_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_vmeq_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_veqm_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_veqm_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_veqm_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_veqm_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_veqm_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_veqm_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_xeq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xeq_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xeq_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_xeq_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xeq_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xeq_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_xpeq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xpeq_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xpeq_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_xpeq_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xpeq_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xpeq_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_xmeq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xmeq_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xmeq_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_xmeq_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xmeq_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xmeq_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- spproj: replaces the F3 functions emitted by lib/perl/build_qla.pl:1087-1110 */
+/* replaces QLA_F3_H_xeqm_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xeqm_spproj_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_pD (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
+void QLA_F3_H_xeqm_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- sprecon: replaces the F3 functions emitted by lib/perl/build_qla.pl:1112-1135 */
+/* replaces QLA_F3_D_xeqm_sprecon_H (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xeqm_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
+void QLA_F3_D_xeqm_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_veq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_veq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_veq_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_veq_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_veq_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_veq_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_veq_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_veq_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_vpeq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_vpeq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_vpeq_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_vpeq_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_vpeq_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_vpeq_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_vpeq_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_vpeq_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_vmeq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_vmeq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_vmeq_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_vmeq_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_vmeq_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_vmeq_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_vmeq_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_vmeq_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_veqm_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_veqm_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_veqm_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_veqm_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_veqm_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_veqm_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_veqm_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_veqm_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xeq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xeq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xeq_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xeq_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xeq_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xeq_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xeq_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xeq_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xpeq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xpeq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xpeq_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xpeq_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xpeq_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xpeq_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xpeq_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xpeq_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xmeq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xmeq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xmeq_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xmeq_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xmeq_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xmeq_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xmeq_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xmeq_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xeqm_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xeqm_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xeqm_V (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xeqm_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_V_xeqm_r_times_pV (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_V_xeqm_r_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_V_xeqm_pV (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_V_xeqm_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_eq_xV (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_eq_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_V_peq_xV (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_peq_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_V_meq_xV (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_meq_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_V_eqm_xV (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_V_eqm_xV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * ja, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_veq_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_veq_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_veq_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_veq_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_veq_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_veq_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_veq_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_veq_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_vpeq_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_vpeq_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_vpeq_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_vpeq_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_vpeq_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_vpeq_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_vpeq_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_vpeq_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_vmeq_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_vmeq_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_vmeq_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_vmeq_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_vmeq_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_vmeq_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_vmeq_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_vmeq_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_veqm_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_veqm_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_veqm_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_veqm_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_veqm_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_veqm_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_veqm_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_veqm_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xeq_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xeq_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xeq_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xeq_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xeq_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xeq_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xeq_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xeq_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xpeq_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xpeq_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xpeq_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xpeq_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xpeq_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xpeq_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xpeq_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xpeq_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xmeq_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xmeq_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xmeq_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xmeq_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xmeq_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xmeq_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xmeq_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xmeq_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xeqm_r_times_H (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xeqm_r_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xeqm_H (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xeqm_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_H_xeqm_r_times_pH (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_H_xeqm_r_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_H_xeqm_pH (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_H_xeqm_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_eq_xH (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_eq_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_H_peq_xH (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_peq_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_H_meq_xH (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_meq_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_H_eqm_xH (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_H_eqm_xH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_veq_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_veq_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_veq_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_veq_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_veq_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_veq_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_veq_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_veq_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_vpeq_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_vpeq_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_vpeq_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_vpeq_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_vpeq_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_vpeq_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_vpeq_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_vpeq_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_vmeq_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_vmeq_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_vmeq_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_vmeq_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_vmeq_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_vmeq_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_vmeq_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_vmeq_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_veqm_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_veqm_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_veqm_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_veqm_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_veqm_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_veqm_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_veqm_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_veqm_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xeq_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xeq_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xeq_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xeq_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xeq_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xeq_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xeq_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xeq_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xpeq_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xpeq_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xpeq_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xpeq_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xpeq_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xpeq_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xpeq_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xpeq_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xmeq_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xmeq_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xmeq_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xmeq_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xmeq_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xmeq_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xmeq_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xmeq_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xeqm_r_times_D (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xeqm_r_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xeqm_D (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xeqm_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_D_xeqm_r_times_pD (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_D_xeqm_r_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_D_xeqm_pD (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_D_xeqm_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_eq_xD (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_eq_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_D_peq_xD (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_peq_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_D_meq_xD (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_meq_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_D_eqm_xD (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_D_eqm_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * ja, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_veq_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_veq_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_veq_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_veq_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_veq_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_veq_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_veq_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_veq_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_vpeq_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_vpeq_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_vpeq_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_vpeq_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_vpeq_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_vpeq_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_vpeq_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_vpeq_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_vmeq_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_vmeq_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_vmeq_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_vmeq_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_vmeq_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_vmeq_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_vmeq_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_vmeq_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_veqm_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_veqm_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_veqm_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_veqm_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_veqm_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_veqm_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_veqm_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_veqm_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xeq_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xeq_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xeq_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xeq_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xeq_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xeq_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xeq_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xeq_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xpeq_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xpeq_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xpeq_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xpeq_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xpeq_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xpeq_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xpeq_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xpeq_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xmeq_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xmeq_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xmeq_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xmeq_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xmeq_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xmeq_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xmeq_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xmeq_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xeqm_r_times_M (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xeqm_r_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xeqm_M (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xeqm_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
+/* replaces QLA_F3_M_xeqm_r_times_pM (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
+void QLA_F3_M_xeqm_r_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- copy: replaces the F3 functions emitted by lib/perl/build_qla.pl:370-400 (assignment / gather) */
+/* replaces QLA_F3_M_xeqm_pM (lib/perl/build_qla.pl:370-400 (assignment / gather)) */
+void QLA_F3_M_xeqm_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_eq_xM (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_eq_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_M_peq_xM (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_peq_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_M_meq_xM (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_meq_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * ja, int n);
+/* replaces QLA_F3_M_eqm_xM (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
+void QLA_F3_M_eqm_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * ja, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_veq_norm2_V (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_r_veq_norm2_pV (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_V_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_V_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_V_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_V_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pV_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pV_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pV_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pV_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_xeq_norm2_V (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_r_xeq_norm2_pV (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_V_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_V_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_V_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_V_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pV_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pV_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pV_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pV_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_veq_norm2_H (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_r_veq_norm2_pH (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_H_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_H_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_H_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_H_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pH_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pH_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pH_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pH_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_xeq_norm2_H (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_r_xeq_norm2_pH (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_H_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_H_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_H_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_H_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pH_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pH_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pH_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pH_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_veq_norm2_D (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_r_veq_norm2_pD (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_D_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_D_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_D_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_D_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pD_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pD_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pD_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pD_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_xeq_norm2_D (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_r_xeq_norm2_pD (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_D_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_D_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_D_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_D_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pD_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pD_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pD_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pD_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_veq_norm2_M (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_r_veq_norm2_pM (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_veq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_M_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_M_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_M_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_M_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pM_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pM_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_veq_pM_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_veq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_veq_re_pM_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_veq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
+/* replaces QLA_F3_r_xeq_norm2_M (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_r_xeq_norm2_pM (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
+void QLA_F3_r_xeq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_M_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_M_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_M_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_M_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pM_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pM_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* ---- dot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2196-2360 */
+/* replaces QLA_F3_c_xeq_pM_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
+void QLA_F3_c_xeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_F3_r_xeq_re_pM_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_F3_r_xeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

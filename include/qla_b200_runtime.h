@@ -1,0 +1,69 @@
+/*
+ * qla_b200_runtime.h -- the small runtime API that a GPU drop-in of QLA needs
+ * and the reference does not have.
+ *
+ * Reference behaviour being extended: every QLA function is void, synchronous,
+ * stateless and works on host memory (doc/qla.tex:259-263).  Here:
+ *  - array arguments are device (or managed) pointers; pointer arrays (`pX`
+ *    arguments) are device arrays of device pointers;
+ *  - scalar inputs (`QLA_F_Real *a` ...) may be host or device pointers: a host
+ *    scalar is read at call time, a device scalar is read by the kernel;
+ *  - reduction outputs may be host or device pointers: a host output makes the
+ *    call synchronous (the reference's semantics), a device output keeps it
+ *    asynchronous on the current stream;
+ *  - calls are issued on a per-host-thread current stream (default: the legacy
+ *    default stream);
+ *  - errors are recorded in a sticky per-thread status, because the QLA
+ *    signatures return void.
+ */
+#ifndef QLA_B200_RUNTIME_H
+#define QLA_B200_RUNTIME_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes of qlagpu_last_error() */
+#define QLAGPU_OK 0
+#define QLAGPU_ERR_NULLPTR 1
+#define QLAGPU_ERR_LAUNCH 2
+#define QLAGPU_ERR_ALLOC 3
+#define QLAGPU_ERR_ARG 4
+#define QLAGPU_ERR_DEVICE 5
+#define QLAGPU_ERR_NOT_DEVICE 6
+
+/* sticky status of this host thread (first error since the last clear) */
+int qlagpu_last_error(void);
+const char *qlagpu_last_error_string(void);
+void qlagpu_clear_error(void);
+
+/* stream subsequent calls of this host thread are issued on (cudaStream_t) */
+void qlagpu_set_stream(void *stream);
+void *qlagpu_get_stream(void);
+/* synchronise the current stream; returns the sticky status */
+int qlagpu_synchronize(void);
+
+/* synchronise, then return the device error word (bit 1: a pipeline wait gave
+ * up; 2: draining copies gave up; 8: an iterative matrix function hit its
+ * iteration cap); clear != 0 resets it */
+unsigned qlagpu_device_error(int clear);
+
+/* autotuner: launch shape (threads per block = sites per tile: 64/128/256,
+ * pipeline stages: 2..8) for one kernel id, as reported by
+ * qla_b200.tune; qlagpu_tune_clear() restores the built-in heuristic */
+int qlagpu_tune_set(const char *kernel_id, int threads, int stages);
+void qlagpu_tune_clear(void);
+
+int qlagpu_sm_count(void);
+const char *qlagpu_version(void);
+
+/* periodic neighbour table on the device: idx[i] = the lexicographic site
+ * (x0 fastest) of x(i) + sign * e_mu on the nd-dimensional torus dims[];
+ * n = prod(dims).  This is the int32 index stream the `xX` gathers take. */
+void qlagpu_shift_index(int *idx, int nd, const int *dims, int mu, int sign);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QLA_B200_RUNTIME_H */

@@ -1,0 +1,35 @@
+/*
+ * Test infrastructure (the oracle) -- NOT product code.
+ * Declarations of the CPU restatement in qla_oracle.c / qla_oracle_body.h.
+ * eqop codes: 0 eq, 1 peq, 2 meq, 3 eqm.  Index arrays may be NULL.
+ */
+#ifndef QLA_ORACLE_H
+#define QLA_ORACLE_H
+
+#define ORA_DECL(SFX, R)                                                           \
+void ora_lmult_##SFX(R *r, const R *a, const R *b, long n, int nc, int ncol,      \
+                     int eqop, int adja, int adjb,                                \
+                     const int *idx_a, const int *idx_b, const int *gang);        \
+void ora_spproj_##SFX(R *r, const R *a, long n, int nc, int mu, int sign,        \
+                      int eqop, const int *idx_a, const int *gang);               \
+void ora_sprecon_##SFX(R *r, const R *a, long n, int nc, int mu, int sign,       \
+                       int eqop, const int *idx_a, const int *gang);              \
+void ora_rtimes_##SFX(R *r, R a, const R *b, long n, int ncplx, int eqop,        \
+                      const int *idx_b, const int *gang);                         \
+double ora_norm2_ref_##SFX(const R *a, long n, int ncplx, const int *idx_a,      \
+                           const int *gang);                                      \
+void ora_dot_ref_##SFX(double *out2, const R *a, const R *b, long n, int ncplx,  \
+                       const int *idx_a, const int *idx_b, const int *gang);      \
+void ora_dot_field_##SFX(R *r, const R *a, const R *b, long n, int ncplx,        \
+                         const int *idx_a, const int *idx_b, const int *gang);    \
+double ora_norm2_exact_##SFX(const R *a, long n, int ncplx, const int *idx_a,    \
+                             const int *gang);                                    \
+void ora_dot_exact_##SFX(double *out2, const R *a, const R *b, long n, int ncplx,\
+                         const int *idx_a, const int *idx_b, const int *gang);
+
+ORA_DECL(f, float)
+ORA_DECL(d, double)
+
+int ora_version(void);
+
+#endif

@@ -1,0 +1,268 @@
+// qla_core.cuh -- device-side building blocks shared by every QLA B200 kernel.
+//
+//  * complex arithmetic that restates the QLA complex macros
+//    (include/qla_complex.h:147-405) with explicitly rounded operations
+//    (__fmul_rn/__fadd_rn/... never contract into FMA), so that site results
+//    are bit-identical to the reference's C compiled on x86-64;
+//  * record load/store helpers for the AoS site records
+//    (include/qla_types.h:29-33: V[nc], H[nc][2], D[nc][4], M[nc][nc]);
+//  * thin inline-PTX wrappers for sm_100a mbarriers and bulk (1-D TMA)
+//    copies, with time-bounded waits that record an error instead of hanging.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qlab {
+
+// ---------------------------------------------------------------------------
+// error bits written by kernels into the device error word (read by the host
+// through qlagpu_device_error()).
+enum : unsigned {
+  QLA_DEVERR_MBAR_TIMEOUT = 1u,   // an mbarrier wait gave up
+  QLA_DEVERR_BULK_TIMEOUT = 2u,   // draining in-flight bulk copies gave up
+  QLA_DEVERR_BAD_INDEX = 4u,      // an index stream entry was out of range
+  QLA_DEVERR_MFUNC_NOCONV = 8u,   // an iterative matrix function hit its cap
+};
+
+// The error word lives in device memory owned by the runtime (one per
+// device); kernels receive its address with their parameters.
+__device__ __forceinline__ void raise_dev_error(unsigned* err, unsigned bits) {
+  if (err) atomicOr(err, bits);
+}
+
+// ---------------------------------------------------------------------------
+// explicitly rounded scalar arithmetic (no FMA contraction)
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+
+template <typename R>
+struct Cx {
+  R re, im;
+};
+
+// eqop codes shared with the host: eq, peq, meq, eqm
+enum Eqop : int { EQ = 0, PEQ = 1, MEQ = 2, EQM = 3 };
+
+// x (+|-)= a*b with the conjugation pattern (ca, cb); restates
+// qla_complex.h:330-333 (c_peq_c_times_c), 386-389 (ca_times_c),
+// 366-369 (c_times_ca), 347-350 (ca_times_ca) and their meq forms.
+template <bool CA, bool CB, typename R>
+__device__ __forceinline__ void cmac(Cx<R>& x, bool minus, Cx<R> a, Cx<R> b) {
+  R re, im;
+  if (!CA && !CB) {
+    re = rsub(rmul(a.re, b.re), rmul(a.im, b.im));
+    im = radd(rmul(a.re, b.im), rmul(a.im, b.re));
+  } else if (CA && !CB) {
+    re = radd(rmul(a.re, b.re), rmul(a.im, b.im));
+    im = rsub(rmul(a.re, b.im), rmul(a.im, b.re));
+  } else if (!CA && CB) {
+    re = radd(rmul(a.re, b.re), rmul(a.im, b.im));
+    im = rsub(rmul(a.im, b.re), rmul(a.re, b.im));
+  } else {
+    re = rsub(rmul(a.re, b.re), rmul(a.im, b.im));
+    im = rsub(rmul(-a.re, b.im), rmul(a.im, b.re));
+  }
+  if (minus) {
+    x.re = rsub(x.re, re);
+    x.im = rsub(x.im, im);
+  } else {
+    x.re = radd(x.re, re);
+    x.im = radd(x.im, im);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// record movement.  A record of N complex numbers of type R lives at an
+// address aligned to sizeof(Cx<R>) (8 B for float, 16 B for double).
+template <typename R, int N>
+__device__ __forceinline__ void load_rec(Cx<R> (&x)[N], const void* p) {
+  if constexpr (sizeof(R) == 4) {
+    const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      float2 v = q[e];
+      x[e].re = v.x;
+      x[e].im = v.y;
+    }
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      double2 v = q[e];
+      x[e].re = v.x;
+      x[e].im = v.y;
+    }
+  }
+}
+
+// read-only global load (the input fields are never written by the kernel)
+template <typename R, int N>
+__device__ __forceinline__ void load_rec_global(Cx<R> (&x)[N], const void* p) {
+  if constexpr (sizeof(R) == 4) {
+    const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      float2 v = __ldg(q + e);
+      x[e].re = v.x;
+      x[e].im = v.y;
+    }
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      double2 v = __ldg(q + e);
+      x[e].re = v.x;
+      x[e].im = v.y;
+    }
+  }
+}
+
+// plain global load (used where the record may alias the output, i.e. the
+// destination of a peq/meq update)
+template <typename R, int N>
+__device__ __forceinline__ void load_rec_rw(Cx<R> (&x)[N], const void* p) {
+  load_rec<R, N>(x, p);
+}
+
+template <typename R, int N>
+__device__ __forceinline__ void store_rec(void* p, const Cx<R> (&x)[N]) {
+  if constexpr (sizeof(R) == 4) {
+    float2* q = reinterpret_cast<float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) q[e] = make_float2(x[e].re, x[e].im);
+  } else {
+    double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) q[e] = make_double2(x[e].re, x[e].im);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sm_90+/sm_100a asynchronous-copy primitives (inline PTX).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Time-bounded wait on an mbarrier phase: gives up after ~limit_ns and
+// records QLA_DEVERR_MBAR_TIMEOUT.  Returns false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err,
+                                                  uint64_t limit_ns = 2000000000ull) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 30); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63u) == 0 && global_ns() - t0 > limit_ns) break;
+  }
+  raise_dev_error(err, QLA_DEVERR_MBAR_TIMEOUT);
+  return false;
+}
+
+// 1-D bulk copy global -> shared, completion signalled on an mbarrier.
+// Requires 16-B aligned addresses and a size that is a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar,
+                                        uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+      "%4;" ::"r"(smem_addr(dst_smem)),
+      "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+      : "memory");
+}
+
+// 1-D bulk copy shared -> global, tracked by the issuing thread's bulk groups.
+__device__ __forceinline__ void bulk_s2g(void* dst_gmem, const void* src_smem, uint32_t bytes, uint64_t policy) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;" ::"l"(dst_gmem),
+               "r"(smem_addr(src_smem)), "r"(bytes), "l"(policy)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// L2 eviction policies for streamed data (read once / written once).
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// double-double accumulation (Knuth TwoSum) for the global reductions.
+struct DD {
+  double hi, lo;
+};
+
+__device__ __forceinline__ void dd_add(DD& s, double x) {
+  double t = __dadd_rn(s.hi, x);
+  double bp = __dsub_rn(t, s.hi);
+  double err = __dadd_rn(__dsub_rn(s.hi, __dsub_rn(t, bp)), __dsub_rn(x, bp));
+  s.hi = t;
+  s.lo = __dadd_rn(s.lo, err);
+}
+
+__device__ __forceinline__ void dd_merge(DD& s, const DD& o) {
+  dd_add(s, o.hi);
+  s.lo = __dadd_rn(s.lo, o.lo);
+}
+
+__device__ __forceinline__ DD dd_shfl_xor(const DD& v, int lane_mask) {
+  DD o;
+  o.hi = __shfl_xor_sync(0xffffffffu, v.hi, lane_mask);
+  o.lo = __shfl_xor_sync(0xffffffffu, v.lo, lane_mask);
+  return o;
+}
+
+}  // namespace qlab

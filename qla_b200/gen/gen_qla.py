@@ -1,0 +1,324 @@
+#!/usr/bin/env python3
+"""Generator of the QLA B200 C-ABI: the QLA level-1 entry points for the hot
+families, as extern "C" wrappers over the CUDA engine, plus their prototypes.
+
+It replaces the reference's Perl generator (lib/perl/build_qla.pl) for the
+site-loop families on the B200 path.  Where build_qla.pl walks every
+(operation x eqop x datatype x indexing variant) and writes one C loop per
+combination (build_qla.pl:186-2705, prototype.pl:450 make_prototype), this
+generator walks the same combinations for the hot families and writes one
+short wrapper per combination that picks a compiled engine OP; the loop body
+itself lives once per family in qla_b200/csrc/qla_ops.cuh.
+
+Naming follows the reference (doc/qla.tex:390-627, prototype.pl:450-520):
+  QLA_<PC>_<dest>_<v|x><eqop>_<args>   with eqop in eq, peq, meq, eqm,
+  `p` before an operand for an array of pointers, a trailing `int *index` for
+  the gang-indexed `x` variants (indirection.pl:66-101), scalars passed by
+  pointer.  The per-operand index forms `..._times_xV(r, a, b, int *jb, n)` are
+  documented by the reference (doc/qla.tex:476-487, variant 5) but not
+  generated there; they are the int32 neighbour-gather form of `pV`.
+
+Outputs (all written by this script, committed):
+  include/qla_b200_<pc>.h               prototypes, each citing what it replaces
+  qla_b200/csrc/gen/<pc>_<family>.cu    wrappers (split per family to compile in parallel)
+  qla_b200/gen/api_manifest.json        every symbol with its family and argument kinds
+"""
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+OUT_INC = os.path.join(REPO, "include")
+OUT_CU = os.path.join(REPO, "qla_b200", "csrc", "gen")
+
+EQOPS = ["eq", "peq", "meq", "eqm"]
+EQ_ENUM = {"eq": "qlab::EQ", "peq": "qlab::PEQ", "meq": "qlab::MEQ", "eqm": "qlab::EQM"}
+# record abbreviation -> (type name, columns per colour row, complex per record at Nc=3)
+REC = {"V": ("ColorVector", 1, 3), "H": ("HalfFermion", 2, 6), "D": ("DiracFermion", 4, 12),
+       "M": ("ColorMatrix", 3, 9)}
+FIELD_TYPES = ["V", "H", "D", "M"]
+
+# citations into the reference generator for each family
+CITE = {
+    "lmult": "lib/perl/build_qla.pl:1588-1622 (left multiplication by a colour matrix), "
+             "expressions_tensor.pl:766",
+    "lmult_x": "doc/qla.tex:476-487 (per-operand index variant 5, not generated by the reference)",
+    "spproj": "lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275",
+    "sprecon": "lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337",
+    "rtimes": "lib/perl/build_qla.pl:1256-1292 (real constant times field)",
+    "copy": "lib/perl/build_qla.pl:370-400 (assignment / gather)",
+    "copy_x": "doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)",
+    "norm2": "lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)",
+    "dot": "lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)",
+    "redot": "lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)",
+}
+
+
+class Fn:
+    def __init__(self, name, params, body, family, cite, kinds):
+        self.name = name
+        self.params = params    # list of (ctype, name)
+        self.body = body
+        self.family = family
+        self.cite = cite
+        self.kinds = kinds      # argument kinds for the Python mirror / tests
+
+    def proto(self, restrict):
+        ps = ", ".join(t.replace("RESTRICT", restrict) + " " + n for t, n in self.params)
+        return f"void {self.name}({ps})"
+
+
+def ptype(pc, t):
+    return f"QLA_{pc}_{REC[t][0]}"
+
+
+def operand(pc, t, ptr, argname, restrict="RESTRICT"):
+    """C parameter and engine operand descriptor for a field operand."""
+    ct = ptype(pc, t)
+    if ptr:
+        return (f"{ct} *RESTRICT *", argname), f"qlab::op_ptr((const void* const*){argname})"
+    return (f"{ct} *RESTRICT", argname), f"qlab::op_contig({argname})"
+
+
+def gen_pc(pc, R, P):
+    """Generate the hot families for colour-3 precision pc (F3/D3)."""
+    fns = []
+    kid = lambda fam: f'"{pc}_{fam}"'
+    # ---- left multiplication by a colour matrix
+    for T in FIELD_TYPES:
+        ncol = REC[T][1]
+        src2s = [(T, False), ("p" + T, True)]
+        if T == "M":
+            src2s += [("Ma", False), ("pMa", True)]
+        for var in ["v", "x"]:
+            for eq in EQOPS:
+                for s1 in ["M", "Ma", "pM", "pMa"]:
+                    adja = "a" in s1[-1:]
+                    p1 = s1.startswith("p")
+                    for s2name, p2 in src2s:
+                        adjb = s2name.endswith("a")
+                        name = f"QLA_{pc}_{T}_{var}{eq}_{s1}_times_{s2name}"
+                        pr = (f"{ptype(pc, T)} *RESTRICT", "r")
+                        pa, oa = operand(pc, "M", p1, "a")
+                        pb, ob = operand(pc, T, p2, "b")
+                        params = [pr, pa, pb]
+                        gang = "nullptr"
+                        if var == "x":
+                            params.append(("int *", "index"))
+                            gang = "index"
+                        params.append(("int", "n"))
+                        op = f"qlab::LMultOp<{R}, 3, {ncol}, {str(adja).lower()}, {str(adjb).lower()}>"
+                        body = (f"qlab::api_map<{op}>({kid('lmult_' + T + str(int(adja)) + str(int(adjb)))}, r, "
+                                f"{oa}, {ob}, {gang}, n, {EQ_ENUM[eq]});")
+                        fns.append(Fn(name, params, body, "lmult", CITE["lmult"],
+                                      dict(dest=T, eqop=eq, var=var, a=s1, b=s2name)))
+            # per-operand int32 index on the field operand (doc variant 5)
+        for eq in EQOPS:
+            for s1 in ["M", "Ma"]:
+                adja = s1 == "Ma"
+                name = f"QLA_{pc}_{T}_{eq}_{s1}_times_x{T}"
+                params = [(f"{ptype(pc, T)} *RESTRICT", "r"), (f"{ptype(pc, 'M')} *RESTRICT", "a"),
+                          (f"{ptype(pc, T)} *RESTRICT", "b"), ("int *", "jb"), ("int", "n")]
+                op = f"qlab::LMultOp<{R}, 3, {ncol}, {str(adja).lower()}, false>"
+                body = (f"qlab::api_map<{op}>({kid('lmult_' + T + str(int(adja)) + '0')}, r, qlab::op_contig(a), "
+                        f"qlab::op_idx(b, jb), nullptr, n, {EQ_ENUM[eq]});")
+                fns.append(Fn(name, params, body, "lmult", CITE["lmult_x"],
+                              dict(dest=T, eqop=eq, var="xb", a=s1, b="x" + T)))
+    # ---- spin projection / reconstruction
+    for var in ["v", "x"]:
+        for eq in EQOPS:
+            for src, p1 in [("D", False), ("pD", True)]:
+                name = f"QLA_{pc}_H_{var}{eq}_spproj_{src}"
+                pa, oa = operand(pc, "D", p1, "a")
+                params = [(f"{ptype(pc, 'H')} *RESTRICT", "r"), pa, ("int", "mu"), ("int", "sign")]
+                gang = "nullptr"
+                if var == "x":
+                    params.append(("int *", "index"))
+                    gang = "index"
+                params.append(("int", "n"))
+                body = ("if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */\n  "
+                        f"qlab::api_map<qlab::SpprojOp<{R}, 3>>({kid('spproj')}, r, {oa}, qlab::Opnd{{}}, {gang}, n, "
+                        f"{EQ_ENUM[eq]}, mu, sign);")
+                fns.append(Fn(name, params, body, "spproj", CITE["spproj"], dict(eqop=eq, var=var, a=src)))
+            for src, p1 in [("H", False), ("pH", True)]:
+                name = f"QLA_{pc}_D_{var}{eq}_sprecon_{src}"
+                pa, oa = operand(pc, "H", p1, "a")
+                params = [(f"{ptype(pc, 'D')} *RESTRICT", "r"), pa, ("int", "mu"), ("int", "sign")]
+                gang = "nullptr"
+                if var == "x":
+                    params.append(("int *", "index"))
+                    gang = "index"
+                params.append(("int", "n"))
+                body = ("if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */\n  "
+                        f"qlab::api_map<qlab::SpreconOp<{R}, 3>>({kid('sprecon')}, r, {oa}, qlab::Opnd{{}}, {gang}, "
+                        f"n, {EQ_ENUM[eq]}, mu, sign);")
+                fns.append(Fn(name, params, body, "sprecon", CITE["sprecon"], dict(eqop=eq, var=var, a=src)))
+    # ---- real constant times field, copies / gathers
+    for T in FIELD_TYPES:
+        nc = REC[T][2]
+        for var in ["v", "x"]:
+            for eq in EQOPS:
+                for src, p1 in [(T, False), ("p" + T, True)]:
+                    name = f"QLA_{pc}_{T}_{var}{eq}_r_times_{src}"
+                    pb, ob = operand(pc, T, p1, "b")
+                    params = [(f"{ptype(pc, T)} *RESTRICT", "r"), (f"QLA_{P}_Real *RESTRICT", "a"), pb]
+                    gang = "nullptr"
+                    if var == "x":
+                        params.append(("int *", "index"))
+                        gang = "index"
+                    params.append(("int", "n"))
+                    body = (f"qlab::api_scalar_map<qlab::RTimesOp<{R}, {nc}>, {R}>({kid('rtimes_' + T)}, r, a, {ob}, "
+                            f"{gang}, n, {EQ_ENUM[eq]});")
+                    fns.append(Fn(name, params, body, "rtimes", CITE["rtimes"],
+                                  dict(dest=T, eqop=eq, var=var, b=src)))
+                    name = f"QLA_{pc}_{T}_{var}{eq}_{src}"
+                    pa, oa = operand(pc, T, p1, "a")
+                    params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa]
+                    if var == "x":
+                        params.append(("int *", "index"))
+                    params.append(("int", "n"))
+                    body = (f"qlab::api_map<qlab::CopyOp<{R}, {nc}>>({kid('copy_' + T)}, r, {oa}, qlab::Opnd{{}}, "
+                            f"{gang}, n, {EQ_ENUM[eq]});")
+                    fns.append(Fn(name, params, body, "copy", CITE["copy"], dict(dest=T, eqop=eq, var=var, a=src)))
+        for eq in EQOPS:
+            name = f"QLA_{pc}_{T}_{eq}_x{T}"
+            params = [(f"{ptype(pc, T)} *RESTRICT", "r"), (f"{ptype(pc, T)} *RESTRICT", "a"), ("int *", "ja"),
+                      ("int", "n")]
+            body = (f"qlab::api_map<qlab::CopyOp<{R}, {nc}>>({kid('copy_' + T)}, r, qlab::op_idx(a, ja), "
+                    f"qlab::Opnd{{}}, nullptr, n, {EQ_ENUM[eq]});")
+            fns.append(Fn(name, params, body, "copy", CITE["copy_x"], dict(dest=T, eqop=eq, var="xa", a="x" + T)))
+    # ---- global reductions
+    red_pcs = [(pc, R, P)]
+    if pc == "F3":
+        red_pcs.append(("DF3", "float", "D"))
+    for rpc, RR, OP in red_pcs:
+        outR = "float" if rpc == "F3" else "double"
+        for T in FIELD_TYPES:
+            nc = REC[T][2]
+            for var in ["v", "x"]:
+                gang = "index" if var == "x" else "nullptr"
+                for src, p1 in [(T, False), ("p" + T, True)]:
+                    name = f"QLA_{rpc}_r_{var}eq_norm2_{src}"
+                    pa, oa = operand(pc, T, p1, "a")
+                    params = [(f"QLA_{OP}_Real *RESTRICT", "r"), pa]
+                    if var == "x":
+                        params.append(("int *", "index"))
+                    params.append(("int", "n"))
+                    body = (f"qlab::api_reduce<qlab::Norm2Op<{RR}, {nc}, {outR}>>({kid('norm2_' + T)}, r, "
+                            f"sizeof({outR}), {oa}, qlab::Opnd{{}}, {gang}, n);")
+                    fns.append(Fn(name, params, body, "norm2", CITE["norm2"], dict(dest="r", var=var, a=src,
+                                                                                    out=outR)))
+                for sa, pa_ in [(T, False), ("p" + T, True)]:
+                    for sb, pb_ in [(T, False), ("p" + T, True)]:
+                        name = f"QLA_{rpc}_c_{var}eq_{sa}_dot_{sb}"
+                        pa, oa = operand(pc, T, pa_, "a")
+                        pb, ob = operand(pc, T, pb_, "b")
+                        params = [(f"QLA_{OP}_Complex *RESTRICT", "r"), pa, pb]
+                        if var == "x":
+                            params.append(("int *", "index"))
+                        params.append(("int", "n"))
+                        body = (f"qlab::api_reduce<qlab::DotOp<{RR}, {nc}, {outR}>>({kid('dot_' + T)}, r, "
+                                f"2 * sizeof({outR}), {oa}, {ob}, {gang}, n);")
+                        fns.append(Fn(name, params, body, "dot", CITE["dot"],
+                                      dict(dest="c", var=var, a=sa, b=sb, out=outR)))
+                        if rpc == "DF3":
+                            continue  # the reference's DF libraries carry no re_dot
+                        name = f"QLA_{rpc}_r_{var}eq_re_{sa}_dot_{sb}"
+                        params = [(f"QLA_{OP}_Real *RESTRICT", "r"), pa, pb]
+                        if var == "x":
+                            params.append(("int *", "index"))
+                        params.append(("int", "n"))
+                        body = (f"qlab::api_reduce<qlab::ReDotOp<{RR}, {nc}, {outR}>>({kid('redot_' + T)}, r, "
+                                f"sizeof({outR}), {oa}, {ob}, {gang}, n);")
+                        fns.append(Fn(name, params, body, "redot", CITE["redot"],
+                                      dict(dest="r", var=var, a=sa, b=sb, out=outR)))
+    return fns
+
+
+HEADER_TOP = """/*
+ * {fname} -- GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+ *
+ * QLA {pc} level-1 entry points implemented by libqla_b200.so (sm_100a).
+ * Each declaration replaces the reference function of the same name, whose
+ * C loop the reference generator emits from the cited section.  Array
+ * arguments are device pointers; see qla_b200_runtime.h for scalars,
+ * reduction outputs, streams and errors.
+ */
+#ifndef {guard}
+#define {guard}
+#include "qla_b200_types.h"
+
+#ifdef __cplusplus
+#define QLA_B200_RESTRICT __restrict__
+extern "C" {{
+#else
+#define QLA_B200_RESTRICT restrict
+#endif
+
+"""
+
+HEADER_END = """
+#ifdef __cplusplus
+}
+#endif
+#endif
+"""
+
+CU_TOP = """// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA {pc} {family} entry points (extern "C"), reference: {cite}
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+
+extern "C" {{
+"""
+
+
+def write_if_changed(path, text):
+    if os.path.exists(path):
+        with open(path) as f:
+            if f.read() == text:
+                return False
+    with open(path, "w") as f:
+        f.write(text)
+    return True
+
+
+def main():
+    os.makedirs(OUT_CU, exist_ok=True)
+    manifest = []
+    groups = {}
+    headers = {}
+    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D")]:
+        for fn in gen_pc(pc, R, P):
+            hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
+            headers.setdefault(hpc, []).append(fn)
+            groups.setdefault((pc, fn.family), []).append(fn)
+            manifest.append(dict(name=fn.name, pc=hpc, family=fn.family, params=[n for _, n in fn.params],
+                                 ctypes=[t.replace("RESTRICT", "").strip() for t, _ in fn.params], **fn.kinds))
+    written = 0
+    for hpc, fns in headers.items():
+        fname = f"qla_b200_{hpc.lower()}.h"
+        text = HEADER_TOP.format(fname=fname, pc=hpc, guard=f"QLA_B200_{hpc}_H")
+        fam = None
+        for fn in fns:
+            if fn.family != fam:
+                fam = fn.family
+                text += f"/* ---- {fam}: replaces the {hpc} functions emitted by {fn.cite.split(',')[0]} */\n"
+            text += f"/* replaces {fn.name} ({fn.cite}) */\n"
+            text += fn.proto("QLA_B200_RESTRICT") + ";\n"
+        text += HEADER_END
+        written += write_if_changed(os.path.join(OUT_INC, fname), text)
+    for (pc, family), fns in groups.items():
+        text = CU_TOP.format(pc=pc, family=family, cite=CITE[family])
+        for fn in fns:
+            text += "QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  " + fn.body + "\n}\n\n"
+        text += "}  // extern \"C\"\n"
+        written += write_if_changed(os.path.join(OUT_CU, f"{pc.lower()}_{family}.cu"), text)
+    mtext = json.dumps(manifest, indent=0, sort_keys=True)
+    written += write_if_changed(os.path.join(HERE, "api_manifest.json"), mtext)
+    print(f"gen_qla: {len(manifest)} entry points, {written} files updated", file=sys.stderr)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+#!/usr/bin/env python3
+"""Writes the golden vectors of the QLA hot path by running the REFERENCE
+library itself (oracle/_ref/libqla_ref.so, built from the reference's own
+generator by oracle/build_ref.sh) on seeded inputs.
+
+QLA ships no golden data (its tests compare the library against itself,
+test/src/protocol_tensor_sng.m4, protocol_idx.m4), so these fixtures are the
+reference's outputs recorded here.  Run with OMP_NUM_THREADS=1 so the
+reductions use the serial summation order:
+
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+
+Output: tests/golden/qla_<pc>_golden.npz  (inputs, index tables, outputs)
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import qla_testlib as T  # noqa: E402
+
+N = 37      # destination sites
+NS = 41     # source records (gathers index into these)
+EQOPS = ["eq", "peq", "meq", "eqm"]
+
+
+def build(pc, dt, seed):
+    rng = np.random.default_rng(seed)
+    R = T.ref()
+    P = pc[0]
+    ins = {
+        "M": T.haar_su3(rng, NS, dt),
+        "M2": T.haar_su3(rng, NS, dt),
+        "V": T.gaussian_field(rng, NS, 3, dt),
+        "H": T.gaussian_field(rng, NS, 6, dt),
+        "D": T.gaussian_field(rng, NS, 12, dt),
+        "D2": T.gaussian_field(rng, NS, 12, dt),
+        "r0V": T.gaussian_field(rng, N, 3, dt),
+        "r0H": T.gaussian_field(rng, N, 6, dt),
+        "r0D": T.gaussian_field(rng, N, 12, dt),
+        "r0M": T.gaussian_field(rng, N, 9, dt),
+        "idx": rng.integers(0, NS, N).astype(np.int32),
+        "gang": rng.permutation(N).astype(np.int32),
+        "scal": np.array([-0.6181], dtype=dt),
+    }
+    out = {}
+    recb = 8 if dt == np.float32 else 16
+
+    def parr(arr, idx, ncplx):
+        base = arr.ctypes.data
+        return (ctypes.c_void_p * len(idx))(*[base + int(j) * ncplx * recb for j in idx])
+
+    def call(name, *args):
+        getattr(R, name)(*args)
+
+    # left multiplication (all eqops, adjoints, pointer and gang variants on V;
+    # a representative set on H, D, M)
+    for dest, nc in (("V", 3), ("H", 6), ("D", 12), ("M", 9)):
+        for eq in EQOPS:
+            for s1 in ("M", "Ma", "pM", "pMa"):
+                for s2 in (dest, "p" + dest) + (("Ma", "pMa") if dest == "M" else ()):
+                    if dest != "V" and eq not in ("eq", "peq"):
+                        continue
+                    for var in ("v", "x"):
+                        name = f"QLA_{pc}_{dest}_{var}{eq}_{s1}_times_{s2}"
+                        r = ins["r0" + dest][:N].copy() if dest != "M" else ins["r0M"].copy()
+                        a = parr(ins["M"], ins["idx"], 9) if s1.startswith("p") else ins["M"].ctypes.data
+                        bsrc = ins["M2"] if dest == "M" else ins[dest]
+                        b = parr(bsrc, ins["idx"][::-1].copy(), nc) if s2.startswith("p") else bsrc.ctypes.data
+                        args = [ctypes.c_void_p(r.ctypes.data), a if s1.startswith("p") else ctypes.c_void_p(a),
+                                b if s2.startswith("p") else ctypes.c_void_p(b)]
+                        if var == "x":
+                            args.append(ctypes.c_void_p(ins["gang"].ctypes.data))
+                        args.append(N)
+                        call(name, *args)
+                        out[name] = r
+    # spin projection / reconstruction, every mu and sign
+    for eq in EQOPS:
+        for mu in range(6):
+            for sign in (1, -1):
+                r = ins["r0H"].copy()
+                call(f"QLA_{pc}_H_v{eq}_spproj_D", ctypes.c_void_p(r.ctypes.data),
+                     ctypes.c_void_p(ins["D"].ctypes.data), mu, sign, N)
+                out[f"QLA_{pc}_H_v{eq}_spproj_D|{mu}|{sign}"] = r
+                r = ins["r0D"].copy()
+                call(f"QLA_{pc}_D_v{eq}_sprecon_H", ctypes.c_void_p(r.ctypes.data),
+                     ctypes.c_void_p(ins["H"].ctypes.data), mu, sign, N)
+                out[f"QLA_{pc}_D_v{eq}_sprecon_H|{mu}|{sign}"] = r
+        r = ins["r0H"].copy()
+        call(f"QLA_{pc}_H_x{eq}_spproj_pD", ctypes.c_void_p(r.ctypes.data), parr(ins["D"], ins["idx"], 12), 2, -1,
+             ctypes.c_void_p(ins["gang"].ctypes.data), N)
+        out[f"QLA_{pc}_H_x{eq}_spproj_pD|2|-1"] = r
+    # real constant times field
+    sc = (ctypes.c_float if dt == np.float32 else ctypes.c_double)(float(ins["scal"][0]))
+    for dest, nc in (("V", 3), ("D", 12), ("M", 9)):
+        for eq in EQOPS:
+            r = ins["r0" + dest].copy()
+            call(f"QLA_{pc}_{dest}_v{eq}_r_times_{dest}", ctypes.c_void_p(r.ctypes.data), ctypes.byref(sc),
+                 ctypes.c_void_p(ins[dest if dest != "M" else "M2"].ctypes.data), N)
+            out[f"QLA_{pc}_{dest}_v{eq}_r_times_{dest}"] = r
+    # reductions
+    rpcs = [(pc, dt)] + ([("DF3", np.float64)] if pc == "F3" else [])
+    for rpc, odt in rpcs:
+        for t, nc in (("V", 3), ("H", 6), ("D", 12), ("M", 9)):
+            src = ins[t]
+            o = np.zeros(1, dtype=odt)
+            call(f"QLA_{rpc}_r_veq_norm2_{t}", ctypes.c_void_p(o.ctypes.data), ctypes.c_void_p(src.ctypes.data), N)
+            out[f"QLA_{rpc}_r_veq_norm2_{t}"] = o
+            o = np.zeros(1, dtype=odt)
+            call(f"QLA_{rpc}_r_xeq_norm2_p{t}", ctypes.c_void_p(o.ctypes.data), parr(src, ins["idx"], nc),
+                 ctypes.c_void_p(ins["gang"].ctypes.data), N)
+            out[f"QLA_{rpc}_r_xeq_norm2_p{t}"] = o
+            o = np.zeros(2, dtype=odt)
+            b = ins["D2"] if t == "D" else ins["M2"] if t == "M" else ins["r0" + t]
+            call(f"QLA_{rpc}_c_veq_{t}_dot_{t}", ctypes.c_void_p(o.ctypes.data), ctypes.c_void_p(src.ctypes.data),
+                 ctypes.c_void_p(b.ctypes.data), N)
+            out[f"QLA_{rpc}_c_veq_{t}_dot_{t}"] = o
+            if rpc != "DF3":
+                o = np.zeros(1, dtype=odt)
+                call(f"QLA_{rpc}_r_veq_re_{t}_dot_{t}", ctypes.c_void_p(o.ctypes.data),
+                     ctypes.c_void_p(src.ctypes.data), ctypes.c_void_p(b.ctypes.data), N)
+                out[f"QLA_{rpc}_r_veq_re_{t}_dot_{t}"] = o
+    return ins, out
+
+
+def main():
+    if os.environ.get("OMP_NUM_THREADS") != "1":
+        sys.exit("run with OMP_NUM_THREADS=1 (serial reference summation order)")
+    if not T.ref_available():
+        sys.exit("oracle/_ref/libqla_ref.so missing: run sh oracle/build_ref.sh")
+    for pc, dt, seed in (("F3", np.float32, 101), ("D3", np.float64, 202)):
+        ins, out = build(pc, dt, seed)
+        blob = {"in__" + k: v for k, v in ins.items()}
+        blob.update({"out__" + k: v for k, v in out.items()})
+        path = os.path.join(HERE, f"qla_{pc.lower()}_golden.npz")
+        np.savez_compressed(path, **blob)
+        print(f"{path}: {len(out)} reference outputs")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+"""Test-side helpers: seeded lattice inputs and ctypes bindings of the checkers.
+
+The checkers are the oracle (oracle/liboracle.so, a CPU restatement of the
+reference algorithms) and, when it has been built, the reference library
+itself (oracle/_ref/libqla_ref.so).  Nothing in the product imports this file.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(REPO, "oracle", "liboracle.so")
+REF_SO = os.path.join(REPO, "oracle", "_ref", "libqla_ref.so")
+
+EQOPS = {"eq": 0, "peq": 1, "meq": 2, "eqm": 3}
+# complex numbers per record for Nc=3 (include/qla_types.h:29-33)
+NCPLX3 = {"V": 3, "H": 6, "D": 12, "M": 9}
+NCOL3 = {"V": 1, "H": 2, "D": 4, "M": 3}
+
+_oracle = None
+_ref = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle/liboracle.so not built (run make -C oracle)")
+        _oracle = ctypes.CDLL(ORACLE_SO)
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)
+    return _ref
+
+
+def ptr(a):
+    """ctypes void pointer to a numpy array (None for None)."""
+    if a is None:
+        return None
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def rtype(dtype):
+    return "f" if np.dtype(dtype) == np.float32 else "d"
+
+
+# ---------------------------------------------------------------------------
+# seeded inputs
+
+def gaussian_field(rng, n, ncplx, dtype=np.float32):
+    """n records of ncplx complex numbers with i.i.d. N(0,1) real/imag parts,
+    as a flat real array of shape (n, 2*ncplx)."""
+    return rng.standard_normal((n, 2 * ncplx)).astype(dtype)
+
+
+def haar_su3(rng, n, dtype=np.float32, nc=3):
+    """n Haar-random SU(nc) matrices: complex Gaussian, QR (Gram-Schmidt via
+    numpy's Householder QR), diagonal phase fix, det normalised to 1.
+    Returned as (n, 2*nc*nc) real array in [ic][jc] complex order."""
+    z = (rng.standard_normal((n, nc, nc)) + 1j * rng.standard_normal((n, nc, nc))) / np.sqrt(2)
+    q, r = np.linalg.qr(z)
+    d = np.diagonal(r, axis1=1, axis2=2)
+    ph = d / np.abs(d)
+    q = q * ph[:, None, :]
+    det = np.linalg.det(q)
+    q = q / (det ** (1.0 / nc))[:, None, None]
+    out = np.empty((n, nc * nc, 2), dtype=np.float64)
+    out[..., 0] = q.reshape(n, -1).real
+    out[..., 1] = q.reshape(n, -1).imag
+    return out.reshape(n, 2 * nc * nc).astype(dtype)
+
+
+def lattice_dims_volume(dims):
+    v = 1
+    for d in dims:
+        v *= d
+    return v
+
+
+def shift_index(dims, mu, sign):
+    """Periodic neighbour table: idx[i] = site at x + sign*e_mu, lexicographic
+    i = x0 + L0*(x1 + L1*(x2 + L2*x3))."""
+    dims = list(dims)
+    coords = np.indices(dims[::-1]).reshape(len(dims), -1)[::-1]  # coords[d][i]
+    c = coords.copy()
+    c[mu] = (c[mu] + sign) % dims[mu]
+    idx = np.zeros(c.shape[1], dtype=np.int64)
+    stride = 1
+    for d in range(len(dims)):
+        idx += c[d] * stride
+        stride *= dims[d]
+    return idx.astype(np.int32)
+
+
+# ---------------------------------------------------------------------------
+# oracle wrappers (numpy in, numpy out)
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def ora_lmult(r, a, b, n, ncol, eqop, adja=0, adjb=0, idx_a=None, idx_b=None, gang=None, nc=3):
+    t = rtype(r.dtype)
+    f = getattr(oracle(), "ora_lmult_" + t)
+    idx_a, idx_b, gang = _i32(idx_a), _i32(idx_b), _i32(gang)
+    f(ptr(r), ptr(a), ptr(b), ctypes.c_long(n), nc, ncol, EQOPS.get(eqop, eqop), adja, adjb,
+      ptr(idx_a), ptr(idx_b), ptr(gang))
+    return r
+
+
+def ora_spproj(r, a, n, mu, sign, eqop, idx_a=None, gang=None, nc=3):
+    f = getattr(oracle(), "ora_spproj_" + rtype(r.dtype))
+    idx_a, gang = _i32(idx_a), _i32(gang)
+    f(ptr(r), ptr(a), ctypes.c_long(n), nc, mu, sign, EQOPS.get(eqop, eqop), ptr(idx_a), ptr(gang))
+    return r
+
+
+def ora_sprecon(r, a, n, mu, sign, eqop, idx_a=None, gang=None, nc=3):
+    f = getattr(oracle(), "ora_sprecon_" + rtype(r.dtype))
+    idx_a, gang = _i32(idx_a), _i32(gang)
+    f(ptr(r), ptr(a), ctypes.c_long(n), nc, mu, sign, EQOPS.get(eqop, eqop), ptr(idx_a), ptr(gang))
+    return r
+
+
+def ora_rtimes(r, s, b, n, ncplx, eqop, idx_b=None, gang=None):
+    t = rtype(r.dtype)
+    f = getattr(oracle(), "ora_rtimes_" + t)
+    cs = ctypes.c_float(s) if t == "f" else ctypes.c_double(s)
+    idx_b, gang = _i32(idx_b), _i32(gang)
+    f(ptr(r), cs, ptr(b), ctypes.c_long(n), ncplx, EQOPS.get(eqop, eqop), ptr(idx_b), ptr(gang))
+    return r
+
+
+def ora_norm2(a, n, ncplx, exact=False, idx_a=None, gang=None):
+    t = rtype(a.dtype)
+    f = getattr(oracle(), ("ora_norm2_exact_" if exact else "ora_norm2_ref_") + t)
+    f.restype = ctypes.c_double
+    idx_a, gang = _i32(idx_a), _i32(gang)
+    return f(ptr(a), ctypes.c_long(n), ncplx, ptr(idx_a), ptr(gang))
+
+
+def ora_dot(a, b, n, ncplx, exact=False, idx_a=None, idx_b=None, gang=None):
+    t = rtype(a.dtype)
+    f = getattr(oracle(), ("ora_dot_exact_" if exact else "ora_dot_ref_") + t)
+    out = np.zeros(2, dtype=np.float64)
+    idx_a, idx_b, gang = _i32(idx_a), _i32(idx_b), _i32(gang)
+    f(ptr(out), ptr(a), ptr(b), ctypes.c_long(n), ncplx, ptr(idx_a), ptr(idx_b), ptr(gang))
+    return complex(out[0], out[1])
+
+
+# ---------------------------------------------------------------------------
+# tolerance rule of the reference test-suite (test/src/compare.h:10-25,
+# protocol_compare.m4:80-91): an element fails only if its absolute difference
+# exceeds NABS*eps AND its relative difference exceeds NREL*eps.
+
+def qla_close(a, b, dtype, nabs=16, nrel=10):
+    eps = np.finfo(dtype).eps
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    diff = np.abs(a - b)
+    scale = np.maximum(np.abs(a), np.abs(b))
+    rel = np.where(scale > 0, diff / np.where(scale > 0, scale, 1), 0)
+    bad = (diff > nabs * eps) & (rel > nrel * eps)
+    return not bool(np.any(bad)), int(np.count_nonzero(bad))
+
+
+# ---------------------------------------------------------------------------
+# device helpers (torch is imported lazily so CPU-only tests never need CUDA)
+
+def to_dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def to_host(t):
+    return t.detach().cpu().numpy()
+
+
+def ptr_array(base_t, idx, rec_bytes):
+    """Device array of device pointers &base[idx[k]] (the `pX` argument form)."""
+    import torch
+    addrs = base_t.data_ptr() + idx.astype(np.int64) * rec_bytes
+    return torch.from_numpy(addrs).cuda()
+
+
+def bits_equal(a, b):
+    """Bit-exact equality of two float arrays (treating +0 and -0 as equal,
+    NaNs must agree in position)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    return bool(np.array_equal(a, b, equal_nan=True))

@@ -1,0 +1,139 @@
+"""Pins the oracle (oracle/liboracle.so, the CPU restatement) to the reference:
+
+1. against the golden vectors in tests/golden/ (outputs of the reference
+   library itself, written by tests/golden/make_golden.py) -- always runs;
+2. against the reference library directly on larger seeded inputs, when
+   oracle/_ref/libqla_ref.so has been built here.
+
+Linear ops and the reference-order reductions must be bit-identical."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import qla_testlib as T
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+NC = {"V": 3, "H": 6, "D": 12, "M": 9}
+NCOL = {"V": 1, "H": 2, "D": 4, "M": 3}
+
+
+def load(pc):
+    z = np.load(os.path.join(GOLDEN, f"qla_{pc.lower()}_golden.npz"))
+    ins = {k[4:]: z[k] for k in z.files if k.startswith("in__")}
+    outs = {k[5:]: z[k] for k in z.files if k.startswith("out__")}
+    return ins, outs
+
+
+def replay(pc, name, ins):
+    """Recompute one golden entry with the oracle."""
+    n = len(ins["gang"])
+    dt = ins["V"].dtype
+    key, *extra = name.split("|")
+    m = re.match(r"QLA_(F3|D3|DF3)_(\w)_([vx])(eq|peq|meq|eqm)_(p?Ma?)_times_(p?\w+)$", key)
+    if m:
+        _, dest, var, eq, s1, s2 = m.groups()
+        r = (ins["r0" + dest] if dest != "M" else ins["r0M"]).copy()
+        bsrc = ins["M2"] if dest == "M" else ins[dest]
+        T.ora_lmult(r, ins["M"], bsrc, n, NCOL[dest], eq, adja=int(s1.endswith("a")),
+                    adjb=int(s2.endswith("a")), idx_a=ins["idx"] if s1.startswith("p") else None,
+                    idx_b=ins["idx"][::-1].copy() if s2.startswith("p") else None,
+                    gang=ins["gang"] if var == "x" else None)
+        return r
+    m = re.match(r"QLA_(F3|D3)_H_([vx])(eq|peq|meq|eqm)_spproj_(p?)D$", key)
+    if m:
+        _, var, eq, p = m.groups()
+        mu, sign = int(extra[0]), int(extra[1])
+        r = ins["r0H"].copy()
+        T.ora_spproj(r, ins["D"], n, mu, sign, eq, idx_a=ins["idx"] if p else None,
+                     gang=ins["gang"] if var == "x" else None)
+        return r
+    m = re.match(r"QLA_(F3|D3)_D_v(eq|peq|meq|eqm)_sprecon_H$", key)
+    if m:
+        r = ins["r0D"].copy()
+        T.ora_sprecon(r, ins["H"], n, int(extra[0]), int(extra[1]), m.group(2))
+        return r
+    m = re.match(r"QLA_(F3|D3)_(\w)_v(eq|peq|meq|eqm)_r_times_\w$", key)
+    if m:
+        dest, eq = m.group(2), m.group(3)
+        r = ins["r0" + dest].copy()
+        T.ora_rtimes(r, float(ins["scal"][0]), ins[dest if dest != "M" else "M2"], n, NC[dest], eq)
+        return r
+    m = re.match(r"QLA_(F3|D3|DF3)_r_([vx])eq_norm2_(p?)(\w)$", key)
+    if m:
+        rpc, var, p, t = m.groups()
+        v = T.ora_norm2(ins[t], n, NC[t], idx_a=ins["idx"] if p else None, gang=ins["gang"] if var == "x" else None)
+        return np.array([v], dtype=np.float32 if rpc == "F3" else np.float64)
+    m = re.match(r"QLA_(F3|D3|DF3)_(c|r)_veq_(re_)?(\w)_dot_\w$", key)
+    if m:
+        rpc, kind, re_, t = m.groups()
+        b = ins["D2"] if t == "D" else ins["M2"] if t == "M" else ins["r0" + t]
+        v = T.ora_dot(ins[t], b, n, NC[t])
+        odt = np.float32 if rpc == "F3" else np.float64
+        return np.array([v.real], dtype=odt) if re_ else np.array([v.real, v.imag], dtype=odt)
+    raise KeyError(name)
+
+
+@pytest.mark.parametrize("pc", ["F3", "D3"])
+def test_oracle_matches_reference_golden_vectors(pc):
+    ins, outs = load(pc)
+    assert len(outs) > 300
+    bad = []
+    for name, want in outs.items():
+        got = replay(pc, name, ins)
+        if not T.bits_equal(got, want):
+            bad.append(name)
+    assert not bad, f"{len(bad)} golden mismatches, e.g. {bad[:5]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+def test_oracle_matches_reference_library_large(pc, dt):
+    """Direct comparison on 20,000 sites (OMP_NUM_THREADS is irrelevant for the
+    linear ops; the reductions are compared to the reference's own rounding)."""
+    rng = np.random.default_rng(77)
+    n = 20000
+    R = T.ref()
+    a = T.haar_su3(rng, n, dt)
+    for dest in ("V", "H", "D", "M"):
+        b = T.gaussian_field(rng, n, NC[dest], dt)
+        r0 = T.gaussian_field(rng, n, NC[dest], dt)
+        for eq in T.EQOPS:
+            for s1 in ("M", "Ma"):
+                rr = r0.copy()
+                getattr(R, f"QLA_{pc}_{dest}_v{eq}_{s1}_times_{dest}")(T.ptr(rr), T.ptr(a), T.ptr(b), n)
+                ro = r0.copy()
+                T.ora_lmult(ro, a, b, n, NCOL[dest], eq, adja=int(s1 == "Ma"))
+                assert T.bits_equal(rr, ro), (dest, eq, s1)
+    d = T.gaussian_field(rng, n, 12, dt)
+    out = np.zeros(1, dtype=np.float64)
+    fn = getattr(R, f"QLA_{'DF3' if pc == 'F3' else 'D3'}_r_veq_norm2_D")
+    fn(T.ptr(out), T.ptr(d), n)
+    ref_v = out[0]
+    ora_v = T.ora_norm2(d, n, 12)
+    assert abs(ref_v - ora_v) <= 1e-12 * ref_v
+
+
+def test_tolerance_rule_matches_reference_harness():
+    """test/src/compare.h:10-25: fail only when abs > 16 eps AND rel > 10 eps."""
+    eps = np.finfo(np.float32).eps
+    ok, _ = T.qla_close([1.0], [1.0 + 8 * eps], np.float32)
+    assert ok
+    ok, nbad = T.qla_close([100.0], [100.0 * (1 + 20 * eps)], np.float32)
+    assert not ok and nbad == 1
+    ok, _ = T.qla_close([1e-9], [2e-9], np.float32)  # tiny absolute difference passes
+    assert ok
+
+
+def test_oracle_detects_a_planted_mistake():
+    """A mistake planted in the oracle's input (a flipped sign in one matrix
+    element) must be caught by the golden comparison."""
+    ins, outs = load("F3")
+    ins = dict(ins)
+    m = ins["M"].copy()
+    m[3, 5] = -m[3, 5]
+    ins["M"] = m
+    name = "QLA_F3_V_veq_M_times_V"
+    assert not T.bits_equal(replay("F3", name, ins), outs[name])
