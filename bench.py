@@ -210,16 +210,29 @@ def run_gpu_arm(args):
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     qla.set_stream(stream)
-    n = NSITES
+    n = args.sites
+    iters = args.iters
     g = torch.Generator(device=dev)
     g.manual_seed(1000 + rank)
-    rng = np.random.default_rng(7)
-    a_vals = rng.uniform(-1, 1, ITERS).astype(np.float32)
+    a_vals = np.random.default_rng(7).uniform(-1, 1, ITERS).astype(np.float32)[:iters]
+    L = qla.lib()
+    fns = {}
+    for nm in ("QLA_F3_D_vpeq_r_times_D", "QLA_DF3_r_veq_norm2_D", "QLA_DF3_c_veq_D_dot_D",
+               "QLA_D3_D_vpeq_r_times_D", "QLA_D3_r_veq_norm2_D", "QLA_D3_c_veq_D_dot_D"):
+        fns[nm] = getattr(L, nm)
+        fns[nm].restype = None
+    chain_f = (fns["QLA_F3_D_vpeq_r_times_D"], fns["QLA_DF3_r_veq_norm2_D"], fns["QLA_DF3_c_veq_D_dot_D"],
+               [ctypes.c_float(float(v)) for v in a_vals])
+    chain_d = (fns["QLA_D3_D_vpeq_r_times_D"], fns["QLA_D3_r_veq_norm2_D"], fns["QLA_D3_c_veq_D_dot_D"],
+               [ctypes.c_double(float(v)) for v in a_vals])
+    nrm = torch.zeros(iters, dtype=torch.float64, device=dev)
+    dot = torch.zeros(iters, 2, dtype=torch.float64, device=dev)
 
     def barrier():
         if world > 1:
@@ -233,23 +246,13 @@ def run_gpu_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---------------- FP32 sites + FP64 reductions chain (F3 / DF3)
-    x = torch.randn(n, 24, device=dev, dtype=torch.float32, generator=g)
-    p = torch.randn(n, 24, device=dev, dtype=torch.float32, generator=g)
-    nrm = torch.zeros(ITERS, dtype=torch.float64, device=dev)
-    dot = torch.zeros(ITERS, 2, dtype=torch.float64, device=dev)
-    L = qla.lib()
-    f_axpy, f_n2, f_dot = L.QLA_F3_D_vpeq_r_times_D, L.QLA_DF3_r_veq_norm2_D, L.QLA_DF3_c_veq_D_dot_D
-    d_axpy, d_n2, d_dot = L.QLA_D3_D_vpeq_r_times_D, L.QLA_D3_r_veq_norm2_D, L.QLA_D3_c_veq_D_dot_D
-    for f in (f_axpy, f_n2, f_dot, d_axpy, d_n2, d_dot):
-        f.restype = None
-    a_f = [ctypes.c_float(float(v)) for v in a_vals]
-    a_d = [ctypes.c_double(float(v)) for v in a_vals]
-
-    def chain(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t, ev=None):
+    def chain(xa, pa, ch, ev=None):
+        """One step: `iters` iterations of axpy, norm2, dot; reduction results
+        stay on the device (asynchronous calls)."""
+        axpy, n2, dt, avals = ch
         xp, pp = ctypes.c_void_p(xa.data_ptr()), ctypes.c_void_p(pa.data_ptr())
-        nb, db = nrm_t.data_ptr(), dot_t.data_ptr()
-        for k in range(ITERS):
+        nb, db = nrm.data_ptr(), dot.data_ptr()
+        for k in range(iters):
             if ev is not None:
                 ev[k][0].record(stream)
             axpy(xp, ctypes.byref(avals[k]), pp, n)
@@ -262,107 +265,119 @@ def run_gpu_arm(args):
             if ev is not None:
                 ev[k][3].record(stream)
 
-    def timed(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t, steps, warmup, per_kernel):
-        for _ in range(warmup):
-            chain(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t)
+    def timed(xa, pa, ch):
+        """Device time of K steps after W warm-up steps (CUDA events on the
+        launching stream, barrier + synchronize on both sides), plus the
+        average duration of each of the three kernels (events around every
+        launch inside the timed region)."""
+        for _ in range(args.warmup):
+            chain(xa, pa, ch)
         qla.check("warm-up")
         evs = []
         barrier()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        for _ in range(steps):
-            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(ITERS)] \
-                if per_kernel else None
-            chain(xa, pa, axpy, n2, dt, avals, nrm_t, dot_t, ev)
-            if ev:
-                evs.append(ev)
+        for _ in range(args.steps):
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(iters)]
+            chain(xa, pa, ch, ev)
+            evs.append(ev)
         t1.record(stream)
         barrier()
         ms = t0.elapsed_time(t1)
         kern = {"axpy": 0.0, "norm2": 0.0, "dot": 0.0}
         for ev in evs:
-            for k in range(ITERS):
+            for k in range(iters):
                 kern["axpy"] += ev[k][0].elapsed_time(ev[k][1])
                 kern["norm2"] += ev[k][1].elapsed_time(ev[k][2])
                 kern["dot"] += ev[k][2].elapsed_time(ev[k][3])
-        nl = max(1, len(evs) * ITERS)
-        kern = {k: v / nl for k, v in kern.items()}  # ms per launch
+        nl = max(1, len(evs) * iters)
         qla.check("timed region")
-        return ms, kern
+        if qla.device_error():
+            raise qla.QLAError("a kernel reported an error in the timed region")
+        return ms, {k: v / nl for k, v in kern.items()}
 
+    # ---------------- FP32 sites + FP64 reductions chain (F3 / DF3)
+    x = torch.randn(n, 24, device=dev, dtype=torch.float32, generator=g)
+    p = torch.randn(n, 24, device=dev, dtype=torch.float32, generator=g)
     clk = ClockSampler(local)
     clk.start()
-    ms_f, kern_f = timed(x, p, f_axpy, f_n2, f_dot, a_f, nrm, dot, args.steps, args.warmup, True)
+    ms_f, kern_f = timed(x, p, chain_f)
     clocks = clk.stop()
     ms_f = max_over_ranks(ms_f)
-    value = world * n * ITERS * args.steps / (ms_f / 1e3)
-    nrm_host = nrm.cpu().numpy()
-    assert np.all(np.isfinite(nrm_host))
+    value = world * n * iters * args.steps / (ms_f / 1e3)
+    assert np.all(np.isfinite(nrm.cpu().numpy()))
 
-    # ---------------- end to end through the C-ABI with host buffers:
-    # per step: pinned host -> device copy of x and p, the 50-iteration chain,
-    # device -> host read of the 100 reduction results.
-    xh = torch.empty((n, 24), dtype=torch.float32, pin_memory=True)
-    ph = torch.empty((n, 24), dtype=torch.float32, pin_memory=True)
-    xh.copy_(x)
-    ph.copy_(p)
-    nrm_h = torch.empty(ITERS, dtype=torch.float64, pin_memory=True)
-    dot_h = torch.empty((ITERS, 2), dtype=torch.float64, pin_memory=True)
-    e_steps = max(1, min(args.steps, 5))
-    for _ in range(1):
-        x.copy_(xh, non_blocking=True)
-        p.copy_(ph, non_blocking=True)
-        chain(x, p, f_axpy, f_n2, f_dot, a_f, nrm, dot)
-        nrm_h.copy_(nrm, non_blocking=True)
-        dot_h.copy_(dot, non_blocking=True)
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e_steps):
-        x.copy_(xh, non_blocking=True)
-        p.copy_(ph, non_blocking=True)
-        chain(x, p, f_axpy, f_n2, f_dot, a_f, nrm, dot)
-        nrm_h.copy_(nrm, non_blocking=True)
-        dot_h.copy_(dot, non_blocking=True)
-    e1.record(stream)
-    barrier()
-    ms_e = max_over_ranks(e0.elapsed_time(e1))
-    e2e = {"value": world * n * ITERS * e_steps / (ms_e / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": int(xh.numel() * 4 + ph.numel() * 4),
-           "d2h_bytes_per_step": int(nrm_h.numel() * 8 + dot_h.numel() * 8), "steps": e_steps}
-    del xh, ph
+    # ---------------- end to end through the C-ABI with host buffers: per step
+    # the pinned host -> device copy of x and p, the chain, and the device ->
+    # host read of the 3*iters reduction results
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.empty((n, 24), dtype=torch.float32, pin_memory=True)
+        ph = torch.empty((n, 24), dtype=torch.float32, pin_memory=True)
+        xh.copy_(x)
+        ph.copy_(p)
+        nrm_h = torch.empty(iters, dtype=torch.float64, pin_memory=True)
+        dot_h = torch.empty((iters, 2), dtype=torch.float64, pin_memory=True)
+        e_steps = max(1, min(args.steps, 5))
 
-    # ---------------- plain FP64 chain (D3) on the same GPU
+        def e2e_step():
+            x.copy_(xh, non_blocking=True)
+            p.copy_(ph, non_blocking=True)
+            chain(x, p, chain_f)
+            nrm_h.copy_(nrm, non_blocking=True)
+            dot_h.copy_(dot, non_blocking=True)
+
+        e2e_step()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            e2e_step()
+        e1.record(stream)
+        barrier()
+        ms_e = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * n * iters * e_steps / (ms_e / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(xh.numel() * 4 + ph.numel() * 4),
+               "d2h_bytes_per_step": int(nrm_h.numel() * 8 + dot_h.numel() * 8), "steps": e_steps,
+               "ms_per_step": ms_e / e_steps}
+        del xh, ph
     del x, p
     torch.cuda.empty_cache()
-    xd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
-    pd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
-    ms_d, kern_d = timed(xd, pd, d_axpy, d_n2, d_dot, a_d, nrm, dot, args.steps, args.warmup, True)
-    ms_d = max_over_ranks(ms_d)
-    value_d = world * n * ITERS * args.steps / (ms_d / 1e3)
-    del xd, pd
-    torch.cuda.empty_cache()
 
-    # ---------------- roofline of the dominant kernel (axpy) and of all three
+    # ---------------- plain FP64 chain (D3) on the same GPU
+    value_d = ms_d = None
+    kern_d = {}
+    if not args.no_fp64:
+        xd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
+        pd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
+        ms_d, kern_d = timed(xd, pd, chain_d)
+        ms_d = max_over_ranks(ms_d)
+        value_d = world * n * iters * args.steps / (ms_d / 1e3)
+        del xd, pd
+        torch.cuda.empty_cache()
+
+    # ---------------- roofline: algorithmic bytes per launch / event-timed duration
     peak, peak_kind = peaks()
-    rl = {}
-    for nm, ms in kern_f.items():
-        ach = BYTES_F3[nm] * n / (ms / 1e3) / 1e9
-        rl[nm] = {"achieved": ach, "frac": ach / peak, "us_per_launch": 1e3 * ms}
-    rl_d = {}
-    for nm, ms in kern_d.items():
-        ach = BYTES_D3[nm] * n / (ms / 1e3) / 1e9
-        rl_d[nm] = {"achieved": ach, "frac": ach / peak, "us_per_launch": 1e3 * ms}
+
+    def roof(kern, bytes_tab):
+        out = {}
+        for nm, ms in kern.items():
+            ach = bytes_tab[nm] * n / (ms / 1e3) / 1e9
+            out[nm] = {"achieved_gbs": ach, "frac": ach / peak, "us_per_launch": 1e3 * ms}
+        return out
+
+    rl = roof(kern_f, BYTES_F3)
+    rl_d = roof(kern_d, BYTES_D3)
     dom = max(kern_f, key=lambda k: kern_f[k])
+    kname = {"axpy": "QLA_F3_D_vpeq_r_times_D", "norm2": "QLA_DF3_r_veq_norm2_D", "dot": "QLA_DF3_c_veq_D_dot_D"}
     traffic = None
     tp = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get("F3_" + dom)
+            traffic = json.load(f).get(kname[dom])
     chain_bytes = sum(BYTES_F3.values())
-    launches = 3 * ITERS * args.steps
 
     # ---------------- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -372,7 +387,7 @@ def run_gpu_arm(args):
         os.environ.setdefault("OMP_PROC_BIND", "close")
         r, it, el, kind, threads = cpu_chain_rate(xs, ps, a_vals, budget_s=args.cpu_seconds)
         cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"{it} chain iterations on the full 48^3x96 field ({el:.1f} s)"}
+               "sample": f"{it} chain iterations on the full {n}-site field ({el:.1f} s)"}
 
     if rank == 0:
         line = {
@@ -380,23 +395,24 @@ def run_gpu_arm(args):
             "warmup": args.warmup, "ms_per_step": ms_f / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 sites, f64 reductions",
             "data": "synthetic (seeded N(0,1) DiracFermions, a_k ~ U[-1,1])",
-            "config": {"workload": "cg_chain_48^3x96", "sites": n, "iterations_per_step": ITERS,
+            "config": {"workload": "cg_chain_48^3x96" if n == NSITES else f"cg_chain_{n}_sites", "sites": n,
+                       "iterations_per_step": iters,
                        "ops": ["QLA_F3_D_vpeq_r_times_D", "QLA_DF3_r_veq_norm2_D", "QLA_DF3_c_veq_D_dot_D"],
-                       "bytes_per_site_update": chain_bytes, "l2": "inputs (2 x 1.02 GB) larger than L2",
+                       "bytes_per_site_update": chain_bytes, "l2": "inputs (2 x 1.02 GB) larger than L2, no flush",
                        "parallelism": f"replicas x{world}"},
             "hbm_frac_chain": value / world * chain_bytes / 1e9 / peak,
-            "fp64_chain": {"value": value_d, "ms_per_step": ms_d / args.steps,
-                           "hbm_frac": value_d / world * 2 * chain_bytes / 1e9 / peak,
-                           "ops": ["QLA_D3_D_vpeq_r_times_D", "QLA_D3_r_veq_norm2_D", "QLA_D3_c_veq_D_dot_D"],
-                           "kernels": rl_d},
-            "speedup_vs_fp64": value / value_d,
-            "roofline": {"bound": "hbm", "kernel": f"QLA_F3_D_vpeq_r_times_D" if dom == "axpy" else dom,
-                         "achieved": rl[dom]["achieved"], "peak": peak, "unit": "GB/s",
-                         "frac": rl[dom]["frac"], "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": BYTES_F3[dom] * n},
+            "fp64_chain": None if value_d is None else {
+                "value": value_d, "ms_per_step": ms_d / args.steps,
+                "hbm_frac": value_d / world * 2 * chain_bytes / 1e9 / peak,
+                "ops": ["QLA_D3_D_vpeq_r_times_D", "QLA_D3_r_veq_norm2_D", "QLA_D3_c_veq_D_dot_D"],
+                "kernels": rl_d},
+            "speedup_vs_fp64": None if value_d is None else value / value_d,
+            "roofline": {"bound": "hbm", "kernel": kname[dom], "achieved": rl[dom]["achieved_gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": rl[dom]["frac"], "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": BYTES_F3[dom] * n},
             "kernels": rl,
             "e2e": e2e,
-            "gpu_launches": launches,
+            "gpu_launches": 3 * iters * args.steps,
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
@@ -413,6 +429,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # smaller cases for profiler captures (the default is the benchmark workload)
+    ap.add_argument("--sites", type=int, default=NSITES)
+    ap.add_argument("--iters", type=int, default=ITERS)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("bench.py: warm-up raised to 3 steps", file=sys.stderr)

@@ -80,7 +80,20 @@ __device__ __forceinline__ void cmac(Cx<R>& x, bool minus, Cx<R> a, Cx<R> b) {
 // address aligned to sizeof(Cx<R>) (8 B for float, 16 B for double).
 template <typename R, int N>
 __device__ __forceinline__ void load_rec(Cx<R> (&x)[N], const void* p) {
-  if constexpr (sizeof(R) == 4) {
+  if constexpr (sizeof(R) == 4 && (N % 2) == 0) {
+    // records of a multiple of 16 B (H, D) start 16-B aligned in a staged
+    // tile: 16-B accesses halve the shared-memory bank conflicts of the
+    // 48/96-B record stride
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int e = 0; e < N / 2; e++) {
+      float4 v = q[e];
+      x[2 * e].re = v.x;
+      x[2 * e].im = v.y;
+      x[2 * e + 1].re = v.z;
+      x[2 * e + 1].im = v.w;
+    }
+  } else if constexpr (sizeof(R) == 4) {
     const float2* q = reinterpret_cast<const float2*>(p);
 #pragma unroll
     for (int e = 0; e < N; e++) {
@@ -96,6 +109,24 @@ __device__ __forceinline__ void load_rec(Cx<R> (&x)[N], const void* p) {
       x[e].re = v.x;
       x[e].im = v.y;
     }
+  }
+}
+
+// shared-memory store of a record; same vector width rule as load_rec
+template <typename R, int N>
+__device__ __forceinline__ void store_rec_smem(void* p, const Cx<R> (&x)[N]) {
+  if constexpr (sizeof(R) == 4 && (N % 2) == 0) {
+    float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int e = 0; e < N / 2; e++) q[e] = make_float4(x[2 * e].re, x[2 * e].im, x[2 * e + 1].re, x[2 * e + 1].im);
+  } else if constexpr (sizeof(R) == 4) {
+    float2* q = reinterpret_cast<float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) q[e] = make_float2(x[e].re, x[e].im);
+  } else {
+    double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) q[e] = make_double2(x[e].re, x[e].im);
   }
 }
 
@@ -125,7 +156,17 @@ __device__ __forceinline__ void load_rec_global(Cx<R> (&x)[N], const void* p) {
 // destination of a peq/meq update)
 template <typename R, int N>
 __device__ __forceinline__ void load_rec_rw(Cx<R> (&x)[N], const void* p) {
-  load_rec<R, N>(x, p);
+  if constexpr (sizeof(R) == 4) {
+    const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      float2 v = q[e];
+      x[e].re = v.x;
+      x[e].im = v.y;
+    }
+  } else {
+    load_rec<R, N>(x, p);
+  }
 }
 
 template <typename R, int N>
@@ -179,18 +220,27 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Time-bounded wait on an mbarrier phase: gives up after ~limit_ns and
-// records QLA_DEVERR_MBAR_TIMEOUT.  Returns false on timeout.
+// Time-bounded wait on an mbarrier phase: gives up after ~limit_ns (or at
+// once when *abort becomes non-zero) and records QLA_DEVERR_MBAR_TIMEOUT.
+// Returns false on timeout / abort.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err,
-                                                  uint64_t limit_ns = 2000000000ull) {
+                                                  uint64_t limit_ns = 2000000000ull,
+                                                  volatile int* abort = nullptr) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < (1u << 30); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63u) == 0 && global_ns() - t0 > limit_ns) break;
+    if ((it & 15u) == 0) {
+      if (abort && *abort) return false;
+      if (global_ns() - t0 > limit_ns) break;
+    }
   }
   raise_dev_error(err, QLA_DEVERR_MBAR_TIMEOUT);
   return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 // 1-D bulk copy global -> shared, completion signalled on an mbarrier.

@@ -182,134 +182,169 @@ __device__ __forceinline__ void acc_fold(DD (&dacc)[ArrN<OP::NACC>::value], cons
 }
 
 // ---------------------------------------------------------------------------
-// Kernel 1: bulk-copy (TMA) pipelined, persistent, one site per thread per tile.
-// Dynamic shared memory: [S mbarriers | S stages | 2 destination tiles].
+// Kernel 1: bulk-copy (TMA) pipeline, persistent, warp-specialised.
+//
+// Block = NW consumer warps (one site per lane per tile, T = 32*NW sites per
+// tile) + 1 producer warp.  Per stage s there is a `full` mbarrier (completed
+// by the bulk-copy transaction bytes) and an `empty` mbarrier (one arrival
+// per consumer warp once it has read the stage).  The producer lane waits on
+// `empty`, re-arms `full` and issues the next tile's loads; consumer warps
+// wait on `full`, compute, release the stage, and write their 32 results
+// through a per-warp double-buffered shared-memory slice with their own bulk
+// store.  No block-wide barrier sits in the tile loop, so every warp runs at
+// its own pace and the next loads go out as soon as a stage is released.
+//
+// Dynamic shared memory: [full[S], empty[S], abort flag | S stages |
+//                         NW x 2 destination slices of 32 records].
+// Every wait is time-bounded; a failed wait raises the abort flag so that all
+// other waits of the block give up at once, and loads still in flight are
+// drained (bounded) before the block exits.
 template <class OP>
-__global__ void __launch_bounds__(256) site_tma_kernel(const SiteParams p) {
+__global__ void __launch_bounds__(288) site_tma_kernel(const SiteParams p) {
   using R = typename OP::R;
   constexpr int OB = OP::NOUT * (int)sizeof(Cx<R>);
   constexpr int NA = ArrN<OP::NACC>::value;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  const int T = blockDim.x;
   const int S = p.stages;
-  unsigned char* stages = smem + 128;
+  const int NW = (blockDim.x >> 5) - 1;  // consumer warps
+  const int T = NW * 32;                 // sites per tile
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + 8;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 8 * 16);
+  unsigned char* stages = smem + 256;
   unsigned char* outbuf = stages + (size_t)S * p.stage_bytes;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long my =
       ((long long)blockIdx.x < p.ntiles) ? (p.ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1 : 0;
-  const uint64_t pol = policy_evict_first();
 
   if (tid == 0) {
-    for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+    for (int s = 0; s < S; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], (unsigned)NW);
+    }
+    *abort_flag = 0;
     mbar_init_fence();
   }
   __syncthreads();
 
-  // issue the loads of local tile k into stage s (thread 0 only)
-  auto issue = [&](long long k, int s) {
-    const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * T;
-    unsigned char* st = stages + (size_t)s * p.stage_bytes;
-    mbar_arrive_expect_tx(&full[s], p.tx_bytes);
-    constexpr int RB[3] = {OP::N0 * (int)sizeof(Cx<R>), OP::N1 * (int)sizeof(Cx<R>),
-                           OP::N2 * (int)sizeof(Cx<R>)};
-#pragma unroll
-    for (int j = 0; j < OP::NIN; j++) {
-      const Opnd& o = p.in[j];
-      if (o.mode == OM_CONTIG)
-        bulk_g2s(st + p.off_in[j], static_cast<const char*>(o.base) + site0 * RB[j], (unsigned)T * RB[j], &full[s],
-                 pol);
-      else if (o.mode == OM_PTR)
-        bulk_g2s(st + p.off_in[j], o.ptrs + site0, (unsigned)T * 8u, &full[s], pol);
-      else
-        bulk_g2s(st + p.off_in[j], o.idx + site0, (unsigned)T * 4u, &full[s], pol);
-    }
-    if constexpr (OP::NOUT > 0) {
-      if (p.out_read)
-        bulk_g2s(st + p.off_out_in, static_cast<const char*>(p.out) + site0 * OB, (unsigned)T * OB, &full[s], pol);
-    }
-  };
-
-  long long issued = 0;
-  if (tid == 0) {
-    for (; issued < my && issued < S; issued++) issue(issued, (int)issued);
-  }
-
   DD dacc[NA];
 #pragma unroll
   for (int a = 0; a < NA; a++) dacc[a] = DD{0.0, 0.0};
-
-  long long k = 0;
   bool alive = true;
-  int s = 0;
-  uint32_t par = 0;
-  for (; k < my; k++) {
-    const bool ok = mbar_wait_bounded(&full[s], par, p.err);
-    const unsigned char* st = stages + (size_t)s * p.stage_bytes;
-    Cx<R> x0[ArrN<OP::N0>::value], x1[ArrN<OP::N1>::value], x2[ArrN<OP::N2>::value];
-    Cx<R> y[ArrN<OP::NOUT>::value];
-    if (ok) {
-      if constexpr (OP::NIN > 0) fetch_staged<OP, OP::N0>(x0, p.in[0], st, p.off_in[0], tid);
-      if constexpr (OP::NIN > 1) fetch_staged<OP, OP::N1>(x1, p.in[1], st, p.off_in[1], tid);
-      if constexpr (OP::NIN > 2) fetch_staged<OP, OP::N2>(x2, p.in[2], st, p.off_in[2], tid);
+  long long issued = 0;  // tiles whose loads the producer issued
+
+  if (warp == NW) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      const uint64_t pol = policy_evict_first();
+      constexpr int RB[3] = {OP::N0 * (int)sizeof(Cx<R>), OP::N1 * (int)sizeof(Cx<R>),
+                             OP::N2 * (int)sizeof(Cx<R>)};
+      long long k = 0;
+      int s = 0;
+      long long round = 0;  // k / S
+      for (; k < my; k++) {
+        // stage s was last filled in round-1; wait until its consumers released it
+        if (round > 0 && !mbar_wait_bounded(&empty[s], (uint32_t)((round - 1) & 1), p.err, 2000000000ull,
+                                            abort_flag)) {
+          *abort_flag = 1;
+          break;
+        }
+        const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * T;
+        unsigned char* st = stages + (size_t)s * p.stage_bytes;
+        mbar_arrive_expect_tx(&full[s], p.tx_bytes);
+#pragma unroll
+        for (int j = 0; j < OP::NIN; j++) {
+          const Opnd& o = p.in[j];
+          if (o.mode == OM_CONTIG)
+            bulk_g2s(st + p.off_in[j], static_cast<const char*>(o.base) + site0 * RB[j], (unsigned)T * RB[j],
+                     &full[s], pol);
+          else if (o.mode == OM_PTR)
+            bulk_g2s(st + p.off_in[j], o.ptrs + site0, (unsigned)T * 8u, &full[s], pol);
+          else
+            bulk_g2s(st + p.off_in[j], o.idx + site0, (unsigned)T * 4u, &full[s], pol);
+        }
+        if constexpr (OP::NOUT > 0) {
+          if (p.out_read)
+            bulk_g2s(st + p.off_out_in, static_cast<const char*>(p.out) + site0 * OB, (unsigned)T * OB, &full[s],
+                     pol);
+        }
+        if (++s == S) {
+          s = 0;
+          round++;
+        }
+      }
+      issued = k;
+    }
+  } else {
+    // ------------------------------------------------------------ consumers
+    const uint64_t pol = policy_evict_first();
+    unsigned char* myout = outbuf + (size_t)warp * 2 * 32 * OB;
+    int s = 0;
+    uint32_t par = 0;
+    for (long long k = 0; k < my; k++) {
+      if (!mbar_wait_bounded(&full[s], par, p.err, 2000000000ull, abort_flag)) {
+        *abort_flag = 1;
+        alive = false;
+        break;
+      }
+      const unsigned char* st = stages + (size_t)s * p.stage_bytes;
+      const int t = warp * 32 + lane;
+      Cx<R> x0[ArrN<OP::N0>::value], x1[ArrN<OP::N1>::value], x2[ArrN<OP::N2>::value];
+      Cx<R> y[ArrN<OP::NOUT>::value];
+      if constexpr (OP::NIN > 0) fetch_staged<OP, OP::N0>(x0, p.in[0], st, p.off_in[0], t);
+      if constexpr (OP::NIN > 1) fetch_staged<OP, OP::N1>(x1, p.in[1], st, p.off_in[1], t);
+      if constexpr (OP::NIN > 2) fetch_staged<OP, OP::N2>(x2, p.in[2], st, p.off_in[2], t);
       if constexpr (OP::NOUT > 0) {
-        if (p.out_read) load_rec<R, OP::NOUT>(y, st + p.off_out_in + (unsigned)tid * OB);
+        if (p.out_read) load_rec<R, OP::NOUT>(y, st + p.off_out_in + (unsigned)t * OB);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
+      if constexpr (OP::NOUT > 0) {
         OP::apply(p, x0, x1, x2, y);
+        unsigned char* ob = myout + (size_t)(k & 1) * 32 * OB;
+        if (lane == 0) bulk_wait_read<1>();  // slice (k&1) no longer read by this warp's store k-2
+        __syncwarp();
+        store_rec_smem<R, OP::NOUT>(ob + (unsigned)lane * OB, y);
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * T + warp * 32;
+          bulk_s2g(static_cast<char*>(p.out) + site0 * OB, ob, 32u * OB, pol);
+          bulk_commit();
+        }
       } else {
         double acc[NA];
         OP::accum(p, x0, x1, x2, acc);
         acc_fold<OP>(dacc, acc);
       }
-    }
-    if constexpr (OP::NOUT > 0) {
-      if (tid == 0) bulk_wait_read<1>();  // destination tile (k&1) no longer read by store k-2
-    }
-    if (!__syncthreads_and(ok)) {  // every thread is done with stage s
-      alive = false;
-      break;
-    }
-    if (tid == 0 && issued < my) {
-      issue(issued, s);
-      issued++;
-    }
-    if constexpr (OP::NOUT > 0) {
-      unsigned char* ob = outbuf + (size_t)(k & 1) * T * OB;
-      store_rec<R, OP::NOUT>(ob + (unsigned)tid * OB, y);
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * T;
-        bulk_s2g(static_cast<char*>(p.out) + site0 * OB, ob, (unsigned)T * OB, pol);
-        bulk_commit();
+      if (++s == S) {
+        s = 0;
+        par ^= 1u;
       }
     }
-    if (++s == S) {
-      s = 0;
-      par ^= 1u;
+    if constexpr (OP::NOUT > 0) {
+      if (lane == 0) bulk_wait_all<0>();
+    }
+    // partial last tile: plain loads by the consumers of the last block
+    if (alive && blockIdx.x == gridDim.x - 1) {
+      const long long k0 = p.ntiles * T + warp * 32 + lane;
+      if (k0 < p.n) {
+        double acc[NA];
+        site_direct<OP>(p, k0, acc);
+        if constexpr (OP::NACC > 0) acc_fold<OP>(dacc, acc);
+      }
     }
   }
-
-  // partial last tile: plain loads by the last block
-  if (alive && blockIdx.x == gridDim.x - 1) {
-    const long long k0 = p.ntiles * T + tid;
-    if (k0 < p.n) {
-      double acc[NA];
-      site_direct<OP>(p, k0, acc);
-      if constexpr (OP::NACC > 0) acc_fold<OP>(dacc, acc);
-    }
+  __syncthreads();
+  if (*abort_flag && warp == NW && lane == 0) {
+    // a wait failed: before the block's shared memory is released, wait
+    // (bounded) until every load still in flight has landed
+    for (long long kk = (issued > S ? issued - S : 0); kk < issued; kk++)
+      if (!mbar_wait_bounded(&full[kk % S], (uint32_t)((kk / S) & 1), p.err, 200000000ull, nullptr))
+        raise_dev_error(p.err, QLA_DEVERR_BULK_TIMEOUT);
   }
-
-  if (tid == 0) {
-    if constexpr (OP::NOUT > 0) bulk_wait_all<0>();
-    if (!alive) {
-      // drain loads still in flight into this block's shared memory
-      for (long long kk = k; kk < issued; kk++)
-        if (!mbar_wait_bounded(&full[kk % S], (uint32_t)((kk / S) & 1), p.err, 200000000ull))
-          raise_dev_error(p.err, QLA_DEVERR_BULK_TIMEOUT);
-    }
-  }
-  // every block takes part in the finish, even after a failed wait, so that the
-  // ticket counter returns to zero (the error word marks the result invalid)
+  // every block takes part in the finish, even after a failed wait, so that
+  // the ticket counter returns to zero (the error word marks the result invalid)
   if constexpr (OP::NACC > 0) reduce_finish<OP>(p, dacc);
 }
 

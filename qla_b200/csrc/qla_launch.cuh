@@ -19,14 +19,27 @@ struct LaunchShape {
   int stages;
 };
 
-// default tile shape from the bytes one site streams through shared memory
+// shared memory of one block of the pipelined kernel
+inline size_t tma_smem_bytes(int threads, int stages, unsigned stage_bytes, unsigned out_bytes) {
+  return 256 + (size_t)stages * stage_bytes + 2 * (size_t)threads * out_bytes;
+}
+
+inline unsigned stage_bytes_for(int threads, unsigned bytes_per_site) {
+  return ((unsigned)threads * bytes_per_site + 127u) & ~127u;
+}
+
+// Default tile shape: two stages, and the largest tile (sites = consumer
+// threads) whose block still fits in ~100 KB of shared memory, so that two to
+// four blocks share an SM.  Measured on B200: more resident blocks beat deeper
+// pipelines for these streaming tiles.
 inline LaunchShape default_shape(unsigned bytes_per_site, unsigned out_bytes) {
-  LaunchShape s;
-  s.threads = bytes_per_site <= 64 ? 256 : (bytes_per_site <= 160 ? 128 : 64);
-  unsigned tile = (unsigned)s.threads * bytes_per_site;
-  int st = (int)(65536u / (tile ? tile : 1));
-  (void)out_bytes;
-  s.stages = st < 2 ? 2 : (st > 8 ? 8 : st);
+  LaunchShape s{64, 2};
+  for (int t : {256, 128, 64}) {
+    if (tma_smem_bytes(t, 2, stage_bytes_for(t, bytes_per_site), out_bytes) <= 100u * 1024u) {
+      s.threads = t;
+      break;
+    }
+  }
   return s;
 }
 
@@ -92,7 +105,7 @@ struct SiteLauncher {
     ReduceScratch* rs = nullptr;
     int sms = device_sm_count();
     if (reduce) {
-      rs = reduce_scratch(st, 8 * sms + 64);
+      rs = reduce_scratch(st, 32 * sms + 64);
       if (!rs) return;
       p.partials = rs->partials;
       p.counter = rs->counter;
@@ -113,9 +126,27 @@ struct SiteLauncher {
       if (OP::NOUT > 0 && p.out_read) bps += OB;
       LaunchShape sh = default_shape(bps, OB);
       int tt, ts;
-      if (tuned_shape(kernel_id, &tt, &ts)) {
+      char key[96];
+      {
+        int q = 0;
+        for (const char* c = kernel_id; *c && q < 80; c++) key[q++] = *c;
+        key[q++] = ':';
+        for (int j = 0; j < OP::NIN; j++) key[q++] = "-cpi"[p.in[j].mode & 3];
+        if (OP::NOUT > 0 && p.out_read) key[q++] = 'r';
+        key[q] = 0;
+      }
+      if (tuned_shape(key, &tt, &ts)) {
         sh.threads = tt;
         sh.stages = ts;
+      }
+      // never exceed the 227 KB per-block limit: shed stages, then halve the tile
+      while (tma_smem_bytes(sh.threads, sh.stages, stage_bytes_for(sh.threads, bps), OB) > 227u * 1024u) {
+        if (sh.stages > 2)
+          sh.stages--;
+        else if (sh.threads > 64)
+          sh.threads /= 2;
+        else
+          break;
       }
       const int T = sh.threads;
       unsigned off = 0;
@@ -133,18 +164,18 @@ struct SiteLauncher {
       }
       p.stage_bytes = (off + 127u) & ~127u;
       p.ntiles = p.n / T;
-      size_t smem = 128 + (size_t)sh.stages * p.stage_bytes + (OP::NOUT > 0 ? 2 * (size_t)T * OB : 0);
-      p.stages = sh.stages < 2 ? 2 : (sh.stages > 8 ? 8 : sh.stages);
-      smem = 128 + (size_t)p.stages * p.stage_bytes + (OP::NOUT > 0 ? 2 * (size_t)T * OB : 0);
+      p.stages = sh.stages;
+      const size_t smem = tma_smem_bytes(T, p.stages, p.stage_bytes, OB);
       const void* fn = reinterpret_cast<const void*>(&site_tma_kernel<OP>);
       set_smem_attr(fn, smem);
-      const int nb = blocks_per_sm(fn, T, smem);
+      const int nb = blocks_per_sm(fn, T + 32, smem);
       long long grid = (long long)nb * sms;
       if (grid > p.ntiles) grid = p.ntiles;
       if (grid < 1) grid = 1;
       if (reduce && grid > rs->max_blocks) grid = rs->max_blocks;
       void* args[] = {&p};
-      if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3((unsigned)T), args, smem, st) != cudaSuccess) {
+      // T consumer threads + one producer warp
+      if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3((unsigned)T + 32u), args, smem, st) != cudaSuccess) {
         check_launch(kernel_id);
         return;
       }

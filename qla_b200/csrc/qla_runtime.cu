@@ -5,8 +5,12 @@
 // (the QLA signatures return void), per-stream scratch for global
 // reductions, and the autotuner's launch-shape table.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <atomic>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -138,11 +142,52 @@ std::map<std::string, std::pair<int, int>> g_tune;
 std::atomic<int> g_tune_count{0};
 }  // namespace
 
+// The shipped table (tune_b200.txt beside the package, written by
+// `python -m qla_b200.tune` on a B200) or the file named by $QLA_B200_TUNE is
+// read once, at the first launch.  Lines: "<kernel id> <threads> <stages>".
+static std::once_flag g_tune_once;
+
+static void load_tune_file() {
+  std::string path;
+  if (const char* env = std::getenv("QLA_B200_TUNE")) {
+    path = env;
+  } else {
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&load_tune_file), &info) && info.dli_fname) {
+      std::string so = info.dli_fname;
+      size_t k = so.rfind('/');
+      std::string dir = (k == std::string::npos) ? std::string(".") : so.substr(0, k);
+      path = dir + "/../tune_b200.txt";
+    }
+  }
+  if (path.empty() || path == "none") return;
+  std::ifstream f(path);
+  if (!f) return;
+  std::string line;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream ss(line);
+    std::string id;
+    int t = 0, st = 0;
+    if (ss >> id >> t >> st && (t == 64 || t == 128 || t == 256) && st >= 2 && st <= 8)
+      g_tune[id] = std::make_pair(t, st);
+  }
+  g_tune_count.store((int)g_tune.size());
+}
+
 bool tuned_shape(const char* kernel_id, int* threads, int* stages) {
+  std::call_once(g_tune_once, load_tune_file);
   if (g_tune_count.load(std::memory_order_relaxed) == 0 || !kernel_id) return false;
   std::lock_guard<std::mutex> g(g_tune_mu);
   auto it = g_tune.find(kernel_id);
-  if (it == g_tune.end()) return false;
+  if (it == g_tune.end()) {
+    // fall back from "<id>:<operand modes>" to the family-wide "<id>"
+    const char* colon = std::strchr(kernel_id, ':');
+    if (!colon) return false;
+    it = g_tune.find(std::string(kernel_id, colon - kernel_id));
+    if (it == g_tune.end()) return false;
+  }
   *threads = it->second.first;
   *stages = it->second.second;
   return true;
@@ -192,6 +237,7 @@ QLAB_EXPORT int qlagpu_synchronize(void) {
 }
 
 QLAB_EXPORT int qlagpu_tune_set(const char* kernel_id, int threads, int stages) {
+  std::call_once(g_tune_once, load_tune_file);
   if (!kernel_id || !(threads == 64 || threads == 128 || threads == 256) || stages < 2 || stages > 8) {
     set_error(QLAGPU_ERR_ARG, "qlagpu_tune_set", "threads must be 64/128/256 and stages 2..8");
     return QLAGPU_ERR_ARG;
@@ -203,6 +249,7 @@ QLAB_EXPORT int qlagpu_tune_set(const char* kernel_id, int threads, int stages) 
 }
 
 QLAB_EXPORT void qlagpu_tune_clear(void) {
+  std::call_once(g_tune_once, load_tune_file);  // a later first launch must not reload it
   std::lock_guard<std::mutex> g(g_tune_mu);
   g_tune.clear();
   g_tune_count.store(0);
