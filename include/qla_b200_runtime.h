@@ -18,6 +18,7 @@
  */
 #ifndef QLA_B200_RUNTIME_H
 #define QLA_B200_RUNTIME_H
+#include "qla_b200_types.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -61,6 +62,21 @@ const char *qlagpu_version(void);
  * (x0 fastest) of x(i) + sign * e_mu on the nd-dimensional torus dims[];
  * n = prod(dims).  This is the int32 index stream the `xX` gathers take. */
 void qlagpu_shift_index(int *idx, int nd, const int *dims, int mu, int sign);
+
+/* No counterpart in the reference (QLA never touches device memory).
+ * QLA_DF3_r_veq_norm2_D for callers that cannot allocate device memory while
+ * they run -- e.g. a program whose own pool allocator reserved the GPU's
+ * memory up front, or one under a hard memory budget: the regular reductions
+ * allocate their scratch on first use, this one allocates nothing.  Its
+ * scratch is a static 1 MiB device array held by every GPU that loads the
+ * library until the process exits; it limits n to 16,777,216 sites (larger n
+ * return QLAGPU_ERR_ARG).  The first call on a device looks the array up
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (e.g. on two
+ * streams at once) race and give wrong results.  r may be a host pointer
+ * (the call synchronises) or a device pointer.  Returns QLAGPU_OK or an error
+ * code. */
+int qlagpu_DF3_r_veq_norm2_D_noalloc(QLA_D_Real *r, QLA_F3_DiracFermion *a, int n);
 
 #ifdef __cplusplus
 }
