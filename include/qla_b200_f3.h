@@ -1219,6 +1219,39 @@ void QLA_F3_M_peq_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix
 void QLA_F3_M_meq_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * ja, int n);
 /* replaces QLA_F3_M_eqm_xM (doc/qla.tex:555-575 (unary per-operand index variant 5, not generated by the reference)) */
 void QLA_F3_M_eqm_xM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * ja, int n);
+/* ---- mfunc: replaces the F3 functions emitted by lib/perl/build_qla.pl:1000-1060 (matrix functions) */
+/* replaces QLA_F3_M_veq_exp_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_veq_exp_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_sqrt_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_veq_sqrt_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_inverse_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_veq_inverse_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_C_veq_det_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_C_veq_det_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_exp_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_veq_exp_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veq_sqrt_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_veq_sqrt_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veq_inverse_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_veq_inverse_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_veq_det_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_C_veq_det_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_xeq_exp_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_xeq_exp_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_sqrt_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_xeq_sqrt_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_inverse_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_xeq_inverse_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_C_xeq_det_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_C_xeq_det_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_exp_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_xeq_exp_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeq_sqrt_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_xeq_sqrt_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeq_inverse_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_M_xeq_inverse_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xeq_det_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
+void QLA_F3_C_xeq_det_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
 /* ---- norm2: replaces the F3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_F3_r_veq_norm2_V (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_F3_r_veq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);

@@ -30,6 +30,18 @@ void ora_dot_exact_##SFX(double *out2, const R *a, const R *b, long n, int ncplx
 ORA_DECL(f, float)
 ORA_DECL(d, double)
 
+/* matrix functions: which = ORA_MF_*; det writes one complex per site */
+#define ORA_MF_EXP 0
+#define ORA_MF_SQRT 1
+#define ORA_MF_INVERSE 2
+#define ORA_MF_DET 3
+void ora_mfunc_f(float *r, const float *a, long n, int nc, int which);
+void ora_mfunc_d(double *r, const double *a, long n, int nc, int which);
+
+/* QLA_I_ integer ops (codes as the product's IntCode, 19 = mask) */
+void ora_int(int code, int eqop, int *r, const int *a, const int *b, const int *c, int s, long n,
+             const int *ia, const int *ib, const int *ic, const int *gang);
+
 int ora_version(void);
 
 #endif

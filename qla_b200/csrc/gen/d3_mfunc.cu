@@ -1,0 +1,72 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA D3 mfunc entry points (extern "C"), reference: lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+#include "../qla_mfunc.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_D3_M_veq_exp_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_map<qlab::ExpOp<double>>("D3_mfunc_exp", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_veq_sqrt_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_map<qlab::SqrtOp<double>>("D3_mfunc_sqrt", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_veq_inverse_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_map<qlab::InverseOp<double>>("D3_mfunc_inverse", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_C_veq_det_M(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_map<qlab::DetOp<double>>("D3_mfunc_det", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_veq_exp_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_map<qlab::ExpOp<double>>("D3_mfunc_exp", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_veq_sqrt_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_map<qlab::SqrtOp<double>>("D3_mfunc_sqrt", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_veq_inverse_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_map<qlab::InverseOp<double>>("D3_mfunc_inverse", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_C_veq_det_pM(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_map<qlab::DetOp<double>>("D3_mfunc_det", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_xeq_exp_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_map<qlab::ExpOp<double>>("D3_mfunc_exp", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_xeq_sqrt_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_map<qlab::SqrtOp<double>>("D3_mfunc_sqrt", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_xeq_inverse_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_map<qlab::InverseOp<double>>("D3_mfunc_inverse", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_C_xeq_det_M(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_map<qlab::DetOp<double>>("D3_mfunc_det", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_xeq_exp_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_map<qlab::ExpOp<double>>("D3_mfunc_exp", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_xeq_sqrt_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_map<qlab::SqrtOp<double>>("D3_mfunc_sqrt", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_M_xeq_inverse_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_map<qlab::InverseOp<double>>("D3_mfunc_inverse", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void QLA_D3_C_xeq_det_pM(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_map<qlab::DetOp<double>>("D3_mfunc_det", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+}  // extern "C"

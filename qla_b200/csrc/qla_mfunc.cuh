@@ -1,0 +1,337 @@
+// qla_mfunc.cuh -- colour-matrix functions for Nc = 3 as engine OPs
+// (QLA_F3/D3 M_veq_exp_M, M_veq_sqrt_M, M_veq_inverse_M, C_veq_det_M).
+//
+//  det, inverse: the reference's closed cofactor forms
+//    (lib/perl/code-templates/C_eq_det_M.c:70-84, M_eq_inverse_M.c:79-119),
+//    restated with explicitly rounded operations in the site precision:
+//    bit-identical to the reference for F3 and D3.
+//  sqrt: the reference's Newton iteration (M_eq_sqrt_M.c:139-180, with the
+//    Gauss-Jordan solve of M_eq_M_inverse_M.c:108-135), always evaluated in
+//    FP64 with the FP64 stopping threshold: bit-identical to QLA_D3 for D3
+//    inputs; for F3 inputs the FP64 result of the promoted matrix, rounded
+//    once to float (more accurate than the reference's FP32 iteration).
+//  exp: Cayley-Hamilton-reduced Taylor series with FP64 coefficients.  With
+//    B = A / 2^k (|B|_F <= 1) and B^3 = c2 B^2 + c1 B + c0 1, every power
+//    B^j / j! = q0 1 + q1 B + q2 B^2 where (q0,q1,q2) follow the recurrence
+//    q' = (q2 c0, q0 + q2 c1, q1 + q2 c2) / (j+1); summing 26 terms gives
+//    exp(B) = f0 1 + f1 B + f2 B^2 with no eigenvalues involved, so nearly
+//    degenerate spectra need no special case; then k squarings.  All of it in
+//    FP64; F3 outputs are rounded once to float.  The reference's F3/D3 use a
+//    rational approximation with scaling (M_eq_exp_M.c:302-367); agreement is
+//    checked against its FP64 (D3) result.
+#pragma once
+#include "qla_engine.cuh"
+
+namespace qlab {
+
+template <typename R>
+using C9 = Cx<R>[9];
+
+__device__ __forceinline__ Cx<double> cd(Cx<float> v) { return Cx<double>{(double)v.re, (double)v.im}; }
+__device__ __forceinline__ Cx<double> cd(Cx<double> v) { return v; }
+template <typename R>
+__device__ __forceinline__ Cx<R> cround(Cx<double> v) {
+  return Cx<R>{(R)v.re, (R)v.im};
+}
+
+// explicitly rounded complex helpers (qla_complex.h order)
+template <typename R>
+__device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {  // c_eq_c_times_c
+  return Cx<R>{rsub(rmul(a.re, b.re), rmul(a.im, b.im)), radd(rmul(a.re, b.im), rmul(a.im, b.re))};
+}
+template <typename R>
+__device__ __forceinline__ void cmms(Cx<R>& c, Cx<R> a, Cx<R> b) {  // c_meq_c_times_c
+  c.re = rsub(c.re, rsub(rmul(a.re, b.re), rmul(a.im, b.im)));
+  c.im = rsub(c.im, radd(rmul(a.re, b.im), rmul(a.im, b.re)));
+}
+template <typename R>
+__device__ __forceinline__ void cpms(Cx<R>& c, Cx<R> a, Cx<R> b) {  // c_peq_c_times_c
+  c.re = radd(c.re, rsub(rmul(a.re, b.re), rmul(a.im, b.im)));
+  c.im = radd(c.im, radd(rmul(a.re, b.im), rmul(a.im, b.re)));
+}
+template <typename R>
+__device__ __forceinline__ R cnorm2(Cx<R> a) {
+  return radd(rmul(a.re, a.re), rmul(a.im, a.im));
+}
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// r = a * b for 3x3 (M_eq_M_times_M order: x = 0; x += a_ik b_kj)
+template <typename R>
+__device__ __forceinline__ void mat3_mul(Cx<R> (&r)[9], const Cx<R> (&a)[9], const Cx<R> (&b)[9]) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      Cx<R> x{R(0), R(0)};
+#pragma unroll
+      for (int k = 0; k < 3; k++) cpms(x, a[i * 3 + k], b[k * 3 + j]);
+      r[i * 3 + j] = x;
+    }
+}
+
+// sum |a_ij|^2, each term in R, summed in double (the templates' maxev2)
+template <typename R>
+__device__ __forceinline__ double fnorm2_3(const Cx<R> (&a)[9]) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; k++) s = __dadd_rn(s, (double)cnorm2(a[k]));
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// C_eq_det_M (nc = 3)
+template <typename R>
+__device__ __forceinline__ Cx<R> det3(const Cx<R> (&a)[9]) {
+  Cx<R> det2 = cmul(a[0], a[4]);
+  cmms(det2, a[1], a[3]);
+  Cx<R> det1 = cmul(a[2], a[3]);
+  cmms(det1, a[0], a[5]);
+  Cx<R> det0 = cmul(a[1], a[5]);
+  cmms(det0, a[2], a[4]);
+  Cx<R> det = cmul(det2, a[8]);
+  cpms(det, det1, a[7]);
+  cpms(det, det0, a[6]);
+  return det;
+}
+
+template <typename R_>
+struct DetOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 1, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1],
+                                               const Cx<R> (&)[1], Cx<R> (&y)[1]) {
+    y[0] = det3(a);
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// ---------------------------------------------------------------------------
+// M_eq_inverse_M (nc = 3)
+template <typename R_>
+struct InverseOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1],
+                                               const Cx<R> (&)[1], Cx<R> (&x)[9]) {
+    Cx<R> det2 = cmul(a[0], a[4]);
+    cmms(det2, a[1], a[3]);
+    Cx<R> det1 = cmul(a[2], a[3]);
+    cmms(det1, a[0], a[5]);
+    Cx<R> det0 = cmul(a[1], a[5]);
+    cmms(det0, a[2], a[4]);
+    Cx<R> det = cmul(det2, a[8]);
+    cpms(det, det1, a[7]);
+    cpms(det, det0, a[6]);
+    // QLA_c_eq_r_div_c(idet, 1, det): t = 1/|det|^2; idet = t*conj(det)
+    const R t = rdiv(R(1), cnorm2(det));
+    const Cx<R> idet{rmul(t, det.re), rmul(-t, det.im)};
+#define QLAB_SET(i0, j0, i1, j1, i2, j2)              \
+  {                                                   \
+    Cx<R> d_ = cmul(a[i1 * 3 + j1], a[i2 * 3 + j2]);  \
+    cmms(d_, a[i1 * 3 + j2], a[i2 * 3 + j1]);         \
+    x[i0 * 3 + j0] = cmul(d_, idet);                  \
+  }
+    QLAB_SET(0, 0, 1, 1, 2, 2);
+    QLAB_SET(0, 1, 2, 1, 0, 2);
+    x[2] = cmul(det0, idet);
+    QLAB_SET(1, 0, 1, 2, 2, 0);
+    QLAB_SET(1, 1, 2, 2, 0, 0);
+    x[5] = cmul(det1, idet);
+    QLAB_SET(2, 0, 1, 0, 2, 1);
+    QLAB_SET(2, 1, 2, 0, 0, 1);
+    x[8] = cmul(det2, idet);
+#undef QLAB_SET
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// ---------------------------------------------------------------------------
+// x = a^-1 b, Gauss-Jordan with partial pivoting (M_eq_M_inverse_M.c:108-135),
+// FP64, rows swapped physically (same arithmetic as the template's row
+// permutation).  Result written into d (in place of the right-hand side).
+__device__ __forceinline__ void gj_solve3(Cx<double> (&c)[9], Cx<double> (&d)[9]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double rmax = cnorm2(c[k * 3 + k]);
+    int imax = k;
+#pragma unroll
+    for (int i = k + 1; i < 3; i++) {
+      const double rr = cnorm2(c[i * 3 + k]);
+      if (rr > rmax) {
+        rmax = rr;
+        imax = i;
+      }
+    }
+#pragma unroll
+    for (int i = k + 1; i < 3; i++) {
+      if (imax == i) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          Cx<double> t = c[k * 3 + j];
+          c[k * 3 + j] = c[i * 3 + j];
+          c[i * 3 + j] = t;
+          t = d[k * 3 + j];
+          d[k * 3 + j] = d[i * 3 + j];
+          d[i * 3 + j] = t;
+        }
+      }
+    }
+    rmax = __ddiv_rn(1.0, rmax);
+    const Cx<double> s{__dmul_rn(rmax, c[k * 3 + k].re), -__dmul_rn(rmax, c[k * 3 + k].im)};
+    c[k * 3 + k] = s;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      if (i == k) continue;
+      const Cx<double> t = cmul(s, c[i * 3 + k]);
+#pragma unroll
+      for (int j = k + 1; j < 3; j++) cmms(c[i * 3 + j], t, c[k * 3 + j]);
+#pragma unroll
+      for (int j = 0; j < 3; j++) cmms(d[i * 3 + j], t, d[k * 3 + j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) d[i * 3 + j] = cmul(c[i * 3 + i], d[i * 3 + j]);
+}
+
+// M_eq_sqrt_M (Newton), FP64
+template <typename R_>
+struct SqrtOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
+  __device__ static void apply(const SiteParams& p, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               Cx<R> (&r)[9]) {
+    Cx<double> ad[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) ad[k] = cd(a[k]);
+    double ds = fnorm2_3(ad);
+    if (ds == 0.0) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) r[k] = Cx<R>{R(0), R(0)};
+      return;
+    }
+    ds = __dsqrt_rn(ds);
+    Cx<double> x[9], e[9], c[9], d[9];
+    const double inv = __ddiv_rn(1.0, ds);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      x[k] = Cx<double>{__dmul_rn(inv, ad[k].re), __dmul_rn(inv, ad[k].im)};  // x = a / ds
+      const double dg = (k % 4 == 0) ? 0.5 : 0.0;                            // e = 0.5 1
+      e[k] = Cx<double>{__dadd_rn(dg, __dmul_rn(-0.5, x[k].re)), __dadd_rn(0.0, __dmul_rn(-0.5, x[k].im))};
+      x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
+    }
+    const double eps = 2.220446049250313080847e-16;  // DBL_EPSILON
+    int nit = 0;
+    double enorm;
+    do {
+      nit++;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        c[k] = x[k];
+        d[k] = e[k];
+      }
+      gj_solve3(c, d);  // d = x^-1 e
+      mat3_mul(c, e, d);  // c = e x^-1 e
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        e[k] = Cx<double>{__dmul_rn(-0.5, c[k].re), __dmul_rn(-0.5, c[k].im)};
+        x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
+      }
+      enorm = fnorm2_3(e);
+    } while (nit < 20 && enorm > eps);
+    const double sds = __dsqrt_rn(ds);
+#pragma unroll
+    for (int k = 0; k < 9; k++) r[k] = cround<R>(Cx<double>{__dmul_rn(sds, x[k].re), __dmul_rn(sds, x[k].im)});
+    (void)p;
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// ---------------------------------------------------------------------------
+// M_eq_exp_M: Cayley-Hamilton-reduced Taylor series in FP64 (see header)
+template <typename R_>
+struct ExpOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
+  static constexpr int kTerms = 26;
+  __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               Cx<R> (&r)[9]) {
+    Cx<double> b[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) b[k] = cd(a[k]);
+    double fn = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) fn += b[k].re * b[k].re + b[k].im * b[k].im;
+    // scale by 2^-k so that |B|_F <= 1 (exact: a power of two)
+    int ks = 0;
+    if (fn > 1.0) {
+      ks = (int)ceil(0.5 * log2(fn));
+      if (ks > 60) ks = 60;
+      const double sc = ldexp(1.0, -ks);
+#pragma unroll
+      for (int k = 0; k < 9; k++) b[k] = Cx<double>{b[k].re * sc, b[k].im * sc};
+    }
+    Cx<double> b2[9];
+    mat3_mul(b2, b, b);
+    const Cx<double> trb{b[0].re + b[4].re + b[8].re, b[0].im + b[4].im + b[8].im};
+    const Cx<double> trb2{b2[0].re + b2[4].re + b2[8].re, b2[0].im + b2[4].im + b2[8].im};
+    const Cx<double> trb_sq = cmul(trb, trb);
+    // B^3 = c2 B^2 + c1 B + c0 1  (Cayley-Hamilton)
+    const Cx<double> c2 = trb;
+    const Cx<double> c1{-0.5 * (trb_sq.re - trb2.re), -0.5 * (trb_sq.im - trb2.im)};
+    const Cx<double> c0 = det3(b);
+    Cx<double> q0{1.0, 0.0}, q1{0.0, 0.0}, q2{0.0, 0.0};
+    Cx<double> f0 = q0, f1 = q1, f2 = q2;
+#pragma unroll 2
+    for (int j = 1; j < kTerms; j++) {
+      const double inv = 1.0 / (double)j;
+      const Cx<double> n0 = cmul(q2, c0);
+      Cx<double> n1 = cmul(q2, c1);
+      Cx<double> n2 = cmul(q2, c2);
+      n1.re += q0.re;
+      n1.im += q0.im;
+      n2.re += q1.re;
+      n2.im += q1.im;
+      q0 = Cx<double>{n0.re * inv, n0.im * inv};
+      q1 = Cx<double>{n1.re * inv, n1.im * inv};
+      q2 = Cx<double>{n2.re * inv, n2.im * inv};
+      f0.re += q0.re;
+      f0.im += q0.im;
+      f1.re += q1.re;
+      f1.im += q1.im;
+      f2.re += q2.re;
+      f2.im += q2.im;
+    }
+    Cx<double> e[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const Cx<double> t1 = cmul(f1, b[k]);
+      const Cx<double> t2 = cmul(f2, b2[k]);
+      e[k] = Cx<double>{t1.re + t2.re, t1.im + t2.im};
+      if (k % 4 == 0) {
+        e[k].re += f0.re;
+        e[k].im += f0.im;
+      }
+    }
+    for (int s = 0; s < ks; s++) {
+      mat3_mul(b2, e, e);
+#pragma unroll
+      for (int k = 0; k < 9; k++) e[k] = b2[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) r[k] = cround<R>(e[k]);
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+}  // namespace qlab

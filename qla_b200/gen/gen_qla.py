@@ -52,7 +52,69 @@ CITE = {
     "norm2": "lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)",
     "dot": "lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)",
     "redot": "lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)",
+    "mfunc": "lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, "
+             "M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143",
 }
+MFUNC_OPS = {"exp": "ExpOp", "sqrt": "SqrtOp", "inverse": "InverseOp"}
+CITE["int"] = "lib/perl/build_qla.pl:1932-2082 (integer fields)"
+# QLA_I_ binary operators offered with veq/xeq only (build_qla.pl:1932-2082)
+INT_BINOPS = {"and": "IC_AND", "divide": "IC_DIVIDE", "eq": "IC_EQ", "ge": "IC_GE", "gt": "IC_GT", "le": "IC_LE",
+              "lshift": "IC_LSHIFT", "lt": "IC_LT", "mask": "IC_MASK", "max": "IC_MAX", "min": "IC_MIN",
+              "minus": "IC_MINUS", "mod": "IC_MOD", "ne": "IC_NE", "or": "IC_OR", "plus": "IC_PLUS",
+              "rshift": "IC_RSHIFT", "xor": "IC_XOR"}
+
+
+def gen_int():
+    """QLA_I_ entry points: the (shape x eqop x indexing) set of the reference's
+    integer library."""
+    fns = []
+    kid = '"I_int"'
+
+    def field(name, ptr):
+        if ptr:
+            return ("QLA_Int *RESTRICT *", name), f"qlab::op_ptr((const void* const*){name})"
+        return ("QLA_Int *RESTRICT", name), f"qlab::op_contig({name})"
+
+    def emit(shape, var, eq, code, fields, scalar):
+        name = f"QLA_I_{var}{eq}_{shape}"
+        params = [("QLA_Int *RESTRICT", "r")]
+        if scalar:
+            params.append(("QLA_Int *RESTRICT", "a"))
+        ops = []
+        for fname_, ptr in fields:
+            pp, oo = field(fname_, ptr)
+            params.append(pp)
+            ops.append(oo)
+        if var == "x":
+            params.append(("int *", "index"))
+        params.append(("int", "n"))
+        while len(ops) < 3:
+            ops.append("qlab::Opnd{}")
+        body = (f"qlab::api_int({kid}, qlab::{code}, {EQ_ENUM[eq]}, (int*)r, {'(const int*)a' if scalar else 'nullptr'}, "
+                f"{ops[0]}, {ops[1]}, {ops[2]}, {len(fields)}, {'index' if var == 'x' else 'nullptr'}, n);")
+        fns.append(Fn(name, params, body, "int", CITE["int"], dict(dest="I", eqop=eq, var=var, shape=shape)))
+
+    P = [("", False), ("p", True)]
+    for var in ["v", "x"]:
+        for eq in EQOPS:
+            for pa, xa in P:
+                emit(f"{pa}I", var, eq, "IC_COPY", [("a", xa)], False)
+                for pb, xb in P:
+                    emit(f"{pa}I_times_{pb}I", var, eq, "IC_TIMES", [("a", xa), ("b", xb)], False)
+                emit(f"i_times_{pa}I", var, eq, "IC_S_TIMES", [("b", xa)], True)
+            emit("i", var, eq, "IC_S", [], True)
+        for opn, code in INT_BINOPS.items():
+            for pa, xa in P:
+                for pb, xb in P:
+                    emit(f"{pa}I_{opn}_{pb}I", var, "eq", code, [("a", xa), ("b", xb)], False)
+        for pa, xa in P:
+            for pm in ("plus", "minus"):
+                for pb, xb in P:
+                    emit(f"i_times_{pa}I_{pm}_{pb}I", var, "eq", "IC_S_TIMES_PLUS" if pm == "plus" else
+                         "IC_S_TIMES_MINUS", [("b", xa), ("c", xb)], True)
+            emit(f"not_{pa}I", var, "eq", "IC_NOT", [("a", xa)], False)
+        emit("zero", var, "eq", "IC_ZERO", [], False)
+    return fns
 
 
 class Fn:
@@ -188,6 +250,25 @@ def gen_pc(pc, R, P):
             body = (f"qlab::api_map<qlab::CopyOp<{R}, {nc}>>({kid('copy_' + T)}, r, qlab::op_idx(a, ja), "
                     f"qlab::Opnd{{}}, nullptr, n, {EQ_ENUM[eq]});")
             fns.append(Fn(name, params, body, "copy", CITE["copy_x"], dict(dest=T, eqop=eq, var="xa", a="x" + T)))
+    # ---- colour-matrix functions
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        for src, p1 in [("M", False), ("pM", True)]:
+            pa, oa = operand(pc, "M", p1, "a")
+            tail = [("int *", "index")] if var == "x" else []
+            for fname, opname in MFUNC_OPS.items():
+                name = f"QLA_{pc}_M_{var}eq_{fname}_{src}"
+                params = [(f"{ptype(pc, 'M')} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                body = (f"qlab::api_map<qlab::{opname}<{R}>>({kid('mfunc_' + fname)}, r, {oa}, qlab::Opnd{{}}, "
+                        f"{gang}, n, qlab::EQ);")
+                fns.append(Fn(name, params, body, "mfunc", CITE["mfunc"], dict(dest="M", eqop="eq", var=var, a=src,
+                                                                                fn=fname)))
+            name = f"QLA_{pc}_C_{var}eq_det_{src}"
+            params = [(f"QLA_{P}_Complex *RESTRICT", "r"), pa] + tail + [("int", "n")]
+            body = (f"qlab::api_map<qlab::DetOp<{R}>>({kid('mfunc_det')}, r, {oa}, qlab::Opnd{{}}, {gang}, n, "
+                    f"qlab::EQ);")
+            fns.append(Fn(name, params, body, "mfunc", CITE["mfunc"], dict(dest="C", eqop="eq", var=var, a=src,
+                                                                            fn="det")))
     # ---- global reductions
     red_pcs = [(pc, R, P)]
     if pc == "F3":
@@ -269,7 +350,7 @@ CU_TOP = """// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
 // QLA {pc} {family} entry points (extern "C"), reference: {cite}
 #include "../../../include/qla_b200_types.h"
 #include "../qla_api.cuh"
-
+{extra_includes}
 extern "C" {{
 """
 
@@ -289,8 +370,8 @@ def main():
     manifest = []
     groups = {}
     headers = {}
-    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D")]:
-        for fn in gen_pc(pc, R, P):
+    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None)]:
+        for fn in (gen_int() if pc == "I" else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
@@ -298,7 +379,7 @@ def main():
                                  ctypes=[t.replace("RESTRICT", "").strip() for t, _ in fn.params], **fn.kinds))
     written = 0
     for hpc, fns in headers.items():
-        fname = f"qla_b200_{hpc.lower()}.h"
+        fname = f"qla_b200_{'int' if hpc == 'I' else hpc.lower()}.h"
         text = HEADER_TOP.format(fname=fname, pc=hpc, guard=f"QLA_B200_{hpc}_H")
         fam = None
         for fn in fns:
@@ -310,7 +391,8 @@ def main():
         text += HEADER_END
         written += write_if_changed(os.path.join(OUT_INC, fname), text)
     for (pc, family), fns in groups.items():
-        text = CU_TOP.format(pc=pc, family=family, cite=CITE[family])
+        extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n'}.get(family, "")
+        text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:
             text += "QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  " + fn.body + "\n}\n\n"
         text += "}  // extern \"C\"\n"

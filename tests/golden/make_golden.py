@@ -123,6 +123,56 @@ def build(pc, dt, seed):
                 call(f"QLA_{rpc}_r_veq_re_{t}_dot_{t}", ctypes.c_void_p(o.ctypes.data),
                      ctypes.c_void_p(src.ctypes.data), ctypes.c_void_p(b.ctypes.data), N)
                 out[f"QLA_{rpc}_r_veq_re_{t}_dot_{t}"] = o
+    # colour-matrix functions (code templates): exp of anti-Hermitian and of
+    # general matrices, sqrt of positive Hermitian, inverse and det of general
+    ins["mf_exp"] = T.antihermitian_exp_inputs(rng, N, dt)[0]
+    ins["mf_gen"] = (T.gaussian_field(rng, N, 9, dt) * 0.8).astype(dt)
+    ins["mf_pos"] = T.positive_hermitian_inputs(rng, N, dt)
+    for fname, src in (("M_veq_exp_M", "mf_exp"), ("M_veq_exp_M", "mf_gen"), ("M_veq_sqrt_M", "mf_pos"),
+                       ("M_veq_inverse_M", "mf_gen"), ("C_veq_det_M", "mf_gen")):
+        r = np.zeros((N, 2 if fname.startswith("C") else 18), dtype=dt)
+        call(f"QLA_{pc}_{fname}", ctypes.c_void_p(r.ctypes.data), ctypes.c_void_p(ins[src].ctypes.data), N)
+        out[f"QLA_{pc}_{fname}|{src}"] = r
+    # the same templates in the N-colour build (FN / DN) at nc = 4 and 8
+    npc = "FN" if pc == "F3" else "DN"
+    for nc in (4, 8):
+        g = (rng.standard_normal((N, 2 * nc * nc)) * (0.25 if nc == 8 else 0.4)).astype(dt)
+        pos = T.positive_hermitian_inputs(rng, N, dt, nc=nc)
+        ins[f"mfN{nc}_gen"] = g
+        ins[f"mfN{nc}_pos"] = pos
+        for fname, src in (("M_veq_exp_M", "gen"), ("M_veq_sqrt_M", "pos"), ("M_veq_inverse_M", "gen"),
+                           ("C_veq_det_M", "gen")):
+            r = np.zeros((N, 2 if fname.startswith("C") else 2 * nc * nc), dtype=dt)
+            call(f"QLA_{npc}_{fname}", nc, ctypes.c_void_p(r.ctypes.data),
+                 ctypes.c_void_p(ins[f"mfN{nc}_{src}"].ctypes.data), N)
+            out[f"QLA_{npc}_{fname}|mfN{nc}_{src}"] = r
+    return ins, out
+
+
+def build_int(seed):
+    """Every QLA_I_ v/x entry point of the reference on int_inputs()."""
+    import re
+    rng = np.random.default_rng(seed)
+    R = T.ref()
+    ins = T.int_inputs(rng, N, NS)
+    names = sorted(set(re.findall(r"void (QLA_I_[vx]\w+) \(", open(os.path.join(
+        os.path.dirname(T.REF_SO), "gen", "include", "qla_int.h")).read())))
+    out = {}
+    keep = []
+
+    def arr(a):
+        keep.append(a)
+        return ctypes.c_void_p(a.ctypes.data)
+
+    def ptrs(a, idx):
+        p = (ctypes.c_void_p * len(idx))(*[a.ctypes.data + 4 * int(j) for j in idx])
+        keep.append(p)
+        return p
+
+    for name in names:
+        r = ins["r0"].copy()
+        getattr(R, name)(*T.int_call_args(name, ins, N, arr(r), arr, ptrs))
+        out[name] = r
     return ins, out
 
 
@@ -138,6 +188,12 @@ def main():
         path = os.path.join(HERE, f"qla_{pc.lower()}_golden.npz")
         np.savez_compressed(path, **blob)
         print(f"{path}: {len(out)} reference outputs")
+    ins, out = build_int(303)
+    blob = {"in__" + k: v for k, v in ins.items()}
+    blob.update({"out__" + k: v for k, v in out.items()})
+    path = os.path.join(HERE, "qla_int_golden.npz")
+    np.savez_compressed(path, **blob)
+    print(f"{path}: {len(out)} reference outputs")
 
 
 if __name__ == "__main__":

@@ -200,3 +200,146 @@ def bits_equal(a, b):
     if a.shape != b.shape:
         return False
     return bool(np.array_equal(a, b, equal_nan=True))
+
+
+# ---------------------------------------------------------------------------
+# matrix-function inputs (config 5) and oracle wrapper
+
+MF = {"exp": 0, "sqrt": 1, "inverse": 2, "det": 3}
+
+
+def to_complex(m, nc=3):
+    m = np.asarray(m, dtype=np.float64)
+    return (m[:, 0::2] + 1j * m[:, 1::2]).reshape(-1, nc, nc)
+
+
+def from_complex(z, dtype):
+    n = z.shape[0]
+    out = np.empty((n, z.shape[1] * z.shape[2], 2))
+    out[..., 0] = z.reshape(n, -1).real
+    out[..., 1] = z.reshape(n, -1).imag
+    return out.reshape(n, -1).astype(dtype)
+
+
+def antihermitian_exp_inputs(rng, n, dtype, degenerate_frac=0.1, nc=3):
+    """A = i Q, Q = W diag(lambda) W^+ with W Haar, lambda real traceless with
+    spectral norm ~ U[0,3]; a fraction of sites get a pair with |l_i - l_j| < 1e-6."""
+    w = to_complex(haar_su3(rng, n, np.float64, nc), nc)
+    lam = rng.uniform(-1, 1, (n, nc))
+    lam -= lam.mean(axis=1, keepdims=True)
+    lam *= (rng.uniform(0, 3, n) / np.maximum(np.abs(lam).max(axis=1), 1e-300))[:, None]
+    deg = rng.random(n) < degenerate_frac
+    gap = rng.uniform(0, 1e-6, n)
+    lam[deg, 1] = lam[deg, 0] + gap[deg]
+    lam[deg] -= lam[deg].mean(axis=1, keepdims=True)
+    q = w @ (lam[:, :, None] * np.conj(np.transpose(w, (0, 2, 1))))
+    return from_complex(1j * q, dtype), deg
+
+
+def positive_hermitian_inputs(rng, n, dtype, nc=3):
+    """A = B^+ B + 0.1 1 with B complex Gaussian."""
+    b = (rng.standard_normal((n, nc, nc)) + 1j * rng.standard_normal((n, nc, nc))) / np.sqrt(2)
+    h = np.conj(np.transpose(b, (0, 2, 1))) @ b + 0.1 * np.eye(nc)
+    return from_complex(h, dtype)
+
+
+def ora_mfunc(a, n, which, nc=3):
+    f = getattr(oracle(), "ora_mfunc_" + rtype(a.dtype))
+    nout = 1 if which == "det" else nc * nc
+    r = np.zeros((n, 2 * nout), dtype=a.dtype)
+    f(ptr(r), ptr(a), ctypes.c_long(n), nc, MF[which])
+    return r
+
+
+# ---------------------------------------------------------------------------
+# QLA_I_ integer ops
+
+INT_CODES = {"and": 6, "divide": 4, "eq": 11, "ge": 16, "gt": 15, "le": 14, "lshift": 9, "lt": 13, "mask": 19,
+             "max": 17, "min": 18, "minus": 3, "mod": 5, "ne": 12, "or": 7, "plus": 2, "rshift": 10, "xor": 8}
+
+
+def int_shape(shape):
+    """(code, [pointer flag per field operand], takes a scalar) for a QLA_I_ shape."""
+    import re
+    p = lambda t: t.startswith("p")  # noqa: E731
+    if shape in ("I", "pI"):
+        return 0, [p(shape)], False
+    if shape == "i":
+        return 22, [], True
+    if shape == "zero":
+        return 21, [], False
+    m = re.match(r"^(p?I)_times_(p?I)$", shape)
+    if m:
+        return 1, [p(m.group(1)), p(m.group(2))], False
+    m = re.match(r"^i_times_(p?I)$", shape)
+    if m:
+        return 23, [p(m.group(1))], True
+    m = re.match(r"^i_times_(p?I)_(plus|minus)_(p?I)$", shape)
+    if m:
+        return (24 if m.group(2) == "plus" else 25), [p(m.group(1)), p(m.group(3))], True
+    m = re.match(r"^not_(p?I)$", shape)
+    if m:
+        return 20, [p(m.group(1))], False
+    m = re.match(r"^(p?I)_(\w+)_(p?I)$", shape)
+    return INT_CODES[m.group(2)], [p(m.group(1)), p(m.group(3))], False
+
+
+def int_inputs(rng, n, ns):
+    """Seeded int32 operands valid for every op (divisors and shift counts in
+    1..31, a 0/1 mask), plus pointer/gang index tables."""
+    return {
+        "a": rng.integers(-1_000_000, 1_000_000, ns).astype(np.int32),
+        "b": rng.integers(-1_000_000, 1_000_000, ns).astype(np.int32),
+        "bs": rng.integers(1, 32, ns).astype(np.int32),
+        "bm": rng.integers(0, 2, ns).astype(np.int32),
+        "c": rng.integers(-1_000_000, 1_000_000, ns).astype(np.int32),
+        "r0": rng.integers(-1_000_000, 1_000_000, n).astype(np.int32),
+        "ia": rng.integers(0, ns, n).astype(np.int32),
+        "ib": rng.integers(0, ns, n).astype(np.int32),
+        "gang": rng.permutation(n).astype(np.int32),
+        "s": np.array([-37], dtype=np.int32),
+    }
+
+
+def int_second(code):
+    return "bs" if code in (4, 5, 9, 10) else ("bm" if code == 19 else "b")
+
+
+def ora_int(name, ins, n):
+    """Oracle result of QLA_I_<var><eqop>_<shape> on int_inputs()."""
+    import re
+    m = re.match(r"QLA_I_([vx])(eq|peq|meq|eqm)_(\w+)$", name)
+    var, eq, shape = m.groups()
+    code, ptrs, scal = int_shape(shape)
+    r = ins["r0"].copy()
+    srcs = ["a", int_second(code), "c"] if not scal else [("a"), int_second(code), "c"]
+    if scal:
+        srcs = ["a", "b"]  # the scalar forms take fields b (and c) of the C API; use a, b here
+    fld = [ins[srcs[j]] for j in range(len(ptrs))] + [None] * (3 - len(ptrs))
+    idx = [(ins["ia"] if j == 0 else ins["ib"]) if ptrs[j] else None for j in range(len(ptrs))] + \
+          [None] * (3 - len(ptrs))
+    gang = ins["gang"] if var == "x" else None
+    f = oracle().ora_int
+    f(code, EQOPS[eq], ptr(r), ptr(fld[0]), ptr(fld[1]), ptr(fld[2]), int(ins["s"][0]), ctypes.c_long(n),
+      ptr(idx[0]), ptr(idx[1]), ptr(idx[2]), ptr(gang))
+    return r
+
+
+def int_call_args(name, ins, n, r, to_arr, to_ptrs):
+    """Argument list of the C entry point, built with the caller's array
+    constructors (host numpy for the reference, device for the product)."""
+    import re
+    m = re.match(r"QLA_I_([vx])(eq|peq|meq|eqm)_(\w+)$", name)
+    var, eq, shape = m.groups()
+    code, ptrs, scal = int_shape(shape)
+    srcs = ["a", "b"] if scal else ["a", int_second(code)]
+    args = [r]
+    if scal:
+        args.append(to_arr(ins["s"]))
+    for j, isp in enumerate(ptrs):
+        src = ins[srcs[j]]
+        args.append(to_ptrs(src, ins["ia"] if j == 0 else ins["ib"]) if isp else to_arr(src))
+    if var == "x":
+        args.append(to_arr(ins["gang"]))
+    args.append(n)
+    return args

@@ -73,6 +73,12 @@ def replay(pc, name, ins):
         v = T.ora_dot(ins[t], b, n, NC[t])
         odt = np.float32 if rpc == "F3" else np.float64
         return np.array([v.real], dtype=odt) if re_ else np.array([v.real, v.imag], dtype=odt)
+    m = re.match(r"QLA_(F3|D3|FN|DN)_(M|C)_veq_(exp|sqrt|inverse|det)_M$", key)
+    if m:
+        pcx, _, fname = m.group(1), m.group(2), m.group(3)
+        src = extra[0]
+        nc = 3 if pcx in ("F3", "D3") else int(src[3])
+        return T.ora_mfunc(ins[src], n, fname, nc=nc)
     raise KeyError(name)
 
 
@@ -137,3 +143,36 @@ def test_oracle_detects_a_planted_mistake():
     ins["M"] = m
     name = "QLA_F3_V_veq_M_times_V"
     assert not T.bits_equal(replay("F3", name, ins), outs[name])
+
+
+def test_int_oracle_matches_reference_golden_vectors():
+    """All 238 QLA_I_ v/x entry points of the reference integer library."""
+    z = np.load(os.path.join(GOLDEN, "qla_int_golden.npz"))
+    ins = {k[4:]: z[k] for k in z.files if k.startswith("in__")}
+    outs = {k[5:]: z[k] for k in z.files if k.startswith("out__")}
+    assert len(outs) == 238
+    bad = [nm for nm, w in outs.items() if not np.array_equal(T.ora_int(nm, ins, len(ins["r0"])), w)]
+    assert not bad, bad[:5]
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref (reference headers) not built")
+def test_prototypes_match_reference_headers():
+    """Every generated entry point that the reference also generates has the
+    reference's parameter list (types and order); the rest are the documented
+    per-operand index (`xX`) forms."""
+    import qla_b200
+    ref = {}
+    for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h"):
+        txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
+        for m in re.finditer(r"void (QLA_\w+) \((.*?)\);", txt):
+            params = [p.replace("QLA_RESTRICT", "").strip() for p in m.group(2).split(",")]
+            # drop the trailing parameter name, keep the type without blanks
+            ref[m.group(1)] = [re.match(r"^(.*?)\w+$", p).group(1).replace(" ", "") for p in params]
+    extra = []
+    for e in qla_b200.manifest():
+        if e["name"] not in ref:
+            extra.append(e["name"])
+            continue
+        ours = [t.replace(" ", "") for t in e["ctypes"]]
+        assert ours == ref[e["name"]], (e["name"], ours, ref[e["name"]])
+    assert all(re.search(r"_x[VHDMI]$", nm) for nm in extra), [nm for nm in extra if not re.search(r"_x[VHDMI]$", nm)][:5]
