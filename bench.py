@@ -421,6 +421,205 @@ def run_gpu_arm(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# secondary workloads (SURVEY configs 1, 2, 4, 5): one JSON line each, same
+# timing rules (warm-up, CUDA events on the launching stream, inputs > L2
+# unless stated).  The default workload above is the benchmark line.
+def _events_time(torch, stream, fn, reps, warmup=3):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_workload(args):
+    import numpy as np
+    import torch
+
+    import qla_b200 as qla
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    qla.set_stream(stream)
+    peak, peak_kind = peaks()
+    L = qla.lib()
+    V = lambda t: ctypes.c_void_p(t if isinstance(t, int) else t.data_ptr())  # noqa: E731
+    out = {"workload": args.workload, "peak_gbs": peak, "peak_kind": peak_kind, "data": "synthetic, seeded"}
+    reps = max(args.steps, 5)
+    if args.workload == "hop":
+        dims = [32, 32, 32, 64]
+        n = int(np.prod(dims))
+        res = {}
+        for pc, dt, e in (("F3", torch.float32, 1), ("D3", torch.float64, 2)):
+            D = torch.randn(n, 24, device="cuda", dtype=dt)
+            Out = torch.zeros(n, 24, device="cuda", dtype=dt)
+            H = torch.empty(n, 12, device="cuda", dtype=dt)
+            H2 = torch.empty(n, 12, device="cuda", dtype=dt)
+            U = [torch.randn(n, 18, device="cuda", dtype=dt) for _ in range(4)]
+            Vv = torch.randn(n, 6, device="cuda", dtype=dt)
+            Vo = torch.empty(n, 6, device="cuda", dtype=dt)
+            nbr = {}
+            for mu in range(4):
+                for sg in (1, -1):
+                    nbr[(mu, sg)] = torch.empty(n, dtype=torch.int32, device="cuda")
+                    qla.shift_index(nbr[(mu, sg)], dims, mu, sg)
+            sp, mh, rc = (getattr(L, f"QLA_{pc}_H_veq_spproj_D"), getattr(L, f"QLA_{pc}_H_eq_M_times_xH"),
+                          getattr(L, f"QLA_{pc}_D_vpeq_sprecon_H"))
+
+            def hop():
+                for mu in range(4):
+                    for sg in (1, -1):
+                        sp(V(H), V(D), mu, sg, n)
+                        mh(V(H2), V(U[mu]), V(H), V(nbr[(mu, sg)]), n)
+                        rc(V(Out), V(H2), mu, sg, n)
+            ms = _events_time(torch, stream, hop, reps)
+            t_sp = _events_time(torch, stream, lambda: sp(V(H), V(D), 0, 1, n), reps * 4)
+            t_mh = _events_time(torch, stream, lambda: mh(V(H2), V(U[0]), V(H), V(nbr[(0, 1)]), n), reps * 4)
+            t_rc = _events_time(torch, stream, lambda: rc(V(Out), V(H2), 0, 1, n), reps * 4)
+            mv = getattr(L, f"QLA_{pc}_V_eq_M_times_xV")
+            t_mv = _events_time(torch, stream, lambda: mv(V(Vo), V(U[0]), V(Vv), V(nbr[(0, 1)]), n), reps * 4)
+            ptrs = (Vv.data_ptr() + nbr[(0, 1)].long() * 24 * e).contiguous()
+            mvp = getattr(L, f"QLA_{pc}_V_veq_M_times_pV")
+            t_mvp = _events_time(torch, stream, lambda: mvp(V(Vo), V(U[0]), V(ptrs), n), reps * 4)
+            qla.check("hop")
+            b = {"spproj": 144 * e, "M_times_xH": 168 * e + 4, "sprecon": 240 * e, "M_times_xV": 120 * e + 4,
+                 "M_times_pV": 120 * e + 8}
+            tk = {"spproj": t_sp, "M_times_xH": t_mh, "sprecon": t_rc, "M_times_xV": t_mv, "M_times_pV": t_mvp}
+            res[pc] = {"site_updates_per_s": n / (ms / 1e3), "ms_per_hop": ms,
+                       "hbm_frac_hop": n * 8 * sum(b[k] for k in ("spproj", "M_times_xH", "sprecon")) / (ms / 1e3)
+                       / 1e9 / peak,
+                       "kernels": {k: {"us": 1e3 * tk[k], "gbs": b[k] * n / (tk[k] / 1e3) / 1e9,
+                                       "frac": b[k] * n / (tk[k] / 1e3) / 1e9 / peak} for k in tk}}
+            del D, Out, H, H2, U, Vv, Vo, nbr, ptrs
+            torch.cuda.empty_cache()
+        out.update({"metric": "Wilson-hop level-1 sequence (8 x spproj, M_times_xH, vpeq_sprecon), 32^3x64",
+                    "unit": "site-updates/s", "value": res["F3"]["site_updates_per_s"], "F3": res["F3"],
+                    "D3": res["D3"], "speedup_vs_fp64": res["F3"]["ms_per_hop"] and
+                    res["D3"]["ms_per_hop"] / res["F3"]["ms_per_hop"]})
+    elif args.workload == "batched":
+        rng = np.random.default_rng(4)
+        choices = [8, 12, 16, 20, 24, 32]
+        dims_list = [[int(x) for x in rng.choice(choices, 4)] for _ in range(64)]
+        vols = [int(np.prod(d)) for d in dims_list]
+
+        def make(dlist):
+            """one field per lattice: links u, u2, vector v, +mu neighbour table"""
+            fl = []
+            for k, dims in enumerate(dlist):
+                n = int(np.prod(dims))
+                nbr = torch.empty(n, dtype=torch.int32, device="cuda")
+                qla.shift_index(nbr, dims, k % 4, 1)
+                fl.append({"r": torch.empty(n, 18, device="cuda"), "u": torch.randn(n, 18, device="cuda"),
+                           "u2": torch.randn(n, 18, device="cuda"), "nbr": nbr,
+                           "w": torch.empty(n, 6, device="cuda"), "v": torch.randn(n, 6, device="cuda"), "n": n})
+            return fl
+        tot = sum(vols)
+        uneven = make(dims_list)
+        plan = qla.BatchPlan(uneven)
+        g = torch.cuda.CUDAGraph()
+        s2 = torch.cuda.Stream()
+        with torch.cuda.stream(s2):
+            qla.set_stream(s2)
+            plan.run()
+            torch.cuda.synchronize()
+            with torch.cuda.graph(g, stream=s2):
+                plan.run()
+        qla.set_stream(stream)
+        ms_b = _events_time(torch, stream, g.replay, reps)
+        mxm, mxv = L.QLA_F3_M_eq_M_times_xM, L.QLA_F3_V_veq_M_times_V
+
+        def separate():
+            for f in uneven:
+                mxm(V(f["r"]), V(f["u"]), V(f["u2"]), V(f["nbr"]), f["n"])
+                mxv(V(f["w"]), V(f["r"]), V(f["v"]), f["n"])
+        ms_s = _events_time(torch, stream, separate, reps)
+        del g
+        plan.close()
+        del uneven
+        torch.cuda.empty_cache()
+        # equal-volume batch of the same total: 64 lattices 16x16x16xLt
+        lt = max(1, round(tot / 64 / 4096))
+        even_n = 4096 * lt
+        even = make([[16, 16, 16, lt]] * 64)
+        plan_e = qla.BatchPlan(even)
+        ms_e = _events_time(torch, stream, plan_e.run, reps)
+        plan_e.close()
+        qla.check("batched")
+        rate_b = tot / (ms_b / 1e3)
+        rate_e = 64 * even_n / (ms_e / 1e3)
+        out.update({"metric": "batched uneven-volume M_times_xM + M_times_V (64 F3 fields, extents in "
+                              "{8..32}^4), one persistent launch replayed from a CUDA graph",
+                    "unit": "site-updates/s", "value": rate_b, "total_sites": tot,
+                    "ms_batched_graph": ms_b, "ms_128_separate_launches": ms_s,
+                    "speedup_vs_separate": ms_s / ms_b, "equal_volume_rate": rate_e,
+                    "uneven_vs_equal_volume": rate_b / rate_e,
+                    "hbm_frac": rate_b * (72 * 3 + 24 * 2 + 4) / 1e9 / peak,
+                    "bytes_per_site": "U 72 + U2 gather 72 + nbr 4 + V 24 + R 72 + W 24 = 268"})
+    elif args.workload == "mfunc":
+        n = 32 * 32 * 32 * 64
+        res = {}
+        for pc, dt in (("F3", torch.float32), ("D3", torch.float64)):
+            a = torch.randn(n, 18, device="cuda", dtype=dt) * 0.5
+            r = torch.empty(n, 18, device="cuda", dtype=dt)
+            c = torch.empty(n, 2, device="cuda", dtype=dt)
+            e = 4 if pc == "F3" else 8
+            for fname, f, outt, nb in (("exp", getattr(L, f"QLA_{pc}_M_veq_exp_M"), r, 36),
+                                       ("sqrt", getattr(L, f"QLA_{pc}_M_veq_sqrt_M"), r, 36),
+                                       ("inverse", getattr(L, f"QLA_{pc}_M_veq_inverse_M"), r, 36),
+                                       ("det", getattr(L, f"QLA_{pc}_C_veq_det_M"), c, 20)):
+                src = a
+                if fname == "sqrt":
+                    z = torch.complex(a[:, 0::2].double(), a[:, 1::2].double()).reshape(n, 3, 3)
+                    h = z.conj().transpose(1, 2) @ z + 0.1 * torch.eye(3, device="cuda", dtype=torch.complex128)
+                    src = torch.view_as_real(h.reshape(n, 9)).reshape(n, 18).to(dt).contiguous()
+                    del z, h
+                ms = _events_time(torch, stream, lambda: f(V(outt), V(src), n), reps)
+                res[f"{pc}_{fname}"] = {"site_updates_per_s": n / (ms / 1e3), "us": 1e3 * ms,
+                                        "gbs": nb * e * n / (ms / 1e3) / 1e9}
+            qla.check("mfunc")
+            del a, r, c
+            torch.cuda.empty_cache()
+        out.update({"metric": "matrix functions exp/sqrt/inverse/det on 32^3x64 sites", "unit": "site-updates/s",
+                    "value": res["F3_exp"]["site_updates_per_s"], "ops": res})
+    elif args.workload == "config1":
+        n = 16 ** 4
+        res = {}
+        for pc, dt in (("F3", torch.float32), ("D3", torch.float64)):
+            a = torch.randn(n, 18, device="cuda", dtype=dt)
+            b = torch.randn(n, 6, device="cuda", dtype=dt)
+            r = torch.empty(n, 6, device="cuda", dtype=dt)
+            o = torch.zeros(1, dtype=torch.float64, device="cuda")
+            rp = "DF3" if pc == "F3" else "D3"
+            for nm, fn in (("V_veq_M_times_V", lambda: getattr(L, f"QLA_{pc}_V_veq_M_times_V")(V(r), V(a), V(b), n)),
+                           ("V_veq_Ma_times_V", lambda: getattr(L, f"QLA_{pc}_V_veq_Ma_times_V")(V(r), V(a), V(b), n)),
+                           ("r_veq_norm2_V", lambda: getattr(L, f"QLA_{rp}_r_veq_norm2_V")(V(o), V(b), n))):
+                g = torch.cuda.CUDAGraph()
+                s2 = torch.cuda.Stream()
+                with torch.cuda.stream(s2):
+                    qla.set_stream(s2)
+                    fn()
+                    torch.cuda.synchronize()
+                    with torch.cuda.graph(g, stream=s2):
+                        for _ in range(1000):
+                            fn()
+                qla.set_stream(stream)
+                ms = _events_time(torch, stream, g.replay, 3)
+                res[f"{pc}_{nm}"] = {"us_per_call": ms, "site_updates_per_s": n * 1000 / (ms / 1e3)}
+                del g
+            qla.check("config1")
+        out.update({"metric": "16^4 F3/D3 V_veq_M_times_V, V_veq_Ma_times_V, r_veq_norm2_V (L2-resident, "
+                              "CUDA graph of 1000 launches)", "unit": "site-updates/s",
+                    "value": res["F3_V_veq_M_times_V"]["site_updates_per_s"], "ops": res,
+                    "note": "8 MB working set lives in L2; no HBM fraction is claimed"})
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -434,12 +633,16 @@ def main():
     ap.add_argument("--iters", type=int, default=ITERS)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "config1"],
+                    help="cg_chain is the benchmark line; the others measure the remaining configurations")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("bench.py: warm-up raised to 3 steps", file=sys.stderr)
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload != "cg_chain":
+        run_workload(args)
     else:
         run_gpu_arm(args)
 

@@ -63,6 +63,30 @@ const char *qlagpu_version(void);
  * n = prod(dims).  This is the int32 index stream the `xX` gathers take. */
 void qlagpu_shift_index(int *idx, int nd, const int *dims, int mu, int sign);
 
+/* Batched uneven-volume execution (no counterpart in the reference, which
+ * handles one field per call).  Per field f and site i < n:
+ *     r[i] = u[i] * u2[nbr[i]]   -- QLA_F3_M_eq_M_times_xM
+ *     w[i] = r[i] * v[i]         -- QLA_F3_V_veq_M_times_V
+ * for all fields in one persistent launch; results are bit-identical to the
+ * two calls per field.  qlagpu_F3_batch_plan copies the field table to the
+ * device (it allocates; call it outside any stream capture);
+ * qlagpu_batch_run is a single kernel launch on the current stream with no
+ * allocation or host synchronisation; qlagpu_batch_destroy frees the plan.
+ * Up to 1024 fields; fields whose arrays are not 16-B aligned take the
+ * plain-load path. */
+typedef struct {
+  QLA_F3_ColorMatrix *r;
+  QLA_F3_ColorMatrix *u;
+  QLA_F3_ColorMatrix *u2;
+  int *nbr;
+  QLA_F3_ColorVector *w;
+  QLA_F3_ColorVector *v;
+  long long n;
+} qlagpu_F3_batch_field;
+void *qlagpu_F3_batch_plan(const qlagpu_F3_batch_field *fields, int nfields);
+int qlagpu_batch_run(void *plan);
+void qlagpu_batch_destroy(void *plan);
+
 /* No counterpart in the reference (QLA never touches device memory).
  * QLA_DF3_r_veq_norm2_D for callers that cannot allocate device memory while
  * they run -- e.g. a program whose own pool allocator reserved the GPU's

@@ -182,3 +182,47 @@ def shift_index(idx, dims, mu, sign):
 
 def version():
     return lib().qlagpu_version().decode()
+
+
+class _BatchField(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_void_p), ("u", ctypes.c_void_p), ("u2", ctypes.c_void_p), ("nbr", ctypes.c_void_p),
+                ("w", ctypes.c_void_p), ("v", ctypes.c_void_p), ("n", ctypes.c_longlong)]
+
+
+class BatchPlan:
+    """Plan of the batched uneven-volume sequence (qlagpu_F3_batch_plan): for
+    every field, r = u * u2[nbr] then w = r * v, all in one persistent launch.
+    `fields` is a list of dicts with CUDA tensors (or device addresses) for
+    keys r, u, u2, nbr, w, v and the site count n."""
+
+    def __init__(self, fields):
+        L = lib()
+        L.qlagpu_F3_batch_plan.restype = ctypes.c_void_p
+        L.qlagpu_F3_batch_plan.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.qlagpu_batch_run.restype = ctypes.c_int
+        L.qlagpu_batch_run.argtypes = [ctypes.c_void_p]
+        L.qlagpu_batch_destroy.argtypes = [ctypes.c_void_p]
+        arr = (_BatchField * len(fields))()
+        for k, f in enumerate(fields):
+            arr[k] = _BatchField(*[_addr(f[key]) for key in ("r", "u", "u2", "nbr", "w", "v")], int(f["n"]))
+        self._keep = fields
+        self.handle = L.qlagpu_F3_batch_plan(ctypes.cast(arr, ctypes.c_void_p), len(fields))
+        if not self.handle:
+            check("qlagpu_F3_batch_plan")
+            raise QLAError("qlagpu_F3_batch_plan failed")
+
+    def run(self):
+        rc = lib().qlagpu_batch_run(self.handle)
+        if rc:
+            check("qlagpu_batch_run")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qlagpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
