@@ -115,20 +115,20 @@ class _Fn:
 
     def __call__(self, *args):
         e = self.entry
-        if len(args) != len(e["params"]) and not (len(args) == len(e["params"]) - 1 and e["params"][0] == "r"
-                                                    and e["family"] in ("norm2", "dot", "redot")):
+        red = e["family"] in ("norm2", "dot", "redot")
+        ridx = e["params"].index("r") if red else 0
+        if len(args) != len(e["params"]) and not (red and len(args) == len(e["params"]) - 1):
             raise TypeError(f"{self.name} takes {len(e['params'])} arguments ({', '.join(e['params'])})")
         cargs = []
         keep = []
         ret = None
-        reduction_host = e["family"] in ("norm2", "dot", "redot") and (len(args) < len(e["params"]) or
-                                                                       args[0] is None)
+        reduction_host = red and (len(args) < len(e["params"]) or args[ridx] is None)
         if reduction_host and len(args) < len(e["params"]):
-            args = (None,) + tuple(args)
+            args = tuple(args[:ridx]) + (None,) + tuple(args[ridx:])
         for i, (t, v) in enumerate(zip(e["ctypes"], args)):
             if t == "int":
                 cargs.append(int(v))
-            elif i == 0 and reduction_host:
+            elif i == ridx and reduction_host:
                 ct = _REAL_CT.get(t) or _CPLX_CT.get(t)
                 n = 2 if t in _CPLX_CT else 1
                 buf = (ct * n)()
@@ -170,6 +170,9 @@ class _Namespace:
 F3 = _Namespace("F3")
 D3 = _Namespace("D3")
 DF3 = _Namespace("DF3")
+FN = _Namespace("FN")
+DFN = _Namespace("DFN")
+I = _Namespace("I")  # noqa: E741
 
 
 def shift_index(idx, dims, mu, sign):

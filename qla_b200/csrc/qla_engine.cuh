@@ -54,7 +54,7 @@ struct SiteParams {
   // bulk-copy pipeline layout (host-computed)
   unsigned stage_bytes, tx_bytes;
   unsigned off_in[3], off_out_in;
-  int stages;        // pipeline depth S (2..8)
+  int stages;        // pipeline depth S (1..8)
   long long ntiles;  // number of full tiles of T sites
 };
 

@@ -139,12 +139,16 @@ struct SiteLauncher {
         sh.threads = tt;
         sh.stages = ts;
       }
-      // never exceed the 227 KB per-block limit: shed stages, then halve the tile
-      while (tma_smem_bytes(sh.threads, sh.stages, stage_bytes_for(sh.threads, bps), OB) > 227u * 1024u) {
+      // stay within the per-block shared-memory limit (227 KB less the static
+      // reduction scratch): shed stages, then halve the tile down to one warp,
+      // then (very large records, e.g. nc = 8 matrices) run unpipelined
+      while (tma_smem_bytes(sh.threads, sh.stages, stage_bytes_for(sh.threads, bps), OB) > 225u * 1024u) {
         if (sh.stages > 2)
           sh.stages--;
-        else if (sh.threads > 64)
+        else if (sh.threads > 32)
           sh.threads /= 2;
+        else if (sh.stages > 1)
+          sh.stages = 1;
         else
           break;
       }

@@ -64,6 +64,138 @@ INT_BINOPS = {"and": "IC_AND", "divide": "IC_DIVIDE", "eq": "IC_EQ", "ge": "IC_G
               "rshift": "IC_RSHIFT", "xor": "IC_XOR"}
 
 
+FN_NCS = [2, 3, 4, 8]          # colour counts with compiled QLA_FN_ kernels
+FN_MFUNC_NCS = [3, 4, 8]       # nc = 1, 2 use complex libm closed forms in the reference
+
+
+def _fn_switch(ncs, call_of_nc, name):
+    """switch (nc) over the compiled colour counts; other nc record an error."""
+    cases = "".join(f"    case {nc}: {call_of_nc(nc)} break;\n" for nc in ncs)
+    return (f"switch (nc) {{\n{cases}    default: qlab::set_error(QLAGPU_ERR_ARG, \"{name}\", "
+            f"\"nc not compiled (supported: {', '.join(map(str, ncs))})\");\n  }}")
+
+
+def gen_fn():
+    """QLA_FN_ / QLA_DFN_ entry points (colour count nc at run time,
+    doc/qla.tex:595-611): the hot families of gen_pc for nc in FN_NCS."""
+    fns = []
+    R = "float"
+    cols = {"V": lambda nc: 1, "H": lambda nc: 2, "D": lambda nc: 4, "M": lambda nc: nc}
+    ncpl = {"V": lambda nc: nc, "H": lambda nc: 2 * nc, "D": lambda nc: 4 * nc, "M": lambda nc: nc * nc}
+    kid = lambda fam: f'"FN_{fam}"'  # noqa: E731
+
+    def opnd(ptr, arg):
+        return (f"qlab::op_ptr((const void* const*){arg})" if ptr else f"qlab::op_contig({arg})")
+
+    def add(name, params, body, family, cite, kinds):
+        fns.append(Fn(name, [("int", "nc")] + params, body, family, cite, kinds))
+
+    for T in FIELD_TYPES:
+        src2s = [(T, False), ("p" + T, True)] + ([("Ma", False), ("pMa", True)] if T == "M" else [])
+        for var in ["v", "x"]:
+            gang = "index" if var == "x" else "nullptr"
+            tail = [("int *", "index")] if var == "x" else []
+            for eq in EQOPS:
+                for s1 in ["M", "Ma", "pM", "pMa"]:
+                    adja = s1.endswith("a")
+                    for s2, p2 in src2s:
+                        adjb = s2.endswith("a")
+                        name = f"QLA_FN_{T}_{var}{eq}_{s1}_times_{s2}"
+                        call = lambda nc, T=T, adja=adja, adjb=adjb, s1=s1, p2=p2, eq=eq, gang=gang: (
+                            f"qlab::api_map<qlab::LMultOp<{R}, {nc}, {cols[T](nc)}, {str(adja).lower()}, "
+                            f"{str(adjb).lower()}>>({kid('lmult')}, r, {opnd(s1.startswith('p'), 'a')}, "
+                            f"{opnd(p2, 'b')}, {gang}, n, {EQ_ENUM[eq]});")
+                        add(name, [("void *", "r"), ("void *", "a"), ("void *", "b")] + tail + [("int", "n")],
+                            _fn_switch(FN_NCS, call, name), "lmult", CITE["lmult"],
+                            dict(dest=T, eqop=eq, var=var, a=s1, b=s2))
+        for eq in EQOPS:
+            for s1 in ["M", "Ma"]:
+                name = f"QLA_FN_{T}_{eq}_{s1}_times_x{T}"
+                call = lambda nc, T=T, s1=s1, eq=eq: (
+                    f"qlab::api_map<qlab::LMultOp<{R}, {nc}, {cols[T](nc)}, {str(s1 == 'Ma').lower()}, false>>("
+                    f"{kid('lmult')}, r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, {EQ_ENUM[eq]});")
+                add(name, [("void *", "r"), ("void *", "a"), ("void *", "b"), ("int *", "jb"), ("int", "n")],
+                    _fn_switch(FN_NCS, call, name), "lmult", CITE["lmult_x"],
+                    dict(dest=T, eqop=eq, var="xb", a=s1, b="x" + T))
+        for var in ["v", "x"]:
+            gang = "index" if var == "x" else "nullptr"
+            tail = [("int *", "index")] if var == "x" else []
+            for eq in EQOPS:
+                for src, p1 in [(T, False), ("p" + T, True)]:
+                    name = f"QLA_FN_{T}_{var}{eq}_r_times_{src}"
+                    call = lambda nc, T=T, p1=p1, eq=eq, gang=gang: (
+                        f"qlab::api_scalar_map<qlab::RTimesOp<{R}, {ncpl[T](nc)}>, {R}>({kid('rtimes')}, r, "
+                        f"(const float*)a, {opnd(p1, 'b')}, {gang}, n, {EQ_ENUM[eq]});")
+                    add(name, [("void *", "r"), ("QLA_F_Real *", "a"), ("void *", "b")] + tail + [("int", "n")],
+                        _fn_switch(FN_NCS, call, name), "rtimes", CITE["rtimes"],
+                        dict(dest=T, eqop=eq, var=var, b=src))
+                    name = f"QLA_FN_{T}_{var}{eq}_{src}"
+                    call = lambda nc, T=T, p1=p1, eq=eq, gang=gang: (
+                        f"qlab::api_map<qlab::CopyOp<{R}, {ncpl[T](nc)}>>({kid('copy')}, r, {opnd(p1, 'a')}, "
+                        f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]});")
+                    add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
+                        _fn_switch(FN_NCS, call, name), "copy", CITE["copy"], dict(dest=T, eqop=eq, var=var, a=src))
+        # global reductions: FN (float result) and DFN (double result)
+        for rpc, outR, OP in (("FN", "float", "F"), ("DFN", "double", "D")):
+            for var in ["v", "x"]:
+                gang = "index" if var == "x" else "nullptr"
+                tail = [("int *", "index")] if var == "x" else []
+                for src, p1 in [(T, False), ("p" + T, True)]:
+                    name = f"QLA_{rpc}_r_{var}eq_norm2_{src}"
+                    call = lambda nc, T=T, p1=p1, gang=gang, outR=outR: (
+                        f"qlab::api_reduce<qlab::Norm2Op<{R}, {ncpl[T](nc)}, {outR}>>({kid('norm2')}, r, "
+                        f"sizeof({outR}), {opnd(p1, 'a')}, qlab::Opnd{{}}, {gang}, n);")
+                    add(name, [(f"QLA_{OP}_Real *", "r"), ("void *", "a")] + tail + [("int", "n")],
+                        _fn_switch(FN_NCS, call, name), "norm2", CITE["norm2"],
+                        dict(dest="r", var=var, a=src, out=outR))
+                for sa, pa_ in [(T, False), ("p" + T, True)]:
+                    for sb, pb_ in [(T, False), ("p" + T, True)]:
+                        name = f"QLA_{rpc}_c_{var}eq_{sa}_dot_{sb}"
+                        call = lambda nc, T=T, pa_=pa_, pb_=pb_, gang=gang, outR=outR: (
+                            f"qlab::api_reduce<qlab::DotOp<{R}, {ncpl[T](nc)}, {outR}>>({kid('dot')}, r, "
+                            f"2 * sizeof({outR}), {opnd(pa_, 'a')}, {opnd(pb_, 'b')}, {gang}, n);")
+                        add(name, [(f"QLA_{OP}_Complex *", "r"), ("void *", "a"), ("void *", "b")] + tail +
+                            [("int", "n")], _fn_switch(FN_NCS, call, name), "dot", CITE["dot"],
+                            dict(dest="c", var=var, a=sa, b=sb, out=outR))
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        tail = [("int *", "index")] if var == "x" else []
+        for eq in EQOPS:
+            for src, p1 in [("D", False), ("pD", True)]:
+                name = f"QLA_FN_H_{var}{eq}_spproj_{src}"
+                call = lambda nc, p1=p1, eq=eq, gang=gang: (
+                    f"qlab::api_map<qlab::SpprojOp<{R}, {nc}>>({kid('spproj')}, r, {opnd(p1, 'a')}, "
+                    f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]}, mu, sign);")
+                add(name, [("void *", "r"), ("void *", "a"), ("int", "mu"), ("int", "sign")] + tail + [("int", "n")],
+                    "if (mu < 0 || mu > 4) return;\n  " + _fn_switch(FN_NCS, call, name), "spproj",
+                    CITE["spproj"], dict(eqop=eq, var=var, a=src))
+            for src, p1 in [("H", False), ("pH", True)]:
+                name = f"QLA_FN_D_{var}{eq}_sprecon_{src}"
+                call = lambda nc, p1=p1, eq=eq, gang=gang: (
+                    f"qlab::api_map<qlab::SpreconOp<{R}, {nc}>>({kid('sprecon')}, r, {opnd(p1, 'a')}, "
+                    f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]}, mu, sign);")
+                add(name, [("void *", "r"), ("void *", "a"), ("int", "mu"), ("int", "sign")] + tail + [("int", "n")],
+                    "if (mu < 0 || mu > 4) return;\n  " + _fn_switch(FN_NCS, call, name), "sprecon",
+                    CITE["sprecon"], dict(eqop=eq, var=var, a=src))
+        for src, p1 in [("M", False), ("pM", True)]:
+            for fname, opname in (("exp", "GenExpOp"), ("sqrt", "GenSqrtOp"), ("inverse", "GenInverseOp")):
+                name = f"QLA_FN_M_{var}eq_{fname}_{src}"
+                call = lambda nc, opname=opname, p1=p1, gang=gang: (
+                    f"qlab::api_map<qlab::{opname}<{R}, {nc}>>({kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
+                    f"{gang}, n, qlab::EQ);")
+                add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
+                    _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
+                    dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
+            name = f"QLA_FN_C_{var}eq_det_{src}"
+            call = lambda nc, p1=p1, gang=gang: (
+                f"qlab::api_map<qlab::GenDetOp<{R}, {nc}>>({kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
+                f"{gang}, n, qlab::EQ);")
+            add(name, [("QLA_F_Complex *", "r"), ("void *", "a")] + tail + [("int", "n")],
+                _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
+                dict(dest="C", eqop="eq", var=var, a=src, fn="det"))
+    return fns
+
+
 def gen_int():
     """QLA_I_ entry points: the (shape x eqop x indexing) set of the reference's
     integer library."""
@@ -370,8 +502,8 @@ def main():
     manifest = []
     groups = {}
     headers = {}
-    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None)]:
-        for fn in (gen_int() if pc == "I" else gen_pc(pc, R, P)):
+    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None)]:
+        for fn in (gen_int() if pc == "I" else gen_fn() if pc == "FN" else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
@@ -392,6 +524,8 @@ def main():
         written += write_if_changed(os.path.join(OUT_INC, fname), text)
     for (pc, family), fns in groups.items():
         extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n'}.get(family, "")
+        if pc == "FN" and family == "mfunc":
+            extra = '#include "../qla_mfunc_generic.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:
             text += "QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  " + fn.body + "\n}\n\n"

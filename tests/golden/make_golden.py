@@ -146,6 +146,43 @@ def build(pc, dt, seed):
             call(f"QLA_{npc}_{fname}", nc, ctypes.c_void_p(r.ctypes.data),
                  ctypes.c_void_p(ins[f"mfN{nc}_{src}"].ctypes.data), N)
             out[f"QLA_{npc}_{fname}|mfN{nc}_{src}"] = r
+    if pc == "F3":
+        # the N-colour level-1 loops at nc = 4 and 8 (QLA_FN_ / QLA_DFN_)
+        for nc in (4, 8):
+            m1 = rng.standard_normal((NS, 2 * nc * nc)).astype(dt)
+            vv = rng.standard_normal((NS, 2 * nc)).astype(dt)
+            hh = rng.standard_normal((NS, 4 * nc)).astype(dt)
+            dd = rng.standard_normal((NS, 8 * nc)).astype(dt)
+            r0 = rng.standard_normal((N, 8 * nc)).astype(dt)
+            ins.update({f"fn{nc}_M": m1, f"fn{nc}_V": vv, f"fn{nc}_H": hh, f"fn{nc}_D": dd, f"fn{nc}_r0": r0})
+            for eq in EQOPS:
+                r = r0[:, :2 * nc].copy()
+                call(f"QLA_FN_V_v{eq}_M_times_V", nc, ctypes.c_void_p(r.ctypes.data),
+                     ctypes.c_void_p(m1.ctypes.data), ctypes.c_void_p(vv.ctypes.data), N)
+                out[f"QLA_FN_V_v{eq}_M_times_V|{nc}"] = r
+                r = np.ascontiguousarray(np.tile(r0[:, :2 * nc], (1, nc)))
+                call(f"QLA_FN_M_v{eq}_Ma_times_pM", nc, ctypes.c_void_p(r.ctypes.data),
+                     ctypes.c_void_p(m1.ctypes.data), parr(m1, ins["idx"], nc * nc), N)
+                out[f"QLA_FN_M_v{eq}_Ma_times_pM|{nc}"] = r
+                for mu in range(5):
+                    r = r0[:, :4 * nc].copy()
+                    call(f"QLA_FN_H_v{eq}_spproj_D", nc, ctypes.c_void_p(r.ctypes.data),
+                         ctypes.c_void_p(dd.ctypes.data), mu, -1, N)
+                    out[f"QLA_FN_H_v{eq}_spproj_D|{nc}|{mu}"] = r
+                    r = r0[:, :8 * nc].copy()
+                    call(f"QLA_FN_D_v{eq}_sprecon_H", nc, ctypes.c_void_p(r.ctypes.data),
+                         ctypes.c_void_p(hh.ctypes.data), mu, 1, N)
+                    out[f"QLA_FN_D_v{eq}_sprecon_H|{nc}|{mu}"] = r
+            vrev = vv[::-1].copy()
+            ins[f"fn{nc}_Vrev"] = vrev
+            for rpc, odt in (("FN", np.float32), ("DFN", np.float64)):
+                o = np.zeros(1, dtype=odt)
+                call(f"QLA_{rpc}_r_veq_norm2_D", nc, ctypes.c_void_p(o.ctypes.data), ctypes.c_void_p(dd.ctypes.data), N)
+                out[f"QLA_{rpc}_r_veq_norm2_D|{nc}"] = o
+                o = np.zeros(2, dtype=odt)
+                call(f"QLA_{rpc}_c_veq_V_dot_V", nc, ctypes.c_void_p(o.ctypes.data), ctypes.c_void_p(vv.ctypes.data),
+                     ctypes.c_void_p(vrev.ctypes.data), N)
+                out[f"QLA_{rpc}_c_veq_V_dot_V|{nc}"] = o
     return ins, out
 
 

@@ -1,0 +1,123 @@
+"""GPU parity of the QLA_FN_ / QLA_DFN_ entry points (colour count nc at run
+time) against the oracle, through the C-ABI, for every compiled nc
+(2, 3, 4, 8; matrix functions 3, 4, 8).  Linear ops and the matrix
+functions (the reference's generic Pade exp, Newton sqrt, Gauss-Jordan
+inverse, LU det, restated in float) must be bit-identical; reductions
+follow the tolerances of tests/test_gpu_reductions.py."""
+import itertools
+
+import numpy as np
+import pytest
+
+import qla_testlib as T
+
+pytestmark = pytest.mark.gpu
+
+NCS = [2, 3, 4, 8]
+
+
+def ncplx(t, nc):
+    return {"V": nc, "H": 2 * nc, "D": 4 * nc, "M": nc * nc}[t]
+
+
+def ncol(t, nc):
+    return {"V": 1, "H": 2, "D": 4, "M": nc}[t]
+
+
+@pytest.mark.parametrize("nc", NCS)
+def test_fn_lmult(qla, nc):
+    rng = np.random.default_rng(50 + nc)
+    n, ns = 1003, 1100
+    idx = rng.integers(0, ns, n).astype(np.int32)
+    gang = rng.permutation(n).astype(np.int32)
+    a = rng.standard_normal((ns, 2 * nc * nc)).astype(np.float32)
+    ad = T.to_dev(a)
+    pa = T.ptr_array(ad, idx, 8 * nc * nc)
+    for dest in ("V", "H", "D", "M"):
+        b = rng.standard_normal((ns, 2 * ncplx(dest, nc))).astype(np.float32)
+        r0 = rng.standard_normal((n, 2 * ncplx(dest, nc))).astype(np.float32)
+        bd = T.to_dev(b)
+        pb = T.ptr_array(bd, idx[::-1].copy(), 8 * ncplx(dest, nc))
+        src2s = [(dest, 0), ("p" + dest, 0)] + ([("Ma", 1)] if dest == "M" else [])
+        for var, eq, s1, (s2, adjb) in itertools.product(["v", "x"], T.EQOPS, ["M", "Ma", "pM"], src2s):
+            if dest != "V" and var == "x" and eq not in ("eq", "meq"):
+                continue
+            r_d = T.to_dev(r0)
+            args = [nc, r_d, pa if s1.startswith("p") else ad, pb if s2.startswith("p") else bd]
+            if var == "x":
+                args.append(T.to_dev(gang))
+            getattr(qla.FN, f"{dest}_{var}{eq}_{s1}_times_{s2}")(*args, n)
+            want = r0.copy()
+            T.ora_lmult(want, a, b, n, ncol(dest, nc), eq, adja=int(s1.endswith("a")), adjb=adjb,
+                        idx_a=idx if s1.startswith("p") else None,
+                        idx_b=idx[::-1].copy() if s2.startswith("p") else None,
+                        gang=gang if var == "x" else None, nc=nc)
+            assert T.bits_equal(T.to_host(r_d), want), (nc, dest, var, eq, s1, s2)
+        r_d = T.to_dev(r0)
+        qla.FN.__getattr__(f"{dest}_peq_M_times_x{dest}")(nc, r_d, ad, bd, T.to_dev(idx), n)
+        want = r0.copy()
+        T.ora_lmult(want, a, b, n, ncol(dest, nc), "peq", idx_b=idx, nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), (nc, dest, "xb")
+
+
+@pytest.mark.parametrize("nc", NCS)
+def test_fn_spin_rtimes_copy_reductions(qla, nc):
+    rng = np.random.default_rng(60 + nc)
+    n = 2049
+    d = rng.standard_normal((n, 8 * nc)).astype(np.float32)
+    h = rng.standard_normal((n, 4 * nc)).astype(np.float32)
+    dd, hd = T.to_dev(d), T.to_dev(h)
+    for eq, mu, sign in itertools.product(T.EQOPS, range(5), (1, -1)):
+        r_d = T.to_dev(h)
+        qla.FN.__getattr__(f"H_v{eq}_spproj_D")(nc, r_d, dd, mu, sign, n)
+        want = h.copy()
+        T.ora_spproj(want, d, n, mu, sign, eq, nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), ("spproj", nc, eq, mu, sign)
+        r_d = T.to_dev(d)
+        qla.FN.__getattr__(f"D_v{eq}_sprecon_H")(nc, r_d, hd, mu, sign, n)
+        want = d.copy()
+        T.ora_sprecon(want, h, n, mu, sign, eq, nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), ("sprecon", nc, eq, mu, sign)
+    for t in ("V", "H", "D", "M"):
+        x = rng.standard_normal((n, 2 * ncplx(t, nc))).astype(np.float32)
+        y = rng.standard_normal((n, 2 * ncplx(t, nc))).astype(np.float32)
+        xd, yd = T.to_dev(x), T.to_dev(y)
+        for eq in T.EQOPS:
+            r_d = T.to_dev(y)
+            qla.FN.__getattr__(f"{t}_v{eq}_r_times_{t}")(nc, r_d, -0.375, xd, n)
+            want = y.copy()
+            T.ora_rtimes(want, -0.375, x, n, ncplx(t, nc), eq)
+            assert T.bits_equal(T.to_host(r_d), want), ("rtimes", nc, t, eq)
+        r_d = T.to_dev(y)
+        qla.FN.__getattr__(f"{t}_vmeq_{t}")(nc, r_d, xd, n)
+        assert T.bits_equal(T.to_host(r_d), y - x)
+        exact = T.ora_norm2(x, n, ncplx(t, nc), exact=True)
+        got = qla.DFN.__getattr__(f"r_veq_norm2_{t}")(nc, None, xd, n)
+        assert abs(got - exact) <= 1e-12 * exact
+        gotf = qla.FN.__getattr__(f"r_veq_norm2_{t}")(nc, None, xd, n)
+        assert abs(gotf - exact) <= 6e-8 * exact
+        ed = T.ora_dot(x, y, n, ncplx(t, nc), exact=True)
+        gd = qla.DFN.__getattr__(f"c_veq_{t}_dot_{t}")(nc, None, xd, yd, n)
+        assert abs(gd - ed) <= 1e-12 * max(1.0, abs(ed)) * 4
+
+
+@pytest.mark.parametrize("nc", [3, 4, 8])
+def test_fn_matrix_functions_bit_exact(qla, nc):
+    rng = np.random.default_rng(70 + nc)
+    n = 4099 if nc < 8 else 1031
+    gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(np.float32)
+    pos = T.positive_hermitian_inputs(rng, n, np.float32, nc=nc)
+    for fname, src in (("exp", gen), ("sqrt", pos), ("inverse", gen), ("det", gen)):
+        nout = 1 if fname == "det" else nc * nc
+        r_d = T.to_dev(np.zeros((n, 2 * nout), np.float32))
+        dest = "C" if fname == "det" else "M"
+        qla.FN.__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
+        assert T.bits_equal(T.to_host(r_d), T.ora_mfunc(src, n, fname, nc=nc)), (nc, fname)
+
+
+def test_fn_unsupported_nc_reports_error(qla):
+    qla.clear_error()
+    qla.lib().QLA_FN_V_veq_M_times_V(5, None, None, None, 10)
+    code, msg = qla.last_error()
+    assert code == 4 and "nc not compiled" in msg
+    qla.clear_error()

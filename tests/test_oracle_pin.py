@@ -73,6 +73,37 @@ def replay(pc, name, ins):
         v = T.ora_dot(ins[t], b, n, NC[t])
         odt = np.float32 if rpc == "F3" else np.float64
         return np.array([v.real], dtype=odt) if re_ else np.array([v.real, v.imag], dtype=odt)
+    m = re.match(r"QLA_FN_(V|M)_v(eq|peq|meq|eqm)_(M|Ma)_times_(p?)(V|M)$", key)
+    if m:
+        dest, eq, s1, p2, _ = m.groups()
+        nc = int(extra[0])
+        if dest == "V":
+            r = ins[f"fn{nc}_r0"][:, :2 * nc].copy()
+            T.ora_lmult(r, ins[f"fn{nc}_M"], ins[f"fn{nc}_V"], n, 1, eq, nc=nc)
+        else:
+            r = np.ascontiguousarray(np.tile(ins[f"fn{nc}_r0"][:, :2 * nc], (1, nc)))
+            T.ora_lmult(r, ins[f"fn{nc}_M"], ins[f"fn{nc}_M"], n, nc, eq, adja=1, idx_b=ins["idx"], nc=nc)
+        return r
+    m = re.match(r"QLA_FN_(H|D)_v(eq|peq|meq|eqm)_(spproj|sprecon)_(D|H)$", key)
+    if m:
+        _, eq, which, _ = m.groups()
+        nc, mu = int(extra[0]), int(extra[1])
+        if which == "spproj":
+            r = ins[f"fn{nc}_r0"][:, :4 * nc].copy()
+            T.ora_spproj(r, ins[f"fn{nc}_D"], n, mu, -1, eq, nc=nc)
+        else:
+            r = ins[f"fn{nc}_r0"][:, :8 * nc].copy()
+            T.ora_sprecon(r, ins[f"fn{nc}_H"], n, mu, 1, eq, nc=nc)
+        return r
+    m = re.match(r"QLA_(FN|DFN)_(r|c)_veq_(norm2_D|V_dot_V)$", key)
+    if m:
+        rpc, kind, what = m.groups()
+        nc = int(extra[0])
+        odt = np.float32 if rpc == "FN" else np.float64
+        if kind == "r":
+            return np.array([T.ora_norm2(ins[f"fn{nc}_D"], n, 4 * nc)], dtype=odt)
+        v = T.ora_dot(ins[f"fn{nc}_V"], ins[f"fn{nc}_Vrev"], n, nc)
+        return np.array([v.real, v.imag], dtype=odt)
     m = re.match(r"QLA_(F3|D3|FN|DN)_(M|C)_veq_(exp|sqrt|inverse|det)_M$", key)
     if m:
         pcx, _, fname = m.group(1), m.group(2), m.group(3)
@@ -162,6 +193,12 @@ def test_prototypes_match_reference_headers():
     per-operand index (`xX`) forms."""
     import qla_b200
     ref = {}
+    nargs_fn = {}
+    for h in ("qla_fn.h", "qla_dfn.h"):
+        txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
+        for m in re.finditer(r"void (QLA_D?FN_\w+) \((.*?)\);", txt):
+            # VLA record types: compare the parameter count (the first is int nc)
+            nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)", m.group(2)))
     for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h"):
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
         for m in re.finditer(r"void (QLA_\w+) \((.*?)\);", txt):
@@ -170,6 +207,9 @@ def test_prototypes_match_reference_headers():
             ref[m.group(1)] = [re.match(r"^(.*?)\w+$", p).group(1).replace(" ", "") for p in params]
     extra = []
     for e in qla_b200.manifest():
+        if e["name"] in nargs_fn:
+            assert len(e["params"]) == nargs_fn[e["name"]], (e["name"], e["params"], nargs_fn[e["name"]])
+            continue
         if e["name"] not in ref:
             extra.append(e["name"])
             continue
