@@ -479,6 +479,13 @@ def run_workload(args):
                         mh(V(H2), V(U[mu]), V(H), V(nbr[(mu, sg)]), n)
                         rc(V(Out), V(H2), mu, sg, n)
             ms = _events_time(torch, stream, hop, reps)
+            fz = getattr(L, f"QLA_{pc}_D_peq_spproj_M_times_xD")
+
+            def hop_fused():
+                for mu in range(4):
+                    for sg in (1, -1):
+                        fz(V(Out), V(U[mu]), V(D), V(nbr[(mu, sg)]), mu, sg, n)
+            ms_f = _events_time(torch, stream, hop_fused, reps)
             t_sp = _events_time(torch, stream, lambda: sp(V(H), V(D), 0, 1, n), reps * 4)
             t_mh = _events_time(torch, stream, lambda: mh(V(H2), V(U[0]), V(H), V(nbr[(0, 1)]), n), reps * 4)
             t_rc = _events_time(torch, stream, lambda: rc(V(Out), V(H2), 0, 1, n), reps * 4)
@@ -492,6 +499,10 @@ def run_workload(args):
                  "M_times_pV": 120 * e + 8}
             tk = {"spproj": t_sp, "M_times_xH": t_mh, "sprecon": t_rc, "M_times_xV": t_mv, "M_times_pV": t_mvp}
             res[pc] = {"site_updates_per_s": n / (ms / 1e3), "ms_per_hop": ms,
+                       "fused": {"op": f"QLA_{pc}_D_peq_spproj_M_times_xD", "ms_per_hop": ms_f,
+                                 "site_updates_per_s": n / (ms_f / 1e3),
+                                 "hbm_frac": n * 8 * (364 * e) / (ms_f / 1e3) / 1e9 / peak,
+                                 "speedup_vs_unfused": ms / ms_f},
                        "hbm_frac_hop": n * 8 * sum(b[k] for k in ("spproj", "M_times_xH", "sprecon")) / (ms / 1e3)
                        / 1e9 / peak,
                        "kernels": {k: {"us": 1e3 * tk[k], "gbs": b[k] * n / (tk[k] / 1e3) / 1e9,

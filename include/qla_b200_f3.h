@@ -803,6 +803,471 @@ void QLA_F3_H_xeqm_spproj_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_Dir
 void QLA_F3_D_xeqm_sprecon_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
 /* replaces QLA_F3_D_xeqm_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
 void QLA_F3_D_xeqm_sprecon_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- hop: replaces the F3 functions emitted by lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix) */
+/* replaces QLA_F3_H_veq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veq_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_veq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veq_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vpeq_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_vpeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vpeq_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_vmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_vmeq_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_vmeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_vmeq_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_H_veqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_veqm_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int n);
+/* replaces QLA_F3_D_veqm_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_veqm_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int n);
+/* replaces QLA_F3_H_xeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeq_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeq_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xpeq_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xpeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xpeq_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xmeq_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xmeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xmeq_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_M_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_M_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_M_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_M_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_M_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_M_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_Ma_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_Ma_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_Ma_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_Ma_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_Ma_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_Ma_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_pM_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_pM_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_pM_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_pM_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_pM_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_pM_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_pMa_times_D(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_xeqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_H_xeqm_spproj_pMa_times_pD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_pMa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_pMa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_pMa_times_H(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_sprecon_pMa_times_pH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_D_xeqm_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_F3_D_xeqm_spproj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* replaces QLA_F3_H_eq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_eq_spproj_M_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eq_spproj_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eq_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eq_sprecon_M_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_eq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_eq_spproj_Ma_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eq_spproj_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eq_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eq_sprecon_Ma_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_peq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_peq_spproj_M_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_peq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_peq_spproj_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_peq_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_peq_sprecon_M_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_peq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_peq_spproj_Ma_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_peq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_peq_spproj_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_peq_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_peq_sprecon_Ma_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_meq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_meq_spproj_M_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_meq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_meq_spproj_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_meq_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_meq_sprecon_M_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_meq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_meq_spproj_Ma_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_meq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_meq_spproj_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_meq_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_meq_sprecon_Ma_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_eqm_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_eqm_spproj_M_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eqm_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eqm_spproj_M_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eqm_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eqm_sprecon_M_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_H_eqm_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_H_eqm_spproj_Ma_times_xD(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eqm_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eqm_spproj_Ma_times_xD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
+/* replaces QLA_F3_D_eqm_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_F3_D_eqm_sprecon_Ma_times_xH(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * jb, int mu, int sign, int n);
 /* ---- rtimes: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1292 (real constant times field) */
 /* replaces QLA_F3_V_veq_r_times_V (lib/perl/build_qla.pl:1256-1292 (real constant times field)) */
 void QLA_F3_V_veq_r_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);

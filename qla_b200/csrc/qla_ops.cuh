@@ -15,34 +15,39 @@ using CxArr1 = Cx<R>[1];
 // r (eqop) A * B, A = a | a^+ (colour matrix), B = b (NC x NCOL) | b^+ (matrix).
 // Restates lib/perl/build_qla.pl:1588-1622 + expressions_tensor.pl:766: per
 // output element x = (peq|meq ? r : 0); x (+|-)= A(i,k) B(k,s) for k in order.
+template <typename R, int NC, int NCOL, bool ADJA, bool ADJB>
+__device__ __forceinline__ void lmult_site(int eqop, bool load, const Cx<R> (&a)[NC * NC],
+                                           const Cx<R> (&b)[NC * NCOL], Cx<R> (&y)[NC * NCOL]) {
+  const bool minus = (eqop == MEQ || eqop == EQM);
+#pragma unroll
+  for (int ic = 0; ic < NC; ic++) {
+#pragma unroll
+    for (int s = 0; s < NCOL; s++) {
+      Cx<R> x;
+      if (load) {
+        x = y[ic * NCOL + s];
+      } else {
+        x.re = R(0);
+        x.im = R(0);
+      }
+#pragma unroll
+      for (int kc = 0; kc < NC; kc++) {
+        const Cx<R> av = ADJA ? a[kc * NC + ic] : a[ic * NC + kc];
+        const Cx<R> bv = ADJB ? b[s * NCOL + kc] : b[kc * NCOL + s];
+        cmac<ADJA, ADJB>(x, minus, av, bv);
+      }
+      y[ic * NCOL + s] = x;
+    }
+  }
+}
+
 template <typename R_, int NC, int NCOL, bool ADJA, bool ADJB>
 struct LMultOp {
   using R = R_;
   static constexpr int NIN = 2, N0 = NC * NC, N1 = NC * NCOL, N2 = 0, NOUT = NC * NCOL, NACC = 0;
   __device__ __forceinline__ static void apply(const SiteParams& p, const Cx<R> (&a)[N0], const Cx<R> (&b)[N1],
                                                const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
-    const bool minus = (p.eqop == MEQ || p.eqop == EQM);
-    const bool load = p.out_read != 0;
-#pragma unroll
-    for (int ic = 0; ic < NC; ic++) {
-#pragma unroll
-      for (int s = 0; s < NCOL; s++) {
-        Cx<R> x;
-        if (load) {
-          x = y[ic * NCOL + s];
-        } else {
-          x.re = R(0);
-          x.im = R(0);
-        }
-#pragma unroll
-        for (int kc = 0; kc < NC; kc++) {
-          const Cx<R> av = ADJA ? a[kc * NC + ic] : a[ic * NC + kc];
-          const Cx<R> bv = ADJB ? b[s * NCOL + kc] : b[kc * NCOL + s];
-          cmac<ADJA, ADJB>(x, minus, av, bv);
-        }
-        y[ic * NCOL + s] = x;
-      }
-    }
+    lmult_site<R, NC, NCOL, ADJA, ADJB>(p.eqop, p.out_read != 0, a, b, y);
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[N1], const Cx<R> (&)[1],
                                double*) {}
@@ -217,6 +222,66 @@ struct SpreconOp {
   __device__ __forceinline__ static void apply(const SiteParams& p, const Cx<R> (&h)[N0], const Cx<R> (&)[1],
                                                const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
     mu_sign_dispatch<Body>(p.mu, p.sign, p.eqop, h, y);
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// ---------------------------------------------------------------------------
+// Fused spin-projection / colour-multiply / reconstruction (the Wilson hop
+// terms), build_qla.pl:1137-1250, make_code_binary.pl:189-336: the
+// intermediates are formed with `eq` exactly as the reference's temporaries
+// t1, t2, and only the last step applies the eqop.
+//   DEST = 2 (H):  r (eqop) A * spproj(b)
+//   DEST = 4 (D):  r (eqop) sprecon(A * spproj(b))
+template <typename R_, int NC, bool ADJA, int DEST>
+struct SpprojMultOp {
+  using R = R_;
+  static constexpr int NIN = 2, N0 = NC * NC, N1 = NC * 4, N2 = 0, NOUT = NC * DEST, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams& p, const Cx<R> (&a)[N0], const Cx<R> (&b)[N1],
+                                               const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
+    Cx<R> t1[NC * 2];
+    mu_sign_dispatch<typename SpprojOp<R, NC>::Body>(p.mu, p.sign, (int)EQ, b, t1);
+    if constexpr (DEST == 2) {
+      lmult_site<R, NC, 2, ADJA, false>(p.eqop, p.out_read != 0, a, t1, y);
+    } else {
+      Cx<R> t2[NC * 2];
+      lmult_site<R, NC, 2, ADJA, false>(EQ, false, a, t1, t2);
+      mu_sign_dispatch<typename SpreconOp<R, NC>::Body>(p.mu, p.sign, p.eqop, t2, y);
+    }
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[N1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// r (eqop) sprecon(A * b), b a HalfFermion (build_qla.pl:1200-1250)
+template <typename R_, int NC, bool ADJA>
+struct SpreconMultOp {
+  using R = R_;
+  static constexpr int NIN = 2, N0 = NC * NC, N1 = NC * 2, N2 = 0, NOUT = NC * 4, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams& p, const Cx<R> (&a)[N0], const Cx<R> (&b)[N1],
+                                               const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
+    Cx<R> t[NC * 2];
+    lmult_site<R, NC, 2, ADJA, false>(EQ, false, a, b, t);
+    mu_sign_dispatch<typename SpreconOp<R, NC>::Body>(p.mu, p.sign, p.eqop, t, y);
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[N1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// D (eqop) spproj(D): projection onto the D record (build_qla.pl:1137-1160)
+template <typename R_, int NC>
+struct SpprojDOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = NC * 4, N1 = 0, N2 = 0, NOUT = NC * 4, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams& p, const Cx<R> (&b)[N0], const Cx<R> (&)[1],
+                                               const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
+    Cx<R> t[NC * 2];
+    mu_sign_dispatch<typename SpprojOp<R, NC>::Body>(p.mu, p.sign, (int)EQ, b, t);
+    mu_sign_dispatch<typename SpreconOp<R, NC>::Body>(p.mu, p.sign, p.eqop, t, y);
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                double*) {}

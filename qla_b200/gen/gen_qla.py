@@ -52,6 +52,8 @@ CITE = {
     "norm2": "lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)",
     "dot": "lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)",
     "redot": "lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)",
+    "hop": "lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336",
+    "hop_x": "doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)",
     "mfunc": "lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, "
              "M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143",
 }
@@ -348,6 +350,54 @@ def gen_pc(pc, R, P):
                         f"qlab::api_map<qlab::SpreconOp<{R}, 3>>({kid('sprecon')}, r, {oa}, qlab::Opnd{{}}, {gang}, "
                         f"n, {EQ_ENUM[eq]}, mu, sign);")
                 fns.append(Fn(name, params, body, "sprecon", CITE["sprecon"], dict(eqop=eq, var=var, a=src)))
+    # ---- fused spin projection x colour matrix (Wilson hop terms)
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        tail = [("int *", "index")] if var == "x" else []
+        for eq in EQOPS:
+            for s1 in ["M", "Ma", "pM", "pMa"]:
+                adja = str(s1.endswith("a")).lower()
+                pa, oa = operand(pc, "M", s1.startswith("p"), "a")
+                for dest, src, opname in (("H", "D", f"SpprojMultOp<{R}, 3, {adja}, 2>"),
+                                          ("D", "D", f"SpprojMultOp<{R}, 3, {adja}, 4>"),
+                                          ("D", "H", f"SpreconMultOp<{R}, 3, {adja}>")):
+                    kind = "sprecon" if src == "H" else "spproj"
+                    for sname, p2 in [(src, False), ("p" + src, True)]:
+                        name = f"QLA_{pc}_{dest}_{var}{eq}_{kind}_{s1}_times_{sname}"
+                        pb, ob = operand(pc, src, p2, "b")
+                        params = [(f"{ptype(pc, dest)} *RESTRICT", "r"), pa, pb, ("int", "mu"),
+                                  ("int", "sign")] + tail + [("int", "n")]
+                        body = ("if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */\n  "
+                                f"qlab::api_map<qlab::{opname}>({kid('hop_' + dest + kind + adja)}, r, {oa}, {ob}, "
+                                f"{gang}, n, {EQ_ENUM[eq]}, mu, sign);")
+                        fns.append(Fn(name, params, body, "hop", CITE["hop"],
+                                      dict(dest=dest, eqop=eq, var=var, a=s1, b=sname, kind=kind)))
+            for sname, p1 in [("D", False), ("pD", True)]:
+                name = f"QLA_{pc}_D_{var}{eq}_spproj_{sname}"
+                pa, oa = operand(pc, "D", p1, "a")
+                params = [(f"{ptype(pc, 'D')} *RESTRICT", "r"), pa, ("int", "mu"), ("int", "sign")] + tail + \
+                    [("int", "n")]
+                body = ("if (mu < 0 || mu > 4) return;\n  "
+                        f"qlab::api_map<qlab::SpprojDOp<{R}, 3>>({kid('hop_Dspproj')}, r, {oa}, qlab::Opnd{{}}, "
+                        f"{gang}, n, {EQ_ENUM[eq]}, mu, sign);")
+                fns.append(Fn(name, params, body, "hop", CITE["hop"], dict(dest="D", eqop=eq, var=var, a=sname,
+                                                                           kind="spproj")))
+    for eq in EQOPS:
+        for s1 in ["M", "Ma"]:
+            adja = str(s1 == "Ma").lower()
+            for dest, src, opname in (("H", "D", f"SpprojMultOp<{R}, 3, {adja}, 2>"),
+                                      ("D", "D", f"SpprojMultOp<{R}, 3, {adja}, 4>"),
+                                      ("D", "H", f"SpreconMultOp<{R}, 3, {adja}>")):
+                kind = "sprecon" if src == "H" else "spproj"
+                name = f"QLA_{pc}_{dest}_{eq}_{kind}_{s1}_times_x{src}"
+                params = [(f"{ptype(pc, dest)} *RESTRICT", "r"), (f"{ptype(pc, 'M')} *RESTRICT", "a"),
+                          (f"{ptype(pc, src)} *RESTRICT", "b"), ("int *", "jb"), ("int", "mu"), ("int", "sign"),
+                          ("int", "n")]
+                body = ("if (mu < 0 || mu > 4) return;\n  "
+                        f"qlab::api_map<qlab::{opname}>({kid('hop_' + dest + kind + adja)}, r, qlab::op_contig(a), "
+                        f"qlab::op_idx(b, jb), nullptr, n, {EQ_ENUM[eq]}, mu, sign);")
+                fns.append(Fn(name, params, body, "hop", CITE["hop_x"],
+                              dict(dest=dest, eqop=eq, var="xb", a=s1, b="x" + src, kind=kind)))
     # ---- real constant times field, copies / gathers
     for T in FIELD_TYPES:
         nc = REC[T][2]

@@ -93,6 +93,21 @@ def build(pc, dt, seed):
         call(f"QLA_{pc}_H_x{eq}_spproj_pD", ctypes.c_void_p(r.ctypes.data), parr(ins["D"], ins["idx"], 12), 2, -1,
              ctypes.c_void_p(ins["gang"].ctypes.data), N)
         out[f"QLA_{pc}_H_x{eq}_spproj_pD|2|-1"] = r
+    # fused spin projection x colour matrix (the Wilson hop terms)
+    for mu in range(5):
+        for sign in (1, -1):
+            for name, dest, bsrc, pb in ((f"QLA_{pc}_D_vpeq_spproj_M_times_pD", "D", "D", True),
+                                         (f"QLA_{pc}_H_veq_spproj_Ma_times_D", "H", "D", False),
+                                         (f"QLA_{pc}_D_veqm_sprecon_M_times_pH", "D", "H", True),
+                                         (f"QLA_{pc}_D_vmeq_spproj_D", "D", "D", False)):
+                r = ins["r0" + dest].copy()
+                nc_b = 12 if bsrc == "D" else 6
+                b = parr(ins[bsrc], ins["idx"], nc_b) if pb else ctypes.c_void_p(ins[bsrc].ctypes.data)
+                if name.endswith("_spproj_D"):
+                    call(name, ctypes.c_void_p(r.ctypes.data), b, mu, sign, N)
+                else:
+                    call(name, ctypes.c_void_p(r.ctypes.data), ctypes.c_void_p(ins["M"].ctypes.data), b, mu, sign, N)
+                out[f"{name}|{mu}|{sign}"] = r
     # real constant times field
     sc = (ctypes.c_float if dt == np.float32 else ctypes.c_double)(float(ins["scal"][0]))
     for dest, nc in (("V", 3), ("D", 12), ("M", 9)):

@@ -343,3 +343,37 @@ def int_call_args(name, ins, n, r, to_arr, to_ptrs):
         args.append(to_arr(ins["gang"]))
     args.append(n)
     return args
+
+
+def ora_hop(r, a, b, n, mu, sign, eqop, dest, kind, adja=0, idx_b=None, gang=None, nc=3):
+    """Fused hop terms composed from the oracle in the reference's order
+    (make_code_binary.pl:189-336): intermediates with `eq`, eqop last.
+    kind 'spproj': b is D; dest H: r (eqop) A spproj(b); dest D: r (eqop)
+    sprecon(A spproj(b)); kind 'sprecon': b is H, r (eqop) sprecon(A b);
+    a None: D (eqop) sprecon(spproj(b))."""
+    dt = r.dtype
+    nall = r.shape[0]
+    sites = np.arange(n) if gang is None else np.asarray(gang)
+    bsel = b[idx_b[sites]] if idx_b is not None else b[sites]
+    asel = a[sites] if a is not None else None
+    m = len(sites)
+    if kind == "spproj":
+        t1 = np.zeros((m, 4 * nc), dt)
+        ora_spproj(t1, np.ascontiguousarray(bsel), m, mu, sign, "eq", nc=nc)
+    else:
+        t1 = np.ascontiguousarray(bsel)
+    if asel is None:
+        t2 = t1
+    elif dest == "H":
+        rr = np.ascontiguousarray(r[sites])
+        ora_lmult(rr, np.ascontiguousarray(asel), t1, m, 2, eqop, adja=adja, nc=nc)
+        r[sites] = rr
+        return r
+    else:
+        t2 = np.zeros((m, 4 * nc), dt)
+        ora_lmult(t2, np.ascontiguousarray(asel), t1, m, 2, "eq", adja=adja, nc=nc)
+    rr = np.ascontiguousarray(r[sites])
+    ora_sprecon(rr, t2, m, mu, sign, eqop, nc=nc)
+    r[sites] = rr
+    del nall
+    return r

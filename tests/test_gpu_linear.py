@@ -178,3 +178,55 @@ def test_shift_index_bit_exact(qla, cuda):
                 idx = cuda.empty(n, dtype=cuda.int32, device="cuda")
                 qla.shift_index(idx, dims, mu, sign)
                 assert np.array_equal(T.to_host(idx), T.shift_index(dims, mu, sign)), (dims, mu, sign)
+
+
+@pytest.mark.parametrize("pc,dt", PCS)
+def test_fused_hop_terms(qla, pc, dt):
+    """D_vpeq_spproj_M_times_pD and its family (the Wilson hop terms), every
+    eqop / adjoint / pointer / gang / index form and every mu, sign."""
+    rng = np.random.default_rng(88)
+    n, ns = 517, 560
+    a = T.haar_su3(rng, ns, dt)
+    d_src = T.gaussian_field(rng, ns, 12, dt)
+    h_src = T.gaussian_field(rng, ns, 6, dt)
+    r0 = {"H": T.gaussian_field(rng, ns, 6, dt), "D": T.gaussian_field(rng, ns, 12, dt)}
+    idx = rng.integers(0, ns, ns).astype(np.int32)
+    gang = rng.permutation(n).astype(np.int32)
+    ad, dd, hd = T.to_dev(a), T.to_dev(d_src), T.to_dev(h_src)
+    pa = T.ptr_array(ad, idx, rec_bytes(pc, "M"))
+    pdd = T.ptr_array(dd, idx, rec_bytes(pc, "D"))
+    phd = T.ptr_array(hd, idx, rec_bytes(pc, "H"))
+    ns_ = getattr(qla, pc)
+    count = 0
+    for (dest, kind), eq, s1, pb, var in itertools.product(
+            [("H", "spproj"), ("D", "spproj"), ("D", "sprecon")], T.EQOPS, ["M", "Ma", "pM"], [0, 1], ["v", "x"]):
+        src = "D" if kind == "spproj" else "H"
+        bsrc, bdev, bptr = (d_src, dd, pdd) if src == "D" else (h_src, hd, phd)
+        for mu, sign in ((0, 1), (1, -1), (2, 1), (3, -1), (4, 1), (4, -1)):
+            r_d = T.to_dev(r0[dest][:n])
+            args = [r_d, pa if s1.startswith("p") else ad, bptr if pb else bdev, mu, sign]
+            if var == "x":
+                args.append(T.to_dev(gang))
+            getattr(ns_, f"{dest}_{var}{eq}_{kind}_{s1}_times_{'p' if pb else ''}{src}")(*args, n)
+            want = r0[dest][:n].copy()
+            aa = a[idx[:n]] if s1.startswith("p") else a[:n]
+            T.ora_hop(want, np.ascontiguousarray(aa), bsrc, n, mu, sign, eq, dest, kind, adja=int(s1.endswith("a")),
+                      idx_b=idx if pb else None, gang=gang if var == "x" else None)
+            assert T.bits_equal(T.to_host(r_d), want), (dest, kind, var, eq, s1, pb, mu, sign)
+            count += 1
+    # int32 neighbour-index form and the D-destination projection
+    for (dest, kind), eq in itertools.product([("H", "spproj"), ("D", "spproj"), ("D", "sprecon")], T.EQOPS):
+        src = "D" if kind == "spproj" else "H"
+        bsrc, bdev = (d_src, dd) if src == "D" else (h_src, hd)
+        r_d = T.to_dev(r0[dest][:n])
+        getattr(ns_, f"{dest}_{eq}_{kind}_M_times_x{src}")(r_d, ad, bdev, T.to_dev(idx), 2, -1, n)
+        want = r0[dest][:n].copy()
+        T.ora_hop(want, np.ascontiguousarray(a[:n]), bsrc, n, 2, -1, eq, dest, kind, idx_b=idx)
+        assert T.bits_equal(T.to_host(r_d), want), (dest, kind, eq, "xb")
+    for eq, mu in itertools.product(T.EQOPS, range(5)):
+        r_d = T.to_dev(r0["D"][:n])
+        getattr(ns_, f"D_v{eq}_spproj_D")(r_d, dd, mu, 1, n)
+        want = r0["D"][:n].copy()
+        T.ora_hop(want, None, d_src, n, mu, 1, eq, "D", "spproj")
+        assert T.bits_equal(T.to_host(r_d), want), ("Dspproj", eq, mu)
+    assert count > 400

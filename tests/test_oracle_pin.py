@@ -50,6 +50,17 @@ def replay(pc, name, ins):
         T.ora_spproj(r, ins["D"], n, mu, sign, eq, idx_a=ins["idx"] if p else None,
                      gang=ins["gang"] if var == "x" else None)
         return r
+    m = re.match(r"QLA_(F3|D3)_(H|D)_v(eq|peq|meq|eqm)_(spproj|sprecon)_(M|Ma)_times_(p?)(D|H)$", key)
+    if m:
+        _, dest, eq, kind, s1, p, _ = m.groups()
+        r = ins["r0" + dest].copy()
+        b = ins["D"] if kind == "spproj" else ins["H"]
+        return T.ora_hop(r, ins["M"], b, n, int(extra[0]), int(extra[1]), eq, dest, kind, adja=int(s1 == "Ma"),
+                         idx_b=ins["idx"] if p else None)
+    m = re.match(r"QLA_(F3|D3)_D_v(eq|peq|meq|eqm)_spproj_D$", key)
+    if m:
+        r = ins["r0D"].copy()
+        return T.ora_hop(r, None, ins["D"], n, int(extra[0]), int(extra[1]), m.group(2), "D", "spproj")
     m = re.match(r"QLA_(F3|D3)_D_v(eq|peq|meq|eqm)_sprecon_H$", key)
     if m:
         r = ins["r0D"].copy()
