@@ -71,11 +71,14 @@ def _workloads(torch, L):
         yield (f"{pc}_norm2_V:c", 24 * e * m, lambda: getattr(L, f"QLA_{rp}_r_veq_norm2_V")(V(red), V(Vv), m))
         yield (f"{pc}_sprecon:cr", 240 * e * m,
                lambda: getattr(L, f"QLA_{pc}_D_vpeq_sprecon_H")(V(D), V(H2), 0, 1, m))
+        Dout = torch.randn(m, 24, device="cuda", dtype=dt)
+        yield (f"{pc}_hop_Dspprojfalse:cir", (364 * e - 4 * (e - 1)) * m,
+               lambda: getattr(L, f"QLA_{pc}_D_peq_spproj_M_times_xD")(V(Dout), V(U), V(D), V(idx), 0, 1, m))
         yield (f"{pc}_lmult_M00:cp", (216 * e + 8) * m,
                lambda: getattr(L, f"QLA_{pc}_M_veq_M_times_pM")(V(Mo), V(U), V(pM), m))
         yield (f"{pc}_lmult_M00:cc", 216 * e * m,
                lambda: getattr(L, f"QLA_{pc}_M_veq_M_times_M")(V(Mo), V(U), V(U2), m))
-        del U, U2, Mo, D, H, H2, Vv, Vo, pH, pV, pM, idx
+        del U, U2, Mo, D, H, H2, Vv, Vo, pH, pV, pM, idx, Dout
         torch.cuda.empty_cache()
 
 
