@@ -56,6 +56,12 @@ int qlagpu_tune_set(const char *kernel_id, int threads, int stages);
 void qlagpu_tune_clear(void);
 
 int qlagpu_sm_count(void);
+
+/* failure-path self-test: a kernel waits on a barrier that nothing completes,
+ * with a limit of limit_us microseconds; returns 1 when the wait gave up and
+ * reported the timeout (the context stays usable), 0 otherwise, < 0 when the
+ * test could not run */
+int qlagpu_selftest_wait_timeout(int limit_us);
 const char *qlagpu_version(void);
 
 /* periodic neighbour table on the device: idx[i] = the lexicographic site

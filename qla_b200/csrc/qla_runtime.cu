@@ -193,6 +193,21 @@ bool tuned_shape(const char* kernel_id, int* threads, int* stages) {
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Self-test of the failure path: one block waits on an mbarrier phase that
+// nothing will ever complete (one expected arrival, none made), with a short
+// time limit.  The wait must give up, raise QLA_DEVERR_MBAR_TIMEOUT in the
+// error word and return, leaving the context usable.
+__global__ void wait_timeout_selftest_kernel(unsigned* err, unsigned long long limit_ns, int* gave_up) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *gave_up = mbar_wait_bounded(&bar, 0u, err, limit_ns) ? 0 : 1;
+}
+
 }  // namespace qlab
 
 // ===========================================================================
@@ -256,6 +271,36 @@ QLAB_EXPORT void qlagpu_tune_clear(void) {
 }
 
 QLAB_EXPORT int qlagpu_sm_count(void) { return device_sm_count(); }
+
+// Runs the failure-path self-test with a wait limit of limit_us microseconds
+// (1..1000000).  Returns 1 when the wait gave up and the error word carries
+// the timeout bit (which is then cleared), 0 when it did not, or a negative
+// value when the test could not run.
+QLAB_EXPORT int qlagpu_selftest_wait_timeout(int limit_us) {
+  if (limit_us < 1 || limit_us > 1000000) {
+    set_error(QLAGPU_ERR_ARG, "qlagpu_selftest_wait_timeout", "limit_us must be in 1..1000000");
+    return -1;
+  }
+  unsigned* err = device_error_word();
+  if (!err) return -2;
+  int* flag = nullptr;
+  if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) {
+    check_launch("qlagpu_selftest_wait_timeout");
+    return -2;
+  }
+  cudaMemset(flag, 0, sizeof(int));
+  cudaMemset(err, 0, sizeof(unsigned));
+  wait_timeout_selftest_kernel<<<1, 32, 0, t_stream>>>(err, 1000ull * (unsigned long long)limit_us, flag);
+  int gave_up = 0;
+  unsigned bits = 0;
+  const bool ok = check_launch("qlagpu_selftest_wait_timeout") &&
+                  cudaMemcpy(&gave_up, flag, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+                  cudaMemcpy(&bits, err, sizeof(unsigned), cudaMemcpyDeviceToHost) == cudaSuccess;
+  cudaFree(flag);
+  if (!ok) return -3;
+  cudaMemset(err, 0, sizeof(unsigned));
+  return (gave_up == 1 && (bits & QLA_DEVERR_MBAR_TIMEOUT)) ? 1 : 0;
+}
 
 QLAB_EXPORT const char* qlagpu_version(void) { return "qla_b200 0.1 (QLA 1.9.0 level-1 API, sm_100a)"; }
 
