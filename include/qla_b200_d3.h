@@ -803,6 +803,135 @@ void QLA_D3_H_xeqm_spproj_pD(QLA_D3_HalfFermion *QLA_B200_RESTRICT r, QLA_D3_Dir
 void QLA_D3_D_xeqm_sprecon_H(QLA_D3_DiracFermion *QLA_B200_RESTRICT r, QLA_D3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
 /* replaces QLA_D3_D_xeqm_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
 void QLA_D3_D_xeqm_sprecon_pH(QLA_D3_DiracFermion *QLA_B200_RESTRICT r, QLA_D3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- multi: replaces the D3 functions emitted by lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d) */
+/* replaces QLA_D3_V_veq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veq_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vpeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vpeq_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_vmeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_vmeq_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veqm_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veqm_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veqm_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veqm_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veqm_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veqm_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_veqm_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);
+/* replaces QLA_D3_V_veqm_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_veqm_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int n, int nd);
+/* replaces QLA_D3_V_xeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeq_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xpeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xpeq_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xmeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xmeq_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_nM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_nMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_nMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_npM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_npM_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_npMa_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n, int nd);
+/* replaces QLA_D3_V_xeqm_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_D3_V_xeqm_npMa_times_npV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT ** a, QLA_D3_ColorVector *QLA_B200_RESTRICT ** b, int * index, int n, int nd);
 /* ---- hop: replaces the D3 functions emitted by lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix) */
 /* replaces QLA_D3_H_veq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
 void QLA_D3_H_veq_spproj_M_times_D(QLA_D3_HalfFermion *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracFermion *QLA_B200_RESTRICT b, int mu, int sign, int n);

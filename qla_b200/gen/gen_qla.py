@@ -54,6 +54,7 @@ CITE = {
     "redot": "lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)",
     "hop": "lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336",
     "hop_x": "doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)",
+    "multi": "lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)",
     "mfunc": "lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, "
              "M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143",
 }
@@ -350,6 +351,25 @@ def gen_pc(pc, R, P):
                         f"qlab::api_map<qlab::SpreconOp<{R}, 3>>({kid('sprecon')}, r, {oa}, qlab::Opnd{{}}, {gang}, "
                         f"n, {EQ_ENUM[eq]}, mu, sign);")
                 fns.append(Fn(name, params, body, "sprecon", CITE["sprecon"], dict(eqop=eq, var=var, a=src)))
+    # ---- multi-direction accumulation r (eqop) sum_d a_d * b_d
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        tail = [("int *", "index")] if var == "x" else []
+        for eq in EQOPS:
+            for s1 in ["nM", "nMa", "npM", "npMa"]:
+                adja = str(s1.endswith("a")).lower()
+                pa = "p" in s1
+                for s2 in ["nV", "npV"]:
+                    pb = "p" in s2
+                    name = f"QLA_{pc}_V_{var}{eq}_{s1}_times_{s2}"
+                    params = [(f"{ptype(pc, 'V')} *RESTRICT", "r"),
+                              (f"{ptype(pc, 'M')} *RESTRICT {'**' if pa else '*'}", "a"),
+                              (f"{ptype(pc, 'V')} *RESTRICT {'**' if pb else '*'}", "b")] + tail + \
+                        [("int", "n"), ("int", "nd")]
+                    body = (f"qlab::api_multi<{R}, {adja}>({kid('multi')}, r, (const void*)a, {str(pa).lower()}, "
+                            f"(const void*)b, {str(pb).lower()}, {gang}, n, nd, {EQ_ENUM[eq]});")
+                    fns.append(Fn(name, params, body, "multi", CITE["multi"],
+                                  dict(dest="V", eqop=eq, var=var, a=s1, b=s2)))
     # ---- fused spin projection x colour matrix (Wilson hop terms)
     for var in ["v", "x"]:
         gang = "index" if var == "x" else "nullptr"
@@ -573,7 +593,8 @@ def main():
         text += HEADER_END
         written += write_if_changed(os.path.join(OUT_INC, fname), text)
     for (pc, family), fns in groups.items():
-        extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n'}.get(family, "")
+        extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n',
+                 "multi": '#include <vector>\n#include "../qla_multi.cuh"\n'}.get(family, "")
         if pc == "FN" and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)

@@ -93,6 +93,25 @@ def build(pc, dt, seed):
         call(f"QLA_{pc}_H_x{eq}_spproj_pD", ctypes.c_void_p(r.ctypes.data), parr(ins["D"], ins["idx"], 12), 2, -1,
              ctypes.c_void_p(ins["gang"].ctypes.data), N)
         out[f"QLA_{pc}_H_x{eq}_spproj_pD|2|-1"] = r
+    # multi-direction accumulation, nd = 4 directions (host arrays of fields)
+    nd = 4
+    ms = [T.haar_su3(rng, NS, dt) for _ in range(nd)]
+    vs = [T.gaussian_field(rng, NS, 3, dt) for _ in range(nd)]
+    for d in range(nd):
+        ins[f"nm_M{d}"], ins[f"nm_V{d}"] = ms[d], vs[d]
+    am = (ctypes.c_void_p * nd)(*[m.ctypes.data for m in ms])
+    bv = (ctypes.c_void_p * nd)(*[v.ctypes.data for v in vs])
+    apm = [parr(m, ins["idx"], 9) for m in ms]
+    bpv = [parr(v, ins["idx"][::-1].copy(), 3) for v in vs]
+    apmm = (ctypes.c_void_p * nd)(*[ctypes.cast(x, ctypes.c_void_p).value for x in apm])
+    bpvv = (ctypes.c_void_p * nd)(*[ctypes.cast(x, ctypes.c_void_p).value for x in bpv])
+    for eq in EQOPS:
+        for s1, a_arg in (("nM", am), ("npMa", apmm)):
+            for s2, b_arg in (("nV", bv), ("npV", bpvv)):
+                name = f"QLA_{pc}_V_v{eq}_{s1}_times_{s2}"
+                r = ins["r0V"].copy()
+                call(name, ctypes.c_void_p(r.ctypes.data), a_arg, b_arg, N, nd)
+                out[name] = r
     # fused spin projection x colour matrix (the Wilson hop terms)
     for mu in range(5):
         for sign in (1, -1):

@@ -230,3 +230,51 @@ def test_fused_hop_terms(qla, pc, dt):
         T.ora_hop(want, None, d_src, n, mu, 1, eq, "D", "spproj")
         assert T.bits_equal(T.to_host(r_d), want), ("Dspproj", eq, mu)
     assert count > 400
+
+
+@pytest.mark.parametrize("pc,dt", PCS)
+@pytest.mark.parametrize("nd", [1, 3, 8, 11])
+def test_multi_direction_sum(qla, cuda, pc, dt, nd):
+    """V_{v,x}{eqop}_n{p}M{a}_times_n{p}V: r (eqop) sum_d A_d b_d with the
+    reference's per-direction rounding; nd = 11 runs in two launches;
+    operand tables on the host and on the device."""
+    rng = np.random.default_rng(90 + nd)
+    n, ns = 1037, 1100
+    ms = [T.haar_su3(rng, ns, dt) for _ in range(nd)]
+    vs = [T.gaussian_field(rng, ns, 3, dt) for _ in range(nd)]
+    r0 = T.gaussian_field(rng, n, 3, dt)
+    ia = rng.integers(0, ns, ns).astype(np.int32)
+    ib = rng.integers(0, ns, ns).astype(np.int32)
+    gang = _perm(rng, n)
+    md = [T.to_dev(m) for m in ms]
+    vd = [T.to_dev(v) for v in vs]
+    pms = [T.ptr_array(m, ia, rec_bytes(pc, "M")) for m in md]
+    pvs = [T.ptr_array(v, ib, rec_bytes(pc, "V")) for v in vd]
+    import ctypes
+    L = qla.lib()
+
+    def table(ts, on_dev):
+        addrs = np.array([t.data_ptr() for t in ts], dtype=np.int64)
+        if on_dev:
+            d = T.to_dev(addrs)
+            return d, d.data_ptr()
+        return addrs, addrs.ctypes.data
+
+    for var, eq, s1, s2 in itertools.product(["v", "x"], T.EQOPS, ["nM", "nMa", "npM"], ["nV", "npV"]):
+        on_dev = (eq in ("peq", "eqm"))
+        keep_a, a_addr = table(pms if "p" in s1 else md, on_dev)
+        keep_b, b_addr = table(pvs if "p" in s2 else vd, not on_dev)
+        r_d = T.to_dev(r0)
+        fn = getattr(L, f"QLA_{pc}_V_{var}{eq}_{s1}_times_{s2}")
+        fn.restype = None
+        args = [ctypes.c_void_p(r_d.data_ptr()), ctypes.c_void_p(a_addr), ctypes.c_void_p(b_addr)]
+        gd = T.to_dev(gang)
+        if var == "x":
+            args.append(ctypes.c_void_p(gd.data_ptr()))
+        fn(*args, ctypes.c_int(n), ctypes.c_int(nd))
+        qla.check(fn.__name__)
+        want = r0.copy() if var == "v" else np.concatenate([r0, np.zeros((ns - n, 6), dt)])[:n].copy()
+        T.ora_multi(want, ms, vs, n, eq, adja=int(s1.endswith("a")), idx_a=ia if "p" in s1 else None,
+                    idx_b=ib if "p" in s2 else None, gang=gang if var == "x" else None)
+        assert T.bits_equal(T.to_host(r_d), want), (var, eq, s1, s2, nd)
+        del keep_a, keep_b

@@ -50,6 +50,14 @@ def replay(pc, name, ins):
         T.ora_spproj(r, ins["D"], n, mu, sign, eq, idx_a=ins["idx"] if p else None,
                      gang=ins["gang"] if var == "x" else None)
         return r
+    m = re.match(r"QLA_(F3|D3)_V_v(eq|peq|meq|eqm)_n(p?)M(a?)_times_n(p?)V$", key)
+    if m:
+        _, eq, pa, adj, pb = m.groups()
+        nd = 4
+        r = ins["r0V"].copy()
+        return T.ora_multi(r, [ins[f"nm_M{d}"] for d in range(nd)], [ins[f"nm_V{d}"] for d in range(nd)], n, eq,
+                           adja=int(bool(adj)), idx_a=ins["idx"] if pa else None,
+                           idx_b=ins["idx"][::-1].copy() if pb else None)
     m = re.match(r"QLA_(F3|D3)_(H|D)_v(eq|peq|meq|eqm)_(spproj|sprecon)_(M|Ma)_times_(p?)(D|H)$", key)
     if m:
         _, dest, eq, kind, s1, p, _ = m.groups()
