@@ -57,6 +57,24 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(value, world, device=None):
+    """Largest per-rank value (the slowest rank's time) across the job."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, sites, iters, steps, ms_max):
+    """Site-updates/s of the whole job: every replica processes `sites`
+    sites through `iters` iterations per step; the job takes the slowest
+    rank's time."""
+    return world * sites * iters * steps / (ms_max / 1e3)
+
+
 # ---------------------------------------------------------------------------
 # clock sampling during the timed region
 class ClockSampler:
@@ -239,13 +257,6 @@ def run_gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def chain(xa, pa, ch, ev=None):
         """One step: `iters` iterations of axpy, norm2, dot; reduction results
         stay on the device (asynchronous calls)."""
@@ -304,8 +315,8 @@ def run_gpu_arm(args):
     clk.start()
     ms_f, kern_f = timed(x, p, chain_f)
     clocks = clk.stop()
-    ms_f = max_over_ranks(ms_f)
-    value = world * n * iters * args.steps / (ms_f / 1e3)
+    ms_f = max_over_ranks(ms_f, world, dev)
+    value = whole_job_rate(world, n, iters, args.steps, ms_f)
     assert np.all(np.isfinite(nrm.cpu().numpy()))
 
     # ---------------- end to end through the C-ABI with host buffers: per step
@@ -337,8 +348,8 @@ def run_gpu_arm(args):
             e2e_step()
         e1.record(stream)
         barrier()
-        ms_e = max_over_ranks(e0.elapsed_time(e1))
-        e2e = {"value": world * n * iters * e_steps / (ms_e / 1e3), "unit": UNIT,
+        ms_e = max_over_ranks(e0.elapsed_time(e1), world, dev)
+        e2e = {"value": whole_job_rate(world, n, iters, e_steps, ms_e), "unit": UNIT,
                "h2d_bytes_per_step": int(xh.numel() * 4 + ph.numel() * 4),
                "d2h_bytes_per_step": int(nrm_h.numel() * 8 + dot_h.numel() * 8), "steps": e_steps,
                "ms_per_step": ms_e / e_steps}
@@ -353,8 +364,8 @@ def run_gpu_arm(args):
         xd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
         pd = torch.randn(n, 24, device=dev, dtype=torch.float64, generator=g)
         ms_d, kern_d = timed(xd, pd, chain_d)
-        ms_d = max_over_ranks(ms_d)
-        value_d = world * n * iters * args.steps / (ms_d / 1e3)
+        ms_d = max_over_ranks(ms_d, world, dev)
+        value_d = whole_job_rate(world, n, iters, args.steps, ms_d)
         del xd, pd
         torch.cuda.empty_cache()
 
@@ -486,6 +497,13 @@ def run_workload(args):
                     for sg in (1, -1):
                         fz(V(Out), V(U[mu]), V(D), V(nbr[(mu, sg)]), mu, sg, n)
             ms_f = _events_time(torch, stream, hop_fused, reps)
+            # staggered-style 4-direction sum r += sum_mu U_mu V[x+mu] through
+            # QLA's pointer form (QLA_<pc>_V_vpeq_nM_times_npV, nd = 4)
+            pv = [(Vv.data_ptr() + nbr[(mu, 1)].long() * 24 * e).contiguous() for mu in range(4)]
+            tab_a = (ctypes.c_void_p * 4)(*[U[mu].data_ptr() for mu in range(4)])
+            tab_b = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in pv])
+            nmv = getattr(L, f"QLA_{pc}_V_vpeq_nM_times_npV")
+            ms_nm = _events_time(torch, stream, lambda: nmv(V(Vo), tab_a, tab_b, n, 4), reps * 4)
             t_sp = _events_time(torch, stream, lambda: sp(V(H), V(D), 0, 1, n), reps * 4)
             t_mh = _events_time(torch, stream, lambda: mh(V(H2), V(U[0]), V(H), V(nbr[(0, 1)]), n), reps * 4)
             t_rc = _events_time(torch, stream, lambda: rc(V(Out), V(H2), 0, 1, n), reps * 4)
@@ -499,6 +517,10 @@ def run_workload(args):
                  "M_times_pV": 120 * e + 8}
             tk = {"spproj": t_sp, "M_times_xH": t_mh, "sprecon": t_rc, "M_times_xV": t_mv, "M_times_pV": t_mvp}
             res[pc] = {"site_updates_per_s": n / (ms / 1e3), "ms_per_hop": ms,
+                       "nM_times_npV_nd4": {"us": 1e3 * ms_nm, "gbs": (4 * (72 * e + 8 + 24 * e) + 48 * e) * n /
+                                            (ms_nm / 1e3) / 1e9,
+                                            "frac": (4 * (72 * e + 8 + 24 * e) + 48 * e) * n / (ms_nm / 1e3) / 1e9
+                                            / peak},
                        "fused": {"op": f"QLA_{pc}_D_peq_spproj_M_times_xD", "ms_per_hop": ms_f,
                                  "site_updates_per_s": n / (ms_f / 1e3),
                                  "hbm_frac": n * 8 * (364 * e) / (ms_f / 1e3) / 1e9 / peak,
@@ -507,7 +529,7 @@ def run_workload(args):
                        / 1e9 / peak,
                        "kernels": {k: {"us": 1e3 * tk[k], "gbs": b[k] * n / (tk[k] / 1e3) / 1e9,
                                        "frac": b[k] * n / (tk[k] / 1e3) / 1e9 / peak} for k in tk}}
-            del D, Out, H, H2, U, Vv, Vo, nbr, ptrs
+            del D, Out, H, H2, U, Vv, Vo, nbr, ptrs, pv
             torch.cuda.empty_cache()
         out.update({"metric": "Wilson-hop level-1 sequence (8 x spproj, M_times_xH, vpeq_sprecon), 32^3x64",
                     "unit": "site-updates/s", "value": res["F3"]["site_updates_per_s"], "F3": res["F3"],
