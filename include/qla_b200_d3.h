@@ -803,6 +803,783 @@ void QLA_D3_H_xeqm_spproj_pD(QLA_D3_HalfFermion *QLA_B200_RESTRICT r, QLA_D3_Dir
 void QLA_D3_D_xeqm_sprecon_H(QLA_D3_DiracFermion *QLA_B200_RESTRICT r, QLA_D3_HalfFermion *QLA_B200_RESTRICT a, int mu, int sign, int * index, int n);
 /* replaces QLA_D3_D_xeqm_sprecon_pH (lib/perl/build_qla.pl:1112-1135, expressions_gamma.pl:309-337) */
 void QLA_D3_D_xeqm_sprecon_pH(QLA_D3_DiracFermion *QLA_B200_RESTRICT r, QLA_D3_HalfFermion *QLA_B200_RESTRICT * a, int mu, int sign, int * index, int n);
+/* ---- prop: replaces the D3 functions emitted by lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products) */
+/* replaces QLA_D3_P_veq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veq_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_M_veq_spintrace_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_M_veq_spintrace_P(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_spintrace_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_M_veq_spintrace_pP(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_P_vpeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vpeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vpeq_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_vmeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_vmeq_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_veqm_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_veqm_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_P_xeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeq_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_M_xeq_spintrace_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_M_xeq_spintrace_P(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_spintrace_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_M_xeq_spintrace_pP(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_P_xpeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xpeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xpeq_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xmeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xmeq_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_M_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_M_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_M_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_M_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Ma_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Ma_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Ma_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Ma_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pM_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pM_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pM_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pM_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pMa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pMa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pMa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pMa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_P_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_Pa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pP_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_M(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_Ma(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_pM(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_pMa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_P(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_Pa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_pP(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_P_xeqm_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_D3_P_xeqm_pPa_times_pPa(QLA_D3_DiracPropagator *QLA_B200_RESTRICT r, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_D3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
 /* ---- multi: replaces the D3 functions emitted by lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d) */
 /* replaces QLA_D3_V_veq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
 void QLA_D3_V_veq_nM_times_nV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n, int nd);

@@ -25,7 +25,9 @@ void ora_dot_field_##SFX(R *r, const R *a, const R *b, long n, int ncplx,       
 double ora_norm2_exact_##SFX(const R *a, long n, int ncplx, const int *idx_a,    \
                              const int *gang);                                    \
 void ora_dot_exact_##SFX(double *out2, const R *a, const R *b, long n, int ncplx,\
-                         const int *idx_a, const int *idx_b, const int *gang);
+                         const int *idx_a, const int *idx_b, const int *gang);                  \
+void ora_prop_##SFX(int kind, int ca, int cb, int eqop, R *r, const R *a, const R *b,  \
+                    long n, const int *idx_a, const int *idx_b, const int *gang);
 
 ORA_DECL(f, float)
 ORA_DECL(d, double)

@@ -36,7 +36,7 @@ EQOPS = ["eq", "peq", "meq", "eqm"]
 EQ_ENUM = {"eq": "qlab::EQ", "peq": "qlab::PEQ", "meq": "qlab::MEQ", "eqm": "qlab::EQM"}
 # record abbreviation -> (type name, columns per colour row, complex per record at Nc=3)
 REC = {"V": ("ColorVector", 1, 3), "H": ("HalfFermion", 2, 6), "D": ("DiracFermion", 4, 12),
-       "M": ("ColorMatrix", 3, 9)}
+       "M": ("ColorMatrix", 3, 9), "P": ("DiracPropagator", 48, 144)}
 FIELD_TYPES = ["V", "H", "D", "M"]
 
 # citations into the reference generator for each family
@@ -55,6 +55,7 @@ CITE = {
     "hop": "lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336",
     "hop_x": "doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)",
     "multi": "lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)",
+    "prop": "lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)",
     "mfunc": "lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, "
              "M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143",
 }
@@ -351,6 +352,36 @@ def gen_pc(pc, R, P):
                         f"qlab::api_map<qlab::SpreconOp<{R}, 3>>({kid('sprecon')}, r, {oa}, qlab::Opnd{{}}, {gang}, "
                         f"n, {EQ_ENUM[eq]}, mu, sign);")
                 fns.append(Fn(name, params, body, "sprecon", CITE["sprecon"], dict(eqop=eq, var=var, a=src)))
+    # ---- DiracPropagator products and spin trace
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        tail = [("int *", "index")] if var == "x" else []
+        for eq in EQOPS:
+            pairs = []
+            for ta in ["M", "Ma", "pM", "pMa"]:
+                for tb in ["P", "Pa", "pP", "pPa"]:
+                    pairs.append((ta, tb, "PK_MP"))
+            for ta in ["P", "Pa", "pP", "pPa"]:
+                for tb in ["M", "Ma", "pM", "pMa"]:
+                    pairs.append((ta, tb, "PK_PM"))
+                for tb in ["P", "Pa", "pP", "pPa"]:
+                    pairs.append((ta, tb, "PK_PP"))
+            for ta, tb, kind in pairs:
+                name = f"QLA_{pc}_P_{var}{eq}_{ta}_times_{tb}"
+                pa, oa = operand(pc, ta.strip("p").rstrip("a"), ta.startswith("p"), "a")
+                pb, ob = operand(pc, tb.strip("p").rstrip("a"), tb.startswith("p"), "b")
+                ca, cb = str(ta.endswith("a")).lower(), str(tb.endswith("a")).lower()
+                params = [(f"{ptype(pc, 'P')} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                body = (f"qlab::api_prop<{R}, qlab::{kind}, {ca}, {cb}>({kid('prop')}, r, {oa}, {ob}, {gang}, n, "
+                        f"{EQ_ENUM[eq]});")
+                fns.append(Fn(name, params, body, "prop", CITE["prop"], dict(dest="P", eqop=eq, var=var, a=ta, b=tb)))
+            for src, p1 in ([("P", False), ("pP", True)] if eq == "eq" else []):
+                name = f"QLA_{pc}_M_{var}{eq}_spintrace_{src}"
+                pa, oa = operand(pc, "P", p1, "a")
+                params = [(f"{ptype(pc, 'M')} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                body = (f"qlab::api_prop<{R}, qlab::PK_TRACE, false, false>({kid('prop')}, r, {oa}, qlab::Opnd{{}}, "
+                        f"{gang}, n, {EQ_ENUM[eq]});")
+                fns.append(Fn(name, params, body, "prop", CITE["prop"], dict(dest="M", eqop=eq, var=var, a=src)))
     # ---- multi-direction accumulation r (eqop) sum_d a_d * b_d
     for var in ["v", "x"]:
         gang = "index" if var == "x" else "nullptr"
@@ -594,7 +625,8 @@ def main():
         written += write_if_changed(os.path.join(OUT_INC, fname), text)
     for (pc, family), fns in groups.items():
         extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n',
-                 "multi": '#include <vector>\n#include "../qla_multi.cuh"\n'}.get(family, "")
+                 "multi": '#include <vector>\n#include "../qla_multi.cuh"\n',
+                 "prop": '#include "../qla_prop.cuh"\n'}.get(family, "")
         if pc == "FN" and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)

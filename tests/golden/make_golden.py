@@ -93,6 +93,25 @@ def build(pc, dt, seed):
         call(f"QLA_{pc}_H_x{eq}_spproj_pD", ctypes.c_void_p(r.ctypes.data), parr(ins["D"], ins["idx"], 12), 2, -1,
              ctypes.c_void_p(ins["gang"].ctypes.data), N)
         out[f"QLA_{pc}_H_x{eq}_spproj_pD|2|-1"] = r
+    # DiracPropagator products and spin trace
+    ins["P1"] = T.gaussian_field(rng, NS, 144, dt)
+    ins["P2"] = T.gaussian_field(rng, NS, 144, dt)
+    ins["r0P"] = T.gaussian_field(rng, N, 144, dt)
+    for name, aa, bb, pb in ((f"QLA_{pc}_P_vpeq_M_times_P", "M", "P1", False),
+                             (f"QLA_{pc}_P_veq_Ma_times_pPa", "M", "P1", True),
+                             (f"QLA_{pc}_P_vmeq_Pa_times_M", "P1", "M", False),
+                             (f"QLA_{pc}_P_veqm_P_times_pMa", "P1", "M", True),
+                             (f"QLA_{pc}_P_veq_P_times_P", "P1", "P2", False),
+                             (f"QLA_{pc}_P_vpeq_Pa_times_pP", "P1", "P2", True),
+                             (f"QLA_{pc}_P_veq_P_times_Pa", "P1", "P2", False)):
+        r = ins["r0P"].copy()
+        nb = 9 if bb == "M" else 144
+        b = parr(ins[bb], ins["idx"], nb) if pb else ctypes.c_void_p(ins[bb].ctypes.data)
+        call(name, ctypes.c_void_p(r.ctypes.data), ctypes.c_void_p(ins[aa].ctypes.data), b, N)
+        out[name] = r
+    r = ins["r0M"].copy()
+    call(f"QLA_{pc}_M_veq_spintrace_P", ctypes.c_void_p(r.ctypes.data), ctypes.c_void_p(ins["P1"].ctypes.data), N)
+    out[f"QLA_{pc}_M_veq_spintrace_P"] = r
     # multi-direction accumulation, nd = 4 directions (host arrays of fields)
     nd = 4
     ms = [T.haar_su3(rng, NS, dt) for _ in range(nd)]

@@ -388,3 +388,14 @@ def ora_multi(r, ms, vs, n, eqop, adja=0, idx_a=None, idx_b=None, gang=None):
         eq_d = eqop if d == 0 else ("meq" if minus else "peq")
         ora_lmult(r, ms[d], vs[d], n, 1, eq_d, adja=adja, idx_a=idx_a, idx_b=idx_b, gang=gang)
     return r
+
+
+PKIND = {"MP": 0, "PM": 1, "PP": 2, "TRACE": 3}
+
+
+def ora_prop(kind, r, a, b, n, eqop, ca=0, cb=0, idx_a=None, idx_b=None, gang=None):
+    f = getattr(oracle(), "ora_prop_" + rtype(r.dtype))
+    idx_a, idx_b, gang = _i32(idx_a), _i32(idx_b), _i32(gang)
+    f(PKIND[kind], ca, cb, EQOPS.get(eqop, eqop), ptr(r), ptr(a), ptr(b), ctypes.c_long(n), ptr(idx_a), ptr(idx_b),
+      ptr(gang))
+    return r

@@ -32,7 +32,7 @@ def replay(pc, name, ins):
     n = len(ins["gang"])
     dt = ins["V"].dtype
     key, *extra = name.split("|")
-    m = re.match(r"QLA_(F3|D3|DF3)_(\w)_([vx])(eq|peq|meq|eqm)_(p?Ma?)_times_(p?\w+)$", key)
+    m = re.match(r"QLA_(F3|D3|DF3)_([VHDM])_([vx])(eq|peq|meq|eqm)_(p?Ma?)_times_(p?\w+)$", key)
     if m:
         _, dest, var, eq, s1, s2 = m.groups()
         r = (ins["r0" + dest] if dest != "M" else ins["r0M"]).copy()
@@ -50,6 +50,18 @@ def replay(pc, name, ins):
         T.ora_spproj(r, ins["D"], n, mu, sign, eq, idx_a=ins["idx"] if p else None,
                      gang=ins["gang"] if var == "x" else None)
         return r
+    m = re.match(r"QLA_(F3|D3)_P_v(eq|peq|meq|eqm)_(p?)(M|P)(a?)_times_(p?)(M|P)(a?)$", key)
+    if m:
+        _, eq, _, ta, ca, pb, tb, cb = m.groups()
+        kind = {"MP": "MP", "PM": "PM", "PP": "PP"}[ta + tb]
+        r = ins["r0P"].copy()
+        a = ins["M"] if ta == "M" else ins["P1"]
+        b = ins["M"] if tb == "M" else (ins["P2"] if ta == "P" else ins["P1"])
+        return T.ora_prop(kind, r, a, b, n, eq, ca=int(bool(ca)), cb=int(bool(cb)), idx_b=ins["idx"] if pb else None)
+    m = re.match(r"QLA_(F3|D3)_M_veq_spintrace_P$", key)
+    if m:
+        r = ins["r0M"].copy()
+        return T.ora_prop("TRACE", r, ins["P1"], None, n, "eq")
     m = re.match(r"QLA_(F3|D3)_V_v(eq|peq|meq|eqm)_n(p?)M(a?)_times_n(p?)V$", key)
     if m:
         _, eq, pa, adj, pb = m.groups()
