@@ -2623,6 +2623,103 @@ void QLA_D3_M_xeq_sqrt_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorM
 void QLA_D3_M_xeq_inverse_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
 /* replaces QLA_D3_C_xeq_det_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_D3_C_xeq_det_pM(QLA_D_Complex *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* ---- mfunc_ext: replaces the D3 functions emitted by lib/perl/build_qla.pl:1022-1061 (matrix functions */
+/* replaces QLA_D3_M_veq_invsqrt_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_invsqrt_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_log_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_log_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_expA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_expA_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_expTA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_expTA_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_sqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_sqrtPH_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_invsqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_invsqrtPH_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_V_veq_eigenvals_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_veq_eigenvals_M(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_V_veq_eigenvalsH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_veq_eigenvalsH_M(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_D3_M_veq_invsqrt_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_invsqrt_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_M_veq_log_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_log_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_M_veq_expA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_expA_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_M_veq_expTA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_expTA_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_M_veq_sqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_sqrtPH_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_M_veq_invsqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_veq_invsqrtPH_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_V_veq_eigenvals_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_veq_eigenvals_pM(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_V_veq_eigenvalsH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_veq_eigenvalsH_pM(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_D3_M_xeq_invsqrt_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_invsqrt_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_log_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_log_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_expA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_expA_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_expTA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_expTA_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_sqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_sqrtPH_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_invsqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_invsqrtPH_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_V_xeq_eigenvals_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_xeq_eigenvals_M(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_V_xeq_eigenvalsH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_xeq_eigenvalsH_M(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_D3_M_xeq_invsqrt_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_invsqrt_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_M_xeq_log_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_log_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_M_xeq_expA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_expA_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_M_xeq_expTA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_expTA_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_M_xeq_sqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_sqrtPH_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_M_xeq_invsqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_M_xeq_invsqrtPH_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_V_xeq_eigenvals_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_xeq_eigenvals_pM(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_V_xeq_eigenvalsH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_D3_V_xeq_eigenvalsH_pM(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_D3_V_veq_M_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_veq_M_inverse_V(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_V_veq_M_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_veq_M_inverse_pV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_V_veq_pM_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_veq_pM_inverse_V(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_V_veq_pM_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_veq_pM_inverse_pV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_V_xeq_M_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_xeq_M_inverse_V(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_V_xeq_M_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_xeq_M_inverse_pV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_V_xeq_pM_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_xeq_pM_inverse_V(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_V_xeq_pM_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_V_xeq_pM_inverse_pV(QLA_D3_ColorVector *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_M_veq_M_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_veq_M_inverse_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_M_veq_M_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_veq_M_inverse_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_M_veq_pM_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_veq_pM_inverse_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_D3_M_veq_pM_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_veq_pM_inverse_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_D3_M_xeq_M_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_xeq_M_inverse_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_M_xeq_M_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_xeq_M_inverse_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_D3_M_xeq_pM_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_xeq_pM_inverse_M(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_D3_M_xeq_pM_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_D3_M_xeq_pM_inverse_pM(QLA_D3_ColorMatrix *QLA_B200_RESTRICT r, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_D3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
 /* ---- norm2: replaces the D3 functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_D3_r_veq_norm2_V (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_D3_r_veq_norm2_V(QLA_D_Real *QLA_B200_RESTRICT r, QLA_D3_ColorVector *QLA_B200_RESTRICT a, int n);

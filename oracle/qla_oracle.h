@@ -37,8 +37,20 @@ ORA_DECL(d, double)
 #define ORA_MF_SQRT 1
 #define ORA_MF_INVERSE 2
 #define ORA_MF_DET 3
-void ora_mfunc_f(float *r, const float *a, long n, int nc, int which);
-void ora_mfunc_d(double *r, const double *a, long n, int nc, int which);
+#define ORA_MF_INVSQRT 4
+#define ORA_MF_LOG 5
+#define ORA_MF_EXPA 6
+#define ORA_MF_EXPTA 7
+#define ORA_MF_SQRTPH 8
+#define ORA_MF_INVSQRTPH 9
+#define ORA_MF_EIGENVALS 10
+#define ORA_MF_EIGENVALSH 11
+int ora_mfunc_f(float *r, const float *a, long n, int nc, int which);
+int ora_mfunc_d(double *r, const double *a, long n, int nc, int which);
+/* r = a^-1 b per site; nb = 1 (ColorVector) or nc (ColorMatrix) */
+void ora_minv_f(float *r, const float *a, const float *b, long n, int nc, int nb, const int *ia, const int *ib);
+void ora_minv_d(double *r, const double *a, const double *b, long n, int nc, int nb, const int *ia,
+                const int *ib);
 
 /* QLA_I_ integer ops (codes as the product's IntCode, 19 = mask) */
 void ora_int(int code, int eqop, int *r, const int *a, const int *b, const int *c, int s, long n,

@@ -67,16 +67,17 @@ static double FN(fnorm2)(const FN(mc) *a, int nc)
  * (M_eq_M_inverse_M.c:108-135; also the generic path of M_eq_inverse_M.c:120-162
  * with b = 1).  Rows are swapped physically; the arithmetic is the same as
  * the template's row-permutation form. */
-static void FN(m_eq_m_inverse_m)(FN(mc) *x, int nc, const FN(mc) *a, const FN(mc) *b)
+static void FN(m_eq_m_inverse_m)(FN(mc) *x, int nc, const FN(mc) *a, const FN(mc) *b, int nb)
 {
   FN(mc) c[ORA_NCMAX * ORA_NCMAX], d[ORA_NCMAX * ORA_NCMAX];
   int row[ORA_NCMAX];
   for (int i = 0; i < nc; i++) {
-    for (int j = 0; j < nc; j++) { EL(c, i, j) = EL(a, i, j); EL(d, i, j) = EL(b, i, j); }
+    for (int j = 0; j < nc; j++) EL(c, i, j) = EL(a, i, j);
+    for (int j = 0; j < nb; j++) d[i * nb + j] = b[i * nb + j];
     row[i] = i;
   }
 #define CC(i, j) EL(c, row[i], j)
-#define DD(i, j) EL(d, row[i], j)
+#define DD(i, j) d[row[i] * nb + (j)]
   for (int k = 0; k < nc; k++) {
     R rmax = CC(k, k).re * CC(k, k).re + CC(k, k).im * CC(k, k).im;
     int imax = k;
@@ -99,17 +100,17 @@ static void FN(m_eq_m_inverse_m)(FN(mc) *x, int nc, const FN(mc) *a, const FN(mc
         CC(i, j).re -= (t.re * CC(k, j).re - t.im * CC(k, j).im);
         CC(i, j).im -= (t.re * CC(k, j).im + t.im * CC(k, j).re);
       }
-      for (int j = 0; j < nc; j++) {
+      for (int j = 0; j < nb; j++) {
         DD(i, j).re -= (t.re * DD(k, j).re - t.im * DD(k, j).im);
         DD(i, j).im -= (t.re * DD(k, j).im + t.im * DD(k, j).re);
       }
     }
   }
   for (int i = 0; i < nc; i++)
-    for (int j = 0; j < nc; j++) {
+    for (int j = 0; j < nb; j++) {
       FN(mc) u = CC(i, i), v = DD(i, j);
-      EL(x, i, j).re = u.re * v.re - u.im * v.im;
-      EL(x, i, j).im = u.re * v.im + u.im * v.re;
+      x[i * nb + j].re = u.re * v.re - u.im * v.im;
+      x[i * nb + j].im = u.re * v.im + u.im * v.re;
     }
 #undef CC
 #undef DD
@@ -199,9 +200,9 @@ static void FN(inverse1)(FN(mc) *x, const FN(mc) *a, int nc)
 #undef SET
     return;
   }
-  FN(mc) one[ORA_NCMAX * ORA_NCMAX];
+  FN(mc) one[ORA_NCMAX * ORA_NCMAX] = {{0}};
   FN(m_eq_d)(one, nc, 1);
-  FN(m_eq_m_inverse_m)(x, nc, a, one);
+  FN(m_eq_m_inverse_m)(x, nc, a, one, nc);
 }
 
 /* ------------------------------------------------------------------ exp */
@@ -239,7 +240,7 @@ static void FN(exp1)(FN(mc) *r, const FN(mc) *a, int nc)
     pb[k].re = qb[k].re - bs6[k].re;
     pb[k].im = qb[k].im - bs6[k].im;
   }
-  FN(m_eq_m_inverse_m)(qb, nc, pb, bs6);
+  FN(m_eq_m_inverse_m)(qb, nc, pb, bs6, nc);
   FN(m_eq_d)(pb, nc, 1);
   FN(m_peq_r_times_m)(pb, nc, (R)2, qb);
   if (s == 1) { memcpy(r, pb, sizeof(FN(mc)) * nc * nc); return; }
@@ -255,44 +256,536 @@ static void FN(exp1)(FN(mc) *r, const FN(mc) *a, int nc)
 /* ----------------------------------------------------------------- sqrt */
 /* M_eq_sqrt_M.c:139-180: Newton iteration e <- -1/2 e x^-1 e, x += e, until
  * |e|_F^2 <= EPS (FLT_EPSILON / DBL_EPSILON) or 20 iterations. */
-static void FN(sqrt1)(FN(mc) *r, const FN(mc) *a, int nc, double eps)
+/* Newton loop shared by sqrt and invsqrt (M_eq_sqrt_M.c:158-171,
+ * M_eq_invsqrt_M.c:160-173): e <- -1/2 e x^-1 e, x += e. */
+static void FN(newton_sqrt)(FN(mc) *x, FN(mc) *e, int nc, double eps)
 {
-  double ds = FN(fnorm2)(a, nc);
-  if (ds == 0) { FN(m_eq_d)(r, nc, 0); return; }
-  ds = sqrt(ds);
-  FN(mc) x[ORA_NCMAX * ORA_NCMAX], e[ORA_NCMAX * ORA_NCMAX], t1[ORA_NCMAX * ORA_NCMAX],
-      t2[ORA_NCMAX * ORA_NCMAX];
-  FN(m_eq_r_times_m)(x, nc, (R)(1 / ds), a);
-  FN(m_eq_d)(e, nc, (R)0.5);
-  FN(m_peq_r_times_m)(e, nc, (R)(-0.5), x);
-  for (int k = 0; k < nc * nc; k++) { x[k].re += e[k].re; x[k].im += e[k].im; }
+  FN(mc) t1[ORA_NCMAX * ORA_NCMAX], t2[ORA_NCMAX * ORA_NCMAX];
   double enorm;
   int nit = 0;
   do {
     nit++;
-    FN(m_eq_m_inverse_m)(t1, nc, x, e);
+    FN(m_eq_m_inverse_m)(t1, nc, x, e, nc);
     FN(m_eq_m_times_m)(t2, nc, e, t1);
     FN(m_eq_r_times_m)(e, nc, (R)(-0.5), t2);
     for (int k = 0; k < nc * nc; k++) { x[k].re += e[k].re; x[k].im += e[k].im; }
     enorm = FN(fnorm2)(e, nc);
   } while (nit < 20 && enorm > eps);
+}
+
+static void FN(sqrt1)(FN(mc) *r, const FN(mc) *a, int nc, double eps)
+{
+  double ds = FN(fnorm2)(a, nc);
+  if (ds == 0) { FN(m_eq_d)(r, nc, 0); return; }
+  ds = sqrt(ds);
+  FN(mc) x[ORA_NCMAX * ORA_NCMAX], e[ORA_NCMAX * ORA_NCMAX];
+  FN(m_eq_r_times_m)(x, nc, (R)(1 / ds), a);
+  FN(m_eq_d)(e, nc, (R)0.5);
+  FN(m_peq_r_times_m)(e, nc, (R)(-0.5), x);
+  for (int k = 0; k < nc * nc; k++) { x[k].re += e[k].re; x[k].im += e[k].im; }
+  FN(newton_sqrt)(x, e, nc, eps);
   FN(m_eq_r_times_m)(r, nc, (R)sqrt(ds), x);
 }
 
+/* -------------------------------------------------------------- invsqrt */
+/* M_eq_invsqrt_M.c:88-127: the same Newton iteration started from
+ * x = 1, e = 0.5 ds a^-1 - 0.5; a zero matrix gives 1/0 on the diagonal. */
+static void FN(invsqrt1)(FN(mc) *r, const FN(mc) *a, int nc, double eps)
+{
+  double ds = FN(fnorm2)(a, nc);
+  if (ds == 0) { FN(m_eq_d)(r, nc, (R)INFINITY); return; }
+  ds = sqrt(ds);
+  FN(mc) x[ORA_NCMAX * ORA_NCMAX], e[ORA_NCMAX * ORA_NCMAX], xi[ORA_NCMAX * ORA_NCMAX];
+  FN(m_eq_d)(x, nc, 1);
+  FN(inverse1)(xi, a, nc);
+  FN(m_eq_d)(e, nc, (R)(-0.5));
+  FN(m_peq_r_times_m)(e, nc, (R)(0.5 * ds), xi);
+  for (int k = 0; k < nc * nc; k++) { x[k].re += e[k].re; x[k].im += e[k].im; }
+  FN(newton_sqrt)(x, e, nc, eps);
+  FN(m_eq_r_times_m)(r, nc, (R)(1 / sqrt(ds)), x);
+}
+
+/* ------------------------------------------------------------------ log */
+/* M_eq_log_M.c:127-199 (every nc > 2): scale by 1/|a|_F, four square roots,
+ * log(1 + x) = x - x^2/2 + x^3 P(x)/Q(x) with the coefficients of :52-68,
+ * times 2^4, plus log|a|_F on the diagonal. */
+static const double FN(logP)[] = {7.70838733755885391666E0, 1.79368678507819816313E1,
+                                  1.44989225341610930846E1, 4.70579119878881725854E0,
+                                  4.97494994976747001425E-1, 1.01875663804580931796E-4};
+static const double FN(logQ)[] = {2.31251620126765340583E1, 7.11544750618563894466E1,
+                                  8.29875266912776603211E1, 4.52279145837532221105E1,
+                                  1.12873587189167450590E1};
+
+static void FN(log1)(FN(mc) *r, const FN(mc) *a, int nc, double eps)
+{
+  double ds = sqrt(FN(fnorm2)(a, nc));
+  if (ds == 0) { FN(m_eq_d)(r, nc, (R)log(0.)); return; }
+  FN(mc) as[ORA_NCMAX * ORA_NCMAX], as2[ORA_NCMAX * ORA_NCMAX], as3[ORA_NCMAX * ORA_NCMAX],
+      as4[ORA_NCMAX * ORA_NCMAX], as5[ORA_NCMAX * ORA_NCMAX], pa[ORA_NCMAX * ORA_NCMAX],
+      qa[ORA_NCMAX * ORA_NCMAX];
+  FN(m_eq_r_times_m)(as, nc, (R)(1 / ds), a);
+  for (int i = 0; i < 4; i++) {
+    memcpy(as2, as, sizeof(FN(mc)) * nc * nc);
+    FN(sqrt1)(as, as2, nc, eps);
+  }
+  for (int i = 0; i < nc; i++) EL(as, i, i).re -= 1;
+  FN(m_eq_d)(pa, nc, (R)FN(logP)[0]);
+  FN(m_eq_d)(qa, nc, (R)FN(logQ)[0]);
+  FN(m_peq_r_times_m)(pa, nc, (R)FN(logP)[1], as);
+  FN(m_peq_r_times_m)(qa, nc, (R)FN(logQ)[1], as);
+  FN(m_eq_m_times_m)(as2, nc, as, as);
+  FN(m_peq_r_times_m)(pa, nc, (R)FN(logP)[2], as2);
+  FN(m_peq_r_times_m)(qa, nc, (R)FN(logQ)[2], as2);
+  FN(m_eq_m_times_m)(as3, nc, as, as2);
+  FN(m_peq_r_times_m)(pa, nc, (R)FN(logP)[3], as3);
+  FN(m_peq_r_times_m)(qa, nc, (R)FN(logQ)[3], as3);
+  FN(m_eq_m_times_m)(as4, nc, as2, as2);
+  FN(m_peq_r_times_m)(pa, nc, (R)FN(logP)[4], as4);
+  FN(m_peq_r_times_m)(qa, nc, (R)FN(logQ)[4], as4);
+  FN(m_eq_m_times_m)(as5, nc, as, as4);
+  FN(m_peq_r_times_m)(pa, nc, (R)FN(logP)[5], as5);
+  for (int k = 0; k < nc * nc; k++) { qa[k].re += as5[k].re; qa[k].im += as5[k].im; }
+  FN(inverse1)(as5, qa, nc);
+  FN(m_eq_m_times_m)(qa, nc, pa, as5);
+  FN(m_eq_m_times_m)(pa, nc, as3, qa);
+  FN(m_peq_r_times_m)(pa, nc, (R)(-0.5), as2);
+  for (int k = 0; k < nc * nc; k++) { pa[k].re += as[k].re; pa[k].im += as[k].im; }
+  FN(m_eq_r_times_m)(r, nc, (R)16, pa);
+  ds = log(ds);
+  for (int i = 0; i < nc; i++) EL(r, i, i).re += ds;
+}
+
+/* --------------------------------------------- closed forms for nc = 3 */
+static FN(mc) FN(cexpi)(R theta)          /* QLA_F_cexpi / QLA_D_cexpi (lib/cmath/QLA_cexpi.c) */
+{
+  R s, c;
+  M_SINCOS(theta, &s, &c);
+  FN(mc) z; z.re = c; z.im = s;
+  return z;
+}
+
+/* x^3 - p2/2 x - det = 0 for the eigenvalues of the traceless Hermitian Q
+ * with i Q the input; exp(iQ) = f0 + f1 (iQ) + f2 (iQ)^2
+ * (getfs of M_eq_expTA_M.c:139-216, identical in M_eq_expA_M.c) */
+static void FN(getfs_exp)(FN(mc) *f0, FN(mc) *f1, FN(mc) *f2, R p2, R det)
+{
+  R q = (1./6.)*p2;
+  R r = -0.5*det;
+  R sq = M_SQRT(M_FABS(q));
+  R sq3 = sq*sq*sq;
+  if (sq3 > M_FABS(r)) {
+    R t = M_ACOS(r/sq3);
+    FN(mc) sct = FN(cexpi)((1./3.)*t);
+    R sqc = sq*sct.re;
+    R sqs = 1.73205080756887729352*sq*sct.im;
+    R l0 = - 2*sqc;
+    R l1 = sqc + sqs;
+    R l2 = sqc - sqs;
+    R d10 = 0.5*(l1-l0);
+    R d20 = 0.5*(l2-l0);
+    R d21 = l2-l1;
+    FN(mc) eid10, eis01, g10, eid20, eis02, g20, ff0, g2010, b2, f10, z;
+    eis01 = FN(cexpi)(0.5*(l0+l1));
+    if (d10 == 0) {
+      eid10.re = 1; eid10.im = 0.;
+      g10 = eis01;
+    } else {
+      eid10 = FN(cexpi)(d10);
+      R sc10 = eid10.im/d10;
+      g10.re = sc10*eis01.re; g10.im = sc10*eis01.im;
+    }
+    ff0.re = eis01.re*eid10.re + eis01.im*eid10.im;   /* eis01 * conj(eid10) */
+    ff0.im = eis01.im*eid10.re - eis01.re*eid10.im;
+    if (d20 == 0) {
+      eid20.re = 1; eid20.im = 0.;
+      eis02 = ff0;
+      g20 = eis02;
+    } else {
+      eid20 = FN(cexpi)(d20);
+      CMUL(eis02, ff0, eid20);
+      R sc20 = eid20.im/d20;
+      g20.re = sc20*eis02.re; g20.im = sc20*eis02.im;
+    }
+    g2010.re = g20.re - g10.re; g2010.im = g20.im - g10.im;
+    if (d21 == 0) {
+      b2.re = 0; b2.im = 0.;
+    } else {
+      R d21i = 1/d21;
+      b2.re = d21i*g2010.re; b2.im = d21i*g2010.im;
+    }
+    f2->re = b2.im; f2->im = -b2.re;
+    f1->re = (-(l0+l1))*b2.re + g10.re; f1->im = (-(l0+l1))*b2.im + g10.im;
+    f10.re = -g10.im; f10.im = g10.re;
+    z.re = (l1)*f2->re + f10.re; z.im = (l1)*f2->im + f10.im;
+    f0->re = (-l0)*z.re + ff0.re; f0->im = (-l0)*z.im + ff0.im;
+  } else {
+    if (r == 0) {
+      f0->re = 0; f0->im = 0.; f1->re = 0; f1->im = 0.; f2->re = 0; f2->im = 0.;
+    } else {
+      R a = -M_CBRT(r);
+      FN(mc) t, eia, ei3a2, eia2 = FN(cexpi)(0.5*a);
+      CMUL(eia, eia2, eia2);
+      CMUL(ei3a2, eia, eia2);
+      R snc = ei3a2.im/(1.5*a);
+      t.re = snc*eia2.re; t.im = snc*eia2.im;
+      f1->re = -t.im; f1->im = t.re;
+      f2->re = 0; f2->im = 0.;
+      t.re = ei3a2.re; t.im = (-1./3.)*ei3a2.im;
+      CMUL(*f0, eia2, t);
+    }
+  }
+}
+
+/* M_eq_expTA_M.c:218-274 / M_eq_expA_M.c:222-298 (expA first removes
+ * i Im(tr)/3 from the diagonal and multiplies the coefficients by its phase) */
+static void FN(exp3_ah)(FN(mc) *e, const FN(mc) *a, int with_trace)
+{
+  FN(mc) iq[9], mqq[9], f, f0, f1, f2, a0, a1, a2, det0, det1, det2;
+  for (int k = 0; k < 9; k++) iq[k] = a[k];
+  if (with_trace) {
+    R tr = iq[0].im + iq[4].im + iq[8].im;
+    R s = (1./3.)*tr;
+    iq[0].im = iq[0].im - s;
+    iq[4].im = iq[4].im - s;
+    iq[8].im = iq[8].im - s;
+    f = FN(cexpi)(s);
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      CMUL(mqq[i * 3 + j], iq[i * 3 + 0], iq[0 * 3 + j]);
+      CPMS(mqq[i * 3 + j], iq[i * 3 + 1], iq[1 * 3 + j]);
+      CPMS(mqq[i * 3 + j], iq[i * 3 + 2], iq[2 * 3 + j]);
+    }
+  R p2 = -mqq[0].re - mqq[4].re - mqq[8].re;
+  R det;
+  CMUL(det2, iq[0], iq[4]); CMMS(det2, iq[1], iq[3]);
+  CMUL(det1, iq[2], iq[3]); CMMS(det1, iq[0], iq[5]);
+  CMUL(det0, iq[1], iq[5]); CMMS(det0, iq[2], iq[4]);
+  det = -det2.re*iq[8].im - det2.im*iq[8].re;          /* QLA_r_eqm_Im_c_times_c */
+  det -= (det1.re*iq[7].im + det1.im*iq[7].re);        /* QLA_r_meq_Im_c_times_c */
+  det -= (det0.re*iq[6].im + det0.im*iq[6].re);
+  if (with_trace) {
+    FN(getfs_exp)(&f0, &f1, &f2, p2, det);
+    CMUL(a0, f, f0);
+    CMUL(a1, f, f1);
+    CMUL(a2, f, f2);
+  } else {
+    FN(getfs_exp)(&a0, &a1, &a2, p2, det);
+  }
+  for (int k = 0; k < 9; k++) {
+    CMUL(e[k], a2, mqq[k]);
+    CPMS(e[k], a1, iq[k]);
+  }
+  for (int i = 0; i < 3; i++) { e[i * 4].re += a0.re; e[i * 4].im += a0.im; }
+}
+
+/* x^3 - tr x^2 + (tr^2 - p2)/2 x - det = 0 for a positive Hermitian matrix;
+ * sqrt (inv = 0) or inverse sqrt (inv = 1) as f0 + f1 m + f2 m^2
+ * (getfs of M_eq_sqrtPH_M.c:84-138 and M_eq_invsqrtPH_M.c:84-142) */
+static void FN(getfs_sqrtph)(R *f0, R *f1, R *f2, R tr, R p2, R det, int inv)
+{
+  R tr3 = (1./3.)*tr;
+  R p23 = (1./3.)*p2;
+  R tr32 = tr3*tr3;
+  R q = 0.5*(p23-tr32);
+  R r = 0.25*tr3*(5*tr32-p2) - 0.5*det;
+  R sq = M_SQRT(M_FABS(q));
+  R sq3 = sq*sq*sq;
+  if (sq3 > M_FABS(r)) {
+    R t = M_ACOS(r/sq3);
+    FN(mc) sct = FN(cexpi)((1./3.)*t);
+    R sqc = sq*sct.re;
+    R sqs = 1.73205080756887729352*sq*sct.im;
+    R l0 = tr3 - 2*sqc;
+    R ll = tr3 + sqc;
+    R l1 = ll + sqs;
+    R l2 = ll - sqs;
+    R sl0 = M_SQRT(M_FABS(l0));
+    R sl1 = M_SQRT(M_FABS(l1));
+    R sl2 = M_SQRT(M_FABS(l2));
+    R u = sl0 + sl1 + sl2;
+    R w = sl0*sl1*sl2;
+    if (!inv) {
+      R v = sl0*(sl1+sl2) + sl1*sl2;
+      R d = (sl0+sl1)*(sl0+sl2)*(sl1+sl2);
+      R di = 1./d;
+      *f0 = u*w*di;
+      *f1 = (tr+v)*di;
+      *f2 = -di;
+    } else {
+      R d = w*(sl0+sl1)*(sl0+sl2)*(sl1+sl2);
+      R di = 1./d;
+      *f0 = (w*u*u+l0*sl0*(l1+l2)+l1*sl1*(l0+l2)+l2*sl2*(l0+l1))*di;
+      *f1 = -(tr*u+w)*di;
+      *f2 = u*di;
+    }
+  } else {
+    if (r == 0) {
+      *f0 = inv ? 1/M_SQRT(M_FABS(tr3)) : M_SQRT(M_FABS(tr3));
+      *f1 = 0;
+      *f2 = 0;
+    } else {
+      R a = -M_CBRT(r);
+      R l0 = tr3 + 2*a;
+      R l1 = tr3 - a;
+      R sl0 = M_SQRT(M_FABS(l0));
+      R sl1 = M_SQRT(M_FABS(l1));
+      R sl01 = sl0 + sl1;
+      if (!inv) {
+        *f2 = 0;
+        *f1 = (sl01==0) ? 0 : 1/sl01;
+        *f0 = sl0*sl1*(*f1);
+      } else {
+        R p01 = sl0 * sl1;
+        R t = p01*sl01;
+        R ti = 1/t;
+        *f2 = 0;
+        *f1 = -ti;
+        *f0 = (p01+l0+l1)*ti;
+      }
+    }
+  }
+}
+
+/* M_eq_sqrtPH_M.c:140-197 / M_eq_invsqrtPH_M.c:144-201 */
+static void FN(sqrtph3)(FN(mc) *fn, const FN(mc) *m, int inv)
+{
+  FN(mc) mm[9], det0, det1, det2;
+  R f0, f1, f2, det;
+  R tr = m[0].re + m[4].re + m[8].re;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      CMUL(mm[i * 3 + j], m[i * 3 + 0], m[0 * 3 + j]);
+      CPMS(mm[i * 3 + j], m[i * 3 + 1], m[1 * 3 + j]);
+      CPMS(mm[i * 3 + j], m[i * 3 + 2], m[2 * 3 + j]);
+    }
+  R p2 = mm[0].re + mm[4].re + mm[8].re;
+  CMUL(det2, m[0], m[4]); CMMS(det2, m[1], m[3]);
+  CMUL(det1, m[2], m[3]); CMMS(det1, m[0], m[5]);
+  CMUL(det0, m[1], m[5]); CMMS(det0, m[2], m[4]);
+  det = det2.re*m[8].re - det2.im*m[8].im;               /* QLA_r_eq_Re_c_times_c */
+  det += (det1.re*m[7].re - det1.im*m[7].im);            /* QLA_r_peq_Re_c_times_c */
+  det += (det0.re*m[6].re - det0.im*m[6].im);
+  FN(getfs_sqrtph)(&f0, &f1, &f2, tr, p2, det, inv);
+  for (int k = 0; k < 9; k++) {
+    fn[k].re = f2*mm[k].re; fn[k].im = f2*mm[k].im;
+    fn[k].re += f1*m[k].re; fn[k].im += f1*m[k].im;
+  }
+  for (int i = 0; i < 3; i++) fn[i * 4].re += f0;
+}
+
+/* eigenvalues of a Hermitian 3x3 matrix (V_eq_eigenvalsH_M.c:106-166) */
+static void FN(eigh3)(FN(mc) *v, const FN(mc) *m)
+{
+  FN(mc) a00 = m[0], a11 = m[4], a22 = m[8], det0, det1, det2;
+  R s1, s2, det;
+  s1 = (1./3.)*(a00.re + a11.re + a22.re);
+  a00.re -= s1;
+  a11.re -= s1;
+  a22.re -= s1;
+  CMUL(det2, a00, a11); CMMS(det2, m[1], m[3]);
+  CMUL(det1, m[2], m[3]); CMMS(det1, a00, m[5]);
+  CMUL(det0, m[1], m[5]); CMMS(det0, m[2], a11);
+  det = det2.re*a22.re - det2.im*a22.im;
+  det += (det1.re*m[7].re - det1.im*m[7].im);
+  det += (det0.re*m[6].re - det0.im*m[6].im);
+  s2 = det2.re;
+  s2 += (a00.re*a22.re - a00.im*a22.im);
+  s2 -= (m[2].re*m[6].re - m[2].im*m[6].im);
+  s2 += (a11.re*a22.re - a11.im*a22.im);
+  s2 -= (m[5].re*m[7].re - m[5].im*m[7].im);
+  R q = (-1./3.)*s2;
+  R r = -0.5*det;
+  R sq = M_SQRT(M_FABS(q));
+  R sq3 = sq*sq*sq;
+  for (int k = 0; k < 3; k++) v[k].im = 0.;
+  if (sq3 > M_FABS(r)) {
+    R t = M_ACOS(r/sq3);
+    FN(mc) sct = FN(cexpi)((1./3.)*t);
+    R sqc = sq*sct.re;
+    R sqs = 1.73205080756887729352*sq*sct.im;
+    R e0 = s1 - 2*sqc;
+    R ee = s1 + sqc;
+    R e1 = ee + sqs;
+    R e2 = ee - sqs;
+    v[0].re = e0; v[1].re = e1; v[2].re = e2;
+  } else {
+    R a = -M_CBRT(r);
+    v[0].re = s1 + 2*a;
+    v[1].re = s1 - a;
+    v[2].re = s1 - a;
+  }
+}
+
+/* QLA_F_csqrt / QLA_D_csqrt (lib/cmath/QLA_csqrt.c:36-62) */
+static FN(mc) FN(csqrt)(FN(mc) z)
+{
+  R n = M_SQRT(z.re*z.re + z.im*z.im);
+  R r = z.re;
+  R i = z.im;
+  R sr = M_SQRT(M_FABS(0.5*(n+r)));
+  R si = M_COPYSIGN(M_SQRT(M_FABS(0.5*(n-r))), i);
+  FN(mc) c; c.re = sr; c.im = si;
+  return c;
+}
+
+/* QLA_F_cpow / QLA_D_cpow (lib/cmath/QLA_cpow.c:36-58) */
+static FN(mc) FN(cpow)(FN(mc) a, R b)
+{
+  R r = pow(a.re*a.re + a.im*a.im, 0.5*b);
+  R theta = b*M_ATAN2(a.im, a.re);
+  FN(mc) c = FN(cexpi)(theta);
+  c.re = r*c.re; c.im = r*c.im;
+  return c;
+}
+
+/* eigenvalues of a general complex 3x3 matrix via the depressed cubic
+ * (V_eq_eigenvals_M.c:127-186, the branch the template compiles) */
+static void FN(eig3)(FN(mc) *v, const FN(mc) *m)
+{
+  FN(mc) a00 = m[0], a11 = m[4], a22 = m[8], s1, s2, det0, det1, det2, det;
+  s1.re = a00.re + a11.re; s1.im = a00.im + a11.im;
+  s1.re += a22.re; s1.im += a22.im;
+  s1.re = (1./3.)*s1.re; s1.im = (1./3.)*s1.im;
+  a00.re -= s1.re; a00.im -= s1.im;
+  a11.re -= s1.re; a11.im -= s1.im;
+  a22.re -= s1.re; a22.im -= s1.im;
+  CMUL(det2, a00, a11); CMMS(det2, m[1], m[3]);
+  CMUL(det1, m[2], m[3]); CMMS(det1, a00, m[5]);
+  CMUL(det0, m[1], m[5]); CMMS(det0, m[2], a11);
+  CMUL(det, det2, a22);
+  CPMS(det, det1, m[7]);
+  CPMS(det, det0, m[6]);
+  s2 = det2;
+  CPMS(s2, a00, a22);
+  CMMS(s2, m[2], m[6]);
+  CPMS(s2, a11, a22);
+  CMMS(s2, m[5], m[7]);
+  FN(mc) p, q, p2, q2, t, d, w0, w, pw0, e0, e1, e2;
+  p.re = (1./3.)*s2.re; p.im = (1./3.)*s2.im;
+  q.re = (-0.5)*det.re; q.im = (-0.5)*det.im;
+  CMUL(p2, p, p);
+  CMUL(q2, q, q);
+  d.re = p.re*p2.re - p.im*p2.im + q2.re;                /* QLA_c_eq_c_times_c_plus_c */
+  d.im = p.re*p2.im + p.im*p2.re + q2.im;
+  t = FN(csqrt)(d);
+  R ts = q.re*t.re + q.im*t.im;                         /* QLA_r_eq_Re_ca_times_c */
+  if (ts >= 0) { q.re += t.re; q.im += t.im; }
+  else { q.re -= t.re; q.im -= t.im; }
+  w0 = FN(cpow)(q, 1./3.);
+  w.re = -0.5; w.im = 0.86602540378443864676;
+  {                                                    /* safedivC(&pw0, &p, &w0, 0) */
+    R dd = w0.re*w0.re + w0.im*w0.im;
+    if (dd == 0) {
+      pw0.re = 0; pw0.im = 0.;
+    } else {
+      R di = 1/dd;
+      pw0.re = p.re*w0.re + p.im*w0.im;
+      pw0.im = p.im*w0.re - p.re*w0.im;
+      pw0.re = di*pw0.re; pw0.im = di*pw0.im;
+    }
+  }
+  e0.re = pw0.re - w0.re; e0.im = pw0.im - w0.im;
+  v[0].re = s1.re + e0.re; v[0].im = s1.im + e0.im;
+  e1.re = w.re*pw0.re + w.im*pw0.im;                   /* conj(w) * pw0 */
+  e1.im = w.re*pw0.im - w.im*pw0.re;
+  CMMS(e1, w, w0);
+  v[1].re = s1.re + e1.re; v[1].im = s1.im + e1.im;
+  CMUL(e2, w, pw0);
+  e2.re -= w.re*w0.re + w.im*w0.im;                    /* -= conj(w) * w0 */
+  e2.im -= w.re*w0.im - w.im*w0.re;
+  v[2].re = s1.re + e2.re; v[2].im = s1.im + e2.im;
+}
+
+/* x = a^-1 b for b with nb columns (a ColorVector: nb = 1; a ColorMatrix:
+ * nb = nc): V_eq_M_inverse_V.c:84-126 for nc = 3 and nb = 1 (Cramer's
+ * rule), else Gauss-Jordan (V_eq_M_inverse_V.c:128-168, M_eq_M_inverse_M.c:85-135) */
+static void FN(minv1)(FN(mc) *x, const FN(mc) *a, const FN(mc) *b, int nc, int nb)
+{
+  if (nc == 3 && nb == 1) {
+    FN(mc) det0, det1, det2, det, idet, r0, r1, r2;
+    CMUL(det2, a[0], a[4]); CMMS(det2, a[1], a[3]);
+    CMUL(det1, a[2], a[3]); CMMS(det1, a[0], a[5]);
+    CMUL(det0, a[1], a[5]); CMMS(det0, a[2], a[4]);
+    CMUL(det, det2, a[8]);
+    CPMS(det, det1, a[7]);
+    CPMS(det, det0, a[6]);
+    {
+      R t = 1 / (det.re * det.re + det.im * det.im);
+      idet.re = t * det.re;
+      idet.im = -t * det.im;
+    }
+#define SETV(rr, j0, i1, j1, i2, j2) \
+    CMUL(det, a[i1 * 3 + j1], a[i2 * 3 + j2]); CMMS(det, a[i1 * 3 + j2], a[i2 * 3 + j1]); CPMS(rr, det, b[j0]);
+    CMUL(r0, det0, b[2]);
+    SETV(r0, 0, 1, 1, 2, 2);
+    SETV(r0, 1, 2, 1, 0, 2);
+    CMUL(r1, det1, b[2]);
+    SETV(r1, 0, 1, 2, 2, 0);
+    SETV(r1, 1, 2, 2, 0, 0);
+    CMUL(r2, det2, b[2]);
+    SETV(r2, 0, 1, 0, 2, 1);
+    SETV(r2, 1, 2, 0, 0, 1);
+#undef SETV
+    CMUL(x[0], r0, idet);
+    CMUL(x[1], r1, idet);
+    CMUL(x[2], r2, idet);
+    return;
+  }
+  FN(m_eq_m_inverse_m)(x, nc, a, b, nb);
+}
+
 /* ------------------------------------------------------------ v-forms */
-void FN(ora_mfunc)(R *r, const R *a, long n, int nc, int which)
+/* r[i] = f(a[i]); eigenvalue functions write nc complex numbers per site,
+ * det one.  The closed nc = 3 forms exist only for nc == 3; other colour
+ * counts take the templates' generic paths (expA / expTA: the exp path;
+ * sqrtPH / invsqrtPH: the Newton paths).  Returns -1 for an eigenvalue
+ * request at nc != 3 (the QR path is not restated). */
+int FN(ora_mfunc)(R *r, const R *a, long n, int nc, int which)
 {
   const FN(mc) *A = (const FN(mc) *)a;
   FN(mc) *O = (FN(mc) *)r;
   const double eps = sizeof(R) == 4 ? (double)FLT_EPSILON : DBL_EPSILON;
+  if ((which == ORA_MF_EIGENVALS || which == ORA_MF_EIGENVALSH) && nc != 3) return -1;
   for (long i = 0; i < n; i++) {
     const FN(mc) *ai = A + i * nc * nc;
+    FN(mc) *oi = O + i * nc * nc;
     switch (which) {
-    case ORA_MF_EXP: FN(exp1)(O + i * nc * nc, ai, nc); break;
-    case ORA_MF_SQRT: FN(sqrt1)(O + i * nc * nc, ai, nc, eps); break;
-    case ORA_MF_INVERSE: FN(inverse1)(O + i * nc * nc, ai, nc); break;
-    default: FN(det1)(O + i, ai, nc); break;
+    case ORA_MF_EXP: FN(exp1)(oi, ai, nc); break;
+    case ORA_MF_SQRT: FN(sqrt1)(oi, ai, nc, eps); break;
+    case ORA_MF_INVERSE: FN(inverse1)(oi, ai, nc); break;
+    case ORA_MF_DET: FN(det1)(O + i, ai, nc); break;
+    case ORA_MF_INVSQRT: FN(invsqrt1)(oi, ai, nc, eps); break;
+    case ORA_MF_LOG: FN(log1)(oi, ai, nc, eps); break;
+    case ORA_MF_EXPA:
+      if (nc == 3) FN(exp3_ah)(oi, ai, 1); else FN(exp1)(oi, ai, nc);
+      break;
+    case ORA_MF_EXPTA:
+      if (nc == 3) FN(exp3_ah)(oi, ai, 0); else FN(exp1)(oi, ai, nc);
+      break;
+    case ORA_MF_SQRTPH:
+      if (nc == 3) FN(sqrtph3)(oi, ai, 0); else FN(sqrt1)(oi, ai, nc, eps);
+      break;
+    case ORA_MF_INVSQRTPH:
+      if (nc == 3) FN(sqrtph3)(oi, ai, 1); else FN(invsqrt1)(oi, ai, nc, eps);
+      break;
+    case ORA_MF_EIGENVALS: FN(eig3)(O + i * 3, ai); break;
+    case ORA_MF_EIGENVALSH: FN(eigh3)(O + i * 3, ai); break;
+    default: return -1;
     }
+  }
+  return 0;
+}
+
+/* r[i] = a[ia[i]]^-1 b[ib[i]] (index arrays may be NULL); b, r hold nb
+ * columns per site (1: ColorVector, nc: ColorMatrix) */
+void FN(ora_minv)(R *r, const R *a, const R *b, long n, int nc, int nb, const int *ia, const int *ib)
+{
+  const FN(mc) *A = (const FN(mc) *)a, *B = (const FN(mc) *)b;
+  FN(mc) *O = (FN(mc) *)r;
+  for (long i = 0; i < n; i++) {
+    const long ja = ia ? ia[i] : i, jb = ib ? ib[i] : i;
+    FN(minv1)(O + i * nc * nb, A + ja * nc * nc, B + jb * nc * nb, nc, nb);
   }
 }
 

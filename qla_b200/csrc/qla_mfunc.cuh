@@ -109,41 +109,46 @@ struct DetOp {
 };
 
 // ---------------------------------------------------------------------------
-// M_eq_inverse_M (nc = 3)
-template <typename R_>
-struct InverseOp {
-  using R = R_;
-  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
-  __device__ __forceinline__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1],
-                                               const Cx<R> (&)[1], Cx<R> (&x)[9]) {
-    Cx<R> det2 = cmul(a[0], a[4]);
-    cmms(det2, a[1], a[3]);
-    Cx<R> det1 = cmul(a[2], a[3]);
-    cmms(det1, a[0], a[5]);
-    Cx<R> det0 = cmul(a[1], a[5]);
-    cmms(det0, a[2], a[4]);
-    Cx<R> det = cmul(det2, a[8]);
-    cpms(det, det1, a[7]);
-    cpms(det, det0, a[6]);
-    // QLA_c_eq_r_div_c(idet, 1, det): t = 1/|det|^2; idet = t*conj(det)
-    const R t = rdiv(R(1), cnorm2(det));
-    const Cx<R> idet{rmul(t, det.re), rmul(-t, det.im)};
+// M_eq_inverse_M (nc = 3): cofactors times 1/det
+template <typename R>
+__device__ __forceinline__ void inv3(Cx<R> (&x)[9], const Cx<R> (&a)[9]) {
+  Cx<R> det2 = cmul(a[0], a[4]);
+  cmms(det2, a[1], a[3]);
+  Cx<R> det1 = cmul(a[2], a[3]);
+  cmms(det1, a[0], a[5]);
+  Cx<R> det0 = cmul(a[1], a[5]);
+  cmms(det0, a[2], a[4]);
+  Cx<R> det = cmul(det2, a[8]);
+  cpms(det, det1, a[7]);
+  cpms(det, det0, a[6]);
+  // QLA_c_eq_r_div_c(idet, 1, det): t = 1/|det|^2; idet = t*conj(det)
+  const R t = rdiv(R(1), cnorm2(det));
+  const Cx<R> idet{rmul(t, det.re), rmul(-t, det.im)};
 #define QLAB_SET(i0, j0, i1, j1, i2, j2)              \
   {                                                   \
     Cx<R> d_ = cmul(a[i1 * 3 + j1], a[i2 * 3 + j2]);  \
     cmms(d_, a[i1 * 3 + j2], a[i2 * 3 + j1]);         \
     x[i0 * 3 + j0] = cmul(d_, idet);                  \
   }
-    QLAB_SET(0, 0, 1, 1, 2, 2);
-    QLAB_SET(0, 1, 2, 1, 0, 2);
-    x[2] = cmul(det0, idet);
-    QLAB_SET(1, 0, 1, 2, 2, 0);
-    QLAB_SET(1, 1, 2, 2, 0, 0);
-    x[5] = cmul(det1, idet);
-    QLAB_SET(2, 0, 1, 0, 2, 1);
-    QLAB_SET(2, 1, 2, 0, 0, 1);
-    x[8] = cmul(det2, idet);
+  QLAB_SET(0, 0, 1, 1, 2, 2);
+  QLAB_SET(0, 1, 2, 1, 0, 2);
+  x[2] = cmul(det0, idet);
+  QLAB_SET(1, 0, 1, 2, 2, 0);
+  QLAB_SET(1, 1, 2, 2, 0, 0);
+  x[5] = cmul(det1, idet);
+  QLAB_SET(2, 0, 1, 0, 2, 1);
+  QLAB_SET(2, 1, 2, 0, 0, 1);
+  x[8] = cmul(det2, idet);
 #undef QLAB_SET
+}
+
+template <typename R_>
+struct InverseOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1],
+                                               const Cx<R> (&)[1], Cx<R> (&x)[9]) {
+    inv3(x, a);
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                double*) {}
@@ -151,17 +156,19 @@ struct InverseOp {
 };
 
 // ---------------------------------------------------------------------------
-// x = a^-1 b, Gauss-Jordan with partial pivoting (M_eq_M_inverse_M.c:108-135),
-// FP64, rows swapped physically (same arithmetic as the template's row
-// permutation).  Result written into d (in place of the right-hand side).
-__device__ __forceinline__ void gj_solve3(Cx<double> (&c)[9], Cx<double> (&d)[9]) {
+// x = a^-1 b, Gauss-Jordan with partial pivoting (M_eq_M_inverse_M.c:108-135)
+// for NB right-hand-side columns, rows swapped physically (same arithmetic
+// as the template's row permutation).  Result written into d (in place of
+// the right-hand side).
+template <typename R, int NB = 3>
+__device__ __forceinline__ void gj_solve3(Cx<R> (&c)[9], Cx<R> (&d)[3 * NB]) {
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    double rmax = cnorm2(c[k * 3 + k]);
+    R rmax = cnorm2(c[k * 3 + k]);
     int imax = k;
 #pragma unroll
     for (int i = k + 1; i < 3; i++) {
-      const double rr = cnorm2(c[i * 3 + k]);
+      const R rr = cnorm2(c[i * 3 + k]);
       if (rr > rmax) {
         rmax = rr;
         imax = i;
@@ -172,32 +179,84 @@ __device__ __forceinline__ void gj_solve3(Cx<double> (&c)[9], Cx<double> (&d)[9]
       if (imax == i) {
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-          Cx<double> t = c[k * 3 + j];
+          const Cx<R> t = c[k * 3 + j];
           c[k * 3 + j] = c[i * 3 + j];
           c[i * 3 + j] = t;
-          t = d[k * 3 + j];
-          d[k * 3 + j] = d[i * 3 + j];
-          d[i * 3 + j] = t;
+        }
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+          const Cx<R> t = d[k * NB + j];
+          d[k * NB + j] = d[i * NB + j];
+          d[i * NB + j] = t;
         }
       }
     }
-    rmax = __ddiv_rn(1.0, rmax);
-    const Cx<double> s{__dmul_rn(rmax, c[k * 3 + k].re), -__dmul_rn(rmax, c[k * 3 + k].im)};
+    rmax = rdiv(R(1), rmax);
+    const Cx<R> s{rmul(rmax, c[k * 3 + k].re), -rmul(rmax, c[k * 3 + k].im)};
     c[k * 3 + k] = s;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
       if (i == k) continue;
-      const Cx<double> t = cmul(s, c[i * 3 + k]);
+      const Cx<R> t = cmul(s, c[i * 3 + k]);
 #pragma unroll
       for (int j = k + 1; j < 3; j++) cmms(c[i * 3 + j], t, c[k * 3 + j]);
 #pragma unroll
-      for (int j = 0; j < 3; j++) cmms(d[i * 3 + j], t, d[k * 3 + j]);
+      for (int j = 0; j < NB; j++) cmms(d[i * NB + j], t, d[k * NB + j]);
     }
   }
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
-    for (int j = 0; j < 3; j++) d[i * 3 + j] = cmul(c[i * 3 + i], d[i * 3 + j]);
+    for (int j = 0; j < NB; j++) d[i * NB + j] = cmul(c[i * 3 + i], d[i * NB + j]);
+}
+
+// Newton loop of M_eq_sqrt_M.c:158-171 / M_eq_invsqrt_M.c:160-173 in FP64:
+// e <- -1/2 e x^-1 e, x += e until |e|_F^2 <= DBL_EPSILON or 20 iterations.
+__device__ __forceinline__ void newton_sqrt3(Cx<double> (&x)[9], Cx<double> (&e)[9]) {
+  const double eps = 2.220446049250313080847e-16;  // DBL_EPSILON
+  Cx<double> c[9], d[9];
+  int nit = 0;
+  double enorm;
+  do {
+    nit++;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      c[k] = x[k];
+      d[k] = e[k];
+    }
+    gj_solve3(c, d);    // d = x^-1 e
+    mat3_mul(c, e, d);  // c = e x^-1 e
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      e[k] = Cx<double>{__dmul_rn(-0.5, c[k].re), __dmul_rn(-0.5, c[k].im)};
+      x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
+    }
+    enorm = fnorm2_3(e);
+  } while (nit < 20 && enorm > eps);
+}
+
+// M_eq_sqrt_M (QLA_D3 arithmetic): r = sqrt(a)
+__device__ __forceinline__ void sqrt3_fp64(Cx<double> (&r)[9], const Cx<double> (&a)[9]) {
+  double ds = fnorm2_3(a);
+  if (ds == 0.0) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) r[k] = Cx<double>{0.0, 0.0};
+    return;
+  }
+  ds = __dsqrt_rn(ds);
+  Cx<double> x[9], e[9];
+  const double inv = __ddiv_rn(1.0, ds);
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    x[k] = Cx<double>{__dmul_rn(inv, a[k].re), __dmul_rn(inv, a[k].im)};  // x = a / ds
+    const double dg = (k % 4 == 0) ? 0.5 : 0.0;                          // e = 0.5 1
+    e[k] = Cx<double>{__dadd_rn(dg, __dmul_rn(-0.5, x[k].re)), __dadd_rn(0.0, __dmul_rn(-0.5, x[k].im))};
+    x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
+  }
+  newton_sqrt3(x, e);
+  const double sds = __dsqrt_rn(ds);
+#pragma unroll
+  for (int k = 0; k < 9; k++) r[k] = Cx<double>{__dmul_rn(sds, x[k].re), __dmul_rn(sds, x[k].im)};
 }
 
 // M_eq_sqrt_M (Newton), FP64
@@ -205,50 +264,14 @@ template <typename R_>
 struct SqrtOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
-  __device__ static void apply(const SiteParams& p, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+  __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                Cx<R> (&r)[9]) {
-    Cx<double> ad[9];
+    Cx<double> ad[9], rd[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) ad[k] = cd(a[k]);
-    double ds = fnorm2_3(ad);
-    if (ds == 0.0) {
+    sqrt3_fp64(rd, ad);
 #pragma unroll
-      for (int k = 0; k < 9; k++) r[k] = Cx<R>{R(0), R(0)};
-      return;
-    }
-    ds = __dsqrt_rn(ds);
-    Cx<double> x[9], e[9], c[9], d[9];
-    const double inv = __ddiv_rn(1.0, ds);
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      x[k] = Cx<double>{__dmul_rn(inv, ad[k].re), __dmul_rn(inv, ad[k].im)};  // x = a / ds
-      const double dg = (k % 4 == 0) ? 0.5 : 0.0;                            // e = 0.5 1
-      e[k] = Cx<double>{__dadd_rn(dg, __dmul_rn(-0.5, x[k].re)), __dadd_rn(0.0, __dmul_rn(-0.5, x[k].im))};
-      x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
-    }
-    const double eps = 2.220446049250313080847e-16;  // DBL_EPSILON
-    int nit = 0;
-    double enorm;
-    do {
-      nit++;
-#pragma unroll
-      for (int k = 0; k < 9; k++) {
-        c[k] = x[k];
-        d[k] = e[k];
-      }
-      gj_solve3(c, d);  // d = x^-1 e
-      mat3_mul(c, e, d);  // c = e x^-1 e
-#pragma unroll
-      for (int k = 0; k < 9; k++) {
-        e[k] = Cx<double>{__dmul_rn(-0.5, c[k].re), __dmul_rn(-0.5, c[k].im)};
-        x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
-      }
-      enorm = fnorm2_3(e);
-    } while (nit < 20 && enorm > eps);
-    const double sds = __dsqrt_rn(ds);
-#pragma unroll
-    for (int k = 0; k < 9; k++) r[k] = cround<R>(Cx<double>{__dmul_rn(sds, x[k].re), __dmul_rn(sds, x[k].im)});
-    (void)p;
+    for (int k = 0; k < 9; k++) r[k] = cround<R>(rd[k]);
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                double*) {}

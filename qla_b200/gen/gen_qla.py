@@ -59,7 +59,18 @@ CITE = {
     "mfunc": "lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, "
              "M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143",
 }
+CITE["mfunc_ext"] = ("lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/"
+                     "M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, "
+                     "M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, "
+                     "V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166")
+CITE["minv"] = ("lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), "
+                "code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135")
 MFUNC_OPS = {"exp": "ExpOp", "sqrt": "SqrtOp", "inverse": "InverseOp"}
+# the remaining matrix functions: name -> OP template (R substituted)
+MFUNC_EXT_OPS = {"invsqrt": "InvsqrtOp<{R}>", "log": "LogOp<{R}>", "expA": "ExpAHOp<{R}, true>",
+                 "expTA": "ExpAHOp<{R}, false>", "sqrtPH": "SqrtPHOp<{R}, false>",
+                 "invsqrtPH": "SqrtPHOp<{R}, true>"}
+EIGEN_OPS = {"eigenvals": "EigenvalsOp<{R}>", "eigenvalsH": "EigenvalsHOp<{R}>"}
 CITE["int"] = "lib/perl/build_qla.pl:1932-2082 (integer fields)"
 # QLA_I_ binary operators offered with veq/xeq only (build_qla.pl:1932-2082)
 INT_BINOPS = {"and": "IC_AND", "divide": "IC_DIVIDE", "eq": "IC_EQ", "ge": "IC_GE", "gt": "IC_GT", "le": "IC_LE",
@@ -502,6 +513,35 @@ def gen_pc(pc, R, P):
                     f"qlab::EQ);")
             fns.append(Fn(name, params, body, "mfunc", CITE["mfunc"], dict(dest="C", eqop="eq", var=var, a=src,
                                                                             fn="det")))
+    # ---- the remaining matrix functions and the eigenvalues
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        tail = [("int *", "index")] if var == "x" else []
+        for src, p1 in [("M", False), ("pM", True)]:
+            pa, oa = operand(pc, "M", p1, "a")
+            for dest, table in (("M", MFUNC_EXT_OPS), ("V", EIGEN_OPS)):
+                for fname, opt in table.items():
+                    name = f"QLA_{pc}_{dest}_{var}eq_{fname}_{src}"
+                    params = [(f"{ptype(pc, dest)} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                    body = (f"qlab::api_map<qlab::{opt.format(R=R)}>({kid('mfunc_' + fname)}, r, {oa}, "
+                            f"qlab::Opnd{{}}, {gang}, n, qlab::EQ);")
+                    fns.append(Fn(name, params, body, "mfunc_ext", CITE["mfunc_ext"],
+                                  dict(dest=dest, eqop="eq", var=var, a=src, fn=fname)))
+    # ---- a^-1 b for a ColorVector or ColorMatrix b
+    for T, nb in (("V", 1), ("M", 3)):
+        for var in ["v", "x"]:
+            gang = "index" if var == "x" else "nullptr"
+            tail = [("int *", "index")] if var == "x" else []
+            for s1, p1 in [("M", False), ("pM", True)]:
+                for s2, p2 in [(T, False), ("p" + T, True)]:
+                    name = f"QLA_{pc}_{T}_{var}eq_{s1}_inverse_{s2}"
+                    pa, oa = operand(pc, "M", p1, "a")
+                    pb, ob = operand(pc, T, p2, "b")
+                    params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                    body = (f"qlab::api_map<qlab::MInverseOp<{R}, {nb}>>({kid('minv_' + T)}, r, {oa}, {ob}, "
+                            f"{gang}, n, qlab::EQ);")
+                    fns.append(Fn(name, params, body, "mfunc_ext", CITE["minv"],
+                                  dict(dest=T, eqop="eq", var=var, a=s1, b=s2, fn="inverse_" + T)))
     # ---- global reductions
     red_pcs = [(pc, R, P)]
     if pc == "F3":
@@ -625,6 +665,7 @@ def main():
         written += write_if_changed(os.path.join(OUT_INC, fname), text)
     for (pc, family), fns in groups.items():
         extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n',
+                 "mfunc_ext": '#include "../qla_mfunc_ext.cuh"\n',
                  "multi": '#include <vector>\n#include "../qla_multi.cuh"\n',
                  "prop": '#include "../qla_prop.cuh"\n'}.get(family, "")
         if pc == "FN" and family == "mfunc":

@@ -236,6 +236,22 @@ def build(pc, dt, seed):
                 call(f"QLA_{rpc}_c_veq_V_dot_V", nc, ctypes.c_void_p(o.ctypes.data), ctypes.c_void_p(vv.ctypes.data),
                      ctypes.c_void_p(vrev.ctypes.data), N)
                 out[f"QLA_{rpc}_c_veq_V_dot_V|{nc}"] = o
+    # the remaining matrix functions (code templates) and a^-1 b
+    ins["mf_aht"] = T.from_complex(T.to_complex(ins["mf_exp"].astype(np.float64))
+                                   + 1j * rng.uniform(-2, 2, N)[:, None, None] * np.eye(3), dt)
+    ins["mf_herm"] = T.hermitian_inputs(rng, N, dt)
+    for fname, src in (("M_veq_invsqrt_M", "mf_pos"), ("M_veq_log_M", "mf_pos"), ("M_veq_log_M", "mf_gen"),
+                       ("M_veq_expTA_M", "mf_exp"), ("M_veq_expA_M", "mf_aht"), ("M_veq_sqrtPH_M", "mf_pos"),
+                       ("M_veq_invsqrtPH_M", "mf_pos"), ("V_veq_eigenvalsH_M", "mf_herm"),
+                       ("V_veq_eigenvals_M", "mf_gen")):
+        r = np.zeros((N, 6 if fname.startswith("V") else 18), dtype=dt)
+        call(f"QLA_{pc}_{fname}", ctypes.c_void_p(r.ctypes.data), ctypes.c_void_p(ins[src].ctypes.data), N)
+        out[f"QLA_{pc}_{fname}|{src}"] = r
+    for dest in ("V", "M"):
+        r = np.zeros((N, 6 if dest == "V" else 18), dtype=dt)
+        call(f"QLA_{pc}_{dest}_veq_M_inverse_{dest}", ctypes.c_void_p(r.ctypes.data),
+             ctypes.c_void_p(ins["mf_gen"].ctypes.data), ctypes.c_void_p(ins["r0" + dest].ctypes.data), N)
+        out[f"QLA_{pc}_{dest}_veq_M_inverse_{dest}|mf_gen|r0{dest}"] = r
     return ins, out
 
 

@@ -205,7 +205,8 @@ def bits_equal(a, b):
 # ---------------------------------------------------------------------------
 # matrix-function inputs (config 5) and oracle wrapper
 
-MF = {"exp": 0, "sqrt": 1, "inverse": 2, "det": 3}
+MF = {"exp": 0, "sqrt": 1, "inverse": 2, "det": 3, "invsqrt": 4, "log": 5, "expA": 6, "expTA": 7, "sqrtPH": 8,
+      "invsqrtPH": 9, "eigenvals": 10, "eigenvalsH": 11}
 
 
 def to_complex(m, nc=3):
@@ -245,10 +246,27 @@ def positive_hermitian_inputs(rng, n, dtype, nc=3):
 
 def ora_mfunc(a, n, which, nc=3):
     f = getattr(oracle(), "ora_mfunc_" + rtype(a.dtype))
-    nout = 1 if which == "det" else nc * nc
+    nout = 1 if which == "det" else nc if which.startswith("eigen") else nc * nc
     r = np.zeros((n, 2 * nout), dtype=a.dtype)
-    f(ptr(r), ptr(a), ctypes.c_long(n), nc, MF[which])
+    rc = f(ptr(r), ptr(a), ctypes.c_long(n), nc, MF[which])
+    if rc != 0:
+        raise ValueError(f"oracle has no {which} at nc={nc}")
     return r
+
+
+def ora_minv(a, b, n, nb, nc=3, idx_a=None, idx_b=None):
+    """r = a^-1 b per site (nb = 1: ColorVector b, nb = nc: ColorMatrix b)."""
+    f = getattr(oracle(), "ora_minv_" + rtype(a.dtype))
+    r = np.zeros((n, 2 * nc * nb), dtype=a.dtype)
+    idx_a, idx_b = _i32(idx_a), _i32(idx_b)
+    f(ptr(r), ptr(a), ptr(b), ctypes.c_long(n), nc, nb, ptr(idx_a), ptr(idx_b))
+    return r
+
+
+def hermitian_inputs(rng, n, dtype, nc=3):
+    """(G + G^+)/2 with G complex Gaussian: real spectrum of both signs."""
+    g = rng.standard_normal((n, nc, nc)) + 1j * rng.standard_normal((n, nc, nc))
+    return from_complex(0.5 * (g + np.conj(np.transpose(g, (0, 2, 1)))), dtype)
 
 
 # ---------------------------------------------------------------------------
