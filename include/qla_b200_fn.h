@@ -1271,6 +1271,24 @@ void QLA_FN_M_veq_sqrt_M(int nc, void * r, void * a, int n);
 void QLA_FN_M_veq_inverse_M(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_C_veq_det_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_FN_C_veq_det_M(int nc, QLA_F_Complex * r, void * a, int n);
+/* ---- mfunc_ext: replaces the FN functions emitted by lib/perl/build_qla.pl:1022-1061 (matrix functions */
+/* replaces QLA_FN_M_veq_invsqrt_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_invsqrt_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_log_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_log_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_expA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_expA_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_expTA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_expTA_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_sqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_sqrtPH_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_invsqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_invsqrtPH_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_V_veq_eigenvals_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_veq_eigenvals_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_V_veq_eigenvalsH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_veq_eigenvalsH_M(int nc, void * r, void * a, int n);
+/* ---- mfunc: replaces the FN functions emitted by lib/perl/build_qla.pl:1000-1060 (matrix functions) */
 /* replaces QLA_FN_M_veq_exp_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_FN_M_veq_exp_pM(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_M_veq_sqrt_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
@@ -1279,6 +1297,39 @@ void QLA_FN_M_veq_sqrt_pM(int nc, void * r, void * a, int n);
 void QLA_FN_M_veq_inverse_pM(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_C_veq_det_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_FN_C_veq_det_pM(int nc, QLA_F_Complex * r, void * a, int n);
+/* ---- mfunc_ext: replaces the FN functions emitted by lib/perl/build_qla.pl:1022-1061 (matrix functions */
+/* replaces QLA_FN_M_veq_invsqrt_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_invsqrt_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_log_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_log_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_expA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_expA_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_expTA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_expTA_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_sqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_sqrtPH_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_M_veq_invsqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_veq_invsqrtPH_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_V_veq_eigenvals_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_veq_eigenvals_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_V_veq_eigenvalsH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_veq_eigenvalsH_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FN_V_veq_M_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_veq_M_inverse_V(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_V_veq_M_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_veq_M_inverse_pV(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_V_veq_pM_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_veq_pM_inverse_V(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_V_veq_pM_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_veq_pM_inverse_pV(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_M_veq_M_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_veq_M_inverse_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_M_veq_M_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_veq_M_inverse_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_M_veq_pM_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_veq_pM_inverse_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_FN_M_veq_pM_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_veq_pM_inverse_pM(int nc, void * r, void * a, void * b, int n);
 /* ---- spproj: replaces the FN functions emitted by lib/perl/build_qla.pl:1087-1110 */
 /* replaces QLA_FN_H_xeq_spproj_D (lib/perl/build_qla.pl:1087-1110, make_code_unary.pl:183-241, expressions_gamma.pl:244-275) */
 void QLA_FN_H_xeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n);
@@ -1328,6 +1379,24 @@ void QLA_FN_M_xeq_sqrt_M(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_M_xeq_inverse_M(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_C_xeq_det_M (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_FN_C_xeq_det_M(int nc, QLA_F_Complex * r, void * a, int * index, int n);
+/* ---- mfunc_ext: replaces the FN functions emitted by lib/perl/build_qla.pl:1022-1061 (matrix functions */
+/* replaces QLA_FN_M_xeq_invsqrt_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_invsqrt_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_log_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_log_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_expA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_expA_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_expTA_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_expTA_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_sqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_sqrtPH_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_invsqrtPH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_invsqrtPH_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_V_xeq_eigenvals_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_xeq_eigenvals_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_V_xeq_eigenvalsH_M (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_xeq_eigenvalsH_M(int nc, void * r, void * a, int * index, int n);
+/* ---- mfunc: replaces the FN functions emitted by lib/perl/build_qla.pl:1000-1060 (matrix functions) */
 /* replaces QLA_FN_M_xeq_exp_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_FN_M_xeq_exp_pM(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_M_xeq_sqrt_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
@@ -1336,6 +1405,39 @@ void QLA_FN_M_xeq_sqrt_pM(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_M_xeq_inverse_pM(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_C_xeq_det_pM (lib/perl/build_qla.pl:1000-1060 (matrix functions), code-templates/M_eq_exp_M.c:243-367, M_eq_sqrt_M.c:73-181, M_eq_inverse_M.c:50-162, C_eq_det_M.c:50-143) */
 void QLA_FN_C_xeq_det_pM(int nc, QLA_F_Complex * r, void * a, int * index, int n);
+/* ---- mfunc_ext: replaces the FN functions emitted by lib/perl/build_qla.pl:1022-1061 (matrix functions */
+/* replaces QLA_FN_M_xeq_invsqrt_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_invsqrt_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_log_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_log_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_expA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_expA_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_expTA_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_expTA_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_sqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_sqrtPH_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_M_xeq_invsqrtPH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_M_xeq_invsqrtPH_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_V_xeq_eigenvals_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_xeq_eigenvals_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_V_xeq_eigenvalsH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
+void QLA_FN_V_xeq_eigenvalsH_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FN_V_xeq_M_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_xeq_M_inverse_V(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_V_xeq_M_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_xeq_M_inverse_pV(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_V_xeq_pM_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_xeq_pM_inverse_V(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_V_xeq_pM_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_V_xeq_pM_inverse_pV(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_M_xeq_M_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_xeq_M_inverse_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_M_xeq_M_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_xeq_M_inverse_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_M_xeq_pM_inverse_M (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_xeq_pM_inverse_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_FN_M_xeq_pM_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
+void QLA_FN_M_xeq_pM_inverse_pM(int nc, void * r, void * a, void * b, int * index, int n);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,16 @@ INT_BINOPS = {"and": "IC_AND", "divide": "IC_DIVIDE", "eq": "IC_EQ", "ge": "IC_G
 
 FN_NCS = [2, 3, 4, 8]          # colour counts with compiled QLA_FN_ kernels
 FN_MFUNC_NCS = [3, 4, 8]       # nc = 1, 2 use complex libm closed forms in the reference
+# remaining matrix functions for QLA_FN_: nc -> OP (closed forms at nc = 3,
+# the templates' generic exp / Newton paths otherwise)
+FN_MFUNC_EXT = {
+    "invsqrt": lambda nc: f"GenMfuncExtOp<float, {nc}, 0>",
+    "log": lambda nc: f"GenMfuncExtOp<float, {nc}, 1>",
+    "expA": lambda nc: "ExpAHOp<float, true>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 2>",
+    "expTA": lambda nc: "ExpAHOp<float, false>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 2>",
+    "sqrtPH": lambda nc: "SqrtPHOp<float, false>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 3>",
+    "invsqrtPH": lambda nc: "SqrtPHOp<float, true>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 4>",
+}
 
 
 def _fn_switch(ncs, call_of_nc, name):
@@ -208,6 +218,34 @@ def gen_fn():
             add(name, [("QLA_F_Complex *", "r"), ("void *", "a")] + tail + [("int", "n")],
                 _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
                 dict(dest="C", eqop="eq", var=var, a=src, fn="det"))
+            # the remaining matrix functions: the Nc = 3 closed forms at nc = 3,
+            # the templates' generic paths otherwise
+            for fname, opf in FN_MFUNC_EXT.items():
+                name = f"QLA_FN_M_{var}eq_{fname}_{src}"
+                call = lambda nc, opf=opf, p1=p1, gang=gang: (
+                    f"qlab::api_map<qlab::{opf(nc)}>({kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
+                    f"{gang}, n, qlab::EQ);")
+                add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
+                    _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["mfunc_ext"],
+                    dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
+            for fname, opn in (("eigenvals", "EigenvalsOp"), ("eigenvalsH", "EigenvalsHOp")):
+                name = f"QLA_FN_V_{var}eq_{fname}_{src}"
+                call = lambda nc, opn=opn, p1=p1, gang=gang: (
+                    f"qlab::api_map<qlab::{opn}<{R}>>({kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
+                    f"{gang}, n, qlab::EQ);")
+                add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
+                    _fn_switch([3], call, name), "mfunc_ext", CITE["mfunc_ext"],
+                    dict(dest="V", eqop="eq", var=var, a=src, fn=fname))
+        for T_ in ("V", "M"):
+            for s1, p1 in (("M", False), ("pM", True)):
+                for s2, p2 in ((T_, False), ("p" + T_, True)):
+                    name = f"QLA_FN_{T_}_{var}eq_{s1}_inverse_{s2}"
+                    call = lambda nc, T_=T_, p1=p1, p2=p2, gang=gang: (
+                        f"qlab::api_map<qlab::GenMInverseOp<{R}, {nc}, {1 if T_ == 'V' else nc}>>({kid('minv')}, r, "
+                        f"{opnd(p1, 'a')}, {opnd(p2, 'b')}, {gang}, n, qlab::EQ);")
+                    add(name, [("void *", "r"), ("void *", "a"), ("void *", "b")] + tail + [("int", "n")],
+                        _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["minv"],
+                        dict(dest=T_, eqop="eq", var=var, a=s1, b=s2, fn="inverse_" + T_))
     return fns
 
 
@@ -670,6 +708,8 @@ def main():
                  "prop": '#include "../qla_prop.cuh"\n'}.get(family, "")
         if pc == "FN" and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
+        if pc == "FN" and family == "mfunc_ext":
+            extra = '#include "../qla_mfunc_generic_ext.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:
             text += "QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  " + fn.body + "\n}\n\n"

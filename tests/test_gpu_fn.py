@@ -115,6 +115,50 @@ def test_fn_matrix_functions_bit_exact(qla, nc):
         assert T.bits_equal(T.to_host(r_d), T.ora_mfunc(src, n, fname, nc=nc)), (nc, fname)
 
 
+@pytest.mark.parametrize("nc", [3, 4, 8])
+def test_fn_remaining_matrix_functions(qla, nc):
+    """invsqrt, log, M^-1 V and M^-1 M take the templates' generic paths in
+    float at every nc: bit-identical (log up to the host libm's log of
+    |A|_F on the diagonal).  expA / expTA / sqrtPH / invsqrtPH take the exp and
+    Newton paths at nc != 3 (bit-identical) and the FP64 closed forms at
+    nc = 3 (the F3 tolerance: FP32 test rule against the FP64 value of the
+    promoted input); eigenvalues exist at nc = 3."""
+    rng = np.random.default_rng(80 + nc)
+    n = 2053 if nc < 8 else 521
+    gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(np.float32)
+    pos = T.positive_hermitian_inputs(rng, n, np.float32, nc=nc)
+    z = T.to_complex(gen.astype(np.float64), nc)
+    ah = T.from_complex(0.5 * (z - np.conj(np.transpose(z, (0, 2, 1)))), np.float32)
+    cases = [("invsqrt", pos), ("log", pos), ("expA", ah), ("expTA", ah), ("sqrtPH", pos), ("invsqrtPH", pos)]
+    if nc == 3:
+        cases += [("eigenvalsH", pos), ("eigenvals", gen)]
+    for fname, src in cases:
+        nout = nc if fname.startswith("eigen") else nc * nc
+        dest = "V" if fname.startswith("eigen") else "M"
+        r_d = T.to_dev(np.zeros((n, 2 * nout), np.float32))
+        qla.FN.__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
+        got = T.to_host(r_d)
+        closed = nc == 3 and fname not in ("invsqrt", "log")
+        if closed:
+            want = T.ora_mfunc(src.astype(np.float64), n, fname, nc=nc)
+            ok, nbad = T.qla_close(got, want, np.float32)
+            assert ok, (nc, fname, nbad)
+        elif fname == "log":
+            want = T.ora_mfunc(src, n, fname, nc=nc)
+            ok, nbad = T.qla_close(got, want, np.float32, nabs=2, nrel=2)
+            assert ok, (nc, fname, nbad)
+            assert np.mean(np.all(got == want, axis=1)) > 0.99
+        else:
+            assert T.bits_equal(got, T.ora_mfunc(src, n, fname, nc=nc)), (nc, fname)
+    for t, nb in (("V", 1), ("M", nc)):
+        b = rng.standard_normal((n, 2 * nc * nb)).astype(np.float32)
+        ib = rng.permutation(n).astype(np.int32)
+        r_d = T.to_dev(np.zeros((n, 2 * nc * nb), np.float32))
+        b_d = T.to_dev(b)
+        qla.FN.__getattr__(f"{t}_veq_M_inverse_p{t}")(nc, r_d, T.to_dev(gen), T.ptr_array(b_d, ib, 8 * nc * nb), n)
+        assert T.bits_equal(T.to_host(r_d), T.ora_minv(gen, b, n, nb, nc=nc, idx_b=ib)), (nc, t)
+
+
 def test_fn_unsupported_nc_reports_error(qla):
     qla.clear_error()
     qla.lib().QLA_FN_V_veq_M_times_V(5, None, None, None, 10)
