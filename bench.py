@@ -595,31 +595,75 @@ def run_workload(args):
                     "hbm_frac": rate_b * (72 * 3 + 24 * 2 + 4) / 1e9 / peak,
                     "bytes_per_site": "U 72 + U2 gather 72 + nbr 4 + V 24 + R 72 + W 24 = 268"})
     elif args.workload == "mfunc":
+        # every colour-matrix function of the code templates on 32^3x64
+        # sites; the reference library (host cores, OpenMP) on a 32,768-site
+        # sample of the same inputs beside it
         n = 32 * 32 * 32 * 64
+        ns = 32768
         res = {}
+        lib_cpu, cpu_kind = cpu_reference_lib()
+        threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        eye = torch.eye(3, device="cuda", dtype=torch.complex128)
+
+        def as_field(z, dt):
+            return torch.view_as_real(z.reshape(n, 9)).reshape(n, 18).to(dt).contiguous()
+
         for pc, dt in (("F3", torch.float32), ("D3", torch.float64)):
-            a = torch.randn(n, 18, device="cuda", dtype=dt) * 0.5
-            r = torch.empty(n, 18, device="cuda", dtype=dt)
-            c = torch.empty(n, 2, device="cuda", dtype=dt)
+            g = torch.randn(n, 3, 3, device="cuda", dtype=torch.complex128) * 0.5
+            gh = g.conj().transpose(1, 2)
+            ins = {"gen": as_field(g, dt), "pos": as_field(gh @ g + 0.1 * eye, dt),
+                   "ah": as_field(0.5 * (g - gh), dt), "herm": as_field(0.5 * (g + gh), dt)}
+            tl = 0.5 * (g - gh)
+            tl = tl - (torch.diagonal(tl, dim1=1, dim2=2).sum(-1) / 3)[:, None, None] * eye
+            ins["ahtl"] = as_field(tl, dt)
+            del g, gh, tl
+            bv = torch.randn(n, 6, device="cuda", dtype=dt)
             e = 4 if pc == "F3" else 8
-            for fname, f, outt, nb in (("exp", getattr(L, f"QLA_{pc}_M_veq_exp_M"), r, 36),
-                                       ("sqrt", getattr(L, f"QLA_{pc}_M_veq_sqrt_M"), r, 36),
-                                       ("inverse", getattr(L, f"QLA_{pc}_M_veq_inverse_M"), r, 36),
-                                       ("det", getattr(L, f"QLA_{pc}_C_veq_det_M"), c, 20)):
-                src = a
-                if fname == "sqrt":
-                    z = torch.complex(a[:, 0::2].double(), a[:, 1::2].double()).reshape(n, 3, 3)
-                    h = z.conj().transpose(1, 2) @ z + 0.1 * torch.eye(3, device="cuda", dtype=torch.complex128)
-                    src = torch.view_as_real(h.reshape(n, 9)).reshape(n, 18).to(dt).contiguous()
-                    del z, h
-                ms = _events_time(torch, stream, lambda: f(V(outt), V(src), n), reps)
-                res[f"{pc}_{fname}"] = {"site_updates_per_s": n / (ms / 1e3), "us": 1e3 * ms,
-                                        "gbs": nb * e * n / (ms / 1e3) / 1e9}
+            rM = torch.empty(n, 18, device="cuda", dtype=dt)
+            rV = torch.empty(n, 6, device="cuda", dtype=dt)
+            rC = torch.empty(n, 2, device="cuda", dtype=dt)
+            table = [("exp", "M", "ahtl", rM, 36), ("expTA", "M", "ahtl", rM, 36), ("expA", "M", "ah", rM, 36),
+                     ("sqrt", "M", "pos", rM, 36), ("invsqrt", "M", "pos", rM, 36), ("sqrtPH", "M", "pos", rM, 36),
+                     ("invsqrtPH", "M", "pos", rM, 36), ("log", "M", "pos", rM, 36), ("inverse", "M", "gen", rM, 36),
+                     ("det", "C", "gen", rC, 20), ("eigenvalsH", "V", "herm", rV, 24),
+                     ("eigenvals", "V", "gen", rV, 24), ("M_inverse_V", "V", "gen", rV, 30),
+                     ("M_inverse_M", "M", "gen", rM, 54)]
+            for fname, dest, src, outt, nb in table:
+                if fname.startswith("M_inverse"):
+                    bb = bv if dest == "V" else ins["pos"]
+                    f = getattr(L, f"QLA_{pc}_{dest}_veq_{fname}")
+                    call = (lambda f=f, outt=outt, src=src, bb=bb: f(V(outt), V(ins[src]), V(bb), n))
+                else:
+                    f = getattr(L, f"QLA_{pc}_{dest}_veq_{fname}_M")
+                    call = (lambda f=f, outt=outt, src=src: f(V(outt), V(ins[src]), n))
+                ms = _events_time(torch, stream, call, reps)
+                row = {"site_updates_per_s": n / (ms / 1e3), "us": 1e3 * ms, "gbs": nb * e * n / (ms / 1e3) / 1e9}
+                if cpu_kind == "reference":
+                    a_h = ins[src][:ns].cpu().numpy()
+                    o_h = np.zeros((ns, outt.shape[1]), dtype=a_h.dtype)
+                    fc = getattr(lib_cpu, f.__name__)
+                    if fname.startswith("M_inverse"):
+                        b_h = bb[:ns].cpu().numpy()
+                        cc = (lambda fc=fc: fc(V(o_h.ctypes.data), V(a_h.ctypes.data), V(b_h.ctypes.data), ns))
+                    else:
+                        cc = (lambda fc=fc: fc(V(o_h.ctypes.data), V(a_h.ctypes.data), ns))
+                    cc()
+                    t0 = time.perf_counter()
+                    it = 0
+                    while time.perf_counter() - t0 < 0.4:
+                        cc()
+                        it += 1
+                    cpu = ns * it / (time.perf_counter() - t0)
+                    row["cpu_site_updates_per_s"] = cpu
+                    row["gpu_over_cpu"] = row["site_updates_per_s"] / cpu
+                res[f"{pc}_{fname}"] = row
             qla.check("mfunc")
-            del a, r, c
+            del ins, bv, rM, rV, rC
             torch.cuda.empty_cache()
-        out.update({"metric": "matrix functions exp/sqrt/inverse/det on 32^3x64 sites", "unit": "site-updates/s",
-                    "value": res["F3_exp"]["site_updates_per_s"], "ops": res})
+        out.update({"metric": "colour-matrix functions on 32^3x64 sites (every function of the code templates)",
+                    "unit": "site-updates/s", "value": res["F3_exp"]["site_updates_per_s"], "ops": res,
+                    "cpu_baseline": {"kind": cpu_kind, "cores": threads,
+                                     "sample": f"{ns} sites of the same inputs, repeated for 0.4 s per op"}})
     elif args.workload == "config1":
         n = 16 ** 4
         res = {}
