@@ -179,6 +179,27 @@ def cpu_chain_rate(x, p, a_vals, budget_s=15.0, max_iters=None):
     return n * it / el, it, el, kind, threads
 
 
+def reduction_errors(x, p, nrm_v, dot_v, chunk=1 << 20):
+    """Relative errors of a GPU norm2 / dot against sums of the same data in
+    extended precision: products in long double (exact for float inputs),
+    each site's 24 terms summed in long double, sites summed with math.fsum."""
+    import math
+
+    import numpy as np
+    n2, dr, di = [], [], []
+    for i in range(0, x.shape[0], chunk):
+        xc = x[i:i + chunk].astype(np.longdouble)
+        pc = p[i:i + chunk].astype(np.longdouble)
+        xr, xi, pr, pi = xc[:, 0::2], xc[:, 1::2], pc[:, 0::2], pc[:, 1::2]
+        n2.append((xc * xc).sum(axis=1).astype(np.float64))
+        dr.append((xr * pr + xi * pi).sum(axis=1).astype(np.float64))
+        di.append((xr * pi - xi * pr).sum(axis=1).astype(np.float64))
+    ref_n = math.fsum(np.concatenate(n2))
+    ref_d = complex(math.fsum(np.concatenate(dr)), math.fsum(np.concatenate(di)))
+    return {"norm2_rel_err": abs(nrm_v - ref_n) / abs(ref_n),
+            "dot_rel_err": abs(complex(*dot_v) - ref_d) / abs(ref_d)}
+
+
 # ---------------------------------------------------------------------------
 def run_reference_arm(args):
     import numpy as np
@@ -318,6 +339,11 @@ def run_gpu_arm(args):
     ms_f = max_over_ranks(ms_f, world, dev)
     value = whole_job_rate(world, n, iters, args.steps, ms_f)
     assert np.all(np.isfinite(nrm.cpu().numpy()))
+    # accuracy of the last iteration's reductions (x as the last axpy left it)
+    red_err = None
+    if not args.no_accuracy:
+        red_err = reduction_errors(x.cpu().numpy(), p.cpu().numpy(), float(nrm[iters - 1]),
+                                   dot[iters - 1].cpu().numpy())
 
     # ---------------- end to end through the C-ABI with host buffers: per step
     # the pinned host -> device copy of x and p, the chain, and the device ->
@@ -366,6 +392,10 @@ def run_gpu_arm(args):
         ms_d, kern_d = timed(xd, pd, chain_d)
         ms_d = max_over_ranks(ms_d, world, dev)
         value_d = whole_job_rate(world, n, iters, args.steps, ms_d)
+        if red_err is not None:
+            ed = reduction_errors(xd.cpu().numpy(), pd.cpu().numpy(), float(nrm[iters - 1]),
+                                  dot[iters - 1].cpu().numpy())
+            red_err.update({"fp64_chain_" + k: v for k, v in ed.items()})
         del xd, pd
         torch.cuda.empty_cache()
 
@@ -422,6 +452,9 @@ def run_gpu_arm(args):
                          "unit": "GB/s", "frac": rl[dom]["frac"], "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": BYTES_F3[dom] * n},
             "kernels": rl,
+            "reductions": None if red_err is None else dict(
+                red_err, reference="the same data in long double (exact products for float inputs), "
+                                   "sites summed with math.fsum; last iteration of the timed region"),
             "e2e": e2e,
             "gpu_launches": 3 * iters * args.steps,
             "clocks": clocks,
@@ -710,6 +743,7 @@ def main():
     ap.add_argument("--iters", type=int, default=ITERS)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the reduction accuracy check")
     ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "config1"],
                     help="cg_chain is the benchmark line; the others measure the remaining configurations")
     args = ap.parse_args()

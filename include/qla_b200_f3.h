@@ -2688,6 +2688,14 @@ void QLA_F3_M_xeq_invsqrtPH_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_C
 void QLA_F3_V_xeq_eigenvals_pM(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
 /* replaces QLA_F3_V_xeq_eigenvalsH_pM (lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenvalues), code-templates/M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166) */
 void QLA_F3_V_xeq_eigenvalsH_pM(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* qlagpu_F3_M_veq_reunit_M: no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64 */
+void qlagpu_F3_M_veq_reunit_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* qlagpu_F3_M_veq_reunit_pM: no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64 */
+void qlagpu_F3_M_veq_reunit_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* qlagpu_F3_M_xeq_reunit_M: no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64 */
+void qlagpu_F3_M_xeq_reunit_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* qlagpu_F3_M_xeq_reunit_pM: no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64 */
+void qlagpu_F3_M_xeq_reunit_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
 /* replaces QLA_F3_V_veq_M_inverse_V (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
 void QLA_F3_V_veq_M_inverse_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
 /* replaces QLA_F3_V_veq_M_inverse_pV (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */

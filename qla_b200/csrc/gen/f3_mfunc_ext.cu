@@ -133,6 +133,22 @@ QLAB_EXPORT void QLA_F3_V_xeq_eigenvalsH_pM(QLA_F3_ColorVector *__restrict__ r, 
   qlab::api_map<qlab::EigenvalsHOp<float>>("F3_mfunc_eigenvalsH", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
+QLAB_EXPORT void qlagpu_F3_M_veq_reunit_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_map<qlab::ReunitOp<float>>("F3_reunit", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void qlagpu_F3_M_veq_reunit_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_map<qlab::ReunitOp<float>>("F3_reunit", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
+}
+
+QLAB_EXPORT void qlagpu_F3_M_xeq_reunit_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_map<qlab::ReunitOp<float>>("F3_reunit", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
+QLAB_EXPORT void qlagpu_F3_M_xeq_reunit_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_map<qlab::ReunitOp<float>>("F3_reunit", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
+}
+
 QLAB_EXPORT void QLA_F3_V_veq_M_inverse_V(QLA_F3_ColorVector *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
   qlab::api_map<qlab::MInverseOp<float, 1>>("F3_minv_V", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }

@@ -173,8 +173,6 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
         load_rec<float, 9>(u, st + (unsigned)t * kRecM);
         const int j = reinterpret_cast<const int*>(st + offI)[t];
         load_rec<float, 3>(v, st + offV + (unsigned)t * kRecV);
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
         load_rec_global<float, 9>(gm, F.u2 + (long long)j * 18);
         MxM::apply(sp, u, gm, dummy, r);
         MxV::apply(sp, r, v, dummy, w);
@@ -183,17 +181,19 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
         __syncwarp();
         store_rec_smem<float, 9>(ob + (unsigned)lane * kRecM, r);
         store_rec_smem<float, 3>(ob + 32 * kRecM + (unsigned)lane * kRecV, w);
+        // orders this lane's stage reads and slice writes before the async
+        // proxy (the stores below and the producer's next copy into the stage)
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
+          mbar_arrive(&empty[s]);  // this warp is done with the stage
           const long long s0 = site0 + warp * 32;
           bulk_s2g(F.r + s0 * 18, ob, 32u * kRecM, pol);
           bulk_s2g(F.w + s0 * 6, ob + 32 * kRecM, 32u * kRecV, pol);
           bulk_commit();
         }
       } else {
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
+        release_stage(&empty[s], lane);  // this warp is done with the stage
         const long long i = site0 + t;
         if (i < F.n) batch_site_direct(F, i, sp);
         if (lane == 0) bulk_commit();  // an empty group keeps the slice bookkeeping aligned

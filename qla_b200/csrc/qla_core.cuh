@@ -243,6 +243,23 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+// A consumer warp hands a staged tile back to the producer.  The warp's
+// shared-memory reads of the stage (generic proxy) must be complete before
+// the producer's next bulk copy (async proxy) lands in it.  The mbarrier
+// arrive by itself did not ensure that on B200: a D3 norm2 of 192-B records
+// read stage data that the next tile's copy had already overwritten.  After
+// the warp has converged, the arriving lane issues a generic-to-async proxy
+// fence first; the loads are warp-wide instructions, so that lane's fence
+// covers every lane's reads.  (A full block-scope memory fence in every lane
+// also works but costs 14% on the axpy kernel; this costs ~2%.)
+__device__ __forceinline__ void release_stage(uint64_t* bar, int lane) {
+  __syncwarp();
+  if (lane == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive(bar);
+  }
+}
+
 // 1-D bulk copy global -> shared, completion signalled on an mbarrier.
 // Requires 16-B aligned addresses and a size that is a multiple of 16.
 __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar,

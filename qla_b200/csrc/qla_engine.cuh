@@ -297,22 +297,25 @@ __global__ void __launch_bounds__(288) site_tma_kernel(const SiteParams p) {
       if constexpr (OP::NOUT > 0) {
         if (p.out_read) load_rec<R, OP::NOUT>(y, st + p.off_out_in + (unsigned)t * OB);
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with the stage
       if constexpr (OP::NOUT > 0) {
         OP::apply(p, x0, x1, x2, y);
         unsigned char* ob = myout + (size_t)(k & 1) * 32 * OB;
         if (lane == 0) bulk_wait_read<1>();  // slice (k&1) no longer read by this warp's store k-2
         __syncwarp();
         store_rec_smem<R, OP::NOUT>(ob + (unsigned)lane * OB, y);
+        // every lane orders its reads of the stage and its writes of the
+        // slice before the async proxy: the slice's bulk store below, and
+        // the producer's next bulk copy into the stage released here
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
+          mbar_arrive(&empty[s]);  // this warp is done with the stage
           const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * T + warp * 32;
           bulk_s2g(static_cast<char*>(p.out) + site0 * OB, ob, 32u * OB, pol);
           bulk_commit();
         }
       } else {
+        release_stage(&empty[s], lane);  // this warp is done with the stage
         double acc[NA];
         OP::accum(p, x0, x1, x2, acc);
         acc_fold<OP>(dacc, acc);

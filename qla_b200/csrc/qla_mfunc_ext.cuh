@@ -10,6 +10,7 @@
 //   sqrtPH, invsqrtPH         M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201
 //   eigenvalsH, eigenvals     V_eq_eigenvalsH_M.c:106-166,
 //                             V_eq_eigenvals_M.c:127-186 (cubic roots)
+//   reunit (no counterpart)   u (u^+ u)^(-1/2) from the pieces above
 //
 // Precision.  a^-1 b uses only +, -, *, / and is evaluated in the site
 // precision with explicitly rounded operations: bit-identical to QLA_F3 and
@@ -25,6 +26,7 @@
 // the templates' branch points.
 #pragma once
 #include "qla_mfunc.cuh"
+#include "qla_ops.cuh"
 
 namespace qlab {
 
@@ -429,31 +431,62 @@ __device__ __forceinline__ void getfs_sqrtph(double& f0, double& f1, double& f2,
   }
 }
 
+// f0 + f1 m + f2 m^2 of a positive Hermitian m (M_eq_sqrtPH_M.c:140-197,
+// M_eq_invsqrtPH_M.c:144-201)
+template <bool INV>
+__device__ __forceinline__ void sqrtph3_fp64(Cx<double> (&r)[9], const Cx<double> (&m)[9]) {
+  Cx<double> mm[9];
+  const double tr = dadd(dadd(m[0].re, m[4].re), m[8].re);
+  mat3_mul_first(mm, m, m);
+  const double p2 = dadd(dadd(mm[0].re, mm[4].re), mm[8].re);
+  Cx<double> det0, det1, det2;
+  cofactors3(det0, det1, det2, m);
+  double det = dsub(dmul(det2.re, m[8].re), dmul(det2.im, m[8].im));
+  det = dadd(det, dsub(dmul(det1.re, m[7].re), dmul(det1.im, m[7].im)));
+  det = dadd(det, dsub(dmul(det0.re, m[6].re), dmul(det0.im, m[6].im)));
+  double f0, f1, f2;
+  getfs_sqrtph<INV>(f0, f1, f2, tr, p2, det);
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    Cx<double> e{dmul(f2, mm[k].re), dmul(f2, mm[k].im)};
+    e = Cx<double>{dadd(e.re, dmul(f1, m[k].re)), dadd(e.im, dmul(f1, m[k].im))};
+    if (k % 4 == 0) e.re = dadd(e.re, f0);
+    r[k] = e;
+  }
+}
+
 template <typename R_, bool INV>
 struct SqrtPHOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
   __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                Cx<R> (&r)[9]) {
-    Cx<double> m[9], mm[9];
+    Cx<double> m[9], y[9];
     promote9(m, a);
-    const double tr = dadd(dadd(m[0].re, m[4].re), m[8].re);
-    mat3_mul_first(mm, m, m);
-    const double p2 = dadd(dadd(mm[0].re, mm[4].re), mm[8].re);
-    Cx<double> det0, det1, det2;
-    cofactors3(det0, det1, det2, m);
-    double det = dsub(dmul(det2.re, m[8].re), dmul(det2.im, m[8].im));
-    det = dadd(det, dsub(dmul(det1.re, m[7].re), dmul(det1.im, m[7].im)));
-    det = dadd(det, dsub(dmul(det0.re, m[6].re), dmul(det0.im, m[6].im)));
-    double f0, f1, f2;
-    getfs_sqrtph<INV>(f0, f1, f2, tr, p2, det);
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      Cx<double> e{dmul(f2, mm[k].re), dmul(f2, mm[k].im)};
-      e = Cx<double>{dadd(e.re, dmul(f1, m[k].re)), dadd(e.im, dmul(f1, m[k].im))};
-      if (k % 4 == 0) e.re = dadd(e.re, f0);
-      r[k] = cround<R>(e);
-    }
+    sqrtph3_fp64<INV>(y, m);
+    round_out(r, y);
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// Unitarity reprojection r = u (u^+ u)^(-1/2), with no counterpart in the
+// reference: the composition QLA_D3_M_eq_Ma_times_M -> M_eq_invsqrtPH_M ->
+// M_eq_M_times_M evaluated in FP64 with those functions' operation order,
+// fused so that u is read once and r written once.
+template <typename R_>
+struct ReunitOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
+  __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               Cx<R> (&r)[9]) {
+    Cx<double> u[9], t[9], s[9];
+    promote9(u, a);
+    lmult_site<double, 3, 3, true, false>(EQ, false, u, u, t);   // u^+ u
+    sqrtph3_fp64<true>(s, t);                                     // (u^+ u)^(-1/2)
+    lmult_site<double, 3, 3, false, false>(EQ, false, u, s, t);  // u s
+    round_out(r, t);
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                double*) {}

@@ -148,15 +148,16 @@ __global__ void __launch_bounds__(288) multi_tma_kernel(const MultiParams p) {
         fetch_staged<LMultOp<R, 3, 1, ADJ, false>, 3>(b, p.b[d], st, p.off_b[d], t);
         multi_site<R, ADJ>(p, a, b, y, d > 0 || p.out_read);
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
       unsigned char* ob = myout + (size_t)(k & 1) * 32 * RV;
       if (lane == 0) bulk_wait_read<1>();
       __syncwarp();
       store_rec_smem<R, 3>(ob + (unsigned)lane * RV, y);
+      // orders this lane's stage reads and slice writes before the async
+      // proxy (the store below and the producer's next copy into the stage)
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) {
+        mbar_arrive(&empty[s]);  // this warp is done with the stage
         const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * T + warp * 32;
         bulk_s2g(static_cast<char*>(p.out) + site0 * RV, ob, 32u * RV, pol);
         bulk_commit();

@@ -63,6 +63,8 @@ CITE["mfunc_ext"] = ("lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenva
                      "M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, "
                      "M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, "
                      "V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166")
+CITE["reunit"] = ("no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of "
+                  "M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64")
 CITE["minv"] = ("lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), "
                 "code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135")
 MFUNC_OPS = {"exp": "ExpOp", "sqrt": "SqrtOp", "inverse": "InverseOp"}
@@ -565,6 +567,18 @@ def gen_pc(pc, R, P):
                             f"qlab::Opnd{{}}, {gang}, n, qlab::EQ);")
                     fns.append(Fn(name, params, body, "mfunc_ext", CITE["mfunc_ext"],
                                   dict(dest=dest, eqop="eq", var=var, a=src, fn=fname)))
+    # ---- unitarity reprojection (no counterpart in the reference)
+    for var in ["v", "x"]:
+        gang = "index" if var == "x" else "nullptr"
+        tail = [("int *", "index")] if var == "x" else []
+        for src, p1 in [("M", False), ("pM", True)]:
+            pa, oa = operand(pc, "M", p1, "a")
+            name = f"qlagpu_{pc}_M_{var}eq_reunit_{src}"
+            params = [(f"{ptype(pc, 'M')} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+            body = (f"qlab::api_map<qlab::ReunitOp<{R}>>({kid('reunit')}, r, {oa}, qlab::Opnd{{}}, {gang}, n, "
+                    f"qlab::EQ);")
+            fns.append(Fn(name, params, body, "mfunc_ext", CITE["reunit"],
+                          dict(dest="M", eqop="eq", var=var, a=src, fn="reunit")))
     # ---- a^-1 b for a ColorVector or ColorMatrix b
     for T, nb in (("V", 1), ("M", 3)):
         for var in ["v", "x"]:
@@ -697,7 +711,10 @@ def main():
             if fn.family != fam:
                 fam = fn.family
                 text += f"/* ---- {fam}: replaces the {hpc} functions emitted by {fn.cite.split(',')[0]} */\n"
-            text += f"/* replaces {fn.name} ({fn.cite}) */\n"
+            if fn.cite.startswith("no counterpart"):
+                text += f"/* {fn.name}: {fn.cite} */\n"
+            else:
+                text += f"/* replaces {fn.name} ({fn.cite}) */\n"
             text += fn.proto("QLA_B200_RESTRICT") + ";\n"
         text += HEADER_END
         written += write_if_changed(os.path.join(OUT_INC, fname), text)

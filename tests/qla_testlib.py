@@ -181,6 +181,11 @@ def to_dev(x):
     return torch.from_numpy(np.ascontiguousarray(x)).cuda()
 
 
+def ptr_dev(t):
+    """ctypes pointer to a device tensor's storage (the caller keeps t alive)."""
+    return ctypes.c_void_p(t.data_ptr())
+
+
 def to_host(t):
     return t.detach().cpu().numpy()
 

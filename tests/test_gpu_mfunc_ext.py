@@ -272,3 +272,42 @@ def test_eigenvals_general(qla):
     ref64 = T.ora_mfunc(af.astype(np.float64), n, "eigenvals").astype(np.float32)
     close = np.abs(gotf - ref64) <= 1e-5 * scale
     assert np.mean(np.all(close, axis=1)) > 0.999
+
+
+def _reunit_ref(u, n):
+    """The D3 composition the fused op stands for: u (u^+ u)^(-1/2) through
+    M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M."""
+    t = np.zeros_like(u)
+    T.ora_lmult(t, u, u, n, 3, "eq", adja=1)
+    s = T.ora_mfunc(t, n, "invsqrtPH")
+    r = np.zeros_like(u)
+    T.ora_lmult(r, u, s, n, 3, "eq")
+    return r
+
+
+@pytest.mark.parametrize("drift,tol", [(1e-7, 1e-9), (1e-3, 1e-12), (0.3, 1e-11)])
+def test_reunit_fused_against_d3_composition(qla, drift, tol):
+    """qlagpu_{F3,D3}_M_veq_reunit_M (no counterpart in the reference) against
+    the D3 composition of reference functions.  Near-unitary inputs make
+    u^+ u nearly triply degenerate, where the invsqrtPH closed form itself is
+    good to ~1e-10, so that case is bounded at 1e-9."""
+    rng = np.random.default_rng(41)
+    n = 40009
+    u = T.haar_su3(rng, n, np.float64) + drift * T.gaussian_field(rng, n, 9, np.float64)
+    want = _reunit_ref(u, n)
+    L = qla.lib()
+    r_d, u_d = T.to_dev(np.zeros_like(u)), T.to_dev(u)
+    L.qlagpu_D3_M_veq_reunit_M(T.ptr_dev(r_d), T.ptr_dev(u_d), n)
+    qla.check("reunit")
+    got = T.to_host(r_d)
+    assert np.abs(got - want).max() <= tol, np.abs(got - want).max()
+    z = T.to_complex(got)
+    assert np.abs(np.conj(np.transpose(z, (0, 2, 1))) @ z - np.eye(3)).max() <= max(tol, 1e-12)
+    uf = u.astype(np.float32)
+    rf, uf_d = T.to_dev(np.zeros_like(uf)), T.to_dev(uf)
+    L.qlagpu_F3_M_veq_reunit_M(T.ptr_dev(rf), T.ptr_dev(uf_d), n)
+    gotf = T.to_host(rf)
+    ok, nbad = T.qla_close(gotf, _reunit_ref(uf.astype(np.float64), n), np.float32)
+    assert ok, nbad
+    zf = T.to_complex(gotf.astype(np.float64))
+    assert np.abs(np.conj(np.transpose(zf, (0, 2, 1))) @ zf - np.eye(3)).max() < 1e-6

@@ -11,6 +11,7 @@ stated per comparison:
     rel <= 1e-6 when it rounds each F3 term to float, rel <= 1e-12 for D3;
   * F3 functions return float: within 1 ulp of the correctly rounded value.
 """
+import ctypes
 import itertools
 
 import numpy as np
@@ -125,3 +126,41 @@ def test_full_size_cg_chain_reductions(qla, cuda):
     e_d = T.ora_dot(want_x, ph, n, 12, exact=True)
     assert _rel(nrm, e_n) <= 1e-12
     assert abs(dot - e_d) <= 1e-12 * abs(e_d)
+
+
+@pytest.mark.parametrize("rp,dt", [("D3", np.float64), ("DF3", np.float32), ("F3", np.float32)])
+def test_reductions_on_large_fields_match_the_direct_path(qla, cuda, rp, dt):
+    """Fields of 2^24 complex numbers run the pipelined kernel with many tiles
+    per block, so every shared-memory stage is refilled many times.  Each of
+    three repeated calls must equal the direct path's result bit for bit (the
+    same per-site terms, both summed in double-double), and match the
+    long-double sum of the data.  A stage refilled before its consumers had
+    finished reading it showed up here first, as run-to-run differences of
+    the D3 DiracFermion norm2 at the 1e-7 level."""
+    import math
+    g = cuda.Generator(device="cuda")
+    g.manual_seed(11)
+    V = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    L = qla.lib()
+    out = cuda.zeros(4, dtype=cuda.float32 if rp == "F3" else cuda.float64, device="cuda")
+    for t in ("V", "H", "D", "M"):
+        nc = T.NCPLX3[t]
+        n = (1 << 24) // nc
+        x = cuda.randn(n, 2 * nc, device="cuda", dtype=cuda.float32 if dt == np.float32 else cuda.float64,
+                       generator=g)
+        y = cuda.randn_like(x)
+        gang = cuda.arange(n, dtype=cuda.int32, device="cuda")
+        getattr(L, f"QLA_{rp}_r_xeq_norm2_{t}")(V(out), V(x), V(gang), n)
+        getattr(L, f"QLA_{rp}_c_xeq_{t}_dot_{t}")(V(out[1:]), V(x), V(y), V(gang), n)
+        ref = out[:3].cpu().numpy().copy()
+        for _ in range(3):
+            getattr(L, f"QLA_{rp}_r_veq_norm2_{t}")(V(out), V(x), n)
+            getattr(L, f"QLA_{rp}_c_veq_{t}_dot_{t}")(V(out[1:]), V(x), V(y), n)
+            got = out[:3].cpu().numpy()
+            assert np.array_equal(got, ref), (t, got, ref)
+        qla.check("large reductions")
+        xs = x.cpu().numpy().astype(np.longdouble)
+        exact = math.fsum((xs * xs).sum(axis=1).astype(np.float64))
+        tol = 6e-8 if rp == "F3" else 1e-12
+        assert abs(float(ref[0]) - exact) <= tol * exact, (t, ref[0], exact)
+        del x, y, gang, xs
