@@ -697,6 +697,36 @@ def run_workload(args):
                     "unit": "site-updates/s", "value": res["F3_exp"]["site_updates_per_s"], "ops": res,
                     "cpu_baseline": {"kind": cpu_kind, "cores": threads,
                                      "sample": f"{ns} sites of the same inputs, repeated for 0.4 s per op"}})
+    elif args.workload == "prop":
+        # DiracPropagator products (1152-B F3 records): M*P, P*M, P*P, P^+*P
+        # (peq forms read the destination too) and the spin trace, 16^3x32
+        n = 16 * 16 * 16 * 32
+        res = {}
+        for pc, dt, e in (("F3", torch.float32, 4), ("D3", torch.float64, 8)):
+            m = torch.randn(n, 18, device="cuda", dtype=dt)
+            pa = torch.randn(n, 288, device="cuda", dtype=dt)
+            pb = torch.randn(n, 288, device="cuda", dtype=dt)
+            pr = torch.randn(n, 288, device="cuda", dtype=dt)
+            mr = torch.empty(n, 18, device="cuda", dtype=dt)
+            P = 288 * e  # bytes of one propagator record
+            table = [("P_veq_M_times_P", (pr, m, pa), 9 * 2 * e + 2 * P),
+                     ("P_veq_P_times_M", (pr, pa, m), 9 * 2 * e + 2 * P),
+                     ("P_vpeq_M_times_P", (pr, m, pa), 9 * 2 * e + 3 * P),
+                     ("P_veq_P_times_P", (pr, pa, pb), 3 * P),
+                     ("P_veq_Pa_times_P", (pr, pa, pb), 3 * P),
+                     ("M_veq_spintrace_P", (mr, pa), P + 9 * 2 * e)]
+            for nm, args_, nb in table:
+                f = getattr(L, f"QLA_{pc}_{nm}")
+                call = (lambda f=f, args_=args_: f(*[V(t) for t in args_], n))
+                ms = _events_time(torch, stream, call, reps)
+                gbs = nb * n / (ms / 1e3) / 1e9
+                res[f"{pc}_{nm}"] = {"site_updates_per_s": n / (ms / 1e3), "us": 1e3 * ms, "bytes_per_site": nb,
+                                     "gbs": gbs, "hbm_frac": gbs / peak}
+            qla.check("prop")
+            del m, pa, pb, pr, mr
+            torch.cuda.empty_cache()
+        out.update({"metric": "DiracPropagator products and spin trace on 16^3x32 sites", "unit": "site-updates/s",
+                    "value": res["F3_P_veq_M_times_P"]["site_updates_per_s"], "ops": res})
     elif args.workload == "config1":
         n = 16 ** 4
         res = {}
@@ -744,7 +774,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the reduction accuracy check")
-    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "config1"],
+    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "prop", "config1"],
                     help="cg_chain is the benchmark line; the others measure the remaining configurations")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -7,14 +7,22 @@
 // (lib/perl/build_qla.pl:1588-1622 left multiplication, :1627-1661 right
 // multiplication, expressions_tensor.pl:766; spin trace build_qla.pl:942-968).
 //
-// A P record does not fit in registers, and one thread per site would read it
-// with a 1152-B stride.  Instead one thread computes ONE output element of one
-// site: consecutive threads produce consecutive elements, so the operand
-// elements they read (P'[..][jc][js] for fixed k) and the results they write
-// are contiguous in memory -- coalesced AoS access without staging -- and the
-// matrix / row operands shared by the 144 threads of a site come from L1.
-// Every output element is accumulated exactly as the reference does (x = 0 or
-// r, then x (+|-)= a*b over k in order), so results are bit-identical.
+// A P record does not fit in one thread's registers, so several threads share
+// a site, and the work is split so that every thread reads each operand
+// element it needs once, in 16-B (F3) / 32-B (D3) runs of two consecutive
+// complex numbers, and consecutive threads touch consecutive runs:
+//   M * P   24 threads per site, thread (is, jc, js pair): the P run
+//           P[kc][is][jc][js..js+1] serves all three output colours ic;
+//   P * M   24 threads per site, thread (ic, is, js pair): the P run
+//           P[ic][is][kc][js..js+1] serves all three output colours jc;
+//   P * P   6 (F3) / 12 (D3) threads per site, thread (jc, js block): a
+//           column block of the second operand held in registers, the first
+//           operand's rows streamed once, 24 / 12 outputs per thread.
+// The 9 matrix elements come from L1 (shared by a site's threads).  Adjoint
+// or pointer operands read element by element.  Every output element is
+// accumulated exactly as the reference does (x = 0 or r, then
+// x (+|-)= a*b over k in order), so results are bit-identical.  The spin
+// trace keeps one thread per output element (9 per site).
 #pragma once
 #include "qla_launch.cuh"
 #include "qla_ops.cuh"
@@ -29,6 +37,7 @@ struct PropParams {
   const int* gang;
   long long n;
   int eqop;
+  int vec_a, vec_b, vec_out;  // 16-B vector access allowed (contiguous, aligned)
 };
 
 template <typename R>
@@ -47,52 +56,245 @@ __device__ __forceinline__ int p_idx(int i, int s, int j, int t, bool adj) {
 }
 __device__ __forceinline__ int m_idx(int i, int j, bool adj) { return adj ? j * 3 + i : i * 3 + j; }
 
-template <typename R, int KIND, bool CA, bool CB>
-__global__ void __launch_bounds__(256) prop_kernel(const PropParams p) {
-  constexpr int NEL = (KIND == PK_TRACE) ? 9 : 144;  // output elements per site
-  constexpr int RP = 144, RM = 9;
-  const long long total = p.n * NEL;
+// two consecutive complex numbers e, e+1 of record k (16 B F3, 32 B D3)
+template <typename R>
+__device__ __forceinline__ void ld2(Cx<R> (&v)[2], const Opnd& o, long long k, int e, int rec, bool vec) {
+  if (vec) {
+    const Cx<R>* base = static_cast<const Cx<R>*>(o.base) + k * rec + e;
+    if constexpr (sizeof(R) == 4) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(base));
+      v[0] = Cx<R>{u.x, u.y};
+      v[1] = Cx<R>{u.z, u.w};
+    } else {
+      const double2* q = reinterpret_cast<const double2*>(base);
+      const double2 u = __ldg(q), w = __ldg(q + 1);
+      v[0] = Cx<R>{u.x, u.y};
+      v[1] = Cx<R>{w.x, w.y};
+    }
+  } else {
+    v[0] = ld_elem<R>(o, k, e, rec);
+    v[1] = ld_elem<R>(o, k, e + 1, rec);
+  }
+}
+template <typename R>
+__device__ __forceinline__ void ld2_out(Cx<R> (&v)[2], const Cx<R>* q, bool vec) {
+  if (vec) {
+    if constexpr (sizeof(R) == 4) {
+      const float4 u = *reinterpret_cast<const float4*>(q);
+      v[0] = Cx<R>{u.x, u.y};
+      v[1] = Cx<R>{u.z, u.w};
+    } else {
+      const double2 u = reinterpret_cast<const double2*>(q)[0], w = reinterpret_cast<const double2*>(q)[1];
+      v[0] = Cx<R>{u.x, u.y};
+      v[1] = Cx<R>{w.x, w.y};
+    }
+  } else {
+    v[0] = q[0];
+    v[1] = q[1];
+  }
+}
+template <typename R>
+__device__ __forceinline__ void st2(Cx<R>* q, const Cx<R> (&v)[2], bool vec) {
+  if (vec) {
+    if constexpr (sizeof(R) == 4) {
+      *reinterpret_cast<float4*>(q) = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+    } else {
+      reinterpret_cast<double2*>(q)[0] = make_double2(v[0].re, v[0].im);
+      reinterpret_cast<double2*>(q)[1] = make_double2(v[1].re, v[1].im);
+    }
+  } else {
+    q[0] = v[0];
+    q[1] = v[1];
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void init2(Cx<R> (&x)[2], const Cx<R>* q, bool load, bool vec) {
+  if (load) {
+    ld2_out<R>(x, q, vec);
+  } else {
+    x[0] = Cx<R>{R(0), R(0)};
+    x[1] = Cx<R>{R(0), R(0)};
+  }
+}
+
+// M * P: 24 threads per site; thread q = (is, jc, jh), outputs (ic, is, jc,
+// 2jh..2jh+1) for ic = 0..2
+template <typename R, bool CA, bool CB>
+__global__ void __launch_bounds__(256) prop_mp_kernel(const PropParams p) {
+  const long long total = p.n * 24;
   const bool minus = (p.eqop == MEQ || p.eqop == EQM);
   const bool load = (p.eqop == PEQ || p.eqop == MEQ);
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (long long)gridDim.x * blockDim.x) {
-    const long long i = g / NEL;
-    const int e = (int)(g - i * NEL);
+    const long long i = g / 24;
+    const int q = (int)(g - i * 24);
+    const int is = q / 6, jc = (q >> 1) % 3, jh = q & 1;
     const long long k = p.gang ? (long long)p.gang[i] : i;
-    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * NEL + e;
-    Cx<R> x = load ? *out : Cx<R>{R(0), R(0)};
-    if constexpr (KIND == PK_TRACE) {
-      const int ic = e / 3, jc = e % 3;
+    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 144 + 2 * q;  // + ic * 48
+    Cx<R> mm[9];
 #pragma unroll
-      for (int s = 0; s < 4; s++) {
-        const Cx<R> v = ld_elem<R>(p.a, k, ((ic * 4 + s) * 3 + jc) * 4 + s, RP);
-        if (minus) {
-          x.re = rsub(x.re, v.re);
-          x.im = rsub(x.im, v.im);
-        } else {
-          x.re = radd(x.re, v.re);
-          x.im = radd(x.im, v.im);
-        }
-      }
-    } else {
-      const int ic = e / 48, is = (e / 12) % 4, jc = (e / 4) % 3, js = e % 4;
-      if constexpr (KIND == PK_MP) {
+    for (int e = 0; e < 9; e++) mm[e] = ld_elem<R>(p.a, k, e, 9);
+    Cx<R> x[3][2];
 #pragma unroll
-        for (int kc = 0; kc < 3; kc++)
-          cmac<CA, CB>(x, minus, ld_elem<R>(p.a, k, m_idx(ic, kc, CA), RM),
-                       ld_elem<R>(p.b, k, p_idx(kc, is, jc, js, CB), RP));
-      } else if constexpr (KIND == PK_PM) {
+    for (int ic = 0; ic < 3; ic++) init2<R>(x[ic], out + ic * 48, load, p.vec_out);
 #pragma unroll
-        for (int kc = 0; kc < 3; kc++)
-          cmac<CA, CB>(x, minus, ld_elem<R>(p.a, k, p_idx(ic, is, kc, js, CA), RP),
-                       ld_elem<R>(p.b, k, m_idx(kc, jc, CB), RM));
+    for (int kc = 0; kc < 3; kc++) {
+      Cx<R> b[2];
+      if constexpr (!CB) {
+        ld2<R>(b, p.b, k, kc * 48 + 2 * q, 144, p.vec_b);
       } else {
 #pragma unroll
-        for (int kc = 0; kc < 3; kc++)
+        for (int j = 0; j < 2; j++) b[j] = ld_elem<R>(p.b, k, p_idx(kc, is, jc, 2 * jh + j, true), 144);
+      }
 #pragma unroll
-          for (int ks = 0; ks < 4; ks++)
-            cmac<CA, CB>(x, minus, ld_elem<R>(p.a, k, p_idx(ic, is, kc, ks, CA), RP),
-                         ld_elem<R>(p.b, k, p_idx(kc, ks, jc, js, CB), RP));
+      for (int ic = 0; ic < 3; ic++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) cmac<CA, CB>(x[ic][j], minus, mm[m_idx(ic, kc, CA)], b[j]);
+    }
+#pragma unroll
+    for (int ic = 0; ic < 3; ic++) st2<R>(out + ic * 48, x[ic], p.vec_out);
+  }
+}
+
+// P * M: 24 threads per site; thread q = (ic, is, jh), outputs (ic, is, jc,
+// 2jh..2jh+1) for jc = 0..2
+template <typename R, bool CA, bool CB>
+__global__ void __launch_bounds__(256) prop_pm_kernel(const PropParams p) {
+  const long long total = p.n * 24;
+  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
+  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long i = g / 24;
+    const int q = (int)(g - i * 24);
+    const int row = q >> 1, jh = q & 1;  // row = ic * 4 + is
+    const int ic = row >> 2, is = row & 3;
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 144 + row * 12 + 2 * jh;  // + jc * 4
+    Cx<R> mm[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) mm[e] = ld_elem<R>(p.b, k, e, 9);
+    Cx<R> x[3][2];
+#pragma unroll
+    for (int jc = 0; jc < 3; jc++) init2<R>(x[jc], out + jc * 4, load, p.vec_out);
+#pragma unroll
+    for (int kc = 0; kc < 3; kc++) {
+      Cx<R> a[2];
+      if constexpr (!CA) {
+        ld2<R>(a, p.a, k, row * 12 + kc * 4 + 2 * jh, 144, p.vec_a);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 2; j++) a[j] = ld_elem<R>(p.a, k, p_idx(ic, is, kc, 2 * jh + j, true), 144);
+      }
+#pragma unroll
+      for (int jc = 0; jc < 3; jc++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) cmac<CA, CB>(x[jc][j], minus, a[j], mm[m_idx(kc, jc, CB)]);
+    }
+#pragma unroll
+    for (int jc = 0; jc < 3; jc++) st2<R>(out + jc * 4, x[jc], p.vec_out);
+  }
+}
+
+// P * P: thread (jc, js block) keeps the second operand's 12 runs
+// B[kc][ks][jc][js block] in registers and streams the rows of the first
+// operand, producing outputs (row, jc, js block) for all 12 rows.  The js
+// block is two spin components in F3 (6 threads per site, 16-B runs) and one
+// in D3 (12 threads per site, 16-B elements), which keeps the FP64 version's
+// registers low enough for two blocks per SM.
+template <typename R, bool CA, bool CB>
+__global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
+  constexpr int JW = sizeof(R) == 4 ? 2 : 1;  // spin components per thread
+  constexpr int TPS = 12 / JW;                 // threads per site
+  const long long total = p.n * TPS;
+  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
+  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long i = g / TPS;
+    const int q = (int)(g - i * TPS);
+    const int jc = q / (4 / JW), js0 = (q % (4 / JW)) * JW;
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 144 + jc * 4 + js0;  // + row * 12
+    Cx<R> b[12][JW];
+#pragma unroll
+    for (int kk = 0; kk < 12; kk++) {  // kk = kc * 4 + ks
+      if constexpr (!CB && JW == 2) {
+        ld2<R>(b[kk], p.b, k, kk * 12 + jc * 4 + js0, 144, p.vec_b);
+      } else {
+#pragma unroll
+        for (int j = 0; j < JW; j++) b[kk][j] = ld_elem<R>(p.b, k, p_idx(kk >> 2, kk & 3, jc, js0 + j, CB), 144);
+      }
+    }
+    // rows of the first operand, the next row's loads issued before the
+    // current row's multiply-adds so that a DRAM round trip overlaps them
+    Cx<R> a[12], an[12];
+    auto load_row = [&](Cx<R>(&dst)[12], int row) {
+#pragma unroll
+      for (int kk = 0; kk < 12; kk += 2) {
+        if constexpr (!CA) {
+          Cx<R> t[2];
+          ld2<R>(t, p.a, k, row * 12 + kk, 144, p.vec_a);
+          dst[kk] = t[0];
+          dst[kk + 1] = t[1];
+        } else {
+#pragma unroll
+          for (int j = 0; j < 2; j++)
+            dst[kk + j] = ld_elem<R>(p.a, k, p_idx(row >> 2, row & 3, (kk + j) >> 2, (kk + j) & 3, true), 144);
+        }
+      }
+    };
+    load_row(a, 0);
+#pragma unroll 1
+    for (int row = 0; row < 12; row++) {
+      if (row + 1 < 12) load_row(an, row + 1);
+      Cx<R> x[JW];
+      if (load) {
+#pragma unroll
+        for (int j = 0; j < JW; j++) x[j] = out[row * 12 + j];
+      } else {
+#pragma unroll
+        for (int j = 0; j < JW; j++) x[j] = Cx<R>{R(0), R(0)};
+      }
+#pragma unroll
+      for (int kk = 0; kk < 12; kk++)
+#pragma unroll
+        for (int j = 0; j < JW; j++) cmac<CA, CB>(x[j], minus, a[kk], b[kk][j]);
+      if constexpr (JW == 2) {
+        st2<R>(out + row * 12, x, p.vec_out);
+      } else {
+        out[row * 12] = x[0];
+      }
+#pragma unroll
+      for (int kk = 0; kk < 12; kk++) a[kk] = an[kk];
+    }
+  }
+}
+
+// the spin trace: one thread per output element (9 per site)
+template <typename R>
+__global__ void __launch_bounds__(256) prop_trace_kernel(const PropParams p) {
+  const long long total = p.n * 9;
+  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
+  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long i = g / 9;
+    const int e = (int)(g - i * 9);
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 9 + e;
+    Cx<R> x = load ? *out : Cx<R>{R(0), R(0)};
+    const int ic = e / 3, jc = e % 3;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const Cx<R> v = ld_elem<R>(p.a, k, ((ic * 4 + s) * 3 + jc) * 4 + s, 144);
+      if (minus) {
+        x.re = rsub(x.re, v.re);
+        x.im = rsub(x.im, v.im);
+      } else {
+        x.re = radd(x.re, v.re);
+        x.im = radd(x.im, v.im);
       }
     }
     *out = x;
@@ -114,11 +316,24 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
   p.gang = gang;
   p.n = n;
   p.eqop = eqop;
-  const long long total = (long long)n * ((KIND == PK_TRACE) ? 9 : 144);
+  p.vec_out = (reinterpret_cast<uintptr_t>(r) & 15u) == 0;
+  p.vec_a = a.mode == OM_CONTIG && (reinterpret_cast<uintptr_t>(a.base) & 15u) == 0;
+  p.vec_b = b.mode == OM_CONTIG && (reinterpret_cast<uintptr_t>(b.base) & 15u) == 0;
+  const int per_site = KIND == PK_TRACE ? 9 : KIND == PK_PP ? (sizeof(R) == 4 ? 6 : 12) : 24;
+  const long long total = (long long)n * per_site;
   long long grid = (total + 255) / 256;
   const long long cap = (long long)device_sm_count() * 16;
   if (grid > cap) grid = cap;
-  prop_kernel<R, KIND, CA, CB><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, current_stream()>>>(p);
+  const unsigned gr = (unsigned)(grid < 1 ? 1 : grid);
+  cudaStream_t st = current_stream();
+  if constexpr (KIND == PK_TRACE)
+    prop_trace_kernel<R><<<gr, 256, 0, st>>>(p);
+  else if constexpr (KIND == PK_MP)
+    prop_mp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+  else if constexpr (KIND == PK_PM)
+    prop_pm_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+  else
+    prop_pp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
   check_launch(kid);
 }
 
