@@ -429,6 +429,18 @@ def run_gpu_arm(args):
         r, it, el, kind, threads = cpu_chain_rate(xs, ps, a_vals, budget_s=args.cpu_seconds)
         cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{it} chain iterations on the full {n}-site field ({el:.1f} s)"}
+        if kind == "reference":
+            # the same chain on one host thread (the reference's OpenMP
+            # runtime set to one thread for this sample, then restored)
+            try:
+                gomp = ctypes.CDLL("libgomp.so.1")
+                gomp.omp_set_num_threads(1)
+                r1, it1, el1, _, _ = cpu_chain_rate(xs, ps, a_vals, budget_s=min(5.0, args.cpu_seconds))
+                gomp.omp_set_num_threads(threads)
+                cpu["single_thread"] = {"value": r1, "unit": UNIT,
+                                        "sample": f"{it1} chain iterations ({el1:.1f} s)"}
+            except OSError:
+                pass
 
     if rank == 0:
         line = {
