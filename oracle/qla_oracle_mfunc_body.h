@@ -697,6 +697,229 @@ static void FN(eig3)(FN(mc) *v, const FN(mc) *m)
   v[2].re = s1.re + e2.re; v[2].im = s1.im + e2.im;
 }
 
+/* ------------------------------------------- eigenvalues, nc > 3 (QR) */
+/* 2x2 eigenvalues used when the QR iteration deflates a 2x2 block: the
+ * Hermitian form (V_eq_eigenvalsH_M.c:82-104) and the general complex form
+ * (V_eq_eigenvals_M.c:82-125, the "more accurate" branch) */
+static void FN(eig2_h)(FN(mc) *v0, FN(mc) *v1, const FN(mc) *m00, const FN(mc) *m01, const FN(mc) *m10,
+                       const FN(mc) *m11)
+{
+  R tr, det;
+  det = m00->re*m11->re - m00->im*m11->im;
+  det -= (m01->re*m10->re - m01->im*m10->im);
+  tr = m00->re + m11->re;
+  if (det == 0) {
+    v0->re = 0; v0->im = 0.;
+    v1->re = tr; v1->im = 0.;
+  } else {
+    R ss = 0.5*tr;
+    R d = ss*ss - det;
+    R sd = M_SQRT(M_FABS(d));
+    R l0, l1 = ss + M_COPYSIGN(sd, ss);
+    l0 = det / l1;
+    v0->re = l0; v0->im = 0.;
+    v1->re = l1; v1->im = 0.;
+  }
+}
+
+static void FN(cdiv)(FN(mc) *c, FN(mc) a, FN(mc) b)    /* QLA_c_eq_c_div_c */
+{
+  R t = 1.0/(b.re*b.re + b.im*b.im);
+  c->re = (a.re*b.re + a.im*b.im)*t;
+  c->im = (a.im*b.re - a.re*b.im)*t;
+}
+
+static void FN(eig2_g)(FN(mc) *v0, FN(mc) *v1, const FN(mc) *m00, const FN(mc) *m01, const FN(mc) *m10,
+                       const FN(mc) *m11)
+{
+  FN(mc) tr, det;
+  CMUL(det, *m00, *m11);
+  CMMS(det, *m01, *m10);
+  tr.re = m00->re + m11->re; tr.im = m00->im + m11->im;
+  if (det.re == 0 && det.im == 0) {
+    v0->re = 0; v0->im = 0.;
+    *v1 = tr;
+  } else {
+    FN(mc) ss, d, sd;
+    ss.re = 0.5*tr.re; ss.im = 0.5*tr.im;
+    CMUL(d, ss, ss);
+    d.re -= det.re; d.im -= det.im;
+    sd = FN(csqrt)(d);
+    R ts = ss.re*sd.re + ss.im*sd.im;
+    if (ts >= 0) { v1->re = ss.re + sd.re; v1->im = ss.im + sd.im; }
+    else { v1->re = ss.re - sd.re; v1->im = ss.im - sd.im; }
+    FN(cdiv)(v0, det, *v1);
+  }
+}
+
+/* Hessenberg reduction with pivoting through a row/column permutation
+ * (V_eq_eigenvalsH_M.c:195-245, identical in V_eq_eigenvals_M.c), then the
+ * implicit double-shift QR iteration (V_eq_eigenvalsH_M.c:315-483).  The
+ * template's iteration has no overall bound (after 100 iterations on one
+ * eigenvalue it writes the diagonal and starts over); here a search for one
+ * eigenvalue gives up after ORA_QR_MAXITS restarts, leaving that diagonal. */
+#define ORA_QR_MAXITS 20
+static void FN(eig_qr)(FN(mc) *v, const FN(mc) *a, int nc, int herm)
+{
+  FN(mc) mm[ORA_NCMAX * ORA_NCMAX], h[ORA_NCMAX * ORA_NCMAX];
+  int rc[ORA_NCMAX];
+  for (int i = 0; i < nc; i++) {
+    for (int j = 0; j < nc; j++) mm[i * nc + j] = a[i * nc + j];
+    rc[i] = i;
+  }
+#define MP(i, j) mm[rc[i] * nc + rc[j]]
+  for (int k = 0; k < nc - 2; k++) {
+    FN(mc) sk;
+    R rmax = MP(k + 1, k).re*MP(k + 1, k).re + MP(k + 1, k).im*MP(k + 1, k).im;
+    int imax = k + 1;
+    for (int i = k + 2; i < nc; i++) {
+      R n2 = MP(i, k).re*MP(i, k).re + MP(i, k).im*MP(i, k).im;
+      if (n2 > rmax) { rmax = n2; imax = i; }
+    }
+    if (rmax == 0) continue;
+    { int rk = rc[k + 1]; rc[k + 1] = rc[imax]; rc[imax] = rk; }
+    rmax = 1/rmax;
+    sk.re = rmax*MP(k + 1, k).re; sk.im = -(rmax*MP(k + 1, k).im);   /* QLA_c_eq_r_times_ca */
+    for (int i = k + 2; i < nc; i++) {
+      FN(mc) t;
+      CMUL(t, sk, MP(i, k));
+      MP(i, k).re = 0; MP(i, k).im = 0.;
+      for (int j = k + 1; j < nc; j++) CMMS(MP(i, j), t, MP(k + 1, j));
+      for (int j = 0; j < nc; j++) CPMS(MP(j, k + 1), t, MP(j, i));
+    }
+  }
+  for (int i = 0; i < nc; i++)
+    for (int j = 0; j < nc; j++) h[i * nc + j] = MP(i, j);
+#undef MP
+#define MH(i, j) h[(i) * nc + (j)]
+#define CABS(z) M_SQRT((z).re*(z).re + (z).im*(z).im)
+#define CNORM2(z) ((z).re*(z).re + (z).im*(z).im)
+  R anorm = 0;
+  for (int i = 0; i < nc; i++)
+    for (int j = (i == 0 ? 0 : i - 1); j < nc; j++) anorm += CABS(MH(i, j));
+  int nn = nc - 1, restarts = 0;
+  FN(mc) t; t.re = 0; t.im = 0.;
+  while (nn >= 0) {
+    int l, its = 0;
+    do {
+      for (l = nn; l > 0; l--) {
+        R s = CABS(MH(l - 1, l - 1)) + CABS(MH(l, l));
+        if (s == 0) s = anorm;
+        R o = CABS(MH(l, l - 1));
+        if (s + o == s) { MH(l, l - 1).re = 0; MH(l, l - 1).im = 0.; break; }
+      }
+      FN(mc) x = MH(nn, nn);
+      if (l == nn) {
+        v[nn].re = x.re + t.re; v[nn].im = x.im + t.im;
+        nn--;
+      } else if (l == nn - 1) {
+        if (herm) FN(eig2_h)(&v[nn - 1], &v[nn], &MH(nn - 1, nn - 1), &MH(nn - 1, nn), &MH(nn, nn - 1), &x);
+        else FN(eig2_g)(&v[nn - 1], &v[nn], &MH(nn - 1, nn - 1), &MH(nn - 1, nn), &MH(nn, nn - 1), &x);
+        v[nn - 1].re += t.re; v[nn - 1].im += t.im;
+        v[nn].re += t.re; v[nn].im += t.im;
+        nn -= 2;
+      } else {
+        if (its >= 100) {
+          for (int i = 0; i <= nn; i++) { v[i].re = MH(i, i).re + t.re; v[i].im = MH(i, i).im + t.im; }
+          break;
+        }
+        FN(mc) y, w, p, q, r;
+        y = MH(nn - 1, nn - 1);
+        CMUL(w, MH(nn, nn - 1), MH(nn - 1, nn));
+        if (its == 10 || its == 20) {
+          t.re += x.re; t.im += x.im;
+          for (int i = 0; i < nn; i++) { MH(i, i).re -= x.re; MH(i, i).im -= x.im; }
+          MH(nn, nn).re = 0; MH(nn, nn).im = 0.;
+          x.re = 0; x.im = 0.;
+          y = MH(nn - 1, nn - 1);
+          R s = CABS(MH(nn, nn - 1)) + CABS(MH(nn - 1, nn - 2));
+          x.re = 0.75*s; x.im = 0.;
+          y = x;
+          w.re = -0.4375*s*s; w.im = 0.;
+        }
+        its++;
+        int m = l;
+        {
+          FN(mc) rr, ss, t1, z = MH(m, m);
+          rr.re = x.re - z.re; rr.im = x.im - z.im;
+          ss.re = y.re - z.re; ss.im = y.im - z.im;
+          CMUL(p, rr, ss);
+          p.re -= w.re; p.im -= w.im;
+          CPMS(p, MH(m + 1, m), MH(m, m + 1));
+          t1.re = MH(m + 1, m + 1).re - z.re; t1.im = MH(m + 1, m + 1).im - z.im;
+          t1.re -= rr.re + ss.re; t1.im -= rr.im + ss.im;
+          CMUL(q, MH(m + 1, m), t1);
+          CMUL(r, MH(m + 1, m), MH(m + 2, m + 1));
+        }
+        for (int k = m; k < nn; k++) {
+          R xx = 0;
+          if (k != m) {
+            p = MH(k, k - 1);
+            q = MH(k + 1, k - 1);
+            r.re = 0; r.im = 0.;
+            if (k + 1 != nn) r = MH(k + 2, k - 1);
+            xx = CABS(p) + CABS(q) + CABS(r);
+            if (xx != 0) {
+              R xxi = 1/xx;
+              p.re = xxi*p.re; p.im = xxi*p.im;
+              q.re = xxi*q.re; q.im = xxi*q.im;
+              r.re = xxi*r.re; r.im = xxi*r.im;
+            }
+          }
+          R p2 = CNORM2(p);
+          R s2 = p2 + CNORM2(q) + CNORM2(r);
+          if (s2 != 0) {
+            FN(mc) sv, t1;
+            if (p2 > 0) { sv.re = (sqrt(s2/p2))*p.re; sv.im = (sqrt(s2/p2))*p.im; }
+            else { sv.re = sqrt(s2); sv.im = 0.; }
+            if (k == m) {
+              if (l != m) { MH(k, k - 1).re = -MH(k, k - 1).re; MH(k, k - 1).im = -MH(k, k - 1).im; }
+            } else {
+              MH(k, k - 1).re = (-xx)*sv.re; MH(k, k - 1).im = (-xx)*sv.im;
+              MH(k + 1, k - 1).re = 0; MH(k + 1, k - 1).im = 0.;
+              if (k + 2 < nc) { MH(k + 2, k - 1).re = 0; MH(k + 2, k - 1).im = 0.; }
+            }
+            p.re += sv.re; p.im += sv.im;
+            FN(cdiv)(&x, p, sv);
+            FN(cdiv)(&y, q, sv);
+            FN(cdiv)(&w, r, sv);
+            FN(cdiv)(&t1, q, p); q = t1;
+            FN(cdiv)(&t1, r, p); r = t1;
+            for (int j = k; j <= nn; j++) {
+              p = MH(k, j);
+              p.re += q.re*MH(k + 1, j).re + q.im*MH(k + 1, j).im;   /* += conj(q) M */
+              p.im += q.re*MH(k + 1, j).im - q.im*MH(k + 1, j).re;
+              if (k + 1 != nn) {
+                p.re += r.re*MH(k + 2, j).re + r.im*MH(k + 2, j).im;
+                p.im += r.re*MH(k + 2, j).im - r.im*MH(k + 2, j).re;
+                CMMS(MH(k + 2, j), p, w);
+              }
+              CMMS(MH(k + 1, j), p, y);
+              CMMS(MH(k, j), p, x);
+            }
+            for (int i = l; i <= (nn < k + 3 ? nn : k + 3); i++) {
+              CMUL(p, x, MH(i, k));
+              CPMS(p, y, MH(i, k + 1));
+              if (k + 1 != nn) {
+                CPMS(p, w, MH(i, k + 2));
+                MH(i, k + 2).re -= p.re*r.re + p.im*r.im;             /* -= p conj(r) */
+                MH(i, k + 2).im -= p.im*r.re - p.re*r.im;
+              }
+              MH(i, k + 1).re -= p.re*q.re + p.im*q.im;
+              MH(i, k + 1).im -= p.im*q.re - p.re*q.im;
+              MH(i, k).re -= p.re; MH(i, k).im -= p.im;
+            }
+          }
+        }
+      }
+    } while (l + 1 < nn);
+    if (its >= 100 && ++restarts >= ORA_QR_MAXITS) break;
+  }
+#undef MH
+#undef CABS
+#undef CNORM2
+}
+
 /* x = a^-1 b for b with nb columns (a ColorVector: nb = 1; a ColorMatrix:
  * nb = nc): V_eq_M_inverse_V.c:84-126 for nc = 3 and nb = 1 (Cramer's
  * rule), else Gauss-Jordan (V_eq_M_inverse_V.c:128-168, M_eq_M_inverse_M.c:85-135) */
@@ -739,14 +962,12 @@ static void FN(minv1)(FN(mc) *x, const FN(mc) *a, const FN(mc) *b, int nc, int n
 /* r[i] = f(a[i]); eigenvalue functions write nc complex numbers per site,
  * det one.  The closed nc = 3 forms exist only for nc == 3; other colour
  * counts take the templates' generic paths (expA / expTA: the exp path;
- * sqrtPH / invsqrtPH: the Newton paths).  Returns -1 for an eigenvalue
- * request at nc != 3 (the QR path is not restated). */
+ * sqrtPH / invsqrtPH: the Newton paths; eigenvalues: Hessenberg + QR). */
 int FN(ora_mfunc)(R *r, const R *a, long n, int nc, int which)
 {
   const FN(mc) *A = (const FN(mc) *)a;
   FN(mc) *O = (FN(mc) *)r;
   const double eps = sizeof(R) == 4 ? (double)FLT_EPSILON : DBL_EPSILON;
-  if ((which == ORA_MF_EIGENVALS || which == ORA_MF_EIGENVALSH) && nc != 3) return -1;
   for (long i = 0; i < n; i++) {
     const FN(mc) *ai = A + i * nc * nc;
     FN(mc) *oi = O + i * nc * nc;
@@ -769,8 +990,12 @@ int FN(ora_mfunc)(R *r, const R *a, long n, int nc, int which)
     case ORA_MF_INVSQRTPH:
       if (nc == 3) FN(sqrtph3)(oi, ai, 1); else FN(invsqrt1)(oi, ai, nc, eps);
       break;
-    case ORA_MF_EIGENVALS: FN(eig3)(O + i * 3, ai); break;
-    case ORA_MF_EIGENVALSH: FN(eigh3)(O + i * 3, ai); break;
+    case ORA_MF_EIGENVALS:
+      if (nc == 3) FN(eig3)(O + i * 3, ai); else FN(eig_qr)(O + i * nc, ai, nc, 0);
+      break;
+    case ORA_MF_EIGENVALSH:
+      if (nc == 3) FN(eigh3)(O + i * 3, ai); else FN(eig_qr)(O + i * nc, ai, nc, 1);
+      break;
     default: return -1;
     }
   }

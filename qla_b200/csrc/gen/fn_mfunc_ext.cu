@@ -62,14 +62,18 @@ QLAB_EXPORT void QLA_FN_M_veq_invsqrtPH_M(int nc, void * r, void * a, int n) {
 QLAB_EXPORT void QLA_FN_V_veq_eigenvals_M(int nc, void * r, void * a, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsOp<float>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvals_M", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, false>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, false>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvals_M", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_eigenvalsH_M(int nc, void * r, void * a, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsHOp<float>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvalsH_M", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, true>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, true>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvalsH_M", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
@@ -130,14 +134,18 @@ QLAB_EXPORT void QLA_FN_M_veq_invsqrtPH_pM(int nc, void * r, void * a, int n) {
 QLAB_EXPORT void QLA_FN_V_veq_eigenvals_pM(int nc, void * r, void * a, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsOp<float>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvals_pM", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, false>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, false>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvals_pM", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_eigenvalsH_pM(int nc, void * r, void * a, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsHOp<float>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvalsH_pM", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, true>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, true>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_veq_eigenvalsH_pM", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
@@ -270,14 +278,18 @@ QLAB_EXPORT void QLA_FN_M_xeq_invsqrtPH_M(int nc, void * r, void * a, int * inde
 QLAB_EXPORT void QLA_FN_V_xeq_eigenvals_M(int nc, void * r, void * a, int * index, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsOp<float>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvals_M", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, false>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, false>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvals_M", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_eigenvalsH_M(int nc, void * r, void * a, int * index, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsHOp<float>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvalsH_M", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, true>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, true>>("FN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvalsH_M", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
@@ -338,14 +350,18 @@ QLAB_EXPORT void QLA_FN_M_xeq_invsqrtPH_pM(int nc, void * r, void * a, int * ind
 QLAB_EXPORT void QLA_FN_V_xeq_eigenvals_pM(int nc, void * r, void * a, int * index, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsOp<float>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvals_pM", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, false>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, false>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvals_pM", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_eigenvalsH_pM(int nc, void * r, void * a, int * index, int n) {
   switch (nc) {
     case 3: qlab::api_map<qlab::EigenvalsHOp<float>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
-    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvalsH_pM", "nc not compiled (supported: 3)");
+    case 4: qlab::api_map<qlab::GenEigenOp<float, 4, true>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::GenEigenOp<float, 8, true>>("FN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_FN_V_xeq_eigenvalsH_pM", "nc not compiled (supported: 3, 4, 8)");
   }
 }
 

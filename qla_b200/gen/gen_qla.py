@@ -230,13 +230,13 @@ def gen_fn():
                 add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
                     _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["mfunc_ext"],
                     dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
-            for fname, opn in (("eigenvals", "EigenvalsOp"), ("eigenvalsH", "EigenvalsHOp")):
+            for fname, opn, herm in (("eigenvals", "EigenvalsOp", "false"), ("eigenvalsH", "EigenvalsHOp", "true")):
                 name = f"QLA_FN_V_{var}eq_{fname}_{src}"
-                call = lambda nc, opn=opn, p1=p1, gang=gang: (
-                    f"qlab::api_map<qlab::{opn}<{R}>>({kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
-                    f"{gang}, n, qlab::EQ);")
+                call = lambda nc, opn=opn, herm=herm, p1=p1, gang=gang: (
+                    f"qlab::api_map<qlab::{opn + '<' + R + '>' if nc == 3 else f'GenEigenOp<{R}, {nc}, {herm}>'}>("
+                    f"{kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, {gang}, n, qlab::EQ);")
                 add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
-                    _fn_switch([3], call, name), "mfunc_ext", CITE["mfunc_ext"],
+                    _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["mfunc_ext"],
                     dict(dest="V", eqop="eq", var=var, a=src, fn=fname))
         for T_ in ("V", "M"):
             for s1, p1 in (("M", False), ("pM", True)):

@@ -252,6 +252,16 @@ def build(pc, dt, seed):
         call(f"QLA_{pc}_{dest}_veq_M_inverse_{dest}", ctypes.c_void_p(r.ctypes.data),
              ctypes.c_void_p(ins["mf_gen"].ctypes.data), ctypes.c_void_p(ins["r0" + dest].ctypes.data), N)
         out[f"QLA_{pc}_{dest}_veq_M_inverse_{dest}|mf_gen|r0{dest}"] = r
+    # the N-colour build's generic paths at nc = 4, 8: Newton invsqrt, log and
+    # the Hessenberg + QR eigenvalues
+    for nc in (4, 8):
+        ins[f"mfN{nc}_herm"] = T.hermitian_inputs(rng, N, dt, nc=nc)
+        for fname, src in (("M_veq_invsqrt_M", "pos"), ("M_veq_log_M", "pos"), ("V_veq_eigenvals_M", "gen"),
+                           ("V_veq_eigenvalsH_M", "herm")):
+            r = np.zeros((N, 2 * nc * (1 if fname.startswith("V") else nc)), dtype=dt)
+            call(f"QLA_{npc}_{fname}", nc, ctypes.c_void_p(r.ctypes.data),
+                 ctypes.c_void_p(ins[f"mfN{nc}_{src}"].ctypes.data), N)
+            out[f"QLA_{npc}_{fname}|mfN{nc}_{src}"] = r
     return ins, out
 
 

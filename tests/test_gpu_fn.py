@@ -122,16 +122,17 @@ def test_fn_remaining_matrix_functions(qla, nc):
     |A|_F on the diagonal).  expA / expTA / sqrtPH / invsqrtPH take the exp and
     Newton paths at nc != 3 (bit-identical) and the FP64 closed forms at
     nc = 3 (the F3 tolerance: FP32 test rule against the FP64 value of the
-    promoted input); eigenvalues exist at nc = 3."""
+    promoted input); eigenvalues take the closed forms at nc = 3 and the
+    templates' Hessenberg + double-shift QR path (bit-identical) otherwise."""
     rng = np.random.default_rng(80 + nc)
     n = 2053 if nc < 8 else 521
     gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(np.float32)
     pos = T.positive_hermitian_inputs(rng, n, np.float32, nc=nc)
     z = T.to_complex(gen.astype(np.float64), nc)
     ah = T.from_complex(0.5 * (z - np.conj(np.transpose(z, (0, 2, 1)))), np.float32)
-    cases = [("invsqrt", pos), ("log", pos), ("expA", ah), ("expTA", ah), ("sqrtPH", pos), ("invsqrtPH", pos)]
-    if nc == 3:
-        cases += [("eigenvalsH", pos), ("eigenvals", gen)]
+    herm = T.hermitian_inputs(rng, n, np.float32, nc=nc)
+    cases = [("invsqrt", pos), ("log", pos), ("expA", ah), ("expTA", ah), ("sqrtPH", pos), ("invsqrtPH", pos),
+             ("eigenvalsH", pos), ("eigenvalsH", herm), ("eigenvals", gen)]
     for fname, src in cases:
         nout = nc if fname.startswith("eigen") else nc * nc
         dest = "V" if fname.startswith("eigen") else "M"

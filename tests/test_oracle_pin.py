@@ -141,9 +141,11 @@ def replay(pc, name, ins):
         src = extra[0]
         nc = 3 if pcx in ("F3", "D3") else int(src[3])
         return T.ora_mfunc(ins[src], n, fname, nc=nc)
-    m = re.match(r"QLA_(F3|D3)_(M|V)_veq_(invsqrt|log|expA|expTA|sqrtPH|invsqrtPH|eigenvals|eigenvalsH)_M$", key)
+    m = re.match(r"QLA_(F3|D3|FN|DN)_(M|V)_veq_(invsqrt|log|expA|expTA|sqrtPH|invsqrtPH|eigenvals|eigenvalsH)_M$", key)
     if m:
-        return T.ora_mfunc(ins[extra[0]], n, m.group(3))
+        src = extra[0]
+        nc = 3 if m.group(1) in ("F3", "D3") else int(src[3])
+        return T.ora_mfunc(ins[src], n, m.group(3), nc=nc)
     m = re.match(r"QLA_(F3|D3)_(V|M)_veq_M_inverse_(V|M)$", key)
     if m:
         return T.ora_minv(ins[extra[0]], ins[extra[1]], n, 1 if m.group(2) == "V" else 3)
@@ -285,3 +287,28 @@ def test_oracle_matrix_functions_match_reference_library(pc, dt):
         rr = np.zeros((n, 6 * nb), dt)
         getattr(R, f"QLA_{pc}_{dest}_veq_M_inverse_{dest}")(T.ptr(rr), T.ptr(gen), T.ptr(b), n)
         assert T.bits_equal(rr, T.ora_minv(gen, b, n, nb)), dest
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("pc,dt", [("FN", np.float32), ("DN", np.float64)])
+def test_oracle_n_colour_matrix_functions_match_reference_library(pc, dt):
+    """The N-colour build's generic paths (Newton invsqrt, log, a^-1 b, and
+    the Hessenberg + double-shift QR eigenvalues) at nc = 4 and 8, bit for bit."""
+    rng = np.random.default_rng(80)
+    n = 1000
+    R = T.ref()
+    for nc in (4, 8):
+        g = rng.standard_normal((n, 2 * nc * nc)).astype(dt)
+        pos = T.positive_hermitian_inputs(rng, n, dt, nc=nc)
+        herm = T.hermitian_inputs(rng, n, dt, nc=nc)
+        for fname, a in (("invsqrt", pos), ("log", pos), ("eigenvals", g), ("eigenvals", herm),
+                         ("eigenvalsH", herm), ("eigenvalsH", pos)):
+            dest = "V" if fname.startswith("eigen") else "M"
+            rr = np.zeros((n, 2 * nc * (1 if dest == "V" else nc)), dt)
+            getattr(R, f"QLA_{pc}_{dest}_veq_{fname}_M")(nc, T.ptr(rr), T.ptr(a), n)
+            assert T.bits_equal(rr, T.ora_mfunc(a, n, fname, nc=nc)), (nc, fname)
+        for dest, nb in (("V", 1), ("M", nc)):
+            b = rng.standard_normal((n, 2 * nc * nb)).astype(dt)
+            rr = np.zeros((n, 2 * nc * nb), dt)
+            getattr(R, f"QLA_{pc}_{dest}_veq_M_inverse_{dest}")(nc, T.ptr(rr), T.ptr(g), T.ptr(b), n)
+            assert T.bits_equal(rr, T.ora_minv(g, b, n, nb, nc=nc)), (nc, dest)
