@@ -739,6 +739,38 @@ def run_workload(args):
             torch.cuda.empty_cache()
         out.update({"metric": "DiracPropagator products and spin trace on 16^3x32 sites", "unit": "site-updates/s",
                     "value": res["F3_P_veq_M_times_P"]["site_updates_per_s"], "ops": res})
+    elif args.workload == "ewise":
+        # element-wise families and site-local products on 32^3x64 sites
+        n = 32 * 32 * 32 * 64
+        res = {}
+        for pc, dt, e in (("F3", torch.float32, 4), ("D3", torch.float64, 8)):
+            D = lambda: torch.randn(n, 24, device="cuda", dtype=dt)  # noqa: E731
+            x, y, z = D(), D(), D()
+            m1, m2 = torch.randn(n, 18, device="cuda", dtype=dt), torch.randn(n, 18, device="cuda", dtype=dt)
+            cf = torch.randn(n, 2, device="cuda", dtype=dt)
+            cs = torch.tensor([0.3, -0.7], device="cuda", dtype=dt)
+            ps = torch.randn(n // 8, 288, device="cuda", dtype=dt)
+            pr = torch.empty_like(ps)
+            rr = torch.empty(n // 8, device="cuda", dtype=dt)
+            table = [("D_vpeq_c_times_D", (x, cs, y), n, 288),
+                     ("D_veq_c_times_D_plus_D", (z, cs, x, y), n, 288),
+                     ("D_veq_C_times_D", (z, cf, x), n, 200),
+                     ("M_veq_Ca_times_Ma", (m1, cf, m2), n, 152),
+                     ("C_vpeq_D_dot_D", (cf, x, y), n, 208),
+                     ("P_veq_c_times_P", (pr, cs, ps), n // 8, 2304),
+                     ("R_veq_norm2_P", (rr, ps), n // 8, 1156)]
+            for nm, targs, nn, nb in table:
+                f = getattr(L, f"QLA_{pc}_{nm}")
+                call = (lambda f=f, targs=targs, nn=nn: f(*[V(t) for t in targs], nn))
+                ms = _events_time(torch, stream, call, reps)
+                gbs = nb * (e // 4) * nn / (ms / 1e3) / 1e9
+                res[f"{pc}_{nm}"] = {"site_updates_per_s": nn / (ms / 1e3), "us": 1e3 * ms, "gbs": gbs,
+                                     "hbm_frac": gbs / peak}
+            qla.check("ewise")
+            del x, y, z, m1, m2, cf, ps, pr, rr
+            torch.cuda.empty_cache()
+        out.update({"metric": "element-wise families and site-local products, 32^3x64 sites (P: 1/8 of the sites)",
+                    "unit": "site-updates/s", "value": res["F3_D_vpeq_c_times_D"]["site_updates_per_s"], "ops": res})
     elif args.workload == "config1":
         n = 16 ** 4
         res = {}
@@ -786,7 +818,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the reduction accuracy check")
-    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "prop", "config1"],
+    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "prop", "ewise", "config1"],
                     help="cg_chain is the benchmark line; the others measure the remaining configurations")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

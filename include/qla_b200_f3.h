@@ -2960,6 +2960,3756 @@ void QLA_F3_c_xeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatr
 /* ---- redot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
 /* replaces QLA_F3_r_xeq_re_pM_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
 void QLA_F3_r_xeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* ---- ewise_v: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1335 (constant multiples of a field) */
+/* replaces QLA_F3_V_veq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_veq_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_veq_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veq_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veq_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_veq_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veq_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_veq_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veq_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_veq_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veq_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_vpeq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_vpeq_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_vpeq_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vpeq_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vpeq_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vpeq_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vpeq_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_vpeq_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vpeq_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_vpeq_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vpeq_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_vpeq_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vpeq_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_vmeq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_vmeq_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_vmeq_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_vmeq_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_vmeq_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_vmeq_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vmeq_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_vmeq_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vmeq_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_vmeq_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vmeq_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_vmeq_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_vmeq_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_veqm_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_veqm_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_veqm_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veqm_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_veqm_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veqm_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veqm_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_veqm_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veqm_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_veqm_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veqm_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_V_veqm_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_veqm_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_V_veq_V_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_V_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_r_times_V_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_V_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_c_times_V_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_V_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_V_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_V_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_r_times_V_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_V_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_c_times_V_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_V_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_V_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_V_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_r_times_V_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_V_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_c_times_V_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_V_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_V_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_V_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_r_times_V_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_V_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_c_times_V_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_V_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_pV_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_pV_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_r_times_pV_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_pV_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_c_times_pV_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_pV_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_pV_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_pV_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_V_veq_r_times_pV_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_pV_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_c_times_pV_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_pV_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_V_veq_pV_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_pV_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_r_times_pV_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_pV_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_c_times_pV_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_pV_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_pV_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_pV_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_V_veq_r_times_pV_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_r_times_pV_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_veq_c_times_pV_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_veq_c_times_pV_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_V_xeq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xeq_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xeq_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeq_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeq_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xeq_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeq_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xeq_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeq_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xeq_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeq_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xpeq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xpeq_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xpeq_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xpeq_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xpeq_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xpeq_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xpeq_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xpeq_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xpeq_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xpeq_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xpeq_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xpeq_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xmeq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xmeq_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xmeq_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xmeq_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xmeq_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xmeq_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xmeq_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xmeq_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xmeq_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xmeq_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xmeq_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xmeq_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xeqm_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xeqm_c_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_c_times_pV (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_V_xeqm_c_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_C_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_C_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_C_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_C_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pC_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_pC_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pC_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_pC_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_Ca_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_Ca_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_Ca_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_Ca_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pCa_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_pCa_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pCa_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_pCa_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_R_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_R_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_R_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_R_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pR_times_V (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_pR_times_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_pR_times_pV (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_V_xeqm_pR_times_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeqm_conj_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeqm_conj_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xeqm_conj_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeqm_conj_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xeqm_i_V (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeqm_i_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_V_xeqm_i_pV (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_V_xeqm_i_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_V_xeq_V_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_V_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_V_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_V_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_V_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_V_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_V_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_V_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_V_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_V_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_V_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_V_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_V_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_V_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_V_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_V_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_V_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_V_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_V_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_V_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_V_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_V_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_V_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_V_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_pV_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_pV_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_pV_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_pV_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_pV_plus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_pV_plus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_pV_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_pV_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_pV_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_pV_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_pV_minus_V (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_pV_minus_V(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_V_xeq_pV_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_pV_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_pV_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_pV_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_pV_plus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_pV_plus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_pV_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_pV_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_V_xeq_r_times_pV_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_r_times_pV_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_V_xeq_c_times_pV_minus_pV (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_V_xeq_c_times_pV_minus_pV(QLA_F3_ColorVector *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, QLA_F3_ColorVector *QLA_B200_RESTRICT * c, int * index, int n);
+/* ---- ewise_h: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1335 (constant multiples of a field) */
+/* replaces QLA_F3_H_veq_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_veq_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_veq_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veq_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veq_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_veq_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veq_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_veq_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veq_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_veq_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veq_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_vpeq_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_vpeq_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_vpeq_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vpeq_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vpeq_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vpeq_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vpeq_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_vpeq_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vpeq_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_vpeq_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vpeq_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_vpeq_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vpeq_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_vmeq_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_vmeq_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_vmeq_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_vmeq_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_vmeq_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_vmeq_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vmeq_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_vmeq_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vmeq_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_vmeq_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vmeq_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_vmeq_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_vmeq_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_veqm_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_veqm_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_veqm_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veqm_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_veqm_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veqm_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veqm_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_veqm_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veqm_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_veqm_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veqm_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_H_veqm_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_veqm_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_H_veq_H_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_H_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_r_times_H_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_H_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_c_times_H_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_H_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_H_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_H_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_r_times_H_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_H_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_c_times_H_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_H_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_H_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_H_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_r_times_H_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_H_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_c_times_H_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_H_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_H_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_H_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_r_times_H_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_H_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_c_times_H_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_H_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_pH_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_pH_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_r_times_pH_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_pH_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_c_times_pH_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_pH_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_pH_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_pH_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_H_veq_r_times_pH_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_pH_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_c_times_pH_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_pH_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_H_veq_pH_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_pH_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_r_times_pH_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_pH_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_c_times_pH_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_pH_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_pH_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_pH_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_H_veq_r_times_pH_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_r_times_pH_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_veq_c_times_pH_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_veq_c_times_pH_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_H_xeq_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xeq_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xeq_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeq_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeq_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xeq_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeq_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xeq_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeq_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xeq_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeq_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xpeq_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xpeq_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xpeq_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xpeq_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xpeq_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xpeq_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xpeq_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xpeq_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xpeq_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xpeq_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xpeq_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xpeq_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xmeq_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xmeq_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xmeq_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xmeq_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xmeq_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xmeq_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xmeq_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xmeq_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xmeq_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xmeq_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xmeq_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xmeq_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xeqm_c_times_H (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xeqm_c_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_c_times_pH (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_H_xeqm_c_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_C_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_C_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_C_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_C_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pC_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_pC_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pC_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_pC_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_Ca_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_Ca_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_Ca_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_Ca_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pCa_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_pCa_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pCa_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_pCa_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_R_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_R_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_R_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_R_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pR_times_H (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_pR_times_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_pR_times_pH (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_H_xeqm_pR_times_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeqm_conj_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeqm_conj_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xeqm_conj_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeqm_conj_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xeqm_i_H (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeqm_i_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_H_xeqm_i_pH (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_H_xeqm_i_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_H_xeq_H_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_H_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_H_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_H_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_H_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_H_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_H_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_H_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_H_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_H_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_H_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_H_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_H_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_H_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_H_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_H_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_H_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_H_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_H_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_H_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_H_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_H_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_H_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_H_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_pH_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_pH_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_pH_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_pH_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_pH_plus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_pH_plus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_pH_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_pH_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_pH_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_pH_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_pH_minus_H (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_pH_minus_H(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_H_xeq_pH_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_pH_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_pH_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_pH_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_pH_plus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_pH_plus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_pH_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_pH_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_H_xeq_r_times_pH_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_r_times_pH_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_H_xeq_c_times_pH_minus_pH (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_H_xeq_c_times_pH_minus_pH(QLA_F3_HalfFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, QLA_F3_HalfFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* ---- ewise_d: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1335 (constant multiples of a field) */
+/* replaces QLA_F3_D_veq_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_veq_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_veq_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veq_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veq_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_veq_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veq_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_veq_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veq_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_veq_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veq_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_vpeq_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_vpeq_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_vpeq_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vpeq_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vpeq_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vpeq_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vpeq_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_vpeq_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vpeq_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_vpeq_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vpeq_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_vpeq_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vpeq_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_vmeq_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_vmeq_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_vmeq_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_vmeq_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_vmeq_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_vmeq_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vmeq_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_vmeq_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vmeq_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_vmeq_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vmeq_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_vmeq_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_vmeq_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_veqm_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_veqm_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_veqm_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veqm_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_veqm_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veqm_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veqm_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_veqm_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veqm_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_veqm_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veqm_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_D_veqm_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_veqm_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_D_veq_D_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_D_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_r_times_D_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_D_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_c_times_D_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_D_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_D_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_D_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_r_times_D_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_D_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_c_times_D_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_D_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_D_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_D_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_r_times_D_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_D_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_c_times_D_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_D_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_D_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_D_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_r_times_D_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_D_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_c_times_D_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_D_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_pD_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_pD_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_r_times_pD_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_pD_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_c_times_pD_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_pD_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_pD_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_pD_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_D_veq_r_times_pD_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_pD_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_c_times_pD_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_pD_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_D_veq_pD_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_pD_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_r_times_pD_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_pD_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_c_times_pD_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_pD_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_pD_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_pD_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_D_veq_r_times_pD_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_r_times_pD_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_veq_c_times_pD_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_veq_c_times_pD_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_D_xeq_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xeq_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xeq_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeq_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeq_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xeq_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeq_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xeq_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeq_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xeq_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeq_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xpeq_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xpeq_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xpeq_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xpeq_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xpeq_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xpeq_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xpeq_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xpeq_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xpeq_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xpeq_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xpeq_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xpeq_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xmeq_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xmeq_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xmeq_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xmeq_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xmeq_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xmeq_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xmeq_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xmeq_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xmeq_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xmeq_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xmeq_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xmeq_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xeqm_c_times_D (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xeqm_c_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_c_times_pD (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_D_xeqm_c_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_C_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_C_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_C_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_C_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pC_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_pC_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pC_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_pC_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_Ca_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_Ca_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_Ca_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_Ca_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pCa_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_pCa_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pCa_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_pCa_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_R_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_R_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_R_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_R_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pR_times_D (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_pR_times_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_pR_times_pD (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_D_xeqm_pR_times_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeqm_conj_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeqm_conj_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xeqm_conj_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeqm_conj_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xeqm_i_D (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeqm_i_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_D_xeqm_i_pD (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_D_xeqm_i_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_D_xeq_D_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_D_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_D_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_D_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_D_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_D_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_D_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_D_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_D_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_D_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_D_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_D_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_D_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_D_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_D_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_D_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_D_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_D_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_D_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_D_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_D_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_D_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_D_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_D_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_pD_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_pD_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_pD_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_pD_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_pD_plus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_pD_plus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_pD_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_pD_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_pD_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_pD_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_pD_minus_D (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_pD_minus_D(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_D_xeq_pD_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_pD_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_pD_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_pD_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_pD_plus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_pD_plus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_pD_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_pD_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_D_xeq_r_times_pD_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_r_times_pD_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_D_xeq_c_times_pD_minus_pD (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_D_xeq_c_times_pD_minus_pD(QLA_F3_DiracFermion *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, QLA_F3_DiracFermion *QLA_B200_RESTRICT * c, int * index, int n);
+/* ---- ewise_m: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1335 (constant multiples of a field) */
+/* replaces QLA_F3_M_veq_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veq_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veq_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veq_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veq_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veq_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veq_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veq_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veq_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veq_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veq_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veq_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veq_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vpeq_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vpeq_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vpeq_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vpeq_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vpeq_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vpeq_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vpeq_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vpeq_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vpeq_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vpeq_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vpeq_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vpeq_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vpeq_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vpeq_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vpeq_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vpeq_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vmeq_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vmeq_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vmeq_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vmeq_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vmeq_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vmeq_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_vmeq_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_vmeq_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vmeq_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vmeq_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vmeq_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vmeq_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vmeq_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_vmeq_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_vmeq_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_vmeq_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veqm_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veqm_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veqm_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veqm_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veqm_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veqm_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_veqm_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_veqm_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veqm_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veqm_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veqm_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veqm_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veqm_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veqm_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_M_veqm_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_veqm_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_M_veq_M_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_M_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_r_times_M_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_M_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_c_times_M_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_M_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_M_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_M_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_r_times_M_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_M_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_c_times_M_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_M_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_M_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_M_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_r_times_M_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_M_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_c_times_M_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_M_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_M_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_M_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_r_times_M_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_M_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_c_times_M_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_M_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_pM_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_pM_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_r_times_pM_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_pM_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_c_times_pM_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_pM_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_pM_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_pM_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_r_times_pM_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_pM_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_c_times_pM_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_pM_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_M_veq_pM_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_pM_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_r_times_pM_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_pM_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_c_times_pM_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_pM_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_pM_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_pM_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_r_times_pM_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_r_times_pM_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_veq_c_times_pM_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_veq_c_times_pM_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_M_xeq_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeq_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeq_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeq_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeq_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeq_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeq_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeq_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeq_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeq_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeq_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeq_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeq_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xpeq_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xpeq_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xpeq_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xpeq_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xpeq_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xpeq_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xpeq_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xpeq_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xpeq_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xmeq_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xmeq_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xmeq_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xmeq_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xmeq_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xmeq_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xmeq_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xmeq_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xmeq_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_c_times_M (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeqm_c_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_c_times_pM (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeqm_c_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_c_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeqm_c_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_r_times_Ma (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeqm_r_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_c_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeqm_c_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_r_times_pMa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_M_xeqm_r_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_C_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_C_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_C_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_C_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_C_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_C_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_C_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_C_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pC_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pC_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pC_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pC_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pC_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pC_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pC_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pC_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ca_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_Ca_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ca_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_Ca_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ca_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_Ca_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ca_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_Ca_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pCa_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pCa_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pCa_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pCa_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pCa_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pCa_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pCa_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pCa_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_R_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_R_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_R_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_R_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_R_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_R_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_R_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_R_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pR_times_M (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pR_times_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pR_times_pM (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pR_times_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pR_times_Ma (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pR_times_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pR_times_pMa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_M_xeqm_pR_times_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_conj_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_conj_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_conj_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_conj_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_i_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_i_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_i_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_i_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_Ma (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_Ma(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pMa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_pMa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_transpose_M (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_transpose_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_M_xeqm_transpose_pM (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_M_xeqm_transpose_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_M_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_M_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_M_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_M_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_M_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_M_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_M_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_M_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_M_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_M_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_M_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_M_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_M_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_M_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_M_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_M_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_M_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_M_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_M_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_M_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_M_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_pM_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_pM_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_pM_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_pM_plus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_pM_plus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_pM_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_pM_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_pM_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_pM_minus_M (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_pM_minus_M(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_pM_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_pM_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_pM_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_pM_plus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_pM_plus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_pM_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_pM_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_r_times_pM_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_r_times_pM_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_M_xeq_c_times_pM_minus_pM (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_M_xeq_c_times_pM_minus_pM(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * c, int * index, int n);
+/* ---- ewise_p: replaces the F3 functions emitted by lib/perl/build_qla.pl:1256-1335 (constant multiples of a field) */
+/* replaces QLA_F3_P_veq_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veq_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veq_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veq_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veq_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veq_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veq_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veq_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veq_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veq_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veq_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veq_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veq_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vpeq_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vpeq_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vpeq_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vpeq_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vpeq_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vpeq_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vpeq_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vpeq_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vpeq_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vpeq_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vpeq_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vpeq_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vpeq_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vpeq_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vpeq_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vmeq_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_vmeq_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_vmeq_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_vmeq_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_vmeq_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vmeq_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vmeq_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vmeq_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vmeq_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vmeq_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vmeq_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vmeq_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_vmeq_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_vmeq_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_vmeq_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veqm_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_veqm_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veqm_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_veqm_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veqm_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veqm_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veqm_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veqm_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veqm_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veqm_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veqm_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veqm_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veqm_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_P_veqm_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_veqm_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_P_veq_P_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_P_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_r_times_P_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_P_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_c_times_P_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_P_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_P_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_P_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_r_times_P_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_P_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_c_times_P_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_P_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_P_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_P_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_r_times_P_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_P_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_c_times_P_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_P_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_P_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_P_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_r_times_P_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_P_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_c_times_P_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_P_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_pP_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_pP_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_r_times_pP_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_pP_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_c_times_pP_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_pP_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_pP_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_pP_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_P_veq_r_times_pP_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_pP_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_c_times_pP_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_pP_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int n);
+/* replaces QLA_F3_P_veq_pP_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_pP_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_r_times_pP_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_pP_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_c_times_pP_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_pP_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_pP_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_pP_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_P_veq_r_times_pP_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_r_times_pP_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_veq_c_times_pP_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_veq_c_times_pP_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int n);
+/* replaces QLA_F3_P_xeq_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeq_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeq_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeq_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeq_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeq_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeq_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeq_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeq_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeq_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeq_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeq_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeq_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xpeq_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xpeq_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xpeq_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xpeq_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xpeq_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xmeq_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xmeq_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xmeq_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xmeq_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xmeq_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_c_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_c_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_r_times_P (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_r_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_c_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_c_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_r_times_pP (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_r_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_c_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_c_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_r_times_Pa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_r_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_c_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_c_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_r_times_pPa (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
+void QLA_F3_P_xeqm_r_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_C_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_C_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_C_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_C_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_C_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_C_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_C_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_C_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pC_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pC_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pC_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pC_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pC_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pC_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pC_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pC_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_Ca_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_Ca_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_Ca_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_Ca_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_Ca_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_Ca_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_Ca_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_Ca_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pCa_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pCa_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pCa_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pCa_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pCa_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pCa_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pCa_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pCa_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_R_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_R_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_R_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_R_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_R_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_R_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_R_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_R_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pR_times_P (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pR_times_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pR_times_pP (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pR_times_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pR_times_Pa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pR_times_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pR_times_pPa (lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)) */
+void QLA_F3_P_xeqm_pR_times_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeqm_conj_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_conj_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_conj_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_conj_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_i_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_i_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_i_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_i_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_Pa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_Pa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pPa (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_pPa(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_transpose_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_transpose_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_transpose_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_transpose_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_P (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_P_xeqm_pP (lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)) */
+void QLA_F3_P_xeqm_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_P_xeq_P_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_P_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_P_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_P_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_P_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_P_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_P_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_P_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_P_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_P_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_P_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_P_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_P_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_P_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_P_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_P_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_P_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_P_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_P_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_P_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_P_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_P_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_P_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_P_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_pP_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_pP_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_pP_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_pP_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_pP_plus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_pP_plus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_pP_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_pP_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_pP_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_pP_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_pP_minus_P (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_pP_minus_P(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT c, int * index, int n);
+/* replaces QLA_F3_P_xeq_pP_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_pP_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_pP_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_pP_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_pP_plus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_pP_plus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_pP_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_pP_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_P_xeq_r_times_pP_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_r_times_pP_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Real *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* replaces QLA_F3_P_xeq_c_times_pP_minus_pP (lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)) */
+void QLA_F3_P_xeq_c_times_pP_minus_pP(QLA_F3_DiracPropagator *QLA_B200_RESTRICT r, QLA_F_Complex *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * c, int * index, int n);
+/* ---- ldot: replaces the F3 functions emitted by lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms) */
+/* replaces QLA_F3_C_veq_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veq_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vpeq_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vpeq_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vmeq_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vmeq_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_veqm_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veqm_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_xeq_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xpeq_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xmeq_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xeqm_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_V_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_V_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_V_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_V_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_V_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_V_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pV_dot_V(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pV_dot_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pV_dot_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pV_dot_pV(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pV_dot_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pV_dot_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_V (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_V(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_pV (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_pV(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_veq_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veq_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vpeq_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vpeq_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vmeq_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vmeq_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_veqm_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veqm_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_xeq_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xpeq_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xmeq_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xeqm_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_H_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_H_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_H_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_H_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_H_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_H_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pH_dot_H(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pH_dot_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pH_dot_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pH_dot_pH(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pH_dot_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pH_dot_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, QLA_F3_HalfFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_H (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_H(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_pH (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_pH(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_HalfFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_veq_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veq_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vpeq_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vpeq_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vmeq_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vmeq_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_veqm_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veqm_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_xeq_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xpeq_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xmeq_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xeqm_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_D_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_D_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_D_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_D_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_D_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_D_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pD_dot_D(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pD_dot_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pD_dot_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pD_dot_pD(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pD_dot_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pD_dot_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, QLA_F3_DiracFermion *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_D (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_D(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_pD (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_pD(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracFermion *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_veq_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veq_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vpeq_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vpeq_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vmeq_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vmeq_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_veqm_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veqm_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_xeq_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xpeq_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xmeq_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xeqm_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_M_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_M_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_M_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_M_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_M_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_M_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pM_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pM_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pM_dot_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pM_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pM_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pM_dot_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_M_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_M_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_M_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_M_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pM_dot_Ma (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pM_dot_Ma(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pM_dot_pMa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pM_dot_pMa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_Ma_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_Ma_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_Ma_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_Ma_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pMa_dot_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pMa_dot_M(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pMa_dot_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pMa_dot_pM(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_M (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_M(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_pM (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_pM(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_ColorMatrix *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_veq_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veq_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veq_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veq_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veq_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veq_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veq_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veq_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vpeq_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vpeq_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vpeq_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vpeq_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vpeq_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vpeq_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vpeq_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vpeq_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_vmeq_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_vmeq_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_vmeq_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_vmeq_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_vmeq_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_vmeq_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_vmeq_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_vmeq_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_veqm_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_R_veqm_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_C_veqm_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_C_veqm_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_veqm_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_R_veqm_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_F3_R_veqm_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_veqm_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_F3_C_xeq_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeq_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeq_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeq_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeq_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xpeq_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xpeq_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xpeq_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xpeq_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xpeq_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xmeq_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xmeq_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xmeq_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xmeq_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xmeq_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_C_xeqm_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_P_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_P_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_P_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_P_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_P_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_P_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pP_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pP_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pP_dot_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pP_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_re_pP_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_re_pP_dot_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_P_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_P_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_P_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_P_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pP_dot_Pa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pP_dot_Pa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pP_dot_pPa (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pP_dot_pPa(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_Pa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_Pa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_Pa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_Pa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pPa_dot_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pPa_dot_P(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_C_xeqm_pPa_dot_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_C_xeqm_pPa_dot_pP(QLA_F_Complex *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_P (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_P(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_F3_R_xeqm_norm2_pP (lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)) */
+void QLA_F3_R_xeqm_norm2_pP(QLA_F_Real *QLA_B200_RESTRICT r, QLA_F3_DiracPropagator *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_F3_M_veq_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veq_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veq_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veq_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veq_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veq_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veq_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vpeq_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vpeq_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vpeq_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vpeq_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vpeq_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vpeq_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vmeq_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vmeq_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_vmeq_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vmeq_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_vmeq_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_vmeq_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veqm_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veqm_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_veqm_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veqm_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_F3_M_veqm_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_veqm_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_F3_M_xeq_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeq_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeq_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeq_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeq_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeq_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xpeq_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xpeq_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xpeq_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xpeq_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xpeq_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xmeq_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xmeq_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xmeq_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xmeq_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xmeq_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_V_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeqm_V_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_V_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeqm_V_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pV_times_Va (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeqm_pV_times_Va(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_F3_M_xeqm_pV_times_pVa (lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)) */
+void QLA_F3_M_xeqm_pV_times_pVa(QLA_F3_ColorMatrix *QLA_B200_RESTRICT r, QLA_F3_ColorVector *QLA_B200_RESTRICT * a, QLA_F3_ColorVector *QLA_B200_RESTRICT * b, int * index, int n);
 
 #ifdef __cplusplus
 }

@@ -52,6 +52,23 @@ void ora_minv_f(float *r, const float *a, const float *b, long n, int nc, int nb
 void ora_minv_d(double *r, const double *a, const double *b, long n, int nc, int nb, const int *ia,
                 const int *ib);
 
+/* element-wise families (shape / perm codes as the product's EwShape / EwPerm),
+ * the ColorVector outer product and site-local dot products (kind as LdKind) */
+void ora_ewise_f(int shape, int perm, int eqop, float *r, const float *b, const float *c, const float *s,
+                 int scal_kind, float sre, float sim, long n, int ne, const int *idx_b, const int *idx_c,
+                 const int *idx_s, const int *gang);
+void ora_ewise_d(int shape, int perm, int eqop, double *r, const double *b, const double *c, const double *s,
+                 int scal_kind, double sre, double sim, long n, int ne, const int *idx_b, const int *idx_c,
+                 const int *idx_s, const int *gang);
+void ora_outer_f(int eqop, float *r, const float *a, const float *b, long n, const int *idx_a, const int *idx_b,
+                 const int *gang);
+void ora_outer_d(int eqop, double *r, const double *a, const double *b, long n, const int *idx_a,
+                 const int *idx_b, const int *gang);
+void ora_ldot_f(int kind, int perm, int eqop, float *r, const float *a, const float *b, long n, int ne,
+                const int *idx_a, const int *idx_b, const int *gang);
+void ora_ldot_d(int kind, int perm, int eqop, double *r, const double *a, const double *b, long n, int ne,
+                const int *idx_a, const int *idx_b, const int *gang);
+
 /* QLA_I_ integer ops (codes as the product's IntCode, 19 = mask) */
 void ora_int(int code, int eqop, int *r, const int *a, const int *b, const int *c, int s, long n,
              const int *ia, const int *ib, const int *ic, const int *gang);

@@ -23,6 +23,7 @@ Outputs (all written by this script, committed):
   qla_b200/csrc/gen/<pc>_<family>.cu    wrappers (split per family to compile in parallel)
   qla_b200/gen/api_manifest.json        every symbol with its family and argument kinds
 """
+import itertools
 import json
 import os
 import sys
@@ -63,6 +64,14 @@ CITE["mfunc_ext"] = ("lib/perl/build_qla.pl:1022-1061 (matrix functions, eigenva
                      "M_eq_invsqrt_M.c:88-127, M_eq_log_M.c:127-199, M_eq_expA_M.c:100-298, "
                      "M_eq_expTA_M.c:96-274, M_eq_sqrtPH_M.c:84-197, M_eq_invsqrtPH_M.c:84-201, "
                      "V_eq_eigenvals_M.c:127-186, V_eq_eigenvalsH_M.c:106-166")
+for _t in "vhdmp":
+    CITE["ewise_" + _t] = "lib/perl/build_qla.pl:403-469, 1256-1420 (element-wise families)"
+CITE["ewise_times"] = "lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400"
+CITE["ewise_field"] = "lib/perl/build_qla.pl:1256-1335 (per-site complex / real field times a field)"
+CITE["ewise_unary"] = "lib/perl/build_qla.pl:403-469 (conj, i, adjoint and transpose copies)"
+CITE["ewise_sum"] = "lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)"
+CITE["ldot"] = "lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)"
+CITE["outer"] = "lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)"
 CITE["reunit"] = ("no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of "
                   "M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64")
 CITE["minv"] = ("lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), "
@@ -639,6 +648,163 @@ def gen_pc(pc, R, P):
                                 f"sizeof({outR}), {oa}, {ob}, {gang}, n);")
                         fns.append(Fn(name, params, body, "redot", CITE["redot"],
                                       dict(dest="r", var=var, a=sa, b=sb, out=outR)))
+    fns += gen_ewise(pc, R, P)
+    return fns
+
+
+# element counts (complex numbers per record) at Nc = 3
+NE3 = {"V": 3, "H": 6, "D": 12, "M": 9, "P": 144}
+PERM_OF = {"M": "qlab::PERM_M", "P": "qlab::PERM_P"}
+
+
+def gen_ewise(pc, R, P):
+    """The element-wise families (constant and field multiples, sums,
+    combinations, conj / i / adjoint / transpose copies), site-local dot
+    products and norms, and the ColorVector outer product, for F3 / D3."""
+    fns = []
+    kid = lambda fam: f'"{pc}_{fam}"'  # noqa: E731
+    cplx, real = f"QLA_{P}_Complex", f"QLA_{P}_Real"
+
+    def var_tail(var):
+        return ([("int *", "index")] if var == "x" else []), ("index" if var == "x" else "nullptr")
+
+    def srcs(T, adj):
+        """(name suffix, pointer?, permutation) of the field source."""
+        out = [(T, False, "qlab::PERM_ID"), ("p" + T, True, "qlab::PERM_ID")]
+        if adj:
+            out += [(T + "a", False, PERM_OF[T]), ("p" + T + "a", True, PERM_OF[T])]
+        return out
+
+    def emit(name, params, body, cite_key, kinds):
+        # one source file per destination type (and for the local products)
+        fam = {"ldot": "ldot", "outer": "ldot"}.get(cite_key, "ewise_" + kinds.get("dest", "x").lower())
+        fns.append(Fn(name, params, body, fam, CITE[cite_key], kinds))
+
+    for T in ["V", "H", "D", "M", "P"]:
+        ne = NE3[T]
+        adj = T in ("M", "P")
+        rt = f"{ptype(pc, T)} *RESTRICT"
+        for var in ["v", "x"]:
+            tail, gang = var_tail(var)
+            for eq in EQOPS:
+                # ---- constant multiples: c_times (all), r_times (P and adjoints; the
+                # plain V/H/D/M forms are the RTimesOp family)
+                for src, p1, perm in srcs(T, adj):
+                    pb, ob = operand(pc, T, p1, "b")
+                    isadj = src.endswith("a")
+                    for kind, st, shape in (("c", cplx, "qlab::EW_CTA" if isadj else "qlab::EW_CT"),
+                                            ("r", real, "qlab::EW_RTA" if isadj else "qlab::EW_RT")):
+                        if kind == "r" and T != "P" and not isadj:
+                            continue
+                        name = f"QLA_{pc}_{T}_{var}{eq}_{kind}_times_{src}"
+                        params = [(rt, "r"), (f"{st} *RESTRICT", "a"), pb] + tail + [("int", "n")]
+                        body = (f"qlab::api_ew<{R}, {ne}, {shape}, {perm}, qlab::SC_CONST, {str(kind == 'r').lower()}>"
+                                f"({kid('ew_' + kind + 'times')}, r, a, qlab::Opnd{{}}, {ob}, qlab::Opnd{{}}, {gang}, n, "
+                                f"{EQ_ENUM[eq]});")
+                        emit(name, params, body, "ewise_times",
+                             dict(dest=T, eqop=eq, var=var, scal=kind, b=src))
+                # ---- per-site field multiples: C, Ca, R (and pointer forms)
+                for sname, sp, shape, sreal, sadj in (("C", False, "CT", False, False), ("pC", True, "CT", False, False),
+                                                      ("Ca", False, "CAT", False, True), ("pCa", True, "CAT", False, True),
+                                                      ("R", False, "RT", True, False), ("pR", True, "RT", True, False)):
+                    st = real if sreal else cplx
+                    sparam = (f"{st} *RESTRICT *", "a") if sp else (f"{st} *RESTRICT", "a")
+                    sop = "qlab::op_ptr((const void* const*)a)" if sp else "qlab::op_contig(a)"
+                    for src, p1, perm in srcs(T, adj):
+                        pb, ob = operand(pc, T, p1, "b")
+                        isadj = src.endswith("a")
+                        sh = {"CT": "CTA", "CAT": "CATA", "RT": "RTA"}[shape] if isadj else shape
+                        name = f"QLA_{pc}_{T}_{var}{eq}_{sname}_times_{src}"
+                        params = [(rt, "r"), sparam, pb] + tail + [("int", "n")]
+                        body = (f"qlab::api_ew<{R}, {ne}, qlab::EW_{sh}, {perm}, qlab::SC_FIELD, {str(sreal).lower()}>"
+                                f"({kid('ew_field')}, r, nullptr, {sop}, {ob}, qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]});")
+                        emit(name, params, body, "ewise_field", dict(dest=T, eqop=eq, var=var, scal=sname, b=src))
+                # ---- conj, i*a, and (M, P) adjoint / transpose copies, P copies
+                unary = [("conj_", "qlab::EW_CONJ", "qlab::PERM_ID", False), ("i_", "qlab::EW_I", "qlab::PERM_ID", False)]
+                if adj:
+                    unary += [("", "qlab::EW_CONJ", PERM_OF[T], True), ("transpose_", "qlab::EW_COPY", PERM_OF[T], False)]
+                if T == "P":
+                    unary += [("", "qlab::EW_COPY", "qlab::PERM_ID", False)]
+                for pre, shape, perm, asadj in unary:
+                    for p1 in (False, True):
+                        pa, oa = operand(pc, T, p1, "a")
+                        src = ("p" if p1 else "") + T + ("a" if asadj else "")
+                        name = f"QLA_{pc}_{T}_{var}{eq}_{pre}{src}"
+                        params = [(rt, "r"), pa] + tail + [("int", "n")]
+                        body = (f"qlab::api_ew<{R}, {ne}, {shape}, {perm}, qlab::SC_NONE, false>({kid('ew_unary')}, r, "
+                                f"nullptr, qlab::Opnd{{}}, {oa}, qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]});")
+                        emit(name, params, body, "ewise_unary", dict(dest=T, eqop=eq, var=var, op=pre or "copy", a=src))
+            # ---- sums and combinations (eq only)
+            for pa_, pb_ in itertools.product((False, True), (False, True)):
+                sa = ("p" if pa_ else "") + T
+                sb = ("p" if pb_ else "") + T
+                for op, shape in (("plus", "PLUS"), ("minus", "MINUS")):
+                    pa, oa = operand(pc, T, pa_, "a")
+                    pb, ob = operand(pc, T, pb_, "b")
+                    name = f"QLA_{pc}_{T}_{var}eq_{sa}_{op}_{sb}"
+                    params = [(rt, "r"), pa, pb] + tail + [("int", "n")]
+                    body = (f"qlab::api_ew<{R}, {ne}, qlab::EW_{shape}, qlab::PERM_ID, qlab::SC_NONE, false>("
+                            f"{kid('ew_sum')}, r, nullptr, qlab::Opnd{{}}, {oa}, {ob}, {gang}, n, qlab::EQ);")
+                    emit(name, params, body, "ewise_sum", dict(dest=T, eqop="eq", var=var, op=op, a=sa, b=sb))
+                    for kind, st in (("r", real), ("c", cplx)):
+                        pb2, ob2 = operand(pc, T, pa_, "b")
+                        pc2, oc2 = operand(pc, T, pb_, "c")
+                        name = f"QLA_{pc}_{T}_{var}eq_{kind}_times_{sa}_{op}_{sb}"
+                        params = [(rt, "r"), (f"{st} *RESTRICT", "a"), pb2, pc2] + tail + [("int", "n")]
+                        sh = ("RT_" if kind == "r" else "CT_") + shape
+                        body = (f"qlab::api_ew<{R}, {ne}, qlab::EW_{sh}, qlab::PERM_ID, qlab::SC_CONST, "
+                                f"{str(kind == 'r').lower()}>({kid('ew_axpby')}, r, a, qlab::Opnd{{}}, {ob2}, {oc2}, "
+                                f"{gang}, n, qlab::EQ);")
+                        emit(name, params, body, "ewise_sum", dict(dest=T, eqop="eq", var=var, op=kind + "_" + op,
+                                                                  a=sa, b=sb))
+    # ---- site-local dot products and norms (complex / real field outputs)
+    for T in ["V", "H", "D", "M", "P"]:
+        ne = NE3[T]
+        for var in ["v", "x"]:
+            tail, gang = var_tail(var)
+            for eq in EQOPS:
+                pairs = [(T, T, "LD_DOT", "qlab::PERM_ID")]
+                if T in ("M", "P"):
+                    pairs += [(T, T + "a", "LD_DOT_AA", PERM_OF[T]), (T + "a", T, "LD_ADOT", PERM_OF[T])]
+                for ta, tb, kind, perm in pairs:
+                    for pa_, pb_ in itertools.product((False, True), (False, True)):
+                        sa = ("p" if pa_ else "") + ta
+                        sb = ("p" if pb_ else "") + tb
+                        pa, oa = operand(pc, T, pa_, "a")
+                        pb, ob = operand(pc, T, pb_, "b")
+                        name = f"QLA_{pc}_C_{var}{eq}_{sa}_dot_{sb}"
+                        params = [(f"{cplx} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                        body = (f"qlab::api_ldot<{R}, {ne}, qlab::{kind}, {perm}>({kid('ldot')}, r, {oa}, {ob}, {gang}, "
+                                f"n, {EQ_ENUM[eq]});")
+                        emit(name, params, body, "ldot", dict(dest="C", eqop=eq, var=var, a=sa, b=sb, kind=kind))
+                        if kind == "LD_DOT":
+                            name = f"QLA_{pc}_R_{var}{eq}_re_{sa}_dot_{sb}"
+                            params = [(f"{real} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                            body = (f"qlab::api_ldot<{R}, {ne}, qlab::LD_REDOT, qlab::PERM_ID>({kid('ldot')}, r, {oa}, "
+                                    f"{ob}, {gang}, n, {EQ_ENUM[eq]});")
+                            emit(name, params, body, "ldot", dict(dest="R", eqop=eq, var=var, a=sa, b=sb,
+                                                                   kind="LD_REDOT"))
+                for pa_ in (False, True):
+                    sa = ("p" if pa_ else "") + T
+                    pa, oa = operand(pc, T, pa_, "a")
+                    name = f"QLA_{pc}_R_{var}{eq}_norm2_{sa}"
+                    params = [(f"{real} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                    body = (f"qlab::api_ldot<{R}, {ne}, qlab::LD_NORM2, qlab::PERM_ID>({kid('ldot')}, r, {oa}, "
+                            f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]});")
+                    emit(name, params, body, "ldot", dict(dest="R", eqop=eq, var=var, a=sa, kind="LD_NORM2"))
+    # ---- outer product of two ColorVectors
+    for var in ["v", "x"]:
+        tail, gang = var_tail(var)
+        for eq in EQOPS:
+            for pa_, pb_ in itertools.product((False, True), (False, True)):
+                sa = ("p" if pa_ else "") + "V"
+                sb = ("p" if pb_ else "") + "Va"
+                pa, oa = operand(pc, "V", pa_, "a")
+                pb, ob = operand(pc, "V", pb_, "b")
+                name = f"QLA_{pc}_M_{var}{eq}_{sa}_times_{sb}"
+                params = [(f"{ptype(pc, 'M')} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                body = f"qlab::api_outer<{R}>({kid('outer')}, r, {oa}, {ob}, {gang}, n, {EQ_ENUM[eq]});"
+                emit(name, params, body, "outer", dict(dest="M", eqop=eq, var=var, a=sa, b=sb))
     return fns
 
 
@@ -722,7 +888,10 @@ def main():
         extra = {"int": '#include "../qla_int.cuh"\n', "mfunc": '#include "../qla_mfunc.cuh"\n',
                  "mfunc_ext": '#include "../qla_mfunc_ext.cuh"\n',
                  "multi": '#include <vector>\n#include "../qla_multi.cuh"\n',
-                 "prop": '#include "../qla_prop.cuh"\n'}.get(family, "")
+                 "prop": '#include "../qla_prop.cuh"\n',
+                 "ldot": '#include "../qla_ewise.cuh"\n'}.get(family, "")
+        if family.startswith("ewise"):
+            extra = '#include "../qla_ewise.cuh"\n'
         if pc == "FN" and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
         if pc == "FN" and family == "mfunc_ext":

@@ -422,3 +422,144 @@ def ora_prop(kind, r, a, b, n, eqop, ca=0, cb=0, idx_a=None, idx_b=None, gang=No
     f(PKIND[kind], ca, cb, EQOPS.get(eqop, eqop), ptr(r), ptr(a), ptr(b), ctypes.c_long(n), ptr(idx_a), ptr(idx_b),
       ptr(gang))
     return r
+
+
+# ---------------------------------------------------------------------------
+# element-wise families, site-local dot products, outer product: a generic
+# case builder driven by the generated manifest (parameter types and kinds)
+
+EW_SHAPES = {"COPY": 0, "CONJ": 1, "I": 2, "CT": 3, "CTA": 4, "CAT": 5, "CATA": 6, "RT": 7, "RTA": 8, "PLUS": 9,
+             "MINUS": 10, "RT_PLUS": 11, "RT_MINUS": 12, "CT_PLUS": 13, "CT_MINUS": 14}
+LD_KINDS = {"LD_DOT": 0, "LD_DOT_AA": 1, "LD_ADOT": 2, "LD_REDOT": 3, "LD_NORM2": 4}
+NE3 = {"V": 3, "H": 6, "D": 12, "M": 9, "P": 144}
+_TYPE_OF = {"ColorVector": "V", "HalfFermion": "H", "DiracFermion": "D", "ColorMatrix": "M",
+            "DiracPropagator": "P", "Complex": "C", "Real": "R"}
+
+
+def param_type(ctype):
+    """(record letter, pointer array?) of a generated parameter type."""
+    for k, v in _TYPE_OF.items():
+        if k in ctype:
+            return v, ctype.replace(" ", "").endswith("**")
+    return None, False
+
+
+def _perm_code(t):
+    return {"M": 1, "P": 2}.get(t, 0)
+
+
+def ewise_oracle_plan(e):
+    """How the oracle computes manifest entry e: (function, keyword arguments
+    that name the inputs)."""
+    fam = e["family"]
+    if fam == "ldot" and e["dest"] == "M":  # outer product
+        return "outer", {}
+    if fam == "ldot":
+        return "ldot", {"kind": LD_KINDS[e["kind"]]}
+    dest = e["dest"]
+    if "scal" in e:
+        sc, src = e["scal"], e["b"]
+        adj = src.endswith("a")
+        base = {"c": "CT", "r": "RT", "C": "CT", "pC": "CT", "Ca": "CAT", "pCa": "CAT", "R": "RT", "pR": "RT"}[sc]
+        shape = base + ("A" if adj else "")
+        kind = 1 if sc in ("c", "r") else (3 if sc in ("R", "pR") else 2)
+        return "ewise", {"shape": EW_SHAPES[shape], "perm": _perm_code(dest) if adj else 0, "scal_kind": kind}
+    op = e["op"]
+    if op in ("plus", "minus", "r_plus", "r_minus", "c_plus", "c_minus"):
+        shape = {"plus": "PLUS", "minus": "MINUS", "r_plus": "RT_PLUS", "r_minus": "RT_MINUS",
+                 "c_plus": "CT_PLUS", "c_minus": "CT_MINUS"}[op]
+        return "ewise", {"shape": EW_SHAPES[shape], "perm": 0, "scal_kind": 1 if op[0] in "rc" else 0}
+    src = e["a"]
+    if op == "conj_":
+        return "ewise", {"shape": 1, "perm": 0, "scal_kind": 0}
+    if op == "i_":
+        return "ewise", {"shape": 2, "perm": 0, "scal_kind": 0}
+    if op == "transpose_":
+        return "ewise", {"shape": 0, "perm": _perm_code(dest), "scal_kind": 0}
+    # "copy": the adjoint copy (Ma, Pa) or the plain P copy
+    if src.endswith("a"):
+        return "ewise", {"shape": 1, "perm": _perm_code(dest), "scal_kind": 0}
+    return "ewise", {"shape": 0, "perm": 0, "scal_kind": 0}
+
+
+def ewise_inputs(e, rng, dt, n, ns):
+    """Seeded host inputs for manifest entry e: a dict param -> array (records
+    of ns sites for sources, n sites for the destination), pointer-form
+    index tables, and the gang subset for x forms."""
+    ins = {}
+    for t, name in zip(e["ctypes"], e["params"]):
+        letter, is_ptr = param_type(t)
+        if name in ("n", "index"):
+            continue
+        if letter is None:
+            continue
+        if name == "r":
+            nrec = n
+        else:
+            nrec = ns
+        if letter == "R":
+            arr = rng.standard_normal(nrec).astype(dt)
+        elif letter == "C":
+            arr = rng.standard_normal((nrec, 2)).astype(dt)
+        else:
+            arr = rng.standard_normal((nrec, 2 * NE3[letter])).astype(dt)
+        ins[name] = (letter, is_ptr, arr)
+    # scalar constants (c / r forms): a single value
+    plan, kw = ewise_oracle_plan(e)
+    if plan == "ewise" and kw["scal_kind"] == 1:
+        letter, is_ptr, _ = ins["a"]
+        ins["a"] = (letter, False, (rng.standard_normal(1 if letter == "R" else 2)).astype(dt))
+    idx = {name: rng.integers(0, ns, n).astype(np.int32) for name, v in ins.items() if v[1]}
+    gang = rng.permutation(n)[: n // 2 + 1].astype(np.int32) if e["var"] == "x" else None
+    return ins, idx, gang
+
+
+def ewise_oracle(e, ins, idx, gang, n):
+    """The oracle's result for manifest entry e on ewise_inputs()."""
+    plan, kw = ewise_oracle_plan(e)
+    r = ins["r"][2].copy()
+    dt = r.dtype
+    t = rtype(dt)
+    g = _i32(gang)
+    nsites = len(gang) if gang is not None else n
+    eq = EQOPS[e.get("eqop", "eq")]
+
+    def arr(name):
+        return ins[name][2] if name in ins else None
+
+    def ix(name):
+        return _i32(idx.get(name))
+
+    if plan == "outer":
+        getattr(oracle(), "ora_outer_" + t)(eq, ptr(r), ptr(arr("a")), ptr(arr("b")), ctypes.c_long(nsites),
+                                           ptr(ix("a")), ptr(ix("b")), ptr(g))
+        return r
+    if plan == "ldot":
+        ne = NE3[ins["a"][0]]
+        getattr(oracle(), "ora_ldot_" + t)(kw["kind"], _perm_code(ins["a"][0]), eq, ptr(r), ptr(arr("a")),
+                                          ptr(arr("b")), ctypes.c_long(nsites), ne, ptr(ix("a")), ptr(ix("b")),
+                                          ptr(g))
+        return r
+    dest = e["dest"]
+    ne = NE3[dest]
+    cs = ctypes.c_float if t == "f" else ctypes.c_double
+    sre = sim = 0.0
+    s_arr, s_idx = None, None
+    two = kw["shape"] >= 9
+    if kw["scal_kind"] == 1:
+        sv = arr("a")
+        sre = float(sv[0])
+        sim = float(sv[1]) if len(sv) > 1 else 0.0
+        b_name, c_name = "b", ("c" if kw["shape"] >= 11 else None)
+    elif kw["scal_kind"] in (2, 3):
+        s_arr, s_idx = arr("a"), ix("a")
+        b_name, c_name = "b", None
+    elif two:
+        b_name, c_name = "a", "b"
+    else:
+        b_name, c_name = "a", None
+    getattr(oracle(), "ora_ewise_" + t)(kw["shape"], kw["perm"], eq, ptr(r), ptr(arr(b_name)),
+                                       ptr(arr(c_name)) if c_name else None, ptr(s_arr), kw["scal_kind"],
+                                       cs(sre), cs(sim), ctypes.c_long(nsites), ne, ptr(ix(b_name)),
+                                       ptr(ix(c_name)) if c_name else None, ptr(s_idx), ptr(g))
+    return r

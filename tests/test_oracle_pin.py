@@ -312,3 +312,52 @@ def test_oracle_n_colour_matrix_functions_match_reference_library(pc, dt):
             rr = np.zeros((n, 2 * nc * nb), dt)
             getattr(R, f"QLA_{pc}_{dest}_veq_M_inverse_{dest}")(nc, T.ptr(rr), T.ptr(g), T.ptr(b), n)
             assert T.bits_equal(rr, T.ora_minv(g, b, n, nb, nc=nc)), (nc, dest)
+
+
+def _ref_args(e, ins, idx, gang, n, r):
+    """Host arguments of manifest entry e for the reference library."""
+    args, keep = [], []
+    for t, name in zip(e["ctypes"], e["params"]):
+        if name == "n":
+            args.append(len(gang) if gang is not None else n)
+        elif name == "index":
+            args.append(T.ptr(gang))
+        elif name == "r":
+            args.append(T.ptr(r))
+        else:
+            letter, is_ptr, arr = ins[name]
+            if is_ptr:
+                rec = arr.itemsize * (1 if letter == "R" else 2 if letter == "C" else 2 * T.NE3[letter])
+                pa = (ctypes.c_void_p * len(idx[name]))(*[arr.ctypes.data + int(j) * rec for j in idx[name]])
+                keep.append(pa)
+                args.append(pa)
+            else:
+                args.append(T.ptr(arr))
+    return args, keep
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+def test_oracle_elementwise_families_match_reference_library(pc, dt):
+    """Every generated element-wise, site-local dot and outer-product entry
+    point: the oracle restatement against the reference library, bit for bit
+    (all eqops, pointer and gang forms; 13 destination sites, 17 sources)."""
+    import json
+    man = json.load(open(os.path.join(os.path.dirname(T.ORACLE_SO), "..", "qla_b200", "gen", "api_manifest.json")))
+    R = T.ref()
+    rng = np.random.default_rng(101)
+    n, ns = 13, 17
+    bad, count = [], 0
+    for e in man:
+        if e["pc"] != pc or not (e["family"].startswith("ewise") or e["family"] == "ldot"):
+            continue
+        ins, idx, gang = T.ewise_inputs(e, rng, dt, n, ns)
+        want = T.ewise_oracle(e, ins, idx, gang, n)
+        r = ins["r"][2].copy()
+        args, keep = _ref_args(e, ins, idx, gang, n, r)
+        getattr(R, e["name"])(*args)
+        count += 1
+        if not T.bits_equal(r, want):
+            bad.append(e["name"])
+    assert count > 1800
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
