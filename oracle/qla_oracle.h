@@ -73,6 +73,26 @@ void ora_ldot_d(int kind, int perm, int eqop, double *r, const double *a, const 
 void ora_int(int code, int eqop, int *r, const int *a, const int *b, const int *c, int s, long n,
              const int *ia, const int *ib, const int *ic, const int *gang);
 
+/* site-field families: fills, copymask, components ('e', 'c', 'd'), gamma
+ * multiplication, traces (kind 0 C, 1 Re, 2 Im, 3 antiherm), global
+ * reductions of P / Ma / Pa in the reference order, global sums */
+#define ORA_SITEFIELD_DECL(R, SFX)                                                               \
+void ora_fill_##SFX(int eqop, R *r, const R *a, long n, int ne, const int *gang);                \
+void ora_diagfill_##SFX(int eqop, R *r, const R *c, long n, const int *gang);                    \
+void ora_zero_##SFX(R *r, long n, int ne, const int *gang);                                      \
+void ora_mask_##SFX(R *r, const R *a, const int *m, long n, int ne, const int *idx_a,           \
+                    const int *idx_m, const int *gang);                                           \
+void ora_component_##SFX(int what, int dst, int src, R *r, const R *a, int i_c, int i_s,         \
+                         int j_c, int j_s, long n, const int *idx_a, const int *gang);          \
+void ora_gamma_##SFX(int right, int ne, int mu, R *r, const R *a, long n, const int *idx_a,      \
+                     const int *gang);                                                            \
+void ora_trace_##SFX(int kind, R *r, const R *a, long n, const int *idx_a, const int *gang);    \
+void ora_gdot_##SFX(int kind, int perm, double *out2, const R *a, const R *b, long n, int ne,     \
+                    const int *idx_a, const int *idx_b, const int *gang);                        \
+void ora_gsum_##SFX(R *r, const R *a, long n, int ne, const int *idx_a, const int *gang);
+ORA_SITEFIELD_DECL(float, f)
+ORA_SITEFIELD_DECL(double, d)
+
 int ora_version(void);
 
 #endif

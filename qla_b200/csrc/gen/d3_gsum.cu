@@ -1,0 +1,88 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA D3 gsum entry points (extern "C"), reference: lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+#include "../qla_sitefield.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_D3_v_veq_sum_V(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ a, int n) {
+  qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_v_veq_sum_pV(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ * a, int n) {
+  qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_h_veq_sum_H(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ a, int n) {
+  qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_h_veq_sum_pH(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ * a, int n) {
+  qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_d_veq_sum_D(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ a, int n) {
+  qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_d_veq_sum_pD(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ * a, int n) {
+  qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_m_veq_sum_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_m_veq_sum_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_p_veq_sum_P(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ a, int n) {
+  qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_p_veq_sum_pP(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ * a, int n) {
+  qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D3_v_xeq_sum_V(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ a, int * index, int n) {
+  qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_v_xeq_sum_pV(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ * a, int * index, int n) {
+  qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_h_xeq_sum_H(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ a, int * index, int n) {
+  qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_h_xeq_sum_pH(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ * a, int * index, int n) {
+  qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_d_xeq_sum_D(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ a, int * index, int n) {
+  qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_d_xeq_sum_pD(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ * a, int * index, int n) {
+  qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_m_xeq_sum_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_m_xeq_sum_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_p_xeq_sum_P(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ a, int * index, int n) {
+  qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D3_p_xeq_sum_pP(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ * a, int * index, int n) {
+  qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+}  // extern "C"

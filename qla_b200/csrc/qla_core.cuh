@@ -38,6 +38,8 @@ __device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
 
 template <typename R>
 struct Cx {

@@ -53,8 +53,6 @@ template <typename R>
 __device__ __forceinline__ R cnorm2(Cx<R> a) {
   return radd(rmul(a.re, a.re), rmul(a.im, a.im));
 }
-__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
-__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
 
 // r = a * b for 3x3 (M_eq_M_times_M order: x = 0; x += a_ik b_kj)
 template <typename R>

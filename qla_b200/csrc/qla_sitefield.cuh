@@ -1,0 +1,664 @@
+// qla_sitefield.cuh -- the site-field families of the F3 / D3 level-1 API
+// that fill, pick apart or re-arrange whole records, and the global
+// reductions over records too large for one thread's registers:
+//
+//   X (eqop) x             one record broadcast to every site (v h d m p)
+//   M (eqop) c             c times the identity at every site (diagfill)
+//   X = zero;  X = a where mask != 0 (copymask)
+//   C = elem(a, ...), elem(X, ...) = C, colour-column / Dirac-vector
+//       extraction and insertion
+//   D = gamma_mu D,  P = gamma_mu P,  P = P gamma_mu   (mu = 0..15)
+//   C / R = trace, Re trace, Im trace of M;  M = traceless antihermitian part
+//   c / r = global sums of Ma.M, P.P, P.Pa-type products, |P|^2
+//   x = sum over sites of X (every component summed separately)
+//
+// Reference sections (lib/perl/build_qla.pl): constant fills :2584-2618,
+// zero fills :2561-2582, copymask :2058-2084, array components :767-820,
+// colour columns :822-876, Dirac vectors :878-931, trace :933-981,
+// antihermitian part :983-1064, gamma multiplication :1358-1412 with the
+// basis of lib/perl/expressions_gamma.pl:59-134, global inner products and
+// norms :2089-2272, global sums :2449-2484.
+//
+// Element maps run one thread per output complex number, like the
+// element-wise families: consecutive threads touch consecutive elements of
+// the AoS records, which coalesces for every record size.  Every map here
+// only moves values or negates / swaps components, except the trace and the
+// antihermitian part, which repeat the reference's additions in its order;
+// all results are bit-identical to the reference.
+#pragma once
+#include <cstdio>
+#include "qla_ewise.cuh"
+
+namespace qlab {
+
+enum SfKind : int {
+  SF_BCAST = 0,   // r (eqop) x                          (x one record)
+  SF_DIAG,        // M r (eqop) c * identity
+  SF_ZERO,        // r = 0
+  SF_MASK,        // r = a where mask != 0
+  SF_SUB,         // r.e[oi[j]] = a.e[si[j]], j < cnt    (components, columns)
+  SF_GAMMA_L,     // r = gamma a   on the first spin index of D / P
+  SF_GAMMA_R,     // r = a gamma   on the second spin index of P
+  SF_TRACE_C,     // C r = trace a
+  SF_TRACE_RE,    // R r = Re trace a
+  SF_TRACE_IM,    // R r = Im trace a
+  SF_ANTIHERM     // M r = traceless antihermitian part of a
+};
+
+struct SfParams {
+  void* out;
+  Opnd a;              // source field
+  Opnd m;              // QLA_Int mask field (SF_MASK)
+  const int* gang;
+  long long n;
+  int eqop;
+  int cnt;             // SF_SUB: components copied per site
+  int oi[12], si[12];  // SF_SUB: destination / source component of copy j
+  int gs[4], gp[4];    // SF_GAMMA_*: source spin and phase (0: 1, 1: i, 2: -1, 3: -i) per destination spin
+  const void* cptr;    // SF_BCAST / SF_DIAG: the constant in device memory, or nullptr (value in the argument)
+};
+
+// a record constant passed by value (kernel parameter space, read-only and
+// broadcast to all threads)
+template <typename R, int NE>
+struct RecConst {
+  Cx<R> v[NE];
+};
+
+// output complex numbers per site of each kind
+template <int KIND, int NE_OUT>
+struct SfOutPerSite {
+  static constexpr int value = (KIND == SF_TRACE_C || KIND == SF_TRACE_RE || KIND == SF_TRACE_IM) ? 1 : NE_OUT;
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> phase_times(int ph, Cx<R> a) {
+  // QLA_c_eq_c, QLA_c_eq_ic, QLA_c_eqm_c, QLA_c_eqm_ic (include/qla_complex.h:147-168)
+  switch (ph) {
+    case 0: return a;
+    case 1: return Cx<R>{-a.im, a.re};
+    case 2: return Cx<R>{-a.re, -a.im};
+    default: return Cx<R>{a.im, -a.re};
+  }
+}
+
+// NE_OUT / NE_SRC: complex numbers per destination / source record.
+// For SF_GAMMA_* the record is a D (12) or a P (144); the spin index being
+// multiplied is decoded from the element index below.
+template <typename R, int NE_OUT, int NE_SRC, int KIND>
+__global__ void __launch_bounds__(256) sf_kernel(const SfParams p, const RecConst<R, (KIND == SF_BCAST) ? NE_OUT : 1> cv) {
+  constexpr int OPS = SfOutPerSite<KIND, NE_OUT>::value;
+  const int ops = (KIND == SF_SUB) ? p.cnt : OPS;
+  const long long total = p.n * ops;
+  Cx<R> c1{R(0), R(0)};
+  if constexpr (KIND == SF_DIAG) c1 = p.cptr ? *static_cast<const Cx<R>*>(p.cptr) : cv.v[0];
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long i = g / ops;
+    const int e = (int)(g - i * ops);
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    if constexpr (KIND == SF_BCAST) {
+      Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * NE_OUT + e;
+      const Cx<R> b = p.cptr ? static_cast<const Cx<R>*>(p.cptr)[e] : cv.v[e];
+      const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+      const Cx<R> x = load ? *out : Cx<R>{R(0), R(0)};
+      *out = ew_apply<R, EW_COPY>(p.eqop, x, Cx<R>{R(0), R(0)}, b, Cx<R>{R(0), R(0)});
+    } else if constexpr (KIND == SF_DIAG) {
+      // QLA_c_<eqop>_r(r_ij, 0.) on every element, then QLA_c_<eqop>_c(r_ii, c)
+      // on the diagonal (build_qla.pl:2603-2616, make_code_unary.pl "diagfill")
+      Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 9 + e;
+      Cx<R> x;
+      switch (p.eqop) {
+        case EQ: x = Cx<R>{R(0), R(0)}; break;
+        case EQM: x = Cx<R>{-R(0), R(0)}; break;
+        case PEQ: x = *out; x.re = radd(x.re, R(0)); break;
+        default: x = *out; x.re = rsub(x.re, R(0)); break;
+      }
+      if (e % 4 == 0) {
+        switch (p.eqop) {
+          case EQ: x = c1; break;
+          case EQM: x = Cx<R>{-c1.re, -c1.im}; break;
+          case PEQ: x = Cx<R>{radd(x.re, c1.re), radd(x.im, c1.im)}; break;
+          default: x = Cx<R>{rsub(x.re, c1.re), rsub(x.im, c1.im)}; break;
+        }
+      }
+      *out = x;
+    } else if constexpr (KIND == SF_ZERO) {
+      static_cast<Cx<R>*>(p.out)[k * NE_OUT + e] = Cx<R>{R(0), R(0)};
+    } else if constexpr (KIND == SF_MASK) {
+      const int mv = (p.m.mode == OM_PTR) ? *static_cast<const int*>(p.m.ptrs[k]) : static_cast<const int*>(p.m.base)[k];
+      if (mv) static_cast<Cx<R>*>(p.out)[k * NE_OUT + e] = rec_ptr<R>(p.a, k, NE_SRC)[e];
+    } else if constexpr (KIND == SF_SUB) {
+      static_cast<Cx<R>*>(p.out)[k * NE_OUT + p.oi[e]] = rec_ptr<R>(p.a, k, NE_SRC)[p.si[e]];
+    } else if constexpr (KIND == SF_GAMMA_L || KIND == SF_GAMMA_R) {
+      // D: e = ic*4 + is; P: e = ((ic*4 + is)*3 + jc)*4 + js
+      int s, base, stride;
+      if constexpr (KIND == SF_GAMMA_R) {
+        s = e & 3;
+        base = e - s;
+        stride = 1;
+      } else if constexpr (NE_OUT == 12) {
+        s = e & 3;
+        base = e - s;
+        stride = 1;
+      } else {
+        s = (e / 12) & 3;
+        base = e - s * 12;
+        stride = 12;
+      }
+      const Cx<R> a = rec_ptr<R>(p.a, k, NE_SRC)[base + p.gs[s] * stride];
+      static_cast<Cx<R>*>(p.out)[k * NE_OUT + e] = phase_times<R>(p.gp[s], a);
+    } else if constexpr (KIND == SF_TRACE_C) {
+      // QLA_c_eq_r(x, 0.); QLA_c_peq_c(x, a_ii) for i = 0, 1, 2 (build_qla.pl:933-981)
+      const Cx<R>* a = rec_ptr<R>(p.a, k, 9);
+      Cx<R> x{R(0), R(0)};
+#pragma unroll
+      for (int c = 0; c < 3; c++) x = Cx<R>{radd(x.re, a[c * 4].re), radd(x.im, a[c * 4].im)};
+      static_cast<Cx<R>*>(p.out)[k] = x;
+    } else if constexpr (KIND == SF_TRACE_RE || KIND == SF_TRACE_IM) {
+      const Cx<R>* a = rec_ptr<R>(p.a, k, 9);
+      R x = R(0);
+#pragma unroll
+      for (int c = 0; c < 3; c++) x = radd(x, KIND == SF_TRACE_RE ? a[c * 4].re : a[c * 4].im);
+      static_cast<R*>(p.out)[k] = x;
+    } else {  // SF_ANTIHERM (build_qla.pl:983-1064)
+      const Cx<R>* a = rec_ptr<R>(p.a, k, 9);
+      const int ic = e / 3, jc = e - 3 * (e / 3);
+      Cx<R> y;
+      if (ic == jc) {
+        // x = sum Im a_cc / 3; r_ii = (0, Im a_ii - x)
+        R x = R(0);
+#pragma unroll
+        for (int c = 0; c < 3; c++) x = radd(x, a[c * 4].im);
+        x = rdiv(x, R(3));
+        y = Cx<R>{R(0), rsub(a[e].im, x)};
+      } else {
+        // x2 = (a_ij - conj(a_ji)) * 0.5 for i < j; r_ij = x2, r_ji = -conj(x2)
+        const int lo = ic < jc ? ic : jc, hi = ic < jc ? jc : ic;
+        const Cx<R> u = a[lo * 3 + hi], v = a[hi * 3 + lo];
+        const Cx<R> x2{rmul(rsub(u.re, v.re), R(0.5)), rmul(radd(u.im, v.im), R(0.5))};
+        y = (ic < jc) ? x2 : Cx<R>{-x2.re, x2.im};
+      }
+      static_cast<Cx<R>*>(p.out)[k * 9 + e] = y;
+    }
+  }
+}
+
+template <typename R, int NE_OUT, int NE_SRC, int KIND>
+inline void sf_launch(const char* kid, SfParams& p, const RecConst<R, (KIND == SF_BCAST) ? NE_OUT : 1>& cv) {
+  const int ops = (KIND == SF_SUB) ? p.cnt : SfOutPerSite<KIND, NE_OUT>::value;
+  const long long total = p.n * ops;
+  const long long cap = (long long)device_sm_count() * 16;
+  long long grid = (total + 255) / 256;
+  if (grid > cap) grid = cap;
+  sf_kernel<R, NE_OUT, NE_SRC, KIND><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, current_stream()>>>(p, cv);
+  check_launch(kid);
+}
+
+inline bool sf_prep(const char* kid, SfParams& p, void* r, Opnd a, const int* gang, int n, int eqop, bool need_a) {
+  if (n <= 0) return false;
+  if (!r || (need_a && !opnd_ok(a))) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return false;
+  }
+  std::memset(&p, 0, sizeof(p));
+  p.out = r;
+  p.a = a;
+  p.gang = gang;
+  p.n = n;
+  p.eqop = eqop;
+  return true;
+}
+
+// X (eqop) x: x is one record, in host or device memory
+template <typename R, int NE>
+inline void api_fill(const char* kid, void* r, const void* x, const int* gang, int n, int eqop) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, Opnd{}, gang, n, eqop, false)) return;
+  if (!x) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  RecConst<R, NE> cv;
+  if (is_device_ptr(x))
+    p.cptr = x;
+  else
+    std::memcpy(&cv, x, sizeof(cv));
+  sf_launch<R, NE, NE, SF_BCAST>(kid, p, cv);
+}
+
+// M (eqop) c * identity: c a complex number in host or device memory
+template <typename R>
+inline void api_diagfill(const char* kid, void* r, const void* c, const int* gang, int n, int eqop) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, Opnd{}, gang, n, eqop, false)) return;
+  if (!c) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  RecConst<R, 1> cv;
+  if (is_device_ptr(c))
+    p.cptr = c;
+  else
+    std::memcpy(&cv, c, sizeof(cv));
+  sf_launch<R, 9, 9, SF_DIAG>(kid, p, cv);
+}
+
+template <typename R, int NE>
+inline void api_zero(const char* kid, void* r, const int* gang, int n) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, Opnd{}, gang, n, EQ, false)) return;
+  sf_launch<R, NE, NE, SF_ZERO>(kid, p, RecConst<R, 1>{});
+}
+
+template <typename R, int NE>
+inline void api_mask(const char* kid, void* r, Opnd a, Opnd m, const int* gang, int n) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
+  if (!opnd_ok(m)) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  p.m = m;
+  sf_launch<R, NE, NE, SF_MASK>(kid, p, RecConst<R, 1>{});
+}
+
+// component index of (ic, is, jc, js) in a record of the given type letter
+// (include/qla_types.h:38-42: colour-major, spin inner)
+inline int sf_elem(char t, int ic, int is, int jc, int js) {
+  switch (t) {
+    case 'V': return ic;
+    case 'H': return ic * 2 + is;
+    case 'D': return ic * 4 + is;
+    case 'M': return ic * 3 + jc;
+    case 'P': return ((ic * 4 + is) * 3 + jc) * 4 + js;
+    default: return 0;  // 'C'
+  }
+}
+
+// r.(DST component) = a.(SRC component) for every colour (and, for Dirac
+// vectors, spin) index the function loops over.  WHAT selects the family:
+//   'e' array component  (C <- X, X <- C; indices fixed by the arguments)
+//   'c' colour column    (V <- H/D/M/P and back; the loop runs over ic)
+//   'd' Dirac vector     (D <- P and back; the loop runs over ic, is)
+template <typename R, int NE_OUT, int NE_SRC>
+inline void api_sub(const char* kid, void* r, Opnd a, const int* gang, int n, char what, char dst, char src,
+                    int i_c, int i_s, int j_c, int j_s) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
+  // the container's fixed indices; the loop variable(s) fill the rest
+  const char cont = (dst == 'V' || dst == 'C' || (what == 'd' && dst == 'D')) ? src : dst;
+  // the reference does not check its indices; out-of-range ones would
+  // address outside the records, so they are refused here
+  if (i_c < 0 || i_c > 2 || i_s < 0 || i_s > (cont == 'H' ? 1 : 3) || j_c < 0 || j_c > 2 || j_s < 0 || j_s > 3) {
+    set_error(QLAGPU_ERR_ARG, kid, "colour or spin index out of range");
+    return;
+  }
+  int cnt = 0;
+  auto put = [&](int ic, int is) {
+    int o, s;
+    if (what == 'e') {
+      o = (dst == 'C') ? 0 : sf_elem(dst, i_c, i_s, j_c, j_s);
+      s = (src == 'C') ? 0 : sf_elem(src, i_c, i_s, j_c, j_s);
+    } else if (what == 'c') {
+      // the colour loop index is ic; in an M the column vector is (ic, j_c)
+      const int ce = sf_elem(cont, ic, i_s, j_c, j_s);
+      o = (dst == 'V') ? ic : ce;
+      s = (src == 'V') ? ic : ce;
+    } else {
+      const int pe = sf_elem('P', ic, is, j_c, j_s);
+      const int de = sf_elem('D', ic, is, 0, 0);
+      o = (dst == 'D') ? de : pe;
+      s = (src == 'D') ? de : pe;
+    }
+    p.oi[cnt] = o;
+    p.si[cnt] = s;
+    cnt++;
+  };
+  if (what == 'e') {
+    put(0, 0);
+  } else if (what == 'c') {
+    for (int ic = 0; ic < 3; ic++) put(ic, 0);
+  } else {
+    for (int ic = 0; ic < 3; ic++)
+      for (int is = 0; is < 4; is++) put(ic, is);
+  }
+  p.cnt = cnt;
+  sf_launch<R, NE_OUT, NE_SRC, SF_SUB>(kid, p, RecConst<R, 1>{});
+}
+
+// gamma_mu = product of the basis matrices gamma_b for the set bits b of mu,
+// in increasing bit order (lib/perl/expressions_gamma.pl:59-134, the
+// DeGrand-Rossi basis).  Every row and column holds exactly one entry from
+// {1, i, -1, -i}.  Entries are (re, im) pairs of small integers.
+struct GammaTable {
+  int row_src[16][4], row_ph[16][4];  // left:  r_s = ph * a_src (row s of gamma)
+  int col_src[16][4], col_ph[16][4];  // right: r_s = ph * a_src (column s of gamma)
+};
+
+inline const GammaTable& gamma_table() {
+  static const GammaTable tab = [] {
+    // basis gamma_x, gamma_y, gamma_z, gamma_t as (re, im) per entry [row][col]
+    static const int G[4][4][4][2] = {
+        {{{0, 0}, {0, 0}, {0, 0}, {0, 1}},
+         {{0, 0}, {0, 0}, {0, 1}, {0, 0}},
+         {{0, 0}, {0, -1}, {0, 0}, {0, 0}},
+         {{0, -1}, {0, 0}, {0, 0}, {0, 0}}},
+        {{{0, 0}, {0, 0}, {0, 0}, {-1, 0}},
+         {{0, 0}, {0, 0}, {1, 0}, {0, 0}},
+         {{0, 0}, {1, 0}, {0, 0}, {0, 0}},
+         {{-1, 0}, {0, 0}, {0, 0}, {0, 0}}},
+        {{{0, 0}, {0, 0}, {0, 1}, {0, 0}},
+         {{0, 0}, {0, 0}, {0, 0}, {0, -1}},
+         {{0, -1}, {0, 0}, {0, 0}, {0, 0}},
+         {{0, 0}, {0, 1}, {0, 0}, {0, 0}}},
+        {{{0, 0}, {0, 0}, {1, 0}, {0, 0}},
+         {{0, 0}, {0, 0}, {0, 0}, {1, 0}},
+         {{1, 0}, {0, 0}, {0, 0}, {0, 0}},
+         {{0, 0}, {1, 0}, {0, 0}, {0, 0}}}};
+    GammaTable t{};
+    for (int mu = 0; mu < 16; mu++) {
+      int m[4][4][2] = {};
+      for (int d = 0; d < 4; d++) m[d][d][0] = 1;
+      for (int b = 0; b < 4; b++) {
+        if (!(mu & (1 << b))) continue;
+        int q[4][4][2] = {};
+        for (int r = 0; r < 4; r++)
+          for (int c = 0; c < 4; c++)
+            for (int x = 0; x < 4; x++) {
+              q[r][c][0] += m[r][x][0] * G[b][x][c][0] - m[r][x][1] * G[b][x][c][1];
+              q[r][c][1] += m[r][x][0] * G[b][x][c][1] + m[r][x][1] * G[b][x][c][0];
+            }
+        std::memcpy(m, q, sizeof(m));
+      }
+      auto ph = [](const int* v) { return v[0] == 1 ? 0 : v[1] == 1 ? 1 : v[0] == -1 ? 2 : 3; };
+      for (int s = 0; s < 4; s++)
+        for (int x = 0; x < 4; x++) {
+          if (m[s][x][0] || m[s][x][1]) {
+            t.row_src[mu][s] = x;
+            t.row_ph[mu][s] = ph(m[s][x]);
+          }
+          if (m[x][s][0] || m[x][s][1]) {
+            t.col_src[mu][s] = x;
+            t.col_ph[mu][s] = ph(m[x][s]);
+          }
+        }
+    }
+    return t;
+  }();
+  return tab;
+}
+
+// D = gamma_mu D, P = gamma_mu P (LEFT) or P = P gamma_mu
+template <typename R, int NE, bool LEFT>
+inline void api_gamma(const char* kid, void* r, Opnd a, int mu, const int* gang, int n) {
+  if (mu < 0 || mu > 15) {
+    // the reference prints this and leaves r unchanged (expressions_gamma.pl:466-470)
+    std::printf("Gamma matrix %d not supported\n", mu);
+    set_error(QLAGPU_ERR_ARG, kid, "gamma matrix index outside 0..15");
+    return;
+  }
+  SfParams p;
+  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
+  const GammaTable& t = gamma_table();
+  for (int s = 0; s < 4; s++) {
+    p.gs[s] = LEFT ? t.row_src[mu][s] : t.col_src[mu][s];
+    p.gp[s] = LEFT ? t.row_ph[mu][s] : t.col_ph[mu][s];
+  }
+  if constexpr (LEFT)
+    sf_launch<R, NE, NE, SF_GAMMA_L>(kid, p, RecConst<R, 1>{});
+  else
+    sf_launch<R, NE, NE, SF_GAMMA_R>(kid, p, RecConst<R, 1>{});
+}
+
+template <typename R, int KIND>
+inline void api_trace(const char* kid, void* r, Opnd a, const int* gang, int n) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
+  sf_launch<R, 1, 9, KIND>(kid, p, RecConst<R, 1>{});
+}
+
+template <typename R>
+inline void api_antiherm(const char* kid, void* r, Opnd a, const int* gang, int n) {
+  SfParams p;
+  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
+  sf_launch<R, 9, 9, SF_ANTIHERM>(kid, p, RecConst<R, 1>{});
+}
+
+// ---------------------------------------------------------------------------
+// Global reductions over P records and over the permuted (Ma, Pa) forms:
+// each site's sum is formed in double in the reference's element order
+// (ldot_site), and the sites are added in double-double, as in the other
+// global reductions.  Records are staged through shared memory with
+// coalesced loads when contiguous, as in ldot_smem_kernel.
+
+template <int KIND, typename OUT>
+struct GDotFinish {
+  static constexpr int NACC = (KIND >= LD_REDOT) ? 1 : 2;
+  __device__ static void finish(const SiteParams& p, const double* tot) {
+    if constexpr (NACC == 1)
+      write_real<OUT>(p, tot[0]);
+    else
+      write_cplx<OUT>(p, tot[0], tot[1]);
+  }
+};
+
+template <typename R, int NE, int KIND, int PERM, int S, typename OUT>
+__global__ void __launch_bounds__(128) gdot_kernel(const EwParams p, const SiteParams rp, int staged) {
+  using FIN = GDotFinish<KIND, OUT>;
+  extern __shared__ __align__(16) unsigned char gdsm[];
+  DD acc[ArrN<FIN::NACC>::value];
+#pragma unroll
+  for (int a = 0; a < ArrN<FIN::NACC>::value; a++) acc[a] = DD{0.0, 0.0};
+  auto add = [&](double xr, double xi) {
+    dd_add(acc[0], xr);
+    if constexpr (FIN::NACC > 1) dd_add(acc[1], xi);
+  };
+  if (staged) {
+    constexpr int ST = NE + 1;
+    Cx<R>* sa = reinterpret_cast<Cx<R>*>(gdsm);
+    Cx<R>* sb = sa + S * ST;
+    const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
+    const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);
+    const long long ntile = (p.n + S - 1) / S;
+    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+      const long long s0 = tile * S;
+      const int ns = (int)((p.n - s0) < S ? (p.n - s0) : S);
+      const long long base = s0 * NE;
+      for (int f = threadIdx.x; f < ns * NE; f += blockDim.x) {
+        const int row = f / NE, col = f - row * NE;
+        sa[row * ST + col] = A[base + f];
+        if constexpr (KIND != LD_NORM2) sb[row * ST + col] = B[base + f];
+      }
+      __syncthreads();
+      if (threadIdx.x < ns) {
+        double xr, xi;
+        const Cx<R>* ra = sa + threadIdx.x * ST;
+        ldot_site<R, NE, KIND, PERM>(ra, KIND == LD_NORM2 ? ra : sb + threadIdx.x * ST, xr, xi);
+        add(xr, xi);
+      }
+      __syncthreads();
+    }
+  } else {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
+         i += (long long)gridDim.x * blockDim.x) {
+      const long long k = p.gang ? (long long)p.gang[i] : i;
+      const Cx<R>* a = rec_ptr<R>(p.b, k, NE);
+      const Cx<R>* b = (KIND == LD_NORM2) ? a : rec_ptr<R>(p.c, k, NE);
+      double xr, xi;
+      ldot_site<R, NE, KIND, PERM>(a, b, xr, xi);
+      add(xr, xi);
+    }
+  }
+  reduce_finish<FIN>(rp, acc);
+}
+
+// r: host (synchronous) or device (asynchronous) output of OUT values
+template <typename R, int NE, int KIND, int PERM, typename OUT>
+inline void api_gdot(const char* kid, void* r, Opnd a, Opnd b, const int* gang, int n) {
+  constexpr int NACC = GDotFinish<KIND, OUT>::NACC;
+  const size_t rbytes = NACC * sizeof(OUT);
+  if (!r || (n > 0 && (!opnd_ok(a) || (KIND != LD_NORM2 && !opnd_ok(b))))) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  cudaStream_t st = current_stream();
+  const bool dev_out = is_device_ptr(r);
+  if (n <= 0) {
+    // the reference loops zero times and stores its zero sum
+    if (dev_out)
+      cudaMemsetAsync(r, 0, rbytes, st);
+    else
+      std::memset(r, 0, rbytes);
+    return;
+  }
+  const int sms = device_sm_count();
+  ReduceScratch* rs = reduce_scratch(st, 32 * sms + 64);
+  if (!rs) return;
+  EwParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.b = a;
+  p.c = b;
+  p.gang = gang;
+  p.n = n;
+  SiteParams rp;
+  std::memset(&rp, 0, sizeof(rp));
+  rp.partials = rs->partials;
+  rp.counter = rs->counter;
+  rp.result = dev_out ? r : rs->result;
+  constexpr int S = NE > 32 ? 32 : 128;
+  const int staged = (gang == nullptr && a.mode == OM_CONTIG && (KIND == LD_NORM2 || b.mode == OM_CONTIG)) ? 1 : 0;
+  const size_t smem = staged ? (size_t)(KIND == LD_NORM2 ? 1 : 2) * S * (NE + 1) * sizeof(Cx<R>) : 0;
+  const void* fn = reinterpret_cast<const void*>(&gdot_kernel<R, NE, KIND, PERM, S, OUT>);
+  static bool attr_set[64] = {false};
+  const int dev = current_device();
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)((size_t)(KIND == LD_NORM2 ? 1 : 2) * S * (NE + 1) * sizeof(Cx<R>)));
+    attr_set[dev] = true;
+  }
+  long long grid = staged ? ((long long)n + S - 1) / S : ((long long)n + 127) / 128;
+  const long long cap = (long long)sms * 8;
+  if (grid > cap) grid = cap;
+  if (grid > rs->max_blocks) grid = rs->max_blocks;
+  gdot_kernel<R, NE, KIND, PERM, S, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 128, smem, st>>>(p, rp, staged);
+  if (!check_launch(kid)) return;
+  if (!dev_out) {
+    if (cudaMemcpyAsync(r, rs->result, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      check_launch(kid);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Global record sums x = sum_i a[i] (build_qla.pl:2449-2484): every real
+// component is summed over the sites separately.  A block of BT threads (a
+// multiple of the NR reals per record and of 32) reads the records as one
+// flat stream, so thread t always meets component t % NR and the loads are
+// coalesced; each thread adds in double-double, the block folds the threads
+// of each component in a fixed order into per-block partials, and the last
+// block folds the partials in block order.
+
+template <typename R, int NR, typename OUT>
+__global__ void __launch_bounds__(1024) gsum_kernel(const EwParams p, DD* partials, unsigned* counter, OUT* result,
+                                                    int flat) {
+  extern __shared__ __align__(16) unsigned char gssm[];
+  DD* red = reinterpret_cast<DD*>(gssm);
+  __shared__ bool is_last;
+  const int BT = blockDim.x;
+  const int c = threadIdx.x % NR;
+  DD acc{0.0, 0.0};
+  const long long total = p.n * NR;
+  for (long long j = (long long)blockIdx.x * BT + threadIdx.x; j < total; j += (long long)gridDim.x * BT) {
+    double v;
+    if (flat) {
+      v = (double)static_cast<const R*>(p.b.base)[j];
+    } else {
+      const long long i = j / NR;
+      const long long k = p.gang ? (long long)p.gang[i] : i;
+      const R* rec = (p.b.mode == OM_PTR) ? static_cast<const R*>(p.b.ptrs[k]) : static_cast<const R*>(p.b.base) + k * NR;
+      v = (double)rec[c];
+    }
+    dd_add(acc, v);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int q = threadIdx.x; q < NR; q += BT) {
+    DD s = red[q];
+    for (int t = q + NR; t < BT; t += NR) dd_merge(s, red[t]);
+    partials[(long long)blockIdx.x * NR + q] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned ticket = atomicAdd(counter, 1u);
+    is_last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  for (int q = threadIdx.x; q < NR; q += BT) {
+    DD s{0.0, 0.0};
+    for (int b = 0; b < (int)gridDim.x; b++) {
+      volatile DD* vp = reinterpret_cast<volatile DD*>(&partials[(long long)b * NR + q]);
+      DD v;
+      v.hi = vp->hi;
+      v.lo = vp->lo;
+      dd_merge(s, v);
+    }
+    result[q] = static_cast<OUT>(__dadd_rn(s.hi, s.lo));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+// r: one record (host: synchronous, device: asynchronous)
+template <typename R, int NE>
+inline void api_gsum(const char* kid, void* r, Opnd a, const int* gang, int n) {
+  constexpr int NR = 2 * NE;
+  const size_t rbytes = NR * sizeof(R);
+  if (!r || (n > 0 && !opnd_ok(a))) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  cudaStream_t st = current_stream();
+  const bool dev_out = is_device_ptr(r);
+  if (n <= 0) {
+    if (dev_out)
+      cudaMemsetAsync(r, 0, rbytes, st);
+    else
+      std::memset(r, 0, rbytes);
+    return;
+  }
+  // block: a multiple of lcm(NR, 32) reals, up to 1024 threads
+  int l = NR;
+  while (l % 32) l += NR;
+  int BT = l;
+  while (BT + l <= 512) BT += l;
+  const int sms = device_sm_count();
+  long long grid = ((long long)n * NR + BT - 1) / BT;
+  const long long cap = (long long)sms * 2;
+  if (grid > cap) grid = cap;
+  if (grid < 1) grid = 1;
+  // partials [grid * NR] DD, then the result record
+  const int need = (int)((grid * NR + (NR * sizeof(R) + sizeof(DD) - 1) / sizeof(DD) + 1) / 2 + 1);
+  ReduceScratch* rs = reduce_scratch(st, need > 32 * sms + 64 ? need : 32 * sms + 64);
+  if (!rs) return;
+  DD* partials = rs->partials;
+  R* res = dev_out ? static_cast<R*>(r) : reinterpret_cast<R*>(rs->partials + grid * NR);
+  EwParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.b = a;
+  p.gang = gang;
+  p.n = n;
+  const int flat = (gang == nullptr && a.mode == OM_CONTIG) ? 1 : 0;
+  gsum_kernel<R, NR, R><<<(unsigned)grid, BT, (size_t)BT * sizeof(DD), st>>>(p, partials, rs->counter, res, flat);
+  if (!check_launch(kid)) return;
+  if (!dev_out) {
+    if (cudaMemcpyAsync(r, res, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      check_launch(kid);
+  }
+}
+
+}  // namespace qlab

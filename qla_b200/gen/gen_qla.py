@@ -72,6 +72,17 @@ CITE["ewise_unary"] = "lib/perl/build_qla.pl:403-469 (conj, i, adjoint and trans
 CITE["ewise_sum"] = "lib/perl/build_qla.pl:1338-1420 (sums, differences, r/c times a field plus / minus a field)"
 CITE["ldot"] = "lib/perl/build_qla.pl:2358-2460 (site-local dot products and norms)"
 CITE["outer"] = "lib/perl/build_qla.pl:1588-1622 (ColorVector times adjoint ColorVector)"
+CITE["fill"] = ("lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), "
+                "make_code_unary.pl (identity, diagfill, zero)")
+CITE["mask"] = "lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)"
+CITE["component"] = ("lib/perl/build_qla.pl:767-931 (array components, colour column vectors and Dirac vectors: "
+                     "extraction and insertion)")
+CITE["gamma"] = ("lib/perl/build_qla.pl:1358-1412 (left / right multiplication by gamma_mu, mu = 0..15), "
+                 "expressions_gamma.pl:59-134, 384-470")
+CITE["trace"] = "lib/perl/build_qla.pl:933-1064 (trace, real / imaginary trace, traceless antihermitian part)"
+CITE["gred"] = ("lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, "
+                "trace of the adjoint-form products Ma.M and Pa.P)")
+CITE["gsum"] = "lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)"
 CITE["reunit"] = ("no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of "
                   "M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64")
 CITE["minv"] = ("lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), "
@@ -649,6 +660,7 @@ def gen_pc(pc, R, P):
                         fns.append(Fn(name, params, body, "redot", CITE["redot"],
                                       dict(dest="r", var=var, a=sa, b=sb, out=outR)))
     fns += gen_ewise(pc, R, P)
+    fns += gen_sitefield(pc, R, P)
     return fns
 
 
@@ -808,6 +820,173 @@ def gen_ewise(pc, R, P):
     return fns
 
 
+def gen_sitefield(pc, R, P):
+    """Fills, copymask, component extraction / insertion, gamma
+    multiplication, traces and the antihermitian part, the global reductions
+    of DiracPropagators and adjoint-form products, and the global sums."""
+    fns = []
+    kid = lambda fam: f'"{pc}_{fam}"'  # noqa: E731
+    cplx, real = f"QLA_{P}_Complex", f"QLA_{P}_Real"
+    outR = R
+
+    def var_tail(var):
+        return ([("int *", "index")] if var == "x" else []), ("index" if var == "x" else "nullptr")
+
+    def emit(name, params, body, fam, kinds):
+        fns.append(Fn(name, params, body, fam, CITE[fam], kinds))
+
+    def src_param(t, p1, argname="a"):
+        """parameter and operand of a field source of record letter t (C and I too)"""
+        ct = {"C": cplx, "R": real, "I": "QLA_Int"}.get(t, ptype(pc, t) if t in REC else None)
+        if p1:
+            return (f"{ct} *RESTRICT *", argname), f"qlab::op_ptr((const void* const*){argname})"
+        return (f"{ct} *RESTRICT", argname), f"qlab::op_contig({argname})"
+
+    for var in ["v", "x"]:
+        tail, gang = var_tail(var)
+        # ---- constant fills, the diagonal fill, zero
+        for T in ["V", "H", "D", "M", "P"]:
+            ne = NE3[T]
+            rt = f"{ptype(pc, T)} *RESTRICT"
+            for eq in EQOPS:
+                name = f"QLA_{pc}_{T}_{var}{eq}_{T.lower()}"
+                params = [(rt, "r"), (f"{ptype(pc, T)} *RESTRICT", "a")] + tail + [("int", "n")]
+                body = f"qlab::api_fill<{R}, {ne}>({kid('fill')}, r, a, {gang}, n, {EQ_ENUM[eq]});"
+                emit(name, params, body, "fill", dict(dest=T, eqop=eq, var=var, op="fill", a=T.lower()))
+            name = f"QLA_{pc}_{T}_{var}eq_zero"
+            params = [(rt, "r")] + tail + [("int", "n")]
+            emit(name, params, f"qlab::api_zero<{R}, {ne}>({kid('fill')}, r, {gang}, n);", "fill",
+                 dict(dest=T, eqop="eq", var=var, op="zero"))
+            # ---- copymask
+            for pa_, pm_ in itertools.product((False, True), (False, True)):
+                pa, oa = src_param(T, pa_)
+                pm, om = src_param("I", pm_, "b")
+                sa = ("p" if pa_ else "") + T
+                sm = ("p" if pm_ else "") + "I"
+                name = f"QLA_{pc}_{T}_{var}eq_{sa}_mask_{sm}"
+                params = [(rt, "r"), pa, pm] + tail + [("int", "n")]
+                body = f"qlab::api_mask<{R}, {ne}>({kid('mask')}, r, {oa}, {om}, {gang}, n);"
+                emit(name, params, body, "mask", dict(dest=T, eqop="eq", var=var, op="mask", a=sa, b=sm))
+        for eq in EQOPS:
+            name = f"QLA_{pc}_M_{var}{eq}_c"
+            params = [(f"{ptype(pc, 'M')} *RESTRICT", "r"), (f"{cplx} *RESTRICT", "a")] + tail + [("int", "n")]
+            body = f"qlab::api_diagfill<{R}>({kid('fill')}, r, a, {gang}, n, {EQ_ENUM[eq]});"
+            emit(name, params, body, "fill", dict(dest="M", eqop=eq, var=var, op="diagfill", a="c"))
+        # ---- array components, colour columns, Dirac vectors
+        idx_args = {"V": ["i_c"], "H": ["i_c", "i_s"], "D": ["i_c", "i_s"], "M": ["i_c", "j_c"],
+                    "P": ["i_c", "i_s", "j_c", "j_s"]}
+        col_args = {"H": ["i_s"], "D": ["i_s"], "M": ["j_c"], "P": ["i_s", "j_c", "j_s"]}
+
+        def call_sub(what, dst, src, args, ne_out, ne_src, oa):
+            vals = {k: (k if k in args else "0") for k in ("i_c", "i_s", "j_c", "j_s")}
+            return (f"qlab::api_sub<{R}, {ne_out}, {ne_src}>({kid('component')}, r, {oa}, {gang}, n, '{what}', "
+                    f"'{dst}', '{src}', {vals['i_c']}, {vals['i_s']}, {vals['j_c']}, {vals['j_s']});")
+
+        for T in ["V", "H", "D", "M", "P"]:
+            args = idx_args[T]
+            ip = [("int", a_) for a_ in args]
+            for p1 in (False, True):
+                # C = elem(T)
+                pa, oa = src_param(T, p1)
+                name = f"QLA_{pc}_C_{var}eq_elem_{'p' if p1 else ''}{T}"
+                params = [(f"{cplx} *RESTRICT", "r"), pa] + ip + tail + [("int", "n")]
+                emit(name, params, call_sub("e", "C", T, args, 1, NE3[T], oa), "component",
+                     dict(dest="C", eqop="eq", var=var, op="elem", a=("p" if p1 else "") + T, idx=args))
+                # elem(T) = C
+                pa, oa = src_param("C", p1)
+                name = f"QLA_{pc}_{T}_{var}eq_elem_{'p' if p1 else ''}C"
+                params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa] + ip + tail + [("int", "n")]
+                emit(name, params, call_sub("e", T, "C", args, NE3[T], 1, oa), "component",
+                     dict(dest=T, eqop="eq", var=var, op="elem", a=("p" if p1 else "") + "C", idx=args))
+        for T in ["H", "D", "M", "P"]:
+            args = col_args[T]
+            ip = [("int", a_) for a_ in args]
+            for p1 in (False, True):
+                pa, oa = src_param(T, p1)
+                name = f"QLA_{pc}_V_{var}eq_colorvec_{'p' if p1 else ''}{T}"
+                params = [(f"{ptype(pc, 'V')} *RESTRICT", "r"), pa] + ip + tail + [("int", "n")]
+                emit(name, params, call_sub("c", "V", T, args, 3, NE3[T], oa), "component",
+                     dict(dest="V", eqop="eq", var=var, op="colorvec", a=("p" if p1 else "") + T, idx=args))
+                pa, oa = src_param("V", p1)
+                name = f"QLA_{pc}_{T}_{var}eq_colorvec_{'p' if p1 else ''}V"
+                params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa] + ip + tail + [("int", "n")]
+                emit(name, params, call_sub("c", T, "V", args, NE3[T], 3, oa), "component",
+                     dict(dest=T, eqop="eq", var=var, op="colorvec", a=("p" if p1 else "") + "V", idx=args))
+        for p1 in (False, True):
+            args = ["j_c", "j_s"]
+            ip = [("int", a_) for a_ in args]
+            pa, oa = src_param("P", p1)
+            name = f"QLA_{pc}_D_{var}eq_diracvec_{'p' if p1 else ''}P"
+            params = [(f"{ptype(pc, 'D')} *RESTRICT", "r"), pa] + ip + tail + [("int", "n")]
+            emit(name, params, call_sub("d", "D", "P", args, 12, 144, oa), "component",
+                 dict(dest="D", eqop="eq", var=var, op="diracvec", a=("p" if p1 else "") + "P", idx=args))
+            pa, oa = src_param("D", p1)
+            name = f"QLA_{pc}_P_{var}eq_diracvec_{'p' if p1 else ''}D"
+            params = [(f"{ptype(pc, 'P')} *RESTRICT", "r"), pa] + ip + tail + [("int", "n")]
+            emit(name, params, call_sub("d", "P", "D", args, 144, 12, oa), "component",
+                 dict(dest="P", eqop="eq", var=var, op="diracvec", a=("p" if p1 else "") + "D", idx=args))
+        # ---- gamma multiplication
+        for T, sides in (("D", ("left",)), ("P", ("left", "right"))):
+            for side in sides:
+                for p1 in (False, True):
+                    pa, oa = src_param(T, p1)
+                    sa = ("p" if p1 else "") + T
+                    name = (f"QLA_{pc}_{T}_{var}eq_gamma_times_{sa}" if side == "left"
+                            else f"QLA_{pc}_{T}_{var}eq_{sa}_times_gamma")
+                    params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa, ("int", "mu")] + tail + [("int", "n")]
+                    body = (f"qlab::api_gamma<{R}, {NE3[T]}, {str(side == 'left').lower()}>({kid('gamma')}, r, {oa}, "
+                            f"mu, {gang}, n);")
+                    emit(name, params, body, "gamma", dict(dest=T, eqop="eq", var=var, op="gamma_" + side, a=sa))
+        # ---- traces and the antihermitian part
+        for p1 in (False, True):
+            pa, oa = src_param("M", p1)
+            sa = ("p" if p1 else "") + "M"
+            for dest, op, kind, rtype in (("C", "trace", "SF_TRACE_C", cplx), ("R", "re_trace", "SF_TRACE_RE", real),
+                                          ("R", "im_trace", "SF_TRACE_IM", real)):
+                name = f"QLA_{pc}_{dest}_{var}eq_{op}_{sa}"
+                params = [(f"{rtype} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                body = f"qlab::api_trace<{R}, qlab::{kind}>({kid('trace')}, r, {oa}, {gang}, n);"
+                emit(name, params, body, "trace", dict(dest=dest, eqop="eq", var=var, op=op, a=sa))
+            name = f"QLA_{pc}_M_{var}eq_antiherm_{sa}"
+            params = [(f"{ptype(pc, 'M')} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+            body = f"qlab::api_antiherm<{R}>({kid('trace')}, r, {oa}, {gang}, n);"
+            emit(name, params, body, "trace", dict(dest="M", eqop="eq", var=var, op="antiherm", a=sa))
+        # ---- global reductions of P and of the adjoint-form products
+        greds = [("c", "Ma", "M", "M", "LD_ADOT", "qlab::PERM_M"), ("c", "P", "P", "P", "LD_DOT", "qlab::PERM_ID"),
+                 ("c", "Pa", "P", "P", "LD_ADOT", "qlab::PERM_P"), ("r", "P", "P", "P", "LD_REDOT", "qlab::PERM_ID")]
+        for dest, ta, T, tb, kind, perm in greds:
+            for pa_, pb_ in itertools.product((False, True), (False, True)):
+                pa, oa = src_param(T, pa_)
+                pb, ob = src_param(tb, pb_, "b")
+                sa = ("p" if pa_ else "") + ta
+                sb = ("p" if pb_ else "") + tb
+                op = "re_" if kind == "LD_REDOT" else ""
+                name = f"QLA_{pc}_{dest}_{var}eq_{op}{sa}_dot_{sb}"
+                rtype = real if dest == "r" else cplx
+                params = [(f"{rtype} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                body = (f"qlab::api_gdot<{R}, {NE3[T]}, qlab::{kind}, {perm}, {outR}>({kid('gred')}, r, {oa}, {ob}, "
+                        f"{gang}, n);")
+                emit(name, params, body, "gred", dict(dest=dest, eqop="eq", var=var, a=sa, b=sb, kind=kind))
+        for p1 in (False, True):
+            pa, oa = src_param("P", p1)
+            sa = ("p" if p1 else "") + "P"
+            name = f"QLA_{pc}_r_{var}eq_norm2_{sa}"
+            params = [(f"{real} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+            body = (f"qlab::api_gdot<{R}, 144, qlab::LD_NORM2, qlab::PERM_ID, {outR}>({kid('gred')}, r, {oa}, "
+                    f"qlab::Opnd{{}}, {gang}, n);")
+            emit(name, params, body, "gred", dict(dest="r", eqop="eq", var=var, a=sa, kind="LD_NORM2"))
+        # ---- global sums
+        for T in ["V", "H", "D", "M", "P"]:
+            for p1 in (False, True):
+                pa, oa = src_param(T, p1)
+                sa = ("p" if p1 else "") + T
+                name = f"QLA_{pc}_{T.lower()}_{var}eq_sum_{sa}"
+                params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                body = f"qlab::api_gsum<{R}, {NE3[T]}>({kid('gsum')}, r, {oa}, {gang}, n);"
+                emit(name, params, body, "gsum", dict(dest=T.lower(), eqop="eq", var=var, a=sa))
+    return fns
+
+
 HEADER_TOP = """/*
  * {fname} -- GENERATED by qla_b200/gen/gen_qla.py; do not edit.
  *
@@ -892,6 +1071,8 @@ def main():
                  "ldot": '#include "../qla_ewise.cuh"\n'}.get(family, "")
         if family.startswith("ewise"):
             extra = '#include "../qla_ewise.cuh"\n'
+        if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum"):
+            extra = '#include "../qla_sitefield.cuh"\n'
         if pc == "FN" and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
         if pc == "FN" and family == "mfunc_ext":

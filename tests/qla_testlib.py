@@ -42,6 +42,22 @@ def ref():
     return _ref
 
 
+class ref_one_thread:
+    """Runs the reference library's OpenMP loops on one thread (the sequential
+    summation order of its reductions) inside the with-block."""
+
+    def __enter__(self):
+        ref()
+        self.gomp = ctypes.CDLL("libgomp.so.1")
+        self.prev = self.gomp.omp_get_max_threads()
+        self.gomp.omp_set_num_threads(1)
+        return self
+
+    def __exit__(self, *exc):
+        self.gomp.omp_set_num_threads(self.prev)
+        return False
+
+
 def ptr(a):
     """ctypes void pointer to a numpy array (None for None)."""
     if a is None:
@@ -433,7 +449,7 @@ EW_SHAPES = {"COPY": 0, "CONJ": 1, "I": 2, "CT": 3, "CTA": 4, "CAT": 5, "CATA": 
 LD_KINDS = {"LD_DOT": 0, "LD_DOT_AA": 1, "LD_ADOT": 2, "LD_REDOT": 3, "LD_NORM2": 4}
 NE3 = {"V": 3, "H": 6, "D": 12, "M": 9, "P": 144}
 _TYPE_OF = {"ColorVector": "V", "HalfFermion": "H", "DiracFermion": "D", "ColorMatrix": "M",
-            "DiracPropagator": "P", "Complex": "C", "Real": "R"}
+            "DiracPropagator": "P", "Complex": "C", "Real": "R", "QLA_Int": "I"}
 
 
 def param_type(ctype):
@@ -562,4 +578,123 @@ def ewise_oracle(e, ins, idx, gang, n):
                                        ptr(arr(c_name)) if c_name else None, ptr(s_arr), kw["scal_kind"],
                                        cs(sre), cs(sim), ctypes.c_long(nsites), ne, ptr(ix(b_name)),
                                        ptr(ix(c_name)) if c_name else None, ptr(s_idx), ptr(g))
+    return r
+
+
+# ---------------------------------------------------------------------------
+# site-field families (fills, copymask, components, gamma multiplication,
+# traces) and the global P / adjoint-form reductions and global sums
+
+SF_FAMILIES = ("fill", "mask", "component", "gamma", "trace")
+NE_OF = dict(NE3, C=1)
+
+
+def rec_bytes(letter, dt):
+    """bytes per record of a field of the given letter in precision dt"""
+    if letter == "I":
+        return 4
+    return np.dtype(dt).itemsize * (1 if letter == "R" else 2 * NE_OF[letter])
+
+
+def _letter(src):
+    return src[1:] if src.startswith("p") and len(src) > 1 else src
+
+
+def sitefield_inputs(e, rng, dt, n, ns):
+    """Seeded inputs for a site-field entry: (ins, idx, gang, ints) with ins
+    as ewise_inputs, ints the values of the int arguments (colour / spin
+    indices, mu)."""
+    ins, ints = {}, {}
+    half = e.get("dest") == "H" or _letter(e.get("a", "")) == "H"
+    for t, name in zip(e["ctypes"], e["params"]):
+        if name in ("n", "index"):
+            continue
+        if t == "int":
+            hi = {"mu": 16, "i_c": 3, "j_c": 3, "i_s": 2 if half else 4, "j_s": 4}[name]
+            ints[name] = int(rng.integers(0, hi))
+            continue
+        letter, is_ptr = param_type(t)
+        nrec = n if name == "r" else ns
+        if name == "a" and e.get("op") in ("fill", "diagfill"):
+            nrec = 1
+        if letter == "I":
+            arr = rng.choice(np.array([0, 0, 1, -3, 7], np.int32), nrec)
+        elif letter == "R":
+            arr = rng.standard_normal(nrec).astype(dt)
+        elif letter == "C":
+            arr = rng.standard_normal((nrec, 2)).astype(dt)
+        else:
+            arr = rng.standard_normal((nrec, 2 * NE3[letter])).astype(dt)
+        if name == "a" and e.get("op") in ("fill", "diagfill"):
+            arr = arr.reshape(-1)
+        ins[name] = (letter, is_ptr, arr)
+    idx = {name: rng.integers(0, ns, n).astype(np.int32) for name, v in ins.items() if v[1]}
+    gang = rng.permutation(n)[: n // 2 + 1].astype(np.int32) if e["var"] == "x" else None
+    return ins, idx, gang, ints
+
+
+def sitefield_oracle(e, ins, idx, gang, n, ints):
+    """The oracle's result for a site-field entry on sitefield_inputs()."""
+    r = ins["r"][2].copy()
+    t = rtype(r.dtype)
+    g = _i32(gang)
+    nsites = ctypes.c_long(len(gang) if gang is not None else n)
+    eq = EQOPS[e.get("eqop", "eq")]
+    O = oracle()
+    op, fam = e.get("op"), e["family"]
+
+    def arr(name):
+        return ins[name][2] if name in ins else None
+
+    def ix(name):
+        return _i32(idx.get(name))
+
+    if op == "fill":
+        getattr(O, "ora_fill_" + t)(eq, ptr(r), ptr(arr("a")), nsites, NE3[e["dest"]], ptr(g))
+    elif op == "diagfill":
+        getattr(O, "ora_diagfill_" + t)(eq, ptr(r), ptr(arr("a")), nsites, ptr(g))
+    elif op == "zero":
+        getattr(O, "ora_zero_" + t)(ptr(r), nsites, NE3[e["dest"]], ptr(g))
+    elif op == "mask":
+        getattr(O, "ora_mask_" + t)(ptr(r), ptr(arr("a")), ptr(arr("b")), nsites, NE3[e["dest"]], ptr(ix("a")),
+                                    ptr(ix("b")), ptr(g))
+    elif fam == "component":
+        what = {"elem": "e", "colorvec": "c", "diracvec": "d"}[op]
+        getattr(O, "ora_component_" + t)(ord(what), ord(e["dest"]), ord(_letter(e["a"])), ptr(r), ptr(arr("a")),
+                                         ints.get("i_c", 0), ints.get("i_s", 0), ints.get("j_c", 0),
+                                         ints.get("j_s", 0), nsites, ptr(ix("a")), ptr(g))
+    elif fam == "gamma":
+        getattr(O, "ora_gamma_" + t)(1 if op == "gamma_right" else 0, NE3[e["dest"]], ints["mu"], ptr(r),
+                                     ptr(arr("a")), nsites, ptr(ix("a")), ptr(g))
+    elif fam == "trace":
+        kind = {"trace": 0, "re_trace": 1, "im_trace": 2, "antiherm": 3}[op]
+        getattr(O, "ora_trace_" + t)(kind, ptr(r), ptr(arr("a")), nsites, ptr(ix("a")), ptr(g))
+    else:
+        raise ValueError(e["name"])
+    return r
+
+
+def gred_oracle(e, ins, idx, gang, n):
+    """Reference-order global reduction (re, im) in double for a gred entry."""
+    a = ins["a"][2]
+    t = rtype(a.dtype)
+    out = np.zeros(2, np.float64)
+    kind = LD_KINDS[e["kind"]]
+    perm = _perm_code(_letter(e["a"]).rstrip("a"))
+    b = ins["b"][2] if "b" in ins else None
+    getattr(oracle(), "ora_gdot_" + t)(kind, perm, ptr(out), ptr(a), ptr(b),
+                                       ctypes.c_long(len(gang) if gang is not None else n),
+                                       NE3[_letter(e["a"]).rstrip("a")], ptr(_i32(idx.get("a"))),
+                                       ptr(_i32(idx.get("b"))), ptr(_i32(gang)))
+    return out
+
+
+def gsum_oracle(e, ins, idx, gang, n):
+    """Reference-order global sum (one record, site precision) for a gsum entry."""
+    a = ins["a"][2]
+    t = rtype(a.dtype)
+    T = _letter(e["a"])
+    r = np.zeros(2 * NE3[T], a.dtype)
+    getattr(oracle(), "ora_gsum_" + t)(ptr(r), ptr(a), ctypes.c_long(len(gang) if gang is not None else n), NE3[T],
+                                       ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
     return r

@@ -314,7 +314,7 @@ def test_oracle_n_colour_matrix_functions_match_reference_library(pc, dt):
             assert T.bits_equal(rr, T.ora_minv(g, b, n, nb, nc=nc)), (nc, dest)
 
 
-def _ref_args(e, ins, idx, gang, n, r):
+def _ref_args(e, ins, idx, gang, n, r, ints=None):
     """Host arguments of manifest entry e for the reference library."""
     args, keep = [], []
     for t, name in zip(e["ctypes"], e["params"]):
@@ -324,10 +324,12 @@ def _ref_args(e, ins, idx, gang, n, r):
             args.append(T.ptr(gang))
         elif name == "r":
             args.append(T.ptr(r))
+        elif t == "int":
+            args.append(ints[name])
         else:
             letter, is_ptr, arr = ins[name]
             if is_ptr:
-                rec = arr.itemsize * (1 if letter == "R" else 2 if letter == "C" else 2 * T.NE3[letter])
+                rec = T.rec_bytes(letter, arr.dtype)
                 pa = (ctypes.c_void_p * len(idx[name]))(*[arr.ctypes.data + int(j) * rec for j in idx[name]])
                 keep.append(pa)
                 args.append(pa)
@@ -360,4 +362,67 @@ def test_oracle_elementwise_families_match_reference_library(pc, dt):
         if not T.bits_equal(r, want):
             bad.append(e["name"])
     assert count > 1800
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+def test_oracle_sitefield_families_match_reference_library(pc, dt):
+    """Fills, copymask, components, gamma multiplication (all 16 mu for D and
+    both sides of P), traces and the antihermitian part: the oracle against
+    the reference library, bit for bit, every generated entry point."""
+    import json
+    man = json.load(open(os.path.join(os.path.dirname(T.ORACLE_SO), "..", "qla_b200", "gen", "api_manifest.json")))
+    R = T.ref()
+    rng = np.random.default_rng(111)
+    n, ns = 13, 17
+    bad, count = [], 0
+    for e in man:
+        if e["pc"] != pc or e["family"] not in T.SF_FAMILIES:
+            continue
+        reps = 16 if e["family"] == "gamma" else 1
+        for rep in range(reps):
+            ins, idx, gang, ints = T.sitefield_inputs(e, rng, dt, n, ns)
+            if "mu" in ints:
+                ints["mu"] = rep
+            want = T.sitefield_oracle(e, ins, idx, gang, n, ints)
+            r = ins["r"][2].copy()
+            args, keep = _ref_args(e, ins, idx, gang, n, r, ints)
+            getattr(R, e["name"])(*args)
+            count += 1
+            if not T.bits_equal(r, want):
+                bad.append((e["name"], ints))
+    assert count > 300
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+def test_oracle_global_p_reductions_and_sums_match_reference_library(pc, dt):
+    """Global reductions of P, Ma.M and Pa.P and the global sums: the oracle
+    (reference summation order) against the reference library run on one
+    OpenMP thread (its sequential order), bit for bit."""
+    import json
+    man = json.load(open(os.path.join(os.path.dirname(T.ORACLE_SO), "..", "qla_b200", "gen", "api_manifest.json")))
+    R = T.ref()
+    rng = np.random.default_rng(112)
+    n, ns = 13, 17
+    bad, count = [], 0
+    for e in man:
+        if e["pc"] != pc or e["family"] not in ("gred", "gsum"):
+            continue
+        ins, idx, gang, _ = T.sitefield_inputs(e, rng, dt, n, ns)
+        if e["family"] == "gred":
+            out = T.gred_oracle(e, ins, idx, gang, n)
+            want = out[:1].astype(dt) if e["dest"] == "r" else out.astype(dt)
+        else:
+            want = T.gsum_oracle(e, ins, idx, gang, n)
+        r = np.zeros_like(want)
+        args, keep = _ref_args(e, ins, idx, gang, n, r)
+        with T.ref_one_thread():
+            getattr(R, e["name"])(*args)
+        count += 1
+        if not T.bits_equal(r, want):
+            bad.append(e["name"])
+    assert count == 56
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
