@@ -89,9 +89,13 @@ void ora_gamma_##SFX(int right, int ne, int mu, R *r, const R *a, long n, const 
 void ora_trace_##SFX(int kind, R *r, const R *a, long n, const int *idx_a, const int *gang);    \
 void ora_gdot_##SFX(int kind, int perm, double *out2, const R *a, const R *b, long n, int ne,     \
                     const int *idx_a, const int *idx_b, const int *gang);                        \
-void ora_gsum_##SFX(R *r, const R *a, long n, int ne, const int *idx_a, const int *gang);
+void ora_gsum_##SFX(double *out, const R *a, long n, int ne, const int *idx_a, const int *gang);
 ORA_SITEFIELD_DECL(float, f)
 ORA_SITEFIELD_DECL(double, d)
+/* precision conversions of n records of nr reals: QLA_DF_c_eq_c (float to
+ * double) and QLA_FD_c_eq_c (double to float, rounded to nearest) */
+void ora_convert_df(double *r, const float *a, long n, int nr, const int *idx_a, const int *gang);
+void ora_convert_fd(float *r, const double *a, long n, int nr, const int *idx_a, const int *gang);
 
 int ora_version(void);
 

@@ -280,17 +280,16 @@ void FN(ora_gdot)(int kind, int perm, double *out2, const R *a, const R *b, long
   out2[1] = si;
 }
 
-/* r = sum over the sites of a, each component in double, rounded to R */
-void FN(ora_gsum)(R *r, const R *a, long n, int ne, const int *idx_a, const int *gang)
+/* out = sum over the sites of a, each component in double (the caller
+ * rounds it to the output precision: R for F3 / D3, double for DF3) */
+void FN(ora_gsum)(double *out, const R *a, long n, int ne, const int *idx_a, const int *gang)
 {
-  double s[288];
-  for (int c = 0; c < 2 * ne; c++) s[c] = 0.;
+  for (int c = 0; c < 2 * ne; c++) out[c] = 0.;
   for (long i = 0; i < n; i++) {
     const long k = gang ? gang[i] : i;
     const long ka = idx_a ? idx_a[k] : k;
-    for (int c = 0; c < 2 * ne; c++) s[c] += (double)a[ka * 2 * ne + c];
+    for (int c = 0; c < 2 * ne; c++) out[c] += (double)a[ka * 2 * ne + c];
   }
-  for (int c = 0; c < 2 * ne; c++) r[c] = (R)s[c];
 }
 
 #undef FN

@@ -115,7 +115,7 @@ class _Fn:
 
     def __call__(self, *args):
         e = self.entry
-        red = e["family"] in ("norm2", "dot", "redot")
+        red = e["family"] in ("norm2", "dot", "redot", "gred")
         ridx = e["params"].index("r") if red else 0
         if len(args) != len(e["params"]) and not (red and len(args) == len(e["params"]) - 1):
             raise TypeError(f"{self.name} takes {len(e['params'])} arguments ({', '.join(e['params'])})")
@@ -170,6 +170,7 @@ class _Namespace:
 F3 = _Namespace("F3")
 D3 = _Namespace("D3")
 DF3 = _Namespace("DF3")
+FD3 = _Namespace("FD3")
 FN = _Namespace("FN")
 DFN = _Namespace("DFN")
 I = _Namespace("I")  # noqa: E741

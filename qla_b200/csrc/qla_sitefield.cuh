@@ -612,11 +612,11 @@ __global__ void __launch_bounds__(1024) gsum_kernel(const EwParams p, DD* partia
   if (threadIdx.x == 0) *counter = 0u;
 }
 
-// r: one record (host: synchronous, device: asynchronous)
-template <typename R, int NE>
+// r: one record of OUT components (host: synchronous, device: asynchronous)
+template <typename R, int NE, typename OUT = R>
 inline void api_gsum(const char* kid, void* r, Opnd a, const int* gang, int n) {
   constexpr int NR = 2 * NE;
-  const size_t rbytes = NR * sizeof(R);
+  const size_t rbytes = NR * sizeof(OUT);
   if (!r || (n > 0 && !opnd_ok(a))) {
     set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
     return;
@@ -641,24 +641,63 @@ inline void api_gsum(const char* kid, void* r, Opnd a, const int* gang, int n) {
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
   // partials [grid * NR] DD, then the result record
-  const int need = (int)((grid * NR + (NR * sizeof(R) + sizeof(DD) - 1) / sizeof(DD) + 1) / 2 + 1);
+  const int need = (int)((grid * NR + (NR * sizeof(OUT) + sizeof(DD) - 1) / sizeof(DD) + 1) / 2 + 1);
   ReduceScratch* rs = reduce_scratch(st, need > 32 * sms + 64 ? need : 32 * sms + 64);
   if (!rs) return;
   DD* partials = rs->partials;
-  R* res = dev_out ? static_cast<R*>(r) : reinterpret_cast<R*>(rs->partials + grid * NR);
+  OUT* res = dev_out ? static_cast<OUT*>(r) : reinterpret_cast<OUT*>(rs->partials + grid * NR);
   EwParams p;
   std::memset(&p, 0, sizeof(p));
   p.b = a;
   p.gang = gang;
   p.n = n;
   const int flat = (gang == nullptr && a.mode == OM_CONTIG) ? 1 : 0;
-  gsum_kernel<R, NR, R><<<(unsigned)grid, BT, (size_t)BT * sizeof(DD), st>>>(p, partials, rs->counter, res, flat);
+  gsum_kernel<R, NR, OUT><<<(unsigned)grid, BT, (size_t)BT * sizeof(DD), st>>>(p, partials, rs->counter, res, flat);
   if (!check_launch(kid)) return;
   if (!dev_out) {
     if (cudaMemcpyAsync(r, res, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
       check_launch(kid);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Precision conversions X_D <- X_F (QLA_DF3_X_*eq_X: exact promotion) and
+// X_F <- X_D (QLA_FD3_X_*eq_X: one round-to-nearest per component),
+// build_qla.pl:356-400 with QLA_DF_c_eq_c / QLA_FD_c_eq_c
+// (include/qla_complex.h): one thread per real component.
+template <typename RIN, typename ROUT, int NR>
+__global__ void __launch_bounds__(256) convert_kernel(const EwParams p) {
+  const long long total = p.n * NR;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long i = g / NR;
+    const int c = (int)(g - i * NR);
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    const RIN* src = (p.b.mode == OM_PTR) ? static_cast<const RIN*>(p.b.ptrs[k]) : static_cast<const RIN*>(p.b.base) + k * NR;
+    static_cast<ROUT*>(p.out)[k * NR + c] = static_cast<ROUT>(src[c]);
+  }
+}
+
+template <typename RIN, typename ROUT, int NE>
+inline void api_convert(const char* kid, void* r, Opnd a, const int* gang, int n) {
+  if (n <= 0) return;
+  if (!r || !opnd_ok(a)) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  EwParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.out = r;
+  p.b = a;
+  p.gang = gang;
+  p.n = n;
+  const long long total = (long long)n * 2 * NE;
+  const long long cap = (long long)device_sm_count() * 16;
+  long long grid = (total + 255) / 256;
+  if (grid > cap) grid = cap;
+  convert_kernel<RIN, ROUT, 2 * NE><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, current_stream()>>>(p);
+  check_launch(kid);
 }
 
 }  // namespace qlab

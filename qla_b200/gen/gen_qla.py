@@ -83,6 +83,8 @@ CITE["trace"] = "lib/perl/build_qla.pl:933-1064 (trace, real / imaginary trace, 
 CITE["gred"] = ("lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, "
                 "trace of the adjoint-form products Ma.M and Pa.P)")
 CITE["gsum"] = "lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)"
+CITE["convert"] = ("lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, "
+                   "QLA_FD_c_eq_c rounding)")
 CITE["reunit"] = ("no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of "
                   "M_veq_Ma_times_M, M_veq_invsqrtPH_M and M_veq_M_times_M fused in FP64")
 CITE["minv"] = ("lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), "
@@ -648,8 +650,6 @@ def gen_pc(pc, R, P):
                                 f"2 * sizeof({outR}), {oa}, {ob}, {gang}, n);")
                         fns.append(Fn(name, params, body, "dot", CITE["dot"],
                                       dict(dest="c", var=var, a=sa, b=sb, out=outR)))
-                        if rpc == "DF3":
-                            continue  # the reference's DF libraries carry no re_dot
                         name = f"QLA_{rpc}_r_{var}eq_re_{sa}_dot_{sb}"
                         params = [(f"QLA_{OP}_Real *RESTRICT", "r"), pa, pb]
                         if var == "x":
@@ -984,6 +984,52 @@ def gen_sitefield(pc, R, P):
                 params = [(f"{ptype(pc, T)} *RESTRICT", "r"), pa] + tail + [("int", "n")]
                 body = f"qlab::api_gsum<{R}, {NE3[T]}>({kid('gsum')}, r, {oa}, {gang}, n);"
                 emit(name, params, body, "gsum", dict(dest=T.lower(), eqop="eq", var=var, a=sa))
+        if pc != "F3":
+            continue
+        # ---- QLA_DF3_: the F3 global reductions and sums returned in double
+        for dest, ta, T, tb, kind, perm in greds:
+            for pa_, pb_ in itertools.product((False, True), (False, True)):
+                pa, oa = src_param(T, pa_)
+                pb, ob = src_param(tb, pb_, "b")
+                sa = ("p" if pa_ else "") + ta
+                sb = ("p" if pb_ else "") + tb
+                op = "re_" if kind == "LD_REDOT" else ""
+                name = f"QLA_DF3_{dest}_{var}eq_{op}{sa}_dot_{sb}"
+                rtype = "QLA_D_Real" if dest == "r" else "QLA_D_Complex"
+                params = [(f"{rtype} *RESTRICT", "r"), pa, pb] + tail + [("int", "n")]
+                body = (f"qlab::api_gdot<float, {NE3[T]}, qlab::{kind}, {perm}, double>({kid('gred_df')}, r, {oa}, "
+                        f"{ob}, {gang}, n);")
+                emit(name, params, body, "gred", dict(dest=dest, eqop="eq", var=var, a=sa, b=sb, kind=kind,
+                                                      out="double"))
+        for p1 in (False, True):
+            pa, oa = src_param("P", p1)
+            sa = ("p" if p1 else "") + "P"
+            name = f"QLA_DF3_r_{var}eq_norm2_{sa}"
+            params = [("QLA_D_Real *RESTRICT", "r"), pa] + tail + [("int", "n")]
+            body = (f"qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, double>({kid('gred_df')}, r, {oa}, "
+                    f"qlab::Opnd{{}}, {gang}, n);")
+            emit(name, params, body, "gred", dict(dest="r", eqop="eq", var=var, a=sa, kind="LD_NORM2", out="double"))
+        for T in ["V", "H", "D", "M", "P"]:
+            for p1 in (False, True):
+                pa, oa = src_param(T, p1)
+                sa = ("p" if p1 else "") + T
+                name = f"QLA_DF3_{T.lower()}_{var}eq_sum_{sa}"
+                params = [(f"{ptype('D3', T)} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                body = f"qlab::api_gsum<float, {NE3[T]}, double>({kid('gsum_df')}, r, {oa}, {gang}, n);"
+                emit(name, params, body, "gsum", dict(dest=T.lower(), eqop="eq", var=var, a=sa, out="double"))
+        # ---- precision conversions D3 <- F3 (QLA_DF3_) and F3 <- D3 (QLA_FD3_)
+        for T in ["V", "H", "D", "M", "P"]:
+            for p1 in (False, True):
+                for lib, rin, rout, pin, pout in (("DF3", "float", "double", "F3", "D3"),
+                                                  ("FD3", "double", "float", "D3", "F3")):
+                    ct = ptype(pin, T)
+                    pa = (f"{ct} *RESTRICT *", "a") if p1 else (f"{ct} *RESTRICT", "a")
+                    oa = "qlab::op_ptr((const void* const*)a)" if p1 else "qlab::op_contig(a)"
+                    sa = ("p" if p1 else "") + T
+                    name = f"QLA_{lib}_{T}_{var}eq_{sa}"
+                    params = [(f"{ptype(pout, T)} *RESTRICT", "r"), pa] + tail + [("int", "n")]
+                    body = f"qlab::api_convert<{rin}, {rout}, {NE3[T]}>({kid('convert')}, r, {oa}, {gang}, n);"
+                    emit(name, params, body, "convert", dict(dest=T, eqop="eq", var=var, a=sa, lib=lib))
     return fns
 
 
@@ -1043,6 +1089,7 @@ def main():
     for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None)]:
         for fn in (gen_int() if pc == "I" else gen_fn() if pc == "FN" else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
+            hpc = {"FD3": "DF3"}.get(hpc, hpc)  # the reference declares QLA_FD3_ in qla_df3.h
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
             manifest.append(dict(name=fn.name, pc=hpc, family=fn.family, params=[n for _, n in fn.params],
@@ -1071,7 +1118,7 @@ def main():
                  "ldot": '#include "../qla_ewise.cuh"\n'}.get(family, "")
         if family.startswith("ewise"):
             extra = '#include "../qla_ewise.cuh"\n'
-        if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum"):
+        if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert"):
             extra = '#include "../qla_sitefield.cuh"\n'
         if pc == "FN" and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'

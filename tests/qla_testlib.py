@@ -690,11 +690,32 @@ def gred_oracle(e, ins, idx, gang, n):
 
 
 def gsum_oracle(e, ins, idx, gang, n):
-    """Reference-order global sum (one record, site precision) for a gsum entry."""
+    """Reference-order global sum (one record) for a gsum entry, rounded to
+    the output precision (the site precision; double for QLA_DF3_)."""
     a = ins["a"][2]
     t = rtype(a.dtype)
     T = _letter(e["a"])
-    r = np.zeros(2 * NE3[T], a.dtype)
-    getattr(oracle(), "ora_gsum_" + t)(ptr(r), ptr(a), ctypes.c_long(len(gang) if gang is not None else n), NE3[T],
-                                       ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
+    out = np.zeros(2 * NE3[T], np.float64)
+    getattr(oracle(), "ora_gsum_" + t)(ptr(out), ptr(a), ctypes.c_long(len(gang) if gang is not None else n),
+                                       NE3[T], ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
+    return out if e.get("out") == "double" else out.astype(a.dtype)
+
+
+def convert_inputs(e, rng, n, ns):
+    """Inputs of a QLA_DF3_ / QLA_FD3_ conversion: (ins, idx, gang)."""
+    src_dt, dst_dt = (np.float32, np.float64) if e["lib"] == "DF3" else (np.float64, np.float32)
+    ne = NE3[e["dest"]]
+    a = rng.standard_normal((ns, 2 * ne)).astype(src_dt)
+    r = rng.standard_normal((n, 2 * ne)).astype(dst_dt)
+    ins = {"r": (e["dest"], False, r), "a": (e["dest"], e["a"].startswith("p"), a)}
+    idx = {"a": rng.integers(0, ns, n).astype(np.int32)} if e["a"].startswith("p") else {}
+    gang = rng.permutation(n)[: n // 2 + 1].astype(np.int32) if e["var"] == "x" else None
+    return ins, idx, gang
+
+
+def convert_oracle(e, ins, idx, gang, n):
+    r = ins["r"][2].copy()
+    f = oracle().ora_convert_df if e["lib"] == "DF3" else oracle().ora_convert_fd
+    f(ptr(r), ptr(ins["a"][2]), ctypes.c_long(len(gang) if gang is not None else n), 2 * NE3[e["dest"]],
+      ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
     return r

@@ -74,9 +74,8 @@ def test_norm2_dot_variants(qla, cuda, pc, dt, t):
         tol = 6e-8 if pc == "F3" else 1e-12
         assert abs(got - exact) <= tol * scale * 2, (var, p1, p2, got, exact)
         assert abs(got - refo) <= (1e-6 if pc == "F3" else 1e-12) * scale * 2
-        if pc != "DF3":
-            gr = getattr(ns_, f"r_{var}eq_re_{sa}_dot_{sb}")(None, pa if p1 else ad, pb if p2 else bd, *extra, n)
-            assert abs(gr - exact.real) <= tol * scale * 2
+        gr = getattr(ns_, f"r_{var}eq_re_{sa}_dot_{sb}")(None, pa if p1 else ad, pb if p2 else bd, *extra, n)
+        assert abs(gr - exact.real) <= tol * scale * 2
 
 
 @pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])

@@ -129,7 +129,7 @@ def _terms_abs(e, ins, idx, gang, n):
     return np.full(2, 0.5 * (np.square(a[ka]).sum() + np.square(b[kb]).sum()))
 
 
-@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64), ("DF3", np.float32)])
 @pytest.mark.parametrize("n", [1, 61, 4099])
 def test_global_p_reductions_and_sums(qla, cuda, pc, dt, n):
     rng = np.random.default_rng(304 + n)
@@ -144,8 +144,9 @@ def test_global_p_reductions_and_sums(qla, cuda, pc, dt, n):
         else:
             want = T.gsum_oracle(e, ins, idx, gang, n).astype(np.float64)
         scale = _terms_abs(e, ins, idx, gang, n)[: len(want)]
+        odt = np.float64 if e.get("out") == "double" else dt
         eps = np.finfo(dt).eps
-        tol = 1e-13 * scale + (4 * eps * np.abs(want) if dt == np.float32 else 0)
+        tol = 1e-13 * scale + (4 * eps * np.abs(want) if odt == np.float32 else 0)
         if dt == np.float32 and e.get("kind") == "LD_NORM2":
             # the reference rounds each |a_e|^2 to float before adding it
             tol = tol + 2 * eps * scale
@@ -153,12 +154,12 @@ def test_global_p_reductions_and_sums(qla, cuda, pc, dt, n):
             keep = []
             args, _ = _dev_args(e, ins, idx, gang, n, dt, {}, keep)
             if dev_out:
-                r_d = cuda.zeros(len(want), dtype=cuda.float32 if dt == np.float32 else cuda.float64, device="cuda")
+                r_d = cuda.zeros(len(want), dtype=cuda.float32 if odt == np.float32 else cuda.float64, device="cuda")
                 args[0] = T.ptr_dev(r_d)
                 getattr(L, e["name"])(*args)
                 got = r_d.cpu().numpy().astype(np.float64)
             else:
-                r_h = np.zeros(len(want), dt)
+                r_h = np.zeros(len(want), odt)
                 args[0] = T.ptr(r_h)
                 getattr(L, e["name"])(*args)
                 got = r_h.astype(np.float64)
@@ -191,3 +192,24 @@ def test_global_sums_are_deterministic_on_large_fields(qla, cuda):
     scale = np.abs(a[:, ::37]).astype(np.float64).sum(axis=0)
     assert np.all(np.abs(got - exact) <= 4 * np.finfo(np.float32).eps * np.abs(exact) + 1e-13 * scale)
     qla.check("large sum")
+
+
+def test_precision_conversions(qla):
+    """QLA_DF3_X_*eq_X and QLA_FD3_X_*eq_X, every entry point, bit for bit."""
+    rng = np.random.default_rng(306)
+    L = qla.lib()
+    n, ns = 61, 67
+    bad = []
+    entries = [x for x in _man() if x["family"] == "convert"]
+    for e in entries:
+        ins, idx, gang = T.convert_inputs(e, rng, n, ns)
+        want = T.convert_oracle(e, ins, idx, gang, n)
+        src_dt = ins["a"][2].dtype
+        keep = []
+        args, r_d = _dev_args(e, ins, idx, gang, n, src_dt, {}, keep)
+        getattr(L, e["name"])(*args)
+        if not T.bits_equal(T.to_host(r_d), want):
+            bad.append(e["name"])
+    qla.check("conversions")
+    assert len(entries) == 40
+    assert not bad, bad[:8]

@@ -397,7 +397,7 @@ def test_oracle_sitefield_families_match_reference_library(pc, dt):
 
 
 @pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
-@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64), ("DF3", np.float32)])
 def test_oracle_global_p_reductions_and_sums_match_reference_library(pc, dt):
     """Global reductions of P, Ma.M and Pa.P and the global sums: the oracle
     (reference summation order) against the reference library run on one
@@ -414,7 +414,8 @@ def test_oracle_global_p_reductions_and_sums_match_reference_library(pc, dt):
         ins, idx, gang, _ = T.sitefield_inputs(e, rng, dt, n, ns)
         if e["family"] == "gred":
             out = T.gred_oracle(e, ins, idx, gang, n)
-            want = out[:1].astype(dt) if e["dest"] == "r" else out.astype(dt)
+            odt = np.float64 if e.get("out") == "double" else dt
+            want = out[:1].astype(odt) if e["dest"] == "r" else out.astype(odt)
         else:
             want = T.gsum_oracle(e, ins, idx, gang, n)
         r = np.zeros_like(want)
@@ -425,4 +426,29 @@ def test_oracle_global_p_reductions_and_sums_match_reference_library(pc, dt):
         if not T.bits_equal(r, want):
             bad.append(e["name"])
     assert count == 56
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+def test_oracle_precision_conversions_match_reference_library():
+    """QLA_DF3_X_*eq_X (float to double) and QLA_FD3_X_*eq_X (double to
+    float): the oracle against the reference library, bit for bit."""
+    import json
+    man = json.load(open(os.path.join(os.path.dirname(T.ORACLE_SO), "..", "qla_b200", "gen", "api_manifest.json")))
+    R = T.ref()
+    rng = np.random.default_rng(113)
+    n, ns = 13, 17
+    bad, count = [], 0
+    for e in man:
+        if e["family"] != "convert":
+            continue
+        ins, idx, gang = T.convert_inputs(e, rng, n, ns)
+        want = T.convert_oracle(e, ins, idx, gang, n)
+        r = ins["r"][2].copy()
+        args, keep = _ref_args(e, ins, idx, gang, n, r)
+        getattr(R, e["name"])(*args)
+        count += 1
+        if not T.bits_equal(r, want):
+            bad.append(e["name"])
+    assert count == 40
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
