@@ -172,6 +172,7 @@ D3 = _Namespace("D3")
 DF3 = _Namespace("DF3")
 FD3 = _Namespace("FD3")
 FN = _Namespace("FN")
+DN = _Namespace("DN")
 DFN = _Namespace("DFN")
 I = _Namespace("I")  # noqa: E741
 

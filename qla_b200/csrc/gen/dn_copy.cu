@@ -1,0 +1,647 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA DN copy entry points (extern "C"), reference: lib/perl/build_qla.pl:370-400 (assignment / gather)
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_DN_V_veq_V(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_veq_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_veq_pV(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_veq_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_vpeq_V(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_vpeq_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_vpeq_pV(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_vpeq_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_vmeq_V(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_vmeq_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_vmeq_pV(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_vmeq_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_veqm_V(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_veqm_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_veqm_pV(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_veqm_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xeq_V(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xeq_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xeq_pV(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xeq_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xpeq_V(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xpeq_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xpeq_pV(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xpeq_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xmeq_V(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xmeq_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xmeq_pV(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xmeq_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xeqm_V(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xeqm_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_V_xeqm_pV(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 2>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 3>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_V_xeqm_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_veq_H(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_veq_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_veq_pH(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_veq_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_vpeq_H(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_vpeq_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_vpeq_pH(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_vpeq_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_vmeq_H(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_vmeq_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_vmeq_pH(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_vmeq_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_veqm_H(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_veqm_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_veqm_pH(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_veqm_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xeq_H(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xeq_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xeq_pH(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xeq_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xpeq_H(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xpeq_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xpeq_pH(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xpeq_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xmeq_H(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xmeq_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xmeq_pH(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xmeq_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xeqm_H(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xeqm_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_H_xeqm_pH(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 6>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_H_xeqm_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_veq_D(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_veq_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_veq_pD(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_veq_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_vpeq_D(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_vpeq_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_vpeq_pD(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_vpeq_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_vmeq_D(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_vmeq_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_vmeq_pD(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_vmeq_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_veqm_D(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_veqm_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_veqm_pD(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_veqm_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xeq_D(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xeq_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xeq_pD(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xeq_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xpeq_D(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xpeq_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xpeq_pD(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xpeq_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xmeq_D(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xmeq_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xmeq_pD(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xmeq_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xeqm_D(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xeqm_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_D_xeqm_pD(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 8>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 12>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 32>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_D_xeqm_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_veq_M(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_veq_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_veq_pM(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_veq_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_vpeq_M(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_vpeq_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_vpeq_pM(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_vpeq_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_vmeq_M(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_vmeq_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_vmeq_pM(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_vmeq_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_veqm_M(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_veqm_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_veqm_pM(int nc, void * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_veqm_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xeq_M(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xeq_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xeq_pM(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xeq_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xpeq_M(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xpeq_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xpeq_pM(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xpeq_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xmeq_M(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xmeq_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xmeq_pM(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xmeq_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xeqm_M(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xeqm_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_M_xeqm_pM(int nc, void * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_map<qlab::CopyOp<double, 4>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 3: qlab::api_map<qlab::CopyOp<double, 9>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 4: qlab::api_map<qlab::CopyOp<double, 16>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    case 8: qlab::api_map<qlab::CopyOp<double, 64>>("DN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_M_xeqm_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,167 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA DN norm2 entry points (extern "C"), reference: lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_DN_r_veq_norm2_V(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_pV(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_V(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_pV(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_H(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_pH(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_H(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_pH(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_D(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 32, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_pD(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 32, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_D(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 32, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_pD(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 32, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_M(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 64, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_norm2_pM(int nc, QLA_D_Real * r, void * a, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 64, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_norm2_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_M(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 64, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_norm2_pM(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 4: qlab::api_reduce<qlab::Norm2Op<double, 16, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    case 8: qlab::api_reduce<qlab::Norm2Op<double, 64, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_norm2_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+}  // extern "C"

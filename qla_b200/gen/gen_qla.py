@@ -124,14 +124,16 @@ def _fn_switch(ncs, call_of_nc, name):
             f"\"nc not compiled (supported: {', '.join(map(str, ncs))})\");\n  }}")
 
 
-def gen_fn():
-    """QLA_FN_ / QLA_DFN_ entry points (colour count nc at run time,
-    doc/qla.tex:595-611): the hot families of gen_pc for nc in FN_NCS."""
+def gen_fn(prec="F"):
+    """QLA_FN_ / QLA_DFN_ (prec "F") or QLA_DN_ (prec "D") entry points
+    (colour count nc at run time, doc/qla.tex:595-611): the hot families of
+    gen_pc for nc in FN_NCS."""
     fns = []
-    R = "float"
+    R = "float" if prec == "F" else "double"
+    LIB = prec + "N"
     cols = {"V": lambda nc: 1, "H": lambda nc: 2, "D": lambda nc: 4, "M": lambda nc: nc}
     ncpl = {"V": lambda nc: nc, "H": lambda nc: 2 * nc, "D": lambda nc: 4 * nc, "M": lambda nc: nc * nc}
-    kid = lambda fam: f'"FN_{fam}"'  # noqa: E731
+    kid = lambda fam: f'"{LIB}_{fam}"'  # noqa: E731
 
     def opnd(ptr, arg):
         return (f"qlab::op_ptr((const void* const*){arg})" if ptr else f"qlab::op_contig({arg})")
@@ -149,7 +151,7 @@ def gen_fn():
                     adja = s1.endswith("a")
                     for s2, p2 in src2s:
                         adjb = s2.endswith("a")
-                        name = f"QLA_FN_{T}_{var}{eq}_{s1}_times_{s2}"
+                        name = f"QLA_{LIB}_{T}_{var}{eq}_{s1}_times_{s2}"
                         call = lambda nc, T=T, adja=adja, adjb=adjb, s1=s1, p2=p2, eq=eq, gang=gang: (
                             f"qlab::api_map<qlab::LMultOp<{R}, {nc}, {cols[T](nc)}, {str(adja).lower()}, "
                             f"{str(adjb).lower()}>>({kid('lmult')}, r, {opnd(s1.startswith('p'), 'a')}, "
@@ -159,7 +161,7 @@ def gen_fn():
                             dict(dest=T, eqop=eq, var=var, a=s1, b=s2))
         for eq in EQOPS:
             for s1 in ["M", "Ma"]:
-                name = f"QLA_FN_{T}_{eq}_{s1}_times_x{T}"
+                name = f"QLA_{LIB}_{T}_{eq}_{s1}_times_x{T}"
                 call = lambda nc, T=T, s1=s1, eq=eq: (
                     f"qlab::api_map<qlab::LMultOp<{R}, {nc}, {cols[T](nc)}, {str(s1 == 'Ma').lower()}, false>>("
                     f"{kid('lmult')}, r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, {EQ_ENUM[eq]});")
@@ -171,21 +173,22 @@ def gen_fn():
             tail = [("int *", "index")] if var == "x" else []
             for eq in EQOPS:
                 for src, p1 in [(T, False), ("p" + T, True)]:
-                    name = f"QLA_FN_{T}_{var}{eq}_r_times_{src}"
+                    name = f"QLA_{LIB}_{T}_{var}{eq}_r_times_{src}"
                     call = lambda nc, T=T, p1=p1, eq=eq, gang=gang: (
                         f"qlab::api_scalar_map<qlab::RTimesOp<{R}, {ncpl[T](nc)}>, {R}>({kid('rtimes')}, r, "
-                        f"(const float*)a, {opnd(p1, 'b')}, {gang}, n, {EQ_ENUM[eq]});")
-                    add(name, [("void *", "r"), ("QLA_F_Real *", "a"), ("void *", "b")] + tail + [("int", "n")],
+                        f"(const {R}*)a, {opnd(p1, 'b')}, {gang}, n, {EQ_ENUM[eq]});")
+                    add(name, [("void *", "r"), (f"QLA_{prec}_Real *", "a"), ("void *", "b")] + tail + [("int", "n")],
                         _fn_switch(FN_NCS, call, name), "rtimes", CITE["rtimes"],
                         dict(dest=T, eqop=eq, var=var, b=src))
-                    name = f"QLA_FN_{T}_{var}{eq}_{src}"
+                    name = f"QLA_{LIB}_{T}_{var}{eq}_{src}"
                     call = lambda nc, T=T, p1=p1, eq=eq, gang=gang: (
                         f"qlab::api_map<qlab::CopyOp<{R}, {ncpl[T](nc)}>>({kid('copy')}, r, {opnd(p1, 'a')}, "
                         f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]});")
                     add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
                         _fn_switch(FN_NCS, call, name), "copy", CITE["copy"], dict(dest=T, eqop=eq, var=var, a=src))
         # global reductions: FN (float result) and DFN (double result)
-        for rpc, outR, OP in (("FN", "float", "F"), ("DFN", "double", "D")):
+        for rpc, outR, OP in ((("FN", "float", "F"), ("DFN", "double", "D")) if prec == "F" else
+                              (("DN", "double", "D"),)):
             for var in ["v", "x"]:
                 gang = "index" if var == "x" else "nullptr"
                 tail = [("int *", "index")] if var == "x" else []
@@ -211,7 +214,7 @@ def gen_fn():
         tail = [("int *", "index")] if var == "x" else []
         for eq in EQOPS:
             for src, p1 in [("D", False), ("pD", True)]:
-                name = f"QLA_FN_H_{var}{eq}_spproj_{src}"
+                name = f"QLA_{LIB}_H_{var}{eq}_spproj_{src}"
                 call = lambda nc, p1=p1, eq=eq, gang=gang: (
                     f"qlab::api_map<qlab::SpprojOp<{R}, {nc}>>({kid('spproj')}, r, {opnd(p1, 'a')}, "
                     f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]}, mu, sign);")
@@ -219,7 +222,7 @@ def gen_fn():
                     "if (mu < 0 || mu > 4) return;\n  " + _fn_switch(FN_NCS, call, name), "spproj",
                     CITE["spproj"], dict(eqop=eq, var=var, a=src))
             for src, p1 in [("H", False), ("pH", True)]:
-                name = f"QLA_FN_D_{var}{eq}_sprecon_{src}"
+                name = f"QLA_{LIB}_D_{var}{eq}_sprecon_{src}"
                 call = lambda nc, p1=p1, eq=eq, gang=gang: (
                     f"qlab::api_map<qlab::SpreconOp<{R}, {nc}>>({kid('sprecon')}, r, {opnd(p1, 'a')}, "
                     f"qlab::Opnd{{}}, {gang}, n, {EQ_ENUM[eq]}, mu, sign);")
@@ -228,32 +231,33 @@ def gen_fn():
                     CITE["sprecon"], dict(eqop=eq, var=var, a=src))
         for src, p1 in [("M", False), ("pM", True)]:
             for fname, opname in (("exp", "GenExpOp"), ("sqrt", "GenSqrtOp"), ("inverse", "GenInverseOp")):
-                name = f"QLA_FN_M_{var}eq_{fname}_{src}"
+                name = f"QLA_{LIB}_M_{var}eq_{fname}_{src}"
                 call = lambda nc, opname=opname, p1=p1, gang=gang: (
                     f"qlab::api_map<qlab::{opname}<{R}, {nc}>>({kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
                     f"{gang}, n, qlab::EQ);")
                 add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
                     _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
                     dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
-            name = f"QLA_FN_C_{var}eq_det_{src}"
+            name = f"QLA_{LIB}_C_{var}eq_det_{src}"
             call = lambda nc, p1=p1, gang=gang: (
                 f"qlab::api_map<qlab::GenDetOp<{R}, {nc}>>({kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
                 f"{gang}, n, qlab::EQ);")
-            add(name, [("QLA_F_Complex *", "r"), ("void *", "a")] + tail + [("int", "n")],
+            add(name, [(f"QLA_{prec}_Complex *", "r"), ("void *", "a")] + tail + [("int", "n")],
                 _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
                 dict(dest="C", eqop="eq", var=var, a=src, fn="det"))
             # the remaining matrix functions: the Nc = 3 closed forms at nc = 3,
             # the templates' generic paths otherwise
             for fname, opf in FN_MFUNC_EXT.items():
-                name = f"QLA_FN_M_{var}eq_{fname}_{src}"
+                name = f"QLA_{LIB}_M_{var}eq_{fname}_{src}"
                 call = lambda nc, opf=opf, p1=p1, gang=gang: (
-                    f"qlab::api_map<qlab::{opf(nc)}>({kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
+                    f"qlab::api_map<qlab::{opf(nc).replace('float', R)}>({kid('mfunc_ext')}, r, {opnd(p1, 'a')}, "
+                    f"qlab::Opnd{{}}, "
                     f"{gang}, n, qlab::EQ);")
                 add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
                     _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["mfunc_ext"],
                     dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
             for fname, opn, herm in (("eigenvals", "EigenvalsOp", "false"), ("eigenvalsH", "EigenvalsHOp", "true")):
-                name = f"QLA_FN_V_{var}eq_{fname}_{src}"
+                name = f"QLA_{LIB}_V_{var}eq_{fname}_{src}"
                 call = lambda nc, opn=opn, herm=herm, p1=p1, gang=gang: (
                     f"qlab::api_map<qlab::{opn + '<' + R + '>' if nc == 3 else f'GenEigenOp<{R}, {nc}, {herm}>'}>("
                     f"{kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, {gang}, n, qlab::EQ);")
@@ -263,7 +267,7 @@ def gen_fn():
         for T_ in ("V", "M"):
             for s1, p1 in (("M", False), ("pM", True)):
                 for s2, p2 in ((T_, False), ("p" + T_, True)):
-                    name = f"QLA_FN_{T_}_{var}eq_{s1}_inverse_{s2}"
+                    name = f"QLA_{LIB}_{T_}_{var}eq_{s1}_inverse_{s2}"
                     call = lambda nc, T_=T_, p1=p1, p2=p2, gang=gang: (
                         f"qlab::api_map<qlab::GenMInverseOp<{R}, {nc}, {1 if T_ == 'V' else nc}>>({kid('minv')}, r, "
                         f"{opnd(p1, 'a')}, {opnd(p2, 'b')}, {gang}, n, qlab::EQ);")
@@ -1086,8 +1090,10 @@ def main():
     manifest = []
     groups = {}
     headers = {}
-    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None)]:
-        for fn in (gen_int() if pc == "I" else gen_fn() if pc == "FN" else gen_pc(pc, R, P)):
+    for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None),
+                     ("DN", None, None)]:
+        for fn in (gen_int() if pc == "I" else gen_fn("F") if pc == "FN" else gen_fn("D") if pc == "DN"
+                   else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
             hpc = {"FD3": "DF3"}.get(hpc, hpc)  # the reference declares QLA_FD3_ in qla_df3.h
             headers.setdefault(hpc, []).append(fn)
@@ -1120,9 +1126,9 @@ def main():
             extra = '#include "../qla_ewise.cuh"\n'
         if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert"):
             extra = '#include "../qla_sitefield.cuh"\n'
-        if pc == "FN" and family == "mfunc":
+        if pc in ("FN", "DN") and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
-        if pc == "FN" and family == "mfunc_ext":
+        if pc in ("FN", "DN") and family == "mfunc_ext":
             extra = '#include "../qla_mfunc_generic_ext.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:

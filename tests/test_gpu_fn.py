@@ -1,9 +1,10 @@
-"""GPU parity of the QLA_FN_ / QLA_DFN_ entry points (colour count nc at run
-time) against the oracle, through the C-ABI, for every compiled nc
-(2, 3, 4, 8; matrix functions 3, 4, 8).  Linear ops and the matrix
-functions (the reference's generic Pade exp, Newton sqrt, Gauss-Jordan
-inverse, LU det, restated in float) must be bit-identical; reductions
-follow the tolerances of tests/test_gpu_reductions.py."""
+"""GPU parity of the QLA_FN_ / QLA_DFN_ and QLA_DN_ entry points (colour
+count nc at run time) against the oracle, through the C-ABI, for every
+compiled nc (2, 3, 4, 8; matrix functions 3, 4, 8).  Linear ops and the
+matrix functions on the templates' generic paths (Pade exp, Newton sqrt,
+Gauss-Jordan inverse, LU det, restated in float for FN and in double for DN)
+must be bit-identical; reductions follow the tolerances of
+tests/test_gpu_reductions.py."""
 import itertools
 
 import numpy as np
@@ -14,6 +15,8 @@ import qla_testlib as T
 pytestmark = pytest.mark.gpu
 
 NCS = [2, 3, 4, 8]
+# (library, site precision, reduction library returning double)
+PRECS = [("FN", np.float32, "DFN"), ("DN", np.float64, "DN")]
 
 
 def ncplx(t, nc):
@@ -24,20 +27,23 @@ def ncol(t, nc):
     return {"V": 1, "H": 2, "D": 4, "M": nc}[t]
 
 
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
 @pytest.mark.parametrize("nc", NCS)
-def test_fn_lmult(qla, nc):
+def test_fn_lmult(qla, nc, lib, dt, rlib):
     rng = np.random.default_rng(50 + nc)
+    ns_ = getattr(qla, lib)
+    cb = 2 * np.dtype(dt).itemsize  # bytes per complex number
     n, ns = 1003, 1100
     idx = rng.integers(0, ns, n).astype(np.int32)
     gang = rng.permutation(n).astype(np.int32)
-    a = rng.standard_normal((ns, 2 * nc * nc)).astype(np.float32)
+    a = rng.standard_normal((ns, 2 * nc * nc)).astype(dt)
     ad = T.to_dev(a)
-    pa = T.ptr_array(ad, idx, 8 * nc * nc)
+    pa = T.ptr_array(ad, idx, cb * nc * nc)
     for dest in ("V", "H", "D", "M"):
-        b = rng.standard_normal((ns, 2 * ncplx(dest, nc))).astype(np.float32)
-        r0 = rng.standard_normal((n, 2 * ncplx(dest, nc))).astype(np.float32)
+        b = rng.standard_normal((ns, 2 * ncplx(dest, nc))).astype(dt)
+        r0 = rng.standard_normal((n, 2 * ncplx(dest, nc))).astype(dt)
         bd = T.to_dev(b)
-        pb = T.ptr_array(bd, idx[::-1].copy(), 8 * ncplx(dest, nc))
+        pb = T.ptr_array(bd, idx[::-1].copy(), cb * ncplx(dest, nc))
         src2s = [(dest, 0), ("p" + dest, 0)] + ([("Ma", 1)] if dest == "M" else [])
         for var, eq, s1, (s2, adjb) in itertools.product(["v", "x"], T.EQOPS, ["M", "Ma", "pM"], src2s):
             if dest != "V" and var == "x" and eq not in ("eq", "meq"):
@@ -46,117 +52,129 @@ def test_fn_lmult(qla, nc):
             args = [nc, r_d, pa if s1.startswith("p") else ad, pb if s2.startswith("p") else bd]
             if var == "x":
                 args.append(T.to_dev(gang))
-            getattr(qla.FN, f"{dest}_{var}{eq}_{s1}_times_{s2}")(*args, n)
+            getattr(ns_, f"{dest}_{var}{eq}_{s1}_times_{s2}")(*args, n)
             want = r0.copy()
             T.ora_lmult(want, a, b, n, ncol(dest, nc), eq, adja=int(s1.endswith("a")), adjb=adjb,
                         idx_a=idx if s1.startswith("p") else None,
                         idx_b=idx[::-1].copy() if s2.startswith("p") else None,
                         gang=gang if var == "x" else None, nc=nc)
-            assert T.bits_equal(T.to_host(r_d), want), (nc, dest, var, eq, s1, s2)
+            assert T.bits_equal(T.to_host(r_d), want), (lib, nc, dest, var, eq, s1, s2)
         r_d = T.to_dev(r0)
-        qla.FN.__getattr__(f"{dest}_peq_M_times_x{dest}")(nc, r_d, ad, bd, T.to_dev(idx), n)
+        ns_.__getattr__(f"{dest}_peq_M_times_x{dest}")(nc, r_d, ad, bd, T.to_dev(idx), n)
         want = r0.copy()
         T.ora_lmult(want, a, b, n, ncol(dest, nc), "peq", idx_b=idx, nc=nc)
         assert T.bits_equal(T.to_host(r_d), want), (nc, dest, "xb")
 
 
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
 @pytest.mark.parametrize("nc", NCS)
-def test_fn_spin_rtimes_copy_reductions(qla, nc):
+def test_fn_spin_rtimes_copy_reductions(qla, nc, lib, dt, rlib):
     rng = np.random.default_rng(60 + nc)
+    ns_, rns = getattr(qla, lib), getattr(qla, rlib)
     n = 2049
-    d = rng.standard_normal((n, 8 * nc)).astype(np.float32)
-    h = rng.standard_normal((n, 4 * nc)).astype(np.float32)
+    d = rng.standard_normal((n, 8 * nc)).astype(dt)
+    h = rng.standard_normal((n, 4 * nc)).astype(dt)
     dd, hd = T.to_dev(d), T.to_dev(h)
     for eq, mu, sign in itertools.product(T.EQOPS, range(5), (1, -1)):
         r_d = T.to_dev(h)
-        qla.FN.__getattr__(f"H_v{eq}_spproj_D")(nc, r_d, dd, mu, sign, n)
+        ns_.__getattr__(f"H_v{eq}_spproj_D")(nc, r_d, dd, mu, sign, n)
         want = h.copy()
         T.ora_spproj(want, d, n, mu, sign, eq, nc=nc)
         assert T.bits_equal(T.to_host(r_d), want), ("spproj", nc, eq, mu, sign)
         r_d = T.to_dev(d)
-        qla.FN.__getattr__(f"D_v{eq}_sprecon_H")(nc, r_d, hd, mu, sign, n)
+        ns_.__getattr__(f"D_v{eq}_sprecon_H")(nc, r_d, hd, mu, sign, n)
         want = d.copy()
         T.ora_sprecon(want, h, n, mu, sign, eq, nc=nc)
         assert T.bits_equal(T.to_host(r_d), want), ("sprecon", nc, eq, mu, sign)
     for t in ("V", "H", "D", "M"):
-        x = rng.standard_normal((n, 2 * ncplx(t, nc))).astype(np.float32)
-        y = rng.standard_normal((n, 2 * ncplx(t, nc))).astype(np.float32)
+        x = rng.standard_normal((n, 2 * ncplx(t, nc))).astype(dt)
+        y = rng.standard_normal((n, 2 * ncplx(t, nc))).astype(dt)
         xd, yd = T.to_dev(x), T.to_dev(y)
         for eq in T.EQOPS:
             r_d = T.to_dev(y)
-            qla.FN.__getattr__(f"{t}_v{eq}_r_times_{t}")(nc, r_d, -0.375, xd, n)
+            ns_.__getattr__(f"{t}_v{eq}_r_times_{t}")(nc, r_d, -0.375, xd, n)
             want = y.copy()
             T.ora_rtimes(want, -0.375, x, n, ncplx(t, nc), eq)
             assert T.bits_equal(T.to_host(r_d), want), ("rtimes", nc, t, eq)
         r_d = T.to_dev(y)
-        qla.FN.__getattr__(f"{t}_vmeq_{t}")(nc, r_d, xd, n)
+        ns_.__getattr__(f"{t}_vmeq_{t}")(nc, r_d, xd, n)
         assert T.bits_equal(T.to_host(r_d), y - x)
         exact = T.ora_norm2(x, n, ncplx(t, nc), exact=True)
-        got = qla.DFN.__getattr__(f"r_veq_norm2_{t}")(nc, None, xd, n)
+        got = rns.__getattr__(f"r_veq_norm2_{t}")(nc, None, xd, n)
         assert abs(got - exact) <= 1e-12 * exact
-        gotf = qla.FN.__getattr__(f"r_veq_norm2_{t}")(nc, None, xd, n)
-        assert abs(gotf - exact) <= 6e-8 * exact
+        if lib == "FN":
+            gotf = ns_.__getattr__(f"r_veq_norm2_{t}")(nc, None, xd, n)
+            assert abs(gotf - exact) <= 6e-8 * exact
         ed = T.ora_dot(x, y, n, ncplx(t, nc), exact=True)
-        gd = qla.DFN.__getattr__(f"c_veq_{t}_dot_{t}")(nc, None, xd, yd, n)
+        gd = rns.__getattr__(f"c_veq_{t}_dot_{t}")(nc, None, xd, yd, n)
         assert abs(gd - ed) <= 1e-12 * max(1.0, abs(ed)) * 4
 
 
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
 @pytest.mark.parametrize("nc", [3, 4, 8])
-def test_fn_matrix_functions_bit_exact(qla, nc):
+def test_fn_matrix_functions_bit_exact(qla, nc, lib, dt, rlib):
     rng = np.random.default_rng(70 + nc)
     n = 4099 if nc < 8 else 1031
-    gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(np.float32)
-    pos = T.positive_hermitian_inputs(rng, n, np.float32, nc=nc)
+    gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(dt)
+    pos = T.positive_hermitian_inputs(rng, n, dt, nc=nc)
     for fname, src in (("exp", gen), ("sqrt", pos), ("inverse", gen), ("det", gen)):
         nout = 1 if fname == "det" else nc * nc
-        r_d = T.to_dev(np.zeros((n, 2 * nout), np.float32))
+        r_d = T.to_dev(np.zeros((n, 2 * nout), dt))
         dest = "C" if fname == "det" else "M"
-        qla.FN.__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
-        assert T.bits_equal(T.to_host(r_d), T.ora_mfunc(src, n, fname, nc=nc)), (nc, fname)
+        getattr(qla, lib).__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
+        assert T.bits_equal(T.to_host(r_d), T.ora_mfunc(src, n, fname, nc=nc)), (lib, nc, fname)
 
 
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
 @pytest.mark.parametrize("nc", [3, 4, 8])
-def test_fn_remaining_matrix_functions(qla, nc):
+def test_fn_remaining_matrix_functions(qla, nc, lib, dt, rlib):
     """invsqrt, log, M^-1 V and M^-1 M take the templates' generic paths in
     float at every nc: bit-identical (log up to the host libm's log of
     |A|_F on the diagonal).  expA / expTA / sqrtPH / invsqrtPH take the exp and
     Newton paths at nc != 3 (bit-identical) and the FP64 closed forms at
-    nc = 3 (the F3 tolerance: FP32 test rule against the FP64 value of the
-    promoted input); eigenvalues take the closed forms at nc = 3 and the
-    templates' Hessenberg + double-shift QR path (bit-identical) otherwise."""
+    nc = 3 (FN: the F3 tolerance, the FP32 test rule against the FP64 value
+    of the promoted input; DN: <= 1e-11 of max(1, |A|_F^2) against the
+    oracle's double closed forms); eigenvalues take the closed forms at
+    nc = 3 and the templates' Hessenberg + double-shift QR path
+    (bit-identical) otherwise."""
     rng = np.random.default_rng(80 + nc)
     n = 2053 if nc < 8 else 521
-    gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(np.float32)
-    pos = T.positive_hermitian_inputs(rng, n, np.float32, nc=nc)
+    gen = (rng.standard_normal((n, 2 * nc * nc)) * (0.4 if nc < 8 else 0.25)).astype(dt)
+    pos = T.positive_hermitian_inputs(rng, n, dt, nc=nc)
     z = T.to_complex(gen.astype(np.float64), nc)
-    ah = T.from_complex(0.5 * (z - np.conj(np.transpose(z, (0, 2, 1)))), np.float32)
-    herm = T.hermitian_inputs(rng, n, np.float32, nc=nc)
+    ah = T.from_complex(0.5 * (z - np.conj(np.transpose(z, (0, 2, 1)))), dt)
+    herm = T.hermitian_inputs(rng, n, dt, nc=nc)
     cases = [("invsqrt", pos), ("log", pos), ("expA", ah), ("expTA", ah), ("sqrtPH", pos), ("invsqrtPH", pos),
              ("eigenvalsH", pos), ("eigenvalsH", herm), ("eigenvals", gen)]
     for fname, src in cases:
         nout = nc if fname.startswith("eigen") else nc * nc
         dest = "V" if fname.startswith("eigen") else "M"
-        r_d = T.to_dev(np.zeros((n, 2 * nout), np.float32))
-        qla.FN.__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
+        r_d = T.to_dev(np.zeros((n, 2 * nout), dt))
+        getattr(qla, lib).__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
         got = T.to_host(r_d)
         closed = nc == 3 and fname not in ("invsqrt", "log")
-        if closed:
+        if closed and lib == "DN":
+            want = T.ora_mfunc(src, n, fname, nc=nc)
+            scale = np.maximum(1.0, np.sum(src.astype(np.float64) ** 2, axis=1))[:, None]
+            assert np.all(np.abs(got - want) <= 1e-11 * scale), (lib, nc, fname)
+        elif closed:
             want = T.ora_mfunc(src.astype(np.float64), n, fname, nc=nc)
-            ok, nbad = T.qla_close(got, want, np.float32)
+            ok, nbad = T.qla_close(got, want, dt)
             assert ok, (nc, fname, nbad)
         elif fname == "log":
             want = T.ora_mfunc(src, n, fname, nc=nc)
-            ok, nbad = T.qla_close(got, want, np.float32, nabs=2, nrel=2)
+            ok, nbad = T.qla_close(got, want, dt, nabs=2, nrel=2)
             assert ok, (nc, fname, nbad)
             assert np.mean(np.all(got == want, axis=1)) > 0.99
         else:
             assert T.bits_equal(got, T.ora_mfunc(src, n, fname, nc=nc)), (nc, fname)
     for t, nb in (("V", 1), ("M", nc)):
-        b = rng.standard_normal((n, 2 * nc * nb)).astype(np.float32)
+        b = rng.standard_normal((n, 2 * nc * nb)).astype(dt)
         ib = rng.permutation(n).astype(np.int32)
-        r_d = T.to_dev(np.zeros((n, 2 * nc * nb), np.float32))
+        r_d = T.to_dev(np.zeros((n, 2 * nc * nb), dt))
         b_d = T.to_dev(b)
-        qla.FN.__getattr__(f"{t}_veq_M_inverse_p{t}")(nc, r_d, T.to_dev(gen), T.ptr_array(b_d, ib, 8 * nc * nb), n)
+        pb = T.ptr_array(b_d, ib, 2 * np.dtype(dt).itemsize * nc * nb)
+        getattr(qla, lib).__getattr__(f"{t}_veq_M_inverse_p{t}")(nc, r_d, T.to_dev(gen), pb, n)
         assert T.bits_equal(T.to_host(r_d), T.ora_minv(gen, b, n, nb, nc=nc, idx_b=ib)), (nc, t)
 
 

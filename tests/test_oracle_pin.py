@@ -233,9 +233,9 @@ def test_prototypes_match_reference_headers():
     import qla_b200
     ref = {}
     nargs_fn = {}
-    for h in ("qla_fn.h", "qla_dfn.h"):
+    for h in ("qla_fn.h", "qla_dfn.h", "qla_dn.h"):
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
-        for m in re.finditer(r"void (QLA_D?FN_\w+) \((.*?)\);", txt):
+        for m in re.finditer(r"void (QLA_(?:D?FN|DN)_\w+) \((.*?)\);", txt):
             # VLA record types: compare the parameter count (the first is int nc)
             nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)", m.group(2)))
     for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h"):
