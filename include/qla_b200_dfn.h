@@ -26,12 +26,27 @@ void QLA_DFN_r_veq_norm2_pV(int nc, QLA_D_Real * r, void * a, int n);
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_V_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_V_dot_V(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_V_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_V_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_V_dot_pV(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_V_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pV_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pV_dot_V(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pV_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pV_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pV_dot_pV(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pV_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_xeq_norm2_V (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_xeq_norm2_V(int nc, QLA_D_Real * r, void * a, int * index, int n);
@@ -40,12 +55,27 @@ void QLA_DFN_r_xeq_norm2_pV(int nc, QLA_D_Real * r, void * a, int * index, int n
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_V_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_V_dot_V(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_V_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_V_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_V_dot_pV(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_V_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pV_dot_V (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pV_dot_V(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pV_dot_V (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pV_dot_pV (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pV_dot_pV(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pV_dot_pV (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_veq_norm2_H (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_veq_norm2_H(int nc, QLA_D_Real * r, void * a, int n);
@@ -54,12 +84,27 @@ void QLA_DFN_r_veq_norm2_pH(int nc, QLA_D_Real * r, void * a, int n);
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_H_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_H_dot_H(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_H_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_H_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_H_dot_pH(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_H_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pH_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pH_dot_H(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pH_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pH_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pH_dot_pH(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pH_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_xeq_norm2_H (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_xeq_norm2_H(int nc, QLA_D_Real * r, void * a, int * index, int n);
@@ -68,12 +113,27 @@ void QLA_DFN_r_xeq_norm2_pH(int nc, QLA_D_Real * r, void * a, int * index, int n
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_H_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_H_dot_H(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_H_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_H_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_H_dot_pH(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_H_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pH_dot_H (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pH_dot_H(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pH_dot_H (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pH_dot_pH (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pH_dot_pH(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pH_dot_pH (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_veq_norm2_D (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_veq_norm2_D(int nc, QLA_D_Real * r, void * a, int n);
@@ -82,12 +142,27 @@ void QLA_DFN_r_veq_norm2_pD(int nc, QLA_D_Real * r, void * a, int n);
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_D_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_D_dot_D(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_D_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_D_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_D_dot_pD(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_D_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pD_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pD_dot_D(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pD_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pD_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pD_dot_pD(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pD_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_xeq_norm2_D (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_xeq_norm2_D(int nc, QLA_D_Real * r, void * a, int * index, int n);
@@ -96,12 +171,27 @@ void QLA_DFN_r_xeq_norm2_pD(int nc, QLA_D_Real * r, void * a, int * index, int n
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_D_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_D_dot_D(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_D_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_D_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_D_dot_pD(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_D_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pD_dot_D (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pD_dot_D(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pD_dot_D (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pD_dot_pD (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pD_dot_pD(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pD_dot_pD (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_veq_norm2_M (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_veq_norm2_M(int nc, QLA_D_Real * r, void * a, int n);
@@ -110,12 +200,27 @@ void QLA_DFN_r_veq_norm2_pM(int nc, QLA_D_Real * r, void * a, int n);
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_M_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_M_dot_M(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_M_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_M_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_M_dot_pM(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_M_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pM_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pM_dot_M(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pM_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_veq_pM_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_veq_pM_dot_pM(int nc, QLA_D_Complex * r, void * a, void * b, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_veq_re_pM_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_veq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int n);
 /* ---- norm2: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2155 */
 /* replaces QLA_DFN_r_xeq_norm2_M (lib/perl/build_qla.pl:2089-2155, make_code_unary.pl:318-365 (global norm2)) */
 void QLA_DFN_r_xeq_norm2_M(int nc, QLA_D_Real * r, void * a, int * index, int n);
@@ -124,12 +229,225 @@ void QLA_DFN_r_xeq_norm2_pM(int nc, QLA_D_Real * r, void * a, int * index, int n
 /* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_M_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_M_dot_M(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_M_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_M_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_M_dot_pM(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_M_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pM_dot_M (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pM_dot_M(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pM_dot_M (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- dot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2196-2360 */
 /* replaces QLA_DFN_c_xeq_pM_dot_pM (lib/perl/build_qla.pl:2196-2360, make_code_binary.pl:110-172 (global inner product)) */
 void QLA_DFN_c_xeq_pM_dot_pM(int nc, QLA_D_Complex * r, void * a, void * b, int * index, int n);
+/* ---- redot: replaces the DFN functions emitted by lib/perl/build_qla.pl:2250-2284 (real part of the global inner product) */
+/* replaces QLA_DFN_r_xeq_re_pM_dot_pM (lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)) */
+void QLA_DFN_r_xeq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n);
+/* ---- gred: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators */
+/* replaces QLA_DFN_c_veq_Ma_dot_M (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_Ma_dot_M(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_Ma_dot_pM (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_Ma_dot_pM(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_pMa_dot_M (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_pMa_dot_M(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_pMa_dot_pM (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_pMa_dot_pM(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_P_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_P_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_P_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_P_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_pP_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_pP_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_pP_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_pP_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_Pa_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_Pa_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_Pa_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_Pa_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_pPa_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_pPa_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_c_veq_pPa_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_veq_pPa_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_r_veq_re_P_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_veq_re_P_dot_P(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_r_veq_re_P_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_veq_re_P_dot_pP(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_r_veq_re_pP_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_veq_re_pP_dot_P(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_r_veq_re_pP_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_veq_re_pP_dot_pP(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int n);
+/* replaces QLA_DFN_r_veq_norm2_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_veq_norm2_P(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, int n);
+/* replaces QLA_DFN_r_veq_norm2_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_veq_norm2_pP(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, int n);
+/* ---- gsum: replaces the DFN functions emitted by lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites) */
+/* replaces QLA_DFN_v_veq_sum_V (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_v_veq_sum_V(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_v_veq_sum_pV (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_v_veq_sum_pV(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_h_veq_sum_H (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_h_veq_sum_H(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_h_veq_sum_pH (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_h_veq_sum_pH(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_d_veq_sum_D (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_d_veq_sum_D(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_d_veq_sum_pD (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_d_veq_sum_pD(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_m_veq_sum_M (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_m_veq_sum_M(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_m_veq_sum_pM (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_m_veq_sum_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_p_veq_sum_P (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_p_veq_sum_P(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_p_veq_sum_pP (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_p_veq_sum_pP(int nc, void * r, void * a, int n);
+/* ---- convert: replaces the DFN functions emitted by lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion */
+/* replaces QLA_DFN_V_veq_V (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_V_veq_V(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_V_veq_V (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_V_veq_V(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_V_veq_pV (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_V_veq_pV(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_V_veq_pV (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_V_veq_pV(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_H_veq_H (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_H_veq_H(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_H_veq_H (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_H_veq_H(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_H_veq_pH (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_H_veq_pH(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_H_veq_pH (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_H_veq_pH(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_D_veq_D (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_D_veq_D(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_D_veq_D (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_D_veq_D(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_D_veq_pD (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_D_veq_pD(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_D_veq_pD (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_D_veq_pD(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_M_veq_M (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_M_veq_M(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_M_veq_M (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_M_veq_M(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_M_veq_pM (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_M_veq_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_M_veq_pM (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_M_veq_pM(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_P_veq_P (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_P_veq_P(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_P_veq_P (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_P_veq_P(int nc, void * r, void * a, int n);
+/* replaces QLA_DFN_P_veq_pP (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_P_veq_pP(int nc, void * r, void * a, int n);
+/* replaces QLA_FDN_P_veq_pP (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_P_veq_pP(int nc, void * r, void * a, int n);
+/* ---- gred: replaces the DFN functions emitted by lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators */
+/* replaces QLA_DFN_c_xeq_Ma_dot_M (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_Ma_dot_M(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_Ma_dot_pM (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_Ma_dot_pM(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_pMa_dot_M (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_pMa_dot_M(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_pMa_dot_pM (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_pMa_dot_pM(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_P_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_P_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_P_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_P_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_pP_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_pP_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_pP_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_pP_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_Pa_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_Pa_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_Pa_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_Pa_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_pPa_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_pPa_dot_P(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_c_xeq_pPa_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_c_xeq_pPa_dot_pP(int nc, QLA_D_Complex *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_r_xeq_re_P_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_xeq_re_P_dot_P(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_r_xeq_re_P_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_xeq_re_P_dot_pP(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_r_xeq_re_pP_dot_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_xeq_re_pP_dot_P(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_r_xeq_re_pP_dot_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_xeq_re_pP_dot_pP(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, void * b, int * index, int n);
+/* replaces QLA_DFN_r_xeq_norm2_P (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_xeq_norm2_P(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, int * index, int n);
+/* replaces QLA_DFN_r_xeq_norm2_pP (lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, trace of the adjoint-form products Ma.M and Pa.P)) */
+void QLA_DFN_r_xeq_norm2_pP(int nc, QLA_D_Real *QLA_B200_RESTRICT r, void * a, int * index, int n);
+/* ---- gsum: replaces the DFN functions emitted by lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites) */
+/* replaces QLA_DFN_v_xeq_sum_V (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_v_xeq_sum_V(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_v_xeq_sum_pV (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_v_xeq_sum_pV(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_h_xeq_sum_H (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_h_xeq_sum_H(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_h_xeq_sum_pH (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_h_xeq_sum_pH(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_d_xeq_sum_D (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_d_xeq_sum_D(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_d_xeq_sum_pD (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_d_xeq_sum_pD(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_m_xeq_sum_M (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_m_xeq_sum_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_m_xeq_sum_pM (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_m_xeq_sum_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_p_xeq_sum_P (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_p_xeq_sum_P(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_p_xeq_sum_pP (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
+void QLA_DFN_p_xeq_sum_pP(int nc, void * r, void * a, int * index, int n);
+/* ---- convert: replaces the DFN functions emitted by lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion */
+/* replaces QLA_DFN_V_xeq_V (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_V_xeq_V(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_V_xeq_V (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_V_xeq_V(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_V_xeq_pV (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_V_xeq_pV(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_V_xeq_pV (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_V_xeq_pV(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_H_xeq_H (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_H_xeq_H(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_H_xeq_H (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_H_xeq_H(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_H_xeq_pH (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_H_xeq_pH(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_H_xeq_pH (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_H_xeq_pH(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_D_xeq_D (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_D_xeq_D(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_D_xeq_D (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_D_xeq_D(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_D_xeq_pD (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_D_xeq_pD(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_D_xeq_pD (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_D_xeq_pD(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_M_xeq_M (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_M_xeq_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_M_xeq_M (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_M_xeq_M(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_M_xeq_pM (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_M_xeq_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_M_xeq_pM (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_M_xeq_pM(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_P_xeq_P (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_P_xeq_P(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_P_xeq_P (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_P_xeq_P(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DFN_P_xeq_pP (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_DFN_P_xeq_pP(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_FDN_P_xeq_pP (lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, QLA_FD_c_eq_c rounding)) */
+void QLA_FDN_P_xeq_pP(int nc, void * r, void * a, int * index, int n);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,27 @@ void ora_gdot_##SFX(int kind, int perm, double *out2, const R *a, const R *b, lo
 void ora_gsum_##SFX(double *out, const R *a, long n, int ne, const int *idx_a, const int *gang);
 ORA_SITEFIELD_DECL(float, f)
 ORA_SITEFIELD_DECL(double, d)
+/* the same families with the colour count nc as the first argument (the
+ * QLA_FN_ / QLA_DN_ libraries) */
+#define ORA_NCOLOR_DECL(R, SFX)                                                                   \
+void ora_ewise_n_##SFX(int nc, int shape, int perm, int eqop, R *r, const R *b, const R *c,       \
+                       const R *s, int scal_kind, R sre, R sim, long n, int ne, const int *idx_b, \
+                       const int *idx_c, const int *idx_s, const int *gang);                     \
+void ora_outer_n_##SFX(int nc, int eqop, R *r, const R *a, const R *b, long n, const int *idx_a,  \
+                       const int *idx_b, const int *gang);                                       \
+void ora_ldot_n_##SFX(int nc, int kind, int perm, int eqop, R *r, const R *a, const R *b, long n, \
+                      int ne, const int *idx_a, const int *idx_b, const int *gang);              \
+void ora_diagfill_n_##SFX(int nc, int eqop, R *r, const R *c, long n, const int *gang);          \
+void ora_component_n_##SFX(int nc, int what, int dst, int src, R *r, const R *a, int i_c,         \
+                           int i_s, int j_c, int j_s, long n, const int *idx_a, const int *gang); \
+void ora_gamma_n_##SFX(int nc, int right, int ne, int mu, R *r, const R *a, long n,              \
+                       const int *idx_a, const int *gang);                                       \
+void ora_trace_n_##SFX(int nc, int kind, R *r, const R *a, long n, const int *idx_a,             \
+                       const int *gang);                                                          \
+void ora_gdot_n_##SFX(int nc, int kind, int perm, double *out2, const R *a, const R *b, long n,    \
+                      int ne, const int *idx_a, const int *idx_b, const int *gang);
+ORA_NCOLOR_DECL(float, f)
+ORA_NCOLOR_DECL(double, d)
 /* precision conversions of n records of nr reals: QLA_DF_c_eq_c (float to
  * double) and QLA_FD_c_eq_c (double to float, rounded to nearest) */
 void ora_convert_df(double *r, const float *a, long n, int nr, const int *idx_a, const int *gang);

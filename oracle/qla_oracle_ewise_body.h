@@ -13,10 +13,12 @@
 
 typedef struct { R re, im; } FN(ec);
 
-static int FN(eperm)(int perm, int e)
+/* element e of the transposed record: perm 1 the nc x nc colour matrix,
+ * perm 2 the (colour, spin) x (colour, spin) propagator of blocks 4 nc */
+static int FN(eperm)(int perm, int e, int nc)
 {
-  if (perm == 1) return (e % 3) * 3 + e / 3;
-  if (perm == 2) return (e % 12) * 12 + e / 12;
+  if (perm == 1) return (e % nc) * nc + e / nc;
+  if (perm == 2) return (e % (4 * nc)) * (4 * nc) + e / (4 * nc);
   return e;
 }
 
@@ -94,9 +96,9 @@ static FN(ec) FN(eapply)(int shape, int eqop, FN(ec) x, FN(ec) s, FN(ec) b, FN(e
  * (or i); b, c, s each either contiguous or gathered through idx_* (the
  * pointer form); scal_kind 0 none, 1 constant (sre, sim), 2 per-site complex
  * field s, 3 per-site real field s */
-void FN(ora_ewise)(int shape, int perm, int eqop, R *r, const R *b, const R *c, const R *s, int scal_kind,
-                   R sre, R sim, long n, int ne, const int *idx_b, const int *idx_c, const int *idx_s,
-                   const int *gang)
+void FN(ora_ewise_n)(int nc, int shape, int perm, int eqop, R *r, const R *b, const R *c, const R *s,
+                     int scal_kind, R sre, R sim, long n, int ne, const int *idx_b, const int *idx_c,
+                     const int *idx_s, const int *gang)
 {
   const FN(ec) *B = (const FN(ec) *)b, *C = (const FN(ec) *)c;
   FN(ec) *O = (FN(ec) *)r;
@@ -108,33 +110,47 @@ void FN(ora_ewise)(int shape, int perm, int eqop, R *r, const R *b, const R *c, 
     else if (scal_kind == 2) { sv = ((const FN(ec) *)s)[ks]; }
     else if (scal_kind == 3) { sv.re = s[ks]; }
     for (int e = 0; e < ne; e++) {
-      FN(ec) bv = B[kb * ne + FN(eperm)(perm, e)], cv; cv.re = 0; cv.im = 0;
+      FN(ec) bv = B[kb * ne + FN(eperm)(perm, e, nc)], cv; cv.re = 0; cv.im = 0;
       if (C) cv = C[kc * ne + e];
       O[k * ne + e] = FN(eapply)(shape, eqop, O[k * ne + e], sv, bv, cv);
     }
   }
 }
 
-/* M (eqop)= a b^+ per site (QLA_c_(eqop)_c_times_ca(r_ij, a_i, b_j)) */
-void FN(ora_outer)(int eqop, R *r, const R *a, const R *b, long n, const int *idx_a, const int *idx_b,
+void FN(ora_ewise)(int shape, int perm, int eqop, R *r, const R *b, const R *c, const R *s, int scal_kind,
+                   R sre, R sim, long n, int ne, const int *idx_b, const int *idx_c, const int *idx_s,
                    const int *gang)
+{
+  FN(ora_ewise_n)(3, shape, perm, eqop, r, b, c, s, scal_kind, sre, sim, n, ne, idx_b, idx_c, idx_s, gang);
+}
+
+/* M (eqop)= a b^+ per site (QLA_c_(eqop)_c_times_ca(r_ij, a_i, b_j)) */
+void FN(ora_outer_n)(int nc, int eqop, R *r, const R *a, const R *b, long n, const int *idx_a, const int *idx_b,
+                     const int *gang)
 {
   const FN(ec) *A = (const FN(ec) *)a, *B = (const FN(ec) *)b;
   FN(ec) *O = (FN(ec) *)r;
   FN(ec) z; z.re = 0; z.im = 0;
+  const int m = nc * nc;
   for (long i = 0; i < n; i++) {
     const long k = gang ? gang[i] : i;
     const long ka = idx_a ? idx_a[k] : k, kb = idx_b ? idx_b[k] : k;
-    for (int e = 0; e < 9; e++)
-      O[k * 9 + e] = FN(eapply)(4, eqop, O[k * 9 + e], A[ka * 3 + e / 3], B[kb * 3 + e % 3], z);
+    for (int e = 0; e < m; e++)
+      O[k * m + e] = FN(eapply)(4, eqop, O[k * m + e], A[ka * nc + e / nc], B[kb * nc + e % nc], z);
   }
+}
+
+void FN(ora_outer)(int eqop, R *r, const R *a, const R *b, long n, const int *idx_a, const int *idx_b,
+                   const int *gang)
+{
+  FN(ora_outer_n)(3, eqop, r, a, b, n, idx_a, idx_b, gang);
 }
 
 /* site-local dot products (kind as the product's LdKind), accumulated in
  * double from promoted elements (QLA_DF_c), then QLA_FD_c and the eqop; real
  * outputs (kind >= 3) combine r and x in double */
-void FN(ora_ldot)(int kind, int perm, int eqop, R *r, const R *a, const R *b, long n, int ne, const int *idx_a,
-                  const int *idx_b, const int *gang)
+void FN(ora_ldot_n)(int nc, int kind, int perm, int eqop, R *r, const R *a, const R *b, long n, int ne,
+                    const int *idx_a, const int *idx_b, const int *gang)
 {
   const FN(ec) *A = (const FN(ec) *)a, *B = (const FN(ec) *)(b ? b : a);
   for (long i = 0; i < n; i++) {
@@ -144,8 +160,8 @@ void FN(ora_ldot)(int kind, int perm, int eqop, R *r, const R *a, const R *b, lo
     for (int e = 0; e < ne; e++) {
       double ur, ui, vr, vi;
       int ea = e, eb = e;
-      if (kind == 2) ea = FN(eperm)(perm, e);
-      if (kind == 1) eb = FN(eperm)(perm, e);
+      if (kind == 2) ea = FN(eperm)(perm, e, nc);
+      if (kind == 1) eb = FN(eperm)(perm, e, nc);
       ur = A[ka * ne + ea].re; ui = A[ka * ne + ea].im;
       vr = B[kb * ne + eb].re; vi = B[kb * ne + eb].im;
       if (kind == 0 || kind == 3 || kind == 4) {       /* peq_ca_times_c */
@@ -173,6 +189,12 @@ void FN(ora_ldot)(int kind, int perm, int eqop, R *r, const R *a, const R *b, lo
       else { q->re -= t.re; q->im -= t.im; }
     }
   }
+}
+
+void FN(ora_ldot)(int kind, int perm, int eqop, R *r, const R *a, const R *b, long n, int ne, const int *idx_a,
+                  const int *idx_b, const int *gang)
+{
+  FN(ora_ldot_n)(3, kind, perm, eqop, r, a, b, n, ne, idx_a, idx_b, gang);
 }
 
 #undef FN

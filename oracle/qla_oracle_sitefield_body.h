@@ -16,16 +16,29 @@
 
 typedef struct { R re, im; } FN(sc);
 
-/* component of (ic, is, jc, js) in a record of letter t (include/qla_types.h:38-42) */
-static int FN(selem)(char t, int ic, int is, int jc, int js)
+/* component of (ic, is, jc, js) in a record of letter t with nc colours
+ * (include/qla_types.h:38-42) */
+static int FN(selem)(char t, int ic, int is, int jc, int js, int nc)
 {
   switch (t) {
   case 'V': return ic;
   case 'H': return ic * 2 + is;
   case 'D': return ic * 4 + is;
-  case 'M': return ic * 3 + jc;
-  case 'P': return ((ic * 4 + is) * 3 + jc) * 4 + js;
+  case 'M': return ic * nc + jc;
+  case 'P': return ((ic * 4 + is) * nc + jc) * 4 + js;
   default: return 0;
+  }
+}
+
+static int FN(sne)(int t, int nc)
+{
+  switch (t) {
+  case 'V': return nc;
+  case 'H': return 2 * nc;
+  case 'D': return 4 * nc;
+  case 'M': return nc * nc;
+  case 'P': return 16 * nc * nc;
+  default: return 1;
   }
 }
 
@@ -48,27 +61,33 @@ void FN(ora_fill)(int eqop, R *r, const R *a, long n, int ne, const int *gang)
 
 /* M r[k] (eqop)= c * 1: QLA_c_(eqop)_r(r_ij, 0.) for all i, j, then
  * QLA_c_(eqop)_c(r_ii, c) (include/qla_complex.h:140-156) */
-void FN(ora_diagfill)(int eqop, R *r, const R *c, long n, const int *gang)
+void FN(ora_diagfill_n)(int nc, int eqop, R *r, const R *c, long n, const int *gang)
 {
   FN(sc) *Rr = (FN(sc) *)r;
   const FN(sc) at = *(const FN(sc) *)c;
+  const int m = nc * nc;
   for (long i = 0; i < n; i++) {
     const long k = gang ? gang[i] : i;
-    for (int ic = 0; ic < 3; ic++) {
-      for (int jc = 0; jc < 3; jc++) {
-        FN(sc) *q = &Rr[k * 9 + ic * 3 + jc];
+    for (int ic = 0; ic < nc; ic++) {
+      for (int jc = 0; jc < nc; jc++) {
+        FN(sc) *q = &Rr[k * m + ic * nc + jc];
         if (eqop == 0) { q->re = 0.; q->im = 0.; }
         else if (eqop == 3) { q->re = -(0.); q->im = 0.; }
         else if (eqop == 1) q->re += 0.;
         else q->re -= 0.;
       }
-      FN(sc) *d = &Rr[k * 9 + ic * 4];
+      FN(sc) *d = &Rr[k * m + ic * (nc + 1)];
       if (eqop == 0) *d = at;
       else if (eqop == 3) { d->re = -at.re; d->im = -at.im; }
       else if (eqop == 1) { d->re += at.re; d->im += at.im; }
       else { d->re -= at.re; d->im -= at.im; }
     }
   }
+}
+
+void FN(ora_diagfill)(int eqop, R *r, const R *c, long n, const int *gang)
+{
+  FN(ora_diagfill_n)(3, eqop, r, c, n, gang);
 }
 
 void FN(ora_zero)(R *r, long n, int ne, const int *gang)
@@ -96,11 +115,10 @@ void FN(ora_mask)(R *r, const R *a, const int *m, long n, int ne, const int *idx
 
 /* what: 'e' array component, 'c' colour column, 'd' Dirac vector; dst / src
  * are the record letters ('C' a single complex number) */
-void FN(ora_component)(int what, int dst, int src, R *r, const R *a, int i_c, int i_s, int j_c, int j_s, long n,
-                       const int *idx_a, const int *gang)
+void FN(ora_component_n)(int nc, int what, int dst, int src, R *r, const R *a, int i_c, int i_s, int j_c,
+                         int j_s, long n, const int *idx_a, const int *gang)
 {
-  const int ne_of[128] = {['C'] = 1, ['V'] = 3, ['H'] = 6, ['D'] = 12, ['M'] = 9, ['P'] = 144};
-  const int nr = ne_of[dst], na = ne_of[src];
+  const int nr = FN(sne)(dst, nc), na = FN(sne)(src, nc);
   FN(sc) *Rr = (FN(sc) *)r;
   const FN(sc) *A = (const FN(sc) *)a;
   for (long i = 0; i < n; i++) {
@@ -109,21 +127,27 @@ void FN(ora_component)(int what, int dst, int src, R *r, const R *a, int i_c, in
     FN(sc) *rr = &Rr[k * nr];
     const FN(sc) *aa = &A[ka * na];
     if (what == 'e') {
-      if (dst == 'C') rr[0] = aa[FN(selem)((char)src, i_c, i_s, j_c, j_s)];
-      else rr[FN(selem)((char)dst, i_c, i_s, j_c, j_s)] = aa[0];
+      if (dst == 'C') rr[0] = aa[FN(selem)((char)src, i_c, i_s, j_c, j_s, nc)];
+      else rr[FN(selem)((char)dst, i_c, i_s, j_c, j_s, nc)] = aa[0];
     } else if (what == 'c') {
-      for (int ic = 0; ic < 3; ic++) {
-        if (dst == 'V') rr[ic] = aa[FN(selem)((char)src, ic, i_s, j_c, j_s)];
-        else rr[FN(selem)((char)dst, ic, i_s, j_c, j_s)] = aa[ic];
+      for (int ic = 0; ic < nc; ic++) {
+        if (dst == 'V') rr[ic] = aa[FN(selem)((char)src, ic, i_s, j_c, j_s, nc)];
+        else rr[FN(selem)((char)dst, ic, i_s, j_c, j_s, nc)] = aa[ic];
       }
     } else {
-      for (int ic = 0; ic < 3; ic++)
+      for (int ic = 0; ic < nc; ic++)
         for (int is = 0; is < 4; is++) {
-          if (dst == 'D') rr[FN(selem)('D', ic, is, 0, 0)] = aa[FN(selem)('P', ic, is, j_c, j_s)];
-          else rr[FN(selem)('P', ic, is, j_c, j_s)] = aa[FN(selem)('D', ic, is, 0, 0)];
+          if (dst == 'D') rr[FN(selem)('D', ic, is, 0, 0, nc)] = aa[FN(selem)('P', ic, is, j_c, j_s, nc)];
+          else rr[FN(selem)('P', ic, is, j_c, j_s, nc)] = aa[FN(selem)('D', ic, is, 0, 0, nc)];
         }
     }
   }
+}
+
+void FN(ora_component)(int what, int dst, int src, R *r, const R *a, int i_c, int i_s, int j_c, int j_s, long n,
+                       const int *idx_a, const int *gang)
+{
+  FN(ora_component_n)(3, what, dst, src, r, a, i_c, i_s, j_c, j_s, n, idx_a, gang);
 }
 
 /* gamma_mu as a product of the basis matrices for the set bits of mu
@@ -167,7 +191,8 @@ static FN(sc) FN(gmul)(const int *ent, FN(sc) a)
 /* left (right == 0): r(.., s, ..) = G[s][t] a(.., t, ..) on the first spin
  * index of a D (ne 12) or P (ne 144); right: r(.., s) = a(.., t) G[t][s] on
  * the last spin index of a P.  mu outside 0..15 leaves r unchanged. */
-void FN(ora_gamma)(int right, int ne, int mu, R *r, const R *a, long n, const int *idx_a, const int *gang)
+void FN(ora_gamma_n)(int nc, int right, int ne, int mu, R *r, const R *a, long n, const int *idx_a,
+                     const int *gang)
 {
   if (mu < 0 || mu > 15) return;
   int g[4][4][2];
@@ -183,65 +208,76 @@ void FN(ora_gamma)(int right, int ne, int mu, R *r, const R *a, long n, const in
   for (long i = 0; i < n; i++) {
     const long k = gang ? gang[i] : i;
     const long ka = idx_a ? idx_a[k] : k;
-    for (int ic = 0; ic < 3; ic++) {
-      if (ne == 12) {
+    for (int ic = 0; ic < nc; ic++) {
+      if (ne == 4 * nc) {
         for (int s = 0; s < 4; s++)
-          Rr[k * 12 + FN(selem)('D', ic, s, 0, 0)] = FN(gmul)(ent[s], A[ka * 12 + FN(selem)('D', ic, src[s], 0, 0)]);
+          Rr[k * ne + FN(selem)('D', ic, s, 0, 0, nc)] = FN(gmul)(ent[s], A[ka * ne + FN(selem)('D', ic, src[s], 0, 0, nc)]);
       } else {
         for (int is = 0; is < 4; is++)
-          for (int jc = 0; jc < 3; jc++)
+          for (int jc = 0; jc < nc; jc++)
             for (int js = 0; js < 4; js++) {
-              const int de = FN(selem)('P', ic, is, jc, js);
-              const int se = right ? FN(selem)('P', ic, is, jc, src[js]) : FN(selem)('P', ic, src[is], jc, js);
+              const int de = FN(selem)('P', ic, is, jc, js, nc);
+              const int se = right ? FN(selem)('P', ic, is, jc, src[js], nc) : FN(selem)('P', ic, src[is], jc, js, nc);
               const int *en = right ? ent[js] : ent[is];
-              Rr[k * 144 + de] = FN(gmul)(en, A[ka * 144 + se]);
+              Rr[k * ne + de] = FN(gmul)(en, A[ka * ne + se]);
             }
       }
     }
   }
 }
 
+void FN(ora_gamma)(int right, int ne, int mu, R *r, const R *a, long n, const int *idx_a, const int *gang)
+{
+  FN(ora_gamma_n)(3, right, ne, mu, r, a, n, idx_a, gang);
+}
+
 /* kind 0: C trace, 1: Re trace, 2: Im trace, 3: traceless antihermitian part */
-void FN(ora_trace)(int kind, R *r, const R *a, long n, const int *idx_a, const int *gang)
+void FN(ora_trace_n)(int nc, int kind, R *r, const R *a, long n, const int *idx_a, const int *gang)
 {
   const FN(sc) *A = (const FN(sc) *)a;
   for (long i = 0; i < n; i++) {
     const long k = gang ? gang[i] : i;
     const long ka = idx_a ? idx_a[k] : k;
-    const FN(sc) *m = &A[ka * 9];
+    const int mm = nc * nc;
+    const FN(sc) *m = &A[ka * mm];
     if (kind == 0) {
       FN(sc) x;
       x.re = 0.; x.im = 0.;
-      for (int c = 0; c < 3; c++) { x.re += m[c * 4].re; x.im += m[c * 4].im; }
+      for (int c = 0; c < nc; c++) { x.re += m[c * (nc + 1)].re; x.im += m[c * (nc + 1)].im; }
       ((FN(sc) *)r)[k] = x;
     } else if (kind == 1 || kind == 2) {
       R x = 0.;
-      for (int c = 0; c < 3; c++) x += (kind == 1) ? m[c * 4].re : m[c * 4].im;
+      for (int c = 0; c < nc; c++) x += (kind == 1) ? m[c * (nc + 1)].re : m[c * (nc + 1)].im;
       r[k] = x;
     } else {
-      FN(sc) *o = (FN(sc) *)r + k * 9;
+      FN(sc) *o = (FN(sc) *)r + k * mm;
       R x = 0.;
-      for (int c = 0; c < 3; c++) x += m[c * 4].im;
-      x = x / 3;
-      for (int c = 0; c < 3; c++) {
-        R x2 = m[c * 4].im;
+      for (int c = 0; c < nc; c++) x += m[c * (nc + 1)].im;
+      x = x / nc;
+      for (int c = 0; c < nc; c++) {
+        R x2 = m[c * (nc + 1)].im;
         x2 = x2 - x;
-        o[c * 4].re = 0.;
-        o[c * 4].im = x2;
+        o[c * (nc + 1)].re = 0.;
+        o[c * (nc + 1)].im = x2;
       }
-      for (int ic = 0; ic < 2; ic++)
-        for (int jc = ic + 1; jc < 3; jc++) {
+      for (int ic = 0; ic < nc - 1; ic++)
+        for (int jc = ic + 1; jc < nc; jc++) {
           FN(sc) x1, x2;
-          x1.re = m[ic * 3 + jc].re - m[jc * 3 + ic].re;
-          x1.im = m[ic * 3 + jc].im + m[jc * 3 + ic].im;
+          x1.re = m[ic * nc + jc].re - m[jc * nc + ic].re;
+          x1.im = m[ic * nc + jc].im + m[jc * nc + ic].im;
           x2.re = x1.re * 0.5;
           x2.im = x1.im * 0.5;
-          o[ic * 3 + jc] = x2;
-          o[jc * 3 + ic].re = -x2.re;
-          o[jc * 3 + ic].im = x2.im;
+          o[ic * nc + jc] = x2;
+          o[jc * nc + ic].re = -x2.re;
+          o[jc * nc + ic].im = x2.im;
         }
     }
   }
+}
+
+void FN(ora_trace)(int kind, R *r, const R *a, long n, const int *idx_a, const int *gang)
+{
+  FN(ora_trace_n)(3, kind, r, a, n, idx_a, gang);
 }
 
 /* global reductions in the reference's order: one double sum over all sites
@@ -250,8 +286,8 @@ void FN(ora_trace)(int kind, R *r, const R *a, long n, const int *idx_a, const i
  * X_dot_X, 4 norm2 (QLA_norm2_c of the site-precision element, evaluated in
  * R, then added in double).  out2 = (re, im) in double before the final
  * rounding. */
-void FN(ora_gdot)(int kind, int perm, double *out2, const R *a, const R *b, long n, int ne, const int *idx_a,
-                  const int *idx_b, const int *gang)
+void FN(ora_gdot_n)(int nc, int kind, int perm, double *out2, const R *a, const R *b, long n, int ne,
+                    const int *idx_a, const int *idx_b, const int *gang)
 {
   const FN(sc) *A = (const FN(sc) *)a, *Bv = (const FN(sc) *)(b ? b : a);
   double sr = 0., si = 0.;
@@ -264,7 +300,8 @@ void FN(ora_gdot)(int kind, int perm, double *out2, const R *a, const R *b, long
         sr += at.re * at.re + at.im * at.im;
         continue;
       }
-      const int ea = (kind == 2) ? (perm == 1 ? (e % 3) * 3 + e / 3 : (e % 12) * 12 + e / 12) : e;
+      const int bl = (perm == 1) ? nc : 4 * nc;
+      const int ea = (kind == 2) ? (e % bl) * bl + e / bl : e;
       const double ur = A[ka * ne + ea].re, ui = A[ka * ne + ea].im;
       const double vr = Bv[kb * ne + e].re, vi = Bv[kb * ne + e].im;
       if (kind == 2) {
@@ -278,6 +315,12 @@ void FN(ora_gdot)(int kind, int perm, double *out2, const R *a, const R *b, long
   }
   out2[0] = sr;
   out2[1] = si;
+}
+
+void FN(ora_gdot)(int kind, int perm, double *out2, const R *a, const R *b, long n, int ne, const int *idx_a,
+                  const int *idx_b, const int *gang)
+{
+  FN(ora_gdot_n)(3, kind, perm, out2, a, b, n, ne, idx_a, idx_b, gang);
 }
 
 /* out = sum over the sites of a, each component in double (the caller

@@ -1,0 +1,327 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA DN redot entry points (extern "C"), reference: lib/perl/build_qla.pl:2250-2284 (real part of the global inner product)
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_DN_r_veq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_V_dot_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_V_dot_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pV_dot_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pV_dot_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_V_dot_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_V_dot_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pV_dot_V", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 3, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pV_dot_pV", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_H_dot_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_H_dot_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pH_dot_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pH_dot_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_H_dot_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_H_dot_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pH_dot_H", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 6, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pH_dot_pH", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_D_dot_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_D_dot_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pD_dot_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pD_dot_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_D_dot_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_D_dot_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pD_dot_D", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 12, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 32, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pD_dot_pD", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_M_dot_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_M_dot_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pM_dot_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_veq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_veq_re_pM_dot_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_M_dot_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_M_dot_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pM_dot_M", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+QLAB_EXPORT void QLA_DN_r_xeq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  switch (nc) {
+    case 2: qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 3: qlab::api_reduce<qlab::ReDotOp<double, 9, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 4: qlab::api_reduce<qlab::ReDotOp<double, 16, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    case 8: qlab::api_reduce<qlab::ReDotOp<double, 64, double>>("DN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
+    default: qlab::set_error(QLAGPU_ERR_ARG, "QLA_DN_r_xeq_re_pM_dot_pM", "nc not compiled (supported: 2, 3, 4, 8)");
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA FN gsum entry points (extern "C"), reference: lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+#include "../qla_ncolor.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_FN_v_veq_sum_V(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_v_veq_sum_pV(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_h_veq_sum_H(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_h_veq_sum_pH(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_d_veq_sum_D(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_d_veq_sum_pD(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_m_veq_sum_M(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_m_veq_sum_pM(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_p_veq_sum_P(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_p_veq_sum_pP(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_v_veq_sum_V(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_v_veq_sum_pV(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_h_veq_sum_H(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_h_veq_sum_pH(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_d_veq_sum_D(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_d_veq_sum_pD(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_m_veq_sum_M(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_m_veq_sum_pM(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_p_veq_sum_P(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_DFN_p_veq_sum_pP(int nc, void * r, void * a, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_FN_v_xeq_sum_V(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_v_xeq_sum_pV(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_h_xeq_sum_H(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_h_xeq_sum_pH(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_d_xeq_sum_D(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_d_xeq_sum_pD(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_m_xeq_sum_M(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_m_xeq_sum_pM(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_p_xeq_sum_P(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_FN_p_xeq_sum_pP(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_v_xeq_sum_V(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_v_xeq_sum_pV(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_h_xeq_sum_H(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_h_xeq_sum_pH(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_d_xeq_sum_D(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_d_xeq_sum_pD(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_m_xeq_sum_M(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_m_xeq_sum_pM(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_p_xeq_sum_P(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_DFN_p_xeq_sum_pP(int nc, void * r, void * a, int * index, int n) {
+  qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+}  // extern "C"

@@ -25,6 +25,7 @@ Outputs (all written by this script, committed):
 """
 import itertools
 import json
+import re
 import os
 import sys
 
@@ -209,6 +210,13 @@ def gen_fn(prec="F"):
                         add(name, [(f"QLA_{OP}_Complex *", "r"), ("void *", "a"), ("void *", "b")] + tail +
                             [("int", "n")], _fn_switch(FN_NCS, call, name), "dot", CITE["dot"],
                             dict(dest="c", var=var, a=sa, b=sb, out=outR))
+                        name = f"QLA_{rpc}_r_{var}eq_re_{sa}_dot_{sb}"
+                        call = lambda nc, T=T, pa_=pa_, pb_=pb_, gang=gang, outR=outR: (
+                            f"qlab::api_reduce<qlab::ReDotOp<{R}, {ncpl[T](nc)}, {outR}>>({kid('redot')}, r, "
+                            f"sizeof({outR}), {opnd(pa_, 'a')}, {opnd(pb_, 'b')}, {gang}, n);")
+                        add(name, [(f"QLA_{OP}_Real *", "r"), ("void *", "a"), ("void *", "b")] + tail +
+                            [("int", "n")], _fn_switch(FN_NCS, call, name), "redot", CITE["redot"],
+                            dict(dest="r", var=var, a=sa, b=sb, out=outR))
     for var in ["v", "x"]:
         gang = "index" if var == "x" else "nullptr"
         tail = [("int *", "index")] if var == "x" else []
@@ -274,6 +282,64 @@ def gen_fn(prec="F"):
                     add(name, [("void *", "r"), ("void *", "a"), ("void *", "b")] + tail + [("int", "n")],
                         _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["minv"],
                         dict(dest=T_, eqop="eq", var=var, a=s1, b=s2, fn="inverse_" + T_))
+    return fns
+
+
+# record length at nc colours for the record lengths of the fixed-colour generator
+NE_AT_NC = {"1": "1", "3": "nc", "6": "2 * nc", "12": "4 * nc", "9": "nc * nc", "144": "16 * nc * nc"}
+
+
+def _ncolor_body(body):
+    """The run-time-nc call (qla_ncolor.cuh) for a fixed-colour body of
+    gen_ewise / gen_sitefield."""
+    m = re.match(r"qlab::(api_\w+)<([^>]*)>\((\"[^\"]*\"), (.*)\);$", body, re.S)
+    api, targs, kid, rest = m.group(1), [t.strip() for t in m.group(2).split(",")], m.group(3), m.group(4)
+    kid = re.sub(r'"(F3|D3)_', lambda mm: '"' + mm.group(1)[0] + "N_", kid)
+    ne = lambda t: NE_AT_NC[t]  # noqa: E731
+    if api == "api_ew":
+        R_, NE_, SH, PERM, SC, SRE = targs
+        return f"qlab::api_ew_n<{R_}, {SH}, {SC}, {SRE}>({kid}, nc, {ne(NE_)}, {PERM}, {rest});"
+    if api == "api_ldot":
+        R_, NE_, KIND, PERM = targs
+        return f"qlab::api_ldot_n<{R_}, {KIND}>({kid}, nc, {ne(NE_)}, {PERM}, {rest});"
+    if api in ("api_outer", "api_diagfill", "api_antiherm"):
+        return f"qlab::{api}_n<{targs[0]}>({kid}, nc, {rest});"
+    if api in ("api_fill", "api_zero", "api_mask"):
+        return f"qlab::{api}_n<{targs[0]}>({kid}, nc, {ne(targs[1])}, {rest});"
+    if api == "api_sub":
+        return f"qlab::api_sub_n<{targs[0]}>({kid}, nc, {rest});"
+    if api == "api_gamma":
+        return f"qlab::api_gamma_n<{targs[0]}, {targs[2]}>({kid}, nc, {ne(targs[1])}, {rest});"
+    if api == "api_trace":
+        return f"qlab::api_trace_n<{targs[0]}, {targs[1]}>({kid}, nc, {rest});"
+    if api == "api_gdot":
+        R_, NE_, KIND, PERM, OUT = targs
+        return f"qlab::api_gdot_n<{R_}, {KIND}, {OUT}>({kid}, nc, {ne(NE_)}, {PERM}, {rest});"
+    if api == "api_gsum":
+        out = targs[2] if len(targs) > 2 else targs[0]
+        return f"qlab::api_gsum_n<{targs[0]}, {out}>({kid}, nc, {ne(targs[1])}, {rest});"
+    if api == "api_convert":
+        return f"qlab::api_convert_n<{targs[0]}, {targs[1]}>({kid}, nc, {ne(targs[2])}, {rest});"
+    raise ValueError(api)
+
+
+def gen_fn_wide(prec):
+    """The element-wise, site-local product, fill / component / gamma /
+    trace, global P / adjoint-form reduction, global sum and (for F)
+    precision-conversion families of QLA_FN_ / QLA_DFN_ / QLA_FDN_ (prec "F")
+    or QLA_DN_ (prec "D"): the entry points of gen_ewise and gen_sitefield
+    with a leading int nc, record arguments as void * (the reference's
+    variably sized records) and the run-time-nc kernels of qla_ncolor.cuh."""
+    src_pc = "F3" if prec == "F" else "D3"
+    R = "float" if prec == "F" else "double"
+    fns = []
+    for fn in gen_ewise(src_pc, R, prec) + gen_sitefield(src_pc, R, prec):
+        m = re.match(r"QLA_(F3|D3|DF3|FD3)_(.*)$", fn.name)
+        lib = {"F3": "FN", "D3": "DN", "DF3": "DFN", "FD3": "FDN"}[m.group(1)]
+        params = [("int", "nc")]
+        for t, nm in fn.params:
+            params.append(("void *", nm) if re.search(r"QLA_[FD]3_", t) else (t, nm))
+        fns.append(Fn(f"QLA_{lib}_{m.group(2)}", params, _ncolor_body(fn.body), fn.family, fn.cite, fn.kinds))
     return fns
 
 
@@ -1092,10 +1158,11 @@ def main():
     headers = {}
     for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None),
                      ("DN", None, None)]:
-        for fn in (gen_int() if pc == "I" else gen_fn("F") if pc == "FN" else gen_fn("D") if pc == "DN"
-                   else gen_pc(pc, R, P)):
+        for fn in (gen_int() if pc == "I" else gen_fn("F") + gen_fn_wide("F") if pc == "FN"
+                   else gen_fn("D") + gen_fn_wide("D") if pc == "DN" else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
-            hpc = {"FD3": "DF3"}.get(hpc, hpc)  # the reference declares QLA_FD3_ in qla_df3.h
+            # the reference declares QLA_FD3_ in qla_df3.h, QLA_FDN_ in qla_dfn.h
+            hpc = {"FD3": "DF3", "FDN": "DFN"}.get(hpc, hpc)
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
             manifest.append(dict(name=fn.name, pc=hpc, family=fn.family, params=[n for _, n in fn.params],
@@ -1126,6 +1193,9 @@ def main():
             extra = '#include "../qla_ewise.cuh"\n'
         if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert"):
             extra = '#include "../qla_sitefield.cuh"\n'
+        if pc in ("FN", "DN") and (family.startswith("ewise") or family in (
+                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert")):
+            extra = '#include "../qla_ncolor.cuh"\n'
         if pc in ("FN", "DN") and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
         if pc in ("FN", "DN") and family == "mfunc_ext":

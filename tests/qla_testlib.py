@@ -498,7 +498,12 @@ def ewise_oracle_plan(e):
     return "ewise", {"shape": 0, "perm": 0, "scal_kind": 0}
 
 
-def ewise_inputs(e, rng, dt, n, ns):
+def ne_at(letter, nc):
+    """complex numbers per record of the given letter at nc colours"""
+    return {"V": nc, "H": 2 * nc, "D": 4 * nc, "M": nc * nc, "P": 16 * nc * nc, "C": 1}[letter]
+
+
+def ewise_inputs(e, rng, dt, n, ns, nc=3):
     """Seeded host inputs for manifest entry e: a dict param -> array (records
     of ns sites for sources, n sites for the destination), pointer-form
     index tables, and the gang subset for x forms."""
@@ -518,7 +523,7 @@ def ewise_inputs(e, rng, dt, n, ns):
         elif letter == "C":
             arr = rng.standard_normal((nrec, 2)).astype(dt)
         else:
-            arr = rng.standard_normal((nrec, 2 * NE3[letter])).astype(dt)
+            arr = rng.standard_normal((nrec, 2 * ne_at(letter, nc))).astype(dt)
         ins[name] = (letter, is_ptr, arr)
     # scalar constants (c / r forms): a single value
     plan, kw = ewise_oracle_plan(e)
@@ -530,7 +535,7 @@ def ewise_inputs(e, rng, dt, n, ns):
     return ins, idx, gang
 
 
-def ewise_oracle(e, ins, idx, gang, n):
+def ewise_oracle(e, ins, idx, gang, n, nc=3):
     """The oracle's result for manifest entry e on ewise_inputs()."""
     plan, kw = ewise_oracle_plan(e)
     r = ins["r"][2].copy()
@@ -547,17 +552,17 @@ def ewise_oracle(e, ins, idx, gang, n):
         return _i32(idx.get(name))
 
     if plan == "outer":
-        getattr(oracle(), "ora_outer_" + t)(eq, ptr(r), ptr(arr("a")), ptr(arr("b")), ctypes.c_long(nsites),
-                                           ptr(ix("a")), ptr(ix("b")), ptr(g))
+        getattr(oracle(), "ora_outer_n_" + t)(nc, eq, ptr(r), ptr(arr("a")), ptr(arr("b")), ctypes.c_long(nsites),
+                                             ptr(ix("a")), ptr(ix("b")), ptr(g))
         return r
     if plan == "ldot":
-        ne = NE3[ins["a"][0]]
-        getattr(oracle(), "ora_ldot_" + t)(kw["kind"], _perm_code(ins["a"][0]), eq, ptr(r), ptr(arr("a")),
-                                          ptr(arr("b")), ctypes.c_long(nsites), ne, ptr(ix("a")), ptr(ix("b")),
-                                          ptr(g))
+        ne = ne_at(ins["a"][0], nc)
+        getattr(oracle(), "ora_ldot_n_" + t)(nc, kw["kind"], _perm_code(ins["a"][0]), eq, ptr(r), ptr(arr("a")),
+                                            ptr(arr("b")), ctypes.c_long(nsites), ne, ptr(ix("a")), ptr(ix("b")),
+                                            ptr(g))
         return r
     dest = e["dest"]
-    ne = NE3[dest]
+    ne = ne_at(dest, nc)
     cs = ctypes.c_float if t == "f" else ctypes.c_double
     sre = sim = 0.0
     s_arr, s_idx = None, None
@@ -574,7 +579,7 @@ def ewise_oracle(e, ins, idx, gang, n):
         b_name, c_name = "a", "b"
     else:
         b_name, c_name = "a", None
-    getattr(oracle(), "ora_ewise_" + t)(kw["shape"], kw["perm"], eq, ptr(r), ptr(arr(b_name)),
+    getattr(oracle(), "ora_ewise_n_" + t)(nc, kw["shape"], kw["perm"], eq, ptr(r), ptr(arr(b_name)),
                                        ptr(arr(c_name)) if c_name else None, ptr(s_arr), kw["scal_kind"],
                                        cs(sre), cs(sim), ctypes.c_long(nsites), ne, ptr(ix(b_name)),
                                        ptr(ix(c_name)) if c_name else None, ptr(s_idx), ptr(g))
@@ -589,18 +594,55 @@ SF_FAMILIES = ("fill", "mask", "component", "gamma", "trace")
 NE_OF = dict(NE3, C=1)
 
 
-def rec_bytes(letter, dt):
+def rec_bytes(letter, dt, nc=3):
     """bytes per record of a field of the given letter in precision dt"""
     if letter == "I":
         return 4
-    return np.dtype(dt).itemsize * (1 if letter == "R" else 2 * NE_OF[letter])
+    return np.dtype(dt).itemsize * (1 if letter == "R" else 2 * ne_at(letter, nc))
+
+
+NCOLOR_FAMILIES = ("ewise_v", "ewise_h", "ewise_d", "ewise_m", "ewise_p", "ldot", "fill", "mask", "component",
+                   "gamma", "trace", "gred", "gsum", "convert")
+
+
+def fixed_colour_twin(name):
+    """The QLA_F3_ / QLA_D3_ / QLA_DF3_ / QLA_FD3_ entry point a QLA_FN_ /
+    QLA_DN_ / QLA_DFN_ / QLA_FDN_ one generalises."""
+    import re
+    m = re.match(r"QLA_(FN|DN|DFN|FDN)_(.*)$", name)
+    return "QLA_" + {"FN": "F3", "DN": "D3", "DFN": "DF3", "FDN": "FD3"}[m.group(1)] + "_" + m.group(2)
+
+
+def ncolor_case(e, rng, n, ns, nc):
+    """(inputs, oracle result, kind) of the fixed-colour twin entry e at nc
+    colours: kind "map" (bit-exact field result), "gred" / "gsum" (one value
+    or record, reference summation order), "convert"."""
+    fam = e["family"]
+    dt = np.float64 if e["pc"] == "D3" else np.float32
+    if fam == "convert":
+        ins, idx, gang = convert_inputs(e, rng, n, ns, nc=nc)
+        return (ins, idx, gang, {}), convert_oracle(e, ins, idx, gang, n, nc=nc), "convert"
+    if fam in ("gred", "gsum"):
+        ins, idx, gang, ints = sitefield_inputs(e, rng, dt, n, ns, nc=nc)
+        if fam == "gred":
+            out = gred_oracle(e, ins, idx, gang, n, nc=nc)
+            odt = np.float64 if e.get("out") == "double" else dt
+            want = out[:1].astype(odt) if e["dest"] == "r" else out.astype(odt)
+        else:
+            want = gsum_oracle(e, ins, idx, gang, n, nc=nc)
+        return (ins, idx, gang, ints), want, fam
+    if fam in SF_FAMILIES:
+        ins, idx, gang, ints = sitefield_inputs(e, rng, dt, n, ns, nc=nc)
+        return (ins, idx, gang, ints), sitefield_oracle(e, ins, idx, gang, n, ints, nc=nc), "map"
+    ins, idx, gang = ewise_inputs(e, rng, dt, n, ns, nc=nc)
+    return (ins, idx, gang, {}), ewise_oracle(e, ins, idx, gang, n, nc=nc), "map"
 
 
 def _letter(src):
     return src[1:] if src.startswith("p") and len(src) > 1 else src
 
 
-def sitefield_inputs(e, rng, dt, n, ns):
+def sitefield_inputs(e, rng, dt, n, ns, nc=3):
     """Seeded inputs for a site-field entry: (ins, idx, gang, ints) with ins
     as ewise_inputs, ints the values of the int arguments (colour / spin
     indices, mu)."""
@@ -610,7 +652,7 @@ def sitefield_inputs(e, rng, dt, n, ns):
         if name in ("n", "index"):
             continue
         if t == "int":
-            hi = {"mu": 16, "i_c": 3, "j_c": 3, "i_s": 2 if half else 4, "j_s": 4}[name]
+            hi = {"mu": 16, "i_c": nc, "j_c": nc, "i_s": 2 if half else 4, "j_s": 4}[name]
             ints[name] = int(rng.integers(0, hi))
             continue
         letter, is_ptr = param_type(t)
@@ -624,7 +666,7 @@ def sitefield_inputs(e, rng, dt, n, ns):
         elif letter == "C":
             arr = rng.standard_normal((nrec, 2)).astype(dt)
         else:
-            arr = rng.standard_normal((nrec, 2 * NE3[letter])).astype(dt)
+            arr = rng.standard_normal((nrec, 2 * ne_at(letter, nc))).astype(dt)
         if name == "a" and e.get("op") in ("fill", "diagfill"):
             arr = arr.reshape(-1)
         ins[name] = (letter, is_ptr, arr)
@@ -633,7 +675,7 @@ def sitefield_inputs(e, rng, dt, n, ns):
     return ins, idx, gang, ints
 
 
-def sitefield_oracle(e, ins, idx, gang, n, ints):
+def sitefield_oracle(e, ins, idx, gang, n, ints, nc=3):
     """The oracle's result for a site-field entry on sitefield_inputs()."""
     r = ins["r"][2].copy()
     t = rtype(r.dtype)
@@ -650,31 +692,31 @@ def sitefield_oracle(e, ins, idx, gang, n, ints):
         return _i32(idx.get(name))
 
     if op == "fill":
-        getattr(O, "ora_fill_" + t)(eq, ptr(r), ptr(arr("a")), nsites, NE3[e["dest"]], ptr(g))
+        getattr(O, "ora_fill_" + t)(eq, ptr(r), ptr(arr("a")), nsites, ne_at(e["dest"], nc), ptr(g))
     elif op == "diagfill":
-        getattr(O, "ora_diagfill_" + t)(eq, ptr(r), ptr(arr("a")), nsites, ptr(g))
+        getattr(O, "ora_diagfill_n_" + t)(nc, eq, ptr(r), ptr(arr("a")), nsites, ptr(g))
     elif op == "zero":
-        getattr(O, "ora_zero_" + t)(ptr(r), nsites, NE3[e["dest"]], ptr(g))
+        getattr(O, "ora_zero_" + t)(ptr(r), nsites, ne_at(e["dest"], nc), ptr(g))
     elif op == "mask":
-        getattr(O, "ora_mask_" + t)(ptr(r), ptr(arr("a")), ptr(arr("b")), nsites, NE3[e["dest"]], ptr(ix("a")),
-                                    ptr(ix("b")), ptr(g))
+        getattr(O, "ora_mask_" + t)(ptr(r), ptr(arr("a")), ptr(arr("b")), nsites, ne_at(e["dest"], nc),
+                                    ptr(ix("a")), ptr(ix("b")), ptr(g))
     elif fam == "component":
         what = {"elem": "e", "colorvec": "c", "diracvec": "d"}[op]
-        getattr(O, "ora_component_" + t)(ord(what), ord(e["dest"]), ord(_letter(e["a"])), ptr(r), ptr(arr("a")),
-                                         ints.get("i_c", 0), ints.get("i_s", 0), ints.get("j_c", 0),
-                                         ints.get("j_s", 0), nsites, ptr(ix("a")), ptr(g))
+        getattr(O, "ora_component_n_" + t)(nc, ord(what), ord(e["dest"]), ord(_letter(e["a"])), ptr(r),
+                                           ptr(arr("a")), ints.get("i_c", 0), ints.get("i_s", 0),
+                                           ints.get("j_c", 0), ints.get("j_s", 0), nsites, ptr(ix("a")), ptr(g))
     elif fam == "gamma":
-        getattr(O, "ora_gamma_" + t)(1 if op == "gamma_right" else 0, NE3[e["dest"]], ints["mu"], ptr(r),
-                                     ptr(arr("a")), nsites, ptr(ix("a")), ptr(g))
+        getattr(O, "ora_gamma_n_" + t)(nc, 1 if op == "gamma_right" else 0, ne_at(e["dest"], nc), ints["mu"],
+                                       ptr(r), ptr(arr("a")), nsites, ptr(ix("a")), ptr(g))
     elif fam == "trace":
         kind = {"trace": 0, "re_trace": 1, "im_trace": 2, "antiherm": 3}[op]
-        getattr(O, "ora_trace_" + t)(kind, ptr(r), ptr(arr("a")), nsites, ptr(ix("a")), ptr(g))
+        getattr(O, "ora_trace_n_" + t)(nc, kind, ptr(r), ptr(arr("a")), nsites, ptr(ix("a")), ptr(g))
     else:
         raise ValueError(e["name"])
     return r
 
 
-def gred_oracle(e, ins, idx, gang, n):
+def gred_oracle(e, ins, idx, gang, n, nc=3):
     """Reference-order global reduction (re, im) in double for a gred entry."""
     a = ins["a"][2]
     t = rtype(a.dtype)
@@ -682,29 +724,29 @@ def gred_oracle(e, ins, idx, gang, n):
     kind = LD_KINDS[e["kind"]]
     perm = _perm_code(_letter(e["a"]).rstrip("a"))
     b = ins["b"][2] if "b" in ins else None
-    getattr(oracle(), "ora_gdot_" + t)(kind, perm, ptr(out), ptr(a), ptr(b),
-                                       ctypes.c_long(len(gang) if gang is not None else n),
-                                       NE3[_letter(e["a"]).rstrip("a")], ptr(_i32(idx.get("a"))),
-                                       ptr(_i32(idx.get("b"))), ptr(_i32(gang)))
+    getattr(oracle(), "ora_gdot_n_" + t)(nc, kind, perm, ptr(out), ptr(a), ptr(b),
+                                         ctypes.c_long(len(gang) if gang is not None else n),
+                                         ne_at(_letter(e["a"]).rstrip("a"), nc), ptr(_i32(idx.get("a"))),
+                                         ptr(_i32(idx.get("b"))), ptr(_i32(gang)))
     return out
 
 
-def gsum_oracle(e, ins, idx, gang, n):
+def gsum_oracle(e, ins, idx, gang, n, nc=3):
     """Reference-order global sum (one record) for a gsum entry, rounded to
     the output precision (the site precision; double for QLA_DF3_)."""
     a = ins["a"][2]
     t = rtype(a.dtype)
     T = _letter(e["a"])
-    out = np.zeros(2 * NE3[T], np.float64)
+    out = np.zeros(2 * ne_at(T, nc), np.float64)
     getattr(oracle(), "ora_gsum_" + t)(ptr(out), ptr(a), ctypes.c_long(len(gang) if gang is not None else n),
-                                       NE3[T], ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
+                                       ne_at(T, nc), ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
     return out if e.get("out") == "double" else out.astype(a.dtype)
 
 
-def convert_inputs(e, rng, n, ns):
+def convert_inputs(e, rng, n, ns, nc=3):
     """Inputs of a QLA_DF3_ / QLA_FD3_ conversion: (ins, idx, gang)."""
     src_dt, dst_dt = (np.float32, np.float64) if e["lib"] == "DF3" else (np.float64, np.float32)
-    ne = NE3[e["dest"]]
+    ne = ne_at(e["dest"], nc)
     a = rng.standard_normal((ns, 2 * ne)).astype(src_dt)
     r = rng.standard_normal((n, 2 * ne)).astype(dst_dt)
     ins = {"r": (e["dest"], False, r), "a": (e["dest"], e["a"].startswith("p"), a)}
@@ -713,9 +755,9 @@ def convert_inputs(e, rng, n, ns):
     return ins, idx, gang
 
 
-def convert_oracle(e, ins, idx, gang, n):
+def convert_oracle(e, ins, idx, gang, n, nc=3):
     r = ins["r"][2].copy()
     f = oracle().ora_convert_df if e["lib"] == "DF3" else oracle().ora_convert_fd
-    f(ptr(r), ptr(ins["a"][2]), ctypes.c_long(len(gang) if gang is not None else n), 2 * NE3[e["dest"]],
+    f(ptr(r), ptr(ins["a"][2]), ctypes.c_long(len(gang) if gang is not None else n), 2 * ne_at(e["dest"], nc),
       ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
     return r

@@ -235,9 +235,9 @@ def test_prototypes_match_reference_headers():
     nargs_fn = {}
     for h in ("qla_fn.h", "qla_dfn.h", "qla_dn.h"):
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
-        for m in re.finditer(r"void (QLA_(?:D?FN|DN)_\w+) \((.*?)\);", txt):
+        for m in re.finditer(r"void (QLA_(?:D?FN|DN|FDN)_\w+) \((.*?)\);", txt):
             # VLA record types: compare the parameter count (the first is int nc)
-            nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)", m.group(2)))
+            nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)|\bQLA_Int\b", m.group(2)))
     for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h"):
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
         for m in re.finditer(r"void (QLA_\w+) \((.*?)\);", txt):
@@ -314,7 +314,7 @@ def test_oracle_n_colour_matrix_functions_match_reference_library(pc, dt):
             assert T.bits_equal(rr, T.ora_minv(g, b, n, nb, nc=nc)), (nc, dest)
 
 
-def _ref_args(e, ins, idx, gang, n, r, ints=None):
+def _ref_args(e, ins, idx, gang, n, r, ints=None, nc=3):
     """Host arguments of manifest entry e for the reference library."""
     args, keep = [], []
     for t, name in zip(e["ctypes"], e["params"]):
@@ -329,7 +329,7 @@ def _ref_args(e, ins, idx, gang, n, r, ints=None):
         else:
             letter, is_ptr, arr = ins[name]
             if is_ptr:
-                rec = T.rec_bytes(letter, arr.dtype)
+                rec = T.rec_bytes(letter, arr.dtype, nc)
                 pa = (ctypes.c_void_p * len(idx[name]))(*[arr.ctypes.data + int(j) * rec for j in idx[name]])
                 keep.append(pa)
                 args.append(pa)
@@ -440,7 +440,7 @@ def test_oracle_precision_conversions_match_reference_library():
     n, ns = 13, 17
     bad, count = [], 0
     for e in man:
-        if e["family"] != "convert":
+        if e["family"] != "convert" or e["pc"] != "DF3":
             continue
         ins, idx, gang = T.convert_inputs(e, rng, n, ns)
         want = T.convert_oracle(e, ins, idx, gang, n)
@@ -451,4 +451,39 @@ def test_oracle_precision_conversions_match_reference_library():
         if not T.bits_equal(r, want):
             bad.append(e["name"])
     assert count == 40
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("lib", ["FN", "DN", "DFN"])
+def test_oracle_ncolor_families_match_reference_library(lib):
+    """The element-wise, site-local product, fill / component / gamma /
+    trace families, global P / adjoint-form reductions, sums and conversions
+    of the N-colour libraries at nc = 2 and 5: the oracle against the
+    reference library, bit for bit, every entry point (the reductions and
+    sums with the library on one OpenMP thread)."""
+    import qla_b200
+    man = qla_b200.manifest()
+    byname = {e["name"]: e for e in man}
+    R = T.ref()
+    rng = np.random.default_rng(114)
+    n, ns = 7, 9
+    bad, count = [], 0
+    for e in man:
+        if e["pc"] != lib or e["family"] not in T.NCOLOR_FAMILIES:
+            continue
+        twin = byname[T.fixed_colour_twin(e["name"])]
+        for nc in (2, 5):
+            (ins, idx, gang, ints), want, kind = T.ncolor_case(twin, rng, n, ns, nc)
+            if "mu" in ints:
+                ints["mu"] = count % 16
+                want = T.sitefield_oracle(twin, ins, idx, gang, n, ints, nc=nc)
+            r = np.zeros_like(want) if kind in ("gred", "gsum") else ins["r"][2].copy()
+            args, keep = _ref_args(twin, ins, idx, gang, n, r, ints, nc=nc)
+            with T.ref_one_thread():
+                getattr(R, e["name"])(nc, *args)
+            count += 1
+            if not T.bits_equal(r, want):
+                bad.append((e["name"], nc))
+    assert count > (150 if lib == "DFN" else 2000)
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
