@@ -1558,6 +1558,471 @@ void QLA_DN_M_xeq_M_inverse_pM(int nc, void * r, void * a, void * b, int * index
 void QLA_DN_M_xeq_pM_inverse_M(int nc, void * r, void * a, void * b, int * index, int n);
 /* replaces QLA_DN_M_xeq_pM_inverse_pM (lib/perl/build_qla.pl:1663-1690 (colour matrix inverse times vector / matrix), code-templates/V_eq_M_inverse_V.c:84-168, M_eq_M_inverse_M.c:85-135) */
 void QLA_DN_M_xeq_pM_inverse_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* ---- hop: replaces the DN functions emitted by lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix) */
+/* replaces QLA_DN_H_veq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_D_veq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_D_vpeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vpeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_vmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_vmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_D_vmeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_vmeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_H_veqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_veqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_D(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_D_veqm_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_veqm_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n);
+/* replaces QLA_DN_H_xeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xpeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xpeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xmeq_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xmeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_M_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_M_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_M_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_M_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_Ma_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_Ma_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_Ma_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_Ma_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_pM_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_pM_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_pM_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_pM_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_xeqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_H_xeqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_pMa_times_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_pMa_times_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_pMa_times_H (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_sprecon_pMa_times_pH (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_D (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_D_xeqm_spproj_pD (lib/perl/build_qla.pl:1137-1250 (fused spin projection x colour matrix), make_code_binary.pl:189-336) */
+void QLA_DN_D_xeqm_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n);
+/* replaces QLA_DN_H_eq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_eq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eq_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eq_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_eq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_eq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eq_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eq_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_peq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_peq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_peq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_peq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_peq_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_peq_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_peq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_peq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_peq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_peq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_peq_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_peq_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_meq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_meq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_meq_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_meq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_meq_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_meq_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_meq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_meq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_meq_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_meq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_meq_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_meq_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_eqm_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_eqm_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eqm_spproj_M_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eqm_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eqm_sprecon_M_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eqm_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_H_eqm_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_H_eqm_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eqm_spproj_Ma_times_xD (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eqm_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
+/* replaces QLA_DN_D_eqm_sprecon_Ma_times_xH (doc/qla.tex:476-487 (per-operand index variant 5 of the fused hop terms, not generated by the reference)) */
+void QLA_DN_D_eqm_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n);
 /* ---- ewise_v: replaces the DN functions emitted by lib/perl/build_qla.pl:1256-1335 (constant multiples of a field) */
 /* replaces QLA_DN_V_veq_c_times_V (lib/perl/build_qla.pl:1256-1335 (constant multiples of a field), include/qla_complex.h:258-400) */
 void QLA_DN_V_veq_c_times_V(int nc, void * r, QLA_D_Complex *QLA_B200_RESTRICT a, void * b, int n);
@@ -5864,6 +6329,783 @@ void QLA_DN_m_xeq_sum_pM(int nc, void * r, void * a, int * index, int n);
 void QLA_DN_p_xeq_sum_P(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_DN_p_xeq_sum_pP (lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)) */
 void QLA_DN_p_xeq_sum_pP(int nc, void * r, void * a, int * index, int n);
+/* ---- prop: replaces the DN functions emitted by lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products) */
+/* replaces QLA_DN_P_veq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_M_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_M_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_M_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_M_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Ma_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Ma_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Ma_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Ma_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pM_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pM_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pM_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pM_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pMa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pMa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pMa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pMa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_P_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_Pa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pP_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veq_pPa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_M_veq_spintrace_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_M_veq_spintrace_P(int nc, void * r, void * a, int n);
+/* replaces QLA_DN_M_veq_spintrace_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_M_veq_spintrace_pP(int nc, void * r, void * a, int n);
+/* replaces QLA_DN_P_vpeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_M_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_M_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_M_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_M_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Ma_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Ma_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Ma_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Ma_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pM_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pM_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pM_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pM_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pMa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pMa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pMa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pMa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_P_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_Pa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pP_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vpeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vpeq_pPa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_M_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_M_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_M_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_M_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Ma_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Ma_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Ma_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Ma_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pM_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pM_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pM_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pM_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pMa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pMa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pMa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pMa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_P_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_Pa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pP_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_vmeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_vmeq_pPa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_M_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_M_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_M_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_M_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Ma_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Ma_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Ma_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Ma_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pM_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pM_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pM_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pM_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pMa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pMa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pMa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pMa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_P_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_Pa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pP_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_M(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_Ma(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_pM(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_pMa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_P(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_Pa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_pP(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_veqm_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_veqm_pPa_times_pPa(int nc, void * r, void * a, void * b, int n);
+/* replaces QLA_DN_P_xeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_M_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_M_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_M_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_M_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Ma_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Ma_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Ma_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Ma_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pM_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pM_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pM_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pM_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pMa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pMa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pMa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pMa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_P_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_Pa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pP_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeq_pPa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_M_xeq_spintrace_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_M_xeq_spintrace_P(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DN_M_xeq_spintrace_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_M_xeq_spintrace_pP(int nc, void * r, void * a, int * index, int n);
+/* replaces QLA_DN_P_xpeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_M_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_M_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_M_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_M_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Ma_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Ma_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Ma_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Ma_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pM_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pM_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pM_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pM_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pMa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pMa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pMa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pMa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_P_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_Pa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pP_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xpeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xpeq_pPa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_M_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_M_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_M_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_M_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Ma_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Ma_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Ma_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Ma_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pM_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pM_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pM_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pM_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pMa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pMa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pMa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pMa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_P_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_Pa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pP_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xmeq_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xmeq_pPa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_M_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_M_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_M_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_M_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_M_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_M_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_M_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_M_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Ma_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Ma_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Ma_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Ma_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Ma_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Ma_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Ma_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Ma_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pM_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pM_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pM_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pM_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pM_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pM_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pM_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pM_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pMa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pMa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pMa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pMa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pMa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pMa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pMa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pMa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_P_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_P_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_Pa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_Pa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pP_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pP_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_M (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_M(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_Ma (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_pM (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_pM(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_pMa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_P (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_P(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_Pa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_Pa(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_pP (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
+/* replaces QLA_DN_P_xeqm_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
+void QLA_DN_P_xeqm_pPa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
 
 #ifdef __cplusplus
 }

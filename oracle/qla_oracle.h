@@ -111,6 +111,10 @@ void ora_trace_n_##SFX(int nc, int kind, R *r, const R *a, long n, const int *id
                        const int *gang);                                                          \
 void ora_gdot_n_##SFX(int nc, int kind, int perm, double *out2, const R *a, const R *b, long n,    \
                       int ne, const int *idx_a, const int *idx_b, const int *gang);
+void ora_prop_n_f(int nc, int kind, int ca, int cb, int eqop, float *r, const float *a, const float *b, long n,
+                  const int *idx_a, const int *idx_b, const int *gang);
+void ora_prop_n_d(int nc, int kind, int ca, int cb, int eqop, double *r, const double *a, const double *b, long n,
+                  const int *idx_a, const int *idx_b, const int *gang);
 ORA_NCOLOR_DECL(float, f)
 ORA_NCOLOR_DECL(double, d)
 /* precision conversions of n records of nr reals: QLA_DF_c_eq_c (float to

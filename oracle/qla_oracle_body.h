@@ -305,18 +305,19 @@ void FN(ora_dot_field)(R *r, const R *a, const R *b, long n, int ncplx,
  * kind 0: r (eqop) A P',  1: r (eqop) P' A,  2: r (eqop) P' P'',  3: M (eqop) spintrace(P)
  * with A = M or M^+ (ca / cb), P' = P or P^+ (P^+[i][s][j][t] = conj P[j][t][i][s]);
  * per output element x = (peq|meq ? r : 0), then x (+|-)= a*b over k (kc, then ks). */
-static inline long FN(pix_)(int i, int s, int j, int t, int adj)
+static inline long FN(pix_)(int i, int s, int j, int t, int adj, int nc)
 {
-  return adj ? ((j * 4 + t) * 3 + i) * 4 + s : ((i * 4 + s) * 3 + j) * 4 + t;
+  return adj ? ((j * 4 + t) * nc + i) * 4 + s : ((i * 4 + s) * nc + j) * 4 + t;
 }
-static inline long FN(mix_)(int i, int j, int adj) { return adj ? j * 3 + i : i * 3 + j; }
+static inline long FN(mix_)(int i, int j, int adj, int nc) { return adj ? j * nc + i : i * nc + j; }
 
-void FN(ora_prop)(int kind, int ca, int cb, int eqop, R *r, const R *a, const R *b, long n,
-                  const int *idx_a, const int *idx_b, const int *gang)
+void FN(ora_prop_n)(int nc, int kind, int ca, int cb, int eqop, R *r, const R *a, const R *b, long n,
+                    const int *idx_a, const int *idx_b, const int *gang)
 {
   const int minus = (eqop == 2 || eqop == 3), load = (eqop == 1 || eqop == 2);
-  const long ra = (kind == 0) ? 9 : 144, rb = (kind == 1) ? 9 : 144;
-  const int nel = (kind == 3) ? 9 : 144;
+  const long nm = nc * nc, np_ = 16 * nc * nc;
+  const long ra = (kind == 0) ? nm : np_, rb = (kind == 1) ? nm : np_;
+  const int nel = (kind == 3) ? nm : np_;
   for (long i = 0; i < n; i++) {
     long k = FN(site_)(gang, i);
     const FN(cplx) *A = (const FN(cplx) *)a + FN(rec_)(idx_a, k) * ra;
@@ -326,24 +327,24 @@ void FN(ora_prop)(int kind, int ca, int cb, int eqop, R *r, const R *a, const R 
       FN(cplx) x;
       if (load) x = O[e]; else { x.re = 0.; x.im = 0.; }
       if (kind == 3) {
-        int ic = e / 3, jc = e % 3;
+        int ic = e / nc, jc = e % nc;
         for (int s2 = 0; s2 < 4; s2++) {
-          FN(cplx) v = A[FN(pix_)(ic, s2, jc, s2, 0)];
+          FN(cplx) v = A[FN(pix_)(ic, s2, jc, s2, 0, nc)];
           if (minus) { x.re -= v.re; x.im -= v.im; } else { x.re += v.re; x.im += v.im; }
         }
       } else {
-        int ic = e / 48, is = (e / 12) % 4, jc = (e / 4) % 3, js = e % 4;
-        for (int kc = 0; kc < 3; kc++) {
+        int ic = e / (16 * nc), is = (e / (4 * nc)) % 4, jc = (e / 4) % nc, js = e % 4;
+        for (int kc = 0; kc < nc; kc++) {
           if (kind == 2) {
             for (int ks = 0; ks < 4; ks++) {
-              FN(cplx) u = A[FN(pix_)(ic, is, kc, ks, ca)], v = B[FN(pix_)(kc, ks, jc, js, cb)];
+              FN(cplx) u = A[FN(pix_)(ic, is, kc, ks, ca, nc)], v = B[FN(pix_)(kc, ks, jc, js, cb, nc)];
               FN(cmac_)(&x, minus, ca, cb, u.re, u.im, v.re, v.im);
             }
           } else if (kind == 0) {
-            FN(cplx) u = A[FN(mix_)(ic, kc, ca)], v = B[FN(pix_)(kc, is, jc, js, cb)];
+            FN(cplx) u = A[FN(mix_)(ic, kc, ca, nc)], v = B[FN(pix_)(kc, is, jc, js, cb, nc)];
             FN(cmac_)(&x, minus, ca, cb, u.re, u.im, v.re, v.im);
           } else {
-            FN(cplx) u = A[FN(pix_)(ic, is, kc, js, ca)], v = B[FN(mix_)(kc, jc, cb)];
+            FN(cplx) u = A[FN(pix_)(ic, is, kc, js, ca, nc)], v = B[FN(mix_)(kc, jc, cb, nc)];
             FN(cmac_)(&x, minus, ca, cb, u.re, u.im, v.re, v.im);
           }
         }
@@ -351,6 +352,12 @@ void FN(ora_prop)(int kind, int ca, int cb, int eqop, R *r, const R *a, const R 
       O[e] = x;
     }
   }
+}
+
+void FN(ora_prop)(int kind, int ca, int cb, int eqop, R *r, const R *a, const R *b, long n,
+                  const int *idx_a, const int *idx_b, const int *gang)
+{
+  FN(ora_prop_n)(3, kind, ca, cb, eqop, r, a, b, n, idx_a, idx_b, gang);
 }
 
 #undef FN

@@ -18,6 +18,7 @@
 // for the record sizes here).
 #pragma once
 #include "qla_sitefield.cuh"
+#include "qla_prop.cuh"
 
 namespace qlab {
 
@@ -812,6 +813,72 @@ inline void api_convert_n(const char* kid, int nc, int ne, void* r, Opnd a, cons
   p.gang = gang;
   p.n = n;
   convertn_kernel<RIN, ROUT><<<nc_grid((long long)n * 2 * ne), 256, 0, current_stream()>>>(p, 2 * ne);
+  check_launch(kid);
+}
+
+// ---------------------------------------------------------------------------
+// DiracPropagator products and the spin trace at nc colours
+// (build_qla.pl:1588-1661, 942-968): one thread per output complex number,
+// x = (peq | meq ? r : 0), then x (+|-)= a * b over k (kc, then ks), each
+// product and sum rounded as the reference's QLA_c_{peq,meq}_*_times_* macros.
+// e = ((ic*4 + is)*nc + jc)*4 + js for P, ic*nc + jc for the trace's M.
+template <typename R, int KIND, bool CA, bool CB>
+__global__ void __launch_bounds__(256) propn_kernel(const EwParams p, int nc) {
+  const int nm = nc * nc, np = 16 * nc * nc;
+  const int nel = (KIND == PK_TRACE) ? nm : np;
+  const int ra = (KIND == PK_MP) ? nm : np, rb = (KIND == PK_PM) ? nm : np;
+  const float inv_nc = 1.0f / (float)nc, inv_4nc = 1.0f / (float)(4 * nc);
+  const bool minus = (p.eqop == MEQ || p.eqop == EQM), load = (p.eqop == PEQ || p.eqop == MEQ);
+  auto pix = [nc](int i, int s, int j, int t, bool adj) {
+    return adj ? ((j * 4 + t) * nc + i) * 4 + s : ((i * 4 + s) * nc + j) * 4 + t;
+  };
+  auto mix = [nc](int i, int j, bool adj) { return adj ? j * nc + i : i * nc + j; };
+  for (SiteElemWalk w(nel); w.i < p.n; w.next(nel)) {
+    const long long k = p.gang ? (long long)p.gang[w.i] : w.i;
+    const Cx<R>* A = rec_ptr<R>(p.b, k, ra);
+    Cx<R>* O = static_cast<Cx<R>*>(p.out) + k * nel + w.e;
+    Cx<R> x = load ? *O : Cx<R>{R(0), R(0)};
+    if constexpr (KIND == PK_TRACE) {
+      const int ic = div_small(w.e, nc, inv_nc), jc = w.e - ic * nc;
+      for (int s2 = 0; s2 < 4; s2++) {
+        const Cx<R> v = A[pix(ic, s2, jc, s2, false)];
+        x = minus ? Cx<R>{rsub(x.re, v.re), rsub(x.im, v.im)} : Cx<R>{radd(x.re, v.re), radd(x.im, v.im)};
+      }
+    } else {
+      const Cx<R>* B = rec_ptr<R>(p.c, k, rb);
+      const int row = div_small(w.e, 4 * nc, inv_4nc), col = w.e - row * 4 * nc;
+      const int ic = row >> 2, is = row & 3, jc = col >> 2, js = col & 3;
+      for (int kc = 0; kc < nc; kc++) {
+        if constexpr (KIND == PK_PP) {
+          for (int ks = 0; ks < 4; ks++) cmac<CA, CB>(x, minus, A[pix(ic, is, kc, ks, CA)], B[pix(kc, ks, jc, js, CB)]);
+        } else if constexpr (KIND == PK_MP) {
+          cmac<CA, CB>(x, minus, A[mix(ic, kc, CA)], B[pix(kc, is, jc, js, CB)]);
+        } else {
+          cmac<CA, CB>(x, minus, A[pix(ic, is, kc, js, CA)], B[mix(kc, jc, CB)]);
+        }
+      }
+    }
+    *O = x;
+  }
+}
+
+template <typename R, int KIND, bool CA, bool CB>
+inline void api_prop_n(const char* kid, int nc, void* r, Opnd a, Opnd b, const int* gang, int n, int eqop) {
+  if (!nc_ok(kid, nc) || n <= 0) return;
+  if (!r || !opnd_ok(a) || (KIND != PK_TRACE && !opnd_ok(b))) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL array argument");
+    return;
+  }
+  EwParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.out = r;
+  p.b = a;
+  p.c = b;
+  p.gang = gang;
+  p.n = n;
+  p.eqop = eqop;
+  const long long nel = (KIND == PK_TRACE) ? (long long)nc * nc : 16LL * nc * nc;
+  propn_kernel<R, KIND, CA, CB><<<nc_grid((long long)n * nel), 256, 0, current_stream()>>>(p, nc);
   check_launch(kid);
 }
 

@@ -282,6 +282,19 @@ def gen_fn(prec="F"):
                     add(name, [("void *", "r"), ("void *", "a"), ("void *", "b")] + tail + [("int", "n")],
                         _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["minv"],
                         dict(dest=T_, eqop="eq", var=var, a=s1, b=s2, fn="inverse_" + T_))
+    # fused hop terms: the fixed-colour generator's entry points with the
+    # colour count of the op templates switched over the compiled nc
+    src_pc = "F3" if prec == "F" else "D3"
+    for fn in gen_pc(src_pc, R, prec):
+        if fn.family != "hop":
+            continue
+        name = fn.name.replace(f"QLA_{src_pc}_", f"QLA_{LIB}_", 1)
+        params = [(("void *", nm) if re.search(r"QLA_[FD]3_", t) else (t, nm)) for t, nm in fn.params]
+        guard, call = fn.body.split("\n  ", 1)
+        call = call.replace(f'"{src_pc}_', f'"{LIB}_')
+        call_of_nc = lambda nc, call=call: re.sub(  # noqa: E731
+            r"(Sp\w+Op<\w+), 3([,>])", lambda m: f"{m.group(1)}, {nc}{m.group(2)}", call)
+        add(name, params, guard + "\n  " + _fn_switch(FN_NCS, call_of_nc, name), "hop", fn.cite, fn.kinds)
     return fns
 
 
@@ -320,6 +333,8 @@ def _ncolor_body(body):
         return f"qlab::api_gsum_n<{targs[0]}, {out}>({kid}, nc, {ne(targs[1])}, {rest});"
     if api == "api_convert":
         return f"qlab::api_convert_n<{targs[0]}, {targs[1]}>({kid}, nc, {ne(targs[2])}, {rest});"
+    if api == "api_prop":
+        return f"qlab::api_prop_n<{', '.join(targs)}>({kid}, nc, {rest});"
     raise ValueError(api)
 
 
@@ -333,7 +348,8 @@ def gen_fn_wide(prec):
     src_pc = "F3" if prec == "F" else "D3"
     R = "float" if prec == "F" else "double"
     fns = []
-    for fn in gen_ewise(src_pc, R, prec) + gen_sitefield(src_pc, R, prec):
+    props = [fn for fn in gen_pc(src_pc, R, prec) if fn.family == "prop"]
+    for fn in gen_ewise(src_pc, R, prec) + gen_sitefield(src_pc, R, prec) + props:
         m = re.match(r"QLA_(F3|D3|DF3|FD3)_(.*)$", fn.name)
         lib = {"F3": "FN", "D3": "DN", "DF3": "DFN", "FD3": "FDN"}[m.group(1)]
         params = [("int", "nc")]
@@ -1194,7 +1210,7 @@ def main():
         if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert"):
             extra = '#include "../qla_sitefield.cuh"\n'
         if pc in ("FN", "DN") and (family.startswith("ewise") or family in (
-                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert")):
+                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop")):
             extra = '#include "../qla_ncolor.cuh"\n'
         if pc in ("FN", "DN") and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'

@@ -432,12 +432,51 @@ def ora_multi(r, ms, vs, n, eqop, adja=0, idx_a=None, idx_b=None, gang=None):
 PKIND = {"MP": 0, "PM": 1, "PP": 2, "TRACE": 3}
 
 
-def ora_prop(kind, r, a, b, n, eqop, ca=0, cb=0, idx_a=None, idx_b=None, gang=None):
-    f = getattr(oracle(), "ora_prop_" + rtype(r.dtype))
+def ora_prop(kind, r, a, b, n, eqop, ca=0, cb=0, idx_a=None, idx_b=None, gang=None, nc=3):
+    f = getattr(oracle(), "ora_prop_n_" + rtype(r.dtype))
     idx_a, idx_b, gang = _i32(idx_a), _i32(idx_b), _i32(gang)
-    f(PKIND[kind], ca, cb, EQOPS.get(eqop, eqop), ptr(r), ptr(a), ptr(b), ctypes.c_long(n), ptr(idx_a), ptr(idx_b),
-      ptr(gang))
+    f(nc, PKIND[kind], ca, cb, EQOPS.get(eqop, eqop), ptr(r), ptr(a), ptr(b), ctypes.c_long(n), ptr(idx_a),
+      ptr(idx_b), ptr(gang))
     return r
+
+
+def prop_cases(lib, names, nc, dt, rng, n, ns):
+    """Inputs and oracle results for the propagator entry points `names` of
+    library `lib` (F3 / D3 / FN / DN) at nc colours.  Yields (name, args
+    builder, want) where args(dev, ptrs_a, ptrs_b, gang_dev) gives the C
+    arguments after the leading nc (FN / DN) in host (pointer) or device
+    form, as the caller provides."""
+    import re
+    m = rng.standard_normal((ns, 2 * nc * nc)).astype(dt)
+    p1 = rng.standard_normal((ns, 32 * nc * nc)).astype(dt)
+    p2 = rng.standard_normal((ns, 32 * nc * nc)).astype(dt)
+    r0p = rng.standard_normal((ns, 32 * nc * nc)).astype(dt)
+    r0m = rng.standard_normal((ns, 2 * nc * nc)).astype(dt)
+    ia = rng.integers(0, ns, ns).astype(np.int32)
+    ib = rng.integers(0, ns, ns).astype(np.int32)
+    gang = rng.permutation(n).astype(np.int32)
+    data = {"M": m, "P1": p1, "P2": p2, "ia": ia, "ib": ib, "gang": gang}
+    out = []
+    pre = f"QLA_{lib}_"
+    for name in names:
+        short = name[len(pre):]
+        mt = re.match(r"M_([vx])eq_spintrace_(p?)P$", short)
+        if mt:
+            var, pa = mt.groups()
+            want = r0m[:n].copy()
+            ora_prop("TRACE", want, p1, None, n, "eq", idx_a=ia if pa else None, gang=gang if var == "x" else None,
+                     nc=nc)
+            out.append((name, dict(var=var, a=("P1", bool(pa)), b=None, r0=r0m[:n]), want))
+            continue
+        var, eq, pa, ta, ca, pb, tb, cb = re.match(
+            r"P_([vx])(eq|peq|meq|eqm)_(p?)(M|P)(a?)_times_(p?)(M|P)(a?)$", short).groups()
+        ka = "M" if ta == "M" else "P1"
+        kb = "M" if tb == "M" else "P2"
+        want = r0p[:n].copy()
+        ora_prop(ta + tb, want, data[ka], data[kb], n, eq, ca=int(bool(ca)), cb=int(bool(cb)),
+                 idx_a=ia if pa else None, idx_b=ib if pb else None, gang=gang if var == "x" else None, nc=nc)
+        out.append((name, dict(var=var, a=(ka, bool(pa)), b=(kb, bool(pb)), r0=r0p[:n]), want))
+    return data, out
 
 
 # ---------------------------------------------------------------------------

@@ -184,3 +184,88 @@ def test_fn_unsupported_nc_reports_error(qla):
     code, msg = qla.last_error()
     assert code == 4 and "nc not compiled" in msg
     qla.clear_error()
+
+
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
+@pytest.mark.parametrize("nc", [2, 4])
+def test_fn_fused_hop_terms(qla, nc, lib, dt, rlib):
+    """{H,D}_*_spproj_{M,Ma,pM,pMa}_times_{D,pD}, D_*_sprecon_*_times_{H,pH},
+    D_*_spproj_D and the int32-index forms at nc colours, against the oracle
+    composition in the reference's order, bit for bit."""
+    rng = np.random.default_rng(90 + nc)
+    ns_ = getattr(qla, lib)
+    cb = 2 * np.dtype(dt).itemsize
+    n, ns = 301, 320
+    a = rng.standard_normal((ns, 2 * nc * nc)).astype(dt)
+    d_src = rng.standard_normal((ns, 8 * nc)).astype(dt)
+    h_src = rng.standard_normal((ns, 4 * nc)).astype(dt)
+    r0 = {"H": rng.standard_normal((ns, 4 * nc)).astype(dt), "D": rng.standard_normal((ns, 8 * nc)).astype(dt)}
+    idx = rng.integers(0, ns, ns).astype(np.int32)
+    gang = rng.permutation(n).astype(np.int32)
+    ad, dd, hd = T.to_dev(a), T.to_dev(d_src), T.to_dev(h_src)
+    pa = T.ptr_array(ad, idx, cb * nc * nc)
+    pdd = T.ptr_array(dd, idx, cb * 4 * nc)
+    phd = T.ptr_array(hd, idx, cb * 2 * nc)
+    for (dest, kind), eq, s1, pb, var in itertools.product(
+            [("H", "spproj"), ("D", "spproj"), ("D", "sprecon")], T.EQOPS, ["M", "Ma", "pMa"], [0, 1], ["v", "x"]):
+        src = "D" if kind == "spproj" else "H"
+        bsrc, bdev, bptr = (d_src, dd, pdd) if src == "D" else (h_src, hd, phd)
+        mu, sign = (eq.count("e") + len(s1) + pb) % 5, (1 if var == "v" else -1)
+        r_d = T.to_dev(r0[dest][:n])
+        args = [nc, r_d, pa if s1.startswith("p") else ad, bptr if pb else bdev, mu, sign]
+        if var == "x":
+            args.append(T.to_dev(gang))
+        getattr(ns_, f"{dest}_{var}{eq}_{kind}_{s1}_times_{'p' if pb else ''}{src}")(*args, n)
+        want = r0[dest][:n].copy()
+        aa = a[idx[:n]] if s1.startswith("p") else a[:n]
+        T.ora_hop(want, np.ascontiguousarray(aa), bsrc, n, mu, sign, eq, dest, kind, adja=int(s1.endswith("a")),
+                  idx_b=idx if pb else None, gang=gang if var == "x" else None, nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), (lib, nc, dest, kind, var, eq, s1, pb, mu, sign)
+    for (dest, kind), eq in itertools.product([("H", "spproj"), ("D", "spproj"), ("D", "sprecon")], T.EQOPS):
+        src = "D" if kind == "spproj" else "H"
+        bsrc, bdev = (d_src, dd) if src == "D" else (h_src, hd)
+        r_d = T.to_dev(r0[dest][:n])
+        ns_.__getattr__(f"{dest}_{eq}_{kind}_M_times_x{src}")(nc, r_d, ad, bdev, T.to_dev(idx), 2, -1, n)
+        want = r0[dest][:n].copy()
+        T.ora_hop(want, np.ascontiguousarray(a[:n]), bsrc, n, 2, -1, eq, dest, kind, idx_b=idx, nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), (lib, nc, dest, kind, eq, "xb")
+    for eq, mu in itertools.product(T.EQOPS, range(5)):
+        r_d = T.to_dev(r0["D"][:n])
+        ns_.__getattr__(f"D_v{eq}_spproj_D")(nc, r_d, dd, mu, 1, n)
+        want = r0["D"][:n].copy()
+        T.ora_hop(want, None, d_src, n, mu, 1, eq, "D", "spproj", nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), (lib, nc, "Dspproj", eq, mu)
+
+
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
+@pytest.mark.parametrize("nc", [2, 4])
+def test_fn_propagator_entry_points(qla, nc, lib, dt, rlib):
+    """Every N-colour DiracPropagator product (M P, P M, P P with adjoint /
+    pointer / gang / eqop forms) and spin trace at nc colours, bit-exact."""
+    rng = np.random.default_rng(95 + nc)
+    n, ns = 67, 71
+    names = [e["name"] for e in qla.manifest() if e["pc"] == lib and e["family"] == "prop"]
+    assert len(names) == 388
+    data, cases = T.prop_cases(lib, names, nc, dt, rng, n, ns)
+    cb = 2 * np.dtype(dt).itemsize
+    dev = {k: T.to_dev(data[k]) for k in ("M", "P1", "P2")}
+    rec = {"M": cb * nc * nc, "P1": cb * 16 * nc * nc, "P2": cb * 16 * nc * nc}
+    ptrs_a = {k: T.ptr_array(v, data["ia"], rec[k]) for k, v in dev.items()}
+    ptrs_b = {k: T.ptr_array(v, data["ib"], rec[k]) for k, v in dev.items()}
+    gd = T.to_dev(data["gang"])
+    L = qla.lib()
+    bad = []
+    for name, spec, want in cases:
+        r_d = T.to_dev(spec["r0"])
+        ka, pa = spec["a"]
+        args = [nc, T.ptr_dev(r_d), T.ptr_dev(ptrs_a[ka] if pa else dev[ka])]
+        if spec["b"] is not None:
+            kb, pb = spec["b"]
+            args.append(T.ptr_dev(ptrs_b[kb] if pb else dev[kb]))
+        if spec["var"] == "x":
+            args.append(T.ptr_dev(gd))
+        getattr(L, name)(*args, n)
+        if not T.bits_equal(T.to_host(r_d), want):
+            bad.append(name)
+    qla.check(f"{lib} prop nc={nc}")
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:6]}"

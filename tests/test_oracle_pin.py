@@ -487,3 +487,69 @@ def test_oracle_ncolor_families_match_reference_library(lib):
                 bad.append((e["name"], nc))
     assert count > (150 if lib == "DFN" else 2000)
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("lib,dt", [("FN", np.float32), ("DN", np.float64)])
+def test_oracle_ncolor_hop_terms_match_reference_library(lib, dt):
+    """The fused hop terms of the N-colour libraries (spproj / sprecon with a
+    colour-matrix multiply, every eqop, M and Ma, every mu and sign) at
+    nc = 2 and 4: the oracle composition against the reference, bit for bit."""
+    import itertools
+    R = T.ref()
+    rng = np.random.default_rng(115)
+    n = 11
+    for nc in (2, 4):
+        a = rng.standard_normal((n, 2 * nc * nc)).astype(dt)
+        d = rng.standard_normal((n, 8 * nc)).astype(dt)
+        h = rng.standard_normal((n, 4 * nc)).astype(dt)
+        r0 = {"H": rng.standard_normal((n, 4 * nc)).astype(dt), "D": rng.standard_normal((n, 8 * nc)).astype(dt)}
+        for (dest, kind), eq, s1, (mu, sign) in itertools.product(
+                [("H", "spproj"), ("D", "spproj"), ("D", "sprecon")], T.EQOPS, ["M", "Ma"],
+                [(0, 1), (1, -1), (2, 1), (3, -1), (4, 1), (4, -1)]):
+            src, b = ("D", d) if kind == "spproj" else ("H", h)
+            rr = r0[dest].copy()
+            getattr(R, f"QLA_{lib}_{dest}_v{eq}_{kind}_{s1}_times_{src}")(nc, T.ptr(rr), T.ptr(a), T.ptr(b), mu, sign,
+                                                                          n)
+            want = r0[dest].copy()
+            T.ora_hop(want, a, b, n, mu, sign, eq, dest, kind, adja=int(s1 == "Ma"), nc=nc)
+            assert T.bits_equal(rr, want), (lib, nc, dest, kind, eq, s1, mu, sign)
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("lib,dt", [("FN", np.float32), ("DN", np.float64)])
+def test_oracle_ncolor_propagator_products_match_reference_library(lib, dt):
+    """Every N-colour DiracPropagator product and spin trace entry point at
+    nc = 2 and 4: the oracle against the reference library, bit for bit."""
+    import qla_b200
+    R = T.ref()
+    rng = np.random.default_rng(116)
+    n, ns = 5, 7
+    names = [e["name"] for e in qla_b200.manifest() if e["pc"] == lib and e["family"] == "prop"]
+    assert len(names) == 388
+    for nc in (2, 4):
+        data, cases = T.prop_cases(lib, names, nc, dt, rng, n, ns)
+        cbytes = 2 * np.dtype(dt).itemsize
+        keep = []
+
+        def host_ptrs(key, idx):
+            rec = cbytes * (nc * nc if key == "M" else 16 * nc * nc)
+            arr = data[key]
+            pa = (ctypes.c_void_p * len(idx))(*[arr.ctypes.data + int(j) * rec for j in idx])
+            keep.append(pa)
+            return pa
+
+        bad = []
+        for name, spec, want in cases:
+            r = spec["r0"].copy()
+            ka, pa = spec["a"]
+            args = [nc, T.ptr(r), host_ptrs(ka, data["ia"]) if pa else T.ptr(data[ka])]
+            if spec["b"] is not None:
+                kb, pb = spec["b"]
+                args.append(host_ptrs(kb, data["ib"]) if pb else T.ptr(data[kb]))
+            if spec["var"] == "x":
+                args.append(T.ptr(data["gang"]))
+            getattr(R, name)(*args, n)
+            if not T.bits_equal(r, want):
+                bad.append((name, nc))
+        assert not bad, f"{len(bad)} mismatches, e.g. {bad[:6]}"
