@@ -7106,6 +7106,135 @@ void QLA_DN_P_xeqm_pPa_times_Pa(int nc, void * r, void * a, void * b, int * inde
 void QLA_DN_P_xeqm_pPa_times_pP(int nc, void * r, void * a, void * b, int * index, int n);
 /* replaces QLA_DN_P_xeqm_pPa_times_pPa (lib/perl/build_qla.pl:1588-1661 (DiracPropagator left/right/full products), :942-968 (spin trace)) */
 void QLA_DN_P_xeqm_pPa_times_pPa(int nc, void * r, void * a, void * b, int * index, int n);
+/* ---- multi: replaces the DN functions emitted by lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d) */
+/* replaces QLA_DN_V_veq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veq_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vpeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vpeq_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_vmeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_vmeq_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_veqm_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_veqm_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd);
+/* replaces QLA_DN_V_xeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeq_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xpeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xpeq_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xmeq_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xmeq_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_nM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_nM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_nMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_nMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_npM_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_npM_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_npMa_times_nV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
+/* replaces QLA_DN_V_xeqm_npMa_times_npV (lib/perl/build_qla.pl:1693-1727 (multi-direction sum r = sum_d a_d * b_d)) */
+void QLA_DN_V_xeqm_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd);
 
 #ifdef __cplusplus
 }

@@ -17,8 +17,10 @@
 // div_small (a float-reciprocal quotient with one integer correction, exact
 // for the record sizes here).
 #pragma once
+#include <vector>
 #include "qla_sitefield.cuh"
 #include "qla_prop.cuh"
+#include "qla_multi.cuh"
 
 namespace qlab {
 
@@ -880,6 +882,75 @@ inline void api_prop_n(const char* kid, int nc, void* r, Opnd a, Opnd b, const i
   const long long nel = (KIND == PK_TRACE) ? (long long)nc * nc : 16LL * nc * nc;
   propn_kernel<R, KIND, CA, CB><<<nc_grid((long long)n * nel), 256, 0, current_stream()>>>(p, nc);
   check_launch(kid);
+}
+
+// ---------------------------------------------------------------------------
+// multi-direction sums r (eqop) sum_d A_d b_d at nc colours (build_qla.pl:
+// 1693-1727): one thread per (site, colour row); the row starts from 0
+// (eq, eqm) or r (peq, meq) and takes every direction's products in the
+// reference's order with the eqop's sign, each product and sum rounded.
+struct MultiNParams {
+  Opnd a[kMaxDirs], b[kMaxDirs];
+  void* out;
+  const int* gang;
+  long long n;
+  int nd, nc, minus, out_read;
+};
+
+template <typename R, bool ADJ>
+__global__ void __launch_bounds__(256) multin_kernel(const MultiNParams p) {
+  const int nc = p.nc;
+  for (SiteElemWalk w(nc); w.i < p.n; w.next(nc)) {
+    const long long k = p.gang ? (long long)p.gang[w.i] : w.i;
+    const int ic = w.e;
+    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * nc + ic;
+    Cx<R> y = p.out_read ? *out : Cx<R>{R(0), R(0)};
+    for (int d = 0; d < p.nd; d++) {
+      const Cx<R>* A = rec_ptr<R>(p.a[d], k, nc * nc);
+      const Cx<R>* B = rec_ptr<R>(p.b[d], k, nc);
+      for (int kc = 0; kc < nc; kc++) cmac<ADJ, false>(y, p.minus != 0, A[ADJ ? kc * nc + ic : ic * nc + kc], B[kc]);
+    }
+    *out = y;
+  }
+}
+
+template <typename R, bool ADJ>
+inline void api_multi_n(const char* kid, int nc, void* r, const void* a, bool pa, const void* b, bool pb,
+                        const int* gang, int n, int nd, int eqop) {
+  if (!nc_ok(kid, nc) || n <= 0 || nd <= 0) return;
+  if (!r || !a || !b) {
+    set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+    return;
+  }
+  std::vector<const void*> av((size_t)nd), bv((size_t)nd);
+  if (!multi_fetch_ptrs(a, nd, av.data()) || !multi_fetch_ptrs(b, nd, bv.data())) {
+    check_launch(kid);
+    return;
+  }
+  for (int d = 0; d < nd; d++)
+    if (!av[(size_t)d] || !bv[(size_t)d]) {
+      set_error(QLAGPU_ERR_NULLPTR, kid, "NULL direction operand");
+      return;
+    }
+  for (int d0 = 0; d0 < nd; d0 += kMaxDirs) {
+    MultiNParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.nd = (nd - d0 < kMaxDirs) ? nd - d0 : kMaxDirs;
+    p.nc = nc;
+    p.out = r;
+    p.gang = gang;
+    p.n = n;
+    p.minus = (eqop == MEQ || eqop == EQM) ? 1 : 0;
+    p.out_read = (d0 > 0 || eqop == PEQ || eqop == MEQ) ? 1 : 0;
+    for (int d = 0; d < p.nd; d++) {
+      const void* ad = av[(size_t)(d0 + d)];
+      const void* bd = bv[(size_t)(d0 + d)];
+      p.a[d] = pa ? op_ptr(static_cast<const void* const*>(ad)) : op_contig(ad);
+      p.b[d] = pb ? op_ptr(static_cast<const void* const*>(bd)) : op_contig(bd);
+    }
+    multin_kernel<R, ADJ><<<nc_grid((long long)n * nc), 256, 0, current_stream()>>>(p);
+    if (!check_launch(kid)) return;
+  }
 }
 
 }  // namespace qlab

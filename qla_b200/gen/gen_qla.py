@@ -335,6 +335,8 @@ def _ncolor_body(body):
         return f"qlab::api_convert_n<{targs[0]}, {targs[1]}>({kid}, nc, {ne(targs[2])}, {rest});"
     if api == "api_prop":
         return f"qlab::api_prop_n<{', '.join(targs)}>({kid}, nc, {rest});"
+    if api == "api_multi":
+        return f"qlab::api_multi_n<{', '.join(targs)}>({kid}, nc, {rest});"
     raise ValueError(api)
 
 
@@ -348,7 +350,7 @@ def gen_fn_wide(prec):
     src_pc = "F3" if prec == "F" else "D3"
     R = "float" if prec == "F" else "double"
     fns = []
-    props = [fn for fn in gen_pc(src_pc, R, prec) if fn.family == "prop"]
+    props = [fn for fn in gen_pc(src_pc, R, prec) if fn.family in ("prop", "multi")]
     for fn in gen_ewise(src_pc, R, prec) + gen_sitefield(src_pc, R, prec) + props:
         m = re.match(r"QLA_(F3|D3|DF3|FD3)_(.*)$", fn.name)
         lib = {"F3": "FN", "D3": "DN", "DF3": "DFN", "FD3": "FDN"}[m.group(1)]
@@ -1210,7 +1212,7 @@ def main():
         if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert"):
             extra = '#include "../qla_sitefield.cuh"\n'
         if pc in ("FN", "DN") and (family.startswith("ewise") or family in (
-                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop")):
+                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop", "multi")):
             extra = '#include "../qla_ncolor.cuh"\n'
         if pc in ("FN", "DN") and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'

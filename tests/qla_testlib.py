@@ -418,14 +418,14 @@ def ora_hop(r, a, b, n, mu, sign, eqop, dest, kind, adja=0, idx_b=None, gang=Non
     return r
 
 
-def ora_multi(r, ms, vs, n, eqop, adja=0, idx_a=None, idx_b=None, gang=None):
+def ora_multi(r, ms, vs, n, eqop, adja=0, idx_a=None, idx_b=None, gang=None, nc=3):
     """r (eqop) sum_d A_d b_d with the reference's per-direction rounding
     (build_qla.pl:1693-1727): direction 0 uses the eqop, later directions
     accumulate into the rounded r with the eqop's sign."""
     minus = eqop in ("meq", "eqm")
     for d in range(len(ms)):
         eq_d = eqop if d == 0 else ("meq" if minus else "peq")
-        ora_lmult(r, ms[d], vs[d], n, 1, eq_d, adja=adja, idx_a=idx_a, idx_b=idx_b, gang=gang)
+        ora_lmult(r, ms[d], vs[d], n, 1, eq_d, adja=adja, idx_a=idx_a, idx_b=idx_b, gang=gang, nc=nc)
     return r
 
 

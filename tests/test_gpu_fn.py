@@ -269,3 +269,52 @@ def test_fn_propagator_entry_points(qla, nc, lib, dt, rlib):
             bad.append(name)
     qla.check(f"{lib} prop nc={nc}")
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:6]}"
+
+
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
+@pytest.mark.parametrize("nc,nd", [(2, 3), (4, 11)])
+def test_fn_multi_direction_sum(qla, nc, nd, lib, dt, rlib):
+    """V_{v,x}{eqop}_n{p}M{a}_times_n{p}V at nc colours: the reference's
+    per-direction rounding, nd = 11 in two launches, operand tables on the
+    host and on the device, bit for bit."""
+    import ctypes
+    rng = np.random.default_rng(97 + nc)
+    cb = 2 * np.dtype(dt).itemsize
+    n, ns = 203, 220
+    ms = [rng.standard_normal((ns, 2 * nc * nc)).astype(dt) for _ in range(nd)]
+    vs = [rng.standard_normal((ns, 2 * nc)).astype(dt) for _ in range(nd)]
+    r0 = rng.standard_normal((n, 2 * nc)).astype(dt)
+    ia = rng.integers(0, ns, ns).astype(np.int32)
+    ib = rng.integers(0, ns, ns).astype(np.int32)
+    gang = rng.permutation(n).astype(np.int32)
+    md = [T.to_dev(m) for m in ms]
+    vd = [T.to_dev(v) for v in vs]
+    pms = [T.ptr_array(m, ia, cb * nc * nc) for m in md]
+    pvs = [T.ptr_array(v, ib, cb * nc) for v in vd]
+    L = qla.lib()
+
+    def table(ts, on_dev):
+        addrs = np.array([t.data_ptr() for t in ts], dtype=np.int64)
+        if on_dev:
+            d = T.to_dev(addrs)
+            return d, d.data_ptr()
+        return addrs, addrs.ctypes.data
+
+    gd = T.to_dev(gang)
+    for var, eq, s1, s2 in itertools.product(["v", "x"], T.EQOPS, ["nM", "nMa", "npMa"], ["nV", "npV"]):
+        on_dev = (eq in ("peq", "eqm"))
+        keep_a, a_addr = table(pms if "p" in s1 else md, on_dev)
+        keep_b, b_addr = table(pvs if "p" in s2 else vd, not on_dev)
+        r_d = T.to_dev(r0)
+        fn = getattr(L, f"QLA_{lib}_V_{var}{eq}_{s1}_times_{s2}")
+        fn.restype = None
+        args = [ctypes.c_int(nc), ctypes.c_void_p(r_d.data_ptr()), ctypes.c_void_p(a_addr), ctypes.c_void_p(b_addr)]
+        if var == "x":
+            args.append(ctypes.c_void_p(gd.data_ptr()))
+        fn(*args, ctypes.c_int(n), ctypes.c_int(nd))
+        qla.check(fn.__name__)
+        want = r0.copy()
+        T.ora_multi(want, ms, vs, n, eq, adja=int(s1.endswith("a")), idx_a=ia if "p" in s1 else None,
+                    idx_b=ib if "p" in s2 else None, gang=gang if var == "x" else None, nc=nc)
+        assert T.bits_equal(T.to_host(r_d), want), (lib, nc, var, eq, s1, s2, nd)
+        del keep_a, keep_b

@@ -553,3 +553,26 @@ def test_oracle_ncolor_propagator_products_match_reference_library(lib, dt):
             if not T.bits_equal(r, want):
                 bad.append((name, nc))
         assert not bad, f"{len(bad)} mismatches, e.g. {bad[:6]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("lib,dt", [("FN", np.float32), ("DN", np.float64)])
+def test_oracle_ncolor_multi_direction_sums_match_reference_library(lib, dt):
+    """QLA_FN_ / QLA_DN_ V_*_n{p}M{a}_times_n{p}V at nc = 2 and 4 with nd = 3:
+    the oracle's per-direction composition against the reference, bit for bit."""
+    import itertools
+    R = T.ref()
+    rng = np.random.default_rng(117)
+    n, nd = 9, 3
+    for nc in (2, 4):
+        ms = [rng.standard_normal((n, 2 * nc * nc)).astype(dt) for _ in range(nd)]
+        vs = [rng.standard_normal((n, 2 * nc)).astype(dt) for _ in range(nd)]
+        r0 = rng.standard_normal((n, 2 * nc)).astype(dt)
+        ta = (ctypes.c_void_p * nd)(*[m.ctypes.data for m in ms])
+        tb = (ctypes.c_void_p * nd)(*[v.ctypes.data for v in vs])
+        for eq, s1 in itertools.product(T.EQOPS, ["nM", "nMa"]):
+            rr = r0.copy()
+            getattr(R, f"QLA_{lib}_V_v{eq}_{s1}_times_nV")(nc, T.ptr(rr), ta, tb, n, nd)
+            want = r0.copy()
+            T.ora_multi(want, ms, vs, n, eq, adja=int(s1 == "nMa"), nc=nc)
+            assert T.bits_equal(rr, want), (lib, nc, eq, s1)
