@@ -5784,6 +5784,11 @@ void QLA_FN_V_vmeq_v(int nc, void * r, void * a, int n);
 void QLA_FN_V_veqm_v(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_V_veq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_V_veq_zero(int nc, void * r, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_V_veq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_V_veq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_FN_V_veq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_V_veq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_V_veq_V_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_V_veq_V_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int n);
@@ -5804,6 +5809,11 @@ void QLA_FN_H_vmeq_h(int nc, void * r, void * a, int n);
 void QLA_FN_H_veqm_h(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_H_veq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_H_veq_zero(int nc, void * r, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_H_veq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_H_veq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_FN_H_veq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_H_veq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_H_veq_H_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_H_veq_H_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int n);
@@ -5824,6 +5834,11 @@ void QLA_FN_D_vmeq_d(int nc, void * r, void * a, int n);
 void QLA_FN_D_veqm_d(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_D_veq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_D_veq_zero(int nc, void * r, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_D_veq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_D_veq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_FN_D_veq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_D_veq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_D_veq_D_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_D_veq_D_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int n);
@@ -5844,6 +5859,11 @@ void QLA_FN_M_vmeq_m(int nc, void * r, void * a, int n);
 void QLA_FN_M_veqm_m(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_M_veq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_M_veq_zero(int nc, void * r, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_M_veq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_M_veq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_FN_M_veq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_M_veq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_M_veq_M_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_M_veq_M_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int n);
@@ -5864,6 +5884,11 @@ void QLA_FN_P_vmeq_p(int nc, void * r, void * a, int n);
 void QLA_FN_P_veqm_p(int nc, void * r, void * a, int n);
 /* replaces QLA_FN_P_veq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_P_veq_zero(int nc, void * r, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_P_veq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_P_veq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_FN_P_veq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_P_veq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_P_veq_P_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_P_veq_P_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int n);
@@ -6062,6 +6087,11 @@ void QLA_FN_V_xmeq_v(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_V_xeqm_v(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_V_xeq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_V_xeq_zero(int nc, void * r, int * index, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_V_xeq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_V_xeq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_FN_V_xeq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_V_xeq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int * index, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_V_xeq_V_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_V_xeq_V_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);
@@ -6082,6 +6112,11 @@ void QLA_FN_H_xmeq_h(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_H_xeqm_h(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_H_xeq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_H_xeq_zero(int nc, void * r, int * index, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_H_xeq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_H_xeq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_FN_H_xeq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_H_xeq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int * index, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_H_xeq_H_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_H_xeq_H_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);
@@ -6102,6 +6137,11 @@ void QLA_FN_D_xmeq_d(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_D_xeqm_d(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_D_xeq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_D_xeq_zero(int nc, void * r, int * index, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_D_xeq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_D_xeq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_FN_D_xeq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_D_xeq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int * index, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_D_xeq_D_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_D_xeq_D_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);
@@ -6122,6 +6162,11 @@ void QLA_FN_M_xmeq_m(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_M_xeqm_m(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_M_xeq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_M_xeq_zero(int nc, void * r, int * index, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_M_xeq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_M_xeq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_FN_M_xeq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_M_xeq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int * index, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_M_xeq_M_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_M_xeq_M_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);
@@ -6142,6 +6187,11 @@ void QLA_FN_P_xmeq_p(int nc, void * r, void * a, int * index, int n);
 void QLA_FN_P_xeqm_p(int nc, void * r, void * a, int * index, int n);
 /* replaces QLA_FN_P_xeq_zero (lib/perl/build_qla.pl:2561-2618 (zero fills, constant fills, diagonal fill of a colour matrix), make_code_unary.pl (identity, diagfill, zero)) */
 void QLA_FN_P_xeq_zero(int nc, void * r, int * index, int n);
+/* ---- random: replaces the FN functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_FN_P_xeq_gaussian_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_P_xeq_gaussian_S(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_FN_P_xeq_gaussian_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_FN_P_xeq_gaussian_pS(int nc, void * r, QLA_RandomState *QLA_B200_RESTRICT * a, int * index, int n);
 /* ---- mask: replaces the FN functions emitted by lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero) */
 /* replaces QLA_FN_P_xeq_P_mask_I (lib/perl/build_qla.pl:2058-2084 (copymask: r = a where the integer mask is non-zero)) */
 void QLA_FN_P_xeq_P_mask_I(int nc, void * r, void * a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);

@@ -495,6 +495,39 @@ void QLA_I_xeq_i_times_pI_minus_pI(QLA_Int *QLA_B200_RESTRICT r, QLA_Int *QLA_B2
 void QLA_I_xeq_not_pI(QLA_Int *QLA_B200_RESTRICT r, QLA_Int *QLA_B200_RESTRICT * a, int * index, int n);
 /* replaces QLA_I_xeq_zero (lib/perl/build_qla.pl:1932-2082 (integer fields)) */
 void QLA_I_xeq_zero(QLA_Int *QLA_B200_RESTRICT r, int * index, int n);
+/* ---- random: replaces the I functions emitted by lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills */
+/* replaces QLA_S_veq_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_S(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_S_veq_S_mask_I (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_S_mask_I(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT a, QLA_Int *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_S_veq_S_mask_pI (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_S_mask_pI(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT a, QLA_Int *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_S_veq_seed_i_I (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_seed_i_I(QLA_RandomState *QLA_B200_RESTRICT r, int seed, QLA_Int *QLA_B200_RESTRICT a, int n);
+/* replaces QLA_S_veq_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_pS(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_S_veq_pS_mask_I (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_pS_mask_I(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT * a, QLA_Int *QLA_B200_RESTRICT b, int n);
+/* replaces QLA_S_veq_pS_mask_pI (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_pS_mask_pI(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT * a, QLA_Int *QLA_B200_RESTRICT * b, int n);
+/* replaces QLA_S_veq_seed_i_pI (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_veq_seed_i_pI(QLA_RandomState *QLA_B200_RESTRICT r, int seed, QLA_Int *QLA_B200_RESTRICT * a, int n);
+/* replaces QLA_S_xeq_S (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_S(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_S_xeq_S_mask_I (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_S_mask_I(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_S_xeq_S_mask_pI (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_S_mask_pI(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT a, QLA_Int *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_S_xeq_seed_i_I (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_seed_i_I(QLA_RandomState *QLA_B200_RESTRICT r, int seed, QLA_Int *QLA_B200_RESTRICT a, int * index, int n);
+/* replaces QLA_S_xeq_pS (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_pS(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT * a, int * index, int n);
+/* replaces QLA_S_xeq_pS_mask_I (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_pS_mask_I(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT * a, QLA_Int *QLA_B200_RESTRICT b, int * index, int n);
+/* replaces QLA_S_xeq_pS_mask_pI (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_pS_mask_pI(QLA_RandomState *QLA_B200_RESTRICT r, QLA_RandomState *QLA_B200_RESTRICT * a, QLA_Int *QLA_B200_RESTRICT * b, int * index, int n);
+/* replaces QLA_S_xeq_seed_i_pI (lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36) */
+void QLA_S_xeq_seed_i_pI(QLA_RandomState *QLA_B200_RESTRICT r, int seed, QLA_Int *QLA_B200_RESTRICT * a, int * index, int n);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,33 @@ typedef QLA_D_Complex QLA_D3_ColorMatrix[3][3];
 typedef QLA_D_Complex QLA_D3_DiracPropagator[3][4][3][4];
 #endif /* _QLA_TYPES_H */
 
+/* per-site random-number generator state (include/qla_random.h:8-14): seven
+ * feedback-shift-register words, the congruential multiplier, addend and
+ * state, and a float scale; QLA_gaussian's MILC variant keeps its spare
+ * deviate in `addend` / `scale` */
+#ifndef _QLA_RANDOM_H
+#define _QLA_RANDOM_H
+typedef struct {
+  unsigned int r0, r1, r2, r3, r4, r5, r6;
+  unsigned int multiplier, addend, ic_state;
+  float scale;
+} QLA_RandomState;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* host functions on one state in host memory (lib/random/QLA_random.c,
+ * QLA_gaussian.c, QLA_seed_random.c), with the same results */
+QLA_F_Real QLA_random(QLA_RandomState *prn_pt);
+QLA_F_Real QLA_gaussian(QLA_RandomState *prn_pt);
+void QLA_seed_random(QLA_RandomState *prn_pt, int seed, QLA_Int index);
+/* non-zero: QLA_gaussian and the gaussian fills use MILC's polar method */
+extern int QLA_use_milc_gaussian;
+#ifdef __cplusplus
+}
+#endif
+#endif /* _QLA_RANDOM_H */
+
 /* QLA_FN / QLA_DN take the colour count at run time (include/qla_types.h:193-239,
  * C99 variable-length types); their arrays are passed as untyped pointers to
  * records of nc*nc (matrix) or nc (vector) complex numbers. */

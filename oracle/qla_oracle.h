@@ -122,6 +122,16 @@ ORA_NCOLOR_DECL(double, d)
 void ora_convert_df(double *r, const float *a, long n, int nr, const int *idx_a, const int *gang);
 void ora_convert_fd(float *r, const double *a, long n, int nr, const int *idx_a, const int *gang);
 
+/* the per-site random-number generator (state: 11 32-bit words) */
+float ora_rng_uniform(void *state);
+float ora_rng_gaussian(void *state, int milc);
+void ora_rng_seed(void *state, int seed, int index);
+void ora_rng_fill_f(int nreal, int gauss, int milc, float *r, void *s, long n, const int *idx_s, const int *gang);
+void ora_rng_fill_d(int nreal, int gauss, int milc, double *r, void *s, long n, const int *idx_s, const int *gang);
+void ora_rng_seedfield(void *r, int seed, const int *a, long n, const int *idx_a, const int *gang);
+void ora_rng_copy(void *r, const void *a, const int *mask, long n, const int *idx_a, const int *idx_m,
+                  const int *gang);
+
 int ora_version(void);
 
 #endif

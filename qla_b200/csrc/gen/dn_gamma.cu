@@ -3,6 +3,7 @@
 #include "../../../include/qla_b200_types.h"
 #include "../qla_api.cuh"
 #include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_D_veq_gamma_times_D(int nc, void * r, void * a, int mu, int n) {

@@ -3,6 +3,7 @@
 #include "../../../include/qla_b200_types.h"
 #include "../qla_api.cuh"
 #include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_C_veq_elem_V(int nc, QLA_F_Complex *__restrict__ r, void * a, int i_c, int n) {

@@ -3,6 +3,7 @@
 #include "../../../include/qla_b200_types.h"
 #include "../qla_api.cuh"
 #include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_P_veq_c_times_P(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {

@@ -3,6 +3,7 @@
 #include "../../../include/qla_b200_types.h"
 #include "../qla_api.cuh"
 #include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_V_veq_v(int nc, void * r, void * a, int n) {

@@ -22,6 +22,7 @@ enum : unsigned {
   QLA_DEVERR_BULK_TIMEOUT = 2u,   // draining in-flight bulk copies gave up
   QLA_DEVERR_BAD_INDEX = 4u,      // an index stream entry was out of range
   QLA_DEVERR_MFUNC_NOCONV = 8u,   // an iterative matrix function hit its cap
+  QLA_DEVERR_RNG = 16u,           // the polar gaussian's rejection loop hit its cap
 };
 
 // The error word lives in device memory owned by the runtime (one per

@@ -22,6 +22,7 @@
 // results are bit-identical.  Local dot products run one thread per site and
 // accumulate in FP64 like the reference's QLA_D temporaries.
 #pragma once
+#include "qla_api.cuh"
 #include "qla_launch.cuh"
 #include "qla_ops.cuh"
 

@@ -84,6 +84,8 @@ CITE["trace"] = "lib/perl/build_qla.pl:933-1064 (trace, real / imaginary trace, 
 CITE["gred"] = ("lib/perl/build_qla.pl:2089-2272 (global norm2 and inner products of DiracPropagators, "
                 "trace of the adjoint-form products Ma.M and Pa.P)")
 CITE["gsum"] = "lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)"
+CITE["random"] = ("lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), "
+                  "lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36")
 CITE["convert"] = ("lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, "
                    "QLA_FD_c_eq_c rounding)")
 CITE["reunit"] = ("no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of "
@@ -335,6 +337,8 @@ def _ncolor_body(body):
         return f"qlab::api_convert_n<{targs[0]}, {targs[1]}>({kid}, nc, {ne(targs[2])}, {rest});"
     if api == "api_prop":
         return f"qlab::api_prop_n<{', '.join(targs)}>({kid}, nc, {rest});"
+    if api == "api_rng_fill":
+        return f"qlab::api_rng_fill_n<{targs[0]}>({kid}, nc, {ne(targs[1])}, {rest});"
     if api == "api_multi":
         return f"qlab::api_multi_n<{', '.join(targs)}>({kid}, nc, {rest});"
     raise ValueError(api)
@@ -411,6 +415,51 @@ def gen_int():
                          "IC_S_TIMES_MINUS", [("b", xa), ("c", xb)], True)
             emit(f"not_{pa}I", var, "eq", "IC_NOT", [("a", xa)], False)
         emit("zero", var, "eq", "IC_ZERO", [], False)
+    # random-number state fields: copies, masked copies, seeding
+    kid_s = '"S_state"'
+    for var in ["v", "x"]:
+        tail = [("int *", "index")] if var == "x" else []
+        gang = "index" if var == "x" else "nullptr"
+        for pa, xa in P:
+            sa = ("QLA_RandomState *RESTRICT *" if xa else "QLA_RandomState *RESTRICT", "a")
+            oa = "qlab::op_ptr((const void* const*)a)" if xa else "qlab::op_contig(a)"
+            fns.append(Fn(f"QLA_S_{var}eq_{pa}S", [("QLA_RandomState *RESTRICT", "r"), sa] + tail + [("int", "n")],
+                          f"qlab::api_rng_copy({kid_s}, r, {oa}, qlab::Opnd{{}}, false, {gang}, n);", "random",
+                          CITE["random"], dict(dest="S", eqop="eq", var=var, op="copy", a=pa + "S")))
+            for pm, xm in P:
+                sm = ("QLA_Int *RESTRICT *" if xm else "QLA_Int *RESTRICT", "b")
+                om = "qlab::op_ptr((const void* const*)b)" if xm else "qlab::op_contig(b)"
+                fns.append(Fn(f"QLA_S_{var}eq_{pa}S_mask_{pm}I",
+                              [("QLA_RandomState *RESTRICT", "r"), sa, sm] + tail + [("int", "n")],
+                              f"qlab::api_rng_copy({kid_s}, r, {oa}, {om}, true, {gang}, n);", "random",
+                              CITE["random"], dict(dest="S", eqop="eq", var=var, op="mask", a=pa + "S", b=pm + "I")))
+            si = ("QLA_Int *RESTRICT *" if xa else "QLA_Int *RESTRICT", "a")
+            fns.append(Fn(f"QLA_S_{var}eq_seed_i_{pa}I",
+                          [("QLA_RandomState *RESTRICT", "r"), ("int", "seed"), si] + tail + [("int", "n")],
+                          f"qlab::api_rng_seed({kid_s}, r, seed, {oa}, {gang}, n);", "random", CITE["random"],
+                          dict(dest="S", eqop="eq", var=var, op="seed", a=pa + "I")))
+    return fns
+
+
+def gen_fd(prec):
+    """QLA_F_ / QLA_D_ (real and complex fields): uniform and gaussian random
+    fills."""
+    fns = []
+    R = "float" if prec == "F" else "double"
+    kid = f'"{prec}_random"'
+    for var in ["v", "x"]:
+        tail = [("int *", "index")] if var == "x" else []
+        gang = "index" if var == "x" else "nullptr"
+        for ps, xs in (("", False), ("p", True)):
+            sa = ("QLA_RandomState *RESTRICT *" if xs else "QLA_RandomState *RESTRICT", "a")
+            oa = "qlab::op_ptr((const void* const*)a)" if xs else "qlab::op_contig(a)"
+            for dest, what in (("R", "random"), ("R", "gaussian"), ("C", "gaussian")):
+                rt = f"QLA_{prec}_{'Real' if dest == 'R' else 'Complex'} *RESTRICT"
+                name = f"QLA_{prec}_{dest}_{var}eq_{what}_{ps}S"
+                body = (f"qlab::api_rng_fill<{R}, 1, {str(dest == 'R').lower()}>({kid}, {int(what == 'gaussian')}, r, "
+                        f"{oa}, {gang}, n);")
+                fns.append(Fn(name, [(rt, "r"), sa] + tail + [("int", "n")], body, "random", CITE["random"],
+                              dict(dest=dest, eqop="eq", var=var, op=what, a=ps + "S")))
     return fns
 
 
@@ -945,6 +994,14 @@ def gen_sitefield(pc, R, P):
             params = [(rt, "r")] + tail + [("int", "n")]
             emit(name, params, f"qlab::api_zero<{R}, {ne}>({kid('fill')}, r, {gang}, n);", "fill",
                  dict(dest=T, eqop="eq", var=var, op="zero"))
+            # gaussian random fills from a field of generator states
+            for ps, xs in (("", False), ("p", True)):
+                sa = ("QLA_RandomState *RESTRICT *" if xs else "QLA_RandomState *RESTRICT", "a")
+                oa = "qlab::op_ptr((const void* const*)a)" if xs else "qlab::op_contig(a)"
+                name = f"QLA_{pc}_{T}_{var}eq_gaussian_{ps}S"
+                body = f"qlab::api_rng_fill<{R}, {ne}, false>({kid('random')}, 1, r, {oa}, {gang}, n);"
+                emit(name, [(rt, "r"), sa] + tail + [("int", "n")], body, "random",
+                     dict(dest=T, eqop="eq", var=var, op="gaussian", a=ps + "S"))
             # ---- copymask
             for pa_, pm_ in itertools.product((False, True), (False, True)):
                 pa, oa = src_param(T, pa_)
@@ -1175,12 +1232,13 @@ def main():
     groups = {}
     headers = {}
     for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None),
-                     ("DN", None, None)]:
+                     ("DN", None, None), ("F", None, None), ("D", None, None)]:
         for fn in (gen_int() if pc == "I" else gen_fn("F") + gen_fn_wide("F") if pc == "FN"
-                   else gen_fn("D") + gen_fn_wide("D") if pc == "DN" else gen_pc(pc, R, P)):
+                   else gen_fn("D") + gen_fn_wide("D") if pc == "DN" else gen_fd(pc) if pc in ("F", "D")
+                   else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
-            # the reference declares QLA_FD3_ in qla_df3.h, QLA_FDN_ in qla_dfn.h
-            hpc = {"FD3": "DF3", "FDN": "DFN"}.get(hpc, hpc)
+            # the reference declares QLA_FD3_ in qla_df3.h, QLA_FDN_ in qla_dfn.h, QLA_S_ in qla_int.h
+            hpc = {"FD3": "DF3", "FDN": "DFN", "S": "I"}.get(hpc, hpc)
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
             manifest.append(dict(name=fn.name, pc=hpc, family=fn.family, params=[n for _, n in fn.params],
@@ -1211,9 +1269,12 @@ def main():
             extra = '#include "../qla_ewise.cuh"\n'
         if family in ("fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert"):
             extra = '#include "../qla_sitefield.cuh"\n'
+        if family == "random":
+            extra = '#include "../qla_random.cuh"\n'
         if pc in ("FN", "DN") and (family.startswith("ewise") or family in (
-                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop", "multi")):
-            extra = '#include "../qla_ncolor.cuh"\n'
+                "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop", "multi",
+                "random")):
+            extra = '#include "../qla_ncolor.cuh"\n#include "../qla_random.cuh"\n'
         if pc in ("FN", "DN") and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
         if pc in ("FN", "DN") and family == "mfunc_ext":

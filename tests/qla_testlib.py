@@ -488,7 +488,7 @@ EW_SHAPES = {"COPY": 0, "CONJ": 1, "I": 2, "CT": 3, "CTA": 4, "CAT": 5, "CATA": 
 LD_KINDS = {"LD_DOT": 0, "LD_DOT_AA": 1, "LD_ADOT": 2, "LD_REDOT": 3, "LD_NORM2": 4}
 NE3 = {"V": 3, "H": 6, "D": 12, "M": 9, "P": 144}
 _TYPE_OF = {"ColorVector": "V", "HalfFermion": "H", "DiracFermion": "D", "ColorMatrix": "M",
-            "DiracPropagator": "P", "Complex": "C", "Real": "R", "QLA_Int": "I"}
+            "DiracPropagator": "P", "Complex": "C", "Real": "R", "QLA_Int": "I", "QLA_RandomState": "S"}
 
 
 def param_type(ctype):
@@ -637,6 +637,8 @@ def rec_bytes(letter, dt, nc=3):
     """bytes per record of a field of the given letter in precision dt"""
     if letter == "I":
         return 4
+    if letter == "S":
+        return 44
     return np.dtype(dt).itemsize * (1 if letter == "R" else 2 * ne_at(letter, nc))
 
 
@@ -800,3 +802,68 @@ def convert_oracle(e, ins, idx, gang, n, nc=3):
     f(ptr(r), ptr(ins["a"][2]), ctypes.c_long(len(gang) if gang is not None else n), 2 * ne_at(e["dest"], nc),
       ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
     return r
+
+
+# ---------------------------------------------------------------------------
+# random-number generator state fields (QLA_RandomState: 11 32-bit words)
+
+def rng_states(rng, ns):
+    """ns seeded generator states (QLA_seed_random with varied seeds and
+    indices), each advanced by a few draws."""
+    st = np.zeros((ns, 11), np.uint32)
+    O = oracle()
+    for k in range(ns):
+        row = st[k]
+        O.ora_rng_seed(ptr(row), int(rng.integers(-2**31, 2**31 - 1)), int(rng.integers(0, 1 << 20)))
+        for _ in range(int(rng.integers(0, 5))):
+            O.ora_rng_uniform(ptr(row))
+    return st
+
+
+def random_case(e, rng, n, ns, nc=3, milc=0):
+    """Inputs and the oracle's results for a random-family entry e (a
+    fixed-colour, F / D or S entry): (ins, idx, gang, ints, want_r, want_states)
+    where ins maps parameter -> (letter, pointer?, array) as ewise_inputs and
+    want_states is the state field after the call (None when not written)."""
+    O = oracle()
+    op = e["op"]
+    gang = rng.permutation(n)[: n // 2 + 1].astype(np.int32) if e["var"] == "x" else None
+    nsites = ctypes.c_long(len(gang) if gang is not None else n)
+    idx, ins, ints = {}, {}, {}
+    if op in ("gaussian", "random"):
+        dt = np.float64 if e["pc"] in ("D3", "D", "DN") else np.float32
+        nreal = 1 if e["dest"] == "R" else (2 if e["dest"] == "C" else 2 * ne_at(e["dest"], nc))
+        r = rng.standard_normal((n, nreal)).astype(dt)
+        st = rng_states(rng, ns)
+        ptr_s = e["a"].startswith("p")
+        ins = {"r": (e["dest"], False, r), "a": ("S", ptr_s, st)}
+        if ptr_s:
+            idx["a"] = rng.permutation(ns)[:n].astype(np.int32)
+        want_r, want_s = r.copy(), st.copy()
+        getattr(O, "ora_rng_fill_" + rtype(dt))(nreal, int(op == "gaussian"), milc, ptr(want_r), ptr(want_s),
+                                                nsites, ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
+        return ins, idx, gang, ints, want_r, want_s
+    r = rng_states(rng, n)
+    ins["r"] = ("S", False, r)
+    want = r.copy()
+    if op == "seed":
+        a = rng.integers(0, 1 << 20, ns).astype(np.int32)
+        ins["a"] = ("I", e["a"].startswith("p"), a)
+        if e["a"].startswith("p"):
+            idx["a"] = rng.integers(0, ns, n).astype(np.int32)
+        ints["seed"] = int(rng.integers(-2**31, 2**31 - 1))
+        O.ora_rng_seedfield(ptr(want), ints["seed"], ptr(a), nsites, ptr(_i32(idx.get("a"))), ptr(_i32(gang)))
+        return ins, idx, gang, ints, want, None
+    a = rng_states(rng, ns)
+    ins["a"] = ("S", e["a"].startswith("p"), a)
+    if e["a"].startswith("p"):
+        idx["a"] = rng.integers(0, ns, n).astype(np.int32)
+    m = None
+    if op == "mask":
+        m = rng.choice(np.array([0, 1, -2, 0], np.int32), ns)
+        ins["b"] = ("I", e["b"].startswith("p"), m)
+        if e["b"].startswith("p"):
+            idx["b"] = rng.integers(0, ns, n).astype(np.int32)
+    O.ora_rng_copy(ptr(want), ptr(a), ptr(m), nsites, ptr(_i32(idx.get("a"))), ptr(_i32(idx.get("b"))),
+                   ptr(_i32(gang)))
+    return ins, idx, gang, ints, want, None

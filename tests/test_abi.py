@@ -66,7 +66,9 @@ def test_manifest_matches_exports():
     import qla_b200
     names = {e["name"] for e in qla_b200.manifest()}
     syms = declared_symbols()
-    assert {s for s in names if s.startswith("QLA_")} == {s for s in syms if s.startswith("QLA_")}
+    # the host functions on one random-number state are hand-written, not generated
+    host_api = {"QLA_seed_random", "QLA_random", "QLA_gaussian"}
+    assert {s for s in names if s.startswith("QLA_")} == {s for s in syms if s.startswith("QLA_")} - host_api
     assert names <= set(syms)
 
 

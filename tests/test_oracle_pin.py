@@ -237,8 +237,8 @@ def test_prototypes_match_reference_headers():
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
         for m in re.finditer(r"void (QLA_(?:D?FN|DN|FDN)_\w+) \((.*?)\);", txt):
             # VLA record types: compare the parameter count (the first is int nc)
-            nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)|\bQLA_Int\b", m.group(2)))
-    for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h"):
+            nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)|\bQLA_Int\b|\bQLA_RandomState\b", m.group(2)))
+    for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h", "qla_f.h", "qla_d.h", "qla_df.h"):
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
         for m in re.finditer(r"void (QLA_\w+) \((.*?)\);", txt):
             params = [p.replace("QLA_RESTRICT", "").strip() for p in m.group(2).split(",")]
@@ -576,3 +576,79 @@ def test_oracle_ncolor_multi_direction_sums_match_reference_library(lib, dt):
             want = r0.copy()
             T.ora_multi(want, ms, vs, n, eq, adja=int(s1 == "nMa"), nc=nc)
             assert T.bits_equal(rr, want), (lib, nc, eq, s1)
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("milc", [0, 1])
+def test_oracle_random_generator_matches_reference_library(milc):
+    """QLA_seed_random, QLA_random and QLA_gaussian (Box-Muller, and MILC's
+    polar method with the switch set): the oracle against the reference's
+    lib/random, value and state bit for bit over many draws."""
+    R = T.ref()
+    O = T.oracle()
+    R.QLA_random.restype = ctypes.c_float
+    R.QLA_gaussian.restype = ctypes.c_float
+    O.ora_rng_uniform.restype = ctypes.c_float
+    O.ora_rng_gaussian.restype = ctypes.c_float
+    flag = ctypes.c_int.in_dll(R, "QLA_use_milc_gaussian")
+    flag.value = milc
+    try:
+        rng = np.random.default_rng(118)
+        for _ in range(40):
+            seed, index = int(rng.integers(-2**31, 2**31 - 1)), int(rng.integers(0, 1 << 22))
+            a = np.zeros(11, np.uint32)
+            b = np.zeros(11, np.uint32)
+            R.QLA_seed_random(T.ptr(a), seed, index)
+            O.ora_rng_seed(T.ptr(b), seed, index)
+            assert T.bits_equal(a, b)
+            for j in range(300):
+                if j % 3 == 0:
+                    x, y = R.QLA_random(T.ptr(a)), O.ora_rng_uniform(T.ptr(b))
+                else:
+                    x, y = R.QLA_gaussian(T.ptr(a)), O.ora_rng_gaussian(T.ptr(b), milc)
+                assert np.float32(x).tobytes() == np.float32(y).tobytes()
+            assert T.bits_equal(a, b)
+    finally:
+        flag.value = 0
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("milc", [0, 1])
+def test_oracle_random_fills_match_reference_library(milc):
+    """Every uniform / gaussian fill, seeding and state copy entry point of
+    the F3, D3, F, D, integer and (nc = 2) N-colour libraries: the oracle
+    against the reference library, values and states bit for bit."""
+    import qla_b200
+    man = qla_b200.manifest()
+    byname = {e["name"]: e for e in man}
+    R = T.ref()
+    flag = ctypes.c_int.in_dll(R, "QLA_use_milc_gaussian")
+    flag.value = milc
+    rng = np.random.default_rng(119)
+    n, ns = 7, 9
+    bad, count = [], 0
+    try:
+        for e in man:
+            if e["family"] != "random":
+                continue
+            nc, lead = 3, []
+            twin = e
+            if e["pc"] in ("FN", "DN"):
+                twin, nc, lead = byname[T.fixed_colour_twin(e["name"])], 2, [2]
+            if milc and twin.get("op") != "gaussian":
+                continue
+            ins, idx, gang, ints, want_r, want_s = T.random_case(twin, rng, n, ns, nc=nc, milc=milc)
+            r = ins["r"][2].copy()
+            st = ins["a"][2].copy() if ins["a"][0] == "S" else None
+            if st is not None:
+                ins = dict(ins, a=("S", ins["a"][1], st))
+            args, keep = _ref_args(twin, ins, idx, gang, n, r, ints, nc=nc)
+            getattr(R, e["name"])(*(lead + args))
+            count += 1
+            ok = T.bits_equal(r, want_r) and (want_s is None or T.bits_equal(st, want_s))
+            if not ok:
+                bad.append(e["name"])
+    finally:
+        flag.value = 0
+    assert count >= (88 if milc else 120)
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
