@@ -132,6 +132,18 @@ void ora_rng_seedfield(void *r, int seed, const int *a, long n, const int *idx_a
 void ora_rng_copy(void *r, const void *a, const int *mask, long n, const int *idx_a, const int *idx_m,
                   const int *gang);
 
+/* QLA_F_ / QLA_D_ real, complex and integer fields (op codes as the
+ * product's ScalarOp) and the reference-order global sums of real / integer
+ * fields (kind 0 dot, 1 norm2, 2 sum) */
+void ora_scalar_f(int op, int eqop, void *r, const void *a, const void *b, const void *c, float s, long n,
+                  const int *ia, const int *ib, const int *ic, const int *gang);
+void ora_scalar_d(int op, int eqop, void *r, const void *a, const void *b, const void *c, double s, long n,
+                  const int *ia, const int *ib, const int *ic, const int *gang);
+double ora_sred_f(int kind, int isint, const void *a, const void *b, long n, const int *ia, const int *ib,
+                  const int *gang);
+double ora_sred_d(int kind, int isint, const void *a, const void *b, long n, const int *ia, const int *ib,
+                  const int *gang);
+
 int ora_version(void);
 
 #endif

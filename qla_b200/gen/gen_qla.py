@@ -86,6 +86,10 @@ CITE["gred"] = ("lib/perl/build_qla.pl:2089-2272 (global norm2 and inner product
 CITE["gsum"] = "lib/perl/build_qla.pl:2449-2521 (global sums of a field over the sites)"
 CITE["random"] = ("lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), "
                   "lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36")
+CITE["scalar"] = ("lib/perl/build_qla.pl:186-355, 1936-2082, 2089-2555 (real, complex and integer fields: "
+                  "elementary functions, arithmetic, comparisons, masks, conversions, reductions), "
+                  "include/qla_complex.h:110-140, 417-428, lib/cmath")
+CITE["cfield"] = CITE["rfield"] = CITE["sglobal"] = CITE["scalar"]
 CITE["convert"] = ("lib/perl/build_qla.pl:356-400 (copying between precisions: QLA_DF_c_eq_c promotion, "
                    "QLA_FD_c_eq_c rounding)")
 CITE["reunit"] = ("no counterpart in the reference: r = a (a^+ a)^(-1/2), the composition of "
@@ -441,11 +445,163 @@ def gen_int():
     return fns
 
 
-def gen_fd(prec):
-    """QLA_F_ / QLA_D_ (real and complex fields): uniform and gaussian random
-    fills."""
+# QLA_F_ / QLA_D_ entry points: (dest, name pattern, operands, all eqops?, plan, spec).
+# Operands are (parameter, letter): R / C / I fields (each with a pointer form
+# `p`), or the constants "r" / "c" passed by pointer.  {a} {b} {c} in the
+# pattern stand for the field operands' names (with `p` for pointer forms).
+_UNARY_R = ["sin", "cos", "tan", "asin", "acos", "atan", "sqrt", "fabs", "exp", "log", "log10", "sinh", "cosh",
+            "tanh", "ceil", "floor", "sign"]
+FD_TABLE = (
+    [("C", "{a}", [("a", "C")], True, "ew", ("COPY", 0)),
+     ("C", "{a}a", [("a", "C")], True, "ew", ("CONJ", 0)),
+     ("C", "i_{a}", [("a", "C")], True, "ew", ("I", 0)),
+     ("C", "c", [("a", "c")], True, "fill", None),
+     ("C", "zero", [], False, "zero", None),
+     ("C", "{a}_mask_{b}", [("a", "C"), ("b", "I")], False, "mask", None),
+     ("C", "{a}", [("a", "R")], False, "scalar", "SO_C_FROM_R"),
+     ("C", "{a}_plus_i_{b}", [("a", "R"), ("b", "R")], False, "scalar", "SO_C_R_PLUS_I_R"),
+     ("C", "{a}_times_{b}", [("a", "C"), ("b", "C")], True, "ew", ("CT", 2)),
+     ("C", "{a}_times_{b}a", [("a", "C"), ("b", "C")], True, "ew", ("CTA", 2)),
+     ("C", "{a}a_times_{b}", [("a", "C"), ("b", "C")], True, "ew", ("CAT", 2)),
+     ("C", "{a}a_times_{b}a", [("a", "C"), ("b", "C")], True, "ew", ("CATA", 2)),
+     ("C", "{a}_times_{b}", [("a", "R"), ("b", "C")], True, "ew", ("RT", 3)),
+     ("C", "{a}_times_{b}a", [("a", "R"), ("b", "C")], True, "ew", ("RTA", 3)),
+     ("C", "c_times_{b}", [("a", "c"), ("b", "C")], True, "ew", ("CT", 1)),
+     ("C", "c_times_{b}a", [("a", "c"), ("b", "C")], True, "ew", ("CTA", 1)),
+     ("C", "r_times_{b}", [("a", "r"), ("b", "C")], True, "ew", ("RT", 1)),
+     ("C", "r_times_{b}a", [("a", "r"), ("b", "C")], True, "ew", ("RTA", 1)),
+     ("C", "{a}_plus_{b}", [("a", "C"), ("b", "C")], False, "ew", ("PLUS", 0)),
+     ("C", "{a}_minus_{b}", [("a", "C"), ("b", "C")], False, "ew", ("MINUS", 0)),
+     ("C", "c_times_{b}_plus_{c}", [("a", "c"), ("b", "C"), ("c", "C")], False, "ew", ("CT_PLUS", 1)),
+     ("C", "c_times_{b}_minus_{c}", [("a", "c"), ("b", "C"), ("c", "C")], False, "ew", ("CT_MINUS", 1)),
+     ("C", "r_times_{b}_plus_{c}", [("a", "r"), ("b", "C"), ("c", "C")], False, "ew", ("RT_PLUS", 1)),
+     ("C", "r_times_{b}_minus_{c}", [("a", "r"), ("b", "C"), ("c", "C")], False, "ew", ("RT_MINUS", 1)),
+     ("C", "{a}_divide_{b}", [("a", "C"), ("b", "C")], False, "scalar", "SO_C_DIVIDE"),
+     ("C", "{a}_dot_{b}", [("a", "C"), ("b", "C")], True, "ldot", "LD_DOT"),
+     ("C", "{a}_dot_{b}a", [("a", "C"), ("b", "C")], True, "ldot", "LD_DOT_AA"),
+     ("C", "{a}a_dot_{b}", [("a", "C"), ("b", "C")], True, "ldot", "LD_ADOT"),
+     ("C", "cexp_{a}", [("a", "C")], False, "scalar", "SO_C_CEXP"),
+     ("C", "clog_{a}", [("a", "C")], False, "scalar", "SO_C_CLOG"),
+     ("C", "csqrt_{a}", [("a", "C")], False, "scalar", "SO_C_CSQRT"),
+     ("C", "cexpi_{a}", [("a", "R")], False, "scalar", "SO_C_CEXPI"),
+     ("R", "{a}", [("a", "R")], True, "scalar", "SO_R_COPY"),
+     ("R", "{a}", [("a", "I")], False, "scalar", "SO_R_FROM_I"),
+     ("R", "r", [("a", "r")], True, "scalar", "SO_R_FILL"),
+     ("R", "zero", [], False, "scalar", "SO_R_ZERO"),
+     ("R", "{a}_mask_{b}", [("a", "R"), ("b", "I")], False, "scalar", "SO_R_MASK"),
+     ("R", "{a}_times_{b}", [("a", "R"), ("b", "R")], True, "scalar", "SO_R_TIMES_R"),
+     ("R", "r_times_{b}", [("a", "r"), ("b", "R")], True, "scalar", "SO_R_RTIMES"),
+     ("R", "r_times_{b}_plus_{c}", [("a", "r"), ("b", "R"), ("c", "R")], False, "scalar", "SO_R_RT_PLUS"),
+     ("R", "r_times_{b}_minus_{c}", [("a", "r"), ("b", "R"), ("c", "R")], False, "scalar", "SO_R_RT_MINUS"),
+     ("R", "{a}_ldexp_{b}", [("a", "R"), ("b", "I")], False, "scalar", "SO_R_LDEXP")]
+    + [("R", "{a}_" + op + "_{b}", [("a", "R"), ("b", "R")], False, "scalar", "SO_R_" + op.upper())
+       for op in ("plus", "minus", "divide", "max", "min", "mod", "pow", "atan2")]
+    + [("R", f + "_{a}", [("a", "R")], False, "scalar", "SO_R_" + f.upper()) for f in _UNARY_R]
+    + [("R", f + "_{a}", [("a", "C")], False, "scalar", "SO_R_" + f.upper()) for f in ("re", "im", "norm", "arg")]
+    + [("R", "norm2_{a}", [("a", "C")], True, "ldot", "LD_NORM2"),
+       ("R", "re_{a}_dot_{b}", [("a", "C"), ("b", "C")], True, "ldot", "LD_REDOT")]
+    + [("I", "{a}_" + op + "_{b}", [("a", "R"), ("b", "R")], False, "scalar", "SO_I_" + op.upper())
+       for op in ("eq", "ge", "gt", "le", "lt", "ne")]
+    + [("I", "round_{a}", [("a", "R")], False, "scalar", "SO_I_ROUND"),
+       ("I", "trunc_{a}", [("a", "R")], False, "scalar", "SO_I_TRUNC")]
+    # global reductions and sums (lower-case destination)
+    + [("c", "{a}_dot_{b}", [("a", "C"), ("b", "C")], False, "gdot", "LD_DOT"),
+       ("c", "{a}a_dot_{b}", [("a", "C"), ("b", "C")], False, "gdot", "LD_ADOT"),
+       ("c", "sum_{a}", [("a", "C")], False, "gsum", None),
+       ("r", "{a}_dot_{b}", [("a", "R"), ("b", "R")], False, "sred", "SR_DOT"),
+       ("r", "{a}_dot_{b}", [("a", "I"), ("b", "I")], False, "sred", "SR_DOT"),
+       ("r", "norm2_{a}", [("a", "C")], False, "gdot", "LD_NORM2"),
+       ("r", "norm2_{a}", [("a", "R")], False, "sred", "SR_NORM2"),
+       ("r", "norm2_{a}", [("a", "I")], False, "sred", "SR_NORM2"),
+       ("r", "re_{a}_dot_{b}", [("a", "C"), ("b", "C")], False, "gdot", "LD_REDOT"),
+       ("r", "sum_{a}", [("a", "R")], False, "sred", "SR_SUM"),
+       ("r", "sum_{a}", [("a", "I")], False, "sred", "SR_SUM")])
+
+# QLA_DF_ reductions of float fields returned in double
+DF_TABLE = [row for row in FD_TABLE if row[0] in "cr" and "I" not in [l for _, l in row[2]]]
+
+
+def _fd_entries(lib, table, R, RW, OUT, prec_in, prec_out):
+    """Entry points of `table` for library `lib` (F, D or DF): field elements
+    of type R (precision prec_in), results in prec_out (OUT for globals)."""
     fns = []
+    kid = lambda fam: f'"{lib}_{fam}"'  # noqa: E731
+    ftype = {"R": f"QLA_{prec_in}_Real", "C": f"QLA_{prec_in}_Complex", "I": "QLA_Int"}
+    dtype = {"R": f"QLA_{prec_out}_Real", "C": f"QLA_{prec_out}_Complex", "I": "QLA_Int",
+             "r": f"QLA_{prec_out}_Real", "c": f"QLA_{prec_out}_Complex"}
+    for dest, pat, opnds, alleq, plan, spec in table:
+        fields = [(nm, l) for nm, l in opnds if l in "RCI"]
+        consts = [(nm, l) for nm, l in opnds if l in "rc"]
+        fam = {"ew": "cfield", "fill": "cfield", "zero": "cfield", "mask": "cfield", "ldot": "cfield",
+               "gdot": "sglobal", "gsum": "sglobal", "sred": "sglobal"}.get(plan, None)
+        if plan == "scalar":
+            fam = "cfield" if dest == "C" else "rfield"
+        for var in ["v", "x"]:
+            tail = [("int *", "index")] if var == "x" else []
+            gang = "index" if var == "x" else "nullptr"
+            for eq in (EQOPS if alleq else ["eq"]):
+                for ptrs in itertools.product((False, True), repeat=len(fields)):
+                    tok = {nm: ("p" if pf else "") + l for (nm, l), pf in zip(fields, ptrs)}
+                    name = f"QLA_{lib}_{dest}_{var}{eq}_" + pat.format(**{k: tok.get(k, "") for k in "abc"})
+                    params = [(f"{dtype[dest]} *RESTRICT", "r")]
+                    ops = {}
+                    for nm, l in opnds:
+                        if l in "rc":
+                            params.append((f"{dtype[l]} *RESTRICT", nm))
+                        else:
+                            pf = tok[nm].startswith("p")
+                            params.append((f"{ftype[l]} *RESTRICT *" if pf else f"{ftype[l]} *RESTRICT", nm))
+                            ops[nm] = f"qlab::op_ptr((const void* const*){nm})" if pf else f"qlab::op_contig({nm})"
+                    params += tail + [("int", "n")]
+                    o = lambda nm: ops.get(nm, "qlab::Opnd{}")  # noqa: E731
+                    E = EQ_ENUM[eq]
+                    if plan == "ew":
+                        shape, sk = spec
+                        sc = {0: "qlab::SC_NONE", 1: "qlab::SC_CONST", 2: "qlab::SC_FIELD", 3: "qlab::SC_FIELD"}[sk]
+                        sreal = "true" if (sk == 3 or (sk == 1 and consts and consts[0][1] == "r")) else "false"
+                        if sk == 0:
+                            two = shape in ("PLUS", "MINUS")
+                            args = f"r, nullptr, qlab::Opnd{{}}, {o('a')}, {o('b') if two else 'qlab::Opnd{}'}"
+                        elif sk == 1:
+                            args = f"r, a, qlab::Opnd{{}}, {o('b')}, {o('c')}"
+                        else:
+                            args = f"r, nullptr, {o('a')}, {o('b')}, qlab::Opnd{{}}"
+                        body = (f"qlab::api_ew<{R}, 1, qlab::EW_{shape}, qlab::PERM_ID, {sc}, {sreal}>({kid('ew')}, "
+                                f"{args}, {gang}, n, {E});")
+                    elif plan == "fill":
+                        body = f"qlab::api_fill<{R}, 1>({kid('fill')}, r, a, {gang}, n, {E});"
+                    elif plan == "zero":
+                        body = f"qlab::api_zero<{R}, 1>({kid('fill')}, r, {gang}, n);"
+                    elif plan == "mask":
+                        body = f"qlab::api_mask<{R}, 1>({kid('mask')}, r, {o('a')}, {o('b')}, {gang}, n);"
+                    elif plan == "ldot":
+                        body = (f"qlab::api_ldot<{R}, 1, qlab::{spec}, qlab::PERM_ID>({kid('ldot')}, r, {o('a')}, "
+                                f"{o('b')}, {gang}, n, {E});")
+                    elif plan == "scalar":
+                        body = (f"qlab::api_scalar<{R}, qlab::{spec}>({kid('scalar')}, r, "
+                                f"{'a' if consts else 'nullptr'}, {o('a') if not consts else 'qlab::Opnd{}'}, "
+                                f"{o('b')}, {o('c')}, {gang}, n, {E});")
+                    elif plan == "gdot":
+                        body = (f"qlab::api_gdot<{R}, 1, qlab::{spec}, qlab::PERM_ID, {OUT}>({kid('gdot')}, r, "
+                                f"{o('a')}, {o('b')}, {gang}, n);")
+                    elif plan == "gsum":
+                        body = f"qlab::api_gsum<{R}, 1, {OUT}>({kid('gsum')}, r, {o('a')}, {gang}, n);"
+                    else:  # sred
+                        rin = "int" if fields[0][1] == "I" else R
+                        body = (f"qlab::api_sred<{rin}, {RW}, qlab::{spec}, {OUT}>({kid('sred')}, r, {o('a')}, "
+                                f"{o('b')}, {gang}, n);")
+                    kinds = dict(dest=dest, eqop=eq, var=var, plan=plan, spec=spec if not isinstance(spec, tuple)
+                                 else list(spec), opnds=[[nm, l] for nm, l in opnds],
+                                 **{nm: tok[nm] for nm in tok})
+                    fns.append(Fn(name, params, body, fam, CITE["scalar"], kinds))
+    return fns
+
+
+def gen_fd(prec):
+    """QLA_F_ / QLA_D_ (real, complex and integer fields): the entry points of
+    FD_TABLE, and the uniform and gaussian random fills."""
     R = "float" if prec == "F" else "double"
+    fns = _fd_entries(prec, FD_TABLE, R, R, R, prec, prec)
     kid = f'"{prec}_random"'
     for var in ["v", "x"]:
         tail = [("int *", "index")] if var == "x" else []
@@ -460,6 +616,34 @@ def gen_fd(prec):
                         f"{oa}, {gang}, n);")
                 fns.append(Fn(name, [(rt, "r"), sa] + tail + [("int", "n")], body, "random", CITE["random"],
                               dict(dest=dest, eqop="eq", var=var, op=what, a=ps + "S")))
+    if prec == "F":
+        fns += gen_df()
+    return fns
+
+
+def gen_df():
+    """QLA_DF_ / QLA_FD_: float <-> double conversions of real and complex
+    fields, and the global reductions of float fields returned in double."""
+    fns = _fd_entries("DF", DF_TABLE, "float", "float", "double", "F", "D")
+    for var in ["v", "x"]:
+        tail = [("int *", "index")] if var == "x" else []
+        gang = "index" if var == "x" else "nullptr"
+        for T in ("R", "C"):
+            for p1 in (False, True):
+                for lib, rin, rout, pin, pout in (("DF", "float", "double", "F", "D"),
+                                                  ("FD", "double", "float", "D", "F")):
+                    tin = f"QLA_{pin}_{'Real' if T == 'R' else 'Complex'}"
+                    tout = f"QLA_{pout}_{'Real' if T == 'R' else 'Complex'}"
+                    pa = (f"{tin} *RESTRICT *" if p1 else f"{tin} *RESTRICT", "a")
+                    oa = "qlab::op_ptr((const void* const*)a)" if p1 else "qlab::op_contig(a)"
+                    name = f"QLA_{lib}_{T}_{var}eq_{'p' if p1 else ''}{T}"
+                    if T == "R":
+                        body = f"qlab::api_rconvert<{rin}, {rout}>(\"DF_convert\", r, {oa}, {gang}, n);"
+                    else:
+                        body = f"qlab::api_convert<{rin}, {rout}, 1>(\"DF_convert\", r, {oa}, {gang}, n);"
+                    fns.append(Fn(name, [(f"{tout} *RESTRICT", "r"), pa] + tail + [("int", "n")], body, "convert",
+                                  CITE["scalar"], dict(dest=T, eqop="eq", var=var, a=("p" if p1 else "") + T,
+                                                       lib=lib)))
     return fns
 
 
@@ -1238,7 +1422,7 @@ def main():
                    else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
             # the reference declares QLA_FD3_ in qla_df3.h, QLA_FDN_ in qla_dfn.h, QLA_S_ in qla_int.h
-            hpc = {"FD3": "DF3", "FDN": "DFN", "S": "I"}.get(hpc, hpc)
+            hpc = {"FD3": "DF3", "FDN": "DFN", "S": "I", "FD": "DF"}.get(hpc, hpc)
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
             manifest.append(dict(name=fn.name, pc=hpc, family=fn.family, params=[n for _, n in fn.params],
@@ -1271,6 +1455,8 @@ def main():
             extra = '#include "../qla_sitefield.cuh"\n'
         if family == "random":
             extra = '#include "../qla_random.cuh"\n'
+        if family in ("cfield", "rfield", "sglobal") or (pc == "F" and family == "convert"):
+            extra = '#include "../qla_scalar.cuh"\n'
         if pc in ("FN", "DN") and (family.startswith("ewise") or family in (
                 "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop", "multi",
                 "random")):

@@ -867,3 +867,186 @@ def random_case(e, rng, n, ns, nc=3, milc=0):
     O.ora_rng_copy(ptr(want), ptr(a), ptr(m), nsites, ptr(_i32(idx.get("a"))), ptr(_i32(idx.get("b"))),
                    ptr(_i32(gang)))
     return ins, idx, gang, ints, want, None
+
+
+# ---------------------------------------------------------------------------
+# QLA_F_ / QLA_D_ / QLA_DF_ real, complex and integer fields
+
+def scalar_op_codes():
+    """name -> code of the product's ScalarOp enumeration (read from its
+    header, the single source of the numbering)."""
+    import re
+    txt = open(os.path.join(REPO, "qla_b200", "csrc", "qla_scalar.cuh")).read()
+    body = txt[txt.index("enum ScalarOp"):]
+    body = body[body.index("{") + 1:body.index("};")]
+    names = re.findall(r"\b(SO_\w+)\b", re.sub(r"//[^\n]*", "", body))
+    return {nm: i for i, nm in enumerate(names)}
+
+
+# transcendental ops: CUDA's functions, compared to the host libm within a few ulp
+SCALAR_APPROX = {"SO_R_SIN", "SO_R_COS", "SO_R_TAN", "SO_R_ASIN", "SO_R_ACOS", "SO_R_ATAN", "SO_R_EXP", "SO_R_LOG",
+                 "SO_R_LOG10", "SO_R_SINH", "SO_R_COSH", "SO_R_TANH", "SO_R_POW", "SO_R_ATAN2", "SO_R_ARG",
+                 "SO_C_CEXP", "SO_C_CEXPI", "SO_C_CLOG"}
+
+
+def _fd_values(rng, spec, name, size, dt):
+    """Seeded values in the domain of scalar op `spec` for operand `name`."""
+    u = lambda lo, hi: rng.uniform(lo, hi, size).astype(dt)  # noqa: E731
+    if spec in ("SO_R_ASIN", "SO_R_ACOS"):
+        return u(-1, 1)
+    if spec in ("SO_R_SQRT", "SO_R_LOG", "SO_R_LOG10"):
+        return u(0.01, 10)
+    if spec == "SO_R_POW":
+        return u(0.1, 3) if name == "a" else u(-2, 2)
+    if spec in ("SO_R_EXP", "SO_R_SINH", "SO_R_COSH", "SO_R_TANH"):
+        return u(-5, 5)
+    if spec == "SO_R_TAN":
+        return u(-1.5, 1.5)
+    if spec in ("SO_I_ROUND", "SO_I_TRUNC"):
+        v = u(-1000, 1000)
+        v[::5] = np.round(v[::5]) + 0.5
+        return v
+    if spec in ("SO_R_DIVIDE", "SO_R_MOD") and name == "b":
+        v = u(0.5, 3)
+        v[::2] *= -1
+        return v
+    return (rng.standard_normal(size) * 3).astype(dt)
+
+
+def fd_case(e, rng, n, ns):
+    """Inputs and the oracle's result for a QLA_F_ / QLA_D_ / QLA_DF_ entry
+    e: (ins, idx, gang, want, mode) with mode "exact", "approx" (within a
+    few ulp), "reduce" (one value, reference summation order) or "convert"."""
+    O = oracle()
+    plan, spec = e.get("plan"), e.get("spec")
+    lib = e["name"].split("_")[1]
+    if e["family"] == "convert":
+        src = np.float32 if e["lib"] == "DF" else np.float64
+        dst = np.float64 if e["lib"] == "DF" else np.float32
+        nr = 1 if e["dest"] == "R" else 2
+        a = rng.standard_normal((ns, nr)).astype(src)
+        r = rng.standard_normal((n, nr)).astype(dst)
+        ptr_a = e["a"].startswith("p")
+        ins = {"r": (e["dest"], False, r), "a": (e["dest"], ptr_a, a)}
+        idx = {"a": rng.integers(0, ns, n).astype(np.int32)} if ptr_a else {}
+        gang = rng.permutation(n)[: n // 2 + 1].astype(np.int32) if e["var"] == "x" else None
+        want = r.copy()
+        f = O.ora_convert_df if e["lib"] == "DF" else O.ora_convert_fd
+        f(ptr(want), ptr(a), ctypes.c_long(len(gang) if gang is not None else n), nr, ptr(_i32(idx.get("a"))),
+          ptr(_i32(gang)))
+        return ins, idx, gang, want, "convert"
+    dt = np.float64 if lib == "D" else np.float32
+    t = "d" if lib == "D" else "f"
+    gang = rng.permutation(n)[: n // 2 + 1].astype(np.int32) if e["var"] == "x" else None
+    nsites = ctypes.c_long(len(gang) if gang is not None else n)
+    ins, idx = {}, {}
+    sval = None
+    for nm, l in e["opnds"]:
+        if l in "rc":
+            v = (rng.standard_normal(1 if l == "r" else 2) * 1.5).astype(dt)
+            ins[nm] = (l.upper(), False, v)
+            sval = v
+            continue
+        tok = e[nm]
+        is_ptr = tok.startswith("p")
+        if l == "I":
+            if spec == "SO_R_MASK" or plan == "mask":
+                arr = rng.choice(np.array([0, 1, -3, 0, 7], np.int32), ns)
+            elif spec == "SO_R_LDEXP":
+                arr = rng.integers(-10, 11, ns).astype(np.int32)
+            else:
+                arr = rng.integers(-1000, 1001, ns).astype(np.int32)
+        elif l == "R":
+            arr = _fd_values(rng, spec, nm, ns, dt)
+            if spec in ("SO_I_EQ", "SO_I_GE", "SO_I_LE", "SO_I_NE") and nm == "b":
+                arr[::3] = ins["a"][2][::3] if not ins["a"][1] else arr[::3]
+        else:
+            arr = (rng.standard_normal((ns, 2)) * 2).astype(dt)
+        ins[nm] = (l, is_ptr, arr)
+        if is_ptr:
+            idx[nm] = rng.integers(0, ns, n).astype(np.int32)
+    dest = e["dest"]
+    if dest in "cr":
+        out_dt = np.float64 if lib in ("D", "DF") else np.float32
+        want_len = 2 if (dest == "c" or (plan == "gsum")) else 1
+        ins["r"] = (dest, False, np.zeros(want_len, out_dt))
+        a, b = ins["a"][2], ins["b"][2] if "b" in ins else None
+        ia, ib = _i32(idx.get("a")), _i32(idx.get("b"))
+        if plan == "gdot":
+            out = np.zeros(2, np.float64)
+            getattr(O, "ora_gdot_" + t)(LD_KINDS[spec], 0, ptr(out), ptr(a), ptr(b), nsites, 1, ptr(ia), ptr(ib),
+                                        ptr(_i32(gang)))
+            want = out[:want_len].astype(out_dt)
+        elif plan == "gsum":
+            out = np.zeros(2, np.float64)
+            getattr(O, "ora_gsum_" + t)(ptr(out), ptr(a), nsites, 1, ptr(ia), ptr(_i32(gang)))
+            want = out.astype(out_dt)
+        else:
+            f = getattr(O, "ora_sred_" + t)
+            f.restype = ctypes.c_double
+            isint = int(ins["a"][0] == "I")
+            v = f({"SR_DOT": 0, "SR_NORM2": 1, "SR_SUM": 2}[spec], isint, ptr(a), ptr(b), nsites, ptr(ia), ptr(ib),
+                  ptr(_i32(gang)))
+            want = np.array([v], out_dt)
+        return ins, idx, gang, want, "reduce"
+    shape_r = {"R": (n,), "I": (n,), "C": (n, 2)}[dest]
+    r = (rng.standard_normal(shape_r) * 2).astype(np.int32 if dest == "I" else dt)
+    ins["r"] = (dest, False, r)
+    want = r.copy()
+    eq = EQOPS[e["eqop"]]
+    arr = lambda nm: ins[nm][2] if nm in ins else None  # noqa: E731
+    ix = lambda nm: _i32(idx.get(nm))  # noqa: E731
+    cs = ctypes.c_float if dt == np.float32 else ctypes.c_double
+    if plan == "ew":
+        shape, sk = spec
+        code = EW_SHAPES[shape]
+        sre = sim = 0.0
+        if sk == 0:
+            bn, cn, sn = "a", ("b" if shape in ("PLUS", "MINUS") else None), None
+        elif sk == 1:
+            bn, cn, sn = "b", ("c" if "c" in ins else None), None
+            sre = float(sval[0])
+            sim = float(sval[1]) if len(sval) > 1 else 0.0
+        else:
+            bn, cn, sn = "b", None, "a"
+        getattr(O, "ora_ewise_n_" + t)(3, code, 0, eq, ptr(want), ptr(arr(bn)), ptr(arr(cn)) if cn else None,
+                                       ptr(arr(sn)) if sn else None, sk, cs(sre), cs(sim), nsites, 1, ptr(ix(bn)),
+                                       ptr(ix(cn)) if cn else None, ptr(ix(sn)) if sn else None, ptr(_i32(gang)))
+        return ins, idx, gang, want, "exact"
+    if plan == "fill":
+        getattr(O, "ora_fill_" + t)(eq, ptr(want), ptr(arr("a")), nsites, 1, ptr(_i32(gang)))
+        return ins, idx, gang, want, "exact"
+    if plan == "zero":
+        getattr(O, "ora_zero_" + t)(ptr(want), nsites, 1, ptr(_i32(gang)))
+        return ins, idx, gang, want, "exact"
+    if plan == "mask":
+        getattr(O, "ora_mask_" + t)(ptr(want), ptr(arr("a")), ptr(arr("b")), nsites, 1, ptr(ix("a")), ptr(ix("b")),
+                                    ptr(_i32(gang)))
+        return ins, idx, gang, want, "exact"
+    if plan == "ldot":
+        getattr(O, "ora_ldot_" + t)(LD_KINDS[spec], 0, eq, ptr(want), ptr(arr("a")), ptr(arr("b")), nsites, 1,
+                                    ptr(ix("a")), ptr(ix("b")), ptr(_i32(gang)))
+        return ins, idx, gang, want, "exact"
+    code = scalar_op_codes()[spec]
+    has_const = any(l in "rc" for _, l in e["opnds"])
+    getattr(O, "ora_scalar_" + t)(code, eq, ptr(want), None if has_const else ptr(arr("a")), ptr(arr("b")),
+                                  ptr(arr("c")), cs(float(sval[0]) if has_const else 0.0), nsites,
+                                  None if has_const else ptr(ix("a")), ptr(ix("b")), ptr(ix("c")), ptr(_i32(gang)))
+    return ins, idx, gang, want, ("approx" if spec in SCALAR_APPROX else "exact")
+
+
+def within_ulps(got, want, k=4):
+    """got and want agree within k units in the last place of want (NaN and
+    infinities must match exactly)."""
+    g = np.asarray(got).ravel()
+    w = np.asarray(want).ravel()
+    if g.dtype != w.dtype:
+        return False
+    nan_g, nan_w = np.isnan(g), np.isnan(w)
+    if np.any(nan_g != nan_w):
+        return False
+    fin = np.isfinite(w) & ~nan_w
+    if np.any(g[~fin & ~nan_w] != w[~fin & ~nan_w]):
+        return False
+    return bool(np.all(np.abs(g[fin].astype(np.float64) - w[fin].astype(np.float64))
+                       <= k * np.spacing(np.abs(w[fin])).astype(np.float64)))

@@ -652,3 +652,30 @@ def test_oracle_random_fills_match_reference_library(milc):
         flag.value = 0
     assert count >= (88 if milc else 120)
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("lib", ["F", "D", "DF"])
+def test_oracle_real_complex_field_libraries_match_reference_library(lib):
+    """Every entry point of the real / complex / integer field libraries
+    (QLA_F_, QLA_D_, QLA_DF_ / QLA_FD_): the oracle against the reference
+    library, bit for bit, including the libm functions (the oracle calls the
+    same host libm) and the global reductions (library on one OpenMP thread)."""
+    import qla_b200
+    R = T.ref()
+    rng = np.random.default_rng(121)
+    n, ns = 11, 13
+    bad, count = [], 0
+    for e in qla_b200.manifest():
+        if e["pc"] != lib or e["family"] not in ("cfield", "rfield", "sglobal", "convert"):
+            continue
+        ins, idx, gang, want, mode = T.fd_case(e, rng, n, ns)
+        r = np.zeros_like(want) if mode == "reduce" else ins["r"][2].copy()
+        args, keep = _ref_args(e, ins, idx, gang, n, r)
+        with T.ref_one_thread():
+            getattr(R, e["name"])(*args)
+        count += 1
+        if not T.bits_equal(r, want):
+            bad.append(e["name"])
+    assert count >= (64 if lib == "DF" else 900)
+    assert not bad, f"{len(bad)} mismatches, e.g. {bad[:10]}"
