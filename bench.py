@@ -771,6 +771,47 @@ def run_workload(args):
             torch.cuda.empty_cache()
         out.update({"metric": "element-wise families and site-local products, 32^3x64 sites (P: 1/8 of the sites)",
                     "unit": "site-updates/s", "value": res["F3_D_vpeq_c_times_D"]["site_updates_per_s"], "ops": res})
+    elif args.workload == "fields":
+        # the widened families: random fills, global P reductions / sums,
+        # gamma and antihermitian maps, N-colour element-wise (nc = 4), the
+        # real / complex field library; 32^3x64 sites (P: 1/8 of the sites)
+        n = 32 * 32 * 32 * 64
+        res = {}
+        st = torch.zeros(n, 11, dtype=torch.int32, device="cuda")
+        seeds = torch.arange(n, dtype=torch.int32, device="cuda")
+        L.QLA_S_veq_seed_i_I(V(st), 2024, V(seeds), n)
+        v6 = torch.empty(n, 6, device="cuda")
+        d = torch.randn(n, 24, device="cuda")
+        d2 = torch.empty_like(d)
+        m = torch.randn(n, 18, device="cuda")
+        m2 = torch.empty_like(m)
+        ps = torch.randn(n // 8, 288, device="cuda")
+        ps2 = torch.randn(n // 8, 288, device="cuda")
+        red = torch.zeros(288, dtype=torch.float64, device="cuda")
+        d4 = torch.randn(n, 32, device="cuda")
+        d4b = torch.randn(n, 32, device="cuda")
+        cs = torch.tensor([0.3, -0.7], device="cuda")
+        ra, rb = torch.rand(n, device="cuda") + 0.5, torch.randn(n, device="cuda")
+        ca, cb, cc = torch.randn(n, 2, device="cuda"), torch.randn(n, 2, device="cuda"), torch.empty(n, 2, device="cuda")
+        rr = torch.empty(n, device="cuda")
+        table = [("QLA_F3_V_veq_gaussian_S", lambda: L.QLA_F3_V_veq_gaussian_S(V(v6), V(st), n), n, 24 + 88),
+                 ("QLA_F3_p_veq_sum_P", lambda: L.QLA_F3_p_veq_sum_P(V(red), V(ps), n // 8), n // 8, 1152),
+                 ("QLA_F3_c_veq_P_dot_P", lambda: L.QLA_F3_c_veq_P_dot_P(V(red), V(ps), V(ps2), n // 8), n // 8, 2304),
+                 ("QLA_F3_D_veq_gamma_times_D", lambda: L.QLA_F3_D_veq_gamma_times_D(V(d2), V(d), 5, n), n, 192),
+                 ("QLA_F3_M_veq_antiherm_M", lambda: L.QLA_F3_M_veq_antiherm_M(V(m2), V(m), n), n, 144),
+                 ("QLA_FN_D_vpeq_c_times_D(nc=4)", lambda: L.QLA_FN_D_vpeq_c_times_D(4, V(d4), V(cs), V(d4b), n), n, 384),
+                 ("QLA_F_R_veq_sin_R", lambda: L.QLA_F_R_veq_sin_R(V(rr), V(rb), n), n, 8),
+                 ("QLA_F_C_veq_C_times_C", lambda: L.QLA_F_C_veq_C_times_C(V(cc), V(ca), V(cb), n), n, 24),
+                 ("QLA_F_r_veq_R_dot_R", lambda: L.QLA_F_r_veq_R_dot_R(V(red), V(ra), V(rb), n), n, 8)]
+        for nm, call, nn, nb in table:
+            ms = _events_time(torch, stream, call, reps)
+            gbs = nb * nn / (ms / 1e3) / 1e9
+            res[nm] = {"site_updates_per_s": nn / (ms / 1e3), "us": 1e3 * ms, "gbs": gbs, "hbm_frac": gbs / peak}
+        qla.check("fields")
+        out.update({"metric": "widened families (random fills, P reductions, gamma, N-colour, real/complex fields), "
+                              "32^3x64 sites (P: 1/8 of the sites)",
+                    "unit": "site-updates/s", "value": res["QLA_F3_D_veq_gamma_times_D"]["site_updates_per_s"],
+                    "ops": res})
     elif args.workload == "config1":
         n = 16 ** 4
         res = {}
@@ -818,7 +859,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the reduction accuracy check")
-    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "prop", "ewise", "config1"],
+    ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "prop", "ewise", "fields", "config1"],
                     help="cg_chain is the benchmark line; the others measure the remaining configurations")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -43,6 +43,18 @@ typedef QLA_F_Complex QLA_F3_DiracFermion[3][4];
 typedef QLA_F_Complex QLA_F3_ColorMatrix[3][3];
 typedef QLA_F_Complex QLA_F3_DiracPropagator[3][4][3][4];
 
+typedef QLA_F_Complex QLA_F2_ColorVector[2];
+typedef QLA_F_Complex QLA_F2_HalfFermion[2][2];
+typedef QLA_F_Complex QLA_F2_DiracFermion[2][4];
+typedef QLA_F_Complex QLA_F2_ColorMatrix[2][2];
+typedef QLA_F_Complex QLA_F2_DiracPropagator[2][4][2][4];
+
+typedef QLA_D_Complex QLA_D2_ColorVector[2];
+typedef QLA_D_Complex QLA_D2_HalfFermion[2][2];
+typedef QLA_D_Complex QLA_D2_DiracFermion[2][4];
+typedef QLA_D_Complex QLA_D2_ColorMatrix[2][2];
+typedef QLA_D_Complex QLA_D2_DiracPropagator[2][4][2][4];
+
 typedef QLA_D_Complex QLA_D3_ColorVector[3];
 typedef QLA_D_Complex QLA_D3_HalfFermion[3][2];
 typedef QLA_D_Complex QLA_D3_DiracFermion[3][4];

@@ -49,7 +49,7 @@ EOF
 
 # libraries whose headers qla.h pulls in (qla.h:113-129) and whose code we compile
 HDR_ONLY="qla_q qla_dq qla_q3 qla_dq3 qla_qn qla_dqn"
-COMPILE="qla_int qla_f qla_d qla_df qla_f3 qla_d3 qla_df3 qla_fn qla_dn qla_dfn"
+COMPILE="qla_int qla_f qla_d qla_df qla_f2 qla_d2 qla_df2 qla_f3 qla_d3 qla_df3 qla_fn qla_dn qla_dfn"
 
 for dir in $COMPILE $HDR_ONLY; do
   tag=$(echo $dir | sed s/_int// | tr a-z A-Z)
@@ -79,11 +79,12 @@ export CFLAGS
 xargs -P "$JOBS" -n 1 -d '\n' sh -c '
   IFS="|"; set -- $1
   case $3 in
-    qla_f|qla_f3|qla_fn) P="-DQLA_PrecisionInt=1" ;;
-    qla_d|qla_d3|qla_dn) P="-DQLA_PrecisionInt=2" ;;
+    qla_f|qla_f2|qla_f3|qla_fn) P="-DQLA_PrecisionInt=1" ;;
+    qla_d|qla_d2|qla_d3|qla_dn) P="-DQLA_PrecisionInt=2" ;;
     *) P="" ;;
   esac
   case $3 in
+    *2) C="-DQLA_Colors=2" ;;
     *3) C="-DQLA_Colors=3" ;;
     qla_fn|qla_dn|qla_dfn) C="-DQLA_Colors='"'"'N'"'"'" ;;
     *) C="" ;;

@@ -1,0 +1,57 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA D2 gamma entry points (extern "C"), reference: lib/perl/build_qla.pl:1358-1412 (left / right multiplication by gamma_mu, mu = 0..15), expressions_gamma.pl:59-134, 384-470
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+#include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_D2_D_veq_gamma_times_D(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_contig(a), mu, nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_D_veq_gamma_times_pD(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), mu, nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_veq_gamma_times_P(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_veq_gamma_times_pP(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_veq_P_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int n) {
+  qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_veq_pP_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int n) {
+  qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_D_xeq_gamma_times_D(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int * index, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_contig(a), mu, index, n);
+}
+
+QLAB_EXPORT void QLA_D2_D_xeq_gamma_times_pD(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int * index, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), mu, index, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_xeq_gamma_times_P(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int * index, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, index, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_xeq_gamma_times_pP(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int * index, int n) {
+  qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, index, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_xeq_P_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int * index, int n) {
+  qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, index, n);
+}
+
+QLAB_EXPORT void QLA_D2_P_xeq_pP_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int * index, int n) {
+  qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, index, n);
+}
+
+}  // extern "C"

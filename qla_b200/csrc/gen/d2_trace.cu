@@ -1,0 +1,73 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA D2 trace entry points (extern "C"), reference: lib/perl/build_qla.pl:933-1064 (trace, real / imaginary trace, traceless antihermitian part)
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+#include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_D2_C_veq_trace_M(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_C>("D2_trace", 2, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_veq_re_trace_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_RE>("D2_trace", 2, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_veq_im_trace_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_IM>("D2_trace", 2, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_M_veq_antiherm_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  qlab::api_antiherm_n<double>("D2_trace", 2, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_C_veq_trace_pM(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_C>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_veq_re_trace_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_RE>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_veq_im_trace_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_IM>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_M_veq_antiherm_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  qlab::api_antiherm_n<double>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_D2_C_xeq_trace_M(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_C>("D2_trace", 2, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_xeq_re_trace_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_RE>("D2_trace", 2, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_xeq_im_trace_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_IM>("D2_trace", 2, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_M_xeq_antiherm_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  qlab::api_antiherm_n<double>("D2_trace", 2, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_C_xeq_trace_pM(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_C>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_xeq_re_trace_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_RE>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_R_xeq_im_trace_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_trace_n<double, qlab::SF_TRACE_IM>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_D2_M_xeq_antiherm_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  qlab::api_antiherm_n<double>("D2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// GENERATED by qla_b200/gen/gen_qla.py; do not edit.
+// QLA F2 random entry points (extern "C"), reference: lib/perl/build_qla.pl:2620-2690 (uniform and gaussian random fills, seeding), lib/random/QLA_random.c:18-36, QLA_gaussian.c:19-55, QLA_seed_random.c:13-36
+#include "../../../include/qla_b200_types.h"
+#include "../qla_api.cuh"
+#include "../qla_ncolor.cuh"
+#include "../qla_random.cuh"
+
+extern "C" {
+QLAB_EXPORT void QLA_F2_V_veq_gaussian_S(QLA_F2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2, 1, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_V_veq_gaussian_pS(QLA_F2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_H_veq_gaussian_S(QLA_F2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_H_veq_gaussian_pS(QLA_F2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_D_veq_gaussian_S(QLA_F2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 4 * 2, 1, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_D_veq_gaussian_pS(QLA_F2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 4 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_M_veq_gaussian_S(QLA_F2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_M_veq_gaussian_pS(QLA_F2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_P_veq_gaussian_S(QLA_F2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 16 * 2 * 2, 1, r, qlab::op_contig(a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_P_veq_gaussian_pS(QLA_F2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 16 * 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
+}
+
+QLAB_EXPORT void QLA_F2_V_xeq_gaussian_S(QLA_F2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2, 1, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_V_xeq_gaussian_pS(QLA_F2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_H_xeq_gaussian_S(QLA_F2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_H_xeq_gaussian_pS(QLA_F2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_D_xeq_gaussian_S(QLA_F2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 4 * 2, 1, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_D_xeq_gaussian_pS(QLA_F2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 4 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_M_xeq_gaussian_S(QLA_F2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_M_xeq_gaussian_pS(QLA_F2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_P_xeq_gaussian_S(QLA_F2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 16 * 2 * 2, 1, r, qlab::op_contig(a), index, n);
+}
+
+QLAB_EXPORT void QLA_F2_P_xeq_gaussian_pS(QLA_F2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  qlab::api_rng_fill_n<float>("F2_random", 2, 16 * 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
+}
+
+}  // extern "C"

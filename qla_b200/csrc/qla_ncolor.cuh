@@ -604,6 +604,47 @@ __global__ void __launch_bounds__(256) gdotn_kernel(const EwParams p, const Site
   reduce_finish<FIN>(rp, acc);
 }
 
+// contiguous fields without a gang index: one flat stream of complex
+// numbers (gdot_flat_kernel's scheme with a run-time record length)
+template <typename R, int KIND, typename OUT>
+__global__ void __launch_bounds__(256) gdotn_flat_kernel(const EwParams p, const SiteParams rp, const NcDims d) {
+  using FIN = GDotFinish<KIND, OUT>;
+  DD accr[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}}, acci[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}};
+  const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
+  const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);
+  const bool pa = (KIND == LD_ADOT), pb = (KIND == LD_DOT_AA);
+  int u = 0;
+  for (SiteElemWalk w(d.ne); w.i < p.n; w.next(d.ne)) {
+    const Cx<R>* a = A + w.i * d.ne;
+    const Cx<R>* b = B + w.i * d.ne;
+    const int pe = (pa || pb) ? perm_elem_n(d.perm, w.e, d.blk, d.inv_blk) : w.e;
+    const Cx<R> ua = a[pa ? pe : w.e], vb = b[pb ? pe : w.e];
+    const double ur = ua.re, ui = ua.im, vr = vb.re, vi = vb.im;
+    double tr, ti = 0.0;
+    if constexpr (KIND == LD_DOT || KIND == LD_REDOT || KIND == LD_NORM2) {
+      tr = __dadd_rn(__dmul_rn(ur, vr), __dmul_rn(ui, vi));
+      if constexpr (KIND == LD_DOT) ti = __dsub_rn(__dmul_rn(ur, vi), __dmul_rn(ui, vr));
+    } else if constexpr (KIND == LD_DOT_AA) {
+      tr = __dsub_rn(__dmul_rn(ur, vr), __dmul_rn(ui, vi));
+      ti = __dsub_rn(__dmul_rn(-ur, vi), __dmul_rn(ui, vr));
+    } else {
+      tr = __dsub_rn(__dmul_rn(ur, vr), __dmul_rn(ui, vi));
+      ti = __dadd_rn(__dmul_rn(ur, vi), __dmul_rn(ui, vr));
+    }
+    dd_add(accr[u], tr);
+    if constexpr (FIN::NACC > 1) dd_add(acci[u], ti);
+    u ^= 1;
+  }
+  DD acc[ArrN<FIN::NACC>::value];
+  acc[0] = accr[0];
+  dd_merge(acc[0], accr[1]);
+  if constexpr (FIN::NACC > 1) {
+    acc[1] = acci[0];
+    dd_merge(acc[1], acci[1]);
+  }
+  reduce_finish<FIN>(rp, acc);
+}
+
 template <typename R, int KIND, typename OUT>
 inline void api_gdot_n(const char* kid, int nc, int ne, int perm, void* r, Opnd a, Opnd b, const int* gang, int n) {
   constexpr int NACC = GDotFinish<KIND, OUT>::NACC;
@@ -636,11 +677,15 @@ inline void api_gdot_n(const char* kid, int nc, int ne, int perm, void* r, Opnd 
   rp.partials = rs->partials;
   rp.counter = rs->counter;
   rp.result = dev_out ? r : rs->result;
-  long long grid = ((long long)n + 255) / 256;
-  const long long cap = (long long)sms * 4;
+  const bool flat = gang == nullptr && a.mode == OM_CONTIG && (KIND == LD_NORM2 || b.mode == OM_CONTIG);
+  long long grid = ((flat ? (long long)n * ne : (long long)n) + 255) / 256;
+  const long long cap = (long long)sms * (flat ? 8 : 4);
   if (grid > cap) grid = cap;
   if (grid > rs->max_blocks) grid = rs->max_blocks;
-  gdotn_kernel<R, KIND, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, st>>>(p, rp, nc_dims(nc, ne, perm));
+  if (flat)
+    gdotn_flat_kernel<R, KIND, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, st>>>(p, rp, nc_dims(nc, ne, perm));
+  else
+    gdotn_kernel<R, KIND, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, st>>>(p, rp, nc_dims(nc, ne, perm));
   if (!check_launch(kid)) return;
   if (!dev_out) {
     if (cudaMemcpyAsync(r, rs->result, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -667,20 +712,31 @@ __global__ void __launch_bounds__(1024) gsumn_kernel(const EwParams p, int NR, i
   const int BT = blockDim.x;
   if (!wide) {
     const int c = threadIdx.x % NR;
-    DD acc{0.0, 0.0};
+    constexpr int GS_U = 8;  // independent accumulators: loads in flight, folded in a fixed order
+    DD accs[GS_U];
+#pragma unroll
+    for (int u = 0; u < GS_U; u++) accs[u] = DD{0.0, 0.0};
     const long long total = p.n * NR;
-    for (long long j = (long long)blockIdx.x * BT + threadIdx.x; j < total; j += (long long)gridDim.x * BT) {
-      double v;
-      if (flat) {
-        v = (double)static_cast<const R*>(p.b.base)[j];
-      } else {
-        const long long i = j / NR;
-        const long long k = p.gang ? (long long)p.gang[i] : i;
-        const R* rec = (p.b.mode == OM_PTR) ? static_cast<const R*>(p.b.ptrs[k]) : static_cast<const R*>(p.b.base) + k * NR;
-        v = (double)rec[c];
-      }
-      dd_add(acc, v);
+    const long long stride = (long long)gridDim.x * BT;
+    auto load = [&](long long j) -> double {
+      if (flat) return (double)static_cast<const R*>(p.b.base)[j];
+      const long long i = j / NR;
+      const long long k = p.gang ? (long long)p.gang[i] : i;
+      const R* rec = (p.b.mode == OM_PTR) ? static_cast<const R*>(p.b.ptrs[k]) : static_cast<const R*>(p.b.base) + k * NR;
+      return (double)rec[c];
+    };
+    long long j = (long long)blockIdx.x * BT + threadIdx.x;
+    for (; j + (GS_U - 1) * stride < total; j += GS_U * stride) {
+      double v[GS_U];
+#pragma unroll
+      for (int u = 0; u < GS_U; u++) v[u] = load(j + u * stride);
+#pragma unroll
+      for (int u = 0; u < GS_U; u++) dd_add(accs[u], v[u]);
     }
+    for (; j < total; j += stride) dd_add(accs[0], load(j));
+    DD acc = accs[0];
+#pragma unroll
+    for (int u = 1; u < GS_U; u++) dd_merge(acc, accs[u]);
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int q = threadIdx.x; q < NR; q += BT) {
@@ -766,7 +822,7 @@ inline void api_gsum_n(const char* kid, int nc, int ne, void* r, Opnd a, const i
   }
   const int sms = device_sm_count();
   long long grid = wide ? (long long)n : ((long long)n * NR + BT - 1) / BT;
-  const long long cap = (long long)sms * 2;
+  const long long cap = (long long)sms * 4;
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
   const long long need_ll = (grid * NR + ((long long)NR * (long long)sizeof(OUT) + (long long)sizeof(DD) - 1) /

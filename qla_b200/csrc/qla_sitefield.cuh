@@ -427,10 +427,10 @@ inline void api_antiherm(const char* kid, void* r, Opnd a, const int* gang, int 
 
 // ---------------------------------------------------------------------------
 // Global reductions over P records and over the permuted (Ma, Pa) forms:
-// each site's sum is formed in double in the reference's element order
-// (ldot_site), and the sites are added in double-double, as in the other
-// global reductions.  Records are staged through shared memory with
-// coalesced loads when contiguous, as in ldot_smem_kernel.
+// every term is formed in double as the reference forms it and added in
+// double-double.  Contiguous fields stream as one flat array of complex
+// numbers (gdot_flat_kernel); gang-indexed or pointer-array fields take one
+// thread per site (gdot_kernel).
 
 template <int KIND, typename OUT>
 struct GDotFinish {
@@ -443,52 +443,99 @@ struct GDotFinish {
   }
 };
 
-template <typename R, int NE, int KIND, int PERM, int S, typename OUT>
-__global__ void __launch_bounds__(128) gdot_kernel(const EwParams p, const SiteParams rp, int staged) {
+// one complex term of the global sum, as ldot_site forms it, for element e
+// of the site whose records start at a / b
+template <typename R, int NE, int KIND, int PERM>
+__device__ __forceinline__ void gdot_term(const Cx<R>* a, const Cx<R>* b, int e, double& tr, double& ti) {
+  Cx<R> ua = a[e], vb = b[e];
+  if constexpr (KIND == LD_ADOT) ua = a[perm_elem<PERM, NE>(e)];
+  if constexpr (KIND == LD_DOT_AA) vb = b[perm_elem<PERM, NE>(e)];
+  const double ur = ua.re, ui = ua.im, vr = vb.re, vi = vb.im;
+  ti = 0.0;
+  if constexpr (KIND == LD_DOT || KIND == LD_REDOT || KIND == LD_NORM2) {
+    tr = __dadd_rn(__dmul_rn(ur, vr), __dmul_rn(ui, vi));
+    if constexpr (KIND == LD_DOT) ti = __dsub_rn(__dmul_rn(ur, vi), __dmul_rn(ui, vr));
+  } else if constexpr (KIND == LD_DOT_AA) {
+    tr = __dsub_rn(__dmul_rn(ur, vr), __dmul_rn(ui, vi));
+    ti = __dsub_rn(__dmul_rn(-ur, vi), __dmul_rn(ui, vr));
+  } else {
+    tr = __dsub_rn(__dmul_rn(ur, vr), __dmul_rn(ui, vi));
+    ti = __dadd_rn(__dmul_rn(ur, vi), __dmul_rn(ui, vr));
+  }
+}
+
+// Contiguous operands without a gang index: the n * NE complex elements are
+// one flat stream; thread g takes elements g, g + stride, ... with GD_U
+// independent double-double accumulators (GD_U loads in flight), folded in a
+// fixed order, then the block / grid fold of reduce_finish.  The order of the
+// sum differs from the reference's single running double (the global sums
+// are compared to it within the stated tolerance); every term is formed in
+// double exactly as the reference forms it.
+constexpr int GD_U = 4;
+
+template <typename R, int NE, int KIND, int PERM, typename OUT>
+__global__ void __launch_bounds__(256) gdot_flat_kernel(const EwParams p, const SiteParams rp) {
   using FIN = GDotFinish<KIND, OUT>;
-  extern __shared__ __align__(16) unsigned char gdsm[];
+  DD accr[GD_U], acci[GD_U];
+#pragma unroll
+  for (int u = 0; u < GD_U; u++) {
+    accr[u] = DD{0.0, 0.0};
+    acci[u] = DD{0.0, 0.0};
+  }
+  const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
+  const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);
+  const long long total = p.n * NE;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; g + (GD_U - 1) * stride < total; g += GD_U * stride) {
+#pragma unroll
+    for (int u = 0; u < GD_U; u++) {
+      const long long q = g + u * stride;
+      const long long i = q / NE;
+      const int e = (int)(q - i * NE);
+      double tr, ti;
+      gdot_term<R, NE, KIND, PERM>(A + i * NE, B + i * NE, e, tr, ti);
+      dd_add(accr[u], tr);
+      if constexpr (FIN::NACC > 1) dd_add(acci[u], ti);
+    }
+  }
+  for (; g < total; g += stride) {
+    const long long i = g / NE;
+    const int e = (int)(g - i * NE);
+    double tr, ti;
+    gdot_term<R, NE, KIND, PERM>(A + i * NE, B + i * NE, e, tr, ti);
+    dd_add(accr[0], tr);
+    if constexpr (FIN::NACC > 1) dd_add(acci[0], ti);
+  }
+  DD acc[ArrN<FIN::NACC>::value];
+  acc[0] = accr[0];
+#pragma unroll
+  for (int u = 1; u < GD_U; u++) dd_merge(acc[0], accr[u]);
+  if constexpr (FIN::NACC > 1) {
+    acc[1] = acci[0];
+#pragma unroll
+    for (int u = 1; u < GD_U; u++) dd_merge(acc[1], acci[u]);
+  }
+  reduce_finish<FIN>(rp, acc);
+}
+
+// gang-indexed or pointer-array operands: one thread per site, the site's
+// sum formed in double in the reference's element order (ldot_site)
+template <typename R, int NE, int KIND, int PERM, typename OUT>
+__global__ void __launch_bounds__(128) gdot_kernel(const EwParams p, const SiteParams rp) {
+  using FIN = GDotFinish<KIND, OUT>;
   DD acc[ArrN<FIN::NACC>::value];
 #pragma unroll
   for (int a = 0; a < ArrN<FIN::NACC>::value; a++) acc[a] = DD{0.0, 0.0};
-  auto add = [&](double xr, double xi) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    const Cx<R>* a = rec_ptr<R>(p.b, k, NE);
+    const Cx<R>* b = (KIND == LD_NORM2) ? a : rec_ptr<R>(p.c, k, NE);
+    double xr, xi;
+    ldot_site<R, NE, KIND, PERM>(a, b, xr, xi);
     dd_add(acc[0], xr);
     if constexpr (FIN::NACC > 1) dd_add(acc[1], xi);
-  };
-  if (staged) {
-    constexpr int ST = NE + 1;
-    Cx<R>* sa = reinterpret_cast<Cx<R>*>(gdsm);
-    Cx<R>* sb = sa + S * ST;
-    const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
-    const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);
-    const long long ntile = (p.n + S - 1) / S;
-    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
-      const long long s0 = tile * S;
-      const int ns = (int)((p.n - s0) < S ? (p.n - s0) : S);
-      const long long base = s0 * NE;
-      for (int f = threadIdx.x; f < ns * NE; f += blockDim.x) {
-        const int row = f / NE, col = f - row * NE;
-        sa[row * ST + col] = A[base + f];
-        if constexpr (KIND != LD_NORM2) sb[row * ST + col] = B[base + f];
-      }
-      __syncthreads();
-      if (threadIdx.x < ns) {
-        double xr, xi;
-        const Cx<R>* ra = sa + threadIdx.x * ST;
-        ldot_site<R, NE, KIND, PERM>(ra, KIND == LD_NORM2 ? ra : sb + threadIdx.x * ST, xr, xi);
-        add(xr, xi);
-      }
-      __syncthreads();
-    }
-  } else {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
-         i += (long long)gridDim.x * blockDim.x) {
-      const long long k = p.gang ? (long long)p.gang[i] : i;
-      const Cx<R>* a = rec_ptr<R>(p.b, k, NE);
-      const Cx<R>* b = (KIND == LD_NORM2) ? a : rec_ptr<R>(p.c, k, NE);
-      double xr, xi;
-      ldot_site<R, NE, KIND, PERM>(a, b, xr, xi);
-      add(xr, xi);
-    }
   }
   reduce_finish<FIN>(rp, acc);
 }
@@ -526,22 +573,20 @@ inline void api_gdot(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
   rp.partials = rs->partials;
   rp.counter = rs->counter;
   rp.result = dev_out ? r : rs->result;
-  constexpr int S = NE > 32 ? 32 : 128;
-  const int staged = (gang == nullptr && a.mode == OM_CONTIG && (KIND == LD_NORM2 || b.mode == OM_CONTIG)) ? 1 : 0;
-  const size_t smem = staged ? (size_t)(KIND == LD_NORM2 ? 1 : 2) * S * (NE + 1) * sizeof(Cx<R>) : 0;
-  const void* fn = reinterpret_cast<const void*>(&gdot_kernel<R, NE, KIND, PERM, S, OUT>);
-  static bool attr_set[64] = {false};
-  const int dev = current_device();
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)((size_t)(KIND == LD_NORM2 ? 1 : 2) * S * (NE + 1) * sizeof(Cx<R>)));
-    attr_set[dev] = true;
+  const bool flat = gang == nullptr && a.mode == OM_CONTIG && (KIND == LD_NORM2 || b.mode == OM_CONTIG);
+  if (flat) {
+    long long grid = ((long long)n * NE + 256 * GD_U - 1) / (256 * GD_U);
+    const long long cap = (long long)sms * 8;
+    if (grid > cap) grid = cap;
+    if (grid > rs->max_blocks) grid = rs->max_blocks;
+    gdot_flat_kernel<R, NE, KIND, PERM, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, st>>>(p, rp);
+  } else {
+    long long grid = ((long long)n + 127) / 128;
+    const long long cap = (long long)sms * 8;
+    if (grid > cap) grid = cap;
+    if (grid > rs->max_blocks) grid = rs->max_blocks;
+    gdot_kernel<R, NE, KIND, PERM, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 128, 0, st>>>(p, rp);
   }
-  long long grid = staged ? ((long long)n + S - 1) / S : ((long long)n + 127) / 128;
-  const long long cap = (long long)sms * 8;
-  if (grid > cap) grid = cap;
-  if (grid > rs->max_blocks) grid = rs->max_blocks;
-  gdot_kernel<R, NE, KIND, PERM, S, OUT><<<(unsigned)(grid < 1 ? 1 : grid), 128, smem, st>>>(p, rp, staged);
   if (!check_launch(kid)) return;
   if (!dev_out) {
     if (cudaMemcpyAsync(r, rs->result, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -567,20 +612,33 @@ __global__ void __launch_bounds__(1024) gsum_kernel(const EwParams p, DD* partia
   __shared__ bool is_last;
   const int BT = blockDim.x;
   const int c = threadIdx.x % NR;
-  DD acc{0.0, 0.0};
+  // GS_U independent accumulators keep GS_U loads in flight per thread; they
+  // are folded in a fixed order, so the sum is deterministic for a grid
+  constexpr int GS_U = 8;
+  DD accs[GS_U];
+#pragma unroll
+  for (int u = 0; u < GS_U; u++) accs[u] = DD{0.0, 0.0};
   const long long total = p.n * NR;
-  for (long long j = (long long)blockIdx.x * BT + threadIdx.x; j < total; j += (long long)gridDim.x * BT) {
-    double v;
-    if (flat) {
-      v = (double)static_cast<const R*>(p.b.base)[j];
-    } else {
-      const long long i = j / NR;
-      const long long k = p.gang ? (long long)p.gang[i] : i;
-      const R* rec = (p.b.mode == OM_PTR) ? static_cast<const R*>(p.b.ptrs[k]) : static_cast<const R*>(p.b.base) + k * NR;
-      v = (double)rec[c];
-    }
-    dd_add(acc, v);
+  const long long stride = (long long)gridDim.x * BT;
+  auto load = [&](long long j) -> double {
+    if (flat) return (double)static_cast<const R*>(p.b.base)[j];
+    const long long i = j / NR;
+    const long long k = p.gang ? (long long)p.gang[i] : i;
+    const R* rec = (p.b.mode == OM_PTR) ? static_cast<const R*>(p.b.ptrs[k]) : static_cast<const R*>(p.b.base) + k * NR;
+    return (double)rec[c];
+  };
+  long long j = (long long)blockIdx.x * BT + threadIdx.x;
+  for (; j + (GS_U - 1) * stride < total; j += GS_U * stride) {
+    double v[GS_U];
+#pragma unroll
+    for (int u = 0; u < GS_U; u++) v[u] = load(j + u * stride);
+#pragma unroll
+    for (int u = 0; u < GS_U; u++) dd_add(accs[u], v[u]);
   }
+  for (; j < total; j += stride) dd_add(accs[0], load(j));
+  DD acc = accs[0];
+#pragma unroll
+  for (int u = 1; u < GS_U; u++) dd_merge(acc, accs[u]);
   red[threadIdx.x] = acc;
   __syncthreads();
   for (int q = threadIdx.x; q < NR; q += BT) {
@@ -637,7 +695,7 @@ inline void api_gsum(const char* kid, void* r, Opnd a, const int* gang, int n) {
   while (BT + l <= 512) BT += l;
   const int sms = device_sm_count();
   long long grid = ((long long)n * NR + BT - 1) / BT;
-  const long long cap = (long long)sms * 2;
+  const long long cap = (long long)sms * 4;
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
   // partials [grid * NR] DD, then the result record

@@ -369,6 +369,36 @@ def gen_fn_wide(prec):
     return fns
 
 
+def gen_two(prec):
+    """QLA_F2_ / QLA_DF2_ / QLA_FD2_ (prec "F") or QLA_D2_ (prec "D"): the
+    two-colour libraries, with the fixed-colour libraries' names and record
+    types (QLA_F2_ColorMatrix ...) and the N-colour implementations at nc = 2."""
+    src_pc, R = ("F3", "float") if prec == "F" else ("D3", "double")
+    twins = {fn.name: fn for fn in gen_pc(src_pc, R, prec)}
+    fns = []
+    for fn in gen_fn(prec) + gen_fn_wide(prec):
+        m = re.match(r"QLA_(FN|DN|DFN|FDN)_(.*)$", fn.name)
+        lib3 = {"FN": "F3", "DN": "D3", "DFN": "DF3", "FDN": "FD3"}[m.group(1)]
+        lib2 = {"FN": "F2", "DN": "D2", "DFN": "DF2", "FDN": "FD2"}[m.group(1)]
+        twin = twins[f"QLA_{lib3}_{m.group(2)}"]
+        params = [(re.sub(r"QLA_([FD])3_", r"QLA_\g<1>2_", t), nm) for t, nm in twin.params]
+        body = fn.body
+        if "switch (nc)" in body:
+            # compiled-colour families: keep the nc = 2 instantiation
+            head = body[:body.index("switch (nc)")]
+            case2 = re.search(r"case 2: (.*?) break;\n", body)
+            if case2:
+                body = head + case2.group(1)
+            else:
+                body = (head + f'qlab::set_error(QLAGPU_ERR_ARG, "QLA_{lib2}_{m.group(2)}", '
+                        '"not built for two colours");')
+        else:
+            body = re.sub(r"\bnc\b", "2", body)
+        body = re.sub(r'"(FN|DN)_', lambda mm: '"' + mm.group(1)[0] + "2_", body)
+        fns.append(Fn(f"QLA_{lib2}_{m.group(2)}", params, body, fn.family, fn.cite, fn.kinds))
+    return fns
+
+
 def gen_int():
     """QLA_I_ entry points: the (shape x eqop x indexing) set of the reference's
     integer library."""
@@ -1416,13 +1446,14 @@ def main():
     groups = {}
     headers = {}
     for pc, R, P in [("F3", "float", "F"), ("D3", "double", "D"), ("I", None, None), ("FN", None, None),
-                     ("DN", None, None), ("F", None, None), ("D", None, None)]:
+                     ("DN", None, None), ("F", None, None), ("D", None, None), ("F2", None, None),
+                     ("D2", None, None)]:
         for fn in (gen_int() if pc == "I" else gen_fn("F") + gen_fn_wide("F") if pc == "FN"
                    else gen_fn("D") + gen_fn_wide("D") if pc == "DN" else gen_fd(pc) if pc in ("F", "D")
-                   else gen_pc(pc, R, P)):
+                   else gen_two(pc[0]) if pc in ("F2", "D2") else gen_pc(pc, R, P)):
             hpc = fn.name.split("_")[1]  # F3 / D3 / DF3
             # the reference declares QLA_FD3_ in qla_df3.h, QLA_FDN_ in qla_dfn.h, QLA_S_ in qla_int.h
-            hpc = {"FD3": "DF3", "FDN": "DFN", "S": "I", "FD": "DF"}.get(hpc, hpc)
+            hpc = {"FD3": "DF3", "FDN": "DFN", "S": "I", "FD": "DF", "FD2": "DF2"}.get(hpc, hpc)
             headers.setdefault(hpc, []).append(fn)
             groups.setdefault((pc, fn.family), []).append(fn)
             manifest.append(dict(name=fn.name, pc=hpc, family=fn.family, params=[n for _, n in fn.params],
@@ -1457,13 +1488,13 @@ def main():
             extra = '#include "../qla_random.cuh"\n'
         if family in ("cfield", "rfield", "sglobal") or (pc == "F" and family == "convert"):
             extra = '#include "../qla_scalar.cuh"\n'
-        if pc in ("FN", "DN") and (family.startswith("ewise") or family in (
+        if pc in ("FN", "DN", "F2", "D2") and (family.startswith("ewise") or family in (
                 "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop", "multi",
                 "random")):
             extra = '#include "../qla_ncolor.cuh"\n#include "../qla_random.cuh"\n'
-        if pc in ("FN", "DN") and family == "mfunc":
+        if pc in ("FN", "DN", "F2", "D2") and family == "mfunc":
             extra = '#include "../qla_mfunc_generic.cuh"\n'
-        if pc in ("FN", "DN") and family == "mfunc_ext":
+        if pc in ("FN", "DN", "F2", "D2") and family == "mfunc_ext":
             extra = '#include "../qla_mfunc_generic_ext.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:

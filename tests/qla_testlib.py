@@ -650,8 +650,9 @@ def fixed_colour_twin(name):
     """The QLA_F3_ / QLA_D3_ / QLA_DF3_ / QLA_FD3_ entry point a QLA_FN_ /
     QLA_DN_ / QLA_DFN_ / QLA_FDN_ one generalises."""
     import re
-    m = re.match(r"QLA_(FN|DN|DFN|FDN)_(.*)$", name)
-    return "QLA_" + {"FN": "F3", "DN": "D3", "DFN": "DF3", "FDN": "FD3"}[m.group(1)] + "_" + m.group(2)
+    m = re.match(r"QLA_(FN|DN|DFN|FDN|F2|D2|DF2|FD2)_(.*)$", name)
+    return "QLA_" + {"FN": "F3", "DN": "D3", "DFN": "DF3", "FDN": "FD3", "F2": "F3", "D2": "D3", "DF2": "DF3",
+                     "FD2": "FD3"}[m.group(1)] + "_" + m.group(2)
 
 
 def ncolor_case(e, rng, n, ns, nc):

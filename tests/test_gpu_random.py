@@ -72,6 +72,8 @@ def test_every_random_entry_point(qla, milc):
             twin = e
             if e["pc"] in ("FN", "DN"):
                 twin, ncs = byname[T.fixed_colour_twin(e["name"])], [2, 4]
+            elif e["pc"] in ("F2", "D2"):
+                twin, ncs = byname[T.fixed_colour_twin(e["name"])], [2]
             if milc and twin.get("op") != "gaussian":
                 continue
             for nc in ncs:

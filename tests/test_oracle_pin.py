@@ -238,7 +238,8 @@ def test_prototypes_match_reference_headers():
         for m in re.finditer(r"void (QLA_(?:D?FN|DN|FDN)_\w+) \((.*?)\);", txt):
             # VLA record types: compare the parameter count (the first is int nc)
             nargs_fn[m.group(1)] = len(re.findall(r"\(\s*\*|\bint\b|QLA_[FD]_(?:Real|Complex)|\bQLA_Int\b|\bQLA_RandomState\b", m.group(2)))
-    for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h", "qla_f.h", "qla_d.h", "qla_df.h"):
+    for h in ("qla_f3.h", "qla_d3.h", "qla_df3.h", "qla_int.h", "qla_f.h", "qla_d.h", "qla_df.h", "qla_f2.h",
+              "qla_d2.h", "qla_df2.h"):
         txt = open(os.path.join(os.path.dirname(T.REF_SO), "gen", "include", h)).read()
         for m in re.finditer(r"void (QLA_\w+) \((.*?)\);", txt):
             params = [p.replace("QLA_RESTRICT", "").strip() for p in m.group(2).split(",")]
@@ -455,7 +456,7 @@ def test_oracle_precision_conversions_match_reference_library():
 
 
 @pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
-@pytest.mark.parametrize("lib", ["FN", "DN", "DFN"])
+@pytest.mark.parametrize("lib", ["FN", "DN", "DFN", "F2", "D2", "DF2"])
 def test_oracle_ncolor_families_match_reference_library(lib):
     """The element-wise, site-local product, fill / component / gamma /
     trace families, global P / adjoint-form reductions, sums and conversions
@@ -473,7 +474,8 @@ def test_oracle_ncolor_families_match_reference_library(lib):
         if e["pc"] != lib or e["family"] not in T.NCOLOR_FAMILIES:
             continue
         twin = byname[T.fixed_colour_twin(e["name"])]
-        for nc in (2, 5):
+        two = lib.endswith("2")
+        for nc in ((2,) if two else (2, 5)):
             (ins, idx, gang, ints), want, kind = T.ncolor_case(twin, rng, n, ns, nc)
             if "mu" in ints:
                 ints["mu"] = count % 16
@@ -481,11 +483,11 @@ def test_oracle_ncolor_families_match_reference_library(lib):
             r = np.zeros_like(want) if kind in ("gred", "gsum") else ins["r"][2].copy()
             args, keep = _ref_args(twin, ins, idx, gang, n, r, ints, nc=nc)
             with T.ref_one_thread():
-                getattr(R, e["name"])(nc, *args)
+                getattr(R, e["name"])(*(([] if two else [nc]) + args))
             count += 1
             if not T.bits_equal(r, want):
                 bad.append((e["name"], nc))
-    assert count > (150 if lib == "DFN" else 2000)
+    assert count > ((75 if two else 150) if lib.startswith("DF") else (1000 if two else 2000))
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
 
 
@@ -635,6 +637,8 @@ def test_oracle_random_fills_match_reference_library(milc):
             twin = e
             if e["pc"] in ("FN", "DN"):
                 twin, nc, lead = byname[T.fixed_colour_twin(e["name"])], 2, [2]
+            elif e["pc"] in ("F2", "D2"):
+                twin, nc, lead = byname[T.fixed_colour_twin(e["name"])], 2, []
             if milc and twin.get("op") != "gaussian":
                 continue
             ins, idx, gang, ints, want_r, want_s = T.random_case(twin, rng, n, ns, nc=nc, milc=milc)
@@ -650,7 +654,7 @@ def test_oracle_random_fills_match_reference_library(milc):
                 bad.append(e["name"])
     finally:
         flag.value = 0
-    assert count >= (88 if milc else 120)
+    assert count >= (128 if milc else 160)
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:8]}"
 
 
