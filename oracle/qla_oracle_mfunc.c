@@ -5,7 +5,7 @@
  * code templates, in F and D precision, for any colour count up to 16 (the
  * reference's QLA_F3/D3 and QLA_FN/DN builds of the same templates).  The
  * libm calls of the F build are the float ones (sqrtf, acosf, cbrtf,
- * sincosf, atan2f, copysignf), as in the templates' QLA_Precision == 'F'
+ * sincosf, atan2f, copysignf, sinhf, expf), as in the templates' QLA_Precision == 'F'
  * branch and lib/cmath.
  */
 #define _GNU_SOURCE
@@ -25,6 +25,8 @@
 #define M_SINCOS sincosf
 #define M_ATAN2 atan2f
 #define M_COPYSIGN copysignf
+#define M_SINH sinhf
+#define M_EXP expf
 #include "qla_oracle_mfunc_body.h"
 #undef R
 #undef SFX
@@ -35,6 +37,8 @@
 #undef M_SINCOS
 #undef M_ATAN2
 #undef M_COPYSIGN
+#undef M_SINH
+#undef M_EXP
 
 #define R double
 #define SFX d
@@ -45,6 +49,8 @@
 #define M_SINCOS sincos
 #define M_ATAN2 atan2
 #define M_COPYSIGN copysign
+#define M_SINH sinh
+#define M_EXP exp
 #include "qla_oracle_mfunc_body.h"
 #undef R
 #undef SFX

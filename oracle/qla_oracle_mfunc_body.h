@@ -3,7 +3,7 @@
  * templates (the C files under lib/perl/code-templates), precision-generic.  Included twice
  * by qla_oracle_mfunc.c with R = float / double and SFX = f / d, mirroring the
  * reference's F and D builds of the same templates.  nc is a run-time colour
- * count (<= ORA_NCMAX), as in the reference's N-colour build; for nc == 3 the
+ * count (<= ORA_NCMAX), as in the reference's N-colour build; for nc == 2 and 3 the
  * closed forms of the templates are used where the templates have them.
  *
  * Every helper restates the generated level-1 function the template calls
@@ -920,11 +920,277 @@ static void FN(eig_qr)(FN(mc) *v, const FN(mc) *a, int nc, int herm)
 #undef CNORM2
 }
 
+/* --------------------------------------------- closed forms for nc = 2 */
+/* The templates' `if(NC==2)` branches, compiled into the two-colour
+ * libraries and taken by the N-colour libraries at nc = 2.  Each operation
+ * restates the complex macro the template calls (include/qla_complex.h):
+ * QLA_c_eq_r_div_c t = a / |b|^2 in R; QLA_c_eq_c_div_c t = 1.0 / |b|^2 in
+ * double, rounded; QLA_c_eq_c_times_c_plus_c left to right. */
+
+/* QLA_F_cexp / QLA_D_cexp (lib/cmath/QLA_cexp.c, the compiled branch) */
+static FN(mc) FN(cexp)(FN(mc) a)
+{
+  R mag = M_EXP(a.re);
+  R s, c;
+  M_SINCOS(a.im, &s, &c);
+  FN(mc) z; z.re = mag*c; z.im = mag*s;
+  return z;
+}
+
+/* QLA_F_clog / QLA_D_clog (lib/cmath/QLA_clog.c): log in double */
+static FN(mc) FN(clog)(FN(mc) a)
+{
+  FN(mc) z;
+  z.re = 0.5*log(a.re*a.re + a.im*a.im);
+  z.im = M_ATAN2(a.im, a.re);
+  return z;
+}
+
+/* QLA_F_csinhcosh / QLA_D_csinhcosh (lib/cmath/QLA_csinhcosh.c, the
+ * compiled branch: cosh x = sqrt(1 + sinh^2 x)) */
+static void FN(csinhcosh)(FN(mc) a, FN(mc) *sh, FN(mc) *ch)
+{
+  R sx = M_SINH(a.re);
+  R cx = M_SQRT(1+sx*sx);
+  R sy, cy;
+  M_SINCOS(a.im, &sy, &cy);
+  sh->re = cy*sx; sh->im = sy*cx;
+  ch->re = cy*cx; ch->im = sy*sx;
+}
+
+static void FN(rdivc)(FN(mc) *c, int a, FN(mc) b)     /* QLA_c_eq_r_div_c, a integer */
+{
+  R t = a/(b.re*b.re + b.im*b.im);
+  c->re = t*b.re;
+  c->im = -t*b.im;
+}
+
+#define CTCPC(r, p, x, q) { (r).re = (p).re*(x).re - (p).im*(x).im + (q).re; \
+                            (r).im = (p).re*(x).im + (p).im*(x).re + (q).im; }
+#define CEQM(r, p, q) { (r).re = -(p).re*(q).re + (p).im*(q).im; (r).im = -(p).re*(q).im - (p).im*(q).re; }
+/* r = c0 + c1 a for complex c0, c1 */
+#define OUT_C(r, c0, c1, a00, a01, a10, a11) { CTCPC(r[0], c1, a00, c0); CMUL(r[1], c1, a01); \
+                                              CMUL(r[2], c1, a10); CTCPC(r[3], c1, a11, c0); }
+/* r = c0 + c1 a for real c0, c1 (QLA_c_eq_c_times_r_plus_r, QLA_c_eq_c_times_r) */
+#define OUT_R(r, c0, c1, a00, a01, a10, a11) { \
+    r[0].re = a00.re*(c1) + (c0); r[0].im = a00.im*(c1); \
+    r[1].re = (c1)*a01.re; r[1].im = (c1)*a01.im; \
+    r[2].re = (c1)*a10.re; r[2].im = (c1)*a10.im; \
+    r[3].re = a11.re*(c1) + (c0); r[3].im = a11.im*(c1); }
+
+/* M_eq_exp_M.c:257-291 */
+static void FN(exp2)(FN(mc) *r, const FN(mc) *a)
+{
+  FN(mc) a00 = a[0], a01 = a[1], a10 = a[2], a11 = a[3], tr, s, mdet, t, st, ch, c0, c1, es;
+  tr.re = a00.re + a11.re; tr.im = a00.im + a11.im;
+  s.re = 0.5*tr.re; s.im = 0.5*tr.im;
+  a00.re -= s.re; a00.im -= s.im;
+  a11.re -= s.re; a11.im -= s.im;
+  CMUL(mdet, a01, a10);
+  CMMS(mdet, a00, a11);
+  t = FN(csqrt)(mdet);
+  if (t.re == 0 && t.im == 0) {
+    st.re = 1; st.im = 0;
+    ch.re = 1; ch.im = 0;
+  } else {
+    FN(mc) sh;
+    FN(csinhcosh)(t, &sh, &ch);
+    FN(cdiv)(&st, sh, t);
+  }
+  es = FN(cexp)(s);
+  CMUL(c0, es, ch);
+  CMUL(c1, es, st);
+  OUT_C(r, c0, c1, a00, a01, a10, a11);
+}
+
+/* eigenvalues l0, l1 of a 2x2 matrix, as M_eq_sqrt_M.c:94-115 and
+ * M_eq_invsqrt_M.c:95-116 compute them (the eig2_g arithmetic) */
+static void FN(sqrt2_common)(FN(mc) *r, const FN(mc) *a, int inv)
+{
+  FN(mc) l0, l1, sl0, sl1, ss, ps, c0, c1, tr;
+  FN(eig2_g)(&l0, &l1, &a[0], &a[1], &a[2], &a[3]);
+  tr.re = a[0].re + a[3].re; tr.im = a[0].im + a[3].im;
+  sl0 = FN(csqrt)(l0);
+  sl1 = FN(csqrt)(l1);
+  ss.re = sl0.re + sl1.re; ss.im = sl0.im + sl1.im;
+  CMUL(ps, sl0, sl1);
+  if (!inv) {                                  /* M_eq_sqrt_M.c:116-132 */
+    if (ss.re == 0 && ss.im == 0) {
+      c0 = sl0;
+      c1.re = 0; c1.im = 0;
+    } else {
+      FN(rdivc)(&c1, 1, ss);
+      CMUL(c0, ps, c1);
+    }
+  } else {                                     /* M_eq_invsqrt_M.c:117-131 */
+    FN(mc) t;
+    CMUL(t, ps, ss);
+    FN(rdivc)(&c1, -1, t);
+    ps.re += tr.re; ps.im += tr.im;
+    CEQM(c0, ps, c1);
+  }
+  OUT_C(r, c0, c1, a[0], a[1], a[2], a[3]);
+}
+
+/* M_eq_log_M.c:103-152 */
+static void FN(log2)(FN(mc) *r, const FN(mc) *a)
+{
+  FN(mc) tr, s, det, d, c0, c1;
+  tr.re = a[0].re + a[3].re; tr.im = a[0].im + a[3].im;
+  s.re = 0.5*tr.re; s.im = 0.5*tr.im;
+  CMUL(det, a[0], a[3]);
+  CMMS(det, a[1], a[2]);
+  CMUL(d, s, s);
+  d.re -= det.re; d.im -= det.im;
+  if (d.re == 0 && d.im == 0) {
+    FN(mc) ls = FN(clog)(s);
+    c0.re = 0; c0.im = 0;
+    FN(cdiv)(&c1, ls, s);
+  } else {
+    FN(mc) e0, e1, de, sd = FN(csqrt)(d), le0, le1, dei, dl, dl0;
+    R ts = s.re*sd.re + s.im*sd.im;
+    if (ts >= 0) {
+      e1.re = s.re + sd.re; e1.im = s.im + sd.im;
+      de.re = 2*sd.re; de.im = 2*sd.im;
+    } else {
+      e1.re = s.re - sd.re; e1.im = s.im - sd.im;
+      de.re = -2*sd.re; de.im = -2*sd.im;
+    }
+    FN(cdiv)(&e0, det, e1);
+    le0 = FN(clog)(e0);
+    le1 = FN(clog)(e1);
+    FN(rdivc)(&dei, 1, de);
+    dl.re = le1.re - le0.re; dl.im = le1.im - le0.im;
+    CMUL(dl0, e1, le0);
+    CMMS(dl0, e0, le1);
+    CMUL(c1, dl, dei);
+    CMUL(c0, dl0, dei);
+  }
+  OUT_C(r, c0, c1, a[0], a[1], a[2], a[3]);
+}
+
+/* M_eq_expA_M.c:312-350 (with_trace) and M_eq_expTA_M.c:301-329 */
+static void FN(expah2)(FN(mc) *r, const FN(mc) *a, int with_trace)
+{
+  FN(mc) a00 = a[0], a01 = a[1], a10 = a[2], a11 = a[3];
+  R det, t;
+  if (with_trace) {
+    FN(mc) tr, s, sc, c0, c1, es;
+    R st, cs;
+    tr.re = a00.re + a11.re; tr.im = a00.im + a11.im;
+    s.re = 0.5*tr.re; s.im = 0.5*tr.im;
+    a00.re -= s.re; a00.im -= s.im;
+    a11.re -= s.re; a11.im -= s.im;
+    det = a00.re*a11.re - a00.im*a11.im;
+    det -= (a01.re*a10.re - a01.im*a10.im);
+    t = M_SQRT(M_FABS(det));
+    if (t == 0) {
+      st = 1;
+      cs = 1;
+    } else {
+      sc = FN(cexpi)(t);
+      st = sc.im/t;
+      cs = sc.re;
+    }
+    es = FN(cexpi)(s.im);
+    c0.re = cs*es.re; c0.im = cs*es.im;
+    c1.re = st*es.re; c1.im = st*es.im;
+    OUT_C(r, c0, c1, a00, a01, a10, a11);
+  } else {
+    R c0, c1;
+    det = a00.re*a11.re - a00.im*a11.im;
+    det -= (a01.re*a10.re - a01.im*a10.im);
+    t = M_SQRT(M_FABS(det));
+    if (t == 0) {
+      c0 = 1;
+      c1 = 1;
+    } else {
+      FN(mc) sc = FN(cexpi)(t);
+      c0 = sc.re;
+      c1 = sc.im/t;
+    }
+    OUT_R(r, c0, c1, a00, a01, a10, a11);
+  }
+}
+
+/* M_eq_sqrtPH_M.c:224-262 (inv = 0) and M_eq_invsqrtPH_M.c:228-251 */
+static void FN(sqrtph2)(FN(mc) *r, const FN(mc) *a, int inv)
+{
+  const FN(mc) a00 = a[0], a01 = a[1], a10 = a[2], a11 = a[3];
+  R tr, det, sdet, c0, c1;
+  det = a00.re*a11.re - a00.im*a11.im;
+  det -= (a01.re*a10.re - a01.im*a10.im);
+  tr = a00.re + a11.re;
+  if (inv) {
+    sdet = M_SQRT(M_FABS(det));
+    c1 = 1/(sdet*M_SQRT(M_FABS(tr+2*sdet)));
+    c0 = (tr+sdet)*c1;
+    c1 = -c1;
+    OUT_R(r, c0, c1, a00, a01, a10, a11);
+  } else if (det == 0) {
+    if (tr == 0) {
+      for (int k = 0; k < 4; k++) { r[k].re = 0; r[k].im = 0; }
+    } else {
+      c1 = 1/M_SQRT(M_FABS(tr));
+      r[0].re = c1*a00.re; r[0].im = c1*a00.im;
+      r[1].re = c1*a01.re; r[1].im = c1*a01.im;
+      r[2].re = c1*a10.re; r[2].im = c1*a10.im;
+      r[3].re = c1*a11.re; r[3].im = c1*a11.im;
+    }
+  } else {
+    sdet = M_SQRT(M_FABS(det));
+    c1 = 1/M_SQRT(M_FABS(tr+2*sdet));
+    c0 = sdet*c1;
+    OUT_R(r, c0, c1, a00, a01, a10, a11);
+  }
+}
+
+/* C_eq_det_M.c:63-69, M_eq_inverse_M.c:64-78 */
+static void FN(det2)(FN(mc) *det, const FN(mc) *a)
+{
+  CMUL(*det, a[0], a[3]);
+  CMMS(*det, a[1], a[2]);
+}
+
+static void FN(inverse2)(FN(mc) *x, const FN(mc) *a)
+{
+  FN(mc) det, idet;
+  FN(det2)(&det, a);
+  FN(rdivc)(&idet, 1, det);
+  CMUL(x[0], a[3], idet);
+  CEQM(x[1], a[1], idet);
+  CEQM(x[2], a[2], idet);
+  CMUL(x[3], a[0], idet);
+}
+
+/* V_eq_M_inverse_V.c:65-83 (nb = 1), M_eq_M_inverse_M.c:65-91 (nb = 2) */
+static void FN(minv2)(FN(mc) *x, const FN(mc) *a, const FN(mc) *b, int nb)
+{
+  FN(mc) det, idet, rr[4];
+  FN(det2)(&det, a);
+  FN(rdivc)(&idet, 1, det);
+  for (int j = 0; j < nb; j++) {
+    CMUL(rr[j], a[3], b[j]);
+    CMMS(rr[j], a[1], b[nb + j]);
+    CMUL(rr[nb + j], a[0], b[nb + j]);
+    CMMS(rr[nb + j], a[2], b[j]);
+  }
+  for (int k = 0; k < 2 * nb; k++) CMUL(x[k], rr[k], idet);
+}
+#undef CTCPC
+#undef CEQM
+#undef OUT_C
+#undef OUT_R
+
 /* x = a^-1 b for b with nb columns (a ColorVector: nb = 1; a ColorMatrix:
  * nb = nc): V_eq_M_inverse_V.c:84-126 for nc = 3 and nb = 1 (Cramer's
  * rule), else Gauss-Jordan (V_eq_M_inverse_V.c:128-168, M_eq_M_inverse_M.c:85-135) */
 static void FN(minv1)(FN(mc) *x, const FN(mc) *a, const FN(mc) *b, int nc, int nb)
 {
+  if (nc == 2) {
+    FN(minv2)(x, a, b, nb);
+    return;
+  }
   if (nc == 3 && nb == 1) {
     FN(mc) det0, det1, det2, det, idet, r0, r1, r2;
     CMUL(det2, a[0], a[4]); CMMS(det2, a[1], a[3]);
@@ -960,8 +1226,8 @@ static void FN(minv1)(FN(mc) *x, const FN(mc) *a, const FN(mc) *b, int nc, int n
 
 /* ------------------------------------------------------------ v-forms */
 /* r[i] = f(a[i]); eigenvalue functions write nc complex numbers per site,
- * det one.  The closed nc = 3 forms exist only for nc == 3; other colour
- * counts take the templates' generic paths (expA / expTA: the exp path;
+ * det one.  nc = 2 takes the templates' two-colour closed forms; the
+ * closed nc = 3 forms exist only for nc == 3; other colour counts take the templates' generic paths (expA / expTA: the exp path;
  * sqrtPH / invsqrtPH: the Newton paths; eigenvalues: Hessenberg + QR). */
 int FN(ora_mfunc)(R *r, const R *a, long n, int nc, int which)
 {
@@ -971,6 +1237,24 @@ int FN(ora_mfunc)(R *r, const R *a, long n, int nc, int which)
   for (long i = 0; i < n; i++) {
     const FN(mc) *ai = A + i * nc * nc;
     FN(mc) *oi = O + i * nc * nc;
+    if (nc == 2) {
+      switch (which) {
+      case ORA_MF_EXP: FN(exp2)(oi, ai); break;
+      case ORA_MF_SQRT: FN(sqrt2_common)(oi, ai, 0); break;
+      case ORA_MF_INVERSE: FN(inverse2)(oi, ai); break;
+      case ORA_MF_DET: FN(det2)(O + i, ai); break;
+      case ORA_MF_INVSQRT: FN(sqrt2_common)(oi, ai, 1); break;
+      case ORA_MF_LOG: FN(log2)(oi, ai); break;
+      case ORA_MF_EXPA: FN(expah2)(oi, ai, 1); break;
+      case ORA_MF_EXPTA: FN(expah2)(oi, ai, 0); break;
+      case ORA_MF_SQRTPH: FN(sqrtph2)(oi, ai, 0); break;
+      case ORA_MF_INVSQRTPH: FN(sqrtph2)(oi, ai, 1); break;
+      case ORA_MF_EIGENVALS: FN(eig2_g)(O + i * 2, O + i * 2 + 1, ai, ai + 1, ai + 2, ai + 3); break;
+      case ORA_MF_EIGENVALSH: FN(eig2_h)(O + i * 2, O + i * 2 + 1, ai, ai + 1, ai + 2, ai + 3); break;
+      default: return -1;
+      }
+      continue;
+    }
     switch (which) {
     case ORA_MF_EXP: FN(exp1)(oi, ai, nc); break;
     case ORA_MF_SQRT: FN(sqrt1)(oi, ai, nc, eps); break;

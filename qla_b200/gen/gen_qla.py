@@ -111,16 +111,30 @@ INT_BINOPS = {"and": "IC_AND", "divide": "IC_DIVIDE", "eq": "IC_EQ", "ge": "IC_G
 
 
 FN_NCS = [2, 3, 4, 8]          # colour counts with compiled QLA_FN_ kernels
-FN_MFUNC_NCS = [3, 4, 8]       # nc = 1, 2 use complex libm closed forms in the reference
-# remaining matrix functions for QLA_FN_: nc -> OP (closed forms at nc = 3,
-# the templates' generic exp / Newton paths otherwise)
+FN_MFUNC_NCS = [2, 3, 4, 8]    # nc = 2: the templates' two-colour closed forms
+# the two-colour closed-form OP of each matrix function (qla_mfunc_nc2.cuh)
+NC2_FN = {"exp": "N2_EXP", "sqrt": "N2_SQRT", "invsqrt": "N2_INVSQRT", "log": "N2_LOG", "expA": "N2_EXPA",
+          "expTA": "N2_EXPTA", "sqrtPH": "N2_SQRTPH", "invsqrtPH": "N2_INVSQRTPH", "inverse": "N2_INVERSE",
+          "det": "N2_DET", "eigenvals": "N2_EIG", "eigenvalsH": "N2_EIGH"}
+
+
+def _nc2_op(fname, R="float"):
+    return f"Nc2MfuncOp<{R}, qlab::{NC2_FN[fname]}>"
+
+
+# remaining matrix functions for QLA_FN_: nc -> OP (closed forms at nc = 2
+# and 3, the templates' generic exp / Newton paths otherwise)
 FN_MFUNC_EXT = {
-    "invsqrt": lambda nc: f"GenMfuncExtOp<float, {nc}, 0>",
-    "log": lambda nc: f"GenMfuncExtOp<float, {nc}, 1>",
-    "expA": lambda nc: "ExpAHOp<float, true>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 2>",
-    "expTA": lambda nc: "ExpAHOp<float, false>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 2>",
-    "sqrtPH": lambda nc: "SqrtPHOp<float, false>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 3>",
-    "invsqrtPH": lambda nc: "SqrtPHOp<float, true>" if nc == 3 else f"GenMfuncExtOp<float, {nc}, 4>",
+    "invsqrt": lambda nc: _nc2_op("invsqrt") if nc == 2 else f"GenMfuncExtOp<float, {nc}, 0>",
+    "log": lambda nc: _nc2_op("log") if nc == 2 else f"GenMfuncExtOp<float, {nc}, 1>",
+    "expA": lambda nc: (_nc2_op("expA") if nc == 2 else "ExpAHOp<float, true>" if nc == 3
+                        else f"GenMfuncExtOp<float, {nc}, 2>"),
+    "expTA": lambda nc: (_nc2_op("expTA") if nc == 2 else "ExpAHOp<float, false>" if nc == 3
+                         else f"GenMfuncExtOp<float, {nc}, 2>"),
+    "sqrtPH": lambda nc: (_nc2_op("sqrtPH") if nc == 2 else "SqrtPHOp<float, false>" if nc == 3
+                          else f"GenMfuncExtOp<float, {nc}, 3>"),
+    "invsqrtPH": lambda nc: (_nc2_op("invsqrtPH") if nc == 2 else "SqrtPHOp<float, true>" if nc == 3
+                             else f"GenMfuncExtOp<float, {nc}, 4>"),
 }
 
 
@@ -246,16 +260,17 @@ def gen_fn(prec="F"):
         for src, p1 in [("M", False), ("pM", True)]:
             for fname, opname in (("exp", "GenExpOp"), ("sqrt", "GenSqrtOp"), ("inverse", "GenInverseOp")):
                 name = f"QLA_{LIB}_M_{var}eq_{fname}_{src}"
-                call = lambda nc, opname=opname, p1=p1, gang=gang: (
-                    f"qlab::api_map<qlab::{opname}<{R}, {nc}>>({kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
+                call = lambda nc, opname=opname, fname=fname, p1=p1, gang=gang: (
+                    f"qlab::api_map<qlab::{_nc2_op(fname, R) if nc == 2 else f'{opname}<{R}, {nc}>'}>("
+                    f"{kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
                     f"{gang}, n, qlab::EQ);")
                 add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
                     _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
                     dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
             name = f"QLA_{LIB}_C_{var}eq_det_{src}"
             call = lambda nc, p1=p1, gang=gang: (
-                f"qlab::api_map<qlab::GenDetOp<{R}, {nc}>>({kid('mfunc')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, "
-                f"{gang}, n, qlab::EQ);")
+                f"qlab::api_map<qlab::{_nc2_op('det', R) if nc == 2 else f'GenDetOp<{R}, {nc}>'}>({kid('mfunc')}, r, "
+                f"{opnd(p1, 'a')}, qlab::Opnd{{}}, {gang}, n, qlab::EQ);")
             add(name, [(f"QLA_{prec}_Complex *", "r"), ("void *", "a")] + tail + [("int", "n")],
                 _fn_switch(FN_MFUNC_NCS, call, name), "mfunc", CITE["mfunc"],
                 dict(dest="C", eqop="eq", var=var, a=src, fn="det"))
@@ -272,8 +287,9 @@ def gen_fn(prec="F"):
                     dict(dest="M", eqop="eq", var=var, a=src, fn=fname))
             for fname, opn, herm in (("eigenvals", "EigenvalsOp", "false"), ("eigenvalsH", "EigenvalsHOp", "true")):
                 name = f"QLA_{LIB}_V_{var}eq_{fname}_{src}"
-                call = lambda nc, opn=opn, herm=herm, p1=p1, gang=gang: (
-                    f"qlab::api_map<qlab::{opn + '<' + R + '>' if nc == 3 else f'GenEigenOp<{R}, {nc}, {herm}>'}>("
+                call = lambda nc, opn=opn, herm=herm, fname=fname, p1=p1, gang=gang: (
+                    f"qlab::api_map<qlab::"
+                    f"{_nc2_op(fname, R) if nc == 2 else opn + '<' + R + '>' if nc == 3 else f'GenEigenOp<{R}, {nc}, {herm}>'}>("
                     f"{kid('mfunc_ext')}, r, {opnd(p1, 'a')}, qlab::Opnd{{}}, {gang}, n, qlab::EQ);")
                 add(name, [("void *", "r"), ("void *", "a")] + tail + [("int", "n")],
                     _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["mfunc_ext"],
@@ -283,8 +299,9 @@ def gen_fn(prec="F"):
                 for s2, p2 in ((T_, False), ("p" + T_, True)):
                     name = f"QLA_{LIB}_{T_}_{var}eq_{s1}_inverse_{s2}"
                     call = lambda nc, T_=T_, p1=p1, p2=p2, gang=gang: (
-                        f"qlab::api_map<qlab::GenMInverseOp<{R}, {nc}, {1 if T_ == 'V' else nc}>>({kid('minv')}, r, "
-                        f"{opnd(p1, 'a')}, {opnd(p2, 'b')}, {gang}, n, qlab::EQ);")
+                        f"qlab::api_map<qlab::"
+                        f"{f'Nc2MInverseOp<{R}, ' if nc == 2 else f'GenMInverseOp<{R}, {nc}, '}{1 if T_ == 'V' else nc}>>("
+                        f"{kid('minv')}, r, {opnd(p1, 'a')}, {opnd(p2, 'b')}, {gang}, n, qlab::EQ);")
                     add(name, [("void *", "r"), ("void *", "a"), ("void *", "b")] + tail + [("int", "n")],
                         _fn_switch(FN_MFUNC_NCS, call, name), "mfunc_ext", CITE["minv"],
                         dict(dest=T_, eqop="eq", var=var, a=s1, b=s2, fn="inverse_" + T_))
@@ -1492,10 +1509,8 @@ def main():
                 "ldot", "fill", "mask", "component", "gamma", "trace", "gred", "gsum", "convert", "prop", "multi",
                 "random")):
             extra = '#include "../qla_ncolor.cuh"\n#include "../qla_random.cuh"\n'
-        if pc in ("FN", "DN", "F2", "D2") and family == "mfunc":
-            extra = '#include "../qla_mfunc_generic.cuh"\n'
-        if pc in ("FN", "DN", "F2", "D2") and family == "mfunc_ext":
-            extra = '#include "../qla_mfunc_generic_ext.cuh"\n'
+        if pc in ("FN", "DN", "F2", "D2") and family in ("mfunc", "mfunc_ext"):
+            extra = '#include "../qla_mfunc_nc2.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:
             text += "QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  " + fn.body + "\n}\n\n"

@@ -1,6 +1,7 @@
 """GPU parity of the QLA_FN_ / QLA_DFN_ and QLA_DN_ entry points (colour
 count nc at run time) against the oracle, through the C-ABI, for every
-compiled nc (2, 3, 4, 8; matrix functions 3, 4, 8).  Linear ops and the
+compiled nc (2, 3, 4, 8; matrix functions at nc = 2 by the templates'
+two-colour closed forms).  Linear ops and the
 matrix functions on the templates' generic paths (Pade exp, Newton sqrt,
 Gauss-Jordan inverse, LU det, restated in float for FN and in double for DN)
 must be bit-identical; reductions follow the tolerances of
@@ -176,6 +177,58 @@ def test_fn_remaining_matrix_functions(qla, nc, lib, dt, rlib):
         pb = T.ptr_array(b_d, ib, 2 * np.dtype(dt).itemsize * nc * nb)
         getattr(qla, lib).__getattr__(f"{t}_veq_M_inverse_p{t}")(nc, r_d, T.to_dev(gen), pb, n)
         assert T.bits_equal(T.to_host(r_d), T.ora_minv(gen, b, n, nb, nc=nc, idx_b=ib)), (nc, t)
+
+
+@pytest.mark.parametrize("lib,dt,rlib", PRECS)
+def test_fn_two_colour_matrix_functions(qla, lib, dt, rlib):
+    """nc = 2 takes the templates' two-colour closed forms (the oracle's are
+    pinned to the reference's F2 / D2 and FN / DN builds).  sqrt, invsqrt,
+    sqrtPH, invsqrtPH, inverse, det, eigenvalues and a^-1 b are bit-identical,
+    zero and singular inputs included; exp, log, expA and expTA call CUDA's
+    sinh / exp / sincos / log / atan2 where the reference calls the host
+    libm: within 64 eps of max(1, max |r|) per site (the test prints the
+    fraction of sites that are bit-identical)."""
+    rng = np.random.default_rng(92)
+    n, nc = 4099, 2
+    gen = (rng.standard_normal((n, 8)) * 0.7).astype(dt)
+    z = T.to_complex(gen.astype(np.float64), nc)
+    ah = T.from_complex(0.5 * (z - np.conj(np.transpose(z, (0, 2, 1)))), dt)
+    aht = T.from_complex(T.to_complex(ah.astype(np.float64), nc)
+                         + 1j * rng.uniform(-1, 1, n)[:, None, None] * np.eye(2), dt)
+    pos = T.positive_hermitian_inputs(rng, n, dt, nc=nc)
+    herm = T.hermitian_inputs(rng, n, dt, nc=nc)
+    u = rng.standard_normal((n, 2)) + 1j * rng.standard_normal((n, 2))
+    rank1 = np.einsum("ni,nj->nij", u, np.conj(u))
+    rank1[::7] = 0
+    psd1 = T.from_complex(rank1, dt)
+    scal = T.from_complex((rng.uniform(0.5, 2, n) + 1j * rng.uniform(-1, 1, n))[:, None, None] * np.eye(2), dt)
+    exact = [("sqrt", pos), ("sqrt", gen), ("sqrt", psd1), ("invsqrt", pos), ("invsqrt", gen), ("inverse", gen),
+             ("det", gen), ("det", psd1), ("sqrtPH", pos), ("sqrtPH", psd1), ("invsqrtPH", pos),
+             ("eigenvals", gen), ("eigenvals", psd1), ("eigenvalsH", herm), ("eigenvalsH", psd1)]
+    approx = [("exp", gen), ("exp", ah), ("exp", scal), ("log", pos), ("log", gen), ("log", scal),
+              ("expA", aht), ("expA", ah), ("expTA", ah)]
+    eps = np.finfo(dt).eps
+    for k, (fname, src) in enumerate(exact + approx):
+        dest = "C" if fname == "det" else "V" if fname.startswith("eigen") else "M"
+        nout = {"C": 1, "V": 2, "M": 4}[dest]
+        r_d = T.to_dev(np.zeros((n, 2 * nout), dt))
+        getattr(qla, lib).__getattr__(f"{dest}_veq_{fname}_M")(nc, r_d, T.to_dev(src), n)
+        got = T.to_host(r_d)
+        want = T.ora_mfunc(src, n, fname, nc=nc)
+        if k < len(exact):
+            assert T.bits_equal(got, want), (lib, fname)
+        else:
+            scale = np.maximum(1.0, np.max(np.abs(want.astype(np.float64)), axis=1))[:, None]
+            assert np.all(np.abs(got.astype(np.float64) - want) <= 64 * eps * scale), (lib, fname)
+            print(f"{lib} nc=2 {fname}: sites bit-identical {np.mean(np.all(got == want, axis=1)):.4f}")
+    for t, nb in (("V", 1), ("M", 2)):
+        b = rng.standard_normal((n, 4 * nb)).astype(dt)
+        ib = rng.permutation(n).astype(np.int32)
+        r_d = T.to_dev(np.zeros((n, 4 * nb), dt))
+        b_d = T.to_dev(b)
+        pb = T.ptr_array(b_d, ib, 2 * np.dtype(dt).itemsize * nc * nb)
+        getattr(qla, lib).__getattr__(f"{t}_veq_M_inverse_p{t}")(nc, r_d, T.to_dev(gen), pb, n)
+        assert T.bits_equal(T.to_host(r_d), T.ora_minv(gen, b, n, nb, nc=nc, idx_b=ib)), (lib, t)
 
 
 def test_fn_unsupported_nc_reports_error(qla):

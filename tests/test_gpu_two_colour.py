@@ -5,8 +5,7 @@ bit for bit afterwards (outputs, and state fields that the random fills
 update).  The N-colour entry points are tested against the oracle at nc = 2
 (tests/test_gpu_ncolor.py, tests/test_gpu_fn.py) and the oracle against the
 reference's two-colour libraries (tests/test_oracle_pin.py).  The matrix
-functions are not built for two colours: both forms must record an error
-and leave their output untouched."""
+functions of both are the templates' two-colour closed forms."""
 import ctypes
 import re
 

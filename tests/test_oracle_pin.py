@@ -315,6 +315,48 @@ def test_oracle_n_colour_matrix_functions_match_reference_library(pc, dt):
             assert T.bits_equal(rr, T.ora_minv(g, b, n, nb, nc=nc)), (nc, dest)
 
 
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+@pytest.mark.parametrize("pc,dt", [("F2", np.float32), ("D2", np.float64), ("FN", np.float32), ("DN", np.float64)])
+def test_oracle_two_colour_matrix_functions_match_reference_library(pc, dt):
+    """The templates' two-colour closed forms (the QLA_F2_/QLA_D2_ builds, and
+    the N-colour builds at nc = 2), every matrix function and a^-1 b, bit for
+    bit on 3,000 sites per input class, including singular and zero inputs
+    of the branches that test for them (det = 0, trace = 0)."""
+    rng = np.random.default_rng(81)
+    n, nc = 3000, 2
+    R = T.ref()
+    lead = [nc] if pc in ("FN", "DN") else []
+    gen = (rng.standard_normal((n, 8)) * 0.7).astype(dt)
+    z = T.to_complex(gen.astype(np.float64), nc)
+    ah = T.from_complex(0.5 * (z - np.conj(np.transpose(z, (0, 2, 1)))), dt)
+    aht = T.from_complex(T.to_complex(ah.astype(np.float64), nc) + 1j * rng.uniform(-1, 1, n)[:, None, None] * np.eye(2),
+                         dt)
+    pos = T.positive_hermitian_inputs(rng, n, dt, nc=nc)
+    herm = T.hermitian_inputs(rng, n, dt, nc=nc)
+    # rank-one and zero matrices (det = 0), scalar multiples of 1 (s^2 - det = 0)
+    u = rng.standard_normal((n, 2)) + 1j * rng.standard_normal((n, 2))
+    rank1 = np.einsum("ni,nj->nij", u, np.conj(u))
+    rank1[::7] = 0
+    psd1 = T.from_complex(rank1, dt)
+    scal = T.from_complex((rng.uniform(0.5, 2, n) + 1j * rng.uniform(-1, 1, n))[:, None, None] * np.eye(2), dt)
+    cases = [("exp", gen), ("exp", ah), ("exp", scal), ("sqrt", pos), ("sqrt", gen), ("sqrt", psd1),
+             ("invsqrt", pos), ("invsqrt", gen), ("inverse", gen), ("det", gen), ("det", psd1),
+             ("log", pos), ("log", gen), ("log", scal), ("expA", aht), ("expA", ah), ("expTA", ah),
+             ("sqrtPH", pos), ("sqrtPH", psd1), ("invsqrtPH", pos), ("eigenvals", gen), ("eigenvals", psd1),
+             ("eigenvalsH", herm), ("eigenvalsH", psd1)]
+    for fname, a in cases:
+        dest = "C" if fname == "det" else "V" if fname.startswith("eigen") else "M"
+        nout = {"C": 1, "V": 2, "M": 4}[dest]
+        rr = np.zeros((n, 2 * nout), dt)
+        getattr(R, f"QLA_{pc}_{dest}_veq_{fname}_M")(*(lead + [T.ptr(rr), T.ptr(a), n]))
+        assert T.bits_equal(rr, T.ora_mfunc(a, n, fname, nc=nc)), (pc, fname)
+    for dest, nb in (("V", 1), ("M", 2)):
+        b = T.gaussian_field(rng, n, 2 * nb, dt)
+        rr = np.zeros((n, 4 * nb), dt)
+        getattr(R, f"QLA_{pc}_{dest}_veq_M_inverse_{dest}")(*(lead + [T.ptr(rr), T.ptr(gen), T.ptr(b), n]))
+        assert T.bits_equal(rr, T.ora_minv(gen, b, n, nb, nc=nc)), (pc, dest)
+
+
 def _ref_args(e, ins, idx, gang, n, r, ints=None, nc=3):
     """Host arguments of manifest entry e for the reference library."""
     args, keep = [], []
