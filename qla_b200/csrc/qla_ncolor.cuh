@@ -700,22 +700,18 @@ inline void api_gdot_n(const char* kid, int nc, int ne, int perm, void* r, Opnd 
 // records give each thread up to GSUM_Q components c = t + q * blockDim of
 // every site, sites striding over the blocks.  Either way every component
 // is added in double-double per thread, folded over the threads of a block
-// in a fixed order, and over the blocks by the last block in block order.
+// in a fixed order into per-block partials, and over the blocks by
+// gsum_fold_kernel (one block per component, a fixed order).
 constexpr int GSUM_Q = 8;
 
-template <typename R, typename OUT>
-__global__ void __launch_bounds__(1024) gsumn_kernel(const EwParams p, int NR, int wide, DD* partials,
-                                                     unsigned* counter, OUT* result, int flat) {
+template <typename R, bool WIDE>
+__global__ void __launch_bounds__(1024, WIDE ? 1 : 2) gsumn_kernel(const EwParams p, int NR, DD* partials, int flat) {
   extern __shared__ __align__(16) unsigned char gsnm[];
   DD* red = reinterpret_cast<DD*>(gsnm);
-  __shared__ bool is_last;
   const int BT = blockDim.x;
-  if (!wide) {
+  if constexpr (!WIDE) {
     const int c = threadIdx.x % NR;
-    constexpr int GS_U = 8;  // independent accumulators: loads in flight, folded in a fixed order
-    DD accs[GS_U];
-#pragma unroll
-    for (int u = 0; u < GS_U; u++) accs[u] = DD{0.0, 0.0};
+    DD acc{0.0, 0.0};  // groups of GS_U loads summed by tree_sum, as gsum_kernel
     const long long total = p.n * NR;
     const long long stride = (long long)gridDim.x * BT;
     auto load = [&](long long j) -> double {
@@ -730,13 +726,9 @@ __global__ void __launch_bounds__(1024) gsumn_kernel(const EwParams p, int NR, i
       double v[GS_U];
 #pragma unroll
       for (int u = 0; u < GS_U; u++) v[u] = load(j + u * stride);
-#pragma unroll
-      for (int u = 0; u < GS_U; u++) dd_add(accs[u], v[u]);
+      dd_add(acc, tree_sum(v));
     }
-    for (; j < total; j += stride) dd_add(accs[0], load(j));
-    DD acc = accs[0];
-#pragma unroll
-    for (int u = 1; u < GS_U; u++) dd_merge(acc, accs[u]);
+    for (; j < total; j += stride) dd_add(acc, load(j));
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int q = threadIdx.x; q < NR; q += BT) {
@@ -763,28 +755,6 @@ __global__ void __launch_bounds__(1024) gsumn_kernel(const EwParams p, int NR, i
       if (c < NR) partials[(long long)blockIdx.x * NR + c] = acc[q];
     }
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned ticket = atomicAdd(counter, 1u);
-    is_last = (ticket == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!is_last) return;
-  __threadfence();
-  for (int q = threadIdx.x; q < NR; q += BT) {
-    DD s{0.0, 0.0};
-    for (int b = 0; b < (int)gridDim.x; b++) {
-      volatile DD* vp = reinterpret_cast<volatile DD*>(&partials[(long long)b * NR + q]);
-      DD v;
-      v.hi = vp->hi;
-      v.lo = vp->lo;
-      dd_merge(s, v);
-    }
-    result[q] = static_cast<OUT>(__dadd_rn(s.hi, s.lo));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) *counter = 0u;
 }
 
 template <typename R, typename OUT = R>
@@ -811,7 +781,7 @@ inline void api_gsum_n(const char* kid, int nc, int ne, void* r, Opnd a, const i
   int BT;
   if (!wide) {
     BT = l;
-    while (BT + l <= 512) BT += l;
+    while (BT + l <= 1024) BT += l;
   } else {
     BT = ((NR + GSUM_Q - 1) / GSUM_Q + 31) / 32 * 32;
     if (BT < 256) BT = 256;
@@ -822,7 +792,8 @@ inline void api_gsum_n(const char* kid, int nc, int ne, void* r, Opnd a, const i
   }
   const int sms = device_sm_count();
   long long grid = wide ? (long long)n : ((long long)n * NR + BT - 1) / BT;
-  const long long cap = (long long)sms * 4;
+  const int per_sm = (wide ? 1024 : 2048) / BT;  // resident blocks (registers: 64 / 32 per thread)
+  const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
   const long long need_ll = (grid * NR + ((long long)NR * (long long)sizeof(OUT) + (long long)sizeof(DD) - 1) /
@@ -838,7 +809,12 @@ inline void api_gsum_n(const char* kid, int nc, int ne, void* r, Opnd a, const i
   p.n = n;
   const int flat = (gang == nullptr && a.mode == OM_CONTIG) ? 1 : 0;
   const size_t smem = wide ? 0 : (size_t)BT * sizeof(DD);
-  gsumn_kernel<R, OUT><<<(unsigned)grid, BT, smem, st>>>(p, NR, wide, rs->partials, rs->counter, res, flat);
+  if (wide)
+    gsumn_kernel<R, true><<<(unsigned)grid, BT, smem, st>>>(p, NR, rs->partials, flat);
+  else
+    gsumn_kernel<R, false><<<(unsigned)grid, BT, smem, st>>>(p, NR, rs->partials, flat);
+  if (!check_launch(kid)) return;
+  gsum_fold_kernel<OUT><<<NR, GS_FOLD, 0, st>>>(rs->partials, (int)grid, NR, res);
   if (!check_launch(kid)) return;
   if (!dev_out) {
     if (cudaMemcpyAsync(r, res, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

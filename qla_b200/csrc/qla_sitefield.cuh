@@ -21,7 +21,10 @@
 //
 // Element maps run one thread per output complex number, like the
 // element-wise families: consecutive threads touch consecutive elements of
-// the AoS records, which coalesces for every record size.  Every map here
+// the AoS records, which coalesces for every record size.  The gamma product
+// on D and the antihermitian part run one site per thread on the site
+// engine instead (GammaDOp, AntihermOp), which stages the records with bulk
+// copies.  Every map here
 // only moves values or negates / swaps components, except the trace and the
 // antihermitian part, which repeat the reference's additions in its order;
 // all results are bit-identical to the reference.
@@ -42,7 +45,7 @@ enum SfKind : int {
   SF_TRACE_C,     // C r = trace a
   SF_TRACE_RE,    // R r = Re trace a
   SF_TRACE_IM,    // R r = Im trace a
-  SF_ANTIHERM     // M r = traceless antihermitian part of a
+  SF_ANTIHERM     // M r = traceless antihermitian part of a (N-colour maps; Nc = 3: AntihermOp)
 };
 
 struct SfParams {
@@ -161,25 +164,6 @@ __global__ void __launch_bounds__(256) sf_kernel(const SfParams p, const RecCons
 #pragma unroll
       for (int c = 0; c < 3; c++) x = radd(x, KIND == SF_TRACE_RE ? a[c * 4].re : a[c * 4].im);
       static_cast<R*>(p.out)[k] = x;
-    } else {  // SF_ANTIHERM (build_qla.pl:983-1064)
-      const Cx<R>* a = rec_ptr<R>(p.a, k, 9);
-      const int ic = e / 3, jc = e - 3 * (e / 3);
-      Cx<R> y;
-      if (ic == jc) {
-        // x = sum Im a_cc / 3; r_ii = (0, Im a_ii - x)
-        R x = R(0);
-#pragma unroll
-        for (int c = 0; c < 3; c++) x = radd(x, a[c * 4].im);
-        x = rdiv(x, R(3));
-        y = Cx<R>{R(0), rsub(a[e].im, x)};
-      } else {
-        // x2 = (a_ij - conj(a_ji)) * 0.5 for i < j; r_ij = x2, r_ji = -conj(x2)
-        const int lo = ic < jc ? ic : jc, hi = ic < jc ? jc : ic;
-        const Cx<R> u = a[lo * 3 + hi], v = a[hi * 3 + lo];
-        const Cx<R> x2{rmul(rsub(u.re, v.re), R(0.5)), rmul(radd(u.im, v.im), R(0.5))};
-        y = (ic < jc) ? x2 : Cx<R>{-x2.re, x2.im};
-      }
-      static_cast<Cx<R>*>(p.out)[k * 9 + e] = y;
     }
   }
 }
@@ -389,6 +373,60 @@ inline const GammaTable& gamma_table() {
   return tab;
 }
 
+// D = gamma_mu D through the site engine: one site per thread, the record
+// staged by the engine's bulk copies.  aux packs, per destination spin s,
+// the source spin (bits 4s..4s+1) and the phase (bits 4s+2..4s+3).
+template <typename R_>
+struct GammaDOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 12, N1 = 0, N2 = 0, NOUT = 12, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams& p, const Cx<R> (&a)[N0], const Cx<R> (&)[1],
+                                               const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const int src = (p.aux >> (4 * s)) & 3, ph = (p.aux >> (4 * s + 2)) & 3;
+#pragma unroll
+      for (int ic = 0; ic < 3; ic++) {
+        const Cx<R> v = src == 0 ? a[ic * 4] : src == 1 ? a[ic * 4 + 1] : src == 2 ? a[ic * 4 + 2] : a[ic * 4 + 3];
+        y[ic * 4 + s] = phase_times<R>(ph, v);
+      }
+    }
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
+// M = traceless antihermitian part of M through the site engine
+// (build_qla.pl:983-1064: x = sum Im a_cc / 3, r_ii = i (Im a_ii - x);
+// x2 = (a_ij - conj(a_ji)) 0.5 for i < j, r_ij = x2, r_ji = -conj(x2))
+template <typename R_>
+struct AntihermOp {
+  using R = R_;
+  static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
+  __device__ __forceinline__ static void apply(const SiteParams&, const Cx<R> (&a)[N0], const Cx<R> (&)[1],
+                                               const Cx<R> (&)[1], Cx<R> (&y)[NOUT]) {
+    R x = R(0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) x = radd(x, a[c * 4].im);
+    x = rdiv(x, R(3));
+#pragma unroll
+    for (int c = 0; c < 3; c++) y[c * 4] = Cx<R>{R(0), rsub(a[c * 4].im, x)};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = i + 1; j < 3; j++) {
+        const Cx<R> u = a[i * 3 + j], v = a[j * 3 + i];
+        const Cx<R> x2{rmul(rsub(u.re, v.re), R(0.5)), rmul(radd(u.im, v.im), R(0.5))};
+        y[i * 3 + j] = x2;
+        y[j * 3 + i] = Cx<R>{-x2.re, x2.im};
+      }
+  }
+  __device__ static void accum(const SiteParams&, const Cx<R> (&)[N0], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                               double*) {}
+  __device__ static void finish(const SiteParams&, const double*) {}
+};
+
 // D = gamma_mu D, P = gamma_mu P (LEFT) or P = P gamma_mu
 template <typename R, int NE, bool LEFT>
 inline void api_gamma(const char* kid, void* r, Opnd a, int mu, const int* gang, int n) {
@@ -398,9 +436,23 @@ inline void api_gamma(const char* kid, void* r, Opnd a, int mu, const int* gang,
     set_error(QLAGPU_ERR_ARG, kid, "gamma matrix index outside 0..15");
     return;
   }
+  const GammaTable& t = gamma_table();
+  if constexpr (NE == 12 && LEFT) {
+    if (n <= 0) return;
+    if (!r || !opnd_ok(a)) {
+      set_error(QLAGPU_ERR_NULLPTR, kid, "NULL argument");
+      return;
+    }
+    SiteParams sp = make_params(n, EQ);
+    sp.in[0] = a;
+    sp.out = r;
+    sp.gang = gang;
+    for (int s = 0; s < 4; s++) sp.aux |= (t.row_src[mu][s] | (t.row_ph[mu][s] << 2)) << (4 * s);
+    SiteLauncher<GammaDOp<R>>::run(sp, kid);
+    return;
+  }
   SfParams p;
   if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
-  const GammaTable& t = gamma_table();
   for (int s = 0; s < 4; s++) {
     p.gs[s] = LEFT ? t.row_src[mu][s] : t.col_src[mu][s];
     p.gp[s] = LEFT ? t.row_ph[mu][s] : t.col_ph[mu][s];
@@ -420,9 +472,7 @@ inline void api_trace(const char* kid, void* r, Opnd a, const int* gang, int n) 
 
 template <typename R>
 inline void api_antiherm(const char* kid, void* r, Opnd a, const int* gang, int n) {
-  SfParams p;
-  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
-  sf_launch<R, 9, 9, SF_ANTIHERM>(kid, p, RecConst<R, 1>{});
+  api_map<AntihermOp<R>>(kid, r, a, Opnd{}, gang, n, EQ);
 }
 
 // ---------------------------------------------------------------------------
@@ -464,57 +514,67 @@ __device__ __forceinline__ void gdot_term(const Cx<R>* a, const Cx<R>* b, int e,
   }
 }
 
+// GS_U loads of one component in flight per thread, summed in double as a
+// fixed pairwise tree (error <= (GS_U - 1) double ulps of the group's
+// magnitude), then one double-double add per group: one accumulator keeps
+// the registers low enough for two blocks of up to 1024 threads per SM.
+constexpr int GS_U = 8;
+
+template <int U>
+__device__ __forceinline__ double tree_sum(const double (&v)[U]) {
+  double w[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) w[u] = v[u];
+#pragma unroll
+  for (int h = U / 2; h >= 1; h >>= 1)
+#pragma unroll
+    for (int u = 0; u < h; u++) w[u] = __dadd_rn(w[u], w[u + h]);
+  return w[0];
+}
+
 // Contiguous operands without a gang index: the n * NE complex elements are
-// one flat stream; thread g takes elements g, g + stride, ... with GD_U
-// independent double-double accumulators (GD_U loads in flight), folded in a
-// fixed order, then the block / grid fold of reduce_finish.  The order of the
-// sum differs from the reference's single running double (the global sums
-// are compared to it within the stated tolerance); every term is formed in
-// double exactly as the reference forms it.
-constexpr int GD_U = 4;
+// one flat stream; thread g takes elements g, g + stride, ..., GD_U of them
+// in flight, whose terms are summed in double by a fixed tree and then added
+// in double-double; then the block / grid fold of reduce_finish.  The order
+// of the sum differs from the reference's single running double (the global
+// sums are compared to it within the stated tolerance); every term is formed
+// in double exactly as the reference forms it.  Element positions are only
+// decoded (a 64-bit division by NE) for the permuted (adjoint) forms.
+constexpr int GD_U = 8;
 
 template <typename R, int NE, int KIND, int PERM, typename OUT>
-__global__ void __launch_bounds__(256) gdot_flat_kernel(const EwParams p, const SiteParams rp) {
+__global__ void __launch_bounds__(256, 4) gdot_flat_kernel(const EwParams p, const SiteParams rp) {
   using FIN = GDotFinish<KIND, OUT>;
-  DD accr[GD_U], acci[GD_U];
+  constexpr bool PLAIN = (KIND == LD_DOT || KIND == LD_REDOT || KIND == LD_NORM2);
+  DD acc[ArrN<FIN::NACC>::value];
 #pragma unroll
-  for (int u = 0; u < GD_U; u++) {
-    accr[u] = DD{0.0, 0.0};
-    acci[u] = DD{0.0, 0.0};
-  }
+  for (int a = 0; a < ArrN<FIN::NACC>::value; a++) acc[a] = DD{0.0, 0.0};
   const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
   const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);
   const long long total = p.n * NE;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  for (; g + (GD_U - 1) * stride < total; g += GD_U * stride) {
-#pragma unroll
-    for (int u = 0; u < GD_U; u++) {
-      const long long q = g + u * stride;
+  auto term = [&](long long q, double& tr, double& ti) {
+    if constexpr (PLAIN) {
+      gdot_term<R, NE, KIND, PERM>(A + q, B + q, 0, tr, ti);
+    } else {
       const long long i = q / NE;
       const int e = (int)(q - i * NE);
-      double tr, ti;
       gdot_term<R, NE, KIND, PERM>(A + i * NE, B + i * NE, e, tr, ti);
-      dd_add(accr[u], tr);
-      if constexpr (FIN::NACC > 1) dd_add(acci[u], ti);
     }
+  };
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; g + (GD_U - 1) * stride < total; g += GD_U * stride) {
+    double tr[GD_U], ti[GD_U];
+#pragma unroll
+    for (int u = 0; u < GD_U; u++) term(g + u * stride, tr[u], ti[u]);
+    dd_add(acc[0], tree_sum(tr));
+    if constexpr (FIN::NACC > 1) dd_add(acc[1], tree_sum(ti));
   }
   for (; g < total; g += stride) {
-    const long long i = g / NE;
-    const int e = (int)(g - i * NE);
     double tr, ti;
-    gdot_term<R, NE, KIND, PERM>(A + i * NE, B + i * NE, e, tr, ti);
-    dd_add(accr[0], tr);
-    if constexpr (FIN::NACC > 1) dd_add(acci[0], ti);
-  }
-  DD acc[ArrN<FIN::NACC>::value];
-  acc[0] = accr[0];
-#pragma unroll
-  for (int u = 1; u < GD_U; u++) dd_merge(acc[0], accr[u]);
-  if constexpr (FIN::NACC > 1) {
-    acc[1] = acci[0];
-#pragma unroll
-    for (int u = 1; u < GD_U; u++) dd_merge(acc[1], acci[u]);
+    term(g, tr, ti);
+    dd_add(acc[0], tr);
+    if constexpr (FIN::NACC > 1) dd_add(acc[1], ti);
   }
   reduce_finish<FIN>(rp, acc);
 }
@@ -600,24 +660,22 @@ inline void api_gdot(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
 // component is summed over the sites separately.  A block of BT threads (a
 // multiple of the NR reals per record and of 32) reads the records as one
 // flat stream, so thread t always meets component t % NR and the loads are
-// coalesced; each thread adds in double-double, the block folds the threads
-// of each component in a fixed order into per-block partials, and the last
-// block folds the partials in block order.
+// coalesced; each thread adds groups of GS_U loads in double-double and the
+// block folds the threads of each component in a fixed order into
+// per-block partials.  A
+// second launch (gsum_fold_kernel, one block per component) folds the
+// partials: thread t takes blocks t, t + 128, ... in order, then a fixed
+// shared-memory tree.  For P records (NR = 288) the partials are megabytes,
+// which one block folding them serially would take longer to read than the
+// field itself.
 
-template <typename R, int NR, typename OUT>
-__global__ void __launch_bounds__(1024) gsum_kernel(const EwParams p, DD* partials, unsigned* counter, OUT* result,
-                                                    int flat) {
+template <typename R, int NR>
+__global__ void __launch_bounds__(1024, 2) gsum_kernel(const EwParams p, DD* partials, int flat) {
   extern __shared__ __align__(16) unsigned char gssm[];
   DD* red = reinterpret_cast<DD*>(gssm);
-  __shared__ bool is_last;
   const int BT = blockDim.x;
   const int c = threadIdx.x % NR;
-  // GS_U independent accumulators keep GS_U loads in flight per thread; they
-  // are folded in a fixed order, so the sum is deterministic for a grid
-  constexpr int GS_U = 8;
-  DD accs[GS_U];
-#pragma unroll
-  for (int u = 0; u < GS_U; u++) accs[u] = DD{0.0, 0.0};
+  DD acc{0.0, 0.0};
   const long long total = p.n * NR;
   const long long stride = (long long)gridDim.x * BT;
   auto load = [&](long long j) -> double {
@@ -632,13 +690,9 @@ __global__ void __launch_bounds__(1024) gsum_kernel(const EwParams p, DD* partia
     double v[GS_U];
 #pragma unroll
     for (int u = 0; u < GS_U; u++) v[u] = load(j + u * stride);
-#pragma unroll
-    for (int u = 0; u < GS_U; u++) dd_add(accs[u], v[u]);
+    dd_add(acc, tree_sum(v));
   }
-  for (; j < total; j += stride) dd_add(accs[0], load(j));
-  DD acc = accs[0];
-#pragma unroll
-  for (int u = 1; u < GS_U; u++) dd_merge(acc, accs[u]);
+  for (; j < total; j += stride) dd_add(acc, load(j));
   red[threadIdx.x] = acc;
   __syncthreads();
   for (int q = threadIdx.x; q < NR; q += BT) {
@@ -646,28 +700,24 @@ __global__ void __launch_bounds__(1024) gsum_kernel(const EwParams p, DD* partia
     for (int t = q + NR; t < BT; t += NR) dd_merge(s, red[t]);
     partials[(long long)blockIdx.x * NR + q] = s;
   }
-  __threadfence();
+}
+
+constexpr int GS_FOLD = 128;
+
+template <typename OUT>
+__global__ void __launch_bounds__(GS_FOLD) gsum_fold_kernel(const DD* __restrict__ partials, int nblk, int nr,
+                                                            OUT* result) {
+  __shared__ DD red[GS_FOLD];
+  const int q = blockIdx.x;
+  DD s{0.0, 0.0};
+  for (int b = threadIdx.x; b < nblk; b += GS_FOLD) dd_merge(s, partials[(long long)b * nr + q]);
+  red[threadIdx.x] = s;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned ticket = atomicAdd(counter, 1u);
-    is_last = (ticket == gridDim.x - 1);
+  for (int w = GS_FOLD / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) dd_merge(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
   }
-  __syncthreads();
-  if (!is_last) return;
-  __threadfence();
-  for (int q = threadIdx.x; q < NR; q += BT) {
-    DD s{0.0, 0.0};
-    for (int b = 0; b < (int)gridDim.x; b++) {
-      volatile DD* vp = reinterpret_cast<volatile DD*>(&partials[(long long)b * NR + q]);
-      DD v;
-      v.hi = vp->hi;
-      v.lo = vp->lo;
-      dd_merge(s, v);
-    }
-    result[q] = static_cast<OUT>(__dadd_rn(s.hi, s.lo));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) *counter = 0u;
+  if (threadIdx.x == 0) result[q] = static_cast<OUT>(__dadd_rn(red[0].hi, red[0].lo));
 }
 
 // r: one record of OUT components (host: synchronous, device: asynchronous)
@@ -688,14 +738,15 @@ inline void api_gsum(const char* kid, void* r, Opnd a, const int* gang, int n) {
       std::memset(r, 0, rbytes);
     return;
   }
-  // block: a multiple of lcm(NR, 32) reals, up to 1024 threads
+  // block: a multiple of lcm(NR, 32) reals, up to 1024 threads; one wave of
+  // blocks (2048 resident threads per SM)
   int l = NR;
   while (l % 32) l += NR;
   int BT = l;
-  while (BT + l <= 512) BT += l;
+  while (BT + l <= 1024) BT += l;
   const int sms = device_sm_count();
   long long grid = ((long long)n * NR + BT - 1) / BT;
-  const long long cap = (long long)sms * 4;
+  const long long cap = (long long)sms * (2048 / BT > 0 ? 2048 / BT : 1);
   if (grid > cap) grid = cap;
   if (grid < 1) grid = 1;
   // partials [grid * NR] DD, then the result record
@@ -710,7 +761,9 @@ inline void api_gsum(const char* kid, void* r, Opnd a, const int* gang, int n) {
   p.gang = gang;
   p.n = n;
   const int flat = (gang == nullptr && a.mode == OM_CONTIG) ? 1 : 0;
-  gsum_kernel<R, NR, OUT><<<(unsigned)grid, BT, (size_t)BT * sizeof(DD), st>>>(p, partials, rs->counter, res, flat);
+  gsum_kernel<R, NR><<<(unsigned)grid, BT, (size_t)BT * sizeof(DD), st>>>(p, partials, flat);
+  if (!check_launch(kid)) return;
+  gsum_fold_kernel<OUT><<<NR, GS_FOLD, 0, st>>>(partials, (int)grid, NR, res);
   if (!check_launch(kid)) return;
   if (!dev_out) {
     if (cudaMemcpyAsync(r, res, rbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
