@@ -328,6 +328,23 @@ __device__ __forceinline__ void dd_merge(DD& s, const DD& o) {
   s.lo = __dadd_rn(s.lo, o.lo);
 }
 
+// sum of U doubles (U a power of two) by a fixed pairwise tree: at most U - 1
+// roundings, each within half an ulp of the group's magnitude.  Reductions
+// sum each thread's group of in-flight terms this way and add the group sum
+// in double-double, so one accumulator serves U loads in flight.
+template <int U>
+__device__ __forceinline__ double tree_sum(const double (&v)[U]) {
+  static_assert((U & (U - 1)) == 0, "tree_sum needs a power of two");
+  double w[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) w[u] = v[u];
+#pragma unroll
+  for (int h = U / 2; h >= 1; h >>= 1)
+#pragma unroll
+    for (int u = 0; u < h; u++) w[u] = __dadd_rn(w[u], w[u + h]);
+  return w[0];
+}
+
 __device__ __forceinline__ DD dd_shfl_xor(const DD& v, int lane_mask) {
   DD o;
   o.hi = __shfl_xor_sync(0xffffffffu, v.hi, lane_mask);

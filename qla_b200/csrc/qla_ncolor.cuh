@@ -605,10 +605,36 @@ __global__ void __launch_bounds__(256) gdotn_kernel(const EwParams p, const Site
 }
 
 // contiguous fields without a gang index: one flat stream of complex
-// numbers (gdot_flat_kernel's scheme with a run-time record length)
+// numbers (gdot_flat_kernel's scheme with a run-time record length; the
+// unpermuted forms need no element positions and take its grouped sums)
 template <typename R, int KIND, typename OUT>
-__global__ void __launch_bounds__(256) gdotn_flat_kernel(const EwParams p, const SiteParams rp, const NcDims d) {
+__global__ void __launch_bounds__(256, 4) gdotn_flat_kernel(const EwParams p, const SiteParams rp, const NcDims d) {
   using FIN = GDotFinish<KIND, OUT>;
+  if constexpr (KIND == LD_DOT || KIND == LD_REDOT || KIND == LD_NORM2) {
+    DD acc[ArrN<FIN::NACC>::value];
+#pragma unroll
+    for (int a = 0; a < ArrN<FIN::NACC>::value; a++) acc[a] = DD{0.0, 0.0};
+    const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
+    const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);
+    const long long total = p.n * d.ne;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; g + (GD_U - 1) * stride < total; g += GD_U * stride) {
+      double tr[GD_U], ti[GD_U];
+#pragma unroll
+      for (int u = 0; u < GD_U; u++) gdot_term<R, 1, KIND, 0>(A + g + u * stride, B + g + u * stride, 0, tr[u], ti[u]);
+      dd_add(acc[0], tree_sum(tr));
+      if constexpr (FIN::NACC > 1) dd_add(acc[1], tree_sum(ti));
+    }
+    for (; g < total; g += stride) {
+      double tr, ti;
+      gdot_term<R, 1, KIND, 0>(A + g, B + g, 0, tr, ti);
+      dd_add(acc[0], tr);
+      if constexpr (FIN::NACC > 1) dd_add(acc[1], ti);
+    }
+    reduce_finish<FIN>(rp, acc);
+    return;
+  }
   DD accr[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}}, acci[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}};
   const Cx<R>* A = static_cast<const Cx<R>*>(p.b.base);
   const Cx<R>* B = static_cast<const Cx<R>*>(KIND == LD_NORM2 ? p.b.base : p.c.base);

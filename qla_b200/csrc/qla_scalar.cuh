@@ -347,28 +347,37 @@ struct SredFinish {
 };
 
 // RIN: field element type (float, double or int); RW: the library's real type
+// Eight terms in flight per thread, summed in double by tree_sum (exact for
+// integer fields below 2^53), each group added in double-double.
 template <typename RIN, typename RW, int KIND, typename OUT>
 __global__ void __launch_bounds__(256) sred_kernel(const EwParams p, const SiteParams rp) {
+  constexpr int U = 8;
   DD acc[1] = {DD{0.0, 0.0}};
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
-       i += (long long)gridDim.x * blockDim.x) {
+  auto term = [&](long long i) -> double {
     const long long k = p.gang ? (long long)p.gang[i] : i;
     const RIN a = ld_s<RIN>(p.b, k);
-    double t;
     if constexpr (KIND == SR_SUM) {
-      t = (double)a;
+      return (double)a;
     } else if constexpr (KIND == SR_DOT) {
       const RIN b = ld_s<RIN>(p.c, k);
       if constexpr (std::is_same<RIN, int>::value)  // the product wraps as the reference's int product
-        t = (double)(int)((unsigned)a * (unsigned)b);
+        return (double)(int)((unsigned)a * (unsigned)b);
       else
-        t = (double)rmul(a, b);
+        return (double)rmul(a, b);
     } else {
       const RW at = (RW)a;
-      t = (double)rmul(at, at);
+      return (double)rmul(at, at);
     }
-    dd_add(acc[0], t);
+  };
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (U - 1) * stride < p.n; i += U * stride) {
+    double t[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) t[u] = term(i + u * stride);
+    dd_add(acc[0], tree_sum(t));
   }
+  for (; i < p.n; i += stride) dd_add(acc[0], term(i));
   reduce_finish<SredFinish<1, OUT>>(rp, acc);
 }
 

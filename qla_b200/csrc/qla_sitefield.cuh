@@ -514,23 +514,10 @@ __device__ __forceinline__ void gdot_term(const Cx<R>* a, const Cx<R>* b, int e,
   }
 }
 
-// GS_U loads of one component in flight per thread, summed in double as a
-// fixed pairwise tree (error <= (GS_U - 1) double ulps of the group's
-// magnitude), then one double-double add per group: one accumulator keeps
-// the registers low enough for two blocks of up to 1024 threads per SM.
+// GS_U loads of one component in flight per thread, summed in double by
+// tree_sum, then one double-double add per group: one accumulator keeps the
+// registers low enough for two blocks of up to 1024 threads per SM.
 constexpr int GS_U = 8;
-
-template <int U>
-__device__ __forceinline__ double tree_sum(const double (&v)[U]) {
-  double w[U];
-#pragma unroll
-  for (int u = 0; u < U; u++) w[u] = v[u];
-#pragma unroll
-  for (int h = U / 2; h >= 1; h >>= 1)
-#pragma unroll
-    for (int u = 0; u < h; u++) w[u] = __dadd_rn(w[u], w[u + h]);
-  return w[0];
-}
 
 // Contiguous operands without a gang index: the n * NE complex elements are
 // one flat stream; thread g takes elements g, g + stride, ..., GD_U of them
