@@ -412,9 +412,11 @@ __device__ __forceinline__ void ldot_store(void* out, long long k, int eqop, dou
 }
 
 // Staged form for contiguous operands without a gang index: a block copies
-// the records of S consecutive sites with coalesced loads into shared memory
-// (rows padded by one complex number against bank conflicts), then each of
-// the first S threads accumulates its site from there.
+// the records of S consecutive sites with coalesced loads (LD_U in flight
+// per thread) into shared memory (rows padded by one complex number against
+// bank conflicts), then each of the first S threads accumulates its site
+// from there.  (Per-thread cp.async copies in two stages measured slower
+// than this on B200: 0.75 against 0.88 of HBM for the D3 D dot product.)
 // one thread per site, records read where they are (gang or pointer forms)
 template <typename R, int NE, int KIND, int PERM>
 __global__ void __launch_bounds__(256) ldot_kernel(const EwParams p) {
@@ -442,10 +444,29 @@ __global__ void __launch_bounds__(128) ldot_smem_kernel(const EwParams p) {
     const long long s0 = tile * S;
     const int ns = (int)((p.n - s0) < S ? (p.n - s0) : S);
     const long long base = s0 * NE;
-    for (int f = threadIdx.x; f < ns * NE; f += blockDim.x) {
-      const int row = f / NE, col = f - row * NE;
-      sa[row * ST + col] = A[base + f];
-      if constexpr (KIND != LD_NORM2) sb[row * ST + col] = B[base + f];
+    const int nf = ns * NE;
+    // LD_U loads per thread issued before their shared-memory stores, so
+    // that many are in flight (a load-store loop would wait for each)
+    constexpr int LD_U = 12;
+    for (int f0 = threadIdx.x; f0 < nf; f0 += LD_U * blockDim.x) {
+      Cx<R> va[LD_U], vb[LD_U];
+#pragma unroll
+      for (int u = 0; u < LD_U; u++) {
+        const int f = f0 + u * blockDim.x;
+        if (f < nf) {
+          va[u] = A[base + f];
+          if constexpr (KIND != LD_NORM2) vb[u] = B[base + f];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < LD_U; u++) {
+        const int f = f0 + u * blockDim.x;
+        if (f < nf) {
+          const int row = f / NE, col = f - row * NE;
+          sa[row * ST + col] = va[u];
+          if constexpr (KIND != LD_NORM2) sb[row * ST + col] = vb[u];
+        }
+      }
     }
     __syncthreads();
     if (threadIdx.x < ns) {

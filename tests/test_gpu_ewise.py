@@ -106,3 +106,39 @@ def test_elementwise_large_fields(qla, pc, dt):
         getattr(L, nm)(*args)
         assert T.bits_equal(T.to_host(r_d), want), nm
     qla.check("elementwise large")
+
+
+@pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
+def test_site_local_reductions_tiles_and_alignment(qla, pc, dt):
+    """The staged path of the site-local dot products and norms (tiles of
+    records copied into shared memory) on lengths that leave a partial last
+    tile, and the same calls on operands that start half a complex number
+    past an aligned address: bit-identical to the oracle either way."""
+    import ctypes
+    rng = np.random.default_rng(204)
+    L = qla.lib()
+    man = {e["name"]: e for e in json.load(open(MANIFEST))}
+    names = [f"QLA_{pc}_C_vpeq_D_dot_D", f"QLA_{pc}_R_veq_norm2_P", f"QLA_{pc}_C_veq_P_dot_P",
+             f"QLA_{pc}_C_veq_M_dot_M", f"QLA_{pc}_R_veq_re_P_dot_P"]
+    item = np.dtype(dt).itemsize
+    for nm in names:
+        e = man[nm]
+        for n in (1, 33, 1031):
+            ins, idx, gang = T.ewise_inputs(e, rng, dt, n, n)
+            want = T.ewise_oracle(e, ins, idx, gang, n)
+            for shift in (0, 1):
+                keep, args = [], []
+                for t, name in zip(e["ctypes"], e["params"]):
+                    if name == "n":
+                        args.append(n)
+                    elif name == "r":
+                        r_d = T.to_dev(ins["r"][2])
+                        args.append(T.ptr_dev(r_d))
+                    else:
+                        flat = np.concatenate([np.zeros(shift, dt), ins[name][2].ravel()])
+                        d = T.to_dev(flat)
+                        keep.append(d)
+                        args.append(ctypes.c_void_p(d.data_ptr() + shift * item))
+                getattr(L, nm)(*args)
+                assert T.bits_equal(T.to_host(r_d), want), (nm, n, shift)
+    qla.check("site-local reductions")
