@@ -40,7 +40,7 @@ enum SfKind : int {
   SF_ZERO,        // r = 0
   SF_MASK,        // r = a where mask != 0
   SF_SUB,         // r.e[oi[j]] = a.e[si[j]], j < cnt    (components, columns)
-  SF_GAMMA_L,     // r = gamma a   on the first spin index of D / P
+  SF_GAMMA_L,     // r = gamma a   on the first spin index of P
   SF_GAMMA_R,     // r = a gamma   on the second spin index of P
   SF_TRACE_C,     // C r = trace a
   SF_TRACE_RE,    // R r = Re trace a
@@ -86,8 +86,8 @@ __device__ __forceinline__ Cx<R> phase_times(int ph, Cx<R> a) {
 }
 
 // NE_OUT / NE_SRC: complex numbers per destination / source record.
-// For SF_GAMMA_* the record is a D (12) or a P (144); the spin index being
-// multiplied is decoded from the element index below.
+// For SF_GAMMA_* the record is a P (144); the spin index being multiplied
+// is decoded from the element index below.
 template <typename R, int NE_OUT, int NE_SRC, int KIND>
 __global__ void __launch_bounds__(256) sf_kernel(const SfParams p, const RecConst<R, (KIND == SF_BCAST) ? NE_OUT : 1> cv) {
   constexpr int OPS = SfOutPerSite<KIND, NE_OUT>::value;
@@ -134,13 +134,9 @@ __global__ void __launch_bounds__(256) sf_kernel(const SfParams p, const RecCons
     } else if constexpr (KIND == SF_SUB) {
       static_cast<Cx<R>*>(p.out)[k * NE_OUT + p.oi[e]] = rec_ptr<R>(p.a, k, NE_SRC)[p.si[e]];
     } else if constexpr (KIND == SF_GAMMA_L || KIND == SF_GAMMA_R) {
-      // D: e = ic*4 + is; P: e = ((ic*4 + is)*3 + jc)*4 + js
+      // P: e = ((ic*4 + is)*3 + jc)*4 + js (D records take GammaDOp)
       int s, base, stride;
       if constexpr (KIND == SF_GAMMA_R) {
-        s = e & 3;
-        base = e - s;
-        stride = 1;
-      } else if constexpr (NE_OUT == 12) {
         s = e & 3;
         base = e - s;
         stride = 1;
@@ -449,18 +445,18 @@ inline void api_gamma(const char* kid, void* r, Opnd a, int mu, const int* gang,
     sp.gang = gang;
     for (int s = 0; s < 4; s++) sp.aux |= (t.row_src[mu][s] | (t.row_ph[mu][s] << 2)) << (4 * s);
     SiteLauncher<GammaDOp<R>>::run(sp, kid);
-    return;
+  } else {
+    SfParams p;
+    if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
+    for (int s = 0; s < 4; s++) {
+      p.gs[s] = LEFT ? t.row_src[mu][s] : t.col_src[mu][s];
+      p.gp[s] = LEFT ? t.row_ph[mu][s] : t.col_ph[mu][s];
+    }
+    if constexpr (LEFT)
+      sf_launch<R, NE, NE, SF_GAMMA_L>(kid, p, RecConst<R, 1>{});
+    else
+      sf_launch<R, NE, NE, SF_GAMMA_R>(kid, p, RecConst<R, 1>{});
   }
-  SfParams p;
-  if (!sf_prep(kid, p, r, a, gang, n, EQ, true)) return;
-  for (int s = 0; s < 4; s++) {
-    p.gs[s] = LEFT ? t.row_src[mu][s] : t.col_src[mu][s];
-    p.gp[s] = LEFT ? t.row_ph[mu][s] : t.col_ph[mu][s];
-  }
-  if constexpr (LEFT)
-    sf_launch<R, NE, NE, SF_GAMMA_L>(kid, p, RecConst<R, 1>{});
-  else
-    sf_launch<R, NE, NE, SF_GAMMA_R>(kid, p, RecConst<R, 1>{});
 }
 
 template <typename R, int KIND>
