@@ -183,11 +183,13 @@ __global__ void __launch_bounds__(256) ew_kernel(const EwParams p) {
 }
 
 // Streaming form of the same map when every operand is contiguous and 16-B
-// aligned, there is no gang index, no permutation and no per-site scalar:
-// the records are one flat array of n*NE complex numbers, and each thread
-// moves 16-B vectors (two F3 / one D3 complex number per vector, two vectors
-// per thread).  Element arithmetic is ew_apply, so results are identical.
-template <typename R, int SHAPE, int SCAL, bool SREAL>
+// aligned, there is no gang index and no permutation: the records are one
+// flat array of n*NE complex numbers, and each thread moves 16-B vectors (two
+// F3 / one D3 complex number per vector, two vectors per thread).  A per-site
+// scalar field (contiguous) is read for each element's site, element / NE
+// (from L1: a site's elements are neighbours).  Element arithmetic is
+// ew_apply, so results are identical.
+template <typename R, int NE, int SHAPE, int SCAL, bool SREAL>
 __global__ void __launch_bounds__(256) ew_flat_kernel(const EwParams p, long long nelem) {
   constexpr bool TWO = SHAPE == EW_PLUS || SHAPE == EW_MINUS || SHAPE >= EW_RT_PLUS;
   constexpr int CPV = 16 / (int)sizeof(Cx<R>);  // complex numbers per 16-B vector
@@ -207,6 +209,18 @@ __global__ void __launch_bounds__(256) ew_flat_kernel(const EwParams p, long lon
   const Cx<R>* B = static_cast<const Cx<R>*>(p.b.base);
   const Cx<R>* C = static_cast<const Cx<R>*>(p.c.base);
   Cx<R>* O = static_cast<Cx<R>*>(p.out);
+  // the scalar of element q: the constant, or the field at site q / NE
+  auto scal_at = [&](long long q) -> Cx<R> {
+    if constexpr (SCAL == SC_FIELD) {
+      const long long site = q / NE;
+      if constexpr (SREAL)
+        return Cx<R>{static_cast<const R*>(p.s.base)[site], R(0)};
+      else
+        return static_cast<const Cx<R>*>(p.s.base)[site];
+    } else {
+      return s;
+    }
+  };
   const long long nvec = nelem / CPT;
   for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvec;
        v += (long long)gridDim.x * blockDim.x) {
@@ -244,7 +258,8 @@ __global__ void __launch_bounds__(256) ew_flat_kernel(const EwParams p, long lon
     }
     Cx<R> y[CPT];
 #pragma unroll
-    for (int j = 0; j < CPT; j++) y[j] = ew_apply<R, SHAPE>(p.eqop, load ? x[j] : Cx<R>{R(0), R(0)}, s, b[j], c[j]);
+    for (int j = 0; j < CPT; j++)
+      y[j] = ew_apply<R, SHAPE>(p.eqop, load ? x[j] : Cx<R>{R(0), R(0)}, scal_at(g0 + j), b[j], c[j]);
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const long long q = g0 + h * CPV;
@@ -261,7 +276,7 @@ __global__ void __launch_bounds__(256) ew_flat_kernel(const EwParams p, long lon
     const Cx<R> x = load ? O[q] : Cx<R>{R(0), R(0)};
     Cx<R> c{R(0), R(0)};
     if constexpr (TWO) c = C[q];
-    O[q] = ew_apply<R, SHAPE>(p.eqop, x, s, B[q], c);
+    O[q] = ew_apply<R, SHAPE>(p.eqop, x, scal_at(q), B[q], c);
   }
 }
 
@@ -297,14 +312,15 @@ inline void api_ew(const char* kid, void* r, const void* scal, Opnd s, Opnd b, O
   }
   const long long total = (long long)n * NE;
   const long long cap = (long long)device_sm_count() * 16;
-  const bool flat = PERM == PERM_ID && SCAL != SC_FIELD && gang == nullptr && b.mode == OM_CONTIG &&
+  const bool flat = PERM == PERM_ID && (SCAL != SC_FIELD || s.mode == OM_CONTIG) && gang == nullptr &&
+                    b.mode == OM_CONTIG &&
                     (reinterpret_cast<uintptr_t>(b.base) & 15u) == 0 && (reinterpret_cast<uintptr_t>(r) & 15u) == 0 &&
                     (!TWO || (c.mode == OM_CONTIG && (reinterpret_cast<uintptr_t>(c.base) & 15u) == 0));
   if (flat) {
     constexpr int CPT = 2 * (16 / (int)sizeof(Cx<R>));
     long long grid = (total / CPT + 255) / 256;
     if (grid > cap) grid = cap;
-    ew_flat_kernel<R, SHAPE, SCAL, SREAL><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, current_stream()>>>(p, total);
+    ew_flat_kernel<R, NE, SHAPE, SCAL, SREAL><<<(unsigned)(grid < 1 ? 1 : grid), 256, 0, current_stream()>>>(p, total);
   } else {
     long long grid = (total + 255) / 256;
     if (grid > cap) grid = cap;
