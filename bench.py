@@ -513,7 +513,7 @@ def run_gpu_arm(args):
 
 
 # ---------------------------------------------------------------------------
-# secondary workloads (SURVEY configs 1, 2, 4, 5): one JSON line each, same
+# secondary workloads (configs 1, 2, 4, 5 of the level-1 study): one JSON line each, same
 # timing rules (warm-up, CUDA events on the launching stream, inputs > L2
 # unless stated).  The default workload above is the benchmark line.
 def _events_time(torch, stream, fn, reps, warmup=3):

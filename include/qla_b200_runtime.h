@@ -46,7 +46,9 @@ int qlagpu_synchronize(void);
 
 /* synchronise, then return the device error word (bit 1: a pipeline wait gave
  * up; 2: draining copies gave up; 8: an iterative matrix function hit its
- * iteration cap); clear != 0 resets it */
+ * iteration cap), together with the bits recorded by
+ * qlagpu_DF3_r_veq_norm2_D_noalloc; clear != 0 resets both.  Allocates no
+ * device memory. */
 unsigned qlagpu_device_error(int clear);
 
 /* autotuner: launch shape (threads per block = sites per tile: 64/128/256,
@@ -104,8 +106,10 @@ void qlagpu_batch_destroy(void *plan);
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * All calls share the array: calls that overlap on the GPU (e.g. on two
  * streams at once) race and give wrong results.  r may be a host pointer
- * (the call synchronises) or a device pointer.  Returns QLAGPU_OK or an error
- * code. */
+ * (the call synchronises and returns QLAGPU_ERR_DEVICE if a pipeline wait
+ * gave up) or a device pointer (the call stays asynchronous; if a wait gave
+ * up, *r is set to NaN and qlagpu_device_error() reports the bits).  Returns
+ * QLAGPU_OK or an error code. */
 int qlagpu_DF3_r_veq_norm2_D_noalloc(QLA_D_Real *r, QLA_F3_DiracFermion *a, int n);
 
 #ifdef __cplusplus

@@ -14,18 +14,31 @@
 #         lib/perl/formatting.pl:90-127 with $have_openmp="yes").
 #         Run with OMP_NUM_THREADS=1 it reproduces the serial summation order.
 #
-# Usage: sh oracle/build_ref.sh [reference-root]   (default: /root/reference)
+# Usage: sh oracle/build_ref.sh <reference-root>
+#        (or QLA_REF_SRC=<reference-root> sh oracle/build_ref.sh)
 set -e
-REF=${1:-${QLA_REF_SRC:-/root/reference}}
+REF=${1:-${QLA_REF_SRC:-}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 JOBS=${JOBS:-$(nproc)}
 
+if [ -z "$REF" ]; then
+  echo "build_ref.sh: name the QLA source tree as the first argument or in QLA_REF_SRC" >&2
+  exit 2
+fi
 if [ ! -f "$REF/lib/perl/build_qla.pl" ]; then
   echo "build_ref.sh: reference tree not found at $REF" >&2
   exit 2
 fi
+# The reference's hand-written API headers (qla.h, qla_types.h, qla_complex.h
+# ...) beside the generated ones, so that a C caller can be compiled against
+# the reference's own headers from oracle/_ref alone (tests/test_c_dropin.py).
+copy_api_headers() {
+  mkdir -p "$OUT/gen/include"
+  for h in "$REF"/include/*.h; do cp "$h" "$OUT/gen/include/"; done
+}
 if [ -f "$OUT/libqla_ref.so" ] && [ "$OUT/libqla_ref.so" -nt "$HERE/build_ref.sh" ]; then
+  copy_api_headers
   echo "build_ref.sh: $OUT/libqla_ref.so is up to date"
   exit 0
 fi
@@ -104,4 +117,5 @@ mv "$OUT/libqla_ref.so.tmp" "$OUT/libqla_ref.so"
 # document the exact prototypes) and drop the bulky generated sources and objects
 rm -rf "$GEN/obj" "$GEN/libqla_ref_all.a"
 for dir in $COMPILE $HDR_ONLY; do rm -f "$GEN/$dir"/QLA_*.c; done
+copy_api_headers
 echo "build_ref.sh: built $OUT/libqla_ref.so"

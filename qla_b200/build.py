@@ -4,8 +4,10 @@
 
 Runs the C-ABI generator (qla_b200/gen/gen_qla.py), compiles every .cu under
 qla_b200/csrc with nvcc (-gencode arch=compute_100a,code=sm_100a), one object
-per file in parallel, and links qla_b200/lib/libqla_b200.so.  Objects are
-rebuilt when their source or any shared header is newer.
+per file in parallel, and links qla_b200/lib/libqla_b200.so.  Each object is
+rebuilt when its source or a header it includes is newer (nvcc writes the
+header list beside the object, `-MD -MF`); an object without that list is
+rebuilt when any header of the package is newer.
 """
 import argparse
 import glob
@@ -43,6 +45,25 @@ def _newest_header():
     return max((os.path.getmtime(h) for h in hs), default=0)
 
 
+def _deps_time(obj):
+    """Newest modification time of the headers recorded for `obj`, or None
+    when the dependency file is missing or names a file that no longer exists."""
+    d = obj + ".d"
+    if not os.path.exists(d):
+        return None
+    with open(d) as f:
+        txt = f.read().replace("\\\n", " ")
+    _, _, rhs = txt.partition(":")
+    newest = 0.0
+    for dep in rhs.split():
+        if not dep.startswith("/usr/"):
+            dep = dep if os.path.isabs(dep) else os.path.join(REPO, dep)
+            if not os.path.exists(dep):
+                return None
+            newest = max(newest, os.path.getmtime(dep))
+    return newest
+
+
 def build(jobs=None, force=False, verbose=True):
     subprocess.check_call([sys.executable, os.path.join(PKG, "gen", "gen_qla.py")])
     os.makedirs(OBJ, exist_ok=True)
@@ -55,17 +76,22 @@ def build(jobs=None, force=False, verbose=True):
         rel = os.path.relpath(s, CSRC).replace(os.sep, "__")
         o = os.path.join(OBJ, rel[:-3] + ".o")
         objs.append(o)
-        if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t):
+        if force or not os.path.exists(o):
+            todo.append((s, o))
+            continue
+        dt = _deps_time(o)
+        if os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t if dt is None else dt):
             todo.append((s, o))
 
     def compile_one(so):
         s, o = so
         # extern "C" entry points must stay visible despite -fvisibility=hidden
-        cmd = [nvcc()] + NVCC_FLAGS + ["-DQLA_B200_BUILD", "-c", s, "-o", o + ".tmp"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        cmd = [nvcc()] + NVCC_FLAGS + ["-DQLA_B200_BUILD", "-c", s, "-o", o + ".tmp", "-MD", "-MF", o + ".d.tmp"]
+        r = subprocess.run(cmd, capture_output=True, text=True, cwd=REPO)
         if r.returncode != 0:
             return s, r.stderr
         os.replace(o + ".tmp", o)
+        os.replace(o + ".d.tmp", o + ".d")
         return s, None
 
     jobs = jobs or min(len(todo) or 1, os.cpu_count() or 4)

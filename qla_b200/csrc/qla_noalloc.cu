@@ -35,18 +35,27 @@ constexpr int kSitesPerTile = 256;
 constexpr int kStages = 2;
 constexpr int kMaxPartials = 65536;
 constexpr long long kMaxSites = (long long)kMaxPartials * kSitesPerTile;
-// layout: [partials: kMaxPartials DD][result: 2 doubles][counter][error word]
+// layout: [partials: kMaxPartials DD][result: 2 doubles][counter][per-call
+// error word][sticky error word]
 constexpr size_t kOffResult = sizeof(DD) * (size_t)kMaxPartials;
 constexpr size_t kOffCounter = kOffResult + 2 * sizeof(double);
 constexpr size_t kOffErr = kOffCounter + sizeof(unsigned);
+constexpr size_t kOffSticky = kOffErr + sizeof(unsigned);
 constexpr size_t kScratchBytes = kOffErr + 256;  // 1 MiB + 272 B
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 using Op = Norm2Op<float, 12, double>;  // QLA_DF3_r_veq_norm2_D
 
-// device address of the scratch on the current device, looked up once per
-// device (the first call on a device does this set-up)
+constexpr unsigned kRecBytes = Op::N0 * sizeof(Cx<float>);
+inline unsigned tile_stage_bytes() { return stage_bytes_for(kSitesPerTile, kRecBytes); }
+inline size_t tile_smem_bytes() { return tma_smem_bytes(kSitesPerTile, kStages, tile_stage_bytes(), 0); }
+
+// Once per device, with that device current (the first call on a device does
+// this set-up): the device address of the scratch, and the pipelined
+// kernel's shared-memory limit raised to what this file's tile needs.  The
+// limit is a property of the kernel shared with the regular norm2 entry
+// point, so it goes through the launcher's helper, which only ever raises it.
 static unsigned char* scratch_on_current_device() {
   static std::mutex mu;
   static unsigned char* addr[64] = {nullptr};
@@ -63,12 +72,46 @@ static unsigned char* scratch_on_current_device() {
       cudaGetLastError();
       return nullptr;
     }
+    SiteLauncher<Op>::set_smem_attr(reinterpret_cast<const void*>(&site_tma_kernel<Op>), tile_smem_bytes());
+    if (cudaGetLastError() != cudaSuccess) return nullptr;
     addr[dev] = static_cast<unsigned char*>(p);
   }
   return addr[dev];
 }
 
+// After the reduction: the call's error bits go into the sticky word (read and
+// cleared by qlagpu_device_error), and a device result is overwritten with a
+// NaN when a wait gave up, so that a caller who never asks still cannot take
+// an incomplete sum for a valid one.
+__global__ void noalloc_fold_error(const unsigned* err, unsigned* sticky, double* dev_result) {
+  const unsigned e = *err;
+  if (e) {
+    atomicOr(sticky, e);
+    if (dev_result) *dev_result = __longlong_as_double(0x7ff8000000000000ll);
+  }
+}
+
 }  // namespace noalloc
+
+// Error bits that calls of the allocation-free entry point recorded on the
+// current device (the sticky word of its static scratch), cleared on request.
+// Reads the symbol directly: allocates nothing.  0xffffffff if the read fails.
+unsigned noalloc_take_device_error(bool clear) {
+  unsigned v = 0;
+  const size_t off = noalloc::kOffSticky;
+  if (cudaMemcpyFromSymbol(&v, noalloc::g_noalloc_scratch, sizeof(v), off, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return 0xffffffffu;
+  }
+  if (clear && v) {
+    const unsigned zero = 0;
+    if (cudaMemcpyToSymbol(noalloc::g_noalloc_scratch, &zero, sizeof(zero), off, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      cudaGetLastError();
+  }
+  return v;
+}
+
 }  // namespace qlab
 
 using namespace qlab;
@@ -109,8 +152,8 @@ extern "C" QLAB_EXPORT int qlagpu_DF3_r_veq_norm2_D_noalloc(QLA_D_Real* r, QLA_F
   double* result = reinterpret_cast<double*>(base + kOffResult);
   unsigned* counter = reinterpret_cast<unsigned*>(base + kOffCounter);
   unsigned* err = reinterpret_cast<unsigned*>(base + kOffErr);
-  // the ticket counter and the error word must start at zero; the array keeps
-  // whatever the previous call (on any stream) left there
+  // the ticket counter and the per-call error word must start at zero; the
+  // array keeps whatever the previous call (on any stream) left there
   if (cudaMemsetAsync(counter, 0, 2 * sizeof(unsigned), st) != cudaSuccess) {
     check_launch(who);
     return QLAGPU_ERR_LAUNCH;
@@ -122,20 +165,15 @@ extern "C" QLAB_EXPORT int qlagpu_DF3_r_veq_norm2_D_noalloc(QLA_D_Real* r, QLA_F
   p.counter = counter;
   p.err = err;
   p.result = dev_out ? static_cast<void*>(r) : static_cast<void*>(result);
-  constexpr unsigned RB = Op::N0 * sizeof(Cx<float>);
   if (aligned16(a)) {
     p.stages = kStages;
-    p.stage_bytes = stage_bytes_for(kSitesPerTile, RB);
-    p.tx_bytes = (unsigned)kSitesPerTile * RB;
+    p.stage_bytes = tile_stage_bytes();
+    p.tx_bytes = (unsigned)kSitesPerTile * kRecBytes;
     p.off_in[0] = 0;
     p.ntiles = (long long)n / kSitesPerTile;
     const long long grid = p.ntiles > 0 ? p.ntiles : 1;  // one tile per block; <= kMaxPartials
-    const size_t smem = tma_smem_bytes(kSitesPerTile, kStages, p.stage_bytes, 0);
+    const size_t smem = tile_smem_bytes();
     const void* fn = reinterpret_cast<const void*>(&site_tma_kernel<Op>);
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-      check_launch(who);
-      return QLAGPU_ERR_LAUNCH;
-    }
     void* args[] = {&p};
     if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kSitesPerTile + 32), args, smem, st) != cudaSuccess) {
       check_launch(who);
@@ -147,6 +185,8 @@ extern "C" QLAB_EXPORT int qlagpu_DF3_r_veq_norm2_D_noalloc(QLA_D_Real* r, QLA_F
     if (grid > kMaxPartials) grid = kMaxPartials;
     site_direct_kernel<Op><<<(unsigned)grid, 256, 0, st>>>(p);
   }
+  if (!check_launch(who)) return QLAGPU_ERR_LAUNCH;
+  noalloc_fold_error<<<1, 1, 0, st>>>(err, reinterpret_cast<unsigned*>(base + kOffSticky), dev_out ? r : nullptr);
   if (!check_launch(who)) return QLAGPU_ERR_LAUNCH;
   if (!dev_out) {
     unsigned e = 0;

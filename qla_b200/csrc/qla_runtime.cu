@@ -208,6 +208,10 @@ __global__ void wait_timeout_selftest_kernel(unsigned* err, unsigned long long l
   if (threadIdx.x == 0) *gave_up = mbar_wait_bounded(&bar, 0u, err, limit_ns) ? 0 : 1;
 }
 
+// error bits recorded by the allocation-free entry point on the current
+// device (defined in qla_noalloc.cu); allocates nothing
+unsigned noalloc_take_device_error(bool clear);
+
 }  // namespace qlab
 
 // ===========================================================================
@@ -229,16 +233,30 @@ QLAB_EXPORT void qlagpu_set_stream(void* stream) { t_stream = static_cast<cudaSt
 
 QLAB_EXPORT void* qlagpu_get_stream(void) { return static_cast<void*>(t_stream); }
 
+// The regular entry points' error word (allocated by the first launch on a
+// device; no kernel can have written to a word that does not exist yet, so it
+// is not allocated here) OR the sticky word of the allocation-free entry
+// point's static scratch.  Allocates nothing.
 QLAB_EXPORT unsigned qlagpu_device_error(int clear) {
-  unsigned* w = device_error_word();
-  if (!w) return 0xffffffffu;
+  unsigned* w = nullptr;
+  {
+    const int d = current_device();
+    std::lock_guard<std::mutex> g(g_mu);
+    w = g_dev[d].err;
+  }
   unsigned v = 0;
   if (cudaStreamSynchronize(t_stream) != cudaSuccess ||
-      cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      (w && cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess)) {
     check_launch("qlagpu_device_error");
     return 0xffffffffu;
   }
   if (clear && v) cudaMemset(w, 0, sizeof(unsigned));
+  const unsigned nv = noalloc_take_device_error(clear != 0);
+  if (nv == 0xffffffffu) {
+    set_error(QLAGPU_ERR_LAUNCH, "qlagpu_device_error", "reading the allocation-free scratch failed");
+    return 0xffffffffu;
+  }
+  v |= nv;
   if (v) set_error(QLAGPU_ERR_DEVICE, "qlagpu_device_error", "a kernel reported an error");
   return v;
 }
