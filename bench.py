@@ -437,6 +437,21 @@ def run_gpu_arm(args):
     # ---------------- roofline: algorithmic bytes per launch / event-timed duration
     peak, peak_kind = peaks()
 
+    # ---------------- the other north-star targets on the same GPU (N=1):
+    # config-2 per-kernel HBM fractions and the hop sequence, config-4 batched
+    # launch (its HBM fraction and its uneven / equal-volume ratio); CUDA
+    # events on the launching stream, inputs larger than L2
+    extra = {}
+    if world == 1 and not args.no_extra:
+        reps = max(args.steps, 5)
+        extra["config2_hop"] = hop_figures(torch, qla, qla.lib(), stream, peak, reps)
+        torch.cuda.empty_cache()
+        extra["config4_batched"] = batched_figures(torch, qla, qla.lib(), stream, peak, reps)
+        torch.cuda.empty_cache()
+        qla.check("secondary configurations")
+        if qla.device_error():
+            raise qla.QLAError("a kernel reported an error in the secondary configurations")
+
     def roof(kern, bytes_tab):
         out = {}
         for nm, ms in kern.items():
@@ -507,6 +522,7 @@ def run_gpu_arm(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -530,6 +546,156 @@ def _events_time(torch, stream, fn, reps, warmup=3):
     return e0.elapsed_time(e1) / reps
 
 
+def hop_figures(torch, qla, L, stream, peak, reps):
+    """Config 2: the Wilson-hop-shaped sequence on the 32^3x64 periodic lattice
+    (8 x spproj -> M_times_xH -> vpeq_sprecon), the fused hop term, the
+    4-direction nM_times_npV, and each kernel of the sequence timed alone;
+    F3 and D3.  Returns the workload's JSON fields."""
+    import numpy as np
+    V = lambda t: ctypes.c_void_p(t if isinstance(t, int) else t.data_ptr())  # noqa: E731
+    out = {}
+    dims = [32, 32, 32, 64]
+    n = int(np.prod(dims))
+    res = {}
+    for pc, dt, e in (("F3", torch.float32, 1), ("D3", torch.float64, 2)):
+        D = torch.randn(n, 24, device="cuda", dtype=dt)
+        Out = torch.zeros(n, 24, device="cuda", dtype=dt)
+        H = torch.empty(n, 12, device="cuda", dtype=dt)
+        H2 = torch.empty(n, 12, device="cuda", dtype=dt)
+        U = [torch.randn(n, 18, device="cuda", dtype=dt) for _ in range(4)]
+        Vv = torch.randn(n, 6, device="cuda", dtype=dt)
+        Vo = torch.empty(n, 6, device="cuda", dtype=dt)
+        nbr = {}
+        for mu in range(4):
+            for sg in (1, -1):
+                nbr[(mu, sg)] = torch.empty(n, dtype=torch.int32, device="cuda")
+                qla.shift_index(nbr[(mu, sg)], dims, mu, sg)
+        sp, mh, rc = (getattr(L, f"QLA_{pc}_H_veq_spproj_D"), getattr(L, f"QLA_{pc}_H_eq_M_times_xH"),
+                      getattr(L, f"QLA_{pc}_D_vpeq_sprecon_H"))
+
+        def hop():
+            for mu in range(4):
+                for sg in (1, -1):
+                    sp(V(H), V(D), mu, sg, n)
+                    mh(V(H2), V(U[mu]), V(H), V(nbr[(mu, sg)]), n)
+                    rc(V(Out), V(H2), mu, sg, n)
+        ms = _events_time(torch, stream, hop, reps)
+        fz = getattr(L, f"QLA_{pc}_D_peq_spproj_M_times_xD")
+
+        def hop_fused():
+            for mu in range(4):
+                for sg in (1, -1):
+                    fz(V(Out), V(U[mu]), V(D), V(nbr[(mu, sg)]), mu, sg, n)
+        ms_f = _events_time(torch, stream, hop_fused, reps)
+        # staggered-style 4-direction sum r += sum_mu U_mu V[x+mu] through
+        # QLA's pointer form (QLA_<pc>_V_vpeq_nM_times_npV, nd = 4)
+        pv = [(Vv.data_ptr() + nbr[(mu, 1)].long() * 24 * e).contiguous() for mu in range(4)]
+        tab_a = (ctypes.c_void_p * 4)(*[U[mu].data_ptr() for mu in range(4)])
+        tab_b = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in pv])
+        nmv = getattr(L, f"QLA_{pc}_V_vpeq_nM_times_npV")
+        ms_nm = _events_time(torch, stream, lambda: nmv(V(Vo), tab_a, tab_b, n, 4), reps * 4)
+        t_sp = _events_time(torch, stream, lambda: sp(V(H), V(D), 0, 1, n), reps * 4)
+        t_mh = _events_time(torch, stream, lambda: mh(V(H2), V(U[0]), V(H), V(nbr[(0, 1)]), n), reps * 4)
+        t_rc = _events_time(torch, stream, lambda: rc(V(Out), V(H2), 0, 1, n), reps * 4)
+        mv = getattr(L, f"QLA_{pc}_V_eq_M_times_xV")
+        t_mv = _events_time(torch, stream, lambda: mv(V(Vo), V(U[0]), V(Vv), V(nbr[(0, 1)]), n), reps * 4)
+        ptrs = (Vv.data_ptr() + nbr[(0, 1)].long() * 24 * e).contiguous()
+        mvp = getattr(L, f"QLA_{pc}_V_veq_M_times_pV")
+        t_mvp = _events_time(torch, stream, lambda: mvp(V(Vo), V(U[0]), V(ptrs), n), reps * 4)
+        qla.check("hop")
+        b = {"spproj": 144 * e, "M_times_xH": 168 * e + 4, "sprecon": 240 * e, "M_times_xV": 120 * e + 4,
+             "M_times_pV": 120 * e + 8}
+        tk = {"spproj": t_sp, "M_times_xH": t_mh, "sprecon": t_rc, "M_times_xV": t_mv, "M_times_pV": t_mvp}
+        res[pc] = {"site_updates_per_s": n / (ms / 1e3), "ms_per_hop": ms,
+                   "nM_times_npV_nd4": {"us": 1e3 * ms_nm, "gbs": (4 * (72 * e + 8 + 24 * e) + 48 * e) * n /
+                                        (ms_nm / 1e3) / 1e9,
+                                        "frac": (4 * (72 * e + 8 + 24 * e) + 48 * e) * n / (ms_nm / 1e3) / 1e9
+                                        / peak},
+                   "fused": {"op": f"QLA_{pc}_D_peq_spproj_M_times_xD", "ms_per_hop": ms_f,
+                             "site_updates_per_s": n / (ms_f / 1e3),
+                             "hbm_frac": n * 8 * (364 * e) / (ms_f / 1e3) / 1e9 / peak,
+                             "speedup_vs_unfused": ms / ms_f},
+                   "hbm_frac_hop": n * 8 * sum(b[k] for k in ("spproj", "M_times_xH", "sprecon")) / (ms / 1e3)
+                   / 1e9 / peak,
+                   "kernels": {k: {"us": 1e3 * tk[k], "gbs": b[k] * n / (tk[k] / 1e3) / 1e9,
+                                   "frac": b[k] * n / (tk[k] / 1e3) / 1e9 / peak} for k in tk}}
+        del D, Out, H, H2, U, Vv, Vo, nbr, ptrs, pv
+        torch.cuda.empty_cache()
+    out.update({"metric": "Wilson-hop level-1 sequence (8 x spproj, M_times_xH, vpeq_sprecon), 32^3x64",
+                "unit": "site-updates/s", "value": res["F3"]["site_updates_per_s"], "F3": res["F3"],
+                "D3": res["D3"], "speedup_vs_fp64": res["F3"]["ms_per_hop"] and
+                res["D3"]["ms_per_hop"] / res["F3"]["ms_per_hop"]})
+    return out
+
+
+def batched_figures(torch, qla, L, stream, peak, reps):
+    """Config 4: 64 F3 fields of uneven extents in one persistent launch
+    replayed from a CUDA graph, against 128 separate launches and an
+    equal-volume batch of the same total.  Returns the workload's JSON fields."""
+    import numpy as np
+    V = lambda t: ctypes.c_void_p(t if isinstance(t, int) else t.data_ptr())  # noqa: E731
+    out = {}
+    rng = np.random.default_rng(4)
+    choices = [8, 12, 16, 20, 24, 32]
+    dims_list = [[int(x) for x in rng.choice(choices, 4)] for _ in range(64)]
+    vols = [int(np.prod(d)) for d in dims_list]
+
+    def make(dlist):
+        """one field per lattice: links u, u2, vector v, +mu neighbour table"""
+        fl = []
+        for k, dims in enumerate(dlist):
+            n = int(np.prod(dims))
+            nbr = torch.empty(n, dtype=torch.int32, device="cuda")
+            qla.shift_index(nbr, dims, k % 4, 1)
+            fl.append({"r": torch.empty(n, 18, device="cuda"), "u": torch.randn(n, 18, device="cuda"),
+                       "u2": torch.randn(n, 18, device="cuda"), "nbr": nbr,
+                       "w": torch.empty(n, 6, device="cuda"), "v": torch.randn(n, 6, device="cuda"), "n": n})
+        return fl
+    tot = sum(vols)
+    uneven = make(dims_list)
+    plan = qla.BatchPlan(uneven)
+    g = torch.cuda.CUDAGraph()
+    s2 = torch.cuda.Stream()
+    with torch.cuda.stream(s2):
+        qla.set_stream(s2)
+        plan.run()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=s2):
+            plan.run()
+    qla.set_stream(stream)
+    ms_b = _events_time(torch, stream, g.replay, reps)
+    mxm, mxv = L.QLA_F3_M_eq_M_times_xM, L.QLA_F3_V_veq_M_times_V
+
+    def separate():
+        for f in uneven:
+            mxm(V(f["r"]), V(f["u"]), V(f["u2"]), V(f["nbr"]), f["n"])
+            mxv(V(f["w"]), V(f["r"]), V(f["v"]), f["n"])
+    ms_s = _events_time(torch, stream, separate, reps)
+    del g
+    plan.close()
+    del uneven
+    torch.cuda.empty_cache()
+    # equal-volume batch of the same total: 64 lattices 16x16x16xLt
+    lt = max(1, round(tot / 64 / 4096))
+    even_n = 4096 * lt
+    even = make([[16, 16, 16, lt]] * 64)
+    plan_e = qla.BatchPlan(even)
+    ms_e = _events_time(torch, stream, plan_e.run, reps)
+    plan_e.close()
+    qla.check("batched")
+    rate_b = tot / (ms_b / 1e3)
+    rate_e = 64 * even_n / (ms_e / 1e3)
+    out.update({"metric": "batched uneven-volume M_times_xM + M_times_V (64 F3 fields, extents in "
+                          "{8..32}^4), one persistent launch replayed from a CUDA graph",
+                "unit": "site-updates/s", "value": rate_b, "total_sites": tot,
+                "ms_batched_graph": ms_b, "ms_128_separate_launches": ms_s,
+                "speedup_vs_separate": ms_s / ms_b, "equal_volume_rate": rate_e,
+                "uneven_vs_equal_volume": rate_b / rate_e,
+                "hbm_frac": rate_b * (72 * 3 + 24 * 2 + 4) / 1e9 / peak,
+                "bytes_per_site": "U 72 + U2 gather 72 + nbr 4 + V 24 + R 72 + W 24 = 268"})
+    return out
+
+
 def run_workload(args):
     import numpy as np
     import torch
@@ -544,136 +710,9 @@ def run_workload(args):
     out = {"workload": args.workload, "peak_gbs": peak, "peak_kind": peak_kind, "data": "synthetic, seeded"}
     reps = max(args.steps, 5)
     if args.workload == "hop":
-        dims = [32, 32, 32, 64]
-        n = int(np.prod(dims))
-        res = {}
-        for pc, dt, e in (("F3", torch.float32, 1), ("D3", torch.float64, 2)):
-            D = torch.randn(n, 24, device="cuda", dtype=dt)
-            Out = torch.zeros(n, 24, device="cuda", dtype=dt)
-            H = torch.empty(n, 12, device="cuda", dtype=dt)
-            H2 = torch.empty(n, 12, device="cuda", dtype=dt)
-            U = [torch.randn(n, 18, device="cuda", dtype=dt) for _ in range(4)]
-            Vv = torch.randn(n, 6, device="cuda", dtype=dt)
-            Vo = torch.empty(n, 6, device="cuda", dtype=dt)
-            nbr = {}
-            for mu in range(4):
-                for sg in (1, -1):
-                    nbr[(mu, sg)] = torch.empty(n, dtype=torch.int32, device="cuda")
-                    qla.shift_index(nbr[(mu, sg)], dims, mu, sg)
-            sp, mh, rc = (getattr(L, f"QLA_{pc}_H_veq_spproj_D"), getattr(L, f"QLA_{pc}_H_eq_M_times_xH"),
-                          getattr(L, f"QLA_{pc}_D_vpeq_sprecon_H"))
-
-            def hop():
-                for mu in range(4):
-                    for sg in (1, -1):
-                        sp(V(H), V(D), mu, sg, n)
-                        mh(V(H2), V(U[mu]), V(H), V(nbr[(mu, sg)]), n)
-                        rc(V(Out), V(H2), mu, sg, n)
-            ms = _events_time(torch, stream, hop, reps)
-            fz = getattr(L, f"QLA_{pc}_D_peq_spproj_M_times_xD")
-
-            def hop_fused():
-                for mu in range(4):
-                    for sg in (1, -1):
-                        fz(V(Out), V(U[mu]), V(D), V(nbr[(mu, sg)]), mu, sg, n)
-            ms_f = _events_time(torch, stream, hop_fused, reps)
-            # staggered-style 4-direction sum r += sum_mu U_mu V[x+mu] through
-            # QLA's pointer form (QLA_<pc>_V_vpeq_nM_times_npV, nd = 4)
-            pv = [(Vv.data_ptr() + nbr[(mu, 1)].long() * 24 * e).contiguous() for mu in range(4)]
-            tab_a = (ctypes.c_void_p * 4)(*[U[mu].data_ptr() for mu in range(4)])
-            tab_b = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in pv])
-            nmv = getattr(L, f"QLA_{pc}_V_vpeq_nM_times_npV")
-            ms_nm = _events_time(torch, stream, lambda: nmv(V(Vo), tab_a, tab_b, n, 4), reps * 4)
-            t_sp = _events_time(torch, stream, lambda: sp(V(H), V(D), 0, 1, n), reps * 4)
-            t_mh = _events_time(torch, stream, lambda: mh(V(H2), V(U[0]), V(H), V(nbr[(0, 1)]), n), reps * 4)
-            t_rc = _events_time(torch, stream, lambda: rc(V(Out), V(H2), 0, 1, n), reps * 4)
-            mv = getattr(L, f"QLA_{pc}_V_eq_M_times_xV")
-            t_mv = _events_time(torch, stream, lambda: mv(V(Vo), V(U[0]), V(Vv), V(nbr[(0, 1)]), n), reps * 4)
-            ptrs = (Vv.data_ptr() + nbr[(0, 1)].long() * 24 * e).contiguous()
-            mvp = getattr(L, f"QLA_{pc}_V_veq_M_times_pV")
-            t_mvp = _events_time(torch, stream, lambda: mvp(V(Vo), V(U[0]), V(ptrs), n), reps * 4)
-            qla.check("hop")
-            b = {"spproj": 144 * e, "M_times_xH": 168 * e + 4, "sprecon": 240 * e, "M_times_xV": 120 * e + 4,
-                 "M_times_pV": 120 * e + 8}
-            tk = {"spproj": t_sp, "M_times_xH": t_mh, "sprecon": t_rc, "M_times_xV": t_mv, "M_times_pV": t_mvp}
-            res[pc] = {"site_updates_per_s": n / (ms / 1e3), "ms_per_hop": ms,
-                       "nM_times_npV_nd4": {"us": 1e3 * ms_nm, "gbs": (4 * (72 * e + 8 + 24 * e) + 48 * e) * n /
-                                            (ms_nm / 1e3) / 1e9,
-                                            "frac": (4 * (72 * e + 8 + 24 * e) + 48 * e) * n / (ms_nm / 1e3) / 1e9
-                                            / peak},
-                       "fused": {"op": f"QLA_{pc}_D_peq_spproj_M_times_xD", "ms_per_hop": ms_f,
-                                 "site_updates_per_s": n / (ms_f / 1e3),
-                                 "hbm_frac": n * 8 * (364 * e) / (ms_f / 1e3) / 1e9 / peak,
-                                 "speedup_vs_unfused": ms / ms_f},
-                       "hbm_frac_hop": n * 8 * sum(b[k] for k in ("spproj", "M_times_xH", "sprecon")) / (ms / 1e3)
-                       / 1e9 / peak,
-                       "kernels": {k: {"us": 1e3 * tk[k], "gbs": b[k] * n / (tk[k] / 1e3) / 1e9,
-                                       "frac": b[k] * n / (tk[k] / 1e3) / 1e9 / peak} for k in tk}}
-            del D, Out, H, H2, U, Vv, Vo, nbr, ptrs, pv
-            torch.cuda.empty_cache()
-        out.update({"metric": "Wilson-hop level-1 sequence (8 x spproj, M_times_xH, vpeq_sprecon), 32^3x64",
-                    "unit": "site-updates/s", "value": res["F3"]["site_updates_per_s"], "F3": res["F3"],
-                    "D3": res["D3"], "speedup_vs_fp64": res["F3"]["ms_per_hop"] and
-                    res["D3"]["ms_per_hop"] / res["F3"]["ms_per_hop"]})
+        out.update(hop_figures(torch, qla, L, stream, peak, reps))
     elif args.workload == "batched":
-        rng = np.random.default_rng(4)
-        choices = [8, 12, 16, 20, 24, 32]
-        dims_list = [[int(x) for x in rng.choice(choices, 4)] for _ in range(64)]
-        vols = [int(np.prod(d)) for d in dims_list]
-
-        def make(dlist):
-            """one field per lattice: links u, u2, vector v, +mu neighbour table"""
-            fl = []
-            for k, dims in enumerate(dlist):
-                n = int(np.prod(dims))
-                nbr = torch.empty(n, dtype=torch.int32, device="cuda")
-                qla.shift_index(nbr, dims, k % 4, 1)
-                fl.append({"r": torch.empty(n, 18, device="cuda"), "u": torch.randn(n, 18, device="cuda"),
-                           "u2": torch.randn(n, 18, device="cuda"), "nbr": nbr,
-                           "w": torch.empty(n, 6, device="cuda"), "v": torch.randn(n, 6, device="cuda"), "n": n})
-            return fl
-        tot = sum(vols)
-        uneven = make(dims_list)
-        plan = qla.BatchPlan(uneven)
-        g = torch.cuda.CUDAGraph()
-        s2 = torch.cuda.Stream()
-        with torch.cuda.stream(s2):
-            qla.set_stream(s2)
-            plan.run()
-            torch.cuda.synchronize()
-            with torch.cuda.graph(g, stream=s2):
-                plan.run()
-        qla.set_stream(stream)
-        ms_b = _events_time(torch, stream, g.replay, reps)
-        mxm, mxv = L.QLA_F3_M_eq_M_times_xM, L.QLA_F3_V_veq_M_times_V
-
-        def separate():
-            for f in uneven:
-                mxm(V(f["r"]), V(f["u"]), V(f["u2"]), V(f["nbr"]), f["n"])
-                mxv(V(f["w"]), V(f["r"]), V(f["v"]), f["n"])
-        ms_s = _events_time(torch, stream, separate, reps)
-        del g
-        plan.close()
-        del uneven
-        torch.cuda.empty_cache()
-        # equal-volume batch of the same total: 64 lattices 16x16x16xLt
-        lt = max(1, round(tot / 64 / 4096))
-        even_n = 4096 * lt
-        even = make([[16, 16, 16, lt]] * 64)
-        plan_e = qla.BatchPlan(even)
-        ms_e = _events_time(torch, stream, plan_e.run, reps)
-        plan_e.close()
-        qla.check("batched")
-        rate_b = tot / (ms_b / 1e3)
-        rate_e = 64 * even_n / (ms_e / 1e3)
-        out.update({"metric": "batched uneven-volume M_times_xM + M_times_V (64 F3 fields, extents in "
-                              "{8..32}^4), one persistent launch replayed from a CUDA graph",
-                    "unit": "site-updates/s", "value": rate_b, "total_sites": tot,
-                    "ms_batched_graph": ms_b, "ms_128_separate_launches": ms_s,
-                    "speedup_vs_separate": ms_s / ms_b, "equal_volume_rate": rate_e,
-                    "uneven_vs_equal_volume": rate_b / rate_e,
-                    "hbm_frac": rate_b * (72 * 3 + 24 * 2 + 4) / 1e9 / peak,
-                    "bytes_per_site": "U 72 + U2 gather 72 + nbr 4 + V 24 + R 72 + W 24 = 268"})
+        out.update(batched_figures(torch, qla, L, stream, peak, reps))
     elif args.workload == "mfunc":
         # every colour-matrix function of the code templates on 32^3x64
         # sites; the reference library (host cores, OpenMP) on a 32,768-site
@@ -894,6 +933,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the reduction accuracy check")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="leave the config-2 / config-4 figures out of the benchmark line")
     ap.add_argument("--workload", default="cg_chain", choices=["cg_chain", "hop", "batched", "mfunc", "prop", "ewise", "fields", "config1"],
                     help="cg_chain is the benchmark line; the others measure the remaining configurations")
     args = ap.parse_args()

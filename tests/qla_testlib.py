@@ -95,6 +95,45 @@ def haar_su3(rng, n, dtype=np.float32, nc=3):
     return out.reshape(n, 2 * nc * nc).astype(dtype)
 
 
+def qla_rng_gaussian(seed, n, nreal):
+    """n records of nreal float N(0,1) deviates drawn the way a QLA program
+    draws them: site i's generator seeded by QLA_seed_random(&S[i], seed, i)
+    (lib/random/QLA_seed_random.c:13-34), then nreal successive QLA_gaussian
+    calls on it (lib/random/QLA_gaussian.c:40-50, Box-Muller), through the
+    oracle's restatement of both (pinned to the reference's lib/random)."""
+    O = oracle()
+    st = np.zeros((n, 11), np.uint32)
+    O.ora_rng_seedfield(ptr(st), int(seed), ptr(np.arange(n, dtype=np.int32)), ctypes.c_long(n), None, None)
+    g = np.zeros((n, nreal), np.float32)
+    O.ora_rng_fill_f(nreal, 1, 0, ptr(g), ptr(st), ctypes.c_long(n), None, None)
+    return g
+
+
+def qla_rng_haar_su3(seed, n, dtype=np.float32):
+    """n Haar-random SU(3) links from QLA's generator: per site 18 QLA_gaussian
+    deviates (qla_rng_gaussian) form a complex Gaussian 3x3 (row-major
+    [ic][jc], re/im interleaved), whose columns go through modified
+    Gram-Schmidt QR in FP64; column j is multiplied by R_jj / |R_jj| (the
+    phase fix), the matrix is divided by the principal cube root of its
+    determinant, and the result is rounded to `dtype`."""
+    g = qla_rng_gaussian(seed, n, 18).astype(np.float64)
+    z = (g[:, 0::2] + 1j * g[:, 1::2]).reshape(n, 3, 3)
+    q = np.empty_like(z)
+    rdiag = np.empty((n, 3), dtype=np.complex128)
+    for j in range(3):
+        v = z[:, :, j].copy()
+        for k in range(j):
+            rkj = np.sum(np.conj(q[:, :, k]) * v, axis=1)
+            v = v - rkj[:, None] * q[:, :, k]
+        rjj = np.sqrt(np.sum(np.abs(v) ** 2, axis=1))
+        q[:, :, j] = v / rjj[:, None]
+        rdiag[:, j] = rjj
+    q = q * (rdiag / np.abs(rdiag))[:, None, :]
+    det = np.linalg.det(q)
+    q = q / np.power(det, 1.0 / 3.0)[:, None, None]
+    return from_complex(q, dtype)
+
+
 def lattice_dims_volume(dims):
     v = 1
     for d in dims:

@@ -725,3 +725,18 @@ def test_oracle_real_complex_field_libraries_match_reference_library(lib):
             bad.append(e["name"])
     assert count >= (64 if lib == "DF" else 900)
     assert not bad, f"{len(bad)} mismatches, e.g. {bad[:10]}"
+
+
+@pytest.mark.skipif(not T.ref_available(), reason="oracle/_ref/libqla_ref.so not built")
+def test_qla_rng_inputs_match_the_reference_generator():
+    """The per-site generator draws used for the config-1 inputs
+    (qla_testlib.qla_rng_gaussian) are the reference library's own
+    QLA_seed_random / QLA_gaussian deviates."""
+    R = T.ref()
+    R.QLA_gaussian.restype = ctypes.c_float
+    g = T.qla_rng_gaussian(1234, 64, 18)
+    for i in (0, 1, 17, 63):
+        st = np.zeros(11, np.uint32)
+        R.QLA_seed_random(T.ptr(st), 1234, i)
+        want = np.array([R.QLA_gaussian(T.ptr(st)) for _ in range(18)], np.float32)
+        assert np.array_equal(g[i], want), i
