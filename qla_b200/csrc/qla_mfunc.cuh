@@ -6,17 +6,18 @@
 //    restated with explicitly rounded operations in the site precision:
 //    bit-identical to the reference for F3 and D3.
 //  sqrt: the reference's Newton iteration (M_eq_sqrt_M.c:139-180, with the
-//    Gauss-Jordan solve of M_eq_M_inverse_M.c:108-135), always evaluated in
-//    FP64 with the FP64 stopping threshold: bit-identical to QLA_D3 for D3
-//    inputs; for F3 inputs the FP64 result of the promoted matrix, rounded
-//    once to float (more accurate than the reference's FP32 iteration).
+//    Gauss-Jordan solve of M_eq_M_inverse_M.c:108-135) in the site precision,
+//    the template's own arithmetic (matrices in float for F3, |a|_F and the
+//    stopping norm in double, FLT_EPSILON / DBL_EPSILON threshold):
+//    bit-identical to QLA_F3 and QLA_D3.
 //  exp: Cayley-Hamilton-reduced Taylor series with FP64 coefficients.  With
 //    B = A / 2^k (|B|_F <= 1) and B^3 = c2 B^2 + c1 B + c0 1, every power
 //    B^j / j! = q0 1 + q1 B + q2 B^2 where (q0,q1,q2) follow the recurrence
-//    q' = (q2 c0, q0 + q2 c1, q1 + q2 c2) / (j+1); summing 26 terms gives
+//    q' = (q2 c0, q0 + q2 c1, q1 + q2 c2) / (j+1); summing the terms gives
 //    exp(B) = f0 1 + f1 B + f2 B^2 with no eigenvalues involved, so nearly
-//    degenerate spectra need no special case; then k squarings.  All of it in
-//    FP64; F3 outputs are rounded once to float.  The reference's F3/D3 use a
+//    degenerate spectra need no special case; then k squarings.  D3: all of
+//    it in FP64 (26 terms).  F3: only the coefficients in FP64 (16 terms);
+//    B^2, the assembly and the squarings in FP32.  The reference's F3/D3 use a
 //    rational approximation with scaling (M_eq_exp_M.c:302-367); agreement is
 //    checked against its FP64 (D3) result.
 #pragma once
@@ -208,11 +209,14 @@ __device__ __forceinline__ void gj_solve3(Cx<R> (&c)[9], Cx<R> (&d)[3 * NB]) {
     for (int j = 0; j < NB; j++) d[i * NB + j] = cmul(c[i * 3 + i], d[i * NB + j]);
 }
 
-// Newton loop of M_eq_sqrt_M.c:158-171 / M_eq_invsqrt_M.c:160-173 in FP64:
-// e <- -1/2 e x^-1 e, x += e until |e|_F^2 <= DBL_EPSILON or 20 iterations.
-__device__ __forceinline__ void newton_sqrt3(Cx<double> (&x)[9], Cx<double> (&e)[9]) {
-  const double eps = 2.220446049250313080847e-16;  // DBL_EPSILON
-  Cx<double> c[9], d[9];
+// Newton loop of M_eq_sqrt_M.c:158-171 / M_eq_invsqrt_M.c:160-173 in the
+// site precision R, the templates' own arithmetic (QLA_F3 in float, QLA_D3 in
+// double): e <- -1/2 e x^-1 e, x += e until |e|_F^2 <= EPS (FLT_EPSILON or
+// DBL_EPSILON; the norm's terms in R, summed in double) or 20 iterations.
+template <typename R>
+__device__ __forceinline__ void newton_sqrt3(Cx<R> (&x)[9], Cx<R> (&e)[9]) {
+  const double eps = sizeof(R) == 4 ? 1.1920928955078125e-07 : 2.220446049250313080847e-16;
+  Cx<R> c[9], d[9];
   int nit = 0;
   double enorm;
   do {
@@ -226,65 +230,192 @@ __device__ __forceinline__ void newton_sqrt3(Cx<double> (&x)[9], Cx<double> (&e)
     mat3_mul(c, e, d);  // c = e x^-1 e
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      e[k] = Cx<double>{__dmul_rn(-0.5, c[k].re), __dmul_rn(-0.5, c[k].im)};
-      x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
+      e[k] = Cx<R>{rmul(R(-0.5), c[k].re), rmul(R(-0.5), c[k].im)};
+      x[k] = Cx<R>{radd(x[k].re, e[k].re), radd(x[k].im, e[k].im)};
     }
     enorm = fnorm2_3(e);
   } while (nit < 20 && enorm > eps);
 }
 
-// M_eq_sqrt_M (QLA_D3 arithmetic): r = sqrt(a)
-__device__ __forceinline__ void sqrt3_fp64(Cx<double> (&r)[9], const Cx<double> (&a)[9]) {
+// M_eq_sqrt_M in the site precision R: r = sqrt(a).  ds = |a|_F is formed in
+// double and enters as (R)(1/ds) and (R)sqrt(ds), as the template's
+// M_eq_d_times_M does (QLA_Real rr = d).
+template <typename R>
+__device__ __forceinline__ void sqrt3(Cx<R> (&r)[9], const Cx<R> (&a)[9]) {
   double ds = fnorm2_3(a);
   if (ds == 0.0) {
 #pragma unroll
-    for (int k = 0; k < 9; k++) r[k] = Cx<double>{0.0, 0.0};
+    for (int k = 0; k < 9; k++) r[k] = Cx<R>{R(0), R(0)};
     return;
   }
   ds = __dsqrt_rn(ds);
-  Cx<double> x[9], e[9];
-  const double inv = __ddiv_rn(1.0, ds);
+  Cx<R> x[9], e[9];
+  const R inv = (R)__ddiv_rn(1.0, ds);
 #pragma unroll
   for (int k = 0; k < 9; k++) {
-    x[k] = Cx<double>{__dmul_rn(inv, a[k].re), __dmul_rn(inv, a[k].im)};  // x = a / ds
-    const double dg = (k % 4 == 0) ? 0.5 : 0.0;                          // e = 0.5 1
-    e[k] = Cx<double>{__dadd_rn(dg, __dmul_rn(-0.5, x[k].re)), __dadd_rn(0.0, __dmul_rn(-0.5, x[k].im))};
-    x[k] = Cx<double>{__dadd_rn(x[k].re, e[k].re), __dadd_rn(x[k].im, e[k].im)};
+    x[k] = Cx<R>{rmul(inv, a[k].re), rmul(inv, a[k].im)};  // x = a / ds
+    const R dg = (k % 4 == 0) ? R(0.5) : R(0);               // e = 0.5 1 - 0.5 x
+    e[k] = Cx<R>{radd(dg, rmul(R(-0.5), x[k].re)), radd(R(0), rmul(R(-0.5), x[k].im))};
+    x[k] = Cx<R>{radd(x[k].re, e[k].re), radd(x[k].im, e[k].im)};
   }
   newton_sqrt3(x, e);
-  const double sds = __dsqrt_rn(ds);
+  const R sds = (R)__dsqrt_rn(ds);
 #pragma unroll
-  for (int k = 0; k < 9; k++) r[k] = Cx<double>{__dmul_rn(sds, x[k].re), __dmul_rn(sds, x[k].im)};
+  for (int k = 0; k < 9; k++) r[k] = Cx<R>{rmul(sds, x[k].re), rmul(sds, x[k].im)};
 }
 
-// M_eq_sqrt_M (Newton), FP64
+// M_eq_sqrt_M (Newton) in the site precision: bit-identical to QLA_F3 / QLA_D3
 template <typename R_>
 struct SqrtOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
   __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                Cx<R> (&r)[9]) {
-    Cx<double> ad[9], rd[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) ad[k] = cd(a[k]);
-    sqrt3_fp64(rd, ad);
-#pragma unroll
-    for (int k = 0; k < 9; k++) r[k] = cround<R>(rd[k]);
+    sqrt3(r, a);
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                double*) {}
   __device__ static void finish(const SiteParams&, const double*) {}
 };
 
+// plain complex arithmetic (the compiler may fuse multiply-adds): for the
+// F3 exp, whose result is not tied to the reference's rounding sequence
+template <typename T>
+__device__ __forceinline__ Cx<T> cmul_fast(Cx<T> a, Cx<T> b) {
+  return Cx<T>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T>
+__device__ __forceinline__ void mat3_mul_fast(Cx<T> (&r)[9], const Cx<T> (&a)[9], const Cx<T> (&b)[9]) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      Cx<T> x = cmul_fast(a[i * 3], b[j]);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        const Cx<T> t = cmul_fast(a[i * 3 + k], b[k * 3 + j]);
+        x.re += t.re;
+        x.im += t.im;
+      }
+      r[i * 3 + j] = x;
+    }
+}
+template <typename T>
+__device__ __forceinline__ Cx<T> det3_fast(const Cx<T> (&a)[9]) {
+  Cx<T> m0 = cmul_fast(a[4], a[8]), m1 = cmul_fast(a[5], a[7]);
+  Cx<T> n0 = cmul_fast(a[3], a[8]), n1 = cmul_fast(a[5], a[6]);
+  Cx<T> o0 = cmul_fast(a[3], a[7]), o1 = cmul_fast(a[4], a[6]);
+  const Cx<T> c0{m0.re - m1.re, m0.im - m1.im}, c1{n0.re - n1.re, n0.im - n1.im}, c2{o0.re - o1.re, o0.im - o1.im};
+  const Cx<T> t0 = cmul_fast(a[0], c0), t1 = cmul_fast(a[1], c1), t2 = cmul_fast(a[2], c2);
+  return Cx<T>{t0.re - t1.re + t2.re, t0.im - t1.im + t2.im};
+}
+
 // ---------------------------------------------------------------------------
-// M_eq_exp_M: Cayley-Hamilton-reduced Taylor series in FP64 (see header)
+// M_eq_exp_M: Cayley-Hamilton-reduced Taylor series (see header)
 template <typename R_>
 struct ExpOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
   static constexpr int kTerms = 26;
-  __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
-                               Cx<R> (&r)[9]) {
+  // F3: 16 terms (the neglected tail is below 1/17! < 3e-15 of the result's
+  // scale when |B|_F <= 1)
+  static constexpr int kTermsF3 = 16;
+  __device__ static void apply(const SiteParams& p, const Cx<R> (&a)[9], const Cx<R> (&x1)[1],
+                               const Cx<R> (&x2)[1], Cx<R> (&r)[9]) {
+    if constexpr (sizeof(R) == 4)
+      apply_f3(a, r);
+    else
+      apply_d3(p, a, x1, x2, r);
+  }
+
+  // F3: FP64 only for the Cayley-Hamilton coefficients (the traces, the
+  // determinant and the Taylor recurrence on q0, q1, q2, computed from the
+  // exactly promoted float B); B^2, the assembly f0 + f1 B + f2 B^2 and the
+  // squarings in FP32 with fused multiply-adds.
+  __device__ static void apply_f3(const Cx<float> (&a)[9], Cx<float> (&r)[9]) {
+    double fn = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) fn = fma((double)a[k].im, (double)a[k].im, fma((double)a[k].re, (double)a[k].re, fn));
+    // B = A / 2^ks with |B|_F^2 <= 1: fn < 2^E, so ks = ceil(E / 2) suffices
+    int ks = 0;
+    if (fn > 1.0) {
+      int E;
+      frexp(fn, &E);
+      ks = (E + 1) >> 1;
+      if (ks > 60) ks = 60;
+    }
+    const float sc = ldexpf(1.0f, -ks);  // exact power of two
+    Cx<float> b[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) b[k] = Cx<float>{a[k].re * sc, a[k].im * sc};
+    // coefficients in FP64: tr B, tr B^2 = sum_ik b_ik b_ki, det B
+    Cx<double> bd[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) bd[k] = cd(b[k]);
+    const Cx<double> trb{bd[0].re + bd[4].re + bd[8].re, bd[0].im + bd[4].im + bd[8].im};
+    Cx<double> trb2{0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const Cx<double> u = bd[i * 3 + k], v = bd[k * 3 + i];
+        trb2.re = fma(u.re, v.re, fma(-u.im, v.im, trb2.re));
+        trb2.im = fma(u.re, v.im, fma(u.im, v.re, trb2.im));
+      }
+    const Cx<double> c2 = trb;
+    const Cx<double> c1{-0.5 * (trb.re * trb.re - trb.im * trb.im - trb2.re),
+                        -0.5 * (2.0 * trb.re * trb.im - trb2.im)};
+    const Cx<double> c0 = det3_fast(bd);
+    Cx<double> q0{1.0, 0.0}, q1{0.0, 0.0}, q2{0.0, 0.0};
+    Cx<double> f0 = q0, f1 = q1, f2 = q2;
+#pragma unroll 3
+    for (int j = 1; j < kTermsF3; j++) {
+      const double inv = 1.0 / (double)j;
+      const Cx<double> n0 = cmul_fast(q2, c0);
+      Cx<double> n1 = cmul_fast(q2, c1);
+      Cx<double> n2 = cmul_fast(q2, c2);
+      n1.re += q0.re;
+      n1.im += q0.im;
+      n2.re += q1.re;
+      n2.im += q1.im;
+      q0 = Cx<double>{n0.re * inv, n0.im * inv};
+      q1 = Cx<double>{n1.re * inv, n1.im * inv};
+      q2 = Cx<double>{n2.re * inv, n2.im * inv};
+      f0.re += q0.re;
+      f0.im += q0.im;
+      f1.re += q1.re;
+      f1.im += q1.im;
+      f2.re += q2.re;
+      f2.im += q2.im;
+    }
+    const Cx<float> g0{(float)f0.re, (float)f0.im}, g1{(float)f1.re, (float)f1.im}, g2{(float)f2.re, (float)f2.im};
+    // FP32: B^2, the assembly, the squarings
+    Cx<float> b2[9], e[9];
+    mat3_mul_fast(b2, b, b);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      Cx<float> t = cmul_fast(g1, b[k]);
+      const Cx<float> u = cmul_fast(g2, b2[k]);
+      t.re += u.re;
+      t.im += u.im;
+      if (k % 4 == 0) {
+        t.re += g0.re;
+        t.im += g0.im;
+      }
+      e[k] = t;
+    }
+    for (int s = 0; s < ks; s++) {
+      mat3_mul_fast(b2, e, e);
+#pragma unroll
+      for (int k = 0; k < 9; k++) e[k] = b2[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) r[k] = e[k];
+  }
+
+  // D3: the whole evaluation in FP64
+  __device__ static void apply_d3(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
+                                  Cx<R> (&r)[9]) {
     Cx<double> b[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) b[k] = cd(a[k]);

@@ -14,13 +14,15 @@
 //
 // Precision.  a^-1 b uses only +, -, *, / and is evaluated in the site
 // precision with explicitly rounded operations: bit-identical to QLA_F3 and
-// QLA_D3.  Every other function is evaluated in FP64 for both F3 and D3 --
-// the coefficients of the cubic, the Newton iterates and the closed-form
+// QLA_D3.  invsqrt and log run the templates' Newton iteration and rational
+// approximation in the site precision too (the templates' own arithmetic:
+// float matrices with double norms for F3), so they equal QLA_F3's and
+// QLA_D3's results except where CUDA's log of |a|_F and the host libm's
+// differ in the last place.  The closed forms are evaluated in FP64 for both
+// F3 and D3 -- the coefficients of the cubic and the closed-form
 // coefficients near degenerate eigenvalues are where FP32 loses digits --
 // in the templates' operation order with explicitly rounded FP64 arithmetic,
-// and the F3 result is rounded once to float.  invsqrt and log call only
-// sqrt and (log) one log of |a|_F, so D3 results equal QLA_D3's except where
-// CUDA's log and the host libm's differ in the last place; the closed forms
+// and the F3 result is rounded once to float; the closed forms
 // call acos, sincos, cbrt, pow and atan2, whose CUDA and host-libm results
 // may differ by an ulp, so D3 agrees with QLA_D3 to a few ulps away from
 // the templates' branch points.
@@ -137,44 +139,59 @@ struct MInverseOp {
 };
 
 // ---------------------------------------------------------------------------
-// M_eq_invsqrt_M: x = 1, e = 0.5 |a|_F a^-1 - 0.5, Newton, r = x / sqrt|a|_F
+// M_eq_invsqrt_M: x = 1, e = 0.5 |a|_F a^-1 - 0.5, Newton, r = x / sqrt|a|_F,
+// in the site precision (double scalars enter as (R)(0.5 ds) and
+// (R)(1/sqrt ds), as the template's M_eq_d_times_M does)
 template <typename R_>
 struct InvsqrtOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = 9, N1 = 0, N2 = 0, NOUT = 9, NACC = 0;
   __device__ static void apply(const SiteParams&, const Cx<R> (&a)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                Cx<R> (&r)[9]) {
-    Cx<double> ad[9];
-    promote9(ad, a);
-    double ds = fnorm2_3(ad);
+    double ds = fnorm2_3(a);
     if (ds == 0.0) {  // M_eq_d(r, 1./0.)
 #pragma unroll
       for (int k = 0; k < 9; k++) r[k] = Cx<R>{(k % 4 == 0) ? R(INFINITY) : R(0), R(0)};
       return;
     }
     ds = __dsqrt_rn(ds);
-    Cx<double> xi[9], x[9], e[9];
-    inv3(xi, ad);
-    const double hds = dmul(0.5, ds);
+    Cx<R> xi[9], x[9], e[9];
+    inv3(xi, a);
+    const R hds = (R)dmul(0.5, ds);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const bool dg = (k % 4 == 0);
-      e[k] = Cx<double>{dadd(dg ? -0.5 : 0.0, dmul(hds, xi[k].re)), dadd(0.0, dmul(hds, xi[k].im))};
-      x[k] = Cx<double>{dadd(dg ? 1.0 : 0.0, e[k].re), dadd(0.0, e[k].im)};
+      e[k] = Cx<R>{radd(dg ? R(-0.5) : R(0), rmul(hds, xi[k].re)), radd(R(0), rmul(hds, xi[k].im))};
+      x[k] = Cx<R>{radd(dg ? R(1) : R(0), e[k].re), radd(R(0), e[k].im)};
     }
     newton_sqrt3(x, e);
-    const double rr = ddiv(1.0, __dsqrt_rn(ds));
+    const R rr = (R)ddiv(1.0, __dsqrt_rn(ds));
 #pragma unroll
-    for (int k = 0; k < 9; k++) r[k] = cround<R>(Cx<double>{dmul(rr, x[k].re), dmul(rr, x[k].im)});
+    for (int k = 0; k < 9; k++) r[k] = Cx<R>{rmul(rr, x[k].re), rmul(rr, x[k].im)};
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],
                                double*) {}
   __device__ static void finish(const SiteParams&, const double*) {}
 };
 
+// m += s * a (QLA_<P>3_M_peq_r_times_M) and m = d 1 (QLA_<P>3_M_eq_c with a
+// real constant) in the site precision
+template <typename R>
+__device__ __forceinline__ void m_peq_r_m_site(Cx<R> (&m)[9], R s, const Cx<R> (&a)[9]) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) m[k] = Cx<R>{radd(m[k].re, rmul(s, a[k].re)), radd(m[k].im, rmul(s, a[k].im))};
+}
+template <typename R>
+__device__ __forceinline__ void m_eq_d_site(Cx<R> (&m)[9], R d) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) m[k] = Cx<R>{(k % 4 == 0) ? d : R(0), R(0)};
+}
+
 // ---------------------------------------------------------------------------
 // M_eq_log_M: as = a/|a|_F, four square roots, log(1+x) with the template's
-// rational coefficients, times 16, plus log|a|_F on the diagonal
+// rational coefficients, times 16, plus log|a|_F on the diagonal -- in the
+// site precision (the coefficients enter as (R)P, (R)Q; log|a|_F is added in
+// double and rounded, as `r += ds` does with a double ds)
 template <typename R_>
 struct LogOp {
   using R = R_;
@@ -187,58 +204,57 @@ struct LogOp {
     constexpr double Q0 = 2.31251620126765340583E1, Q1 = 7.11544750618563894466E1,
                      Q2 = 8.29875266912776603211E1, Q3 = 4.52279145837532221105E1,
                      Q4 = 1.12873587189167450590E1;
-    Cx<double> as[9], t[9];
-    promote9(as, a);
-    double ds = __dsqrt_rn(fnorm2_3(as));
+    Cx<R> as[9], t[9];
+    double ds = __dsqrt_rn(fnorm2_3(a));
     if (ds == 0.0) {  // M_eq_d(r, log(0))
 #pragma unroll
       for (int k = 0; k < 9; k++) r[k] = Cx<R>{(k % 4 == 0) ? R(-INFINITY) : R(0), R(0)};
       return;
     }
-    const double rr = ddiv(1.0, ds);
+    const R rr = (R)ddiv(1.0, ds);
 #pragma unroll
-    for (int k = 0; k < 9; k++) as[k] = Cx<double>{dmul(rr, as[k].re), dmul(rr, as[k].im)};
+    for (int k = 0; k < 9; k++) as[k] = Cx<R>{rmul(rr, a[k].re), rmul(rr, a[k].im)};
 #pragma unroll 1
     for (int i = 0; i < 4; i++) {
 #pragma unroll
       for (int k = 0; k < 9; k++) t[k] = as[k];
-      sqrt3_fp64(as, t);
+      sqrt3(as, t);
     }
 #pragma unroll
-    for (int i = 0; i < 3; i++) as[i * 4].re = dsub(as[i * 4].re, 1.0);
-    Cx<double> pa[9], qa[9], as2[9], as3[9];
-    m_eq_d(pa, P0);
-    m_eq_d(qa, Q0);
-    m_peq_r_m(pa, P1, as);
-    m_peq_r_m(qa, Q1, as);
+    for (int i = 0; i < 3; i++) as[i * 4].re = rsub(as[i * 4].re, R(1));
+    Cx<R> pa[9], qa[9], as2[9], as3[9];
+    m_eq_d_site(pa, (R)P0);
+    m_eq_d_site(qa, (R)Q0);
+    m_peq_r_m_site(pa, (R)P1, as);
+    m_peq_r_m_site(qa, (R)Q1, as);
     mat3_mul(as2, as, as);
-    m_peq_r_m(pa, P2, as2);
-    m_peq_r_m(qa, Q2, as2);
+    m_peq_r_m_site(pa, (R)P2, as2);
+    m_peq_r_m_site(qa, (R)Q2, as2);
     mat3_mul(as3, as, as2);
-    m_peq_r_m(pa, P3, as3);
-    m_peq_r_m(qa, Q3, as3);
+    m_peq_r_m_site(pa, (R)P3, as3);
+    m_peq_r_m_site(qa, (R)Q3, as3);
     mat3_mul(t, as2, as2);  // as4
-    m_peq_r_m(pa, P4, t);
-    m_peq_r_m(qa, Q4, t);
+    m_peq_r_m_site(pa, (R)P4, t);
+    m_peq_r_m_site(qa, (R)Q4, t);
     {
-      Cx<double> as5[9];
+      Cx<R> as5[9];
       mat3_mul(as5, as, t);
-      m_peq_r_m(pa, P5, as5);
+      m_peq_r_m_site(pa, (R)P5, as5);
 #pragma unroll
-      for (int k = 0; k < 9; k++) qa[k] = Cx<double>{dadd(qa[k].re, as5[k].re), dadd(qa[k].im, as5[k].im)};
+      for (int k = 0; k < 9; k++) qa[k] = Cx<R>{radd(qa[k].re, as5[k].re), radd(qa[k].im, as5[k].im)};
     }
     inv3(t, qa);        // as5 = qa^-1
     mat3_mul(qa, pa, t);
     mat3_mul(pa, as3, qa);
-    m_peq_r_m(pa, -0.5, as2);
+    m_peq_r_m_site(pa, R(-0.5), as2);
 #pragma unroll
-    for (int k = 0; k < 9; k++) pa[k] = Cx<double>{dadd(pa[k].re, as[k].re), dadd(pa[k].im, as[k].im)};
+    for (int k = 0; k < 9; k++) pa[k] = Cx<R>{radd(pa[k].re, as[k].re), radd(pa[k].im, as[k].im)};
     ds = log(ds);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      Cx<double> v{dmul(16.0, pa[k].re), dmul(16.0, pa[k].im)};
-      if (k % 4 == 0) v.re = dadd(v.re, ds);
-      r[k] = cround<R>(v);
+      Cx<R> v{rmul(R(16), pa[k].re), rmul(R(16), pa[k].im)};
+      if (k % 4 == 0) v.re = (R)dadd((double)v.re, ds);
+      r[k] = v;
     }
   }
   __device__ static void accum(const SiteParams&, const Cx<R> (&)[9], const Cx<R> (&)[1], const Cx<R> (&)[1],

@@ -15,9 +15,12 @@ using CxArr1 = Cx<R>[1];
 // r (eqop) A * B, A = a | a^+ (colour matrix), B = b (NC x NCOL) | b^+ (matrix).
 // Restates lib/perl/build_qla.pl:1588-1622 + expressions_tensor.pl:766: per
 // output element x = (peq|meq ? r : 0); x (+|-)= A(i,k) B(k,s) for k in order.
-template <typename R, int NC, int NCOL, bool ADJA, bool ADJB>
-__device__ __forceinline__ void lmult_site(int eqop, bool load, const Cx<R> (&a)[NC * NC],
-                                           const Cx<R> (&b)[NC * NCOL], Cx<R> (&y)[NC * NCOL]) {
+// (the record arrays may be longer than the records: callers that keep
+// records of several kinds in one fixed-size array pass that array)
+template <typename R, int NC, int NCOL, bool ADJA, bool ADJB, int LA, int LB, int LY>
+__device__ __forceinline__ void lmult_site(int eqop, bool load, const Cx<R> (&a)[LA], const Cx<R> (&b)[LB],
+                                           Cx<R> (&y)[LY]) {
+  static_assert(LA >= NC * NC && LB >= NC * NCOL && LY >= NC * NCOL, "record array too short");
   const bool minus = (eqop == MEQ || eqop == EQM);
 #pragma unroll
   for (int ic = 0; ic < NC; ic++) {
@@ -176,8 +179,9 @@ struct SpprojOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = NC * 4, N1 = 0, N2 = 0, NOUT = NC * 2, NACC = 0;
   struct Body {
-    template <int MU, int SG>
-    __device__ __forceinline__ static void run(int eqop, const Cx<R> (&a)[N0], Cx<R> (&y)[NOUT]) {
+    template <int MU, int SG, int LA, int LY>
+    __device__ __forceinline__ static void run(int eqop, const Cx<R> (&a)[LA], Cx<R> (&y)[LY]) {
+      static_assert(LA >= N0 && LY >= NOUT, "record array too short");
       constexpr int k0 = SpinTables::spproj[SG][MU][0][0], a0 = SpinTables::spproj[SG][MU][0][1],
                     b0 = SpinTables::spproj[SG][MU][0][2];
       constexpr int k1 = SpinTables::spproj[SG][MU][1][0], a1 = SpinTables::spproj[SG][MU][1][1],
@@ -204,8 +208,9 @@ struct SpreconOp {
   using R = R_;
   static constexpr int NIN = 1, N0 = NC * 2, N1 = 0, N2 = 0, NOUT = NC * 4, NACC = 0;
   struct Body {
-    template <int MU, int SG>
-    __device__ __forceinline__ static void run(int eqop, const Cx<R> (&h)[N0], Cx<R> (&y)[NOUT]) {
+    template <int MU, int SG, int LH, int LY>
+    __device__ __forceinline__ static void run(int eqop, const Cx<R> (&h)[LH], Cx<R> (&y)[LY]) {
+      static_assert(LH >= N0 && LY >= NOUT, "record array too short");
       constexpr int o0 = SpinTables::sprecon[SG][MU][0][0], s0 = SpinTables::sprecon[SG][MU][0][1];
       constexpr int o1 = SpinTables::sprecon[SG][MU][1][0], s1 = SpinTables::sprecon[SG][MU][1][1];
       constexpr int o2 = SpinTables::sprecon[SG][MU][2][0], s2 = SpinTables::sprecon[SG][MU][2][1];

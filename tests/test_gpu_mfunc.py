@@ -2,9 +2,9 @@
 config-5-shaped inputs, through the C-ABI.
 
   det, inverse : bit-identical to the reference's closed forms (F3 and D3);
-  sqrt         : the reference's Newton iteration in FP64 -- bit-identical to
-                 QLA_D3 for D3, and for F3 exactly the FP64 result of the
-                 promoted input rounded to float;
+  sqrt         : the reference's Newton iteration in the site precision --
+                 bit-identical to QLA_F3 and QLA_D3; F3 within
+                 1e-5 * max(1, |A|_F) of the FP64 result of the same input;
   exp          : Cayley-Hamilton/Taylor in FP64, compared with the reference
                  algorithm evaluated in FP64 (QLA_D3, bit-pinned oracle):
                  D3 |diff| <= 1e-13 * max(1, |A|_F^2) elementwise for the
@@ -57,14 +57,16 @@ def test_det_inverse_bit_exact(qla, pc, dt):
         assert T.bits_equal(got[gang], want[gang]), fname + " xeq"
 
 
-def test_sqrt_bit_exact_fp64_newton(qla):
+def test_sqrt_bit_exact_newton(qla):
     rng = np.random.default_rng(22)
     n = 50021
     ad = T.positive_hermitian_inputs(rng, n, np.float64)
     assert T.bits_equal(_run(qla, "D3", "sqrt", ad, n), T.ora_mfunc(ad, n, "sqrt"))
     af = ad.astype(np.float32)
-    want = T.ora_mfunc(af.astype(np.float64), n, "sqrt").astype(np.float32)
-    assert T.bits_equal(_run(qla, "F3", "sqrt", af, n), want)
+    got = _run(qla, "F3", "sqrt", af, n)
+    assert T.bits_equal(got, T.ora_mfunc(af, n, "sqrt"))   # the reference's FP32 iteration
+    scale = np.maximum(1.0, np.sqrt(np.sum(af.astype(np.float64) ** 2, axis=1)))[:, None]
+    assert (np.abs(got - T.ora_mfunc(af.astype(np.float64), n, "sqrt")) / scale).max() <= 1e-5
     # and the result squares back to the input
     s = T.to_complex(_run(qla, "D3", "sqrt", ad, n))
     assert np.max(np.abs(s @ s - T.to_complex(ad))) < 1e-12 * np.max(np.abs(T.to_complex(ad)))

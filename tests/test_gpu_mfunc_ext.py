@@ -3,14 +3,16 @@
 Tolerances (all against the bit-pinned oracle restatement of the reference):
 
   M_inverse_V, M_inverse_M : bit-identical to QLA_F3 / QLA_D3 (+, -, *, / only).
-  invsqrt                  : the reference's Newton iteration in FP64 --
-                             bit-identical to QLA_D3; F3 equals the FP64
-                             result of the promoted input rounded to float.
-  log                      : FP64; D3 differs from QLA_D3 only through CUDA's
-                             log of |A|_F on the diagonal:
-                             |diff| <= 2 eps64 (|r_ii| + |log|A|_F|).
-                             F3 within the reference test rule (16 eps abs or
-                             10 eps rel, FLT_EPSILON) of the FP64 value.
+  invsqrt                  : the reference's Newton iteration in the site
+                             precision -- bit-identical to QLA_F3 and QLA_D3.
+  log                      : the reference's algorithm in the site precision;
+                             it differs from QLA_D3 / QLA_F3 only through
+                             CUDA's log of |A|_F on the diagonal:
+                             D3 |diff| <= 2 eps64 (|r_ii| + |log|A|_F|),
+                             F3 at most one float ulp on the diagonal.
+  F3 sqrt, invsqrt, log    : within 1e-5 max(1, |A|_F) of the FP64 result of
+                             the same input (the reference's FP32 algorithms
+                             measure <= 2.3e-6).
   expTA, expA, sqrtPH,     : the templates' closed forms in FP64.  Against
   invsqrtPH, eigenvalsH,     QLA_D3: <= 1e-13 relative to max(1, |A|_F^2) on
   eigenvals                  well-separated spectra; on the near-degenerate
@@ -110,7 +112,7 @@ def test_m_inverse_m_solves(qla):
     assert np.max(np.abs(T.to_complex(a) @ x - np.eye(3))) < 1e-10
 
 
-def test_invsqrt_bit_exact_fp64_newton(qla):
+def test_invsqrt_bit_exact_newton(qla):
     rng = np.random.default_rng(33)
     n = 50021
     ad = T.positive_hermitian_inputs(rng, n, np.float64)
@@ -119,13 +121,15 @@ def test_invsqrt_bit_exact_fp64_newton(qla):
     assert T.bits_equal(got, T.ora_mfunc(ad, n, "invsqrt"))
     assert np.isinf(got[0, 0]) and got[0, 0] > 0
     af = ad.astype(np.float32)
-    want = T.ora_mfunc(af.astype(np.float64), n, "invsqrt").astype(np.float32)
-    assert T.bits_equal(_run(qla, "F3", "invsqrt", af, n), want)
+    gotf = _run(qla, "F3", "invsqrt", af, n)
+    assert T.bits_equal(gotf, T.ora_mfunc(af, n, "invsqrt"))   # the reference's FP32 iteration
+    scale = np.maximum(1.0, np.sqrt(np.sum(af.astype(np.float64) ** 2, axis=1)))[1:, None]
+    assert (np.abs(gotf[1:] - T.ora_mfunc(af.astype(np.float64), n, "invsqrt")[1:]) / scale).max() <= 1e-5
     s = T.to_complex(got[1:])
     assert np.max(np.abs(s @ s @ T.to_complex(ad[1:]) - np.eye(3))) < 1e-10
 
 
-def test_log_fp64(qla):
+def test_log_site_precision(qla):
     rng = np.random.default_rng(34)
     n = 40009
     a = T.positive_hermitian_inputs(rng, n, np.float64)
@@ -152,9 +156,15 @@ def test_log_fp64(qla):
     assert np.max(np.abs(back - T.to_complex(a[1:1000]))) < 1e-9 * np.max(np.abs(a[1:1000]))
     af = a.astype(np.float32)
     gotf = _run(qla, "F3", "log", af, n)
+    wantf = T.ora_mfunc(af, n, "log")    # the reference's FP32 algorithm
+    assert np.array_equal(np.isinf(gotf), np.isinf(wantf))
+    assert np.array_equal(gotf[1:][:, ~diag[0]], wantf[1:][:, ~diag[0]])
+    dd = np.abs(gotf[1:][:, diag[0]].astype(np.float64) - wantf[1:][:, diag[0]])
+    assert np.all(dd <= np.spacing(np.abs(wantf[1:][:, diag[0]])))
+    print(f"log F3: {np.mean(np.all(gotf[1:] == wantf[1:], axis=1)):.4f} of sites bit-identical")
     ref64 = T.ora_mfunc(af.astype(np.float64), n, "log")
-    ok, nbad = T.qla_close(gotf[1:], ref64[1:], np.float32)
-    assert ok, nbad
+    scale = np.maximum(1.0, np.sqrt(np.sum(af.astype(np.float64) ** 2, axis=1)))[1:, None]
+    assert (np.abs(gotf[1:] - ref64[1:]) / scale).max() <= 1e-5
 
 
 @pytest.mark.parametrize("fname", ["expTA", "expA"])
