@@ -439,14 +439,17 @@ def run_gpu_arm(args):
 
     # ---------------- the other north-star targets on the same GPU (N=1):
     # config-2 per-kernel HBM fractions and the hop sequence, config-4 batched
-    # launch (its HBM fraction and its uneven / equal-volume ratio); CUDA
-    # events on the launching stream, inputs larger than L2
+    # launch (its HBM fraction and its uneven / equal-volume ratio), the
+    # DiracPropagator products and the F3 matrix exp; CUDA events on the
+    # launching stream, inputs larger than L2
     extra = {}
     if world == 1 and not args.no_extra:
         reps = max(args.steps, 5)
         extra["config2_hop"] = hop_figures(torch, qla, qla.lib(), stream, peak, reps)
         torch.cuda.empty_cache()
         extra["config4_batched"] = batched_figures(torch, qla, qla.lib(), stream, peak, reps)
+        torch.cuda.empty_cache()
+        extra["prop_and_exp"] = prop_mfunc_figures(torch, qla, qla.lib(), stream, peak, reps)
         torch.cuda.empty_cache()
         qla.check("secondary configurations")
         if qla.device_error():
@@ -693,6 +696,43 @@ def batched_figures(torch, qla, L, stream, peak, reps):
                 "uneven_vs_equal_volume": rate_b / rate_e,
                 "hbm_frac": rate_b * (72 * 3 + 24 * 2 + 4) / 1e9 / peak,
                 "bytes_per_site": "U 72 + U2 gather 72 + nbr 4 + V 24 + R 72 + W 24 = 268"})
+    return out
+
+
+def prop_mfunc_figures(torch, qla, L, stream, peak, reps):
+    """The DiracPropagator products P*P and P^+*P (16^3x32 sites, 3456
+    algorithmic bytes per site F3) and the F3 matrix exp (32^3x64 sites of
+    i Q, Q traceless Hermitian with Frobenius norm uniform in [0, 3 sqrt 2];
+    144 bytes per site), CUDA events on the launching stream, inputs larger
+    than L2."""
+    V = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    out = {}
+    n = 16 * 16 * 16 * 32
+    for pc, dt, e in (("F3", torch.float32, 4), ("D3", torch.float64, 8)):
+        pa = torch.randn(n, 288, device="cuda", dtype=dt)
+        pb = torch.randn(n, 288, device="cuda", dtype=dt)
+        pr = torch.empty(n, 288, device="cuda", dtype=dt)
+        for nm in ("P_veq_P_times_P", "P_veq_Pa_times_P"):
+            f = getattr(L, f"QLA_{pc}_{nm}")
+            ms = _events_time(torch, stream, lambda f=f: f(V(pr), V(pa), V(pb), n), reps)
+            gbs = 3 * 288 * e * n / (ms / 1e3) / 1e9
+            out[f"{pc}_{nm}"] = {"site_updates_per_s": n / (ms / 1e3), "us": 1e3 * ms, "gbs": gbs,
+                                 "hbm_frac": gbs / peak, "sites": n}
+        del pa, pb, pr
+    n = 32 * 32 * 32 * 64
+    q = torch.randn(n, 3, 3, device="cuda", dtype=torch.complex128)
+    q = 0.5 * (q + q.conj().transpose(1, 2))
+    q = q - (torch.diagonal(q, dim1=1, dim2=2).sum(-1) / 3)[:, None, None] * torch.eye(3, device="cuda")
+    fro = torch.sqrt((q.abs() ** 2).sum(dim=(1, 2)))
+    q = q * (torch.rand(n, device="cuda", dtype=torch.float64) * 3 * 2 ** 0.5 / fro)[:, None, None]
+    a = torch.view_as_real((1j * q).reshape(n, 9)).reshape(n, 18).to(torch.float32).contiguous()
+    r = torch.empty_like(a)
+    del q
+    ms = _events_time(torch, stream, lambda: L.QLA_F3_M_veq_exp_M(V(r), V(a), n), reps)
+    out["F3_M_veq_exp_M"] = {"site_updates_per_s": n / (ms / 1e3), "us": 1e3 * ms,
+                             "gbs": 144 * n / (ms / 1e3) / 1e9, "sites": n,
+                             "note": "FP64 Cayley-Hamilton coefficients, FP32 assembly and squarings"}
+    del a, r
     return out
 
 

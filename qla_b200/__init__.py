@@ -185,6 +185,17 @@ def shift_index(idx, dims, mu, sign):
     check("qlagpu_shift_index")
 
 
+def check_index(idx, n, nsrc):
+    """qlagpu_check_index: (return code, first bad position or -1) for the
+    int32 index stream idx[0..n) against [0, nsrc)."""
+    L = lib()
+    L.qlagpu_check_index.restype = ctypes.c_int
+    L.qlagpu_check_index.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_void_p]
+    first = ctypes.c_longlong(-2)
+    rc = L.qlagpu_check_index(_addr(idx), int(n), int(nsrc), ctypes.byref(first))
+    return rc, first.value
+
+
 def version():
     return lib().qlagpu_version().decode()
 
@@ -231,3 +242,71 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# batched sequences (qlagpu_F3_batch_plan_program)
+REC = {"V": 0, "H": 1, "D": 2, "M": 3}
+ROLE = {"in": 0, "out": 1, "inout": 2}
+BOP = {"lmult": 0, "spproj": 1, "sprecon": 2, "rtimes": 3, "copy": 4}
+EQOP = {"eq": 0, "peq": 1, "meq": 2, "eqm": 3}
+REG0, REG1 = 8, 9
+
+
+class _BatchStream(ctypes.Structure):
+    _fields_ = [("base", ctypes.c_void_p), ("index", ctypes.c_void_p), ("nsrc", ctypes.c_longlong),
+                ("kind", ctypes.c_int), ("role", ctypes.c_int)]
+
+
+class _BatchStep(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int), ("eqop", ctypes.c_int), ("a", ctypes.c_int), ("b", ctypes.c_int),
+                ("dst", ctypes.c_int), ("store", ctypes.c_int), ("adja", ctypes.c_int), ("adjb", ctypes.c_int),
+                ("mu", ctypes.c_int), ("sign", ctypes.c_int), ("r", ctypes.c_float)]
+
+
+class _BatchProgram(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_longlong), ("nstreams", ctypes.c_int), ("nsteps", ctypes.c_int),
+                ("stream", _BatchStream * 8), ("step", _BatchStep * 8)]
+
+
+class BatchProgramPlan(BatchPlan):
+    """Plan of per-field level-1 programs (qlagpu_F3_batch_plan_program), all
+    fields in one persistent launch.  `programs` is a list of dicts:
+
+        {"n": sites,
+         "streams": [{"base": tensor, "index": int32 tensor or None, "nsrc": 0,
+                      "kind": "V"|"H"|"D"|"M", "role": "in"|"out"|"inout"}, ...],
+         "steps": [{"op": "lmult"|"spproj"|"sprecon"|"rtimes"|"copy",
+                    "eqop": "eq"|"peq"|"meq"|"eqm", "a": stream or REG0/REG1,
+                    "b": ..., "dst": REG0|REG1, "store": stream or -1,
+                    "adja": 0, "adjb": 0, "mu": 0, "sign": 1, "r": 0.0}, ...]}
+    """
+
+    def __init__(self, programs):
+        L = lib()
+        L.qlagpu_F3_batch_plan_program.restype = ctypes.c_void_p
+        L.qlagpu_F3_batch_plan_program.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.qlagpu_batch_run.restype = ctypes.c_int
+        L.qlagpu_batch_run.argtypes = [ctypes.c_void_p]
+        L.qlagpu_batch_destroy.argtypes = [ctypes.c_void_p]
+        arr = (_BatchProgram * len(programs))()
+        for k, pr in enumerate(programs):
+            q = arr[k]
+            q.n = int(pr["n"])
+            q.nstreams = len(pr["streams"])
+            q.nsteps = len(pr["steps"])
+            for j, st in enumerate(pr["streams"]):
+                idx = st.get("index")
+                q.stream[j] = _BatchStream(_addr(st["base"]), _addr(idx) if idx is not None else None,
+                                           int(st.get("nsrc", 0)), REC[st["kind"]], ROLE[st["role"]])
+            for j, sp in enumerate(pr["steps"]):
+                q.step[j] = _BatchStep(BOP[sp["op"]], EQOP[sp.get("eqop", "eq")], int(sp["a"]), int(sp.get("b", 0)),
+                                       int(sp.get("dst", REG0)), int(sp.get("store", -1)), int(sp.get("adja", 0)),
+                                       int(sp.get("adjb", 0)), int(sp.get("mu", 0)), int(sp.get("sign", 1)),
+                                       float(sp.get("r", 0.0)))
+        self._keep = programs
+        self.handle = L.qlagpu_F3_batch_plan_program(ctypes.cast(arr, ctypes.c_void_p), len(programs))
+        if not self.handle:
+            check("qlagpu_F3_batch_plan_program")
+            raise QLAError("qlagpu_F3_batch_plan_program failed")
+

@@ -7,50 +7,62 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D2_D_veq_gamma_times_D(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int n) {
+  QLAB_TRACE("QLA_D2_D_veq_gamma_times_D");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_contig(a), mu, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_veq_gamma_times_pD(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int n) {
+  QLAB_TRACE("QLA_D2_D_veq_gamma_times_pD");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), mu, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_veq_gamma_times_P(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int n) {
+  QLAB_TRACE("QLA_D2_P_veq_gamma_times_P");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_veq_gamma_times_pP(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int n) {
+  QLAB_TRACE("QLA_D2_P_veq_gamma_times_pP");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_veq_P_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int n) {
+  QLAB_TRACE("QLA_D2_P_veq_P_times_gamma");
   qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_veq_pP_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int n) {
+  QLAB_TRACE("QLA_D2_P_veq_pP_times_gamma");
   qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_xeq_gamma_times_D(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int * index, int n) {
+  QLAB_TRACE("QLA_D2_D_xeq_gamma_times_D");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_contig(a), mu, index, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_xeq_gamma_times_pD(QLA_D2_DiracFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int * index, int n) {
+  QLAB_TRACE("QLA_D2_D_xeq_gamma_times_pD");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), mu, index, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_xeq_gamma_times_P(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int * index, int n) {
+  QLAB_TRACE("QLA_D2_P_xeq_gamma_times_P");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, index, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_xeq_gamma_times_pP(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int * index, int n) {
+  QLAB_TRACE("QLA_D2_P_xeq_gamma_times_pP");
   qlab::api_gamma_n<double, true>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, index, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_xeq_P_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ a, int mu, int * index, int n) {
+  QLAB_TRACE("QLA_D2_P_xeq_P_times_gamma");
   qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_contig(a), mu, index, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_xeq_pP_times_gamma(QLA_D2_DiracPropagator *__restrict__ r, QLA_D2_DiracPropagator *__restrict__ * a, int mu, int * index, int n) {
+  QLAB_TRACE("QLA_D2_P_xeq_pP_times_gamma");
   qlab::api_gamma_n<double, false>("D2_gamma", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), mu, index, n);
 }
 

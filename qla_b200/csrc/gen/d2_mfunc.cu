@@ -6,66 +6,82 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D2_M_veq_exp_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_exp_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_sqrt_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_sqrt_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_inverse_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_inverse_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_C_veq_det_M(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_C_veq_det_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_exp_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_exp_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_sqrt_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_sqrt_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_inverse_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_inverse_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_C_veq_det_pM(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_C_veq_det_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_exp_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_exp_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_sqrt_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_sqrt_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_inverse_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_inverse_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_C_xeq_det_M(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_C_xeq_det_M");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("D2_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_exp_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_exp_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_sqrt_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_sqrt_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_inverse_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_inverse_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_D2_C_xeq_det_pM(QLA_D_Complex *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_C_xeq_det_pM");
   qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("D2_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 

@@ -7,82 +7,102 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D2_V_veq_gaussian_S(QLA_D2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_V_veq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2, 1, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_V_veq_gaussian_pS(QLA_D2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_V_veq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_H_veq_gaussian_S(QLA_D2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_H_veq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_H_veq_gaussian_pS(QLA_D2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_H_veq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_veq_gaussian_S(QLA_D2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_D_veq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 4 * 2, 1, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_veq_gaussian_pS(QLA_D2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_D_veq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 4 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_gaussian_S(QLA_D2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_M_veq_gaussian_pS(QLA_D2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_M_veq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_veq_gaussian_S(QLA_D2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D2_P_veq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 16 * 2 * 2, 1, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_veq_gaussian_pS(QLA_D2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D2_P_veq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 16 * 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_V_xeq_gaussian_S(QLA_D2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_V_xeq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2, 1, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_V_xeq_gaussian_pS(QLA_D2_ColorVector *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_V_xeq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_H_xeq_gaussian_S(QLA_D2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xeq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_H_xeq_gaussian_pS(QLA_D2_HalfFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xeq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_xeq_gaussian_S(QLA_D2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_D_xeq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 4 * 2, 1, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_D_xeq_gaussian_pS(QLA_D2_DiracFermion *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_D_xeq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 4 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_gaussian_S(QLA_D2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_M_xeq_gaussian_pS(QLA_D2_ColorMatrix *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_M_xeq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_xeq_gaussian_S(QLA_D2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_P_xeq_gaussian_S");
   qlab::api_rng_fill_n<double>("D2_random", 2, 16 * 2 * 2, 1, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_P_xeq_gaussian_pS(QLA_D2_DiracPropagator *__restrict__ r, QLA_RandomState *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D2_P_xeq_gaussian_pS");
   qlab::api_rng_fill_n<double>("D2_random", 2, 16 * 2 * 2, 1, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -5,130 +5,162 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D2_r_veq_re_V_dot_V(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ a, QLA_D2_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_V_dot_V");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_V_dot_pV(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ a, QLA_D2_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_V_dot_pV");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pV_dot_V(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ * a, QLA_D2_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pV_dot_V");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pV_dot_pV(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ * a, QLA_D2_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pV_dot_pV");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_V_dot_V(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ a, QLA_D2_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_V_dot_V");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_V_dot_pV(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ a, QLA_D2_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_V_dot_pV");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pV_dot_V(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ * a, QLA_D2_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pV_dot_V");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pV_dot_pV(QLA_D_Real *__restrict__ r, QLA_D2_ColorVector *__restrict__ * a, QLA_D2_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pV_dot_pV");
   qlab::api_reduce<qlab::ReDotOp<double, 2, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_H_dot_H(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ a, QLA_D2_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_H_dot_H");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_H_dot_pH(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ a, QLA_D2_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_H_dot_pH");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pH_dot_H(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ * a, QLA_D2_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pH_dot_H");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pH_dot_pH(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ * a, QLA_D2_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pH_dot_pH");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_H_dot_H(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ a, QLA_D2_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_H_dot_H");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_H_dot_pH(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ a, QLA_D2_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_H_dot_pH");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pH_dot_H(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ * a, QLA_D2_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pH_dot_H");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pH_dot_pH(QLA_D_Real *__restrict__ r, QLA_D2_HalfFermion *__restrict__ * a, QLA_D2_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pH_dot_pH");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_D_dot_D(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, QLA_D2_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_D_dot_D");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_D_dot_pD(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, QLA_D2_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_D_dot_pD");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pD_dot_D(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, QLA_D2_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pD_dot_D");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pD_dot_pD(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, QLA_D2_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pD_dot_pD");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_D_dot_D(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, QLA_D2_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_D_dot_D");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_D_dot_pD(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, QLA_D2_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_D_dot_pD");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pD_dot_D(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, QLA_D2_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pD_dot_D");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pD_dot_pD(QLA_D_Real *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, QLA_D2_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pD_dot_pD");
   qlab::api_reduce<qlab::ReDotOp<double, 8, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_M_dot_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, QLA_D2_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_M_dot_M");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_M_dot_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, QLA_D2_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_M_dot_pM");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pM_dot_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, QLA_D2_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pM_dot_M");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_veq_re_pM_dot_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, QLA_D2_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_D2_r_veq_re_pM_dot_pM");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_M_dot_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, QLA_D2_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_M_dot_M");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_M_dot_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ a, QLA_D2_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_M_dot_pM");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pM_dot_M(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, QLA_D2_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pM_dot_M");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_D2_r_xeq_re_pM_dot_pM(QLA_D_Real *__restrict__ r, QLA_D2_ColorMatrix *__restrict__ * a, QLA_D2_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_D2_r_xeq_re_pM_dot_pM");
   qlab::api_reduce<qlab::ReDotOp<double, 4, double>>("D2_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 

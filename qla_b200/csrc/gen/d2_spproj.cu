@@ -5,81 +5,97 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D2_H_veq_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_veq_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_veq_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_veq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_vpeq_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_vpeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_vpeq_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_vpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_vmeq_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_vmeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_vmeq_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_vmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_veqm_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_veqm_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_veqm_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_D2_H_veqm_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xeq_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xeq_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xpeq_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xpeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xpeq_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xmeq_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xmeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xmeq_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xeqm_spproj_D(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xeqm_spproj_D");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_D2_H_xeqm_spproj_pD(QLA_D2_HalfFermion *__restrict__ r, QLA_D2_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_D2_H_xeqm_spproj_pD");
   if (mu < 0 || mu > 4) return;
   qlab::api_map<qlab::SpprojOp<double, 2>>("D2_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign);
 }

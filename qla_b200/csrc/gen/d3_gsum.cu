@@ -6,82 +6,102 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D3_v_veq_sum_V(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_v_veq_sum_V");
   qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_v_veq_sum_pV(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_v_veq_sum_pV");
   qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_h_veq_sum_H(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_h_veq_sum_H");
   qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_h_veq_sum_pH(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_h_veq_sum_pH");
   qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_d_veq_sum_D(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_d_veq_sum_D");
   qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_d_veq_sum_pD(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_d_veq_sum_pD");
   qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_m_veq_sum_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_m_veq_sum_M");
   qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_m_veq_sum_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_m_veq_sum_pM");
   qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_p_veq_sum_P(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_p_veq_sum_P");
   qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_p_veq_sum_pP(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_p_veq_sum_pP");
   qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_v_xeq_sum_V(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_v_xeq_sum_V");
   qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_v_xeq_sum_pV(QLA_D3_ColorVector *__restrict__ r, QLA_D3_ColorVector *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_v_xeq_sum_pV");
   qlab::api_gsum<double, 3>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_h_xeq_sum_H(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_h_xeq_sum_H");
   qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_h_xeq_sum_pH(QLA_D3_HalfFermion *__restrict__ r, QLA_D3_HalfFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_h_xeq_sum_pH");
   qlab::api_gsum<double, 6>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_d_xeq_sum_D(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_d_xeq_sum_D");
   qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_d_xeq_sum_pD(QLA_D3_DiracFermion *__restrict__ r, QLA_D3_DiracFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_d_xeq_sum_pD");
   qlab::api_gsum<double, 12>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_m_xeq_sum_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_m_xeq_sum_M");
   qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_m_xeq_sum_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_m_xeq_sum_pM");
   qlab::api_gsum<double, 9>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_p_xeq_sum_P(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_p_xeq_sum_P");
   qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_p_xeq_sum_pP(QLA_D3_DiracPropagator *__restrict__ r, QLA_D3_DiracPropagator *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_p_xeq_sum_pP");
   qlab::api_gsum<double, 144>("D3_gsum", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -5,66 +5,82 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D3_r_veq_norm2_V(QLA_D_Real *__restrict__ r, QLA_D3_ColorVector *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_V");
   qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("D3_norm2_V", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_pV(QLA_D_Real *__restrict__ r, QLA_D3_ColorVector *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_pV");
   qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("D3_norm2_V", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_V(QLA_D_Real *__restrict__ r, QLA_D3_ColorVector *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_V");
   qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("D3_norm2_V", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_pV(QLA_D_Real *__restrict__ r, QLA_D3_ColorVector *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_pV");
   qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("D3_norm2_V", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_H(QLA_D_Real *__restrict__ r, QLA_D3_HalfFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_H");
   qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("D3_norm2_H", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_pH(QLA_D_Real *__restrict__ r, QLA_D3_HalfFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_pH");
   qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("D3_norm2_H", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_H(QLA_D_Real *__restrict__ r, QLA_D3_HalfFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_H");
   qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("D3_norm2_H", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_pH(QLA_D_Real *__restrict__ r, QLA_D3_HalfFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_pH");
   qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("D3_norm2_H", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_D(QLA_D_Real *__restrict__ r, QLA_D3_DiracFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_D");
   qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("D3_norm2_D", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_pD(QLA_D_Real *__restrict__ r, QLA_D3_DiracFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_pD");
   qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("D3_norm2_D", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_D(QLA_D_Real *__restrict__ r, QLA_D3_DiracFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_D");
   qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("D3_norm2_D", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_pD(QLA_D_Real *__restrict__ r, QLA_D3_DiracFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_pD");
   qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("D3_norm2_D", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_M(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_M");
   qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("D3_norm2_M", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_veq_norm2_pM(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_r_veq_norm2_pM");
   qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("D3_norm2_M", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_M(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_M");
   qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("D3_norm2_M", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_D3_r_xeq_norm2_pM(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_r_xeq_norm2_pM");
   qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("D3_norm2_M", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 

@@ -6,66 +6,82 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_D3_C_veq_trace_M(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_C_veq_trace_M");
   qlab::api_trace<double, qlab::SF_TRACE_C>("D3_trace", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_veq_re_trace_M(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_R_veq_re_trace_M");
   qlab::api_trace<double, qlab::SF_TRACE_RE>("D3_trace", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_veq_im_trace_M(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_R_veq_im_trace_M");
   qlab::api_trace<double, qlab::SF_TRACE_IM>("D3_trace", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_M_veq_antiherm_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_D3_M_veq_antiherm_M");
   qlab::api_antiherm<double>("D3_trace", r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_C_veq_trace_pM(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_C_veq_trace_pM");
   qlab::api_trace<double, qlab::SF_TRACE_C>("D3_trace", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_veq_re_trace_pM(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_R_veq_re_trace_pM");
   qlab::api_trace<double, qlab::SF_TRACE_RE>("D3_trace", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_veq_im_trace_pM(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_R_veq_im_trace_pM");
   qlab::api_trace<double, qlab::SF_TRACE_IM>("D3_trace", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_M_veq_antiherm_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_D3_M_veq_antiherm_pM");
   qlab::api_antiherm<double>("D3_trace", r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_D3_C_xeq_trace_M(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_C_xeq_trace_M");
   qlab::api_trace<double, qlab::SF_TRACE_C>("D3_trace", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_xeq_re_trace_M(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_R_xeq_re_trace_M");
   qlab::api_trace<double, qlab::SF_TRACE_RE>("D3_trace", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_xeq_im_trace_M(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_R_xeq_im_trace_M");
   qlab::api_trace<double, qlab::SF_TRACE_IM>("D3_trace", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_M_xeq_antiherm_M(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_M_xeq_antiherm_M");
   qlab::api_antiherm<double>("D3_trace", r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_C_xeq_trace_pM(QLA_D_Complex *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_C_xeq_trace_pM");
   qlab::api_trace<double, qlab::SF_TRACE_C>("D3_trace", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_xeq_re_trace_pM(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_R_xeq_re_trace_pM");
   qlab::api_trace<double, qlab::SF_TRACE_RE>("D3_trace", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_R_xeq_im_trace_pM(QLA_D_Real *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_R_xeq_im_trace_pM");
   qlab::api_trace<double, qlab::SF_TRACE_IM>("D3_trace", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_D3_M_xeq_antiherm_pM(QLA_D3_ColorMatrix *__restrict__ r, QLA_D3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_D3_M_xeq_antiherm_pM");
   qlab::api_antiherm<double>("D3_trace", r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -7,1538 +7,1922 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_P_veq_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_conj_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_conj_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_i_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_i_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_Pa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pPa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_transpose_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_transpose_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_conj_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_conj_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_i_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_i_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_Pa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pPa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_transpose_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_transpose_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vpeq_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vpeq_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_conj_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_conj_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_i_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_i_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_Pa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pPa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_transpose_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_transpose_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_vmeq_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_vmeq_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_conj_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_conj_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_i_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_i_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_Pa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pPa(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_transpose_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_transpose_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veqm_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_P_veqm_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_P_plus_P(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_P_plus_P");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_P_plus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_P_plus_P");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_P_plus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_P_plus_P");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_P_minus_P(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_P_minus_P");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_P_minus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_P_minus_P");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_P_minus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_P_minus_P");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_P_plus_pP(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_P_plus_pP");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_P_plus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_P_plus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_P_plus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_P_plus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_P_minus_pP(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_P_minus_pP");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_P_minus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_P_minus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_P_minus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_P_minus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pP_plus_P(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pP_plus_P");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_pP_plus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_pP_plus_P");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_pP_plus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_pP_plus_P");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pP_minus_P(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pP_minus_P");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_pP_minus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_pP_minus_P");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_pP_minus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_pP_minus_P");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pP_plus_pP(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pP_plus_pP");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_pP_plus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_pP_plus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_pP_plus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_pP_plus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_pP_minus_pP(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_pP_minus_pP");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_r_times_pP_minus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_r_times_pP_minus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_veq_c_times_pP_minus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_DN_P_veq_c_times_pP_minus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_conj_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_conj_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_i_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_i_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_Pa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pPa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_transpose_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_transpose_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_conj_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_conj_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_i_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_i_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_Pa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pPa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_transpose_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_transpose_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xpeq_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xpeq_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_conj_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_conj_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_i_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_i_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_Pa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pPa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_transpose_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_transpose_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xmeq_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xmeq_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_c_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_c_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_r_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_r_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_c_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_c_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_r_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_r_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_c_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_c_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_r_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_r_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_c_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_c_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_CONST, false>("DN_ew_ctimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_r_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_r_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_CONST, true>("DN_ew_rtimes", nc, 16 * nc * nc, qlab::PERM_P, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_C_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_C_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_C_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_C_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_C_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_C_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_C_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_C_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pC_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pC_times_P");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pC_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pC_times_pP");
   qlab::api_ew_n<double, qlab::EW_CT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pC_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pC_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pC_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pC_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CTA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_Ca_times_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_Ca_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_Ca_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_Ca_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_Ca_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_Ca_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_Ca_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_Ca_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pCa_times_P(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pCa_times_P");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pCa_times_pP(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pCa_times_pP");
   qlab::api_ew_n<double, qlab::EW_CAT, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pCa_times_Pa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pCa_times_Pa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pCa_times_pPa(int nc, void * r, QLA_D_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pCa_times_pPa");
   qlab::api_ew_n<double, qlab::EW_CATA, qlab::SC_FIELD, false>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_R_times_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_R_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_R_times_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_R_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_R_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_R_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_R_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_R_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pR_times_P(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pR_times_P");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pR_times_pP(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pR_times_pP");
   qlab::api_ew_n<double, qlab::EW_RT, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pR_times_Pa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pR_times_Pa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pR_times_pPa(int nc, void * r, QLA_D_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pR_times_pPa");
   qlab::api_ew_n<double, qlab::EW_RTA, qlab::SC_FIELD, true>("DN_ew_field", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_conj_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_conj_P");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_conj_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_conj_pP");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_i_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_i_P");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_i_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_i_pP");
   qlab::api_ew_n<double, qlab::EW_I, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_Pa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_Pa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pPa(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pPa");
   qlab::api_ew_n<double, qlab::EW_CONJ, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_transpose_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_transpose_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_transpose_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_transpose_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_P, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_P");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeqm_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeqm_pP");
   qlab::api_ew_n<double, qlab::EW_COPY, qlab::SC_NONE, false>("DN_ew_unary", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_P_plus_P(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_P_plus_P");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_P_plus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_P_plus_P");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_P_plus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_P_plus_P");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_P_minus_P(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_P_minus_P");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_P_minus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_P_minus_P");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_P_minus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_P_minus_P");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_P_plus_pP(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_P_plus_pP");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_P_plus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_P_plus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_P_plus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_P_plus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_P_minus_pP(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_P_minus_pP");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_P_minus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_P_minus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_P_minus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_P_minus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pP_plus_P(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pP_plus_P");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_pP_plus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_pP_plus_P");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_pP_plus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_pP_plus_P");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pP_minus_P(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pP_minus_P");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_pP_minus_P(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_pP_minus_P");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_pP_minus_P(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_pP_minus_P");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pP_plus_pP(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pP_plus_pP");
   qlab::api_ew_n<double, qlab::EW_PLUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_pP_plus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_pP_plus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_pP_plus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_pP_plus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_pP_minus_pP(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_pP_minus_pP");
   qlab::api_ew_n<double, qlab::EW_MINUS, qlab::SC_NONE, false>("DN_ew_sum", nc, 16 * nc * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_r_times_pP_minus_pP(int nc, void * r, QLA_D_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_r_times_pP_minus_pP");
   qlab::api_ew_n<double, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_P_xeq_c_times_pP_minus_pP(int nc, void * r, QLA_D_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_DN_P_xeq_c_times_pP_minus_pP");
   qlab::api_ew_n<double, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("DN_ew_axpby", nc, 16 * nc * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 

@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_H_veq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -16,6 +17,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_M_times_D(int nc, void * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -27,6 +29,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_M_times_pD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -38,6 +41,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_M_times_D(int nc, void * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -49,6 +53,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_M_times_pD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -60,6 +65,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_M_times_H(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -71,6 +77,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_M_times_pH(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -82,6 +89,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_Ma_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -93,6 +101,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_Ma_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -104,6 +113,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_Ma_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -115,6 +125,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_Ma_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -126,6 +137,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_Ma_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -137,6 +149,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_Ma_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -148,6 +161,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_pM_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -159,6 +173,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_pM_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -170,6 +185,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_pM_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -181,6 +197,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_pM_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -192,6 +209,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_pM_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -203,6 +221,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_pM_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -214,6 +233,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_pMa_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -225,6 +245,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_pMa_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -236,6 +257,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_pMa_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -247,6 +269,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_pMa_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -258,6 +281,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_pMa_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ, mu, sign); break;
@@ -269,6 +293,7 @@ QLAB_EXPORT void QLA_DN_D_veq_sprecon_pMa_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign); break;
@@ -280,6 +305,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_D(int nc, void * r, void * a, int mu, int s
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign); break;
@@ -291,6 +317,7 @@ QLAB_EXPORT void QLA_DN_D_veq_spproj_pD(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -302,6 +329,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -313,6 +341,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -324,6 +353,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -335,6 +365,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -346,6 +377,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_M_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -357,6 +389,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_M_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -368,6 +401,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -379,6 +413,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -390,6 +425,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -401,6 +437,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -412,6 +449,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_Ma_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -423,6 +461,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_Ma_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -434,6 +473,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -445,6 +485,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -456,6 +497,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -467,6 +509,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -478,6 +521,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pM_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -489,6 +533,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pM_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -500,6 +545,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -511,6 +557,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -522,6 +569,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -533,6 +581,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -544,6 +593,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pMa_times_H(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -555,6 +605,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_sprecon_pMa_times_pH(int nc, void * r, void * a, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign); break;
@@ -566,6 +617,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign); break;
@@ -577,6 +629,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -588,6 +641,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -599,6 +653,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -610,6 +665,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -621,6 +677,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -632,6 +689,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_M_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -643,6 +701,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_M_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -654,6 +713,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -665,6 +725,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -676,6 +737,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -687,6 +749,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -698,6 +761,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_Ma_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -709,6 +773,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_Ma_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -720,6 +785,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -731,6 +797,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -742,6 +809,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -753,6 +821,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -764,6 +833,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pM_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -775,6 +845,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pM_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -786,6 +857,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -797,6 +869,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -808,6 +881,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -819,6 +893,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -830,6 +905,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pMa_times_H(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -841,6 +917,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_sprecon_pMa_times_pH(int nc, void * r, void * a, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign); break;
@@ -852,6 +929,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign); break;
@@ -863,6 +941,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -874,6 +953,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -885,6 +965,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -896,6 +977,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -907,6 +989,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -918,6 +1001,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_M_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -929,6 +1013,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_M_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -940,6 +1025,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -951,6 +1037,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -962,6 +1049,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -973,6 +1061,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -984,6 +1073,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_Ma_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -995,6 +1085,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_Ma_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1006,6 +1097,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1017,6 +1109,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1028,6 +1121,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1039,6 +1133,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1050,6 +1145,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pM_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1061,6 +1157,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pM_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1072,6 +1169,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1083,6 +1181,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1094,6 +1193,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1105,6 +1205,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1116,6 +1217,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pMa_times_H(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM, mu, sign); break;
@@ -1127,6 +1229,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_sprecon_pMa_times_pH(int nc, void * r, void * a, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign); break;
@@ -1138,6 +1241,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign); break;
@@ -1149,6 +1253,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1160,6 +1265,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_M_times_D(int nc, void * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1171,6 +1277,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_M_times_pD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1182,6 +1289,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_M_times_D(int nc, void * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1193,6 +1301,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_M_times_pD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1204,6 +1313,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_M_times_H(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1215,6 +1325,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_M_times_pH(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1226,6 +1337,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_Ma_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1237,6 +1349,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_Ma_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1248,6 +1361,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_Ma_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1259,6 +1373,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_Ma_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1270,6 +1385,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_Ma_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1281,6 +1397,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_Ma_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1292,6 +1409,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_pM_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1303,6 +1421,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_pM_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1314,6 +1433,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_pM_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1325,6 +1445,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_pM_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1336,6 +1457,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pM_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1347,6 +1469,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pM_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1358,6 +1481,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_pMa_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1369,6 +1493,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_pMa_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1380,6 +1505,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_pMa_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1391,6 +1517,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_pMa_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ, mu, sign); break;
@@ -1402,6 +1529,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pMa_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ, mu, sign); break;
@@ -1413,6 +1541,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_sprecon_pMa_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign); break;
@@ -1424,6 +1553,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_D(int nc, void * r, void * a, int mu, int s
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign); break;
@@ -1435,6 +1565,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_spproj_pD(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1446,6 +1577,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1457,6 +1589,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1468,6 +1601,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1479,6 +1613,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1490,6 +1625,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_M_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1501,6 +1637,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_M_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1512,6 +1649,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1523,6 +1661,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1534,6 +1673,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1545,6 +1685,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1556,6 +1697,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_Ma_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1567,6 +1709,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_Ma_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1578,6 +1721,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1589,6 +1733,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1600,6 +1745,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1611,6 +1757,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1622,6 +1769,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pM_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1633,6 +1781,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pM_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1644,6 +1793,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1655,6 +1805,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1666,6 +1817,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1677,6 +1829,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ, mu, sign); break;
@@ -1688,6 +1841,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pMa_times_H(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ, mu, sign); break;
@@ -1699,6 +1853,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_sprecon_pMa_times_pH(int nc, void * r, void * a, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign); break;
@@ -1710,6 +1865,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign); break;
@@ -1721,6 +1877,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1732,6 +1889,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1743,6 +1901,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1754,6 +1913,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1765,6 +1925,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1776,6 +1937,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_M_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1787,6 +1949,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_M_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1798,6 +1961,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1809,6 +1973,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1820,6 +1985,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1831,6 +1997,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1842,6 +2009,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_Ma_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1853,6 +2021,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_Ma_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1864,6 +2033,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1875,6 +2045,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1886,6 +2057,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1897,6 +2069,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1908,6 +2081,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pM_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1919,6 +2093,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pM_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1930,6 +2105,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1941,6 +2117,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1952,6 +2129,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1963,6 +2141,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ, mu, sign); break;
@@ -1974,6 +2153,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pMa_times_H(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ, mu, sign); break;
@@ -1985,6 +2165,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_sprecon_pMa_times_pH(int nc, void * r, void * a, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign); break;
@@ -1996,6 +2177,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign); break;
@@ -2007,6 +2189,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2018,6 +2201,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2029,6 +2213,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_M_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_M_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2040,6 +2225,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_M_times_D(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_M_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_M_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2051,6 +2237,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_M_times_pD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_M_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_M_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2062,6 +2249,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_M_times_H(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_M_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_M_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2073,6 +2261,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_M_times_pH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2084,6 +2273,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2095,6 +2285,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_Ma_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_Ma_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2106,6 +2297,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_Ma_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_Ma_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_Ma_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2117,6 +2309,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_Ma_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_Ma_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_Ma_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2128,6 +2321,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_Ma_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_Ma_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_Ma_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2139,6 +2333,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_Ma_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2150,6 +2345,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2161,6 +2357,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pM_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_pM_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2172,6 +2369,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pM_times_D(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pM_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_pM_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2183,6 +2381,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pM_times_pD(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pM_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_pM_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2194,6 +2393,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pM_times_H(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pM_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_pM_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2205,6 +2405,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pM_times_pH(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2216,6 +2417,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2227,6 +2429,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pMa_times_D(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_pMa_times_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2238,6 +2441,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pMa_times_D(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pMa_times_pD(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_pMa_times_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2249,6 +2453,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pMa_times_pD(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pMa_times_H(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_pMa_times_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM, mu, sign); break;
@@ -2260,6 +2465,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pMa_times_H(int nc, void * r, void * a, v
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pMa_times_pH(int nc, void * r, void * a, void * b, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_sprecon_pMa_times_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM, mu, sign); break;
@@ -2271,6 +2477,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_sprecon_pMa_times_pH(int nc, void * r, void * a, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign); break;
@@ -2282,6 +2489,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojDOp<double, 2>>("DN_hop_Dspproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign); break;
@@ -2293,6 +2501,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_eq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_eq_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ, mu, sign); break;
@@ -2304,6 +2513,7 @@ QLAB_EXPORT void QLA_DN_H_eq_spproj_M_times_xD(int nc, void * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_DN_D_eq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eq_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ, mu, sign); break;
@@ -2315,6 +2525,7 @@ QLAB_EXPORT void QLA_DN_D_eq_spproj_M_times_xD(int nc, void * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_DN_D_eq_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eq_sprecon_M_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ, mu, sign); break;
@@ -2326,6 +2537,7 @@ QLAB_EXPORT void QLA_DN_D_eq_sprecon_M_times_xH(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_H_eq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_eq_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ, mu, sign); break;
@@ -2337,6 +2549,7 @@ QLAB_EXPORT void QLA_DN_H_eq_spproj_Ma_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_eq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eq_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ, mu, sign); break;
@@ -2348,6 +2561,7 @@ QLAB_EXPORT void QLA_DN_D_eq_spproj_Ma_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_eq_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eq_sprecon_Ma_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ, mu, sign); break;
@@ -2359,6 +2573,7 @@ QLAB_EXPORT void QLA_DN_D_eq_sprecon_Ma_times_xH(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_peq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_peq_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -2370,6 +2585,7 @@ QLAB_EXPORT void QLA_DN_H_peq_spproj_M_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_peq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_peq_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -2381,6 +2597,7 @@ QLAB_EXPORT void QLA_DN_D_peq_spproj_M_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_peq_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_peq_sprecon_M_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -2392,6 +2609,7 @@ QLAB_EXPORT void QLA_DN_D_peq_sprecon_M_times_xH(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_peq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_peq_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -2403,6 +2621,7 @@ QLAB_EXPORT void QLA_DN_H_peq_spproj_Ma_times_xD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_peq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_peq_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -2414,6 +2633,7 @@ QLAB_EXPORT void QLA_DN_D_peq_spproj_Ma_times_xD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_peq_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_peq_sprecon_Ma_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ, mu, sign); break;
@@ -2425,6 +2645,7 @@ QLAB_EXPORT void QLA_DN_D_peq_sprecon_Ma_times_xH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_meq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_meq_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -2436,6 +2657,7 @@ QLAB_EXPORT void QLA_DN_H_meq_spproj_M_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_meq_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_meq_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -2447,6 +2669,7 @@ QLAB_EXPORT void QLA_DN_D_meq_spproj_M_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_meq_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_meq_sprecon_M_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -2458,6 +2681,7 @@ QLAB_EXPORT void QLA_DN_D_meq_sprecon_M_times_xH(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_meq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_meq_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -2469,6 +2693,7 @@ QLAB_EXPORT void QLA_DN_H_meq_spproj_Ma_times_xD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_meq_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_meq_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -2480,6 +2705,7 @@ QLAB_EXPORT void QLA_DN_D_meq_spproj_Ma_times_xD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_meq_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_meq_sprecon_Ma_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ, mu, sign); break;
@@ -2491,6 +2717,7 @@ QLAB_EXPORT void QLA_DN_D_meq_sprecon_Ma_times_xH(int nc, void * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DN_H_eqm_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_eqm_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 2>>("DN_hop_Hspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM, mu, sign); break;
@@ -2502,6 +2729,7 @@ QLAB_EXPORT void QLA_DN_H_eqm_spproj_M_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_eqm_spproj_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eqm_spproj_M_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, false, 4>>("DN_hop_Dspprojfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM, mu, sign); break;
@@ -2513,6 +2741,7 @@ QLAB_EXPORT void QLA_DN_D_eqm_spproj_M_times_xD(int nc, void * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DN_D_eqm_sprecon_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eqm_sprecon_M_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, false>>("DN_hop_Dspreconfalse", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM, mu, sign); break;
@@ -2524,6 +2753,7 @@ QLAB_EXPORT void QLA_DN_D_eqm_sprecon_M_times_xH(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_H_eqm_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_eqm_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 2>>("DN_hop_Hspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM, mu, sign); break;
@@ -2535,6 +2765,7 @@ QLAB_EXPORT void QLA_DN_H_eqm_spproj_Ma_times_xD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_eqm_spproj_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eqm_spproj_Ma_times_xD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojMultOp<double, 2, true, 4>>("DN_hop_Dspprojtrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM, mu, sign); break;
@@ -2546,6 +2777,7 @@ QLAB_EXPORT void QLA_DN_D_eqm_spproj_Ma_times_xD(int nc, void * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DN_D_eqm_sprecon_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_D_eqm_sprecon_Ma_times_xH");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpreconMultOp<double, 2, true>>("DN_hop_Dsprecontrue", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM, mu, sign); break;

@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_V_veq_M_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -15,6 +16,7 @@ QLAB_EXPORT void QLA_DN_V_veq_M_times_V(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_M_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -25,6 +27,7 @@ QLAB_EXPORT void QLA_DN_V_veq_M_times_pV(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_Ma_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -35,6 +38,7 @@ QLAB_EXPORT void QLA_DN_V_veq_Ma_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_Ma_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -45,6 +49,7 @@ QLAB_EXPORT void QLA_DN_V_veq_Ma_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_pM_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -55,6 +60,7 @@ QLAB_EXPORT void QLA_DN_V_veq_pM_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_pM_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -65,6 +71,7 @@ QLAB_EXPORT void QLA_DN_V_veq_pM_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_pMa_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -75,6 +82,7 @@ QLAB_EXPORT void QLA_DN_V_veq_pMa_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_pMa_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -85,6 +93,7 @@ QLAB_EXPORT void QLA_DN_V_veq_pMa_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_M_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -95,6 +104,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_M_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_M_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -105,6 +115,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_M_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_Ma_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -115,6 +126,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_Ma_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_Ma_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -125,6 +137,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_Ma_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_pM_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -135,6 +148,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_pM_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_pM_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -145,6 +159,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_pM_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_pMa_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -155,6 +170,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_pMa_times_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_pMa_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vpeq_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -165,6 +181,7 @@ QLAB_EXPORT void QLA_DN_V_vpeq_pMa_times_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_M_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -175,6 +192,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_M_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_M_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -185,6 +203,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_M_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_Ma_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -195,6 +214,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_Ma_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_Ma_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -205,6 +225,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_Ma_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_pM_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -215,6 +236,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_pM_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_pM_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -225,6 +247,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_pM_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_pMa_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -235,6 +258,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_pMa_times_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_pMa_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_vmeq_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -245,6 +269,7 @@ QLAB_EXPORT void QLA_DN_V_vmeq_pMa_times_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_M_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -255,6 +280,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_M_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_M_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -265,6 +291,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_M_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_Ma_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -275,6 +302,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_Ma_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_Ma_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -285,6 +313,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_Ma_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_pM_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -295,6 +324,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_pM_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_pM_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -305,6 +335,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_pM_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_pMa_times_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -315,6 +346,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_pMa_times_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_pMa_times_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veqm_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -325,6 +357,7 @@ QLAB_EXPORT void QLA_DN_V_veqm_pMa_times_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_M_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -335,6 +368,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_M_times_V(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_M_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -345,6 +379,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_M_times_pV(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_Ma_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -355,6 +390,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_Ma_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_Ma_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -365,6 +401,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_Ma_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_pM_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -375,6 +412,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_pM_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_pM_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -385,6 +423,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_pM_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_pMa_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -395,6 +434,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_pMa_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_pMa_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -405,6 +445,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_pMa_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_M_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -415,6 +456,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_M_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_M_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -425,6 +467,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_M_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_Ma_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -435,6 +478,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_Ma_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_Ma_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -445,6 +489,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_Ma_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_pM_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -455,6 +500,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_pM_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_pM_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -465,6 +511,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_pM_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_pMa_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -475,6 +522,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_pMa_times_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_pMa_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xpeq_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -485,6 +533,7 @@ QLAB_EXPORT void QLA_DN_V_xpeq_pMa_times_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_M_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -495,6 +544,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_M_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_M_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -505,6 +555,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_M_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_Ma_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -515,6 +566,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_Ma_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_Ma_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -525,6 +577,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_Ma_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_pM_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -535,6 +588,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_pM_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_pM_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -545,6 +599,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_pM_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_pMa_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -555,6 +610,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_pMa_times_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_pMa_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xmeq_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -565,6 +621,7 @@ QLAB_EXPORT void QLA_DN_V_xmeq_pMa_times_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_M_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_M_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -575,6 +632,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_M_times_V(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_M_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_M_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -585,6 +643,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_M_times_pV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_Ma_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_Ma_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -595,6 +654,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_Ma_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_Ma_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_Ma_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -605,6 +665,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_Ma_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_pM_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_pM_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -615,6 +676,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_pM_times_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_pM_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_pM_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -625,6 +687,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_pM_times_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_pMa_times_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_pMa_times_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -635,6 +698,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_pMa_times_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_pMa_times_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeqm_pMa_times_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -645,6 +709,7 @@ QLAB_EXPORT void QLA_DN_V_xeqm_pMa_times_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_V_eq_M_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_eq_M_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -655,6 +720,7 @@ QLAB_EXPORT void QLA_DN_V_eq_M_times_xV(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_V_eq_Ma_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_eq_Ma_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -665,6 +731,7 @@ QLAB_EXPORT void QLA_DN_V_eq_Ma_times_xV(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_peq_M_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_peq_M_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -675,6 +742,7 @@ QLAB_EXPORT void QLA_DN_V_peq_M_times_xV(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_peq_Ma_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_peq_Ma_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -685,6 +753,7 @@ QLAB_EXPORT void QLA_DN_V_peq_Ma_times_xV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_meq_M_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_meq_M_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -695,6 +764,7 @@ QLAB_EXPORT void QLA_DN_V_meq_M_times_xV(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_meq_Ma_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_meq_Ma_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -705,6 +775,7 @@ QLAB_EXPORT void QLA_DN_V_meq_Ma_times_xV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_eqm_M_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_eqm_M_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -715,6 +786,7 @@ QLAB_EXPORT void QLA_DN_V_eqm_M_times_xV(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_V_eqm_Ma_times_xV(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_V_eqm_Ma_times_xV");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 1, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -725,6 +797,7 @@ QLAB_EXPORT void QLA_DN_V_eqm_Ma_times_xV(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_M_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -735,6 +808,7 @@ QLAB_EXPORT void QLA_DN_H_veq_M_times_H(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_M_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -745,6 +819,7 @@ QLAB_EXPORT void QLA_DN_H_veq_M_times_pH(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_Ma_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -755,6 +830,7 @@ QLAB_EXPORT void QLA_DN_H_veq_Ma_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_Ma_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -765,6 +841,7 @@ QLAB_EXPORT void QLA_DN_H_veq_Ma_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_pM_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -775,6 +852,7 @@ QLAB_EXPORT void QLA_DN_H_veq_pM_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_pM_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -785,6 +863,7 @@ QLAB_EXPORT void QLA_DN_H_veq_pM_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_pMa_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -795,6 +874,7 @@ QLAB_EXPORT void QLA_DN_H_veq_pMa_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_pMa_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -805,6 +885,7 @@ QLAB_EXPORT void QLA_DN_H_veq_pMa_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_M_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -815,6 +896,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_M_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_M_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -825,6 +907,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_M_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_Ma_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -835,6 +918,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_Ma_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_Ma_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -845,6 +929,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_Ma_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_pM_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -855,6 +940,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_pM_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_pM_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -865,6 +951,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_pM_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_pMa_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -875,6 +962,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_pMa_times_H(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_pMa_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -885,6 +973,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_pMa_times_pH(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_M_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -895,6 +984,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_M_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_M_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -905,6 +995,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_M_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_Ma_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -915,6 +1006,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_Ma_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_Ma_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -925,6 +1017,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_Ma_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_pM_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -935,6 +1028,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_pM_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_pM_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -945,6 +1039,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_pM_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_pMa_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -955,6 +1050,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_pMa_times_H(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_pMa_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -965,6 +1061,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_pMa_times_pH(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_M_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -975,6 +1072,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_M_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_M_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -985,6 +1083,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_M_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_Ma_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -995,6 +1094,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_Ma_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_Ma_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1005,6 +1105,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_Ma_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_pM_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -1015,6 +1116,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_pM_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_pM_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1025,6 +1127,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_pM_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_pMa_times_H(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -1035,6 +1138,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_pMa_times_H(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_pMa_times_pH(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1045,6 +1149,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_pMa_times_pH(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_M_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1055,6 +1160,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_M_times_H(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_M_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1065,6 +1171,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_M_times_pH(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_Ma_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1075,6 +1182,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_Ma_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_Ma_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1085,6 +1193,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_Ma_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_pM_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1095,6 +1204,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_pM_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_pM_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1105,6 +1215,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_pM_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_pMa_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1115,6 +1226,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_pMa_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_pMa_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1125,6 +1237,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_pMa_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_M_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1135,6 +1248,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_M_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_M_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1145,6 +1259,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_M_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_Ma_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1155,6 +1270,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_Ma_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_Ma_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1165,6 +1281,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_Ma_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_pM_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1175,6 +1292,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_pM_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_pM_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1185,6 +1303,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_pM_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_pMa_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1195,6 +1314,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_pMa_times_H(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_pMa_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1205,6 +1325,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_pMa_times_pH(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_M_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1215,6 +1336,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_M_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_M_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1225,6 +1347,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_M_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_Ma_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1235,6 +1358,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_Ma_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_Ma_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1245,6 +1369,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_Ma_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_pM_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1255,6 +1380,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_pM_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_pM_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1265,6 +1391,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_pM_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_pMa_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1275,6 +1402,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_pMa_times_H(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_pMa_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1285,6 +1413,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_pMa_times_pH(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_M_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_M_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -1295,6 +1424,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_M_times_H(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_M_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_M_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -1305,6 +1435,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_M_times_pH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_Ma_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_Ma_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -1315,6 +1446,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_Ma_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_Ma_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_Ma_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -1325,6 +1457,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_Ma_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_pM_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_pM_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -1335,6 +1468,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_pM_times_H(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_pM_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_pM_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -1345,6 +1479,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_pM_times_pH(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_pMa_times_H(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_pMa_times_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -1355,6 +1490,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_pMa_times_H(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_pMa_times_pH(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_pMa_times_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -1365,6 +1501,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_pMa_times_pH(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_H_eq_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_eq_M_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -1375,6 +1512,7 @@ QLAB_EXPORT void QLA_DN_H_eq_M_times_xH(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_H_eq_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_eq_Ma_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -1385,6 +1523,7 @@ QLAB_EXPORT void QLA_DN_H_eq_Ma_times_xH(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_peq_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_peq_M_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -1395,6 +1534,7 @@ QLAB_EXPORT void QLA_DN_H_peq_M_times_xH(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_peq_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_peq_Ma_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -1405,6 +1545,7 @@ QLAB_EXPORT void QLA_DN_H_peq_Ma_times_xH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_meq_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_meq_M_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -1415,6 +1556,7 @@ QLAB_EXPORT void QLA_DN_H_meq_M_times_xH(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_meq_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_meq_Ma_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -1425,6 +1567,7 @@ QLAB_EXPORT void QLA_DN_H_meq_Ma_times_xH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_H_eqm_M_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_eqm_M_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -1435,6 +1578,7 @@ QLAB_EXPORT void QLA_DN_H_eqm_M_times_xH(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_H_eqm_Ma_times_xH(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_H_eqm_Ma_times_xH");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -1445,6 +1589,7 @@ QLAB_EXPORT void QLA_DN_H_eqm_Ma_times_xH(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_M_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -1455,6 +1600,7 @@ QLAB_EXPORT void QLA_DN_D_veq_M_times_D(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_M_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -1465,6 +1611,7 @@ QLAB_EXPORT void QLA_DN_D_veq_M_times_pD(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_Ma_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -1475,6 +1622,7 @@ QLAB_EXPORT void QLA_DN_D_veq_Ma_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_Ma_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -1485,6 +1633,7 @@ QLAB_EXPORT void QLA_DN_D_veq_Ma_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_pM_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -1495,6 +1644,7 @@ QLAB_EXPORT void QLA_DN_D_veq_pM_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_pM_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -1505,6 +1655,7 @@ QLAB_EXPORT void QLA_DN_D_veq_pM_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_pMa_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -1515,6 +1666,7 @@ QLAB_EXPORT void QLA_DN_D_veq_pMa_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veq_pMa_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veq_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -1525,6 +1677,7 @@ QLAB_EXPORT void QLA_DN_D_veq_pMa_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_M_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -1535,6 +1688,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_M_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_M_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -1545,6 +1699,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_M_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_Ma_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -1555,6 +1710,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_Ma_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_Ma_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -1565,6 +1721,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_Ma_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_pM_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -1575,6 +1732,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_pM_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_pM_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -1585,6 +1743,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_pM_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_pMa_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -1595,6 +1754,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_pMa_times_D(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vpeq_pMa_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vpeq_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -1605,6 +1765,7 @@ QLAB_EXPORT void QLA_DN_D_vpeq_pMa_times_pD(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_M_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -1615,6 +1776,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_M_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_M_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -1625,6 +1787,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_M_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_Ma_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -1635,6 +1798,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_Ma_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_Ma_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -1645,6 +1809,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_Ma_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_pM_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -1655,6 +1820,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_pM_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_pM_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -1665,6 +1831,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_pM_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_pMa_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -1675,6 +1842,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_pMa_times_D(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_vmeq_pMa_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_vmeq_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -1685,6 +1853,7 @@ QLAB_EXPORT void QLA_DN_D_vmeq_pMa_times_pD(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_M_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -1695,6 +1864,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_M_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_M_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1705,6 +1875,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_M_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_Ma_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -1715,6 +1886,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_Ma_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_Ma_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1725,6 +1897,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_Ma_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_pM_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -1735,6 +1908,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_pM_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_pM_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1745,6 +1919,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_pM_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_pMa_times_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -1755,6 +1930,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_pMa_times_D(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_veqm_pMa_times_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_D_veqm_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -1765,6 +1941,7 @@ QLAB_EXPORT void QLA_DN_D_veqm_pMa_times_pD(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_M_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1775,6 +1952,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_M_times_D(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_M_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1785,6 +1963,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_M_times_pD(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_Ma_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1795,6 +1974,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_Ma_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_Ma_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1805,6 +1985,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_Ma_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_pM_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1815,6 +1996,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_pM_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_pM_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1825,6 +2007,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_pM_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_pMa_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -1835,6 +2018,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_pMa_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeq_pMa_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeq_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -1845,6 +2029,7 @@ QLAB_EXPORT void QLA_DN_D_xeq_pMa_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_M_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1855,6 +2040,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_M_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_M_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1865,6 +2051,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_M_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_Ma_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1875,6 +2062,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_Ma_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_Ma_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1885,6 +2073,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_Ma_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_pM_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1895,6 +2084,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_pM_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_pM_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1905,6 +2095,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_pM_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_pMa_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -1915,6 +2106,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_pMa_times_D(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xpeq_pMa_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xpeq_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -1925,6 +2117,7 @@ QLAB_EXPORT void QLA_DN_D_xpeq_pMa_times_pD(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_M_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1935,6 +2128,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_M_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_M_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1945,6 +2139,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_M_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_Ma_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1955,6 +2150,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_Ma_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_Ma_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1965,6 +2161,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_Ma_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_pM_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1975,6 +2172,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_pM_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_pM_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -1985,6 +2183,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_pM_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_pMa_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -1995,6 +2194,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_pMa_times_D(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xmeq_pMa_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xmeq_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -2005,6 +2205,7 @@ QLAB_EXPORT void QLA_DN_D_xmeq_pMa_times_pD(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_M_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_M_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -2015,6 +2216,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_M_times_D(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_M_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_M_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -2025,6 +2227,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_M_times_pD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_Ma_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_Ma_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -2035,6 +2238,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_Ma_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_Ma_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_Ma_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -2045,6 +2249,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_Ma_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_pM_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_pM_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -2055,6 +2260,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_pM_times_D(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_pM_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_pM_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -2065,6 +2271,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_pM_times_pD(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_pMa_times_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_pMa_times_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -2075,6 +2282,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_pMa_times_D(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_D_xeqm_pMa_times_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_D_xeqm_pMa_times_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -2085,6 +2293,7 @@ QLAB_EXPORT void QLA_DN_D_xeqm_pMa_times_pD(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_D_eq_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_eq_M_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -2095,6 +2304,7 @@ QLAB_EXPORT void QLA_DN_D_eq_M_times_xD(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_D_eq_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_eq_Ma_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -2105,6 +2315,7 @@ QLAB_EXPORT void QLA_DN_D_eq_Ma_times_xD(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_peq_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_peq_M_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -2115,6 +2326,7 @@ QLAB_EXPORT void QLA_DN_D_peq_M_times_xD(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_peq_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_peq_Ma_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -2125,6 +2337,7 @@ QLAB_EXPORT void QLA_DN_D_peq_Ma_times_xD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_meq_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_meq_M_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -2135,6 +2348,7 @@ QLAB_EXPORT void QLA_DN_D_meq_M_times_xD(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_meq_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_meq_Ma_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -2145,6 +2359,7 @@ QLAB_EXPORT void QLA_DN_D_meq_Ma_times_xD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_D_eqm_M_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_eqm_M_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -2155,6 +2370,7 @@ QLAB_EXPORT void QLA_DN_D_eqm_M_times_xD(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_D_eqm_Ma_times_xD(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_D_eqm_Ma_times_xD");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 4, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -2165,6 +2381,7 @@ QLAB_EXPORT void QLA_DN_D_eqm_Ma_times_xD(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_M_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2175,6 +2392,7 @@ QLAB_EXPORT void QLA_DN_M_veq_M_times_M(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_M_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2185,6 +2403,7 @@ QLAB_EXPORT void QLA_DN_M_veq_M_times_pM(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_M_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2195,6 +2414,7 @@ QLAB_EXPORT void QLA_DN_M_veq_M_times_Ma(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_M_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2205,6 +2425,7 @@ QLAB_EXPORT void QLA_DN_M_veq_M_times_pMa(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_Ma_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2215,6 +2436,7 @@ QLAB_EXPORT void QLA_DN_M_veq_Ma_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_Ma_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2225,6 +2447,7 @@ QLAB_EXPORT void QLA_DN_M_veq_Ma_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_Ma_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2235,6 +2458,7 @@ QLAB_EXPORT void QLA_DN_M_veq_Ma_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_Ma_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2245,6 +2469,7 @@ QLAB_EXPORT void QLA_DN_M_veq_Ma_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pM_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2255,6 +2480,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pM_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pM_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2265,6 +2491,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pM_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pM_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2275,6 +2502,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pM_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pM_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2285,6 +2513,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pM_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pMa_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2295,6 +2524,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pMa_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pMa_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2305,6 +2535,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pMa_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pMa_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -2315,6 +2546,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pMa_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pMa_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -2325,6 +2557,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pMa_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_M_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2335,6 +2568,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_M_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_M_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2345,6 +2579,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_M_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_M_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2355,6 +2590,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_M_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_M_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2365,6 +2601,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_M_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2375,6 +2612,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2385,6 +2623,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2395,6 +2634,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2405,6 +2645,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_Ma_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2415,6 +2656,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2425,6 +2667,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2435,6 +2678,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2445,6 +2689,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pM_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2455,6 +2700,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2465,6 +2711,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -2475,6 +2722,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_Ma(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vpeq_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -2485,6 +2733,7 @@ QLAB_EXPORT void QLA_DN_M_vpeq_pMa_times_pMa(int nc, void * r, void * a, void * 
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_M_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2495,6 +2744,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_M_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_M_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2505,6 +2755,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_M_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_M_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2515,6 +2766,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_M_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_M_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2525,6 +2777,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_M_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2535,6 +2788,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2545,6 +2799,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2555,6 +2810,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2565,6 +2821,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_Ma_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2575,6 +2832,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2585,6 +2843,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2595,6 +2854,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2605,6 +2865,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pM_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2615,6 +2876,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2625,6 +2887,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -2635,6 +2898,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_Ma(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_vmeq_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -2645,6 +2909,7 @@ QLAB_EXPORT void QLA_DN_M_vmeq_pMa_times_pMa(int nc, void * r, void * a, void * 
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_M_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2655,6 +2920,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_M_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_M_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2665,6 +2931,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_M_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_M_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2675,6 +2942,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_M_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_M_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2685,6 +2953,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_M_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2695,6 +2964,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2705,6 +2975,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2715,6 +2986,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2725,6 +2997,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_Ma_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pM_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2735,6 +3008,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pM_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pM_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2745,6 +3019,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pM_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pM_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2755,6 +3030,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pM_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pM_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2765,6 +3041,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pM_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2775,6 +3052,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2785,6 +3063,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_Ma(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -2795,6 +3074,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_Ma(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_pMa(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veqm_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -2805,6 +3085,7 @@ QLAB_EXPORT void QLA_DN_M_veqm_pMa_times_pMa(int nc, void * r, void * a, void * 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_M_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2815,6 +3096,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_M_times_M(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_M_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2825,6 +3107,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_M_times_pM(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_M_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2835,6 +3118,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_M_times_Ma(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_M_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2845,6 +3129,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_M_times_pMa(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2855,6 +3140,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2865,6 +3151,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2875,6 +3162,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2885,6 +3173,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_Ma_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pM_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2895,6 +3184,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pM_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pM_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2905,6 +3195,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pM_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pM_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2915,6 +3206,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pM_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pM_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2925,6 +3217,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pM_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2935,6 +3228,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2945,6 +3239,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -2955,6 +3250,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -2965,6 +3261,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pMa_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_M_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -2975,6 +3272,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_M_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_M_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -2985,6 +3283,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_M_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_M_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -2995,6 +3294,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_M_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_M_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3005,6 +3305,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_M_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -3015,6 +3316,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3025,6 +3327,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -3035,6 +3338,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3045,6 +3349,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_Ma_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -3055,6 +3360,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3065,6 +3371,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -3075,6 +3382,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3085,6 +3393,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pM_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -3095,6 +3404,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3105,6 +3415,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -3115,6 +3426,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_Ma(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xpeq_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -3125,6 +3437,7 @@ QLAB_EXPORT void QLA_DN_M_xpeq_pMa_times_pMa(int nc, void * r, void * a, void * 
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_M_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3135,6 +3448,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_M_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_M_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3145,6 +3459,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_M_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_M_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3155,6 +3470,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_M_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_M_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3165,6 +3481,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_M_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3175,6 +3492,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3185,6 +3503,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3195,6 +3514,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3205,6 +3525,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_Ma_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3215,6 +3536,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3225,6 +3547,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3235,6 +3558,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3245,6 +3569,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pM_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3255,6 +3580,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3265,6 +3591,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -3275,6 +3602,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_Ma(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xmeq_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -3285,6 +3613,7 @@ QLAB_EXPORT void QLA_DN_M_xmeq_pMa_times_pMa(int nc, void * r, void * a, void * 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_M_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_M_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3295,6 +3624,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_M_times_M(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_M_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_M_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3305,6 +3635,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_M_times_pM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_M_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_M_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3315,6 +3646,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_M_times_Ma(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_M_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_M_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3325,6 +3657,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_M_times_pMa(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_Ma_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3335,6 +3668,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_Ma_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3345,6 +3679,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_Ma_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3355,6 +3690,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_Ma_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3365,6 +3701,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_Ma_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pM_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3375,6 +3712,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pM_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3385,6 +3723,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pM_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3395,6 +3734,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_Ma(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pM_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3405,6 +3745,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pM_times_pMa(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pMa_times_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3415,6 +3756,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pMa_times_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3425,6 +3767,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_Ma(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pMa_times_Ma");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -3435,6 +3778,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_Ma(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_pMa(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeqm_pMa_times_pMa");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, true>>("DN_lmult", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -3445,6 +3789,7 @@ QLAB_EXPORT void QLA_DN_M_xeqm_pMa_times_pMa(int nc, void * r, void * a, void * 
 }
 
 QLAB_EXPORT void QLA_DN_M_eq_M_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_eq_M_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -3455,6 +3800,7 @@ QLAB_EXPORT void QLA_DN_M_eq_M_times_xM(int nc, void * r, void * a, void * b, in
 }
 
 QLAB_EXPORT void QLA_DN_M_eq_Ma_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_eq_Ma_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQ); break;
@@ -3465,6 +3811,7 @@ QLAB_EXPORT void QLA_DN_M_eq_Ma_times_xM(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_peq_M_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_peq_M_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -3475,6 +3822,7 @@ QLAB_EXPORT void QLA_DN_M_peq_M_times_xM(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_peq_Ma_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_peq_Ma_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::PEQ); break;
@@ -3485,6 +3833,7 @@ QLAB_EXPORT void QLA_DN_M_peq_Ma_times_xM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_meq_M_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_meq_M_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -3495,6 +3844,7 @@ QLAB_EXPORT void QLA_DN_M_meq_M_times_xM(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_meq_Ma_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_meq_Ma_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::MEQ); break;
@@ -3505,6 +3855,7 @@ QLAB_EXPORT void QLA_DN_M_meq_Ma_times_xM(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_eqm_M_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_eqm_M_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, false, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
@@ -3515,6 +3866,7 @@ QLAB_EXPORT void QLA_DN_M_eqm_M_times_xM(int nc, void * r, void * a, void * b, i
 }
 
 QLAB_EXPORT void QLA_DN_M_eqm_Ma_times_xM(int nc, void * r, void * a, void * b, int * jb, int n) {
+  QLAB_TRACE("QLA_DN_M_eqm_Ma_times_xM");
   switch (nc) {
     case 2: qlab::api_map<qlab::LMultOp<double, 2, 2, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::LMultOp<double, 3, 3, true, false>>("DN_lmult", r, qlab::op_contig(a), qlab::op_idx(b, jb), nullptr, n, qlab::EQM); break;

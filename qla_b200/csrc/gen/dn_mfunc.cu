@@ -6,6 +6,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_M_veq_exp_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_exp_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenExpOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -16,6 +17,7 @@ QLAB_EXPORT void QLA_DN_M_veq_exp_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_sqrt_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_sqrt_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenSqrtOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -26,6 +28,7 @@ QLAB_EXPORT void QLA_DN_M_veq_sqrt_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_inverse_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_inverse_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenInverseOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -36,6 +39,7 @@ QLAB_EXPORT void QLA_DN_M_veq_inverse_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_C_veq_det_M(int nc, QLA_D_Complex * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_C_veq_det_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenDetOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -46,6 +50,7 @@ QLAB_EXPORT void QLA_DN_C_veq_det_M(int nc, QLA_D_Complex * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_exp_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_exp_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenExpOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -56,6 +61,7 @@ QLAB_EXPORT void QLA_DN_M_veq_exp_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_sqrt_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_sqrt_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenSqrtOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -66,6 +72,7 @@ QLAB_EXPORT void QLA_DN_M_veq_sqrt_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_inverse_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_inverse_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenInverseOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -76,6 +83,7 @@ QLAB_EXPORT void QLA_DN_M_veq_inverse_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_C_veq_det_pM(int nc, QLA_D_Complex * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_C_veq_det_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenDetOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -86,6 +94,7 @@ QLAB_EXPORT void QLA_DN_C_veq_det_pM(int nc, QLA_D_Complex * r, void * a, int n)
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_exp_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_exp_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenExpOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -96,6 +105,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_exp_M(int nc, void * r, void * a, int * index, int
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_sqrt_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_sqrt_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenSqrtOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -106,6 +116,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_sqrt_M(int nc, void * r, void * a, int * index, in
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_inverse_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_inverse_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenInverseOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -116,6 +127,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_inverse_M(int nc, void * r, void * a, int * index,
 }
 
 QLAB_EXPORT void QLA_DN_C_xeq_det_M(int nc, QLA_D_Complex * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_C_xeq_det_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenDetOp<double, 3>>("DN_mfunc", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -126,6 +138,7 @@ QLAB_EXPORT void QLA_DN_C_xeq_det_M(int nc, QLA_D_Complex * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_exp_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_exp_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXP>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenExpOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -136,6 +149,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_exp_pM(int nc, void * r, void * a, int * index, in
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_sqrt_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_sqrt_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRT>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenSqrtOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -146,6 +160,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_sqrt_pM(int nc, void * r, void * a, int * index, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_inverse_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_inverse_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVERSE>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenInverseOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -156,6 +171,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_inverse_pM(int nc, void * r, void * a, int * index
 }
 
 QLAB_EXPORT void QLA_DN_C_xeq_det_pM(int nc, QLA_D_Complex * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_C_xeq_det_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_DET>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenDetOp<double, 3>>("DN_mfunc", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;

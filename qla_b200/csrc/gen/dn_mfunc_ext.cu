@@ -6,6 +6,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_M_veq_invsqrt_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_invsqrt_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRT>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 0>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -16,6 +17,7 @@ QLAB_EXPORT void QLA_DN_M_veq_invsqrt_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_log_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_log_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_LOG>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 1>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -26,6 +28,7 @@ QLAB_EXPORT void QLA_DN_M_veq_log_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_expA_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_expA_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPA>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, true>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -36,6 +39,7 @@ QLAB_EXPORT void QLA_DN_M_veq_expA_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_expTA_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_expTA_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPTA>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, false>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -46,6 +50,7 @@ QLAB_EXPORT void QLA_DN_M_veq_expTA_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_sqrtPH_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_sqrtPH_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRTPH>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, false>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -56,6 +61,7 @@ QLAB_EXPORT void QLA_DN_M_veq_sqrtPH_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_invsqrtPH_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_invsqrtPH_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRTPH>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, true>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -66,6 +72,7 @@ QLAB_EXPORT void QLA_DN_M_veq_invsqrtPH_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_eigenvals_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_eigenvals_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIG>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsOp<double>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -76,6 +83,7 @@ QLAB_EXPORT void QLA_DN_V_veq_eigenvals_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_eigenvalsH_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_eigenvalsH_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIGH>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsHOp<double>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -86,6 +94,7 @@ QLAB_EXPORT void QLA_DN_V_veq_eigenvalsH_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_invsqrt_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_invsqrt_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRT>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 0>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -96,6 +105,7 @@ QLAB_EXPORT void QLA_DN_M_veq_invsqrt_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_log_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_log_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_LOG>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 1>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -106,6 +116,7 @@ QLAB_EXPORT void QLA_DN_M_veq_log_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_expA_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_expA_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPA>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, true>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -116,6 +127,7 @@ QLAB_EXPORT void QLA_DN_M_veq_expA_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_expTA_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_expTA_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPTA>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, false>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -126,6 +138,7 @@ QLAB_EXPORT void QLA_DN_M_veq_expTA_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_sqrtPH_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_sqrtPH_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRTPH>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, false>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -136,6 +149,7 @@ QLAB_EXPORT void QLA_DN_M_veq_sqrtPH_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_invsqrtPH_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_invsqrtPH_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRTPH>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, true>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -146,6 +160,7 @@ QLAB_EXPORT void QLA_DN_M_veq_invsqrtPH_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_eigenvals_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_eigenvals_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIG>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsOp<double>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -156,6 +171,7 @@ QLAB_EXPORT void QLA_DN_V_veq_eigenvals_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_eigenvalsH_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_eigenvalsH_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIGH>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsHOp<double>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -166,6 +182,7 @@ QLAB_EXPORT void QLA_DN_V_veq_eigenvalsH_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_M_inverse_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_M_inverse_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -176,6 +193,7 @@ QLAB_EXPORT void QLA_DN_V_veq_M_inverse_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_M_inverse_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_M_inverse_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -186,6 +204,7 @@ QLAB_EXPORT void QLA_DN_V_veq_M_inverse_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_pM_inverse_V(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_pM_inverse_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -196,6 +215,7 @@ QLAB_EXPORT void QLA_DN_V_veq_pM_inverse_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_pM_inverse_pV(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_V_veq_pM_inverse_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -206,6 +226,7 @@ QLAB_EXPORT void QLA_DN_V_veq_pM_inverse_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_M_inverse_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_M_inverse_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -216,6 +237,7 @@ QLAB_EXPORT void QLA_DN_M_veq_M_inverse_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_M_inverse_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_M_inverse_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -226,6 +248,7 @@ QLAB_EXPORT void QLA_DN_M_veq_M_inverse_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pM_inverse_M(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pM_inverse_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -236,6 +259,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pM_inverse_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_veq_pM_inverse_pM(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DN_M_veq_pM_inverse_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -246,6 +270,7 @@ QLAB_EXPORT void QLA_DN_M_veq_pM_inverse_pM(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_invsqrt_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_invsqrt_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRT>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 0>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -256,6 +281,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_invsqrt_M(int nc, void * r, void * a, int * index,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_log_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_log_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_LOG>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 1>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -266,6 +292,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_log_M(int nc, void * r, void * a, int * index, int
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_expA_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_expA_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPA>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, true>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -276,6 +303,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_expA_M(int nc, void * r, void * a, int * index, in
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_expTA_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_expTA_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPTA>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, false>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -286,6 +314,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_expTA_M(int nc, void * r, void * a, int * index, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_sqrtPH_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_sqrtPH_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRTPH>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, false>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -296,6 +325,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_sqrtPH_M(int nc, void * r, void * a, int * index, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_invsqrtPH_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_invsqrtPH_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRTPH>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, true>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -306,6 +336,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_invsqrtPH_M(int nc, void * r, void * a, int * inde
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_eigenvals_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_eigenvals_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIG>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsOp<double>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -316,6 +347,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_eigenvals_M(int nc, void * r, void * a, int * inde
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_eigenvalsH_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_eigenvalsH_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIGH>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsHOp<double>>("DN_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -326,6 +358,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_eigenvalsH_M(int nc, void * r, void * a, int * ind
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_invsqrt_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_invsqrt_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRT>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 0>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -336,6 +369,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_invsqrt_pM(int nc, void * r, void * a, int * index
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_log_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_log_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_LOG>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMfuncExtOp<double, 3, 1>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -346,6 +380,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_log_pM(int nc, void * r, void * a, int * index, in
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_expA_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_expA_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPA>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, true>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -356,6 +391,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_expA_pM(int nc, void * r, void * a, int * index, i
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_expTA_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_expTA_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EXPTA>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::ExpAHOp<double, false>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -366,6 +402,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_expTA_pM(int nc, void * r, void * a, int * index, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_sqrtPH_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_sqrtPH_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_SQRTPH>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, false>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -376,6 +413,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_sqrtPH_pM(int nc, void * r, void * a, int * index,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_invsqrtPH_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_invsqrtPH_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_INVSQRTPH>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::SqrtPHOp<double, true>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -386,6 +424,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_invsqrtPH_pM(int nc, void * r, void * a, int * ind
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_eigenvals_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_eigenvals_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIG>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsOp<double>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -396,6 +435,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_eigenvals_pM(int nc, void * r, void * a, int * ind
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_eigenvalsH_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_eigenvalsH_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MfuncOp<double, qlab::N2_EIGH>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::EigenvalsHOp<double>>("DN_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -406,6 +446,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_eigenvalsH_pM(int nc, void * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_M_inverse_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_M_inverse_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -416,6 +457,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_M_inverse_V(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_M_inverse_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_M_inverse_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -426,6 +468,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_M_inverse_pV(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_pM_inverse_V(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_pM_inverse_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -436,6 +479,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_pM_inverse_V(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_pM_inverse_pV(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_V_xeq_pM_inverse_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 1>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -446,6 +490,7 @@ QLAB_EXPORT void QLA_DN_V_xeq_pM_inverse_pV(int nc, void * r, void * a, void * b
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_M_inverse_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_M_inverse_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -456,6 +501,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_M_inverse_M(int nc, void * r, void * a, void * b, 
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_M_inverse_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_M_inverse_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -466,6 +512,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_M_inverse_pM(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pM_inverse_M(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pM_inverse_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -476,6 +523,7 @@ QLAB_EXPORT void QLA_DN_M_xeq_pM_inverse_M(int nc, void * r, void * a, void * b,
 }
 
 QLAB_EXPORT void QLA_DN_M_xeq_pM_inverse_pM(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DN_M_xeq_pM_inverse_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::Nc2MInverseOp<double, 2>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::GenMInverseOp<double, 3, 3>>("DN_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;

@@ -7,258 +7,322 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_V_veq_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veq_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veq_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vpeq_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vpeq_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_vmeq_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_vmeq_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_nM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_nM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_nMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_nMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_npM_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_npM_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_npMa_times_nV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_veqm_npMa_times_npV(int nc, void * r, void * a, void * b, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_veqm_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, nullptr, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeq_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeq_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xpeq_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xpeq_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xmeq_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xmeq_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_nM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_nM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_nM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_nM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_nMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_nMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, false, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_nMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_nMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, false, (const void*)b, true, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_npM_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_npM_times_nV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_npM_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_npM_times_npV");
   qlab::api_multi_n<double, false>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_npMa_times_nV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_npMa_times_nV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, false, index, n, nd, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_DN_V_xeqm_npMa_times_npV(int nc, void * r, void * a, void * b, int * index, int n, int nd) {
+  QLAB_TRACE("QLA_DN_V_xeqm_npMa_times_npV");
   qlab::api_multi_n<double, true>("DN_multi", nc, r, (const void*)a, true, (const void*)b, true, index, n, nd, qlab::EQM);
 }
 

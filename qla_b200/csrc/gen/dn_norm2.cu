@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_r_veq_norm2_V(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -15,6 +16,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_V(int nc, QLA_D_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_pV(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -25,6 +27,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_pV(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_V(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -35,6 +38,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_V(int nc, QLA_D_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_pV(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 2, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 3, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -45,6 +49,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_pV(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_H(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -55,6 +60,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_H(int nc, QLA_D_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_pH(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -65,6 +71,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_pH(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_H(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -75,6 +82,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_H(int nc, QLA_D_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_pH(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 6, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -85,6 +93,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_pH(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_D(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -95,6 +104,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_D(int nc, QLA_D_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_pD(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -105,6 +115,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_pD(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_D(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -115,6 +126,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_D(int nc, QLA_D_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_pD(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 8, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 12, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -125,6 +137,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_pD(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_M(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -135,6 +148,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_M(int nc, QLA_D_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_DN_r_veq_norm2_pM(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DN_r_veq_norm2_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -145,6 +159,7 @@ QLAB_EXPORT void QLA_DN_r_veq_norm2_pM(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_M(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -155,6 +170,7 @@ QLAB_EXPORT void QLA_DN_r_xeq_norm2_M(int nc, QLA_D_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_DN_r_xeq_norm2_pM(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DN_r_xeq_norm2_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<double, 4, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<double, 9, double>>("DN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;

@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_DN_H_veq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign); break;
@@ -16,6 +17,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_D(int nc, void * r, void * a, int mu, int s
 }
 
 QLAB_EXPORT void QLA_DN_H_veq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign); break;
@@ -27,6 +29,7 @@ QLAB_EXPORT void QLA_DN_H_veq_spproj_pD(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign); break;
@@ -38,6 +41,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign); break;
@@ -49,6 +53,7 @@ QLAB_EXPORT void QLA_DN_H_vpeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign); break;
@@ -60,6 +65,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_vmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign); break;
@@ -71,6 +77,7 @@ QLAB_EXPORT void QLA_DN_H_vmeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_D(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign); break;
@@ -82,6 +89,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_veqm_spproj_pD(int nc, void * r, void * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_DN_H_veqm_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign); break;
@@ -93,6 +101,7 @@ QLAB_EXPORT void QLA_DN_H_veqm_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign); break;
@@ -104,6 +113,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_D(int nc, void * r, void * a, int mu, int s
 }
 
 QLAB_EXPORT void QLA_DN_H_xeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign); break;
@@ -115,6 +125,7 @@ QLAB_EXPORT void QLA_DN_H_xeq_spproj_pD(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign); break;
@@ -126,6 +137,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign); break;
@@ -137,6 +149,7 @@ QLAB_EXPORT void QLA_DN_H_xpeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign); break;
@@ -148,6 +161,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign); break;
@@ -159,6 +173,7 @@ QLAB_EXPORT void QLA_DN_H_xmeq_spproj_pD(int nc, void * r, void * a, int mu, int
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_D(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_D");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign); break;
@@ -170,6 +185,7 @@ QLAB_EXPORT void QLA_DN_H_xeqm_spproj_D(int nc, void * r, void * a, int mu, int 
 }
 
 QLAB_EXPORT void QLA_DN_H_xeqm_spproj_pD(int nc, void * r, void * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_DN_H_xeqm_spproj_pD");
   if (mu < 0 || mu > 4) return;
   switch (nc) {
     case 2: qlab::api_map<qlab::SpprojOp<double, 2>>("DN_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign); break;

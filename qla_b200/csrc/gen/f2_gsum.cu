@@ -7,162 +7,202 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F2_v_veq_sum_V(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_v_veq_sum_V");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_v_veq_sum_pV(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_v_veq_sum_pV");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_h_veq_sum_H(QLA_F2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_h_veq_sum_H");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_h_veq_sum_pH(QLA_F2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_h_veq_sum_pH");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_d_veq_sum_D(QLA_F2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_d_veq_sum_D");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 4 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_d_veq_sum_pD(QLA_F2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_d_veq_sum_pD");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_m_veq_sum_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_m_veq_sum_M");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_m_veq_sum_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_m_veq_sum_pM");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_p_veq_sum_P(QLA_F2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_p_veq_sum_P");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 16 * 2 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_p_veq_sum_pP(QLA_F2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_p_veq_sum_pP");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_v_veq_sum_V(QLA_D2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_v_veq_sum_V");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_v_veq_sum_pV(QLA_D2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_v_veq_sum_pV");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_h_veq_sum_H(QLA_D2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_h_veq_sum_H");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_h_veq_sum_pH(QLA_D2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_h_veq_sum_pH");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_d_veq_sum_D(QLA_D2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_d_veq_sum_D");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 4 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_d_veq_sum_pD(QLA_D2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_d_veq_sum_pD");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_m_veq_sum_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_m_veq_sum_M");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_m_veq_sum_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_m_veq_sum_pM");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_p_veq_sum_P(QLA_D2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_p_veq_sum_P");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 16 * 2 * 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_p_veq_sum_pP(QLA_D2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_p_veq_sum_pP");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_v_xeq_sum_V(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_v_xeq_sum_V");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_v_xeq_sum_pV(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_v_xeq_sum_pV");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_h_xeq_sum_H(QLA_F2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_h_xeq_sum_H");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_h_xeq_sum_pH(QLA_F2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_h_xeq_sum_pH");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_d_xeq_sum_D(QLA_F2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_d_xeq_sum_D");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 4 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_d_xeq_sum_pD(QLA_F2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_d_xeq_sum_pD");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_m_xeq_sum_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_m_xeq_sum_M");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_m_xeq_sum_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_m_xeq_sum_pM");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_p_xeq_sum_P(QLA_F2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_p_xeq_sum_P");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 16 * 2 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_p_xeq_sum_pP(QLA_F2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_p_xeq_sum_pP");
   qlab::api_gsum_n<float, float>("F2_gsum", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_v_xeq_sum_V(QLA_D2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_v_xeq_sum_V");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_v_xeq_sum_pV(QLA_D2_ColorVector *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_v_xeq_sum_pV");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_h_xeq_sum_H(QLA_D2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_h_xeq_sum_H");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_h_xeq_sum_pH(QLA_D2_HalfFermion *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_h_xeq_sum_pH");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_d_xeq_sum_D(QLA_D2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_d_xeq_sum_D");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 4 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_d_xeq_sum_pD(QLA_D2_DiracFermion *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_d_xeq_sum_pD");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 4 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_m_xeq_sum_M(QLA_D2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_m_xeq_sum_M");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_m_xeq_sum_pM(QLA_D2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_m_xeq_sum_pM");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 2 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_p_xeq_sum_P(QLA_D2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_p_xeq_sum_P");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 16 * 2 * 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_p_xeq_sum_pP(QLA_D2_DiracPropagator *__restrict__ r, QLA_F2_DiracPropagator *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_p_xeq_sum_pP");
   qlab::api_gsum_n<float, double>("F2_gsum_df", 2, 16 * 2 * 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -6,194 +6,242 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F2_M_veq_invsqrt_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_invsqrt_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRT>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_log_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_log_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_LOG>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_expA_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_expA_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPA>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_expTA_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_expTA_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPTA>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_sqrtPH_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_sqrtPH_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_SQRTPH>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_invsqrtPH_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_invsqrtPH_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRTPH>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_eigenvals_M(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_eigenvals_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIG>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_eigenvalsH_M(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_eigenvalsH_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIGH>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_invsqrt_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_invsqrt_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRT>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_log_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_log_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_LOG>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_expA_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_expA_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPA>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_expTA_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_expTA_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPTA>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_sqrtPH_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_sqrtPH_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_SQRTPH>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_invsqrtPH_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_invsqrtPH_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRTPH>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_eigenvals_pM(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_eigenvals_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIG>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_eigenvalsH_pM(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_eigenvalsH_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIGH>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_M_inverse_V(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_M_inverse_V");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_M_inverse_pV(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_M_inverse_pV");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_pM_inverse_V(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_pM_inverse_V");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_veq_pM_inverse_pV(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F2_V_veq_pM_inverse_pV");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_M_inverse_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_M_inverse_M");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_M_inverse_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_M_inverse_pM");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_pM_inverse_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_pM_inverse_M");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_pM_inverse_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_pM_inverse_pM");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_invsqrt_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_invsqrt_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRT>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_log_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_log_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_LOG>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_expA_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_expA_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPA>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_expTA_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_expTA_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPTA>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_sqrtPH_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_sqrtPH_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_SQRTPH>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_invsqrtPH_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_invsqrtPH_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRTPH>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_eigenvals_M(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_eigenvals_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIG>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_eigenvalsH_M(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_eigenvalsH_M");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIGH>>("F2_mfunc_ext", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_invsqrt_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_invsqrt_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRT>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_log_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_log_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_LOG>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_expA_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_expA_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPA>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_expTA_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_expTA_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EXPTA>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_sqrtPH_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_sqrtPH_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_SQRTPH>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_invsqrtPH_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_invsqrtPH_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_INVSQRTPH>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_eigenvals_pM(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_eigenvals_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIG>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_eigenvalsH_pM(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_eigenvalsH_pM");
   qlab::api_map<qlab::Nc2MfuncOp<float, qlab::N2_EIGH>>("F2_mfunc_ext", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_M_inverse_V(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_M_inverse_V");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_M_inverse_pV(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_M_inverse_pV");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_pM_inverse_V(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_pM_inverse_V");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_V_xeq_pM_inverse_pV(QLA_F2_ColorVector *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_V_xeq_pM_inverse_pV");
   qlab::api_map<qlab::Nc2MInverseOp<float, 1>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_M_inverse_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_M_inverse_M");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_M_inverse_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, QLA_F2_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_M_inverse_pM");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_pM_inverse_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_pM_inverse_M");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_pM_inverse_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, QLA_F2_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_pM_inverse_pM");
   qlab::api_map<qlab::Nc2MInverseOp<float, 2>>("F2_minv", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 

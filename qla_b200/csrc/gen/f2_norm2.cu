@@ -5,130 +5,162 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F2_r_veq_norm2_V(QLA_F_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_V");
   qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_pV(QLA_F_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_pV");
   qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_V(QLA_F_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_V");
   qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_pV(QLA_F_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_pV");
   qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_V(QLA_D_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_V");
   qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_pV(QLA_D_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_pV");
   qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_V(QLA_D_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_V");
   qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_pV(QLA_D_Real *__restrict__ r, QLA_F2_ColorVector *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_pV");
   qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_H(QLA_F_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_H");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_pH(QLA_F_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_pH");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_H(QLA_F_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_H");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_pH(QLA_F_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_pH");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_H(QLA_D_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_H");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_pH(QLA_D_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_pH");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_H(QLA_D_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_H");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_pH(QLA_D_Real *__restrict__ r, QLA_F2_HalfFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_pH");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_D(QLA_F_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_D");
   qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_pD(QLA_F_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_pD");
   qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_D(QLA_F_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_D");
   qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_pD(QLA_F_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_pD");
   qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_D(QLA_D_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_D");
   qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_pD(QLA_D_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_pD");
   qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_D(QLA_D_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_D");
   qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_pD(QLA_D_Real *__restrict__ r, QLA_F2_DiracFermion *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_pD");
   qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_M(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_M");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_veq_norm2_pM(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_r_veq_norm2_pM");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_M(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_M");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F2_r_xeq_norm2_pM(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_r_xeq_norm2_pM");
   qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("F2_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_M(QLA_D_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_M");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_veq_norm2_pM(QLA_D_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF2_r_veq_norm2_pM");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_M(QLA_D_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_M");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF2_r_xeq_norm2_pM(QLA_D_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF2_r_xeq_norm2_pM");
   qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("F2_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 

@@ -7,66 +7,82 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F2_C_veq_trace_M(QLA_F_Complex *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_C_veq_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("F2_trace", 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_veq_re_trace_M(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_R_veq_re_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("F2_trace", 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_veq_im_trace_M(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_R_veq_im_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("F2_trace", 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_antiherm_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_antiherm_M");
   qlab::api_antiherm_n<float>("F2_trace", 2, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_C_veq_trace_pM(QLA_F_Complex *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_C_veq_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_veq_re_trace_pM(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_R_veq_re_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_veq_im_trace_pM(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_R_veq_im_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_M_veq_antiherm_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F2_M_veq_antiherm_pM");
   qlab::api_antiherm_n<float>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F2_C_xeq_trace_M(QLA_F_Complex *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_C_xeq_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("F2_trace", 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_xeq_re_trace_M(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_R_xeq_re_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("F2_trace", 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_xeq_im_trace_M(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_R_xeq_im_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("F2_trace", 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_antiherm_M(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_antiherm_M");
   qlab::api_antiherm_n<float>("F2_trace", 2, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_C_xeq_trace_pM(QLA_F_Complex *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_C_xeq_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_xeq_re_trace_pM(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_R_xeq_re_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_R_xeq_im_trace_pM(QLA_F_Real *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_R_xeq_im_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_F2_M_xeq_antiherm_pM(QLA_F2_ColorMatrix *__restrict__ r, QLA_F2_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F2_M_xeq_antiherm_pM");
   qlab::api_antiherm_n<float>("F2_trace", 2, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -5,258 +5,322 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F3_c_veq_V_dot_V(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_V_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_V_dot_pV(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_V_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pV_dot_V(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pV_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pV_dot_pV(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pV_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_V_dot_V(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_V_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_V_dot_pV(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_V_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pV_dot_V(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pV_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pV_dot_pV(QLA_F_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pV_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, float>>("F3_dot_V", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_H_dot_H(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_H_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_H_dot_pH(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_H_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pH_dot_H(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pH_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pH_dot_pH(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pH_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_H_dot_H(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_H_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_H_dot_pH(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_H_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pH_dot_H(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pH_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pH_dot_pH(QLA_F_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pH_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, float>>("F3_dot_H", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_D_dot_D(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_D_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_D_dot_pD(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_D_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pD_dot_D(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pD_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pD_dot_pD(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pD_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_D_dot_D(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_D_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_D_dot_pD(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_D_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pD_dot_D(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pD_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pD_dot_pD(QLA_F_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pD_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, float>>("F3_dot_D", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_M_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_M_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_M_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_M_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pM_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pM_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pM_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pM_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_M_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_M_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_M_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_M_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pM_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pM_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pM_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pM_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, float>>("F3_dot_M", r, 2 * sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_V_dot_V(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_V_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_V_dot_pV(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_V_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pV_dot_V(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pV_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pV_dot_pV(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pV_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_V_dot_V(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_V_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_V_dot_pV(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_V_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pV_dot_V(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pV_dot_V");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pV_dot_pV(QLA_D_Complex *__restrict__ r, QLA_F3_ColorVector *__restrict__ * a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pV_dot_pV");
   qlab::api_reduce<qlab::DotOp<float, 3, double>>("F3_dot_V", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_H_dot_H(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_H_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_H_dot_pH(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_H_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pH_dot_H(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pH_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pH_dot_pH(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pH_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_H_dot_H(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_H_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_H_dot_pH(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_H_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pH_dot_H(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pH_dot_H");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pH_dot_pH(QLA_D_Complex *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pH_dot_pH");
   qlab::api_reduce<qlab::DotOp<float, 6, double>>("F3_dot_H", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_D_dot_D(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_D_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_D_dot_pD(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_D_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pD_dot_D(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pD_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pD_dot_pD(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pD_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_D_dot_D(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_D_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_D_dot_pD(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_D_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pD_dot_D(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pD_dot_D");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pD_dot_pD(QLA_D_Complex *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pD_dot_pD");
   qlab::api_reduce<qlab::DotOp<float, 12, double>>("F3_dot_D", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_M_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_M_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_M_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_M_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pM_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pM_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pM_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pM_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_M_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_M_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_M_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_M_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pM_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pM_dot_M");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pM_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pM_dot_pM");
   qlab::api_reduce<qlab::DotOp<float, 9, double>>("F3_dot_M", r, 2 * sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 

@@ -6,290 +6,362 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F3_c_veq_Ma_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_Ma_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_Ma_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_Ma_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pMa_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pMa_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pMa_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pMa_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_P_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_P_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pP_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pP_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_Pa_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_Pa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_Pa_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_Pa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pPa_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pPa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_veq_pPa_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_c_veq_pPa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_veq_re_P_dot_P(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_r_veq_re_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_veq_re_P_dot_pP(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_r_veq_re_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_veq_re_pP_dot_P(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_r_veq_re_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_veq_re_pP_dot_pP(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_r_veq_re_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_veq_norm2_P(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F3_r_veq_norm2_P");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_veq_norm2_pP(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F3_r_veq_norm2_pP");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_Ma_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_Ma_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_Ma_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_Ma_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pMa_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pMa_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pMa_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pMa_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_P_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_P_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pP_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pP_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_Pa_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_Pa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_Pa_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_Pa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pPa_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pPa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_veq_pPa_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_c_veq_pPa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_veq_re_P_dot_P(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_r_veq_re_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_veq_re_P_dot_pP(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_r_veq_re_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_veq_re_pP_dot_P(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_DF3_r_veq_re_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_veq_re_pP_dot_pP(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_DF3_r_veq_re_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_veq_norm2_P(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_DF3_r_veq_norm2_P");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_veq_norm2_pP(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_DF3_r_veq_norm2_pP");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_Ma_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_Ma_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_Ma_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_Ma_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pMa_dot_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pMa_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pMa_dot_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pMa_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_P_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_P_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pP_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pP_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_Pa_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_Pa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_Pa_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_Pa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pPa_dot_P(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pPa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_c_xeq_pPa_dot_pP(QLA_F_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_c_xeq_pPa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_xeq_re_P_dot_P(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_r_xeq_re_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_xeq_re_P_dot_pP(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_r_xeq_re_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_xeq_re_pP_dot_P(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_r_xeq_re_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_xeq_re_pP_dot_pP(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_r_xeq_re_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_xeq_norm2_P(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_r_xeq_norm2_P");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, float>("F3_gred", r, qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_F3_r_xeq_norm2_pP(QLA_F_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_r_xeq_norm2_pP");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, float>("F3_gred", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_Ma_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_Ma_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_Ma_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_Ma_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pMa_dot_M(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pMa_dot_M");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pMa_dot_pM(QLA_D_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pMa_dot_pM");
   qlab::api_gdot<float, 9, qlab::LD_ADOT, qlab::PERM_M, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_P_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_P_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pP_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pP_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_DOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_Pa_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_Pa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_Pa_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_Pa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pPa_dot_P(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pPa_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_c_xeq_pPa_dot_pP(QLA_D_Complex *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_c_xeq_pPa_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_ADOT, qlab::PERM_P, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_xeq_re_P_dot_P(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_r_xeq_re_P_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_xeq_re_P_dot_pP(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_r_xeq_re_P_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_xeq_re_pP_dot_P(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_r_xeq_re_pP_dot_P");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_xeq_re_pP_dot_pP(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, QLA_F3_DiracPropagator *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_r_xeq_re_pP_dot_pP");
   qlab::api_gdot<float, 144, qlab::LD_REDOT, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_xeq_norm2_P(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_r_xeq_norm2_P");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_contig(a), qlab::Opnd{}, index, n);
 }
 
 QLAB_EXPORT void QLA_DF3_r_xeq_norm2_pP(QLA_D_Real *__restrict__ r, QLA_F3_DiracPropagator *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_DF3_r_xeq_norm2_pP");
   qlab::api_gdot<float, 144, qlab::LD_NORM2, qlab::PERM_ID, double>("F3_gred_df", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n);
 }
 

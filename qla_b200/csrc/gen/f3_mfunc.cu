@@ -6,66 +6,82 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F3_M_veq_exp_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_exp_M");
   qlab::api_map<qlab::ExpOp<float>>("F3_mfunc_exp", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_sqrt_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_sqrt_M");
   qlab::api_map<qlab::SqrtOp<float>>("F3_mfunc_sqrt", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_inverse_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_inverse_M");
   qlab::api_map<qlab::InverseOp<float>>("F3_mfunc_inverse", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_C_veq_det_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_F3_C_veq_det_M");
   qlab::api_map<qlab::DetOp<float>>("F3_mfunc_det", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_exp_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_exp_pM");
   qlab::api_map<qlab::ExpOp<float>>("F3_mfunc_exp", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_sqrt_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_sqrt_pM");
   qlab::api_map<qlab::SqrtOp<float>>("F3_mfunc_sqrt", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_inverse_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_inverse_pM");
   qlab::api_map<qlab::InverseOp<float>>("F3_mfunc_inverse", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_C_veq_det_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int n) {
+  QLAB_TRACE("QLA_F3_C_veq_det_pM");
   qlab::api_map<qlab::DetOp<float>>("F3_mfunc_det", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_exp_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_exp_M");
   qlab::api_map<qlab::ExpOp<float>>("F3_mfunc_exp", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_sqrt_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_sqrt_M");
   qlab::api_map<qlab::SqrtOp<float>>("F3_mfunc_sqrt", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_inverse_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_inverse_M");
   qlab::api_map<qlab::InverseOp<float>>("F3_mfunc_inverse", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_C_xeq_det_M(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_C_xeq_det_M");
   qlab::api_map<qlab::DetOp<float>>("F3_mfunc_det", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_exp_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_exp_pM");
   qlab::api_map<qlab::ExpOp<float>>("F3_mfunc_exp", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_sqrt_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_sqrt_pM");
   qlab::api_map<qlab::SqrtOp<float>>("F3_mfunc_sqrt", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_inverse_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_inverse_pM");
   qlab::api_map<qlab::InverseOp<float>>("F3_mfunc_inverse", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_C_xeq_det_pM(QLA_F_Complex *__restrict__ r, QLA_F3_ColorMatrix *__restrict__ * a, int * index, int n) {
+  QLAB_TRACE("QLA_F3_C_xeq_det_pM");
   qlab::api_map<qlab::DetOp<float>>("F3_mfunc_det", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 

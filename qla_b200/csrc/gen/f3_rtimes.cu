@@ -5,258 +5,322 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F3_V_veq_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_V_veq_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_veq_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_V_veq_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_vpeq_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_V_vpeq_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_vpeq_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_V_vpeq_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_vmeq_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_V_vmeq_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_vmeq_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_V_vmeq_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_veqm_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_V_veqm_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_V_veqm_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_V_veqm_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_V_xeq_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xeq_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_xeq_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xeq_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_xpeq_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xpeq_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_xpeq_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xpeq_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_xmeq_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xmeq_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_xmeq_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xmeq_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_V_xeqm_r_times_V(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xeqm_r_times_V");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_contig(b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_V_xeqm_r_times_pV(QLA_F3_ColorVector *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorVector *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_V_xeqm_r_times_pV");
   qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("F3_rtimes_V", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_H_veq_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_H_veq_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_veq_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_H_veq_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_vpeq_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_H_vpeq_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_vpeq_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_H_vpeq_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_vmeq_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_H_vmeq_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_vmeq_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_H_vmeq_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_veqm_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_H_veqm_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_H_veqm_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_H_veqm_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeq_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeq_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeq_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeq_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_xpeq_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xpeq_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_xpeq_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xpeq_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_xmeq_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xmeq_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_xmeq_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xmeq_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeqm_r_times_H(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeqm_r_times_H");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_contig(b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeqm_r_times_pH(QLA_F3_HalfFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_HalfFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeqm_r_times_pH");
   qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("F3_rtimes_H", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_D_veq_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_D_veq_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_veq_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_D_veq_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_vpeq_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_D_vpeq_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_vpeq_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_D_vpeq_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_vmeq_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_D_vmeq_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_vmeq_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_D_vmeq_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_veqm_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_D_veqm_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_D_veqm_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_D_veqm_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeq_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeq_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeq_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeq_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_xpeq_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xpeq_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_xpeq_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xpeq_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_xmeq_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xmeq_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_xmeq_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xmeq_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeqm_r_times_D(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeqm_r_times_D");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_contig(b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeqm_r_times_pD(QLA_F3_DiracFermion *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_DiracFermion *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeqm_r_times_pD");
   qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("F3_rtimes_D", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veq_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_M_veq_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_vpeq_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_M_vpeq_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_vpeq_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_M_vpeq_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_vmeq_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_M_vmeq_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_vmeq_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_M_vmeq_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_veqm_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_F3_M_veqm_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_M_veqm_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_F3_M_veqm_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeq_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeq_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xpeq_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xpeq_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xpeq_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xpeq_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xmeq_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xmeq_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xmeq_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xmeq_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeqm_r_times_M(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeqm_r_times_M");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_contig(b), index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_F3_M_xeqm_r_times_pM(QLA_F3_ColorMatrix *__restrict__ r, QLA_F_Real *__restrict__ a, QLA_F3_ColorMatrix *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_F3_M_xeqm_r_times_pM");
   qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("F3_rtimes_M", r, a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM);
 }
 

@@ -5,81 +5,97 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F3_H_veq_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_veq_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_veq_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_veq_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_vpeq_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_vpeq_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_vpeq_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_vpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_vmeq_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_vmeq_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_vmeq_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_vmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_veqm_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_veqm_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_veqm_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_H_veqm_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeq_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeq_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeq_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeq_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xpeq_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xpeq_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xpeq_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xpeq_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xmeq_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xmeq_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xmeq_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xmeq_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeqm_spproj_D(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeqm_spproj_D");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_H_xeqm_spproj_pD(QLA_F3_HalfFermion *__restrict__ r, QLA_F3_DiracFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_H_xeqm_spproj_pD");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpprojOp<float, 3>>("F3_spproj", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign);
 }

@@ -5,81 +5,97 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_F3_D_veq_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_veq_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_veq_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_veq_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_vpeq_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_vpeq_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_vpeq_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_vpeq_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_vmeq_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_vmeq_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_vmeq_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_vmeq_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_veqm_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_veqm_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_veqm_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int n) {
+  QLAB_TRACE("QLA_F3_D_veqm_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeq_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeq_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeq_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeq_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xpeq_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xpeq_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xpeq_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xpeq_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xmeq_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xmeq_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xmeq_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xmeq_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeqm_sprecon_H(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeqm_sprecon_H");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign);
 }
 
 QLAB_EXPORT void QLA_F3_D_xeqm_sprecon_pH(QLA_F3_DiracFermion *__restrict__ r, QLA_F3_HalfFermion *__restrict__ * a, int mu, int sign, int * index, int n) {
+  QLAB_TRACE("QLA_F3_D_xeqm_sprecon_pH");
   if (mu < 0 || mu > 4) return;  /* the reference's switch has no default */
   qlab::api_map<qlab::SpreconOp<float, 3>>("F3_sprecon", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM, mu, sign);
 }

@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_V_veq_V(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -15,6 +16,7 @@ QLAB_EXPORT void QLA_FN_V_veq_V(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_pV(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -25,6 +27,7 @@ QLAB_EXPORT void QLA_FN_V_veq_pV(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_vpeq_V(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_vpeq_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -35,6 +38,7 @@ QLAB_EXPORT void QLA_FN_V_vpeq_V(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_vpeq_pV(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_vpeq_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -45,6 +49,7 @@ QLAB_EXPORT void QLA_FN_V_vpeq_pV(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_vmeq_V(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_vmeq_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -55,6 +60,7 @@ QLAB_EXPORT void QLA_FN_V_vmeq_V(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_vmeq_pV(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_vmeq_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -65,6 +71,7 @@ QLAB_EXPORT void QLA_FN_V_vmeq_pV(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_veqm_V(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_veqm_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -75,6 +82,7 @@ QLAB_EXPORT void QLA_FN_V_veqm_V(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_veqm_pV(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_veqm_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -85,6 +93,7 @@ QLAB_EXPORT void QLA_FN_V_veqm_pV(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_V(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -95,6 +104,7 @@ QLAB_EXPORT void QLA_FN_V_xeq_V(int nc, void * r, void * a, int * index, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_pV(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -105,6 +115,7 @@ QLAB_EXPORT void QLA_FN_V_xeq_pV(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_V_xpeq_V(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xpeq_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -115,6 +126,7 @@ QLAB_EXPORT void QLA_FN_V_xpeq_V(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_V_xpeq_pV(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xpeq_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -125,6 +137,7 @@ QLAB_EXPORT void QLA_FN_V_xpeq_pV(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_V_xmeq_V(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xmeq_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -135,6 +148,7 @@ QLAB_EXPORT void QLA_FN_V_xmeq_V(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_V_xmeq_pV(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xmeq_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -145,6 +159,7 @@ QLAB_EXPORT void QLA_FN_V_xmeq_pV(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_V_xeqm_V(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeqm_V");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -155,6 +170,7 @@ QLAB_EXPORT void QLA_FN_V_xeqm_V(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_V_xeqm_pV(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeqm_pV");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 2>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 3>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -165,6 +181,7 @@ QLAB_EXPORT void QLA_FN_V_xeqm_pV(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_H(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -175,6 +192,7 @@ QLAB_EXPORT void QLA_FN_H_veq_H(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_pH(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -185,6 +203,7 @@ QLAB_EXPORT void QLA_FN_H_veq_pH(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_vpeq_H(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_vpeq_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -195,6 +214,7 @@ QLAB_EXPORT void QLA_FN_H_vpeq_H(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_vpeq_pH(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_vpeq_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -205,6 +225,7 @@ QLAB_EXPORT void QLA_FN_H_vpeq_pH(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_vmeq_H(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_vmeq_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -215,6 +236,7 @@ QLAB_EXPORT void QLA_FN_H_vmeq_H(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_vmeq_pH(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_vmeq_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -225,6 +247,7 @@ QLAB_EXPORT void QLA_FN_H_vmeq_pH(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_veqm_H(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_veqm_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -235,6 +258,7 @@ QLAB_EXPORT void QLA_FN_H_veqm_H(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_veqm_pH(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_veqm_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -245,6 +269,7 @@ QLAB_EXPORT void QLA_FN_H_veqm_pH(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_H(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -255,6 +280,7 @@ QLAB_EXPORT void QLA_FN_H_xeq_H(int nc, void * r, void * a, int * index, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_pH(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -265,6 +291,7 @@ QLAB_EXPORT void QLA_FN_H_xeq_pH(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_H_xpeq_H(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xpeq_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -275,6 +302,7 @@ QLAB_EXPORT void QLA_FN_H_xpeq_H(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_H_xpeq_pH(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xpeq_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -285,6 +313,7 @@ QLAB_EXPORT void QLA_FN_H_xpeq_pH(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_H_xmeq_H(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xmeq_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -295,6 +324,7 @@ QLAB_EXPORT void QLA_FN_H_xmeq_H(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_H_xmeq_pH(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xmeq_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -305,6 +335,7 @@ QLAB_EXPORT void QLA_FN_H_xmeq_pH(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_H_xeqm_H(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeqm_H");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -315,6 +346,7 @@ QLAB_EXPORT void QLA_FN_H_xeqm_H(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_H_xeqm_pH(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeqm_pH");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 6>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -325,6 +357,7 @@ QLAB_EXPORT void QLA_FN_H_xeqm_pH(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -335,6 +368,7 @@ QLAB_EXPORT void QLA_FN_D_veq_D(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -345,6 +379,7 @@ QLAB_EXPORT void QLA_FN_D_veq_pD(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -355,6 +390,7 @@ QLAB_EXPORT void QLA_FN_D_vpeq_D(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -365,6 +401,7 @@ QLAB_EXPORT void QLA_FN_D_vpeq_pD(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -375,6 +412,7 @@ QLAB_EXPORT void QLA_FN_D_vmeq_D(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -385,6 +423,7 @@ QLAB_EXPORT void QLA_FN_D_vmeq_pD(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -395,6 +434,7 @@ QLAB_EXPORT void QLA_FN_D_veqm_D(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -405,6 +445,7 @@ QLAB_EXPORT void QLA_FN_D_veqm_pD(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -415,6 +456,7 @@ QLAB_EXPORT void QLA_FN_D_xeq_D(int nc, void * r, void * a, int * index, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -425,6 +467,7 @@ QLAB_EXPORT void QLA_FN_D_xeq_pD(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -435,6 +478,7 @@ QLAB_EXPORT void QLA_FN_D_xpeq_D(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -445,6 +489,7 @@ QLAB_EXPORT void QLA_FN_D_xpeq_pD(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -455,6 +500,7 @@ QLAB_EXPORT void QLA_FN_D_xmeq_D(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -465,6 +511,7 @@ QLAB_EXPORT void QLA_FN_D_xmeq_pD(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_D");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -475,6 +522,7 @@ QLAB_EXPORT void QLA_FN_D_xeqm_D(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pD");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 8>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 12>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -485,6 +533,7 @@ QLAB_EXPORT void QLA_FN_D_xeqm_pD(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -495,6 +544,7 @@ QLAB_EXPORT void QLA_FN_M_veq_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ); break;
@@ -505,6 +555,7 @@ QLAB_EXPORT void QLA_FN_M_veq_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_vpeq_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_vpeq_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -515,6 +566,7 @@ QLAB_EXPORT void QLA_FN_M_vpeq_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_vpeq_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_vpeq_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ); break;
@@ -525,6 +577,7 @@ QLAB_EXPORT void QLA_FN_M_vpeq_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_vmeq_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_vmeq_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -535,6 +588,7 @@ QLAB_EXPORT void QLA_FN_M_vmeq_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_vmeq_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_vmeq_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ); break;
@@ -545,6 +599,7 @@ QLAB_EXPORT void QLA_FN_M_vmeq_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_veqm_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veqm_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -555,6 +610,7 @@ QLAB_EXPORT void QLA_FN_M_veqm_M(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_veqm_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veqm_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM); break;
@@ -565,6 +621,7 @@ QLAB_EXPORT void QLA_FN_M_veqm_pM(int nc, void * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -575,6 +632,7 @@ QLAB_EXPORT void QLA_FN_M_xeq_M(int nc, void * r, void * a, int * index, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ); break;
@@ -585,6 +643,7 @@ QLAB_EXPORT void QLA_FN_M_xeq_pM(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_M_xpeq_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xpeq_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -595,6 +654,7 @@ QLAB_EXPORT void QLA_FN_M_xpeq_M(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_M_xpeq_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xpeq_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ); break;
@@ -605,6 +665,7 @@ QLAB_EXPORT void QLA_FN_M_xpeq_pM(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_M_xmeq_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xmeq_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -615,6 +676,7 @@ QLAB_EXPORT void QLA_FN_M_xmeq_M(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_M_xmeq_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xmeq_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ); break;
@@ -625,6 +687,7 @@ QLAB_EXPORT void QLA_FN_M_xmeq_pM(int nc, void * r, void * a, int * index, int n
 }
 
 QLAB_EXPORT void QLA_FN_M_xeqm_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeqm_M");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM); break;
@@ -635,6 +698,7 @@ QLAB_EXPORT void QLA_FN_M_xeqm_M(int nc, void * r, void * a, int * index, int n)
 }
 
 QLAB_EXPORT void QLA_FN_M_xeqm_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeqm_pM");
   switch (nc) {
     case 2: qlab::api_map<qlab::CopyOp<float, 4>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;
     case 3: qlab::api_map<qlab::CopyOp<float, 9>>("FN_copy", r, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM); break;

@@ -7,770 +7,962 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_D_veq_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_conj_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_conj_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_i_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_i_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_conj_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_conj_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_i_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_i_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_conj_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_conj_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_i_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_i_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_conj_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_conj_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_i_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_i_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D_plus_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D_plus_D");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_D_plus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_D_plus_D");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_D_plus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_D_plus_D");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D_minus_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D_minus_D");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_D_minus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_D_minus_D");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_D_minus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_D_minus_D");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D_plus_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D_plus_pD");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_D_plus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_D_plus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_D_plus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_D_plus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D_minus_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D_minus_pD");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_D_minus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_D_minus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_D_minus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_D_minus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD_plus_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD_plus_D");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_pD_plus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_pD_plus_D");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_pD_plus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_pD_plus_D");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD_minus_D(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD_minus_D");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_pD_minus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_pD_minus_D");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_pD_minus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_pD_minus_D");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD_plus_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD_plus_pD");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_pD_plus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_pD_plus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_pD_plus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_pD_plus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD_minus_pD(int nc, void * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD_minus_pD");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_pD_minus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_pD_minus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_c_times_pD_minus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_c_times_pD_minus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_conj_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_conj_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_i_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_i_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_conj_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_conj_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_i_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_i_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_conj_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_conj_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_i_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_i_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_c_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_c_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_c_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_c_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_CONST, false>("FN_ew_ctimes", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_C_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_C_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_C_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_C_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pC_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pC_times_D");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pC_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pC_times_pD");
   qlab::api_ew_n<float, qlab::EW_CT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_Ca_times_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_Ca_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_Ca_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_Ca_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pCa_times_D(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pCa_times_D");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pCa_times_pD(int nc, void * r, QLA_F_Complex *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pCa_times_pD");
   qlab::api_ew_n<float, qlab::EW_CAT, qlab::SC_FIELD, false>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_R_times_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_R_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_R_times_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_R_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pR_times_D(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pR_times_D");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_pR_times_pD(int nc, void * r, QLA_F_Real *__restrict__ * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_pR_times_pD");
   qlab::api_ew_n<float, qlab::EW_RT, qlab::SC_FIELD, true>("FN_ew_field", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_conj_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_conj_D");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_conj_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_conj_pD");
   qlab::api_ew_n<float, qlab::EW_CONJ, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_i_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_i_D");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_i_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_i_pD");
   qlab::api_ew_n<float, qlab::EW_I, qlab::SC_NONE, false>("FN_ew_unary", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D_plus_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D_plus_D");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_D_plus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_D_plus_D");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_D_plus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_D_plus_D");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D_minus_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D_minus_D");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_D_minus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_D_minus_D");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_D_minus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_D_minus_D");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D_plus_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D_plus_pD");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_D_plus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_D_plus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_D_plus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_D_plus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D_minus_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D_minus_pD");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_D_minus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_D_minus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_D_minus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_D_minus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_contig(b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD_plus_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD_plus_D");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_pD_plus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_pD_plus_D");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_pD_plus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_pD_plus_D");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD_minus_D(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD_minus_D");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_pD_minus_D(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_pD_minus_D");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_pD_minus_D(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_pD_minus_D");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_contig(c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD_plus_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD_plus_pD");
   qlab::api_ew_n<float, qlab::EW_PLUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_pD_plus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_pD_plus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_PLUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_pD_plus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_pD_plus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_PLUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD_minus_pD(int nc, void * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD_minus_pD");
   qlab::api_ew_n<float, qlab::EW_MINUS, qlab::SC_NONE, false>("FN_ew_sum", nc, 4 * nc, qlab::PERM_ID, r, nullptr, qlab::Opnd{}, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_pD_minus_pD(int nc, void * r, QLA_F_Real *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_pD_minus_pD");
   qlab::api_ew_n<float, qlab::EW_RT_MINUS, qlab::SC_CONST, true>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_c_times_pD_minus_pD(int nc, void * r, QLA_F_Complex *__restrict__ a, void * b, void * c, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_c_times_pD_minus_pD");
   qlab::api_ew_n<float, qlab::EW_CT_MINUS, qlab::SC_CONST, false>("FN_ew_axpby", nc, 4 * nc, qlab::PERM_ID, r, a, qlab::Opnd{}, qlab::op_ptr((const void* const*)b), qlab::op_ptr((const void* const*)c), index, n, qlab::EQ);
 }
 

@@ -7,234 +7,292 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_V_veq_v(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_V_vpeq_v(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_vpeq_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_V_vmeq_v(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_vmeq_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_V_veqm_v(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_V_veqm_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_zero(int nc, void * r, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, nc, r, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_h(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_H_vpeq_h(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_vpeq_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_H_vmeq_h(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_vmeq_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_H_veqm_h(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_H_veqm_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_zero(int nc, void * r, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, 2 * nc, r, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_d(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_d(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_d(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_d(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_zero(int nc, void * r, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, 4 * nc, r, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_m(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_vpeq_m(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_vpeq_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_vmeq_m(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_vmeq_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_veqm_m(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veqm_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_zero(int nc, void * r, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, nc * nc, r, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_veq_p(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_P_veq_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_P_vpeq_p(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_P_vpeq_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_P_vmeq_p(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_P_vmeq_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_P_veqm_p(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_P_veqm_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_P_veq_zero(int nc, void * r, int n) {
+  QLAB_TRACE("QLA_FN_P_veq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, 16 * nc * nc, r, nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, nullptr, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_vpeq_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_FN_M_vpeq_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, nullptr, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_vmeq_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_FN_M_vmeq_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, nullptr, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_veqm_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int n) {
+  QLAB_TRACE("QLA_FN_M_veqm_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, nullptr, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_v(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_V_xpeq_v(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xpeq_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_V_xmeq_v(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xmeq_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeqm_v(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeqm_v");
   qlab::api_fill_n<float>("FN_fill", nc, nc, r, a, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_zero(int nc, void * r, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, nc, r, index, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_h(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_H_xpeq_h(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xpeq_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_H_xmeq_h(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xmeq_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeqm_h(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeqm_h");
   qlab::api_fill_n<float>("FN_fill", nc, 2 * nc, r, a, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_zero(int nc, void * r, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, 2 * nc, r, index, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_d(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_d(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_d(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_d(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_d");
   qlab::api_fill_n<float>("FN_fill", nc, 4 * nc, r, a, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_zero(int nc, void * r, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, 4 * nc, r, index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_m(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_xpeq_m(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xpeq_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_xmeq_m(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xmeq_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeqm_m(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeqm_m");
   qlab::api_fill_n<float>("FN_fill", nc, nc * nc, r, a, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_zero(int nc, void * r, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, nc * nc, r, index, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeq_p(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeq_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_P_xpeq_p(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xpeq_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_P_xmeq_p(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xmeq_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeqm_p(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeqm_p");
   qlab::api_fill_n<float>("FN_fill", nc, 16 * nc * nc, r, a, index, n, qlab::EQM);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeq_zero(int nc, void * r, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeq_zero");
   qlab::api_zero_n<float>("FN_fill", nc, 16 * nc * nc, r, index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, index, n, qlab::EQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_xpeq_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xpeq_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, index, n, qlab::PEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_xmeq_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xmeq_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, index, n, qlab::MEQ);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeqm_c(int nc, void * r, QLA_F_Complex *__restrict__ a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeqm_c");
   qlab::api_diagfill_n<float>("FN_fill", nc, r, a, index, n, qlab::EQM);
 }
 

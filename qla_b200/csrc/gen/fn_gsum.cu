@@ -7,162 +7,202 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_v_veq_sum_V(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_v_veq_sum_V");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_v_veq_sum_pV(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_v_veq_sum_pV");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_h_veq_sum_H(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_h_veq_sum_H");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_h_veq_sum_pH(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_h_veq_sum_pH");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_d_veq_sum_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_d_veq_sum_D");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_d_veq_sum_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_d_veq_sum_pD");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_m_veq_sum_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_m_veq_sum_M");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_m_veq_sum_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_m_veq_sum_pM");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_p_veq_sum_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_p_veq_sum_P");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_p_veq_sum_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_p_veq_sum_pP");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_v_veq_sum_V(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_v_veq_sum_V");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_v_veq_sum_pV(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_v_veq_sum_pV");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_h_veq_sum_H(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_h_veq_sum_H");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_h_veq_sum_pH(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_h_veq_sum_pH");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_d_veq_sum_D(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_d_veq_sum_D");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_d_veq_sum_pD(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_d_veq_sum_pD");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_m_veq_sum_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_m_veq_sum_M");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_m_veq_sum_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_m_veq_sum_pM");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_p_veq_sum_P(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_p_veq_sum_P");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_DFN_p_veq_sum_pP(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_p_veq_sum_pP");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_v_xeq_sum_V(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_v_xeq_sum_V");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_v_xeq_sum_pV(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_v_xeq_sum_pV");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_h_xeq_sum_H(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_h_xeq_sum_H");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_h_xeq_sum_pH(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_h_xeq_sum_pH");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_d_xeq_sum_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_d_xeq_sum_D");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_d_xeq_sum_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_d_xeq_sum_pD");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_m_xeq_sum_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_m_xeq_sum_M");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_m_xeq_sum_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_m_xeq_sum_pM");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_p_xeq_sum_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_p_xeq_sum_P");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_p_xeq_sum_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_p_xeq_sum_pP");
   qlab::api_gsum_n<float, float>("FN_gsum", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_v_xeq_sum_V(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_v_xeq_sum_V");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_v_xeq_sum_pV(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_v_xeq_sum_pV");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_h_xeq_sum_H(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_h_xeq_sum_H");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_h_xeq_sum_pH(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_h_xeq_sum_pH");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_d_xeq_sum_D(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_d_xeq_sum_D");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_d_xeq_sum_pD(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_d_xeq_sum_pD");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_m_xeq_sum_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_m_xeq_sum_M");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_m_xeq_sum_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_m_xeq_sum_pM");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_p_xeq_sum_P(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_p_xeq_sum_P");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_DFN_p_xeq_sum_pP(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_p_xeq_sum_pP");
   qlab::api_gsum_n<float, double>("FN_gsum_df", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -7,162 +7,202 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_V_veq_V_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_V_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_V_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_V_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_pV_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_pV_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_pV_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_pV_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_H_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_H_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_H_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_H_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_pH_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_pH_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_pH_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_pH_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_D_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_D_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_pD_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_pD_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_M_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_M_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_M_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_M_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_pM_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_pM_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_pM_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_pM_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_veq_P_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_P_veq_P_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_contig(a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_veq_P_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_P_veq_P_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_veq_pP_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int n) {
+  QLAB_TRACE("QLA_FN_P_veq_pP_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_veq_pP_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int n) {
+  QLAB_TRACE("QLA_FN_P_veq_pP_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_V_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_V_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_V_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_V_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_pV_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_pV_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_pV_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_pV_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_H_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_H_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_H_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_H_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_pH_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_pH_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_pH_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_pH_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 2 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_D_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_D_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_pD_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_pD_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 4 * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_M_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_M_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_M_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_M_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_pM_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_pM_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_pM_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_pM_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeq_P_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeq_P_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_contig(a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeq_P_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeq_P_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeq_pP_mask_I(int nc, void * r, void * a, QLA_Int *__restrict__ b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeq_pP_mask_I");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_P_xeq_pP_mask_pI(int nc, void * r, void * a, QLA_Int *__restrict__ * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_P_xeq_pP_mask_pI");
   qlab::api_mask_n<float>("FN_mask", nc, 16 * nc * nc, r, qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n);
 }
 

@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_r_veq_norm2_V(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -15,6 +16,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_V(int nc, QLA_F_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_pV(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -25,6 +27,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_pV(int nc, QLA_F_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_V(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -35,6 +38,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_V(int nc, QLA_F_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_pV(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -45,6 +49,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_pV(int nc, QLA_F_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_V(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -55,6 +60,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_V(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_pV(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -65,6 +71,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_pV(int nc, QLA_D_Real * r, void * a, int n)
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_V(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -75,6 +82,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_V(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pV(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 2, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 3, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -85,6 +93,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pV(int nc, QLA_D_Real * r, void * a, int * 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_H(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -95,6 +104,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_H(int nc, QLA_F_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_pH(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -105,6 +115,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_pH(int nc, QLA_F_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_H(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -115,6 +126,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_H(int nc, QLA_F_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_pH(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -125,6 +137,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_pH(int nc, QLA_F_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_H(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -135,6 +148,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_H(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_pH(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -145,6 +159,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_pH(int nc, QLA_D_Real * r, void * a, int n)
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_H(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -155,6 +170,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_H(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pH(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 6, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -165,6 +181,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pH(int nc, QLA_D_Real * r, void * a, int * 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_D(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -175,6 +192,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_D(int nc, QLA_F_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_pD(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -185,6 +203,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_pD(int nc, QLA_F_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_D(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -195,6 +214,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_D(int nc, QLA_F_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_pD(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -205,6 +225,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_pD(int nc, QLA_F_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_D(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -215,6 +236,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_D(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_pD(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -225,6 +247,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_pD(int nc, QLA_D_Real * r, void * a, int n)
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_D(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -235,6 +258,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_D(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pD(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 8, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 12, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -245,6 +269,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pD(int nc, QLA_D_Real * r, void * a, int * 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_M(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -255,6 +280,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_M(int nc, QLA_F_Real * r, void * a, int n) {
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_norm2_pM(int nc, QLA_F_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_norm2_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -265,6 +291,7 @@ QLAB_EXPORT void QLA_FN_r_veq_norm2_pM(int nc, QLA_F_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_M(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, float>>("FN_norm2", r, sizeof(float), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -275,6 +302,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_M(int nc, QLA_F_Real * r, void * a, int * in
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_norm2_pM(int nc, QLA_F_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_norm2_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, float>>("FN_norm2", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
@@ -285,6 +313,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_norm2_pM(int nc, QLA_F_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_M(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, nullptr, n); break;
@@ -295,6 +324,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_M(int nc, QLA_D_Real * r, void * a, int n) 
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_norm2_pM(int nc, QLA_D_Real * r, void * a, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_norm2_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, nullptr, n); break;
@@ -305,6 +335,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_norm2_pM(int nc, QLA_D_Real * r, void * a, int n)
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_M(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, double>>("FN_norm2", r, sizeof(double), qlab::op_contig(a), qlab::Opnd{}, index, n); break;
@@ -315,6 +346,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_norm2_M(int nc, QLA_D_Real * r, void * a, int * i
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_norm2_pM(int nc, QLA_D_Real * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_norm2_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::Norm2Op<float, 4, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;
     case 3: qlab::api_reduce<qlab::Norm2Op<float, 9, double>>("FN_norm2", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::Opnd{}, index, n); break;

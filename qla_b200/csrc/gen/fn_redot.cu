@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_r_veq_re_V_dot_V(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_V_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -15,6 +16,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_V_dot_V(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_V_dot_pV(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_V_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -25,6 +27,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_V_dot_pV(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pV_dot_V(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pV_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -35,6 +38,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pV_dot_V(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pV_dot_pV(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pV_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -45,6 +49,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pV_dot_pV(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_V_dot_V(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_V_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -55,6 +60,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_V_dot_V(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_V_dot_pV(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_V_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -65,6 +71,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_V_dot_pV(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pV_dot_V(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pV_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -75,6 +82,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pV_dot_V(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pV_dot_pV(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pV_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -85,6 +93,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pV_dot_pV(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_V_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -95,6 +104,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_V_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -105,6 +115,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pV_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -115,6 +126,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pV_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -125,6 +137,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_V_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -135,6 +148,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_V_dot_V(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_V_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -145,6 +159,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_V_dot_pV(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pV_dot_V");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -155,6 +170,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pV_dot_V(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pV_dot_pV");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 2, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 3, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -165,6 +181,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pV_dot_pV(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_H_dot_H(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_H_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -175,6 +192,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_H_dot_H(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_H_dot_pH(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_H_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -185,6 +203,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_H_dot_pH(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pH_dot_H(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pH_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -195,6 +214,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pH_dot_H(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pH_dot_pH(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pH_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -205,6 +225,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pH_dot_pH(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_H_dot_H(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_H_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -215,6 +236,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_H_dot_H(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_H_dot_pH(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_H_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -225,6 +247,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_H_dot_pH(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pH_dot_H(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pH_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -235,6 +258,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pH_dot_H(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pH_dot_pH(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pH_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -245,6 +269,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pH_dot_pH(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_H_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -255,6 +280,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_H_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -265,6 +291,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pH_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -275,6 +302,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pH_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -285,6 +313,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_H_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -295,6 +324,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_H_dot_H(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_H_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -305,6 +335,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_H_dot_pH(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pH_dot_H");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -315,6 +346,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pH_dot_H(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pH_dot_pH");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 6, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -325,6 +357,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pH_dot_pH(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_D_dot_D(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_D_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -335,6 +368,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_D_dot_D(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_D_dot_pD(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_D_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -345,6 +379,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_D_dot_pD(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pD_dot_D(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pD_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -355,6 +390,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pD_dot_D(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pD_dot_pD(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pD_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -365,6 +401,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pD_dot_pD(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_D_dot_D(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_D_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -375,6 +412,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_D_dot_D(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_D_dot_pD(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_D_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -385,6 +423,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_D_dot_pD(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pD_dot_D(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pD_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -395,6 +434,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pD_dot_D(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pD_dot_pD(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pD_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -405,6 +445,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pD_dot_pD(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_D_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -415,6 +456,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_D_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -425,6 +467,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pD_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -435,6 +478,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pD_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -445,6 +489,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_D_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -455,6 +500,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_D_dot_D(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_D_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -465,6 +511,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_D_dot_pD(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pD_dot_D");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -475,6 +522,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pD_dot_D(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pD_dot_pD");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 8, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 12, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -485,6 +533,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pD_dot_pD(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_M_dot_M(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_M_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -495,6 +544,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_M_dot_M(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_M_dot_pM(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_M_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -505,6 +555,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_M_dot_pM(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pM_dot_M(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pM_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -515,6 +566,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pM_dot_M(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_veq_re_pM_dot_pM(int nc, QLA_F_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_r_veq_re_pM_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -525,6 +577,7 @@ QLAB_EXPORT void QLA_FN_r_veq_re_pM_dot_pM(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_M_dot_M(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_M_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -535,6 +588,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_M_dot_M(int nc, QLA_F_Real * r, void * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_M_dot_pM(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_M_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -545,6 +599,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_M_dot_pM(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pM_dot_M(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pM_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -555,6 +610,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pM_dot_M(int nc, QLA_F_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_FN_r_xeq_re_pM_dot_pM(int nc, QLA_F_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_r_xeq_re_pM_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, float>>("FN_redot", r, sizeof(float), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -565,6 +621,7 @@ QLAB_EXPORT void QLA_FN_r_xeq_re_pM_dot_pM(int nc, QLA_F_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_M_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), nullptr, n); break;
@@ -575,6 +632,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_M_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -585,6 +643,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pM_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), nullptr, n); break;
@@ -595,6 +654,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_veq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int n) {
+  QLAB_TRACE("QLA_DFN_r_veq_re_pM_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), nullptr, n); break;
@@ -605,6 +665,7 @@ QLAB_EXPORT void QLA_DFN_r_veq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, vo
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_M_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_contig(b), index, n); break;
@@ -615,6 +676,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_M_dot_M(int nc, QLA_D_Real * r, void * a, void
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_M_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_contig(a), qlab::op_ptr((const void* const*)b), index, n); break;
@@ -625,6 +687,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_M_dot_pM(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pM_dot_M");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_contig(b), index, n); break;
@@ -635,6 +698,7 @@ QLAB_EXPORT void QLA_DFN_r_xeq_re_pM_dot_M(int nc, QLA_D_Real * r, void * a, voi
 }
 
 QLAB_EXPORT void QLA_DFN_r_xeq_re_pM_dot_pM(int nc, QLA_D_Real * r, void * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_DFN_r_xeq_re_pM_dot_pM");
   switch (nc) {
     case 2: qlab::api_reduce<qlab::ReDotOp<float, 4, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;
     case 3: qlab::api_reduce<qlab::ReDotOp<float, 9, double>>("FN_redot", r, sizeof(double), qlab::op_ptr((const void* const*)a), qlab::op_ptr((const void* const*)b), index, n); break;

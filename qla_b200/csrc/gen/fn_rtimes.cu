@@ -5,6 +5,7 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_V_veq_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -15,6 +16,7 @@ QLAB_EXPORT void QLA_FN_V_veq_r_times_V(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_V_veq_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_veq_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -25,6 +27,7 @@ QLAB_EXPORT void QLA_FN_V_veq_r_times_pV(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_vpeq_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_vpeq_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -35,6 +38,7 @@ QLAB_EXPORT void QLA_FN_V_vpeq_r_times_V(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_vpeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_vpeq_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -45,6 +49,7 @@ QLAB_EXPORT void QLA_FN_V_vpeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_V_vmeq_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_vmeq_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -55,6 +60,7 @@ QLAB_EXPORT void QLA_FN_V_vmeq_r_times_V(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_vmeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_vmeq_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -65,6 +71,7 @@ QLAB_EXPORT void QLA_FN_V_vmeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_V_veqm_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_veqm_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -75,6 +82,7 @@ QLAB_EXPORT void QLA_FN_V_veqm_r_times_V(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_veqm_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_V_veqm_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -85,6 +93,7 @@ QLAB_EXPORT void QLA_FN_V_veqm_r_times_pV(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -95,6 +104,7 @@ QLAB_EXPORT void QLA_FN_V_xeq_r_times_V(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_V_xeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeq_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -105,6 +115,7 @@ QLAB_EXPORT void QLA_FN_V_xeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_xpeq_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xpeq_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -115,6 +126,7 @@ QLAB_EXPORT void QLA_FN_V_xpeq_r_times_V(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_xpeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xpeq_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -125,6 +137,7 @@ QLAB_EXPORT void QLA_FN_V_xpeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_V_xmeq_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xmeq_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -135,6 +148,7 @@ QLAB_EXPORT void QLA_FN_V_xmeq_r_times_V(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_xmeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xmeq_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -145,6 +159,7 @@ QLAB_EXPORT void QLA_FN_V_xmeq_r_times_pV(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_V_xeqm_r_times_V(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeqm_r_times_V");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -155,6 +170,7 @@ QLAB_EXPORT void QLA_FN_V_xeqm_r_times_V(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_V_xeqm_r_times_pV(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_V_xeqm_r_times_pV");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 2>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 3>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -165,6 +181,7 @@ QLAB_EXPORT void QLA_FN_V_xeqm_r_times_pV(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -175,6 +192,7 @@ QLAB_EXPORT void QLA_FN_H_veq_r_times_H(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_H_veq_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_veq_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -185,6 +203,7 @@ QLAB_EXPORT void QLA_FN_H_veq_r_times_pH(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_vpeq_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_vpeq_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -195,6 +214,7 @@ QLAB_EXPORT void QLA_FN_H_vpeq_r_times_H(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_vpeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_vpeq_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -205,6 +225,7 @@ QLAB_EXPORT void QLA_FN_H_vpeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_H_vmeq_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_vmeq_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -215,6 +236,7 @@ QLAB_EXPORT void QLA_FN_H_vmeq_r_times_H(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_vmeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_vmeq_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -225,6 +247,7 @@ QLAB_EXPORT void QLA_FN_H_vmeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_H_veqm_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_veqm_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -235,6 +258,7 @@ QLAB_EXPORT void QLA_FN_H_veqm_r_times_H(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_veqm_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_H_veqm_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -245,6 +269,7 @@ QLAB_EXPORT void QLA_FN_H_veqm_r_times_pH(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -255,6 +280,7 @@ QLAB_EXPORT void QLA_FN_H_xeq_r_times_H(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_H_xeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeq_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -265,6 +291,7 @@ QLAB_EXPORT void QLA_FN_H_xeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_xpeq_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xpeq_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -275,6 +302,7 @@ QLAB_EXPORT void QLA_FN_H_xpeq_r_times_H(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_xpeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xpeq_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -285,6 +313,7 @@ QLAB_EXPORT void QLA_FN_H_xpeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_H_xmeq_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xmeq_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -295,6 +324,7 @@ QLAB_EXPORT void QLA_FN_H_xmeq_r_times_H(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_xmeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xmeq_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -305,6 +335,7 @@ QLAB_EXPORT void QLA_FN_H_xmeq_r_times_pH(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_H_xeqm_r_times_H(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeqm_r_times_H");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -315,6 +346,7 @@ QLAB_EXPORT void QLA_FN_H_xeqm_r_times_H(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_H_xeqm_r_times_pH(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_H_xeqm_r_times_pH");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 6>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -325,6 +357,7 @@ QLAB_EXPORT void QLA_FN_H_xeqm_r_times_pH(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -335,6 +368,7 @@ QLAB_EXPORT void QLA_FN_D_veq_r_times_D(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_D_veq_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veq_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -345,6 +379,7 @@ QLAB_EXPORT void QLA_FN_D_veq_r_times_pD(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -355,6 +390,7 @@ QLAB_EXPORT void QLA_FN_D_vpeq_r_times_D(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_vpeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vpeq_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -365,6 +401,7 @@ QLAB_EXPORT void QLA_FN_D_vpeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -375,6 +412,7 @@ QLAB_EXPORT void QLA_FN_D_vmeq_r_times_D(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_vmeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_vmeq_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -385,6 +423,7 @@ QLAB_EXPORT void QLA_FN_D_vmeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -395,6 +434,7 @@ QLAB_EXPORT void QLA_FN_D_veqm_r_times_D(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_veqm_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_D_veqm_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -405,6 +445,7 @@ QLAB_EXPORT void QLA_FN_D_veqm_r_times_pD(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -415,6 +456,7 @@ QLAB_EXPORT void QLA_FN_D_xeq_r_times_D(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_D_xeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeq_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -425,6 +467,7 @@ QLAB_EXPORT void QLA_FN_D_xeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -435,6 +478,7 @@ QLAB_EXPORT void QLA_FN_D_xpeq_r_times_D(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_xpeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xpeq_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -445,6 +489,7 @@ QLAB_EXPORT void QLA_FN_D_xpeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -455,6 +500,7 @@ QLAB_EXPORT void QLA_FN_D_xmeq_r_times_D(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_xmeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xmeq_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -465,6 +511,7 @@ QLAB_EXPORT void QLA_FN_D_xmeq_r_times_pD(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_r_times_D(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_r_times_D");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -475,6 +522,7 @@ QLAB_EXPORT void QLA_FN_D_xeqm_r_times_D(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_D_xeqm_r_times_pD(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_D_xeqm_r_times_pD");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 8>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 12>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
@@ -485,6 +533,7 @@ QLAB_EXPORT void QLA_FN_D_xeqm_r_times_pD(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQ); break;
@@ -495,6 +544,7 @@ QLAB_EXPORT void QLA_FN_M_veq_r_times_M(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQ); break;
@@ -505,6 +555,7 @@ QLAB_EXPORT void QLA_FN_M_veq_r_times_pM(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_vpeq_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_vpeq_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::PEQ); break;
@@ -515,6 +566,7 @@ QLAB_EXPORT void QLA_FN_M_vpeq_r_times_M(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_vpeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_vpeq_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::PEQ); break;
@@ -525,6 +577,7 @@ QLAB_EXPORT void QLA_FN_M_vpeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_M_vmeq_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_vmeq_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::MEQ); break;
@@ -535,6 +588,7 @@ QLAB_EXPORT void QLA_FN_M_vmeq_r_times_M(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_vmeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_vmeq_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::MEQ); break;
@@ -545,6 +599,7 @@ QLAB_EXPORT void QLA_FN_M_vmeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_M_veqm_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_veqm_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), nullptr, n, qlab::EQM); break;
@@ -555,6 +610,7 @@ QLAB_EXPORT void QLA_FN_M_veqm_r_times_M(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_veqm_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int n) {
+  QLAB_TRACE("QLA_FN_M_veqm_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), nullptr, n, qlab::EQM); break;
@@ -565,6 +621,7 @@ QLAB_EXPORT void QLA_FN_M_veqm_r_times_pM(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQ); break;
@@ -575,6 +632,7 @@ QLAB_EXPORT void QLA_FN_M_xeq_r_times_M(int nc, void * r, QLA_F_Real * a, void *
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQ); break;
@@ -585,6 +643,7 @@ QLAB_EXPORT void QLA_FN_M_xeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_xpeq_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xpeq_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::PEQ); break;
@@ -595,6 +654,7 @@ QLAB_EXPORT void QLA_FN_M_xpeq_r_times_M(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_xpeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xpeq_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::PEQ); break;
@@ -605,6 +665,7 @@ QLAB_EXPORT void QLA_FN_M_xpeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_M_xmeq_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xmeq_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::MEQ); break;
@@ -615,6 +676,7 @@ QLAB_EXPORT void QLA_FN_M_xmeq_r_times_M(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_xmeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xmeq_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::MEQ); break;
@@ -625,6 +687,7 @@ QLAB_EXPORT void QLA_FN_M_xmeq_r_times_pM(int nc, void * r, QLA_F_Real * a, void
 }
 
 QLAB_EXPORT void QLA_FN_M_xeqm_r_times_M(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeqm_r_times_M");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_contig(b), index, n, qlab::EQM); break;
@@ -635,6 +698,7 @@ QLAB_EXPORT void QLA_FN_M_xeqm_r_times_M(int nc, void * r, QLA_F_Real * a, void 
 }
 
 QLAB_EXPORT void QLA_FN_M_xeqm_r_times_pM(int nc, void * r, QLA_F_Real * a, void * b, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeqm_r_times_pM");
   switch (nc) {
     case 2: qlab::api_scalar_map<qlab::RTimesOp<float, 4>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;
     case 3: qlab::api_scalar_map<qlab::RTimesOp<float, 9>, float>("FN_rtimes", r, (const float*)a, qlab::op_ptr((const void* const*)b), index, n, qlab::EQM); break;

@@ -7,66 +7,82 @@
 
 extern "C" {
 QLAB_EXPORT void QLA_FN_C_veq_trace_M(int nc, QLA_F_Complex *__restrict__ r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_C_veq_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("FN_trace", nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_veq_re_trace_M(int nc, QLA_F_Real *__restrict__ r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_R_veq_re_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("FN_trace", nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_veq_im_trace_M(int nc, QLA_F_Real *__restrict__ r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_R_veq_im_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("FN_trace", nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_antiherm_M(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_antiherm_M");
   qlab::api_antiherm_n<float>("FN_trace", nc, r, qlab::op_contig(a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_C_veq_trace_pM(int nc, QLA_F_Complex *__restrict__ r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_C_veq_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_veq_re_trace_pM(int nc, QLA_F_Real *__restrict__ r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_R_veq_re_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_veq_im_trace_pM(int nc, QLA_F_Real *__restrict__ r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_R_veq_im_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_veq_antiherm_pM(int nc, void * r, void * a, int n) {
+  QLAB_TRACE("QLA_FN_M_veq_antiherm_pM");
   qlab::api_antiherm_n<float>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), nullptr, n);
 }
 
 QLAB_EXPORT void QLA_FN_C_xeq_trace_M(int nc, QLA_F_Complex *__restrict__ r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_C_xeq_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("FN_trace", nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_xeq_re_trace_M(int nc, QLA_F_Real *__restrict__ r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_R_xeq_re_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("FN_trace", nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_xeq_im_trace_M(int nc, QLA_F_Real *__restrict__ r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_R_xeq_im_trace_M");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("FN_trace", nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_antiherm_M(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_antiherm_M");
   qlab::api_antiherm_n<float>("FN_trace", nc, r, qlab::op_contig(a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_C_xeq_trace_pM(int nc, QLA_F_Complex *__restrict__ r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_C_xeq_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_C>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_xeq_re_trace_pM(int nc, QLA_F_Real *__restrict__ r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_R_xeq_re_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_RE>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_R_xeq_im_trace_pM(int nc, QLA_F_Real *__restrict__ r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_R_xeq_im_trace_pM");
   qlab::api_trace_n<float, qlab::SF_TRACE_IM>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 
 QLAB_EXPORT void QLA_FN_M_xeq_antiherm_pM(int nc, void * r, void * a, int * index, int n) {
+  QLAB_TRACE("QLA_FN_M_xeq_antiherm_pM");
   qlab::api_antiherm_n<float>("FN_trace", nc, r, qlab::op_ptr((const void* const*)a), index, n);
 }
 

@@ -1,23 +1,35 @@
-// qla_batch.cu -- many fields of uneven volume in one persistent launch.
+// qla_batch.cu -- many fields of uneven volume, each running its own short
+// sequence of level-1 operations, in one persistent launch.
 //
-// A lattice code often applies the same short level-1 sequence to many
-// independent fields (sub-lattices, sources, time slices).  Launching QLA's
-// functions once per field costs a launch each and leaves the GPU idle on
-// the small fields.  Here a plan flattens the fields' tiles into one global
-// tile list (prefix sums over per-field tile counts, kept on the device) and
-// one persistent, warp-specialised bulk-copy pipeline walks that list.
+// A lattice code often applies a short level-1 sequence to many independent
+// fields (sub-lattices, sources, time slices).  Launching QLA's functions
+// once per field and step costs a launch each and leaves the GPU idle on the
+// small fields.  Here a plan flattens every field's tiles into one global
+// tile list (prefix sums over per-field tile counts) and one persistent,
+// warp-specialised bulk-copy pipeline walks that list.  Each field carries a
+// small program (qlagpu_F3_batch_program): streams (its record arrays, some
+// gathered through an int32 index) and steps drawn from the engine's per-site
+// operators -- colour-matrix left multiplication (lmult_site), spin
+// projection and reconstruction (the SpprojOp / SpreconOp bodies), real
+// multiples and copies -- so a field's results are bit-identical to the
+// separate QLA_F3 calls the steps stand for.
 //
-// The sequence is, per field f and site i:
-//     r_f[i] = u_f[i] * u2_f[nbr_f[i]]      (QLA_F3_M_eq_M_times_xM, int32 neighbour gather)
-//     w_f[i] = r_f[i] * v_f[i]              (QLA_F3_V_veq_M_times_V)
-// Both are site-local, so one block computes both for a tile without any
-// dependency on other blocks; r is kept in registers between the two and
-// still written out.  Results are bit-identical to the two separate calls.
+// Per tile the producer lane copies, with 1-D bulk copies into the next
+// pipeline stage, every contiguous input stream of the field, the index tile
+// of every gathered stream and the old values of every INOUT stream.  The
+// consumer warps run the program one site per lane: operands come from the
+// stage, from gathers (read-only global loads at the staged index) or from
+// two per-site registers; stored results go through a per-warp
+// double-buffered shared slice and one bulk store per output stream.  Steps
+// only see values of the same site, so sites are independent and the launch
+// needs no grid-wide ordering.  Partial tiles, and fields whose arrays are
+// not 16-B aligned, run the same program with plain loads and stores.
 //
-// The launch itself (qlagpu_batch_run) only passes the plan's device pointer:
-// it can be replayed from a captured CUDA graph.
+// The launch (qlagpu_batch_run) passes only the plan's device table: it can
+// be replayed from a captured CUDA graph.
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -27,42 +39,56 @@
 
 namespace qlab {
 
-struct BatchField {
-  float* r;
-  const float* u;
-  const float* u2;
-  const int* nbr;
-  float* w;
-  const float* v;
-  long long n;
-  long long tile0;  // first global tile of this field
-  int direct;       // 1: pointers not 16-B aligned, every tile by plain loads
-  int pad;
+constexpr int kMaxStreams = 8, kMaxSteps = 8, kMaxFields = 1024;
+constexpr int kReg0 = 8, kReg1 = 9;
+enum BKind : int { BK_V = 0, BK_H = 1, BK_D = 2, BK_M = 3 };
+enum BRole : int { BR_IN = 0, BR_OUT = 1, BR_INOUT = 2 };
+enum BOp : int { BOP_LMULT = 0, BOP_SPPROJ = 1, BOP_SPRECON = 2, BOP_RTIMES = 3, BOP_COPY = 4 };
+// complex numbers per V, H, D, M record (F3)
+__host__ __device__ constexpr int kncplx(int kind) { return kind == BK_V ? 3 : kind == BK_H ? 6 : kind == BK_D ? 12 : 9; }
+
+struct BStream {
+  char* base;
+  const int* idx;
+  long long nsrc;
+  int kind, role;
+  unsigned stage_off;  // contiguous IN / INOUT: record tile; gathered IN: index tile
+  unsigned out_off;    // OUT / INOUT: this stream's part of a warp's output slice
 };
 
-struct BatchPlan {
-  BatchField* dfields;  // device copy
-  int nfields;
-  long long ntiles;
-  int threads;  // consumer threads = sites per tile
-  int stages;
-  int device;
-  int grid;
-  size_t smem;
+struct BStep {
+  int op, eqop, a, b, dst, store, adja, adjb, mu, sign;
+  int kind_a, kind_b, kind_r;  // operand and result kinds (checked on the host)
+  int load_stream;             // peq / meq: the old value comes from this INOUT stream's tile, else -1
+  float r;
+};
+
+struct alignas(16) BField {
+  BStream s[kMaxStreams];
+  BStep st[kMaxSteps];
+  int nstreams, nsteps;
+  long long n, tile0;
+  unsigned tx_bytes;  // bytes the producer copies per full tile
+  int direct;         // some base not 16-B aligned: every tile by plain loads
 };
 
 struct BatchParams {
-  const BatchField* fields;
+  const BField* fields;
   int nfields;
   long long ntiles;
   int stages;
-  unsigned stage_bytes;
+  unsigned stage_bytes, out_slice_bytes;  // out slice: 32 sites of every output stream
   unsigned* err;
 };
 
-using MxM = LMultOp<float, 3, 3, false, false>;
-using MxV = LMultOp<float, 3, 1, false, false>;
-constexpr int kRecM = 72, kRecV = 24;
+struct BatchPlan {
+  BField* dfields;
+  int nfields;
+  long long ntiles;
+  int threads, stages, grid;
+  unsigned stage_bytes, out_slice_bytes;
+  size_t smem;
+};
 
 __device__ __forceinline__ int find_field(const long long* tile0, int nf, long long g) {
   int lo = 0, hi = nf - 1;  // last field with tile0 <= g
@@ -76,22 +102,268 @@ __device__ __forceinline__ int find_field(const long long* tile0, int nf, long l
   return lo;
 }
 
-// one site, plain loads/stores (partial tiles and unaligned fields)
-__device__ __forceinline__ void batch_site_direct(const BatchField& F, long long i, const SiteParams& sp) {
-  Cx<float> u[9], g[9], v[3], r[9], w[3];
-  Cx<float> dummy[1];
-  load_rec_global<float, 9>(u, F.u + i * 18);
-  load_rec_global<float, 9>(g, F.u2 + (long long)F.nbr[i] * 18);
-  load_rec_global<float, 3>(v, F.v + i * 6);
-  MxM::apply(sp, u, g, dummy, r);
-  MxV::apply(sp, r, v, dummy, w);
-  store_rec<float, 9>(F.r + i * 18, r);
-  store_rec<float, 3>(F.w + i * 6, w);
+using Rec = Cx<float>[12];  // one record of any kind (D is the longest)
+
+// --- record movement with a compile-time length N (complex numbers)
+template <int N>
+__device__ __forceinline__ void ld_smem(Rec& x, const unsigned char* p) {
+  if constexpr (N % 2 == 0) {  // H, D: 16-B multiples
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int e = 0; e < N / 2; e++) {
+      const float4 v = q[e];
+      x[2 * e] = Cx<float>{v.x, v.y};
+      x[2 * e + 1] = Cx<float>{v.z, v.w};
+    }
+  } else {
+    const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      const float2 v = q[e];
+      x[e] = Cx<float>{v.x, v.y};
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ void st_smem(unsigned char* p, const Rec& y) {
+  if constexpr (N % 2 == 0) {
+    float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int e = 0; e < N / 2; e++) q[e] = make_float4(y[2 * e].re, y[2 * e].im, y[2 * e + 1].re, y[2 * e + 1].im);
+  } else {
+    float2* q = reinterpret_cast<float2*>(p);
+#pragma unroll
+    for (int e = 0; e < N; e++) q[e] = make_float2(y[e].re, y[e].im);
+  }
+}
+template <int N>
+__device__ __forceinline__ void ld_global(Rec& x, const void* p) {
+  const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    const float2 v = __ldg(q + e);
+    x[e] = Cx<float>{v.x, v.y};
+  }
+}
+template <int N>
+__device__ __forceinline__ void ld_global_rw(Rec& x, const void* p) {  // a stream this launch also writes
+  const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    const float2 v = q[e];
+    x[e] = Cx<float>{v.x, v.y};
+  }
+}
+template <int N>
+__device__ __forceinline__ void st_global(void* p, const Rec& y) {
+  float2* q = reinterpret_cast<float2*>(p);
+#pragma unroll
+  for (int e = 0; e < N; e++) q[e] = make_float2(y[e].re, y[e].im);
+}
+__device__ __forceinline__ void zero_rec(Rec& x) {
+#pragma unroll
+  for (int e = 0; e < 12; e++) x[e] = Cx<float>{0.f, 0.f};
 }
 
-// Dynamic smem: [full[8], empty[8], abort, field table | S stages (U, idx, V)
-//               | NW x 2 slices of 32 (R, W) records]
-__global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p) {
+// Where one site's operands live: the staged tile (stage != nullptr, lane
+// t) or global memory (site i); the site's two step registers live in shared
+// memory, element-major (element e of register k of thread t at
+// regs + ((k * 12 + e) * T + t) * 8), so that a warp touches consecutive words.
+struct SiteSrc {
+  const unsigned char* stage;
+  int t;
+  long long i;
+  unsigned* err;
+  unsigned char* regs;
+  int T;
+};
+template <int N>
+__device__ __forceinline__ void reg_load(Rec& x, const SiteSrc& src, int slot) {
+  const float2* q = reinterpret_cast<const float2*>(src.regs) + (size_t)slot * 12 * src.T + src.t;
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    const float2 v = q[(size_t)e * src.T];
+    x[e] = Cx<float>{v.x, v.y};
+  }
+}
+template <int N>
+__device__ __forceinline__ void reg_store(const SiteSrc& src, int slot, const Rec& y) {
+  float2* q = reinterpret_cast<float2*>(src.regs) + (size_t)slot * 12 * src.T + src.t;
+#pragma unroll
+  for (int e = 0; e < N; e++) q[(size_t)e * src.T] = make_float2(y[e].re, y[e].im);
+}
+
+// record of stream S at this site, as an input (gathered through its index)
+template <int N>
+__device__ __forceinline__ void fetch_stream(Rec& x, const BStream& S, const SiteSrc& src) {
+  if (S.idx) {
+    long long j = src.stage ? reinterpret_cast<const int*>(src.stage + S.stage_off)[src.t] : S.idx[src.i];
+    if (S.nsrc > 0 && (j < 0 || j >= S.nsrc)) {
+      raise_dev_error(src.err, QLA_DEVERR_BAD_INDEX);
+      zero_rec(x);
+      return;
+    }
+    ld_global<N>(x, S.base + j * (long long)(N * 8));
+  } else if (src.stage) {
+    ld_smem<N>(x, src.stage + S.stage_off + (unsigned)src.t * (N * 8));
+  } else if (S.role == BR_INOUT) {
+    ld_global_rw<N>(x, S.base + src.i * (N * 8));
+  } else {
+    ld_global<N>(x, S.base + src.i * (N * 8));
+  }
+}
+template <int N>
+__device__ __forceinline__ void fetch_n(Rec& x, int ref, const BField& F, const SiteSrc& src) {
+  if (ref >= kReg0)
+    reg_load<N>(x, src, ref - kReg0);
+  else
+    fetch_stream<N>(x, F.s[ref], src);
+}
+__device__ __forceinline__ void fetch(Rec& x, int ref, int kind, const BField& F, const SiteSrc& src) {
+  switch (kind) {
+    case BK_V: fetch_n<3>(x, ref, F, src); break;
+    case BK_H: fetch_n<6>(x, ref, F, src); break;
+    case BK_D: fetch_n<12>(x, ref, F, src); break;
+    default: fetch_n<9>(x, ref, F, src); break;
+  }
+}
+__device__ __forceinline__ void set_reg(const SiteSrc& src, int slot, int kind, const Rec& y) {
+  switch (kind) {
+    case BK_V: reg_store<3>(src, slot, y); break;
+    case BK_H: reg_store<6>(src, slot, y); break;
+    case BK_D: reg_store<12>(src, slot, y); break;
+    default: reg_store<9>(src, slot, y); break;
+  }
+}
+
+// --- the per-site arithmetic of each step kind (the engine's operators)
+template <int N>
+__device__ __forceinline__ void rtimes_n(int eqop, float at, const Rec& b, Rec& y) {  // RTimesOp
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    const float pr = rmul(at, b[e].re), pi = rmul(at, b[e].im);
+    switch (eqop) {
+      case EQ: y[e].re = pr; y[e].im = pi; break;
+      case EQM: y[e].re = -pr; y[e].im = -pi; break;
+      case PEQ: y[e].re = radd(y[e].re, pr); y[e].im = radd(y[e].im, pi); break;
+      default: y[e].re = rsub(y[e].re, pr); y[e].im = rsub(y[e].im, pi); break;
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ void copy_n(int eqop, const Rec& b, Rec& y) {  // CopyOp
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    switch (eqop) {
+      case EQ: y[e] = b[e]; break;
+      case EQM: y[e].re = -b[e].re; y[e].im = -b[e].im; break;
+      case PEQ: y[e].re = radd(y[e].re, b[e].re); y[e].im = radd(y[e].im, b[e].im); break;
+      default: y[e].re = rsub(y[e].re, b[e].re); y[e].im = rsub(y[e].im, b[e].im); break;
+    }
+  }
+}
+
+__device__ __forceinline__ void exec_step(const BStep& S, const Rec& xa, const Rec& xb, Rec& y) {
+  const bool load = (S.eqop == PEQ || S.eqop == MEQ);
+  switch (S.op) {
+    case BOP_LMULT:
+      switch (S.kind_b * 4 + S.adja * 2 + S.adjb) {
+        case BK_V * 4 + 0: lmult_site<float, 3, 1, false, false>(S.eqop, load, xa, xb, y); break;
+        case BK_V * 4 + 2: lmult_site<float, 3, 1, true, false>(S.eqop, load, xa, xb, y); break;
+        case BK_H * 4 + 0: lmult_site<float, 3, 2, false, false>(S.eqop, load, xa, xb, y); break;
+        case BK_H * 4 + 2: lmult_site<float, 3, 2, true, false>(S.eqop, load, xa, xb, y); break;
+        case BK_D * 4 + 0: lmult_site<float, 3, 4, false, false>(S.eqop, load, xa, xb, y); break;
+        case BK_D * 4 + 2: lmult_site<float, 3, 4, true, false>(S.eqop, load, xa, xb, y); break;
+        case BK_M * 4 + 0: lmult_site<float, 3, 3, false, false>(S.eqop, load, xa, xb, y); break;
+        case BK_M * 4 + 1: lmult_site<float, 3, 3, false, true>(S.eqop, load, xa, xb, y); break;
+        case BK_M * 4 + 2: lmult_site<float, 3, 3, true, false>(S.eqop, load, xa, xb, y); break;
+        default: lmult_site<float, 3, 3, true, true>(S.eqop, load, xa, xb, y); break;
+      }
+      break;
+    case BOP_SPPROJ: mu_sign_dispatch<SpprojOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y); break;
+    case BOP_SPRECON: mu_sign_dispatch<SpreconOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y); break;
+    case BOP_RTIMES:
+      switch (S.kind_r) {
+        case BK_V: rtimes_n<3>(S.eqop, S.r, xa, y); break;
+        case BK_H: rtimes_n<6>(S.eqop, S.r, xa, y); break;
+        case BK_D: rtimes_n<12>(S.eqop, S.r, xa, y); break;
+        default: rtimes_n<9>(S.eqop, S.r, xa, y); break;
+      }
+      break;
+    default:
+      switch (S.kind_r) {
+        case BK_V: copy_n<3>(S.eqop, xa, y); break;
+        case BK_H: copy_n<6>(S.eqop, xa, y); break;
+        case BK_D: copy_n<12>(S.eqop, xa, y); break;
+        default: copy_n<9>(S.eqop, xa, y); break;
+      }
+      break;
+  }
+}
+
+// stored result y of stream S: into the warp's output slice (out != nullptr,
+// lane `lane`) or straight to global memory (site i)
+__device__ __forceinline__ void put(const BStream& S, const Rec& y, unsigned char* out, int lane, long long i) {
+  switch (S.kind) {
+    case BK_V:
+      if (out) st_smem<3>(out + S.out_off + (unsigned)lane * 24u, y); else st_global<3>(S.base + i * 24, y);
+      break;
+    case BK_H:
+      if (out) st_smem<6>(out + S.out_off + (unsigned)lane * 48u, y); else st_global<6>(S.base + i * 48, y);
+      break;
+    case BK_D:
+      if (out) st_smem<12>(out + S.out_off + (unsigned)lane * 96u, y); else st_global<12>(S.base + i * 96, y);
+      break;
+    default:
+      if (out) st_smem<9>(out + S.out_off + (unsigned)lane * 72u, y); else st_global<9>(S.base + i * 72, y);
+      break;
+  }
+}
+
+// One site through the field's whole program.
+__device__ __forceinline__ void run_program(const BField& F, const SiteSrc& src, unsigned char* out, int lane) {
+  const int ns = F.nsteps;
+  for (int k = 0; k < ns; k++) {
+    const BStep S = F.st[k];  // uniform across the warp
+    Rec xa, xb, y;
+    fetch(xa, S.a, S.kind_a, F, src);
+    if (S.op == BOP_LMULT) fetch(xb, S.b, S.kind_b, F, src);
+    if (S.eqop == PEQ || S.eqop == MEQ) fetch(y, S.load_stream >= 0 ? S.load_stream : S.dst, S.kind_r, F, src);
+    exec_step(S, xa, xb, y);
+    if (k + 1 < ns) set_reg(src, S.dst - kReg0, S.kind_r, y);  // the last step's register is never read
+    if (S.store >= 0) put(F.s[S.store], y, out, lane, src.i);
+  }
+}
+
+// Copy of field f's descriptor in this warp's shared slot (all lanes take
+// part; the caller's lanes then read it from shared memory, not global), kept
+// while consecutive tiles belong to the same field.
+constexpr int kDescWords = (int)((sizeof(BField) + 15) / 16);  // 16-B words
+__device__ __forceinline__ const BField& cached_field(const BatchParams& p, int f, int& cached, uint4* slot,
+                                                      int lane) {
+  if (f != cached) {
+    __syncwarp();  // every lane is done with the previous field's descriptor
+    const uint4* src = reinterpret_cast<const uint4*>(p.fields + f);
+    for (int w = lane; w < kDescWords; w += 32) slot[w] = __ldg(src + w);
+    __syncwarp();
+    cached = f;
+  }
+  return *reinterpret_cast<const BField*>(slot);
+}
+// the same for the producer, a single lane
+__device__ __forceinline__ const BField& cached_field_1(const BatchParams& p, int f, int& cached, uint4* slot) {
+  if (f != cached) {
+    const uint4* src = reinterpret_cast<const uint4*>(p.fields + f);
+    for (int w = 0; w < kDescWords; w++) slot[w] = __ldg(src + w);
+    cached = f;
+  }
+  return *reinterpret_cast<const BField*>(slot);
+}
+
+// Dynamic smem: [full[8], empty[8] | abort | tile0 table (8 KB) | S stages |
+//               NW x 2 output slices | step registers: 2 x 12 complex x T |
+//               (NW + 1) field descriptors]
+__global__ void __launch_bounds__(288) batch_program_kernel(const BatchParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   const int NW = (blockDim.x >> 5) - 1;
@@ -99,13 +371,15 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + 8;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 128);
-  long long* tile0 = reinterpret_cast<long long*>(smem + 256);  // up to 1024 fields
-  unsigned char* stages = smem + 256 + 8 * 1024;
+  long long* tile0 = reinterpret_cast<long long*>(smem + 256);
+  unsigned char* stages = smem + 256 + 8 * kMaxFields;
   unsigned char* outbuf = stages + (size_t)S * p.stage_bytes;
-  const unsigned offI = (unsigned)T * kRecM, offV = offI + (unsigned)T * 4;
+  unsigned char* regs = outbuf + (size_t)NW * 2 * p.out_slice_bytes;  // 2 x 12 complex per thread
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long my =
       ((long long)blockIdx.x < p.ntiles) ? (p.ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1 : 0;
+  uint4* desc = reinterpret_cast<uint4*>(regs + (size_t)2 * 12 * 8 * T) + (size_t)warp * kDescWords;
+  int cached = -1;
 
   for (int f = tid; f < p.nfields; f += blockDim.x) tile0[f] = p.fields[f].tile0;
   if (tid == 0) {
@@ -117,13 +391,10 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
     mbar_init_fence();
   }
   __syncthreads();
-
-  SiteParams sp;  // the per-site ops only read eqop / out_read
-  sp.eqop = EQ;
-  sp.out_read = 0;
   long long issued = 0;
 
   if (warp == NW) {
+    // ------------------------------------------------------------ producer
     if (lane == 0) {
       const uint64_t pol = policy_evict_first();
       long long k = 0, round = 0;
@@ -135,14 +406,19 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
           break;
         }
         const long long g = (long long)blockIdx.x + k * gridDim.x;
-        const BatchField& F = p.fields[find_field(tile0, p.nfields, g)];
+        const BField& F = cached_field_1(p, find_field(tile0, p.nfields, g), cached, desc);
         const long long site0 = (g - F.tile0) * T;
         unsigned char* st = stages + (size_t)s * p.stage_bytes;
         if (!F.direct && site0 + T <= F.n) {
-          mbar_arrive_expect_tx(&full[s], (unsigned)T * (kRecM + 4 + kRecV));
-          bulk_g2s(st, F.u + site0 * 18, (unsigned)T * kRecM, &full[s], pol);
-          bulk_g2s(st + offI, F.nbr + site0, (unsigned)T * 4, &full[s], pol);
-          bulk_g2s(st + offV, F.v + site0 * 6, (unsigned)T * kRecV, &full[s], pol);
+          mbar_arrive_expect_tx(&full[s], F.tx_bytes);
+          for (int j = 0; j < F.nstreams; j++) {
+            const BStream& B = F.s[j];
+            const unsigned rb = (unsigned)kncplx(B.kind) * 8u;
+            if (B.role == BR_IN && B.idx)
+              bulk_g2s(st + B.stage_off, B.idx + site0, (unsigned)T * 4u, &full[s], pol);
+            else if (B.role != BR_OUT)
+              bulk_g2s(st + B.stage_off, B.base + site0 * rb, (unsigned)T * rb, &full[s], pol);
+          }
         } else {
           mbar_arrive(&full[s]);  // partial / unaligned tile: consumers use plain loads
         }
@@ -154,8 +430,9 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
       issued = k;
     }
   } else {
+    // ------------------------------------------------------------ consumers
     const uint64_t pol = policy_evict_first();
-    unsigned char* myout = outbuf + (size_t)warp * 2 * 32 * (kRecM + kRecV);
+    unsigned char* myout = outbuf + (size_t)warp * 2 * p.out_slice_bytes;
     int s = 0;
     uint32_t par = 0;
     for (long long k = 0; k < my; k++) {
@@ -164,39 +441,42 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
         break;
       }
       const long long g = (long long)blockIdx.x + k * gridDim.x;
-      const BatchField& F = p.fields[find_field(tile0, p.nfields, g)];
+      const BField& F = cached_field(p, find_field(tile0, p.nfields, g), cached, desc, lane);
       const long long site0 = (g - F.tile0) * T;
       const int t = warp * 32 + lane;
-      if (!F.direct && site0 + T <= F.n) {
-        const unsigned char* st = stages + (size_t)s * p.stage_bytes;
-        Cx<float> u[9], gm[9], v[3], r[9], w[3], dummy[1];
-        load_rec<float, 9>(u, st + (unsigned)t * kRecM);
-        const int j = reinterpret_cast<const int*>(st + offI)[t];
-        load_rec<float, 3>(v, st + offV + (unsigned)t * kRecV);
-        load_rec_global<float, 9>(gm, F.u2 + (long long)j * 18);
-        MxM::apply(sp, u, gm, dummy, r);
-        MxV::apply(sp, r, v, dummy, w);
-        unsigned char* ob = myout + (size_t)(k & 1) * 32 * (kRecM + kRecV);
-        if (lane == 0) bulk_wait_read<1>();
+      const long long i = site0 + t;
+      // staged: a full tile of a 16-B aligned field, in the stage; else the
+      // same program with plain loads and stores (partial / unaligned tiles)
+      const bool staged = !F.direct && site0 + T <= F.n;
+      unsigned char* ob = myout + (size_t)(k & 1) * p.out_slice_bytes;
+      if (staged) {
+        if (lane == 0) bulk_wait_read<1>();  // slice (k&1) no longer read by this warp's store k-2
         __syncwarp();
-        store_rec_smem<float, 9>(ob + (unsigned)lane * kRecM, r);
-        store_rec_smem<float, 3>(ob + 32 * kRecM + (unsigned)lane * kRecV, w);
-        // orders this lane's stage reads and slice writes before the async
-        // proxy (the stores below and the producer's next copy into the stage)
+      } else {
+        release_stage(&empty[s], lane);  // this warp is done with the stage
+      }
+      if (staged || i < F.n)  // one call site: the program is inlined once
+        run_program(F, SiteSrc{staged ? stages + (size_t)s * p.stage_bytes : nullptr, t, i, p.err, regs, T},
+                    staged ? ob : nullptr, lane);
+      if (staged) {
+        // every lane orders its reads of the stage and its writes of the
+        // slice before the async proxy: the slice's bulk stores below, and
+        // the producer's next bulk copy into the stage released here
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
           mbar_arrive(&empty[s]);  // this warp is done with the stage
           const long long s0 = site0 + warp * 32;
-          bulk_s2g(F.r + s0 * 18, ob, 32u * kRecM, pol);
-          bulk_s2g(F.w + s0 * 6, ob + 32 * kRecM, 32u * kRecV, pol);
+          for (int j = 0; j < F.nstreams; j++) {
+            const BStream& B = F.s[j];
+            if (B.role == BR_IN) continue;
+            const unsigned rb = (unsigned)kncplx(B.kind) * 8u;
+            bulk_s2g(B.base + s0 * rb, ob + B.out_off, 32u * rb, pol);
+          }
           bulk_commit();
         }
-      } else {
-        release_stage(&empty[s], lane);  // this warp is done with the stage
-        const long long i = site0 + t;
-        if (i < F.n) batch_site_direct(F, i, sp);
-        if (lane == 0) bulk_commit();  // an empty group keeps the slice bookkeeping aligned
+      } else if (lane == 0) {
+        bulk_commit();  // an empty group keeps the slice bookkeeping aligned
       }
       if (++s == S) {
         s = 0;
@@ -207,47 +487,183 @@ __global__ void __launch_bounds__(288) batch_mxm_mxv_kernel(const BatchParams p)
   }
   __syncthreads();
   if (*abort_flag && warp == NW && lane == 0) {
+    // a wait failed: wait (bounded) for every load still in flight before the
+    // block's shared memory is released
     for (long long kk = (issued > S ? issued - S : 0); kk < issued; kk++)
       if (!mbar_wait_bounded(&full[kk % S], (uint32_t)((kk / S) & 1), p.err, 200000000ull, nullptr))
         raise_dev_error(p.err, QLA_DEVERR_BULK_TIMEOUT);
   }
 }
 
-}  // namespace qlab
+// ---------------------------------------------------------------------------
+// host side: validation, stage layout, plan
 
-using namespace qlab;
+static bool plan_error(const char* who, int f, int k, const char* what) {
+  char msg[160];
+  if (k >= 0)
+    std::snprintf(msg, sizeof msg, "field %d, step %d: %s", f, k, what);
+  else
+    std::snprintf(msg, sizeof msg, "field %d: %s", f, what);
+  set_error(QLAGPU_ERR_ARG, who, msg);
+  return false;
+}
 
-extern "C" QLAB_EXPORT void* qlagpu_F3_batch_plan(const qlagpu_F3_batch_field* fields, int nfields) {
-  const char* who = "qlagpu_F3_batch_plan";
-  if (!fields || nfields <= 0 || nfields > 1024) {
+static bool aligned(const void* p, unsigned a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
+
+// Checks one program and fills its device descriptor (kinds, stage offsets
+// for a tile of T sites, output slice offsets).  Returns false with the
+// sticky error set when the program is malformed.
+static bool build_field(const char* who, int f, const qlagpu_F3_batch_program& q, int T, BField& b,
+                        unsigned& stage_bytes, unsigned& out_slice_bytes) {
+  std::memset(&b, 0, sizeof(b));
+  if (q.n < 0 || q.nstreams < 0 || q.nstreams > kMaxStreams || q.nsteps < 1 || q.nsteps > kMaxSteps)
+    return plan_error(who, f, -1, "need n >= 0, 0..8 streams and 1..8 steps");
+  b.nstreams = q.nstreams;
+  b.nsteps = q.nsteps;
+  b.n = q.n;
+  bool al16 = true;
+  unsigned off = 0, oo = 0;
+  for (int j = 0; j < q.nstreams; j++) {
+    const qlagpu_batch_stream& s = q.stream[j];
+    BStream& d = b.s[j];
+    if (s.kind < 0 || s.kind > 3 || s.role < 0 || s.role > 2)
+      return plan_error(who, f, -1, "stream kind or role out of range");
+    if (!s.base && q.n > 0) return plan_error(who, f, -1, "NULL stream base");
+    if (s.index && s.role != BR_IN) return plan_error(who, f, -1, "only IN streams may gather through an index");
+    if (s.index && s.nsrc < 0) return plan_error(who, f, -1, "nsrc < 0");
+    if (!aligned(s.base, 8) || (s.index && !aligned(s.index, 4)))
+      return plan_error(who, f, -1, "stream base must be 8-B aligned and an index 4-B aligned");
+    d.base = static_cast<char*>(s.base);
+    d.idx = s.index;
+    d.nsrc = s.index ? s.nsrc : 0;
+    d.kind = s.kind;
+    d.role = s.role;
+    const unsigned rb = (unsigned)kncplx(s.kind) * 8u;
+    if (s.role == BR_IN && s.index) {
+      d.stage_off = off;
+      off += ((unsigned)T * 4u + 15u) & ~15u;
+      b.tx_bytes += (unsigned)T * 4u;
+      al16 = al16 && aligned(s.index, 16);
+    } else if (s.role != BR_OUT) {
+      d.stage_off = off;
+      off += ((unsigned)T * rb + 15u) & ~15u;
+      b.tx_bytes += (unsigned)T * rb;
+    }
+    if (!s.index || s.role != BR_IN) al16 = al16 && aligned(s.base, 16);
+    if (s.role != BR_IN) {
+      d.out_off = oo;
+      oo += 32u * rb;
+    }
+  }
+  b.direct = al16 ? 0 : 1;
+  int regkind[2] = {-1, -1};
+  bool stored[kMaxStreams] = {false};
+  auto opnd_kind = [&](int ref, int& kind) -> const char* {
+    if (ref == kReg0 || ref == kReg1) {
+      kind = regkind[ref - kReg0];
+      return kind < 0 ? "operand register read before any step wrote it" : nullptr;
+    }
+    if (ref < 0 || ref >= q.nstreams) return "operand is neither a stream of the field nor a register";
+    if (q.stream[ref].role == BR_OUT) return "operand stream is an output of this launch";
+    kind = q.stream[ref].kind;
+    return nullptr;
+  };
+  for (int k = 0; k < q.nsteps; k++) {
+    const qlagpu_batch_step& s = q.step[k];
+    BStep& d = b.st[k];
+    d.op = s.op;
+    d.eqop = s.eqop;
+    d.a = s.a;
+    d.b = s.b;
+    d.dst = s.dst;
+    d.store = s.store;
+    d.adja = s.adja ? 1 : 0;
+    d.adjb = s.adjb ? 1 : 0;
+    d.mu = s.mu;
+    d.sign = s.sign == 1 ? 1 : -1;
+    d.r = s.r;
+    d.load_stream = -1;
+    if (s.op < 0 || s.op > 4) return plan_error(who, f, k, "unknown op");
+    if (s.eqop < 0 || s.eqop > 3) return plan_error(who, f, k, "eqop out of range");
+    if (s.dst != kReg0 && s.dst != kReg1) return plan_error(who, f, k, "dst must be QLAGPU_REG0 or QLAGPU_REG1");
+    if (const char* e = opnd_kind(s.a, d.kind_a)) return plan_error(who, f, k, e);
+    switch (s.op) {
+      case BOP_LMULT:
+        if (d.kind_a != BK_M) return plan_error(who, f, k, "LMULT: a must be a colour matrix");
+        if (const char* e = opnd_kind(s.b, d.kind_b)) return plan_error(who, f, k, e);
+        if (d.adjb && d.kind_b != BK_M) return plan_error(who, f, k, "LMULT: adjb needs a colour-matrix b");
+        d.kind_r = d.kind_b;
+        break;
+      case BOP_SPPROJ:
+        if (d.kind_a != BK_D) return plan_error(who, f, k, "SPPROJ: a must be a DiracFermion");
+        if (s.mu < 0 || s.mu > 4) return plan_error(who, f, k, "mu must be 0..4");
+        d.kind_r = BK_H;
+        break;
+      case BOP_SPRECON:
+        if (d.kind_a != BK_H) return plan_error(who, f, k, "SPRECON: a must be a HalfFermion");
+        if (s.mu < 0 || s.mu > 4) return plan_error(who, f, k, "mu must be 0..4");
+        d.kind_r = BK_D;
+        break;
+      default:
+        d.kind_r = d.kind_a;
+        break;
+    }
+    if (s.op != BOP_LMULT) d.kind_b = d.kind_a;
+    if (s.store >= 0) {
+      if (s.store >= q.nstreams || q.stream[s.store].role == BR_IN)
+        return plan_error(who, f, k, "store must name an OUT or INOUT stream");
+      if (q.stream[s.store].kind != d.kind_r) return plan_error(who, f, k, "stored stream has another kind");
+      if (stored[s.store]) return plan_error(who, f, k, "a stream is stored by more than one step");
+      stored[s.store] = true;
+    } else if (s.store != -1) {
+      return plan_error(who, f, k, "store must be a stream or -1");
+    }
+    if (s.eqop == PEQ || s.eqop == MEQ) {
+      if (s.store >= 0 && q.stream[s.store].role == BR_INOUT) {
+        d.load_stream = s.store;
+      } else if (regkind[s.dst - kReg0] != d.kind_r) {
+        return plan_error(who, f, k, "peq / meq needs an INOUT store stream or a dst register of the result kind");
+      }
+    }
+    regkind[s.dst - kReg0] = d.kind_r;
+  }
+  for (int j = 0; j < q.nstreams; j++)
+    if (q.stream[j].role != BR_IN && !stored[j]) return plan_error(who, f, -1, "an output stream is never stored");
+  if (off > stage_bytes) stage_bytes = off;
+  if (oo > out_slice_bytes) out_slice_bytes = oo;
+  return true;
+}
+
+static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fields, int nfields) {
+  if (!fields || nfields <= 0 || nfields > kMaxFields) {
     set_error(QLAGPU_ERR_ARG, who, "need 1 <= nfields <= 1024 and a field table");
     return nullptr;
   }
   int t = 128, st = 3;
-  if (!tuned_shape("F3_batch_mxm_mxv", &t, &st)) {
+  if (!tuned_shape("F3_batch_program", &t, &st)) {
     t = 128;
     st = 3;
   }
-  std::vector<BatchField> h((size_t)nfields);
+  std::vector<BField> h((size_t)nfields);
+  unsigned stage_bytes = 0, out_slice = 0;
   long long tiles = 0;
   for (int f = 0; f < nfields; f++) {
-    const qlagpu_F3_batch_field& q = fields[f];
-    if (!q.r || !q.u || !q.u2 || !q.nbr || !q.w || !q.v || q.n < 0) {
-      set_error(QLAGPU_ERR_NULLPTR, who, "NULL array in a field (or n < 0)");
-      return nullptr;
-    }
-    BatchField& b = h[(size_t)f];
-    b.r = reinterpret_cast<float*>(q.r);
-    b.u = reinterpret_cast<const float*>(q.u);
-    b.u2 = reinterpret_cast<const float*>(q.u2);
-    b.nbr = q.nbr;
-    b.w = reinterpret_cast<float*>(q.w);
-    b.v = reinterpret_cast<const float*>(q.v);
-    b.n = q.n;
-    b.tile0 = tiles;
-    b.direct = !(aligned16(q.r) && aligned16(q.u) && aligned16(q.nbr) && aligned16(q.w) && aligned16(q.v));
-    b.pad = 0;
-    tiles += (q.n + t - 1) / t;
+    if (!build_field(who, f, fields[f], t, h[(size_t)f], stage_bytes, out_slice)) return nullptr;
+    h[(size_t)f].tile0 = tiles;
+    tiles += (fields[f].n + t - 1) / t;
+  }
+  stage_bytes = (stage_bytes + 127u) & ~127u;
+  if (stage_bytes == 0) stage_bytes = 128;
+  out_slice = (out_slice + 127u) & ~127u;
+  auto smem_for = [&](int stages) {
+    return 256 + 8 * (size_t)kMaxFields + (size_t)stages * stage_bytes + 2 * (size_t)(t / 32) * out_slice +
+           2 * 12 * 8 * (size_t)t + 16 * (size_t)kDescWords * (t / 32 + 1);
+  };
+  size_t smem = smem_for(st);
+  while (smem > 225u * 1024u && st > 2) smem = smem_for(--st);  // shed stages before giving up
+  if (smem > 225u * 1024u) {
+    set_error(QLAGPU_ERR_ARG, who, "the programs' streams need more shared memory per tile than a block has");
+    return nullptr;
   }
   if (!device_error_word()) return nullptr;  // allocate it now, not inside a later capture
   BatchPlan* plan = new BatchPlan();
@@ -255,28 +671,70 @@ extern "C" QLAB_EXPORT void* qlagpu_F3_batch_plan(const qlagpu_F3_batch_field* f
   plan->ntiles = tiles;
   plan->threads = t;
   plan->stages = st;
-  plan->device = current_device();
-  if (cudaMalloc(&plan->dfields, sizeof(BatchField) * (size_t)nfields) != cudaSuccess ||
-      cudaMemcpy(plan->dfields, h.data(), sizeof(BatchField) * (size_t)nfields, cudaMemcpyHostToDevice) !=
+  plan->stage_bytes = stage_bytes;
+  plan->out_slice_bytes = out_slice;
+  plan->smem = smem;
+  if (cudaMalloc(&plan->dfields, sizeof(BField) * (size_t)nfields) != cudaSuccess ||
+      cudaMemcpy(plan->dfields, h.data(), sizeof(BField) * (size_t)nfields, cudaMemcpyHostToDevice) !=
           cudaSuccess) {
     check_launch(who);
     set_error(QLAGPU_ERR_ALLOC, who, "plan table allocation failed");
+    cudaFree(plan->dfields);
     delete plan;
     return nullptr;
   }
-  const unsigned stage_bytes = ((unsigned)t * (kRecM + 4 + kRecV) + 127u) & ~127u;
-  plan->smem = 256 + 8 * 1024 + (size_t)st * stage_bytes + 2 * (size_t)t * (kRecM + kRecV);
-  const void* fn = reinterpret_cast<const void*>(&batch_mxm_mxv_kernel);
+  const void* fn = reinterpret_cast<const void*>(&batch_program_kernel);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem);
   int nb = 1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, t + 32, plan->smem) != cudaSuccess || nb < 1) nb = 1;
+  cudaGetLastError();
   long long grid = (long long)nb * device_sm_count();
   if (grid > tiles) grid = tiles;
   plan->grid = (int)(grid < 1 ? 1 : grid);
   return plan;
 }
 
+}  // namespace qlab
+
+using namespace qlab;
+
+extern "C" QLAB_EXPORT void* qlagpu_F3_batch_plan_program(const qlagpu_F3_batch_program* fields, int nfields) {
+  return make_plan("qlagpu_F3_batch_plan_program", fields, nfields);
+}
+
+// The fixed sequence r = u * u2[nbr] (QLA_F3_M_eq_M_times_xM), w = r * v
+// (QLA_F3_V_veq_M_times_V) as a two-step program per field.
+extern "C" QLAB_EXPORT void* qlagpu_F3_batch_plan(const qlagpu_F3_batch_field* fields, int nfields) {
+  const char* who = "qlagpu_F3_batch_plan";
+  if (!fields || nfields <= 0 || nfields > kMaxFields) {
+    set_error(QLAGPU_ERR_ARG, who, "need 1 <= nfields <= 1024 and a field table");
+    return nullptr;
+  }
+  std::vector<qlagpu_F3_batch_program> prog((size_t)nfields);
+  for (int f = 0; f < nfields; f++) {
+    const qlagpu_F3_batch_field& q = fields[f];
+    if (!q.r || !q.u || !q.u2 || !q.nbr || !q.w || !q.v || q.n < 0) {
+      set_error(QLAGPU_ERR_NULLPTR, who, "NULL array in a field (or n < 0)");
+      return nullptr;
+    }
+    qlagpu_F3_batch_program& p = prog[(size_t)f];
+    std::memset(&p, 0, sizeof(p));
+    p.n = q.n;
+    p.nstreams = 5;
+    p.nsteps = 2;
+    p.stream[0] = qlagpu_batch_stream{q.u, nullptr, 0, QLAGPU_REC_M, QLAGPU_STREAM_IN};
+    p.stream[1] = qlagpu_batch_stream{q.u2, q.nbr, 0, QLAGPU_REC_M, QLAGPU_STREAM_IN};
+    p.stream[2] = qlagpu_batch_stream{q.v, nullptr, 0, QLAGPU_REC_V, QLAGPU_STREAM_IN};
+    p.stream[3] = qlagpu_batch_stream{q.r, nullptr, 0, QLAGPU_REC_M, QLAGPU_STREAM_OUT};
+    p.stream[4] = qlagpu_batch_stream{q.w, nullptr, 0, QLAGPU_REC_V, QLAGPU_STREAM_OUT};
+    p.step[0] = qlagpu_batch_step{QLAGPU_BOP_LMULT, QLAGPU_EQ, 0, 1, QLAGPU_REG0, 3, 0, 0, 0, 1, 0.f};
+    p.step[1] = qlagpu_batch_step{QLAGPU_BOP_LMULT, QLAGPU_EQ, QLAGPU_REG0, 2, QLAGPU_REG1, 4, 0, 0, 0, 1, 0.f};
+  }
+  return make_plan(who, prog.data(), nfields);
+}
+
 extern "C" QLAB_EXPORT int qlagpu_batch_run(void* handle) {
+  QLAB_TRACE("qlagpu_batch_run");
   BatchPlan* plan = static_cast<BatchPlan*>(handle);
   if (!plan) {
     set_error(QLAGPU_ERR_NULLPTR, "qlagpu_batch_run", "NULL plan");
@@ -288,10 +746,11 @@ extern "C" QLAB_EXPORT int qlagpu_batch_run(void* handle) {
   p.nfields = plan->nfields;
   p.ntiles = plan->ntiles;
   p.stages = plan->stages;
-  p.stage_bytes = ((unsigned)plan->threads * (kRecM + 4 + kRecV) + 127u) & ~127u;
+  p.stage_bytes = plan->stage_bytes;
+  p.out_slice_bytes = plan->out_slice_bytes;
   p.err = device_error_word();
   void* args[] = {&p};
-  if (cudaLaunchKernel(reinterpret_cast<const void*>(&batch_mxm_mxv_kernel), dim3((unsigned)plan->grid),
+  if (cudaLaunchKernel(reinterpret_cast<const void*>(&batch_program_kernel), dim3((unsigned)plan->grid),
                        dim3((unsigned)plan->threads + 32u), args, plan->smem, current_stream()) != cudaSuccess) {
     check_launch("qlagpu_batch_run");
     return QLAGPU_ERR_LAUNCH;

@@ -38,7 +38,84 @@ struct PropParams {
   long long n;
   int eqop;
   int vec_a, vec_b, vec_out;  // 16-B vector access allowed (contiguous, aligned)
+  float negzero;              // -0.0f, passed at run time (see mul_rn_x2)
 };
+
+// ---------------------------------------------------------------------------
+// Packed FP32x2 arithmetic with per-lane rounding identical to the scalar
+// __fmul_rn / __fadd_rn / __fsub_rn.  The packed add and sub are used as
+// they are.  A packed product followed by a packed add is fused into one
+// multiply-add by the compiler even with explicit .rn rounding (measured on
+// sm_100a: every result equal to fmaf, none to the separately rounded pair),
+// so the product is written as fma(a, b, z) with z = -0: a*b + (-0) rounds
+// exactly as a*b alone, signed zeros included, and because z is a kernel
+// argument the compiler cannot fold it into a plain product again.
+__device__ __forceinline__ float2 mul_rn_x2(float2 a, float2 b, float z) {
+  float2 r;
+  asm("{.reg .b64 pa, pb, pc, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "mov.b64 pc, {%6, %6};\n\t"
+      "fma.rn.f32x2 pd, pa, pb, pc;\n\t"
+      "mov.b64 {%0, %1}, pd;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(z));
+  return r;
+}
+__device__ __forceinline__ float2 add_rn_x2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pd, pa, pb;\n\t"
+      "mov.b64 {%0, %1}, pd;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 sub_rn_x2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pd, pa, pb;\n\t"
+      "mov.b64 {%0, %1}, pd;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+// x (+|-)= a * b for two output columns at once: lanes hold columns j0, j1
+// (b's real parts bre, imaginary parts bim), a is broadcast.  Per lane the
+// operations and their order are cmac<CA, CB>'s.
+template <bool CA, bool CB>
+__device__ __forceinline__ void cmac_x2(float2& xre, float2& xim, bool minus, Cx<float> a, float2 bre, float2 bim,
+                                        float z) {
+  const float2 ar = make_float2(a.re, a.re), ai = make_float2(a.im, a.im);
+  const float2 p1 = mul_rn_x2(ar, bre, z), p2 = mul_rn_x2(ai, bim, z);
+  const float2 p3 = mul_rn_x2(ar, bim, z), p4 = mul_rn_x2(ai, bre, z);
+  float2 re, im;
+  if constexpr (!CA && !CB) {
+    re = sub_rn_x2(p1, p2);
+    im = add_rn_x2(p3, p4);
+  } else if constexpr (CA && !CB) {
+    re = add_rn_x2(p1, p2);
+    im = sub_rn_x2(p3, p4);
+  } else if constexpr (!CA && CB) {
+    re = add_rn_x2(p1, p2);
+    im = sub_rn_x2(p4, p3);
+  } else {
+    re = sub_rn_x2(p1, p2);
+    im = sub_rn_x2(make_float2(-p3.x, -p3.y), p4);  // (-a.re) b.im = -(a.re b.im) exactly
+  }
+  if (minus) {
+    xre = sub_rn_x2(xre, re);
+    xim = sub_rn_x2(xim, im);
+  } else {
+    xre = add_rn_x2(xre, re);
+    xim = add_rn_x2(xim, im);
+  }
+}
 
 template <typename R>
 __device__ __forceinline__ Cx<R> ld_elem(const Opnd& o, long long k, int e, int rec) {
@@ -246,6 +323,33 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
       }
     };
     load_row(a, 0);
+    if constexpr (sizeof(R) == 4) {
+      // F3: both output columns in packed FP32x2 arithmetic (cmac_x2)
+      float2 bre[12], bim[12];
+#pragma unroll
+      for (int kk = 0; kk < 12; kk++) {
+        bre[kk] = make_float2(b[kk][0].re, b[kk][1].re);
+        bim[kk] = make_float2(b[kk][0].im, b[kk][1].im);
+      }
+#pragma unroll 1
+      for (int row = 0; row < 12; row++) {
+        if (row + 1 < 12) load_row(an, row + 1);
+        float2 xre = make_float2(0.f, 0.f), xim = make_float2(0.f, 0.f);
+        if (load) {
+          Cx<R> x0[2];
+          ld2_out<R>(x0, out + row * 12, p.vec_out);
+          xre = make_float2(x0[0].re, x0[1].re);
+          xim = make_float2(x0[0].im, x0[1].im);
+        }
+#pragma unroll
+        for (int kk = 0; kk < 12; kk++) cmac_x2<CA, CB>(xre, xim, minus, a[kk], bre[kk], bim[kk], p.negzero);
+        const Cx<R> x[2] = {Cx<R>{xre.x, xim.x}, Cx<R>{xre.y, xim.y}};
+        st2<R>(out + row * 12, x, p.vec_out);
+#pragma unroll
+        for (int kk = 0; kk < 12; kk++) a[kk] = an[kk];
+      }
+      continue;
+    }
 #pragma unroll 1
     for (int row = 0; row < 12; row++) {
       if (row + 1 < 12) load_row(an, row + 1);
@@ -268,6 +372,119 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
       }
 #pragma unroll
       for (int kk = 0; kk < 12; kk++) a[kk] = an[kk];
+    }
+  }
+}
+
+// P * P for contiguous, 16-B aligned operands without a gang index: one
+// thread per (site, output row), SPB sites per block.  The block copies the
+// second operand's SPB records into shared memory with coalesced 16-B loads
+// (for F3 also a copy with each complex number's parts swapped), then every
+// thread keeps its row of the first operand (of P, or of P^+) in registers
+// and walks the 12 rows of the second operand (of P or P^+) in shared memory;
+// the 12 threads of a site read the same words (broadcasts).  Output rows are
+// written with 16-B stores.
+//
+// F3 packs the real and imaginary part of one output element into the two
+// lanes of an FP32x2 register: with b = (br, bi) and its swap bs = (bi, br),
+//   (re, im) = (ar, sa ar) * b + (ta ai, tb ai) * bs
+// where the signs sa, ta, tb follow the conjugations (CA, CB) so that each lane
+// forms the same two rounded products and the same rounded sum as cmac<CA, CB>
+// (a product of a negated operand is the exactly negated product, and
+// x + (-y) is x - y); the accumulation x (+|-)= (re, im) is a packed add or
+// subtract.  D3 runs cmac<CA, CB> on the same mapping.  Bit-identical either way.
+template <typename R, bool CA, bool CB, int SPB>
+__global__ void __launch_bounds__(12 * SPB) prop_pp_rows_kernel(const PropParams p) {
+  extern __shared__ __align__(16) unsigned char psm[];
+  constexpr bool F32 = sizeof(R) == 4;
+  Cx<R>* Bs = reinterpret_cast<Cx<R>*>(psm);  // [SPB][144]
+  Cx<R>* Bw = Bs + SPB * 144;                  // F3: the same records, parts swapped
+  const long long site0 = (long long)blockIdx.x * SPB;
+  const long long left = p.n - site0;
+  const int nloc = left < SPB ? (int)left : SPB;
+  {
+    const int words = nloc * 144 * (int)sizeof(Cx<R>) / 16;
+    const char* Bg = static_cast<const char*>(p.b.base) + site0 * 144 * (long long)sizeof(Cx<R>);
+    for (int w = threadIdx.x; w < words; w += blockDim.x) {
+      if constexpr (F32) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(Bg) + w);
+        reinterpret_cast<float4*>(Bs)[w] = v;
+        reinterpret_cast<float4*>(Bw)[w] = make_float4(v.y, v.x, v.w, v.z);
+      } else {
+        reinterpret_cast<double2*>(Bs)[w] = __ldg(reinterpret_cast<const double2*>(Bg) + w);
+      }
+    }
+  }
+  __syncthreads();
+  const int ls = threadIdx.x / 12, row = threadIdx.x - ls * 12;  // local site, output row ic * 4 + is
+  if (ls >= nloc) return;                                         // (after the block's only barrier)
+  const long long k = site0 + ls;
+  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
+  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+  const Cx<R>* A = static_cast<const Cx<R>*>(p.a.base) + k * 144;
+  Cx<R> a[12];
+  if constexpr (!CA) {
+#pragma unroll
+    for (int kk = 0; kk < 12; kk += 2) {
+      Cx<R> t[2];
+      ld2_out<R>(t, A + row * 12 + kk, true);
+      a[kk] = t[0];
+      a[kk + 1] = t[1];
+    }
+  } else {
+#pragma unroll
+    for (int kk = 0; kk < 12; kk++) a[kk] = A[kk * 12 + row];  // P^+[row][kk] = conj P[kk][row]
+  }
+  Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 144 + row * 12;
+  const Cx<R>* B = Bs + ls * 144;
+  // element (kk, jj) of the second operand before conjugation: P[kk][jj], or P[jj][kk] for P^+
+  auto bidx = [](int kk, int jj) { return CB ? jj * 12 + kk : kk * 12 + jj; };
+  if constexpr (F32) {
+    const Cx<float>* W = Bw + ls * 144;
+    constexpr float sa = CB ? -1.f : 1.f;
+    constexpr float ta = (CA == CB) ? -1.f : 1.f, tb = CA ? -1.f : 1.f;
+    float2 x[12];
+#pragma unroll
+    for (int jj = 0; jj < 12; jj += 2) {
+      if (load) {
+        Cx<float> t[2];
+        ld2_out<float>(t, out + jj, true);
+        x[jj] = make_float2(t[0].re, t[0].im);
+        x[jj + 1] = make_float2(t[1].re, t[1].im);
+      } else {
+        x[jj] = make_float2(0.f, 0.f);
+        x[jj + 1] = make_float2(0.f, 0.f);
+      }
+    }
+    const float z = p.negzero;
+#pragma unroll
+    for (int kk = 0; kk < 12; kk++) {
+      const float2 pa = make_float2(a[kk].re, sa * a[kk].re), qa = make_float2(ta * a[kk].im, tb * a[kk].im);
+#pragma unroll
+      for (int jj = 0; jj < 12; jj++) {
+        const Cx<float> bv = B[bidx(kk, jj)], bw = W[bidx(kk, jj)];
+        const float2 prod =
+            add_rn_x2(mul_rn_x2(pa, make_float2(bv.re, bv.im), z), mul_rn_x2(qa, make_float2(bw.re, bw.im), z));
+        x[jj] = minus ? sub_rn_x2(x[jj], prod) : add_rn_x2(x[jj], prod);
+      }
+    }
+#pragma unroll
+    for (int jj = 0; jj < 12; jj += 2) {
+      const Cx<float> t[2] = {Cx<float>{x[jj].x, x[jj].y}, Cx<float>{x[jj + 1].x, x[jj + 1].y}};
+      st2<float>(out + jj, t, true);
+    }
+  } else {
+    Cx<R> x[12];
+#pragma unroll
+    for (int jj = 0; jj < 12; jj++) x[jj] = load ? out[jj] : Cx<R>{R(0), R(0)};
+#pragma unroll
+    for (int kk = 0; kk < 12; kk++)
+#pragma unroll
+      for (int jj = 0; jj < 12; jj++) cmac<CA, CB>(x[jj], minus, a[kk], B[bidx(kk, jj)]);
+#pragma unroll
+    for (int jj = 0; jj < 12; jj += 2) {
+      const Cx<R> t[2] = {x[jj], x[jj + 1]};
+      st2<R>(out + jj, t, true);
     }
   }
 }
@@ -319,6 +536,7 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
   p.vec_out = (reinterpret_cast<uintptr_t>(r) & 15u) == 0;
   p.vec_a = a.mode == OM_CONTIG && (reinterpret_cast<uintptr_t>(a.base) & 15u) == 0;
   p.vec_b = b.mode == OM_CONTIG && (reinterpret_cast<uintptr_t>(b.base) & 15u) == 0;
+  p.negzero = -0.0f;
   const int per_site = KIND == PK_TRACE ? 9 : KIND == PK_PP ? (sizeof(R) == 4 ? 6 : 12) : 24;
   const long long total = (long long)n * per_site;
   long long grid = (total + 255) / 256;
@@ -332,8 +550,14 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
     prop_mp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
   else if constexpr (KIND == PK_PM)
     prop_pm_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
-  else
+  else if (gang == nullptr && a.mode == OM_CONTIG && b.mode == OM_CONTIG && p.vec_a && p.vec_b && p.vec_out) {
+    constexpr int SPB = sizeof(R) == 4 ? 16 : 8;  // sites per block
+    const size_t smem = (size_t)SPB * 144 * sizeof(Cx<R>) * (sizeof(R) == 4 ? 2 : 1);
+    const long long blocks = ((long long)n + SPB - 1) / SPB;
+    prop_pp_rows_kernel<R, CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p);
+  } else {
     prop_pp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+  }
   check_launch(kid);
 }
 

@@ -6,6 +6,7 @@
 // reductions, and the autotuner's launch-shape table.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstdlib>
@@ -207,6 +208,16 @@ __global__ void wait_timeout_selftest_kernel(unsigned* err, unsigned long long l
   __syncthreads();
   if (threadIdx.x == 0) *gave_up = mbar_wait_bounded(&bar, 0u, err, limit_ns) ? 0 : 1;
 }
+
+bool trace_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QLA_B200_NVTX");
+    return e && e[0] && e[0] != '0';
+  }();
+  return on;
+}
+void trace_push(const char* name) { nvtxRangePushA(name); }
+void trace_pop() { nvtxRangePop(); }
 
 // error bits recorded by the allocation-free entry point on the current
 // device (defined in qla_noalloc.cu); allocates nothing

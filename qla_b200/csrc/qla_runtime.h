@@ -45,4 +45,22 @@ unsigned* device_error_word();
 // check the last launch and record an error on failure
 bool check_launch(const char* where);
 
+// Tracing: with QLA_B200_NVTX=1 in the environment (read once) every C-ABI
+// entry point is an NVTX range named after its QLA function, for timeline
+// tools; otherwise a range costs one predictable branch.
+bool trace_enabled();
+void trace_push(const char* name);
+void trace_pop();
+struct TraceRange {
+  bool on;
+  explicit TraceRange(const char* name) : on(trace_enabled()) {
+    if (on) trace_push(name);
+  }
+  ~TraceRange() {
+    if (on) trace_pop();
+  }
+};
+
 }  // namespace qlab
+
+#define QLAB_TRACE(name) ::qlab::TraceRange qlab_trace_range_(name)

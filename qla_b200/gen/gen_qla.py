@@ -1513,7 +1513,8 @@ def main():
             extra = '#include "../qla_mfunc_nc2.cuh"\n'
         text = CU_TOP.format(pc=pc, family=family, cite=CITE[family], extra_includes=extra)
         for fn in fns:
-            text += "QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  " + fn.body + "\n}\n\n"
+            text += ("QLAB_EXPORT " + fn.proto("__restrict__") + " {\n  QLAB_TRACE(\"" + fn.name + "\");\n  " +
+                     fn.body + "\n}\n\n")
         text += "}  // extern \"C\"\n"
         written += write_if_changed(os.path.join(OUT_CU, f"{pc.lower()}_{family}.cu"), text)
     mtext = json.dumps(manifest, indent=0, sort_keys=True)
