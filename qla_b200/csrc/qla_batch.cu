@@ -20,7 +20,7 @@
 // consumer warps run the program one site per lane: operands come from the
 // stage, from gathers (read-only global loads at the staged index) or from
 // two per-site registers; stored results go through a per-warp
-// double-buffered shared slice and one bulk store per output stream.  Steps
+// per-warp shared slice and one bulk store per output stream.  Steps
 // only see values of the same site, so sites are independent and the launch
 // needs no grid-wide ordering.  Partial tiles, and fields whose arrays are
 // not 16-B aligned, run the same program with plain loads and stores.
@@ -31,6 +31,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/qla_b200_runtime.h"
@@ -60,6 +61,8 @@ struct BStep {
   int op, eqop, a, b, dst, store, adja, adjb, mu, sign;
   int kind_a, kind_b, kind_r;  // operand and result kinds (checked on the host)
   int load_stream;             // peq / meq: the old value comes from this INOUT stream's tile, else -1
+  int spill;                   // a later step other than the next one reads this result's register
+  int src_a, src_b;            // SrcKind of the operands (classified by the planner)
   float r;
 };
 
@@ -78,6 +81,7 @@ struct BatchParams {
   long long ntiles;
   int stages;
   unsigned stage_bytes, out_slice_bytes;  // out slice: 32 sites of every output stream
+  int spill_regs;                         // some program keeps a register in shared memory
   unsigned* err;
 };
 
@@ -87,6 +91,9 @@ struct BatchPlan {
   long long ntiles;
   int threads, stages, grid;
   unsigned stage_bytes, out_slice_bytes;
+  int spill_regs;
+  int mc;     // record capacity of the kernel instance: 9 or 12 complex numbers
+  int shape;  // ShapeId of the kernel instance (SH_GENERIC: the interpreter)
   size_t smem;
 };
 
@@ -102,11 +109,15 @@ __device__ __forceinline__ int find_field(const long long* tile0, int nf, long l
   return lo;
 }
 
-using Rec = Cx<float>[12];  // one record of any kind (D is the longest)
+// One record of any kind the plan uses, MC complex numbers long: 12 when
+// some field uses DiracFermions, else 9 (colour matrices are the longest),
+// which keeps the kernel's registers down for V / H / M programs.
+template <int MC>
+using Rec = Cx<float>[MC];
 
 // --- record movement with a compile-time length N (complex numbers)
-template <int N>
-__device__ __forceinline__ void ld_smem(Rec& x, const unsigned char* p) {
+template <int N, int MC>
+__device__ __forceinline__ void ld_smem(Rec<MC>& x, const unsigned char* p) {
   if constexpr (N % 2 == 0) {  // H, D: 16-B multiples
     const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
@@ -124,8 +135,8 @@ __device__ __forceinline__ void ld_smem(Rec& x, const unsigned char* p) {
     }
   }
 }
-template <int N>
-__device__ __forceinline__ void st_smem(unsigned char* p, const Rec& y) {
+template <int N, int MC>
+__device__ __forceinline__ void st_smem(unsigned char* p, const Rec<MC>& y) {
   if constexpr (N % 2 == 0) {
     float4* q = reinterpret_cast<float4*>(p);
 #pragma unroll
@@ -136,8 +147,8 @@ __device__ __forceinline__ void st_smem(unsigned char* p, const Rec& y) {
     for (int e = 0; e < N; e++) q[e] = make_float2(y[e].re, y[e].im);
   }
 }
-template <int N>
-__device__ __forceinline__ void ld_global(Rec& x, const void* p) {
+template <int N, int MC>
+__device__ __forceinline__ void ld_global(Rec<MC>& x, const void* p) {
   const float2* q = reinterpret_cast<const float2*>(p);
 #pragma unroll
   for (int e = 0; e < N; e++) {
@@ -145,8 +156,8 @@ __device__ __forceinline__ void ld_global(Rec& x, const void* p) {
     x[e] = Cx<float>{v.x, v.y};
   }
 }
-template <int N>
-__device__ __forceinline__ void ld_global_rw(Rec& x, const void* p) {  // a stream this launch also writes
+template <int N, int MC>
+__device__ __forceinline__ void ld_global_rw(Rec<MC>& x, const void* p) {  // a stream this launch also writes
   const float2* q = reinterpret_cast<const float2*>(p);
 #pragma unroll
   for (int e = 0; e < N; e++) {
@@ -154,21 +165,29 @@ __device__ __forceinline__ void ld_global_rw(Rec& x, const void* p) {  // a stre
     x[e] = Cx<float>{v.x, v.y};
   }
 }
-template <int N>
-__device__ __forceinline__ void st_global(void* p, const Rec& y) {
+template <int N, int MC>
+__device__ __forceinline__ void st_global(void* p, const Rec<MC>& y) {
   float2* q = reinterpret_cast<float2*>(p);
 #pragma unroll
   for (int e = 0; e < N; e++) q[e] = make_float2(y[e].re, y[e].im);
 }
-__device__ __forceinline__ void zero_rec(Rec& x) {
+template <int MC>
+__device__ __forceinline__ void zero_rec(Rec<MC>& x) {
 #pragma unroll
-  for (int e = 0; e < 12; e++) x[e] = Cx<float>{0.f, 0.f};
+  for (int e = 0; e < MC; e++) x[e] = Cx<float>{0.f, 0.f};
+}
+template <int MC>
+__device__ __forceinline__ void copy_rec(Rec<MC>& x, const Rec<MC>& y) {
+#pragma unroll
+  for (int e = 0; e < MC; e++) x[e] = y[e];
 }
 
 // Where one site's operands live: the staged tile (stage != nullptr, lane
-// t) or global memory (site i); the site's two step registers live in shared
-// memory, element-major (element e of register k of thread t at
-// regs + ((k * 12 + e) * T + t) * 8), so that a warp touches consecutive words.
+// t) or global memory (site i).  Step registers: the previous step's result
+// stays in registers (`prev`); a result that a later, non-adjacent step reads
+// is also kept in shared memory, element-major (element e of register k of
+// thread t at regs + ((k * 12 + e) * T + t) * 8), so a warp touches
+// consecutive words.
 struct SiteSrc {
   const unsigned char* stage;
   int t;
@@ -177,8 +196,8 @@ struct SiteSrc {
   unsigned char* regs;
   int T;
 };
-template <int N>
-__device__ __forceinline__ void reg_load(Rec& x, const SiteSrc& src, int slot) {
+template <int N, int MC>
+__device__ __forceinline__ void reg_load(Rec<MC>& x, const SiteSrc& src, int slot) {
   const float2* q = reinterpret_cast<const float2*>(src.regs) + (size_t)slot * 12 * src.T + src.t;
 #pragma unroll
   for (int e = 0; e < N; e++) {
@@ -186,16 +205,16 @@ __device__ __forceinline__ void reg_load(Rec& x, const SiteSrc& src, int slot) {
     x[e] = Cx<float>{v.x, v.y};
   }
 }
-template <int N>
-__device__ __forceinline__ void reg_store(const SiteSrc& src, int slot, const Rec& y) {
+template <int N, int MC>
+__device__ __forceinline__ void reg_store(const SiteSrc& src, int slot, const Rec<MC>& y) {
   float2* q = reinterpret_cast<float2*>(src.regs) + (size_t)slot * 12 * src.T + src.t;
 #pragma unroll
   for (int e = 0; e < N; e++) q[(size_t)e * src.T] = make_float2(y[e].re, y[e].im);
 }
 
 // record of stream S at this site, as an input (gathered through its index)
-template <int N>
-__device__ __forceinline__ void fetch_stream(Rec& x, const BStream& S, const SiteSrc& src) {
+template <int N, int MC>
+__device__ __forceinline__ void fetch_stream(Rec<MC>& x, const BStream& S, const SiteSrc& src) {
   if (S.idx) {
     long long j = src.stage ? reinterpret_cast<const int*>(src.stage + S.stage_off)[src.t] : S.idx[src.i];
     if (S.nsrc > 0 && (j < 0 || j >= S.nsrc)) {
@@ -212,33 +231,45 @@ __device__ __forceinline__ void fetch_stream(Rec& x, const BStream& S, const Sit
     ld_global<N>(x, S.base + src.i * (N * 8));
   }
 }
-template <int N>
-__device__ __forceinline__ void fetch_n(Rec& x, int ref, const BField& F, const SiteSrc& src) {
-  if (ref >= kReg0)
+// operand `ref` (a stream, or a register) of kind `kind`; prev / prev_reg:
+// the previous step's result and its register
+template <int N, int MC>
+__device__ __forceinline__ void fetch_n(Rec<MC>& x, int ref, const BField& F, const SiteSrc& src,
+                                        const Rec<MC>& prev, int prev_reg) {
+  if (ref == prev_reg)
+    copy_rec(x, prev);
+  else if (ref >= kReg0)
     reg_load<N>(x, src, ref - kReg0);
   else
     fetch_stream<N>(x, F.s[ref], src);
 }
-__device__ __forceinline__ void fetch(Rec& x, int ref, int kind, const BField& F, const SiteSrc& src) {
+template <int MC>
+__device__ __forceinline__ void fetch(Rec<MC>& x, int ref, int kind, const BField& F, const SiteSrc& src,
+                                      const Rec<MC>& prev, int prev_reg) {
   switch (kind) {
-    case BK_V: fetch_n<3>(x, ref, F, src); break;
-    case BK_H: fetch_n<6>(x, ref, F, src); break;
-    case BK_D: fetch_n<12>(x, ref, F, src); break;
-    default: fetch_n<9>(x, ref, F, src); break;
+    case BK_V: fetch_n<3>(x, ref, F, src, prev, prev_reg); break;
+    case BK_H: fetch_n<6>(x, ref, F, src, prev, prev_reg); break;
+    case BK_M: fetch_n<9>(x, ref, F, src, prev, prev_reg); break;
+    default:
+      if constexpr (MC >= 12) fetch_n<12>(x, ref, F, src, prev, prev_reg);
+      break;
   }
 }
-__device__ __forceinline__ void set_reg(const SiteSrc& src, int slot, int kind, const Rec& y) {
+template <int MC>
+__device__ __forceinline__ void set_reg(const SiteSrc& src, int slot, int kind, const Rec<MC>& y) {
   switch (kind) {
     case BK_V: reg_store<3>(src, slot, y); break;
     case BK_H: reg_store<6>(src, slot, y); break;
-    case BK_D: reg_store<12>(src, slot, y); break;
-    default: reg_store<9>(src, slot, y); break;
+    case BK_M: reg_store<9>(src, slot, y); break;
+    default:
+      if constexpr (MC >= 12) reg_store<12>(src, slot, y);
+      break;
   }
 }
 
 // --- the per-site arithmetic of each step kind (the engine's operators)
-template <int N>
-__device__ __forceinline__ void rtimes_n(int eqop, float at, const Rec& b, Rec& y) {  // RTimesOp
+template <int N, int MC>
+__device__ __forceinline__ void rtimes_n(int eqop, float at, const Rec<MC>& b, Rec<MC>& y) {  // RTimesOp
 #pragma unroll
   for (int e = 0; e < N; e++) {
     const float pr = rmul(at, b[e].re), pi = rmul(at, b[e].im);
@@ -250,8 +281,8 @@ __device__ __forceinline__ void rtimes_n(int eqop, float at, const Rec& b, Rec& 
     }
   }
 }
-template <int N>
-__device__ __forceinline__ void copy_n(int eqop, const Rec& b, Rec& y) {  // CopyOp
+template <int N, int MC>
+__device__ __forceinline__ void copy_n(int eqop, const Rec<MC>& b, Rec<MC>& y) {  // CopyOp
 #pragma unroll
   for (int e = 0; e < N; e++) {
     switch (eqop) {
@@ -263,7 +294,8 @@ __device__ __forceinline__ void copy_n(int eqop, const Rec& b, Rec& y) {  // Cop
   }
 }
 
-__device__ __forceinline__ void exec_step(const BStep& S, const Rec& xa, const Rec& xb, Rec& y) {
+template <int MC>
+__device__ __forceinline__ void exec_step(const BStep& S, const Rec<MC>& xa, const Rec<MC>& xb, Rec<MC>& y) {
   const bool load = (S.eqop == PEQ || S.eqop == MEQ);
   switch (S.op) {
     case BOP_LMULT:
@@ -272,30 +304,44 @@ __device__ __forceinline__ void exec_step(const BStep& S, const Rec& xa, const R
         case BK_V * 4 + 2: lmult_site<float, 3, 1, true, false>(S.eqop, load, xa, xb, y); break;
         case BK_H * 4 + 0: lmult_site<float, 3, 2, false, false>(S.eqop, load, xa, xb, y); break;
         case BK_H * 4 + 2: lmult_site<float, 3, 2, true, false>(S.eqop, load, xa, xb, y); break;
-        case BK_D * 4 + 0: lmult_site<float, 3, 4, false, false>(S.eqop, load, xa, xb, y); break;
-        case BK_D * 4 + 2: lmult_site<float, 3, 4, true, false>(S.eqop, load, xa, xb, y); break;
         case BK_M * 4 + 0: lmult_site<float, 3, 3, false, false>(S.eqop, load, xa, xb, y); break;
         case BK_M * 4 + 1: lmult_site<float, 3, 3, false, true>(S.eqop, load, xa, xb, y); break;
         case BK_M * 4 + 2: lmult_site<float, 3, 3, true, false>(S.eqop, load, xa, xb, y); break;
-        default: lmult_site<float, 3, 3, true, true>(S.eqop, load, xa, xb, y); break;
+        case BK_M * 4 + 3: lmult_site<float, 3, 3, true, true>(S.eqop, load, xa, xb, y); break;
+        default:
+          if constexpr (MC >= 12) {
+            if (S.adja)
+              lmult_site<float, 3, 4, true, false>(S.eqop, load, xa, xb, y);
+            else
+              lmult_site<float, 3, 4, false, false>(S.eqop, load, xa, xb, y);
+          }
+          break;
       }
       break;
-    case BOP_SPPROJ: mu_sign_dispatch<SpprojOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y); break;
-    case BOP_SPRECON: mu_sign_dispatch<SpreconOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y); break;
+    case BOP_SPPROJ:
+      if constexpr (MC >= 12) mu_sign_dispatch<SpprojOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y);
+      break;
+    case BOP_SPRECON:
+      if constexpr (MC >= 12) mu_sign_dispatch<SpreconOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y);
+      break;
     case BOP_RTIMES:
       switch (S.kind_r) {
         case BK_V: rtimes_n<3>(S.eqop, S.r, xa, y); break;
         case BK_H: rtimes_n<6>(S.eqop, S.r, xa, y); break;
-        case BK_D: rtimes_n<12>(S.eqop, S.r, xa, y); break;
-        default: rtimes_n<9>(S.eqop, S.r, xa, y); break;
+        case BK_M: rtimes_n<9>(S.eqop, S.r, xa, y); break;
+        default:
+          if constexpr (MC >= 12) rtimes_n<12>(S.eqop, S.r, xa, y);
+          break;
       }
       break;
     default:
       switch (S.kind_r) {
         case BK_V: copy_n<3>(S.eqop, xa, y); break;
         case BK_H: copy_n<6>(S.eqop, xa, y); break;
-        case BK_D: copy_n<12>(S.eqop, xa, y); break;
-        default: copy_n<9>(S.eqop, xa, y); break;
+        case BK_M: copy_n<9>(S.eqop, xa, y); break;
+        default:
+          if constexpr (MC >= 12) copy_n<12>(S.eqop, xa, y);
+          break;
       }
       break;
   }
@@ -303,7 +349,8 @@ __device__ __forceinline__ void exec_step(const BStep& S, const Rec& xa, const R
 
 // stored result y of stream S: into the warp's output slice (out != nullptr,
 // lane `lane`) or straight to global memory (site i)
-__device__ __forceinline__ void put(const BStream& S, const Rec& y, unsigned char* out, int lane, long long i) {
+template <int MC>
+__device__ __forceinline__ void put(const BStream& S, const Rec<MC>& y, unsigned char* out, int lane, long long i) {
   switch (S.kind) {
     case BK_V:
       if (out) st_smem<3>(out + S.out_off + (unsigned)lane * 24u, y); else st_global<3>(S.base + i * 24, y);
@@ -311,28 +358,160 @@ __device__ __forceinline__ void put(const BStream& S, const Rec& y, unsigned cha
     case BK_H:
       if (out) st_smem<6>(out + S.out_off + (unsigned)lane * 48u, y); else st_global<6>(S.base + i * 48, y);
       break;
-    case BK_D:
-      if (out) st_smem<12>(out + S.out_off + (unsigned)lane * 96u, y); else st_global<12>(S.base + i * 96, y);
+    case BK_M:
+      if (out) st_smem<9>(out + S.out_off + (unsigned)lane * 72u, y); else st_global<9>(S.base + i * 72, y);
       break;
     default:
-      if (out) st_smem<9>(out + S.out_off + (unsigned)lane * 72u, y); else st_global<9>(S.base + i * 72, y);
+      if constexpr (MC >= 12) {
+        if (out) st_smem<12>(out + S.out_off + (unsigned)lane * 96u, y); else st_global<12>(S.base + i * 96, y);
+      }
       break;
   }
 }
 
-// One site through the field's whole program.
-__device__ __forceinline__ void run_program(const BField& F, const SiteSrc& src, unsigned char* out, int lane) {
+// One site through the field's whole program (the generic interpreter).
+template <int MC>
+__device__ __forceinline__ void run_program_generic(const BField& F, const SiteSrc& src, unsigned char* out,
+                                                    int lane) {
   const int ns = F.nsteps;
+  Rec<MC> prev;
+  int prev_reg = -1;
   for (int k = 0; k < ns; k++) {
     const BStep S = F.st[k];  // uniform across the warp
-    Rec xa, xb, y;
-    fetch(xa, S.a, S.kind_a, F, src);
-    if (S.op == BOP_LMULT) fetch(xb, S.b, S.kind_b, F, src);
-    if (S.eqop == PEQ || S.eqop == MEQ) fetch(y, S.load_stream >= 0 ? S.load_stream : S.dst, S.kind_r, F, src);
+    Rec<MC> xa, xb, y;
+    fetch(xa, S.a, S.kind_a, F, src, prev, prev_reg);
+    if (S.op == BOP_LMULT) fetch(xb, S.b, S.kind_b, F, src, prev, prev_reg);
+    if (S.eqop == PEQ || S.eqop == MEQ)
+      fetch(y, S.load_stream >= 0 ? S.load_stream : S.dst, S.kind_r, F, src, prev, prev_reg);
     exec_step(S, xa, xb, y);
-    if (k + 1 < ns) set_reg(src, S.dst - kReg0, S.kind_r, y);  // the last step's register is never read
+    if (S.spill) set_reg(src, S.dst - kReg0, S.kind_r, y);  // a later, non-adjacent step reads it
     if (S.store >= 0) put(F.s[S.store], y, out, lane, src.i);
+    copy_rec(prev, y);
+    prev_reg = S.dst;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Compiled program shapes.  A shape fixes each step's operation, operand
+// kinds and adjoints at compile time; a plan whose fields all share one
+// shape of the catalogue below runs a kernel instantiated for it: the steps
+// are unrolled, every record has its exact length and no step is decoded.
+// Operand streams and registers, eqops, mu / sign and the scalar stay
+// run-time values of the field's descriptor, and the per-site arithmetic is
+// the same as the interpreter's (bit-identical results).
+// where a step's operand comes from (classified by the planner)
+enum SrcKind : int { SRC_CONTIG = 0, SRC_GATHER = 1, SRC_INOUT = 2, SRC_PREV = 3, SRC_REG = 4, SRC_NONE = 5 };
+template <int OP, int KA, int KB, int ADJA, int ADJB, int SA, int SB, int EQOP = -1>  // EQOP -1: run time
+struct StepShape {
+  static constexpr int op = OP, ka = KA, kb = KB, adja = ADJA, adjb = ADJB, sa = SA, sb = SB, eqop = EQOP;
+  static constexpr int kr = OP == BOP_LMULT ? KB : OP == BOP_SPPROJ ? BK_H : OP == BOP_SPRECON ? BK_D : KA;
+};
+template <class... S>
+struct Shape {
+  static constexpr int nsteps = sizeof...(S);
+};
+struct GenericShape {};
+
+// r = u * u2[nbr], w = r * v                          (config 4)
+using ShapeConfig4 = Shape<StepShape<BOP_LMULT, BK_M, BK_M, 0, 0, SRC_CONTIG, SRC_GATHER, EQ>,
+                           StepShape<BOP_LMULT, BK_M, BK_V, 0, 0, SRC_PREV, SRC_CONTIG, EQ>>;
+// out (eqop) sprecon(U spproj(D[nbr]))                 (one Wilson hop direction)
+using ShapeHop = Shape<StepShape<BOP_SPPROJ, BK_D, BK_D, 0, 0, SRC_GATHER, SRC_NONE>,
+                       StepShape<BOP_LMULT, BK_M, BK_H, 0, 0, SRC_CONTIG, SRC_PREV>,
+                       StepShape<BOP_SPRECON, BK_H, BK_H, 0, 0, SRC_PREV, SRC_NONE>>;
+// y (eqop) r x, w = U^+ y
+using ShapeAxpyMaD = Shape<StepShape<BOP_RTIMES, BK_D, BK_D, 0, 0, SRC_CONTIG, SRC_NONE>,
+                           StepShape<BOP_LMULT, BK_M, BK_D, 1, 0, SRC_CONTIG, SRC_PREV>>;
+// R = U U2^+, Q (eqop) R
+using ShapeMMaCopy = Shape<StepShape<BOP_LMULT, BK_M, BK_M, 0, 1, SRC_CONTIG, SRC_CONTIG>,
+                           StepShape<BOP_COPY, BK_M, BK_M, 0, 0, SRC_PREV, SRC_NONE>>;
+enum ShapeId : int { SH_GENERIC = 0, SH_CONFIG4 = 1, SH_HOP = 2, SH_AXPY_MAD = 3, SH_MMA_COPY = 4 };
+
+template <class SS, int MC>
+__device__ __forceinline__ void exec_shaped(const BStep& S, const Rec<MC>& xa, const Rec<MC>& xb, Rec<MC>& y) {
+  const bool load = (S.eqop == PEQ || S.eqop == MEQ);
+  constexpr int NR = kncplx(SS::kr);
+  if constexpr (SS::op == BOP_LMULT) {
+    constexpr int NCOL = SS::kb == BK_V ? 1 : SS::kb == BK_H ? 2 : SS::kb == BK_D ? 4 : 3;
+    lmult_site<float, 3, NCOL, SS::adja != 0, SS::adjb != 0>(S.eqop, load, xa, xb, y);
+  } else if constexpr (SS::op == BOP_SPPROJ) {
+    mu_sign_dispatch<SpprojOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y);
+  } else if constexpr (SS::op == BOP_SPRECON) {
+    mu_sign_dispatch<SpreconOp<float, 3>::Body>(S.mu, S.sign, S.eqop, xa, y);
+  } else if constexpr (SS::op == BOP_RTIMES) {
+    rtimes_n<NR>(S.eqop, S.r, xa, y);
+  } else {
+    copy_n<NR>(S.eqop, xa, y);
+  }
+}
+
+template <int N, int MC>
+__device__ __forceinline__ void put_n(const BStream& S, const Rec<MC>& y, unsigned char* out, int lane, long long i) {
+  if (out)
+    st_smem<N>(out + S.out_off + (unsigned)lane * (N * 8), y);
+  else
+    st_global<N>(S.base + i * (N * 8), y);
+}
+
+// operand `ref` of compile-time source SRC and length N
+template <int SRC, int N, int MC>
+__device__ __forceinline__ void fetch_src(Rec<MC>& x, int ref, const BField& F, const SiteSrc& src,
+                                          const Rec<MC>& prev) {
+  if constexpr (SRC == SRC_PREV) {
+    copy_rec(x, prev);
+  } else if constexpr (SRC == SRC_REG) {
+    reg_load<N>(x, src, ref - kReg0);
+  } else if constexpr (SRC == SRC_GATHER) {
+    const BStream& S = F.s[ref];
+    long long j = src.stage ? reinterpret_cast<const int*>(src.stage + S.stage_off)[src.t] : S.idx[src.i];
+    if (S.nsrc > 0 && (j < 0 || j >= S.nsrc)) {
+      raise_dev_error(src.err, QLA_DEVERR_BAD_INDEX);
+      zero_rec(x);
+    } else {
+      ld_global<N>(x, S.base + j * (long long)(N * 8));
+    }
+  } else {  // SRC_CONTIG, SRC_INOUT
+    const BStream& S = F.s[ref];
+    if (src.stage)
+      ld_smem<N>(x, src.stage + S.stage_off + (unsigned)src.t * (N * 8));
+    else if constexpr (SRC == SRC_INOUT)
+      ld_global_rw<N>(x, S.base + src.i * (N * 8));
+    else
+      ld_global<N>(x, S.base + src.i * (N * 8));
+  }
+}
+
+template <int MC, int K, class SS, class... Rest>
+__device__ __forceinline__ void run_shaped(const BField& F, const SiteSrc& src, unsigned char* out, int lane,
+                                           Rec<MC>& prev, int prev_reg) {
+  BStep S = F.st[K];
+  if constexpr (SS::eqop >= 0) S.eqop = SS::eqop;  // a compiled eqop (the planner matched it)
+  constexpr int NA = kncplx(SS::ka), NB = kncplx(SS::kb), NR = kncplx(SS::kr);
+  Rec<MC> xa, xb, y;
+  fetch_src<SS::sa, NA>(xa, S.a, F, src, prev);
+  if constexpr (SS::op == BOP_LMULT) fetch_src<SS::sb, NB>(xb, S.b, F, src, prev);
+  if (S.eqop == PEQ || S.eqop == MEQ) fetch_n<NR>(y, S.load_stream >= 0 ? S.load_stream : S.dst, F, src, prev, prev_reg);
+  exec_shaped<SS>(S, xa, xb, y);
+  if (S.spill) reg_store<NR>(src, S.dst - kReg0, y);
+  if (S.store >= 0) put_n<NR>(F.s[S.store], y, out, lane, src.i);
+  if constexpr (sizeof...(Rest) > 0) {
+    copy_rec(prev, y);
+    run_shaped<MC, K + 1, Rest...>(F, src, out, lane, prev, S.dst);
+  }
+}
+template <int MC, class... SS>
+__device__ __forceinline__ void run_shape(Shape<SS...>, const BField& F, const SiteSrc& src, unsigned char* out,
+                                          int lane) {
+  Rec<MC> prev;
+  run_shaped<MC, 0, SS...>(F, src, out, lane, prev, -1);
+}
+
+template <int MC, class SH>
+__device__ __forceinline__ void run_program(const BField& F, const SiteSrc& src, unsigned char* out, int lane) {
+  if constexpr (std::is_same<SH, GenericShape>::value)
+    run_program_generic<MC>(F, src, out, lane);
+  else
+    run_shape<MC>(SH{}, F, src, out, lane);
 }
 
 // Copy of field f's descriptor in this warp's shared slot (all lanes take
@@ -361,9 +540,20 @@ __device__ __forceinline__ const BField& cached_field_1(const BatchParams& p, in
 }
 
 // Dynamic smem: [full[8], empty[8] | abort | tile0 table (8 KB) | S stages |
-//               NW x 2 output slices | step registers: 2 x 12 complex x T |
-//               (NW + 1) field descriptors]
-__global__ void __launch_bounds__(288) batch_program_kernel(const BatchParams p) {
+//               NW output slices | step registers (only when some
+//               program spills one): 2 x 12 complex x T | (NW + 1) field
+//               descriptors]
+// 128 consumer threads (or 64) and one producer warp.  Blocks per SM: four
+// for compiled V / H / M shapes (<= 96 registers), three for the V / H / M
+// interpreter, two for DiracFermion programs.
+constexpr int kBatchThreadsMax = 160;
+template <int MC, class SH>
+constexpr int batch_min_blocks() {
+  return MC == 9 ? (std::is_same<SH, GenericShape>::value ? 3 : 4) : 2;
+}
+template <int MC, class SH>
+__global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) batch_program_kernel(
+    const BatchParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = p.stages;
   const int NW = (blockDim.x >> 5) - 1;
@@ -374,11 +564,11 @@ __global__ void __launch_bounds__(288) batch_program_kernel(const BatchParams p)
   long long* tile0 = reinterpret_cast<long long*>(smem + 256);
   unsigned char* stages = smem + 256 + 8 * kMaxFields;
   unsigned char* outbuf = stages + (size_t)S * p.stage_bytes;
-  unsigned char* regs = outbuf + (size_t)NW * 2 * p.out_slice_bytes;  // 2 x 12 complex per thread
+  unsigned char* regs = outbuf + (size_t)NW * p.out_slice_bytes;  // 2 x 12 complex per thread, if needed
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long my =
       ((long long)blockIdx.x < p.ntiles) ? (p.ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1 : 0;
-  uint4* desc = reinterpret_cast<uint4*>(regs + (size_t)2 * 12 * 8 * T) + (size_t)warp * kDescWords;
+  uint4* desc = reinterpret_cast<uint4*>(regs + (p.spill_regs ? (size_t)2 * 12 * 8 * T : 0)) + (size_t)warp * kDescWords;
   int cached = -1;
 
   for (int f = tid; f < p.nfields; f += blockDim.x) tile0[f] = p.fields[f].tile0;
@@ -432,7 +622,7 @@ __global__ void __launch_bounds__(288) batch_program_kernel(const BatchParams p)
   } else {
     // ------------------------------------------------------------ consumers
     const uint64_t pol = policy_evict_first();
-    unsigned char* myout = outbuf + (size_t)warp * 2 * p.out_slice_bytes;
+    unsigned char* myout = outbuf + (size_t)warp * p.out_slice_bytes;
     int s = 0;
     uint32_t par = 0;
     for (long long k = 0; k < my; k++) {
@@ -448,16 +638,16 @@ __global__ void __launch_bounds__(288) batch_program_kernel(const BatchParams p)
       // staged: a full tile of a 16-B aligned field, in the stage; else the
       // same program with plain loads and stores (partial / unaligned tiles)
       const bool staged = !F.direct && site0 + T <= F.n;
-      unsigned char* ob = myout + (size_t)(k & 1) * p.out_slice_bytes;
+      unsigned char* ob = myout;
       if (staged) {
-        if (lane == 0) bulk_wait_read<1>();  // slice (k&1) no longer read by this warp's store k-2
+        if (lane == 0) bulk_wait_read<0>();  // the slice is no longer read by this warp's previous store
         __syncwarp();
       } else {
         release_stage(&empty[s], lane);  // this warp is done with the stage
       }
       if (staged || i < F.n)  // one call site: the program is inlined once
-        run_program(F, SiteSrc{staged ? stages + (size_t)s * p.stage_bytes : nullptr, t, i, p.err, regs, T},
-                    staged ? ob : nullptr, lane);
+        run_program<MC, SH>(F, SiteSrc{staged ? stages + (size_t)s * p.stage_bytes : nullptr, t, i, p.err, regs, T},
+                            staged ? ob : nullptr, lane);
       if (staged) {
         // every lane orders its reads of the stage and its writes of the
         // slice before the async proxy: the slice's bulk stores below, and
@@ -514,7 +704,7 @@ static bool aligned(const void* p, unsigned a) { return (reinterpret_cast<uintpt
 // for a tile of T sites, output slice offsets).  Returns false with the
 // sticky error set when the program is malformed.
 static bool build_field(const char* who, int f, const qlagpu_F3_batch_program& q, int T, BField& b,
-                        unsigned& stage_bytes, unsigned& out_slice_bytes) {
+                        unsigned& stage_bytes, unsigned& out_slice_bytes, bool& spills, bool& uses_d) {
   std::memset(&b, 0, sizeof(b));
   if (q.n < 0 || q.nstreams < 0 || q.nstreams > kMaxStreams || q.nsteps < 1 || q.nsteps > kMaxSteps)
     return plan_error(who, f, -1, "need n >= 0, 0..8 streams and 1..8 steps");
@@ -629,9 +819,77 @@ static bool build_field(const char* who, int f, const qlagpu_F3_batch_program& q
   }
   for (int j = 0; j < q.nstreams; j++)
     if (q.stream[j].role != BR_IN && !stored[j]) return plan_error(who, f, -1, "an output stream is never stored");
+  // register liveness: a register read by a step other than the one right
+  // after its writer is also kept in shared memory (the writer spills it)
+  for (int k = 0; k < q.nsteps; k++) {
+    const BStep& d = b.st[k];
+    const int reads[3] = {d.a, d.op == BOP_LMULT ? d.b : -1,
+                          ((d.eqop == PEQ || d.eqop == MEQ) && d.load_stream < 0) ? d.dst : -1};
+    for (int r : reads) {
+      if (r != kReg0 && r != kReg1) continue;
+      int w = k - 1;
+      while (w >= 0 && b.st[w].dst != r) w--;
+      if (w >= 0 && w != k - 1) {
+        b.st[w].spill = 1;
+        spills = true;
+      }
+    }
+  }
+  // operand sources, for matching a compiled shape
+  for (int k = 0; k < q.nsteps; k++) {
+    BStep& d = b.st[k];
+    auto src_of = [&](int ref) {
+      if (ref == kReg0 || ref == kReg1) return (k > 0 && b.st[k - 1].dst == ref) ? (int)SRC_PREV : (int)SRC_REG;
+      if (q.stream[ref].role == BR_INOUT) return (int)SRC_INOUT;
+      return q.stream[ref].index ? (int)SRC_GATHER : (int)SRC_CONTIG;
+    };
+    d.src_a = src_of(d.a);
+    d.src_b = d.op == BOP_LMULT ? src_of(d.b) : (int)SRC_NONE;
+  }
+  for (int j = 0; j < q.nstreams; j++) uses_d = uses_d || q.stream[j].kind == BK_D;
+  for (int k = 0; k < q.nsteps; k++)
+    uses_d = uses_d || b.st[k].kind_r == BK_D || b.st[k].kind_a == BK_D || b.st[k].kind_b == BK_D;
   if (off > stage_bytes) stage_bytes = off;
   if (oo > out_slice_bytes) out_slice_bytes = oo;
   return true;
+}
+
+// the catalogue shape that every field's program has, or SH_GENERIC
+template <class... SS>
+static bool has_shape(const BField& b, Shape<SS...>) {
+  constexpr int ops[] = {SS::op...}, ka[] = {SS::ka...}, kb[] = {SS::kb...}, aa[] = {SS::adja...},
+                ab[] = {SS::adjb...}, sa[] = {SS::sa...}, sb[] = {SS::sb...}, eq[] = {SS::eqop...};
+  if (b.nsteps != (int)sizeof...(SS)) return false;
+  for (int k = 0; k < b.nsteps; k++) {
+    const BStep& d = b.st[k];
+    if (d.op != ops[k] || d.kind_a != ka[k] || (d.op == BOP_LMULT && d.kind_b != kb[k]) || d.adja != aa[k] ||
+        d.adjb != ab[k] || d.src_a != sa[k] || d.src_b != sb[k] || (eq[k] >= 0 && d.eqop != eq[k]))
+      return false;
+  }
+  return true;
+}
+static int common_shape(const BField* h, int nfields) {
+  auto all = [&](auto shape) {
+    for (int f = 0; f < nfields; f++)
+      if (!has_shape(h[f], shape)) return false;
+    return true;
+  };
+  if (all(ShapeConfig4{})) return SH_CONFIG4;
+  if (all(ShapeHop{})) return SH_HOP;
+  if (all(ShapeAxpyMaD{})) return SH_AXPY_MAD;
+  if (all(ShapeMMaCopy{})) return SH_MMA_COPY;
+  return SH_GENERIC;
+}
+static const void* batch_kernel_for(const BatchPlan* plan) {
+  switch (plan->shape) {
+    case SH_CONFIG4: return reinterpret_cast<const void*>(&batch_program_kernel<9, ShapeConfig4>);
+    case SH_HOP: return reinterpret_cast<const void*>(&batch_program_kernel<12, ShapeHop>);
+    case SH_AXPY_MAD: return reinterpret_cast<const void*>(&batch_program_kernel<12, ShapeAxpyMaD>);
+    case SH_MMA_COPY: return reinterpret_cast<const void*>(&batch_program_kernel<9, ShapeMMaCopy>);
+    default:
+      return plan->mc == 12 ? reinterpret_cast<const void*>(&batch_program_kernel<12, GenericShape>)
+                            : reinterpret_cast<const void*>(&batch_program_kernel<9, GenericShape>);
+  }
 }
 
 static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fields, int nfields) {
@@ -639,16 +897,17 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
     set_error(QLAGPU_ERR_ARG, who, "need 1 <= nfields <= 1024 and a field table");
     return nullptr;
   }
-  int t = 128, st = 3;
-  if (!tuned_shape("F3_batch_program", &t, &st)) {
-    t = 128;
-    st = 3;
+  int t = 128, st = 2;
+  if (!tuned_shape("F3_batch_program", &t, &st) || (t != 64 && t != 128)) {
+    t = 128;  // the kernel's launch bounds allow 64 or 128 sites per tile
+    st = 2;
   }
   std::vector<BField> h((size_t)nfields);
   unsigned stage_bytes = 0, out_slice = 0;
+  bool spills = false, uses_d = false;
   long long tiles = 0;
   for (int f = 0; f < nfields; f++) {
-    if (!build_field(who, f, fields[f], t, h[(size_t)f], stage_bytes, out_slice)) return nullptr;
+    if (!build_field(who, f, fields[f], t, h[(size_t)f], stage_bytes, out_slice, spills, uses_d)) return nullptr;
     h[(size_t)f].tile0 = tiles;
     tiles += (fields[f].n + t - 1) / t;
   }
@@ -656,8 +915,8 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
   if (stage_bytes == 0) stage_bytes = 128;
   out_slice = (out_slice + 127u) & ~127u;
   auto smem_for = [&](int stages) {
-    return 256 + 8 * (size_t)kMaxFields + (size_t)stages * stage_bytes + 2 * (size_t)(t / 32) * out_slice +
-           2 * 12 * 8 * (size_t)t + 16 * (size_t)kDescWords * (t / 32 + 1);
+    return 256 + 8 * (size_t)kMaxFields + (size_t)stages * stage_bytes + (size_t)(t / 32) * out_slice +
+           (spills ? 2 * 12 * 8 * (size_t)t : 0) + 16 * (size_t)kDescWords * (t / 32 + 1);
   };
   size_t smem = smem_for(st);
   while (smem > 225u * 1024u && st > 2) smem = smem_for(--st);  // shed stages before giving up
@@ -673,6 +932,9 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
   plan->stages = st;
   plan->stage_bytes = stage_bytes;
   plan->out_slice_bytes = out_slice;
+  plan->spill_regs = spills ? 1 : 0;
+  plan->mc = uses_d ? 12 : 9;
+  plan->shape = common_shape(h.data(), nfields);
   plan->smem = smem;
   if (cudaMalloc(&plan->dfields, sizeof(BField) * (size_t)nfields) != cudaSuccess ||
       cudaMemcpy(plan->dfields, h.data(), sizeof(BField) * (size_t)nfields, cudaMemcpyHostToDevice) !=
@@ -683,7 +945,7 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
     delete plan;
     return nullptr;
   }
-  const void* fn = reinterpret_cast<const void*>(&batch_program_kernel);
+  const void* fn = batch_kernel_for(plan);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem);
   int nb = 1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, t + 32, plan->smem) != cudaSuccess || nb < 1) nb = 1;
@@ -748,9 +1010,11 @@ extern "C" QLAB_EXPORT int qlagpu_batch_run(void* handle) {
   p.stages = plan->stages;
   p.stage_bytes = plan->stage_bytes;
   p.out_slice_bytes = plan->out_slice_bytes;
+  p.spill_regs = plan->spill_regs;
   p.err = device_error_word();
   void* args[] = {&p};
-  if (cudaLaunchKernel(reinterpret_cast<const void*>(&batch_program_kernel), dim3((unsigned)plan->grid),
+  const void* fn = batch_kernel_for(plan);
+  if (cudaLaunchKernel(fn, dim3((unsigned)plan->grid),
                        dim3((unsigned)plan->threads + 32u), args, plan->smem, current_stream()) != cudaSuccess) {
     check_launch("qlagpu_batch_run");
     return QLAGPU_ERR_LAUNCH;

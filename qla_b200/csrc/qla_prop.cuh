@@ -489,6 +489,137 @@ __global__ void __launch_bounds__(12 * SPB) prop_pp_rows_kernel(const PropParams
   }
 }
 
+// 16-B asynchronous global -> shared copies (sm_80+ cp.async, L1 bypassed)
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst_smem)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// P * P (F3) for contiguous, 16-B aligned operands without a gang index:
+// persistent blocks of 12 * SPB threads, one thread per (site, output row),
+// looping over tiles of SPB sites with software pipelining.  Before computing
+// tile t every thread starts the copies of tile t+1: its share of the first
+// operand's records with cp.async into the other shared buffer, and its share
+// of the second operand's records into registers; after computing it writes
+// those registers to the other buffer in operand order (P, or P^+ read
+// transposed) as separate real and imaginary planes, so that two output
+// columns share one FP32x2 register (cmac_x2: per-lane rounding as
+// cmac<CA, CB>).  One block barrier per tile hands the buffers over.  Every
+// output element is accumulated as the reference does: bit-identical.
+template <bool CA, bool CB, int SPB>
+__global__ void __launch_bounds__(12 * SPB) prop_pp_pipe_kernel(const PropParams p, long long ntiles) {
+  extern __shared__ __align__(16) unsigned char psm[];
+  constexpr int NT = 12 * SPB;          // threads
+  constexpr int WPS = 72;               // 16-B words per record
+  constexpr int WPT = SPB * WPS / NT;   // words per thread per tile (6)
+  constexpr int BUF = SPB * 1152;       // bytes of one tile of records
+  static_assert(SPB * WPS % NT == 0, "tile words must split evenly");
+  unsigned char* bbuf = psm;            // [2][BUF]: second operand, re / im planes per site
+  unsigned char* abuf = psm + 2 * BUF;  // [2][BUF]: first operand, records as stored
+  const int tid = threadIdx.x, ls = tid / 12, row = tid - ls * 12;
+  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
+  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+  const uint4* Ag = static_cast<const uint4*>(p.a.base);
+  const uint4* Bg = static_cast<const uint4*>(p.b.base);
+  Cx<float>* Og = static_cast<Cx<float>*>(p.out);
+  uint4 nb[WPT];
+  // start the copies of tile t: first operand -> abuf[b] (asynchronous),
+  // second operand -> registers nb
+  auto fetch = [&](long long t, int b) {
+    const long long s0 = t * SPB;
+    const long long words = ((p.n - s0) < SPB ? (p.n - s0) : SPB) * WPS;
+    uint4* adst = reinterpret_cast<uint4*>(abuf + (size_t)b * BUF);
+#pragma unroll
+    for (int i = 0; i < WPT; i++) {
+      const int w = tid + i * NT;
+      if (w < words) {
+        cp_async16(adst + w, Ag + s0 * WPS + w);
+        nb[i] = __ldg(Bg + s0 * WPS + w);
+      }
+    }
+    cp_async_commit();
+  };
+  // registers nb -> bbuf[b], element (kk, jj) at kk * 12 + jj of each plane
+  auto stash = [&](int b) {
+    float* base = reinterpret_cast<float*>(bbuf + (size_t)b * BUF);
+#pragma unroll
+    for (int i = 0; i < WPT; i++) {
+      const int w = tid + i * NT, site = w / WPS, e0 = (w - site * WPS) * 2;
+      const uint4 v = nb[i];
+      float* re = base + site * 288;
+      float* im = re + 144;
+      const int o0 = CB ? (e0 % 12) * 12 + e0 / 12 : e0;
+      const int o1 = CB ? ((e0 + 1) % 12) * 12 + (e0 + 1) / 12 : e0 + 1;
+      re[o0] = __uint_as_float(v.x);
+      im[o0] = __uint_as_float(v.y);
+      re[o1] = __uint_as_float(v.z);
+      im[o1] = __uint_as_float(v.w);
+    }
+  };
+  long long t = blockIdx.x;
+  if (t >= ntiles) return;
+  fetch(t, 0);
+  stash(0);
+  cp_async_wait_all();
+  __syncthreads();
+  for (int b = 0; t < ntiles; t += gridDim.x, b ^= 1) {
+    const long long tn = t + gridDim.x;
+    if (tn < ntiles) fetch(tn, b ^ 1);  // in flight during the arithmetic below
+    const long long k = t * SPB + ls;
+    if (k < p.n) {
+      Cx<float>* out = Og + k * 144 + row * 12;
+      const Cx<float>* A = reinterpret_cast<const Cx<float>*>(abuf + (size_t)b * BUF) + ls * 144;
+      Cx<float> a[12];
+      if constexpr (!CA) {
+#pragma unroll
+        for (int kk = 0; kk < 12; kk += 2) {
+          Cx<float> t2[2];
+          ld2_out<float>(t2, A + row * 12 + kk, true);
+          a[kk] = t2[0];
+          a[kk + 1] = t2[1];
+        }
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < 12; kk++) a[kk] = A[kk * 12 + row];  // P^+[row][kk] = conj P[kk][row]
+      }
+      const float* re = reinterpret_cast<const float*>(bbuf + (size_t)b * BUF) + ls * 288;
+      const float* im = re + 144;
+      float2 xr[6], xi[6];  // lanes: output columns 2c, 2c + 1
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        if (load) {
+          Cx<float> t2[2];
+          ld2_out<float>(t2, out + 2 * c, true);
+          xr[c] = make_float2(t2[0].re, t2[1].re);
+          xi[c] = make_float2(t2[0].im, t2[1].im);
+        } else {
+          xr[c] = make_float2(0.f, 0.f);
+          xi[c] = make_float2(0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < 12; kk++)
+#pragma unroll
+        for (int c = 0; c < 6; c += 2) {  // 16-B loads: two column pairs each
+          const float4 r4 = *reinterpret_cast<const float4*>(re + kk * 12 + 2 * c);
+          const float4 i4 = *reinterpret_cast<const float4*>(im + kk * 12 + 2 * c);
+          cmac_x2<CA, CB>(xr[c], xi[c], minus, a[kk], make_float2(r4.x, r4.y), make_float2(i4.x, i4.y), p.negzero);
+          cmac_x2<CA, CB>(xr[c + 1], xi[c + 1], minus, a[kk], make_float2(r4.z, r4.w), make_float2(i4.z, i4.w),
+                          p.negzero);
+        }
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        const Cx<float> t2[2] = {Cx<float>{xr[c].x, xi[c].x}, Cx<float>{xr[c].y, xi[c].y}};
+        st2<float>(out + 2 * c, t2, true);
+      }
+    }
+    if (tn < ntiles) stash(b ^ 1);  // the other buffers were last read before the previous barrier
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
 // the spin trace: one thread per output element (9 per site)
 template <typename R>
 __global__ void __launch_bounds__(256) prop_trace_kernel(const PropParams p) {
@@ -550,13 +681,30 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
     prop_mp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
   else if constexpr (KIND == PK_PM)
     prop_pm_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
-  else if (gang == nullptr && a.mode == OM_CONTIG && b.mode == OM_CONTIG && p.vec_a && p.vec_b && p.vec_out) {
-    constexpr int SPB = sizeof(R) == 4 ? 16 : 8;  // sites per block
-    const size_t smem = (size_t)SPB * 144 * sizeof(Cx<R>) * (sizeof(R) == 4 ? 2 : 1);
-    const long long blocks = ((long long)n + SPB - 1) / SPB;
-    prop_pp_rows_kernel<R, CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p);
-  } else {
-    prop_pp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+  else {
+    const bool contig = gang == nullptr && a.mode == OM_CONTIG && b.mode == OM_CONTIG && p.vec_a && p.vec_b &&
+                        p.vec_out;
+    if (!contig) {
+      prop_pp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+    } else if constexpr (sizeof(R) == 8) {
+      constexpr int SPB = 8;  // D3: one tile per block (the pipelined form's prefetch registers would not fit)
+      const size_t smem = (size_t)SPB * 144 * sizeof(Cx<R>);
+      const long long blocks = ((long long)n + SPB - 1) / SPB;
+      prop_pp_rows_kernel<R, CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p);
+    } else {
+      // F3: 8 sites per tile, 96 threads and 36 KB per block: at ~128 registers
+      // five blocks (15 warps) share an SM
+      constexpr int SPB = 8;
+      const size_t smem = 4 * (size_t)SPB * 1152;  // two buffers of each operand
+      const long long ntiles = ((long long)n + SPB - 1) / SPB;
+      const void* fn = reinterpret_cast<const void*>(&prop_pp_pipe_kernel<CA, CB, SPB>);
+      int nb = 1;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 12 * SPB, smem) != cudaSuccess || nb < 1) nb = 1;
+      cudaGetLastError();
+      long long blocks = (long long)nb * device_sm_count();
+      if (blocks > ntiles) blocks = ntiles;
+      prop_pp_pipe_kernel<CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p, ntiles);
+    }
   }
   check_launch(kid);
 }
