@@ -73,6 +73,7 @@ struct alignas(16) BField {
   long long n, tile0;
   unsigned tx_bytes;  // bytes the producer copies per full tile
   int direct;         // some base not 16-B aligned: every tile by plain loads
+  int shape;          // ShapeId of this field's program (SH_GENERIC: none of the catalogue)
 };
 
 struct BatchParams {
@@ -114,6 +115,7 @@ __device__ __forceinline__ int find_field(const long long* tile0, int nf, long l
 // which keeps the kernel's registers down for V / H / M programs.
 template <int MC>
 using Rec = Cx<float>[MC];
+
 
 // --- record movement with a compile-time length N (complex numbers)
 template <int N, int MC>
@@ -180,6 +182,11 @@ template <int MC>
 __device__ __forceinline__ void copy_rec(Rec<MC>& x, const Rec<MC>& y) {
 #pragma unroll
   for (int e = 0; e < MC; e++) x[e] = y[e];
+}
+template <int N, int MC>  // the first N complex numbers only
+__device__ __forceinline__ void copy_rec_n(Rec<MC>& x, const Rec<MC>& y) {
+#pragma unroll
+  for (int e = 0; e < N; e++) x[e] = y[e];
 }
 
 // Where one site's operands live: the staged tile (stage != nullptr, lane
@@ -425,7 +432,7 @@ using ShapeAxpyMaD = Shape<StepShape<BOP_RTIMES, BK_D, BK_D, 0, 0, SRC_CONTIG, S
 // R = U U2^+, Q (eqop) R
 using ShapeMMaCopy = Shape<StepShape<BOP_LMULT, BK_M, BK_M, 0, 1, SRC_CONTIG, SRC_CONTIG>,
                            StepShape<BOP_COPY, BK_M, BK_M, 0, 0, SRC_PREV, SRC_NONE>>;
-enum ShapeId : int { SH_GENERIC = 0, SH_CONFIG4 = 1, SH_HOP = 2, SH_AXPY_MAD = 3, SH_MMA_COPY = 4 };
+enum ShapeId : int { SH_GENERIC = 0, SH_CONFIG4 = 1, SH_HOP = 2, SH_AXPY_MAD = 3, SH_MMA_COPY = 4, SH_MULTI = 5 };
 
 template <class SS, int MC>
 __device__ __forceinline__ void exec_shaped(const BStep& S, const Rec<MC>& xa, const Rec<MC>& xb, Rec<MC>& y) {
@@ -458,7 +465,7 @@ template <int SRC, int N, int MC>
 __device__ __forceinline__ void fetch_src(Rec<MC>& x, int ref, const BField& F, const SiteSrc& src,
                                           const Rec<MC>& prev) {
   if constexpr (SRC == SRC_PREV) {
-    copy_rec(x, prev);
+    copy_rec_n<N>(x, prev);
   } else if constexpr (SRC == SRC_REG) {
     reg_load<N>(x, src, ref - kReg0);
   } else if constexpr (SRC == SRC_GATHER) {
@@ -495,7 +502,7 @@ __device__ __forceinline__ void run_shaped(const BField& F, const SiteSrc& src, 
   if (S.spill) reg_store<NR>(src, S.dst - kReg0, y);
   if (S.store >= 0) put_n<NR>(F.s[S.store], y, out, lane, src.i);
   if constexpr (sizeof...(Rest) > 0) {
-    copy_rec(prev, y);
+    copy_rec_n<NR>(prev, y);
     run_shaped<MC, K + 1, Rest...>(F, src, out, lane, prev, S.dst);
   }
 }
@@ -506,12 +513,28 @@ __device__ __forceinline__ void run_shape(Shape<SS...>, const BField& F, const S
   run_shaped<MC, 0, SS...>(F, src, out, lane, prev, -1);
 }
 
+// A plan whose fields all have catalogue shapes, but not one shape, runs the
+// multi-shape kernel: each field's compiled path, chosen per tile (uniform).
+// Other plans run the interpreter.
+struct MultiShape {};
 template <int MC, class SH>
 __device__ __forceinline__ void run_program(const BField& F, const SiteSrc& src, unsigned char* out, int lane) {
-  if constexpr (std::is_same<SH, GenericShape>::value)
+  if constexpr (std::is_same<SH, GenericShape>::value) {
     run_program_generic<MC>(F, src, out, lane);
-  else
+  } else if constexpr (std::is_same<SH, MultiShape>::value) {
+    switch (F.shape) {
+      case SH_CONFIG4: run_shape<MC>(ShapeConfig4{}, F, src, out, lane); break;
+      case SH_MMA_COPY: run_shape<MC>(ShapeMMaCopy{}, F, src, out, lane); break;
+      case SH_HOP:
+        if constexpr (MC >= 12) run_shape<MC>(ShapeHop{}, F, src, out, lane);
+        break;
+      default:
+        if constexpr (MC >= 12) run_shape<MC>(ShapeAxpyMaD{}, F, src, out, lane);
+        break;
+    }
+  } else {
     run_shape<MC>(SH{}, F, src, out, lane);
+  }
 }
 
 // Copy of field f's descriptor in this warp's shared slot (all lanes take
@@ -543,13 +566,16 @@ __device__ __forceinline__ const BField& cached_field_1(const BatchParams& p, in
 //               NW output slices | step registers (only when some
 //               program spills one): 2 x 12 complex x T | (NW + 1) field
 //               descriptors]
-// 128 consumer threads (or 64) and one producer warp.  Blocks per SM: four
-// for compiled V / H / M shapes (<= 96 registers), three for the V / H / M
-// interpreter, two for DiracFermion programs.
+// 128 consumer threads (or 64) and one producer warp.  Blocks per SM (the
+// register budget each instance compiles to without spilling): a compiled
+// shape four (V / H / M records, <= 96 registers) or three (DiracFermions,
+// <= 128); the interpreter and the multi-shape kernel three (V / H / M) or
+// two (DiracFermions).
 constexpr int kBatchThreadsMax = 160;
 template <int MC, class SH>
 constexpr int batch_min_blocks() {
-  return MC == 9 ? (std::is_same<SH, GenericShape>::value ? 3 : 4) : 2;
+  constexpr bool compiled = !std::is_same<SH, GenericShape>::value && !std::is_same<SH, MultiShape>::value;
+  return MC == 9 ? (compiled ? 4 : 3) : (compiled ? 3 : 2);
 }
 template <int MC, class SH>
 __global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) batch_program_kernel(
@@ -868,17 +894,25 @@ static bool has_shape(const BField& b, Shape<SS...>) {
   }
   return true;
 }
-static int common_shape(const BField* h, int nfields) {
-  auto all = [&](auto shape) {
-    for (int f = 0; f < nfields; f++)
-      if (!has_shape(h[f], shape)) return false;
-    return true;
-  };
-  if (all(ShapeConfig4{})) return SH_CONFIG4;
-  if (all(ShapeHop{})) return SH_HOP;
-  if (all(ShapeAxpyMaD{})) return SH_AXPY_MAD;
-  if (all(ShapeMMaCopy{})) return SH_MMA_COPY;
+static int shape_of(const BField& b) {
+  if (has_shape(b, ShapeConfig4{})) return SH_CONFIG4;
+  if (has_shape(b, ShapeHop{})) return SH_HOP;
+  if (has_shape(b, ShapeAxpyMaD{})) return SH_AXPY_MAD;
+  if (has_shape(b, ShapeMMaCopy{})) return SH_MMA_COPY;
   return SH_GENERIC;
+}
+// sets each field's shape; returns the shape all fields share, SH_MULTI when
+// every field has a catalogue shape but not the same one, else SH_GENERIC
+static int common_shape(BField* h, int nfields) {
+  int common = -1;
+  bool all_known = true;
+  for (int f = 0; f < nfields; f++) {
+    h[f].shape = shape_of(h[f]);
+    all_known = all_known && h[f].shape != SH_GENERIC;
+    common = (common < 0 || common == h[f].shape) ? h[f].shape : SH_MULTI;
+  }
+  if (!all_known || common < 0) return SH_GENERIC;
+  return common;
 }
 static const void* batch_kernel_for(const BatchPlan* plan) {
   switch (plan->shape) {
@@ -886,6 +920,9 @@ static const void* batch_kernel_for(const BatchPlan* plan) {
     case SH_HOP: return reinterpret_cast<const void*>(&batch_program_kernel<12, ShapeHop>);
     case SH_AXPY_MAD: return reinterpret_cast<const void*>(&batch_program_kernel<12, ShapeAxpyMaD>);
     case SH_MMA_COPY: return reinterpret_cast<const void*>(&batch_program_kernel<9, ShapeMMaCopy>);
+    case SH_MULTI:
+      return plan->mc == 12 ? reinterpret_cast<const void*>(&batch_program_kernel<12, MultiShape>)
+                            : reinterpret_cast<const void*>(&batch_program_kernel<9, MultiShape>);
     default:
       return plan->mc == 12 ? reinterpret_cast<const void*>(&batch_program_kernel<12, GenericShape>)
                             : reinterpret_cast<const void*>(&batch_program_kernel<9, GenericShape>);
@@ -924,6 +961,7 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
     set_error(QLAGPU_ERR_ARG, who, "the programs' streams need more shared memory per tile than a block has");
     return nullptr;
   }
+  const int shape = common_shape(h.data(), nfields);  // also each field's own shape
   if (!device_error_word()) return nullptr;  // allocate it now, not inside a later capture
   BatchPlan* plan = new BatchPlan();
   plan->nfields = nfields;
@@ -934,7 +972,7 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
   plan->out_slice_bytes = out_slice;
   plan->spill_regs = spills ? 1 : 0;
   plan->mc = uses_d ? 12 : 9;
-  plan->shape = common_shape(h.data(), nfields);
+  plan->shape = shape;
   plan->smem = smem;
   if (cudaMalloc(&plan->dfields, sizeof(BField) * (size_t)nfields) != cudaSuccess ||
       cudaMemcpy(plan->dfields, h.data(), sizeof(BField) * (size_t)nfields, cudaMemcpyHostToDevice) !=
