@@ -202,35 +202,53 @@ __global__ void __launch_bounds__(256) prop_mp_kernel(const PropParams p) {
   const long long total = p.n * 24;
   const bool minus = (p.eqop == MEQ || p.eqop == EQM);
   const bool load = (p.eqop == PEQ || p.eqop == MEQ);
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
-       g += (long long)gridDim.x * blockDim.x) {
-    const long long i = g / 24;
-    const int q = (int)(g - i * 24);
-    const int is = q / 6, jc = (q >> 1) % 3, jh = q & 1;
-    const long long k = p.gang ? (long long)p.gang[i] : i;
-    Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 144 + 2 * q;  // + ic * 48
-    Cx<R> mm[9];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  // two elements per iteration (g and g + stride): both elements' operand
+  // loads are issued before either's arithmetic, twice the bytes in flight
+  for (long long g0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; g0 < total; g0 += 2 * stride) {
+    constexpr int U = 2;
+    long long kk[U];
+    int qq[U];
+    bool on[U];
+    Cx<R> mm[U][9], bb[U][3][2];
 #pragma unroll
-    for (int e = 0; e < 9; e++) mm[e] = ld_elem<R>(p.a, k, e, 9);
-    Cx<R> x[3][2];
+    for (int u = 0; u < U; u++) {
+      const long long g = g0 + u * stride;
+      on[u] = g < total;
+      const long long i = on[u] ? g / 24 : 0;
+      qq[u] = (int)(g - i * 24);
+      kk[u] = !on[u] ? 0 : p.gang ? (long long)p.gang[i] : i;
+      if (!on[u]) continue;
+      const int q = qq[u], is = q / 6, jc = (q >> 1) % 3, jh = q & 1;
 #pragma unroll
-    for (int ic = 0; ic < 3; ic++) init2<R>(x[ic], out + ic * 48, load, p.vec_out);
+      for (int e = 0; e < 9; e++) mm[u][e] = ld_elem<R>(p.a, kk[u], e, 9);
 #pragma unroll
-    for (int kc = 0; kc < 3; kc++) {
-      Cx<R> b[2];
-      if constexpr (!CB) {
-        ld2<R>(b, p.b, k, kc * 48 + 2 * q, 144, p.vec_b);
-      } else {
+      for (int kc = 0; kc < 3; kc++) {
+        if constexpr (!CB) {
+          ld2<R>(bb[u][kc], p.b, kk[u], kc * 48 + 2 * q, 144, p.vec_b);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 2; j++) b[j] = ld_elem<R>(p.b, k, p_idx(kc, is, jc, 2 * jh + j, true), 144);
+          for (int j = 0; j < 2; j++)
+            bb[u][kc][j] = ld_elem<R>(p.b, kk[u], p_idx(kc, is, jc, 2 * jh + j, true), 144);
+        }
       }
-#pragma unroll
-      for (int ic = 0; ic < 3; ic++)
-#pragma unroll
-        for (int j = 0; j < 2; j++) cmac<CA, CB>(x[ic][j], minus, mm[m_idx(ic, kc, CA)], b[j]);
     }
 #pragma unroll
-    for (int ic = 0; ic < 3; ic++) st2<R>(out + ic * 48, x[ic], p.vec_out);
+    for (int u = 0; u < U; u++) {
+      if (!on[u]) continue;
+      Cx<R>* out = static_cast<Cx<R>*>(p.out) + kk[u] * 144 + 2 * qq[u];  // + ic * 48
+      Cx<R> x[3][2];
+#pragma unroll
+      for (int ic = 0; ic < 3; ic++) init2<R>(x[ic], out + ic * 48, load, p.vec_out);
+#pragma unroll
+      for (int kc = 0; kc < 3; kc++)
+#pragma unroll
+        for (int ic = 0; ic < 3; ic++)
+#pragma unroll
+          for (int j = 0; j < 2; j++) cmac<CA, CB>(x[ic][j], minus, mm[u][m_idx(ic, kc, CA)], bb[u][kc][j]);
+#pragma unroll
+      for (int ic = 0; ic < 3; ic++) st2<R>(out + ic * 48, x[ic], p.vec_out);
+    }
   }
 }
 
