@@ -242,6 +242,35 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// The same wait for a thread with nothing else to do (a producer lane ahead
+// of its consumers, a consumer ahead of its data): each try suspends the
+// thread for up to hint_ns or until the phase completes, so that waiting
+// warps do not take issue slots from the computing ones.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded_idle(uint64_t* bar, uint32_t parity, unsigned* err,
+                                                       uint64_t limit_ns = 2000000000ull,
+                                                       volatile int* abort = nullptr, uint32_t hint_ns = 20000u) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 30); ++it) {
+    if (mbar_try_wait_hint(bar, parity, hint_ns)) return true;
+    if (abort && *abort) return false;
+    if (global_ns() - t0 > limit_ns) break;
+  }
+  raise_dev_error(err, QLA_DEVERR_MBAR_TIMEOUT);
+  return false;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }

@@ -15,9 +15,14 @@
 //           P[kc][is][jc][js..js+1] serves all three output colours ic;
 //   P * M   24 threads per site, thread (ic, is, js pair): the P run
 //           P[ic][is][kc][js..js+1] serves all three output colours jc;
-//   P * P   6 (F3) / 12 (D3) threads per site, thread (jc, js block): a
-//           column block of the second operand held in registers, the first
-//           operand's rows streamed once, 24 / 12 outputs per thread.
+//   P * P   contiguous operands: F3 through a bulk-copy (TMA) pipeline of
+//           8-site tiles, 12 threads per site, 2 output rows x 6 columns per
+//           thread in packed FP32x2 arithmetic (prop_pp_tma_kernel); D3 with
+//           12 threads per site, one output row each, the second operand's
+//           records staged in shared memory (prop_pp_rows_kernel); gang,
+//           pointer or unaligned operands 6 (F3) / 12 (D3) threads per site,
+//           a column block of the second operand in registers
+//           (prop_pp_kernel).
 // The 9 matrix elements come from L1 (shared by a site's threads).  Adjoint
 // or pointer operands read element by element.  Every output element is
 // accumulated exactly as the reference does (x = 0 or r, then
@@ -39,6 +44,8 @@ struct PropParams {
   int eqop;
   int vec_a, vec_b, vec_out;  // 16-B vector access allowed (contiguous, aligned)
   float negzero;              // -0.0f, passed at run time (see mul_rn_x2)
+  unsigned* err;              // device error word (bounded waits of the bulk-copy P * P)
+  int stages;                 // stage ring depth of the bulk-copy P * P
 };
 
 // ---------------------------------------------------------------------------
@@ -394,44 +401,27 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
   }
 }
 
-// P * P for contiguous, 16-B aligned operands without a gang index: one
+// P * P (D3) for contiguous, 16-B aligned operands without a gang index: one
 // thread per (site, output row), SPB sites per block.  The block copies the
-// second operand's SPB records into shared memory with coalesced 16-B loads
-// (for F3 also a copy with each complex number's parts swapped), then every
-// thread keeps its row of the first operand (of P, or of P^+) in registers
-// and walks the 12 rows of the second operand (of P or P^+) in shared memory;
-// the 12 threads of a site read the same words (broadcasts).  Output rows are
-// written with 16-B stores.
-//
-// F3 packs the real and imaginary part of one output element into the two
-// lanes of an FP32x2 register: with b = (br, bi) and its swap bs = (bi, br),
-//   (re, im) = (ar, sa ar) * b + (ta ai, tb ai) * bs
-// where the signs sa, ta, tb follow the conjugations (CA, CB) so that each lane
-// forms the same two rounded products and the same rounded sum as cmac<CA, CB>
-// (a product of a negated operand is the exactly negated product, and
-// x + (-y) is x - y); the accumulation x (+|-)= (re, im) is a packed add or
-// subtract.  D3 runs cmac<CA, CB> on the same mapping.  Bit-identical either way.
+// second operand's SPB records into shared memory with coalesced 16-B loads,
+// then every thread keeps its row of the first operand (of P, or of P^+) in
+// registers and walks the 12 rows of the second operand (of P or P^+) in
+// shared memory, accumulating with cmac<CA, CB> in the reference's order
+// (bit-identical); the 12 threads of a site read the same words
+// (broadcasts).  Output rows are written with 16-B stores.
 template <typename R, bool CA, bool CB, int SPB>
 __global__ void __launch_bounds__(12 * SPB) prop_pp_rows_kernel(const PropParams p) {
+  static_assert(sizeof(R) == 8, "the F3 product runs prop_pp_tma_kernel");
   extern __shared__ __align__(16) unsigned char psm[];
-  constexpr bool F32 = sizeof(R) == 4;
   Cx<R>* Bs = reinterpret_cast<Cx<R>*>(psm);  // [SPB][144]
-  Cx<R>* Bw = Bs + SPB * 144;                  // F3: the same records, parts swapped
   const long long site0 = (long long)blockIdx.x * SPB;
   const long long left = p.n - site0;
   const int nloc = left < SPB ? (int)left : SPB;
   {
     const int words = nloc * 144 * (int)sizeof(Cx<R>) / 16;
     const char* Bg = static_cast<const char*>(p.b.base) + site0 * 144 * (long long)sizeof(Cx<R>);
-    for (int w = threadIdx.x; w < words; w += blockDim.x) {
-      if constexpr (F32) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(Bg) + w);
-        reinterpret_cast<float4*>(Bs)[w] = v;
-        reinterpret_cast<float4*>(Bw)[w] = make_float4(v.y, v.x, v.w, v.z);
-      } else {
-        reinterpret_cast<double2*>(Bs)[w] = __ldg(reinterpret_cast<const double2*>(Bg) + w);
-      }
-    }
+    for (int w = threadIdx.x; w < words; w += blockDim.x)
+      reinterpret_cast<double2*>(Bs)[w] = __ldg(reinterpret_cast<const double2*>(Bg) + w);
   }
   __syncthreads();
   const int ls = threadIdx.x / 12, row = threadIdx.x - ls * 12;  // local site, output row ic * 4 + is
@@ -457,185 +447,231 @@ __global__ void __launch_bounds__(12 * SPB) prop_pp_rows_kernel(const PropParams
   const Cx<R>* B = Bs + ls * 144;
   // element (kk, jj) of the second operand before conjugation: P[kk][jj], or P[jj][kk] for P^+
   auto bidx = [](int kk, int jj) { return CB ? jj * 12 + kk : kk * 12 + jj; };
-  if constexpr (F32) {
-    const Cx<float>* W = Bw + ls * 144;
-    constexpr float sa = CB ? -1.f : 1.f;
-    constexpr float ta = (CA == CB) ? -1.f : 1.f, tb = CA ? -1.f : 1.f;
-    float2 x[12];
+  Cx<R> x[12];
 #pragma unroll
-    for (int jj = 0; jj < 12; jj += 2) {
-      if (load) {
-        Cx<float> t[2];
-        ld2_out<float>(t, out + jj, true);
-        x[jj] = make_float2(t[0].re, t[0].im);
-        x[jj + 1] = make_float2(t[1].re, t[1].im);
-      } else {
-        x[jj] = make_float2(0.f, 0.f);
-        x[jj + 1] = make_float2(0.f, 0.f);
-      }
-    }
-    const float z = p.negzero;
+  for (int jj = 0; jj < 12; jj++) x[jj] = load ? out[jj] : Cx<R>{R(0), R(0)};
 #pragma unroll
-    for (int kk = 0; kk < 12; kk++) {
-      const float2 pa = make_float2(a[kk].re, sa * a[kk].re), qa = make_float2(ta * a[kk].im, tb * a[kk].im);
+  for (int kk = 0; kk < 12; kk++)
 #pragma unroll
-      for (int jj = 0; jj < 12; jj++) {
-        const Cx<float> bv = B[bidx(kk, jj)], bw = W[bidx(kk, jj)];
-        const float2 prod =
-            add_rn_x2(mul_rn_x2(pa, make_float2(bv.re, bv.im), z), mul_rn_x2(qa, make_float2(bw.re, bw.im), z));
-        x[jj] = minus ? sub_rn_x2(x[jj], prod) : add_rn_x2(x[jj], prod);
-      }
-    }
+    for (int jj = 0; jj < 12; jj++) cmac<CA, CB>(x[jj], minus, a[kk], B[bidx(kk, jj)]);
 #pragma unroll
-    for (int jj = 0; jj < 12; jj += 2) {
-      const Cx<float> t[2] = {Cx<float>{x[jj].x, x[jj].y}, Cx<float>{x[jj + 1].x, x[jj + 1].y}};
-      st2<float>(out + jj, t, true);
-    }
-  } else {
-    Cx<R> x[12];
-#pragma unroll
-    for (int jj = 0; jj < 12; jj++) x[jj] = load ? out[jj] : Cx<R>{R(0), R(0)};
-#pragma unroll
-    for (int kk = 0; kk < 12; kk++)
-#pragma unroll
-      for (int jj = 0; jj < 12; jj++) cmac<CA, CB>(x[jj], minus, a[kk], B[bidx(kk, jj)]);
-#pragma unroll
-    for (int jj = 0; jj < 12; jj += 2) {
-      const Cx<R> t[2] = {x[jj], x[jj + 1]};
-      st2<R>(out + jj, t, true);
-    }
+  for (int jj = 0; jj < 12; jj += 2) {
+    const Cx<R> t[2] = {x[jj], x[jj + 1]};
+    st2<R>(out + jj, t, true);
   }
 }
-
-// 16-B asynchronous global -> shared copies (sm_80+ cp.async, L1 bypassed)
-__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst_smem)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // P * P (F3) for contiguous, 16-B aligned operands without a gang index:
-// persistent blocks of 12 * SPB threads, one thread per (site, output row),
-// looping over tiles of SPB sites with software pipelining.  Before computing
-// tile t every thread starts the copies of tile t+1: its share of the first
-// operand's records with cp.async into the other shared buffer, and its share
-// of the second operand's records into registers; after computing it writes
-// those registers to the other buffer in operand order (P, or P^+ read
-// transposed) as separate real and imaginary planes, so that two output
-// columns share one FP32x2 register (cmac_x2: per-lane rounding as
-// cmac<CA, CB>).  One block barrier per tile hands the buffers over.  Every
-// output element is accumulated as the reference does: bit-identical.
-template <bool CA, bool CB, int SPB>
-__global__ void __launch_bounds__(12 * SPB) prop_pp_pipe_kernel(const PropParams p, long long ntiles) {
-  extern __shared__ __align__(16) unsigned char psm[];
-  constexpr int NT = 12 * SPB;          // threads
-  constexpr int WPS = 72;               // 16-B words per record
-  constexpr int WPT = SPB * WPS / NT;   // words per thread per tile (6)
-  constexpr int BUF = SPB * 1152;       // bytes of one tile of records
-  static_assert(SPB * WPS % NT == 0, "tile words must split evenly");
-  unsigned char* bbuf = psm;            // [2][BUF]: second operand, re / im planes per site
-  unsigned char* abuf = psm + 2 * BUF;  // [2][BUF]: first operand, records as stored
-  const int tid = threadIdx.x, ls = tid / 12, row = tid - ls * 12;
-  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
-  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
-  const uint4* Ag = static_cast<const uint4*>(p.a.base);
-  const uint4* Bg = static_cast<const uint4*>(p.b.base);
-  Cx<float>* Og = static_cast<Cx<float>*>(p.out);
-  uint4 nb[WPT];
-  // start the copies of tile t: first operand -> abuf[b] (asynchronous),
-  // second operand -> registers nb
-  auto fetch = [&](long long t, int b) {
-    const long long s0 = t * SPB;
-    const long long words = ((p.n - s0) < SPB ? (p.n - s0) : SPB) * WPS;
-    uint4* adst = reinterpret_cast<uint4*>(abuf + (size_t)b * BUF);
-#pragma unroll
-    for (int i = 0; i < WPT; i++) {
-      const int w = tid + i * NT;
-      if (w < words) {
-        cp_async16(adst + w, Ag + s0 * WPS + w);
-        nb[i] = __ldg(Bg + s0 * WPS + w);
+// bulk-copy (TMA) pipeline, persistent, warp-specialised like the site engine.
+// Block = 12 * SPB consumer threads (12 per site of a tile of SPB sites) + one
+// producer warp.  Per stage of the ring there is a `full` mbarrier (completed
+// by the copies' transaction bytes) and an `empty` mbarrier (one arrival per
+// consumer warp).  The producer issues one 1152-B bulk copy per site and
+// operand into the stage (sites SA / SB floats apart, so that the sites one
+// warp covers spread over the banks); consumers wait on `full`, compute from
+// the stage, release it and store their results with 16-B stores.  No block
+// barrier sits in the tile loop.
+//
+// Thread (rg, cg) of a site accumulates the 12 output elements of rows 2rg,
+// 2rg+1 at the column pairs {2(cg + 2q), 2(cg + 2q) + 1}, q = 0..2, two columns
+// per FP32x2 register (cmac_x2: per-lane rounding as cmac<CA, CB>); every
+// element is accumulated over k in order as the reference does, so results
+// are bit-identical.  Every wait is time-bounded; a failed wait raises the
+// block's abort flag, which ends every other wait of the block at once, and
+// loads still in flight are drained (bounded) before the block exits.
+//
+// Dynamic shared memory: [full[8] | empty[8] | abort flag | pad to 256 B |
+//                         stages x (SPB x SA + SPB x SB floats)].
+template <bool CA, bool CB, int SPB, int MINB>
+__global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const PropParams p, long long ntiles) {
+  extern __shared__ __align__(128) unsigned char ptm[];
+  constexpr int NCT = 12 * SPB;  // consumer threads
+  constexpr int NCW = NCT / 32;  // consumer warps
+  constexpr int SA = 292, SB = 296;
+  constexpr unsigned STAGE = SPB * (SA + SB) * 4u;
+  static_assert(NCT % 32 == 0, "consumer threads fill whole warps");
+  static_assert(2 * SPB <= 32, "one producer lane per site and operand");
+  const int S = p.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(ptm);
+  uint64_t* empty = full + 8;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(ptm + 8 * 16);
+  unsigned char* stages = ptm + 256;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long my = ((long long)blockIdx.x < ntiles) ? (ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1 : 0;
+  if (tid == 0) {
+    for (int i = 0; i < S; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], (unsigned)NCW);
+    }
+    *abort_flag = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  long long issued = 0;
+  if (warp == NCW) {
+    // ------------------------------------------------------------ producer
+    const uint64_t pol = policy_evict_first();
+    const char* Ag = static_cast<const char*>(p.a.base);
+    const char* Bg = static_cast<const char*>(p.b.base);
+    int st = 0;
+    long long round = 0, k = 0;
+    for (; k < my; k++) {
+      bool ok = true;
+      if (lane == 0 && round > 0)
+        ok = mbar_wait_bounded_idle(&empty[st], (uint32_t)((round - 1) & 1), p.err, 2000000000ull, abort_flag);
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) {
+        if (lane == 0) *abort_flag = 1;
+        break;
+      }
+      const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * SPB;
+      const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
+      float* sa = reinterpret_cast<float*>(stages + (size_t)st * STAGE);
+      float* sb = sa + SPB * SA;
+      if (lane == 0) mbar_arrive_expect_tx(&full[st], (uint32_t)nloc * 2304u);
+      __syncwarp();
+      if (lane < nloc)
+        bulk_g2s(sa + lane * SA, Ag + (site0 + lane) * 1152, 1152u, &full[st], pol);
+      else if (lane >= SPB && lane - SPB < nloc)
+        bulk_g2s(sb + (lane - SPB) * SB, Bg + (site0 + lane - SPB) * 1152, 1152u, &full[st], pol);
+      if (++st == S) {
+        st = 0;
+        round++;
       }
     }
-    cp_async_commit();
-  };
-  // registers nb -> bbuf[b], element (kk, jj) at kk * 12 + jj of each plane
-  auto stash = [&](int b) {
-    float* base = reinterpret_cast<float*>(bbuf + (size_t)b * BUF);
+    issued = k;
+  } else {
+    // ------------------------------------------------------------ consumers
+    const int ls = tid / 12, t12 = tid - ls * 12, rg = t12 >> 1, cg = t12 & 1;
+    const bool minus = (p.eqop == MEQ || p.eqop == EQM);
+    const bool load = (p.eqop == PEQ || p.eqop == MEQ);
+    const float z = p.negzero;
+    int st = 0;
+    uint32_t par = 0;
+    for (long long k = 0; k < my; k++) {
+      // warp-uniform, so that the warp leaves the loop as a whole
+      const bool ok =
+          __all_sync(0xffffffffu, mbar_wait_bounded_idle(&full[st], par, p.err, 2000000000ull, abort_flag));
+      const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * SPB;
+      const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
+      const bool active = ok && ls < nloc;
+      const float* A = reinterpret_cast<const float*>(stages + (size_t)st * STAGE) + ls * SA;
+      const float* B = A - ls * SA + SPB * SA + ls * SB;
+      const Cx<float>* og = static_cast<const Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
+      float2 xr[2][3], xi[2][3];  // [row 2rg + i][q]: lanes = columns 2(cg + 2q), +1
 #pragma unroll
-    for (int i = 0; i < WPT; i++) {
-      const int w = tid + i * NT, site = w / WPS, e0 = (w - site * WPS) * 2;
-      const uint4 v = nb[i];
-      float* re = base + site * 288;
-      float* im = re + 144;
-      const int o0 = CB ? (e0 % 12) * 12 + e0 / 12 : e0;
-      const int o1 = CB ? ((e0 + 1) % 12) * 12 + (e0 + 1) / 12 : e0 + 1;
-      re[o0] = __uint_as_float(v.x);
-      im[o0] = __uint_as_float(v.y);
-      re[o1] = __uint_as_float(v.z);
-      im[o1] = __uint_as_float(v.w);
-    }
-  };
-  long long t = blockIdx.x;
-  if (t >= ntiles) return;
-  fetch(t, 0);
-  stash(0);
-  cp_async_wait_all();
-  __syncthreads();
-  for (int b = 0; t < ntiles; t += gridDim.x, b ^= 1) {
-    const long long tn = t + gridDim.x;
-    if (tn < ntiles) fetch(tn, b ^ 1);  // in flight during the arithmetic below
-    const long long k = t * SPB + ls;
-    if (k < p.n) {
-      Cx<float>* out = Og + k * 144 + row * 12;
-      const Cx<float>* A = reinterpret_cast<const Cx<float>*>(abuf + (size_t)b * BUF) + ls * 144;
-      Cx<float> a[12];
-      if constexpr (!CA) {
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          if (load && active) {
+            const float4 v = *reinterpret_cast<const float4*>(og + (2 * rg + i) * 12 + 4 * q);
+            xr[i][q] = make_float2(v.x, v.z);
+            xi[i][q] = make_float2(v.y, v.w);
+          } else {
+            xr[i][q] = make_float2(0.f, 0.f);
+            xi[i][q] = make_float2(0.f, 0.f);
+          }
+        }
+      if (active) {
 #pragma unroll
         for (int kk = 0; kk < 12; kk += 2) {
-          Cx<float> t2[2];
-          ld2_out<float>(t2, A + row * 12 + kk, true);
-          a[kk] = t2[0];
-          a[kk + 1] = t2[1];
-        }
-      } else {
+          Cx<float> a[2][2];  // element (row 2rg + i, kk + h) before conjugation
+          if constexpr (!CA) {
 #pragma unroll
-        for (int kk = 0; kk < 12; kk++) a[kk] = A[kk * 12 + row];  // P^+[row][kk] = conj P[kk][row]
+            for (int i = 0; i < 2; i++) {
+              const float4 v = *reinterpret_cast<const float4*>(A + ((2 * rg + i) * 12 + kk) * 2);
+              a[i][0] = Cx<float>{v.x, v.y};
+              a[i][1] = Cx<float>{v.z, v.w};
+            }
+          } else {  // P^+[r][kk] = conj P[kk][r]: elements (kk + h, 2rg), (kk + h, 2rg + 1) are adjacent
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const float4 v = *reinterpret_cast<const float4*>(A + ((kk + h) * 12 + 2 * rg) * 2);
+              a[0][h] = Cx<float>{v.x, v.y};
+              a[1][h] = Cx<float>{v.z, v.w};
+            }
+          }
+          // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before conjugation
+          float2 bre[2][3], bim[2][3];
+          if constexpr (!CB) {
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+#pragma unroll
+              for (int q = 0; q < 3; q++) {
+                const float4 v = *reinterpret_cast<const float4*>(B + (kk + h) * 24 + 4 * (cg + 2 * q));
+                bre[h][q] = make_float2(v.x, v.z);
+                bim[h][q] = make_float2(v.y, v.w);
+              }
+          } else {  // P^+[kk][j] = conj P[j][kk]: elements (j, kk), (j, kk + 1) are adjacent
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+              const int j = 2 * (cg + 2 * q);
+              const float4 v0 = *reinterpret_cast<const float4*>(B + j * 24 + 2 * kk);
+              const float4 v1 = *reinterpret_cast<const float4*>(B + (j + 1) * 24 + 2 * kk);
+              bre[0][q] = make_float2(v0.x, v1.x);
+              bim[0][q] = make_float2(v0.y, v1.y);
+              bre[1][q] = make_float2(v0.z, v1.z);
+              bim[1][q] = make_float2(v0.w, v1.w);
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+              for (int q = 0; q < 3; q++)
+                cmac_x2<CA, CB>(xr[i][q], xi[i][q], minus, a[i][h], bre[h][q], bim[h][q], z);
+        }
       }
-      const float* re = reinterpret_cast<const float*>(bbuf + (size_t)b * BUF) + ls * 288;
-      const float* im = re + 144;
-      float2 xr[6], xi[6];  // lanes: output columns 2c, 2c + 1
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        if (load) {
-          Cx<float> t2[2];
-          ld2_out<float>(t2, out + 2 * c, true);
-          xr[c] = make_float2(t2[0].re, t2[1].re);
-          xi[c] = make_float2(t2[0].im, t2[1].im);
-        } else {
-          xr[c] = make_float2(0.f, 0.f);
-          xi[c] = make_float2(0.f, 0.f);
-        }
+      release_stage(&empty[st], lane);  // this warp is done with the stage
+      if (!ok) {
+        *abort_flag = 1;
+        break;
       }
+      if (ls < nloc) {
+        Cx<float>* o = static_cast<Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
 #pragma unroll
-      for (int kk = 0; kk < 12; kk++)
+        for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int c = 0; c < 6; c += 2) {  // 16-B loads: two column pairs each
-          const float4 r4 = *reinterpret_cast<const float4*>(re + kk * 12 + 2 * c);
-          const float4 i4 = *reinterpret_cast<const float4*>(im + kk * 12 + 2 * c);
-          cmac_x2<CA, CB>(xr[c], xi[c], minus, a[kk], make_float2(r4.x, r4.y), make_float2(i4.x, i4.y), p.negzero);
-          cmac_x2<CA, CB>(xr[c + 1], xi[c + 1], minus, a[kk], make_float2(r4.z, r4.w), make_float2(i4.z, i4.w),
-                          p.negzero);
-        }
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        const Cx<float> t2[2] = {Cx<float>{xr[c].x, xi[c].x}, Cx<float>{xr[c].y, xi[c].y}};
-        st2<float>(out + 2 * c, t2, true);
+          for (int q = 0; q < 3; q++)
+            *reinterpret_cast<float4*>(o + (2 * rg + i) * 12 + 4 * q) =
+                make_float4(xr[i][q].x, xi[i][q].x, xr[i][q].y, xi[i][q].y);
+      }
+      if (++st == S) {
+        st = 0;
+        par ^= 1u;
       }
     }
-    if (tn < ntiles) stash(b ^ 1);  // the other buffers were last read before the previous barrier
-    cp_async_wait_all();
-    __syncthreads();
   }
+  __syncthreads();
+  if (*abort_flag && warp == NCW && lane == 0) {
+    // a wait failed: before the block's shared memory is released, wait
+    // (bounded) until every load still in flight has landed
+    for (long long kk = (issued > S ? issued - S : 0); kk < issued; kk++)
+      if (!mbar_wait_bounded(&full[kk % S], (uint32_t)((kk / S) & 1), p.err, 200000000ull, nullptr))
+        raise_dev_error(p.err, QLA_DEVERR_BULK_TIMEOUT);
+  }
+}
+
+// shared-memory bytes of prop_pp_tma_kernel<.., SPB> with `stages` stages
+constexpr size_t pp_tma_smem(int spb, int stages) { return 256 + (size_t)stages * spb * (292 + 296) * 4; }
+
+// blocks per SM of a kernel at (threads, smem), raising its dynamic
+// shared-memory limit once per device
+inline int prop_blocks_per_sm(const void* fn, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+  const int dev = current_device();
+  std::lock_guard<std::mutex> g(mu);
+  const auto key = std::make_tuple(dev, fn, threads, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess || nb < 1) nb = 1;
+  cudaGetLastError();
+  cache[key] = nb;
+  return nb;
 }
 
 // the spin trace: one thread per output element (9 per site)
@@ -710,18 +746,22 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
       const long long blocks = ((long long)n + SPB - 1) / SPB;
       prop_pp_rows_kernel<R, CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p);
     } else {
-      // F3: 8 sites per tile, 96 threads and 36 KB per block: at ~128 registers
-      // five blocks (15 warps) share an SM
+      // F3: bulk-copy pipeline, tiles of 8 sites, 96 consumer threads + one
+      // producer warp per block, three stages (57 KB): four blocks per SM at
+      // up to 128 registers.  Measured on B200 (131,072 sites): 90 us, where
+      // two stages took 92 us and five or six blocks per SM at 80-96
+      // registers 95-98 us (fewer registers cost more than the extra warps
+      // gain).
       constexpr int SPB = 8;
-      const size_t smem = 4 * (size_t)SPB * 1152;  // two buffers of each operand
+      p.stages = 3;
+      p.err = device_error_word();
+      const size_t smem = pp_tma_smem(SPB, p.stages);
       const long long ntiles = ((long long)n + SPB - 1) / SPB;
-      const void* fn = reinterpret_cast<const void*>(&prop_pp_pipe_kernel<CA, CB, SPB>);
-      int nb = 1;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 12 * SPB, smem) != cudaSuccess || nb < 1) nb = 1;
-      cudaGetLastError();
-      long long blocks = (long long)nb * device_sm_count();
+      constexpr int MINB = 4;
+      const void* fn = reinterpret_cast<const void*>(&prop_pp_tma_kernel<CA, CB, SPB, MINB>);
+      long long blocks = (long long)prop_blocks_per_sm(fn, 12 * SPB + 32, smem) * device_sm_count();
       if (blocks > ntiles) blocks = ntiles;
-      prop_pp_pipe_kernel<CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p, ntiles);
+      prop_pp_tma_kernel<CA, CB, SPB, MINB><<<(unsigned)blocks, 12 * SPB + 32, smem, st>>>(p, ntiles);
     }
   }
   check_launch(kid);
