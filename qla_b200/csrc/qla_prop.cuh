@@ -15,13 +15,11 @@
 //           P[kc][is][jc][js..js+1] serves all three output colours ic;
 //   P * M   24 threads per site, thread (ic, is, js pair): the P run
 //           P[ic][is][kc][js..js+1] serves all three output colours jc;
-//   P * P   contiguous operands: F3 through a bulk-copy (TMA) pipeline of
+//   P * P   contiguous operands through a bulk-copy (TMA) pipeline of
 //           8-site tiles, 12 threads per site, 2 output rows x 6 columns per
-//           thread in packed FP32x2 arithmetic (prop_pp_tma_kernel); D3 with
-//           12 threads per site, one output row each, the second operand's
-//           records staged in shared memory (prop_pp_rows_kernel); gang,
-//           pointer or unaligned operands 6 (F3) / 12 (D3) threads per site,
-//           a column block of the second operand in registers
+//           thread (F3 in packed FP32x2 arithmetic; prop_pp_tma_kernel);
+//           gang, pointer or unaligned operands 6 (F3) / 12 (D3) threads per
+//           site, a column block of the second operand in registers
 //           (prop_pp_kernel).
 // The 9 matrix elements come from L1 (shared by a site's threads).  Adjoint
 // or pointer operands read element by element.  Every output element is
@@ -401,68 +399,9 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
   }
 }
 
-// P * P (D3) for contiguous, 16-B aligned operands without a gang index: one
-// thread per (site, output row), SPB sites per block.  The block copies the
-// second operand's SPB records into shared memory with coalesced 16-B loads,
-// then every thread keeps its row of the first operand (of P, or of P^+) in
-// registers and walks the 12 rows of the second operand (of P or P^+) in
-// shared memory, accumulating with cmac<CA, CB> in the reference's order
-// (bit-identical); the 12 threads of a site read the same words
-// (broadcasts).  Output rows are written with 16-B stores.
-template <typename R, bool CA, bool CB, int SPB>
-__global__ void __launch_bounds__(12 * SPB) prop_pp_rows_kernel(const PropParams p) {
-  static_assert(sizeof(R) == 8, "the F3 product runs prop_pp_tma_kernel");
-  extern __shared__ __align__(16) unsigned char psm[];
-  Cx<R>* Bs = reinterpret_cast<Cx<R>*>(psm);  // [SPB][144]
-  const long long site0 = (long long)blockIdx.x * SPB;
-  const long long left = p.n - site0;
-  const int nloc = left < SPB ? (int)left : SPB;
-  {
-    const int words = nloc * 144 * (int)sizeof(Cx<R>) / 16;
-    const char* Bg = static_cast<const char*>(p.b.base) + site0 * 144 * (long long)sizeof(Cx<R>);
-    for (int w = threadIdx.x; w < words; w += blockDim.x)
-      reinterpret_cast<double2*>(Bs)[w] = __ldg(reinterpret_cast<const double2*>(Bg) + w);
-  }
-  __syncthreads();
-  const int ls = threadIdx.x / 12, row = threadIdx.x - ls * 12;  // local site, output row ic * 4 + is
-  if (ls >= nloc) return;                                         // (after the block's only barrier)
-  const long long k = site0 + ls;
-  const bool minus = (p.eqop == MEQ || p.eqop == EQM);
-  const bool load = (p.eqop == PEQ || p.eqop == MEQ);
-  const Cx<R>* A = static_cast<const Cx<R>*>(p.a.base) + k * 144;
-  Cx<R> a[12];
-  if constexpr (!CA) {
-#pragma unroll
-    for (int kk = 0; kk < 12; kk += 2) {
-      Cx<R> t[2];
-      ld2_out<R>(t, A + row * 12 + kk, true);
-      a[kk] = t[0];
-      a[kk + 1] = t[1];
-    }
-  } else {
-#pragma unroll
-    for (int kk = 0; kk < 12; kk++) a[kk] = A[kk * 12 + row];  // P^+[row][kk] = conj P[kk][row]
-  }
-  Cx<R>* out = static_cast<Cx<R>*>(p.out) + k * 144 + row * 12;
-  const Cx<R>* B = Bs + ls * 144;
-  // element (kk, jj) of the second operand before conjugation: P[kk][jj], or P[jj][kk] for P^+
-  auto bidx = [](int kk, int jj) { return CB ? jj * 12 + kk : kk * 12 + jj; };
-  Cx<R> x[12];
-#pragma unroll
-  for (int jj = 0; jj < 12; jj++) x[jj] = load ? out[jj] : Cx<R>{R(0), R(0)};
-#pragma unroll
-  for (int kk = 0; kk < 12; kk++)
-#pragma unroll
-    for (int jj = 0; jj < 12; jj++) cmac<CA, CB>(x[jj], minus, a[kk], B[bidx(kk, jj)]);
-#pragma unroll
-  for (int jj = 0; jj < 12; jj += 2) {
-    const Cx<R> t[2] = {x[jj], x[jj + 1]};
-    st2<R>(out + jj, t, true);
-  }
-}
-
-// P * P (F3) for contiguous, 16-B aligned operands without a gang index:
-// bulk-copy (TMA) pipeline, persistent, warp-specialised like the site engine.
+// P * P (F3 and D3) for contiguous, 16-B aligned operands without a gang
+// index: bulk-copy (TMA) pipeline, persistent, warp-specialised like the site
+// engine.
 // Block = 12 * SPB consumer threads (12 per site of a tile of SPB sites) + one
 // producer warp.  Per stage of the ring there is a `full` mbarrier (completed
 // by the copies' transaction bytes) and an `empty` mbarrier (one arrival per
@@ -473,22 +412,36 @@ __global__ void __launch_bounds__(12 * SPB) prop_pp_rows_kernel(const PropParams
 // barrier sits in the tile loop.
 //
 // Thread (rg, cg) of a site accumulates the 12 output elements of rows 2rg,
-// 2rg+1 at the column pairs {2(cg + 2q), 2(cg + 2q) + 1}, q = 0..2, two columns
-// per FP32x2 register (cmac_x2: per-lane rounding as cmac<CA, CB>); every
-// element is accumulated over k in order as the reference does, so results
-// are bit-identical.  Every wait is time-bounded; a failed wait raises the
+// 2rg+1: in F3 at the column pairs {2(cg + 2q), 2(cg + 2q) + 1}, q = 0..2, two
+// columns per FP32x2 register (cmac_x2: per-lane rounding as cmac<CA, CB>),
+// in D3 at the columns cg + 2q, q = 0..5, with cmac<CA, CB>; every element is
+// accumulated over k in order as the reference does, so results are
+// bit-identical.  Every wait is time-bounded; a failed wait raises the
 // block's abort flag, which ends every other wait of the block at once, and
 // loads still in flight are drained (bounded) before the block exits.
 //
 // Dynamic shared memory: [full[8] | empty[8] | abort flag | pad to 256 B |
 //                         stages x (SPB x SA + SPB x SB floats)].
-template <bool CA, bool CB, int SPB, int MINB>
+template <typename R>
+struct PPStride;  // bytes per site of the first / second operand in a stage
+template <>
+struct PPStride<float> {
+  static constexpr unsigned A = 1168, B = 1184;
+};
+template <>
+struct PPStride<double> {
+  static constexpr unsigned A = 2336, B = 2336;
+};
+
+template <typename R, bool CA, bool CB, int SPB, int MINB>
 __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const PropParams p, long long ntiles) {
   extern __shared__ __align__(128) unsigned char ptm[];
   constexpr int NCT = 12 * SPB;  // consumer threads
   constexpr int NCW = NCT / 32;  // consumer warps
-  constexpr int SA = 292, SB = 296;
-  constexpr unsigned STAGE = SPB * (SA + SB) * 4u;
+  constexpr unsigned RB = 144 * sizeof(Cx<R>);  // bytes per record
+  constexpr unsigned SA = PPStride<R>::A, SB = PPStride<R>::B;
+  constexpr unsigned STAGE = SPB * (SA + SB);
+  static_assert(SA % 16 == 0 && SB % 16 == 0 && SA >= RB && SB >= RB, "stage slots keep 16-B alignment");
   static_assert(NCT % 32 == 0, "consumer threads fill whole warps");
   static_assert(2 * SPB <= 32, "one producer lane per site and operand");
   const int S = p.stages;
@@ -526,14 +479,14 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
       }
       const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * SPB;
       const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
-      float* sa = reinterpret_cast<float*>(stages + (size_t)st * STAGE);
-      float* sb = sa + SPB * SA;
-      if (lane == 0) mbar_arrive_expect_tx(&full[st], (uint32_t)nloc * 2304u);
+      unsigned char* sa = stages + (size_t)st * STAGE;
+      unsigned char* sb = sa + SPB * SA;
+      if (lane == 0) mbar_arrive_expect_tx(&full[st], (uint32_t)nloc * 2u * RB);
       __syncwarp();
       if (lane < nloc)
-        bulk_g2s(sa + lane * SA, Ag + (site0 + lane) * 1152, 1152u, &full[st], pol);
+        bulk_g2s(sa + lane * SA, Ag + (site0 + lane) * RB, RB, &full[st], pol);
       else if (lane >= SPB && lane - SPB < nloc)
-        bulk_g2s(sb + (lane - SPB) * SB, Bg + (site0 + lane - SPB) * 1152, 1152u, &full[st], pol);
+        bulk_g2s(sb + (lane - SPB) * SB, Bg + (site0 + lane - SPB) * RB, RB, &full[st], pol);
       if (++st == S) {
         st = 0;
         round++;
@@ -545,7 +498,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
     const int ls = tid / 12, t12 = tid - ls * 12, rg = t12 >> 1, cg = t12 & 1;
     const bool minus = (p.eqop == MEQ || p.eqop == EQM);
     const bool load = (p.eqop == PEQ || p.eqop == MEQ);
-    const float z = p.negzero;
+    const float z = p.negzero;  // (F3 products)
     int st = 0;
     uint32_t par = 0;
     for (long long k = 0; k < my; k++) {
@@ -555,87 +508,140 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
       const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * SPB;
       const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
       const bool active = ok && ls < nloc;
-      const float* A = reinterpret_cast<const float*>(stages + (size_t)st * STAGE) + ls * SA;
-      const float* B = A - ls * SA + SPB * SA + ls * SB;
-      const Cx<float>* og = static_cast<const Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
-      float2 xr[2][3], xi[2][3];  // [row 2rg + i][q]: lanes = columns 2(cg + 2q), +1
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-          if (load && active) {
-            const float4 v = *reinterpret_cast<const float4*>(og + (2 * rg + i) * 12 + 4 * q);
-            xr[i][q] = make_float2(v.x, v.z);
-            xi[i][q] = make_float2(v.y, v.w);
-          } else {
-            xr[i][q] = make_float2(0.f, 0.f);
-            xi[i][q] = make_float2(0.f, 0.f);
-          }
-        }
-      if (active) {
-#pragma unroll
-        for (int kk = 0; kk < 12; kk += 2) {
-          Cx<float> a[2][2];  // element (row 2rg + i, kk + h) before conjugation
-          if constexpr (!CA) {
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-              const float4 v = *reinterpret_cast<const float4*>(A + ((2 * rg + i) * 12 + kk) * 2);
-              a[i][0] = Cx<float>{v.x, v.y};
-              a[i][1] = Cx<float>{v.z, v.w};
-            }
-          } else {  // P^+[r][kk] = conj P[kk][r]: elements (kk + h, 2rg), (kk + h, 2rg + 1) are adjacent
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const float4 v = *reinterpret_cast<const float4*>(A + ((kk + h) * 12 + 2 * rg) * 2);
-              a[0][h] = Cx<float>{v.x, v.y};
-              a[1][h] = Cx<float>{v.z, v.w};
-            }
-          }
-          // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before conjugation
-          float2 bre[2][3], bim[2][3];
-          if constexpr (!CB) {
-#pragma unroll
-            for (int h = 0; h < 2; h++)
-#pragma unroll
-              for (int q = 0; q < 3; q++) {
-                const float4 v = *reinterpret_cast<const float4*>(B + (kk + h) * 24 + 4 * (cg + 2 * q));
-                bre[h][q] = make_float2(v.x, v.z);
-                bim[h][q] = make_float2(v.y, v.w);
-              }
-          } else {  // P^+[kk][j] = conj P[j][kk]: elements (j, kk), (j, kk + 1) are adjacent
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-              const int j = 2 * (cg + 2 * q);
-              const float4 v0 = *reinterpret_cast<const float4*>(B + j * 24 + 2 * kk);
-              const float4 v1 = *reinterpret_cast<const float4*>(B + (j + 1) * 24 + 2 * kk);
-              bre[0][q] = make_float2(v0.x, v1.x);
-              bim[0][q] = make_float2(v0.y, v1.y);
-              bre[1][q] = make_float2(v0.z, v1.z);
-              bim[1][q] = make_float2(v0.w, v1.w);
-            }
-          }
-#pragma unroll
-          for (int h = 0; h < 2; h++)
-#pragma unroll
-            for (int i = 0; i < 2; i++)
-#pragma unroll
-              for (int q = 0; q < 3; q++)
-                cmac_x2<CA, CB>(xr[i][q], xi[i][q], minus, a[i][h], bre[h][q], bim[h][q], z);
-        }
-      }
-      release_stage(&empty[st], lane);  // this warp is done with the stage
-      if (!ok) {
-        *abort_flag = 1;
-        break;
-      }
-      if (ls < nloc) {
-        Cx<float>* o = static_cast<Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
+      const unsigned char* stg = stages + (size_t)st * STAGE;
+      if constexpr (sizeof(R) == 4) {
+        const float* A = reinterpret_cast<const float*>(stg + ls * SA);
+        const float* B = reinterpret_cast<const float*>(stg + SPB * SA + ls * SB);
+        const Cx<float>* og = static_cast<const Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
+        float2 xr[2][3], xi[2][3];  // [row 2rg + i][q]: lanes = columns 2(cg + 2q), +1
 #pragma unroll
         for (int i = 0; i < 2; i++)
 #pragma unroll
-          for (int q = 0; q < 3; q++)
-            *reinterpret_cast<float4*>(o + (2 * rg + i) * 12 + 4 * q) =
-                make_float4(xr[i][q].x, xi[i][q].x, xr[i][q].y, xi[i][q].y);
+          for (int q = 0; q < 3; q++) {
+            if (load && active) {
+              const float4 v = *reinterpret_cast<const float4*>(og + (2 * rg + i) * 12 + 4 * q);
+              xr[i][q] = make_float2(v.x, v.z);
+              xi[i][q] = make_float2(v.y, v.w);
+            } else {
+              xr[i][q] = make_float2(0.f, 0.f);
+              xi[i][q] = make_float2(0.f, 0.f);
+            }
+          }
+        if (active) {
+#pragma unroll
+          for (int kk = 0; kk < 12; kk += 2) {
+            Cx<float> a[2][2];  // element (row 2rg + i, kk + h) before conjugation
+            if constexpr (!CA) {
+#pragma unroll
+              for (int i = 0; i < 2; i++) {
+                const float4 v = *reinterpret_cast<const float4*>(A + ((2 * rg + i) * 12 + kk) * 2);
+                a[i][0] = Cx<float>{v.x, v.y};
+                a[i][1] = Cx<float>{v.z, v.w};
+              }
+            } else {  // P^+[r][kk] = conj P[kk][r]: elements (kk + h, 2rg), (kk + h, 2rg + 1) are adjacent
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const float4 v = *reinterpret_cast<const float4*>(A + ((kk + h) * 12 + 2 * rg) * 2);
+                a[0][h] = Cx<float>{v.x, v.y};
+                a[1][h] = Cx<float>{v.z, v.w};
+              }
+            }
+            // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before conjugation
+            float2 bre[2][3], bim[2][3];
+            if constexpr (!CB) {
+#pragma unroll
+              for (int h = 0; h < 2; h++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                  const float4 v = *reinterpret_cast<const float4*>(B + (kk + h) * 24 + 4 * (cg + 2 * q));
+                  bre[h][q] = make_float2(v.x, v.z);
+                  bim[h][q] = make_float2(v.y, v.w);
+                }
+            } else {  // P^+[kk][j] = conj P[j][kk]: elements (j, kk), (j, kk + 1) are adjacent
+#pragma unroll
+              for (int q = 0; q < 3; q++) {
+                const int j = 2 * (cg + 2 * q);
+                const float4 v0 = *reinterpret_cast<const float4*>(B + j * 24 + 2 * kk);
+                const float4 v1 = *reinterpret_cast<const float4*>(B + (j + 1) * 24 + 2 * kk);
+                bre[0][q] = make_float2(v0.x, v1.x);
+                bim[0][q] = make_float2(v0.y, v1.y);
+                bre[1][q] = make_float2(v0.z, v1.z);
+                bim[1][q] = make_float2(v0.w, v1.w);
+              }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+#pragma unroll
+              for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+                  cmac_x2<CA, CB>(xr[i][q], xi[i][q], minus, a[i][h], bre[h][q], bim[h][q], z);
+          }
+        }
+        release_stage(&empty[st], lane);  // this warp is done with the stage
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+        if (ls < nloc) {
+          Cx<float>* o = static_cast<Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+              *reinterpret_cast<float4*>(o + (2 * rg + i) * 12 + 4 * q) =
+                  make_float4(xr[i][q].x, xi[i][q].x, xr[i][q].y, xi[i][q].y);
+        }
+      } else {
+        // D3: thread (rg, cg) accumulates rows 2rg, 2rg+1 at columns cg + 2q,
+        // q = 0..5, with cmac<CA, CB>
+        const Cx<double>* A = reinterpret_cast<const Cx<double>*>(stg + ls * SA);
+        const Cx<double>* B = reinterpret_cast<const Cx<double>*>(stg + SPB * SA + ls * SB);
+        Cx<double>* o = static_cast<Cx<double>*>(p.out) + (site0 + ls) * 144 + cg;
+        Cx<double> x[2][6];
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int q = 0; q < 6; q++) {
+            if (load && active) {
+              const double2 v = *reinterpret_cast<const double2*>(o + (2 * rg + i) * 12 + 2 * q);
+              x[i][q] = Cx<double>{v.x, v.y};
+            } else {
+              x[i][q] = Cx<double>{0.0, 0.0};
+            }
+          }
+        if (active) {
+#pragma unroll 2
+          for (int kk = 0; kk < 12; kk++) {
+            Cx<double> a[2];  // element (row 2rg + i, kk) before conjugation (P^+[r][kk] = conj P[kk][r])
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+              const double2 v =
+                  *reinterpret_cast<const double2*>(A + (CA ? kk * 12 + 2 * rg + i : (2 * rg + i) * 12 + kk));
+              a[i] = Cx<double>{v.x, v.y};
+            }
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+              const int j = cg + 2 * q;  // P^+[kk][j] = conj P[j][kk]
+              const double2 v = *reinterpret_cast<const double2*>(B + (CB ? j * 12 + kk : kk * 12 + j));
+              const Cx<double> bv{v.x, v.y};
+#pragma unroll
+              for (int i = 0; i < 2; i++) cmac<CA, CB>(x[i][q], minus, a[i], bv);
+            }
+          }
+        }
+        release_stage(&empty[st], lane);  // this warp is done with the stage
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+        if (ls < nloc) {
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+              *reinterpret_cast<double2*>(o + (2 * rg + i) * 12 + 2 * q) = make_double2(x[i][q].re, x[i][q].im);
+        }
       }
       if (++st == S) {
         st = 0;
@@ -654,7 +660,10 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
 }
 
 // shared-memory bytes of prop_pp_tma_kernel<.., SPB> with `stages` stages
-constexpr size_t pp_tma_smem(int spb, int stages) { return 256 + (size_t)stages * spb * (292 + 296) * 4; }
+template <typename R>
+constexpr size_t pp_tma_smem(int spb, int stages) {
+  return 256 + (size_t)stages * spb * (PPStride<R>::A + PPStride<R>::B);
+}
 
 // blocks per SM of a kernel at (threads, smem), raising its dynamic
 // shared-memory limit once per device
@@ -740,28 +749,24 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
                         p.vec_out;
     if (!contig) {
       prop_pp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
-    } else if constexpr (sizeof(R) == 8) {
-      constexpr int SPB = 8;  // D3: one tile per block (the pipelined form's prefetch registers would not fit)
-      const size_t smem = (size_t)SPB * 144 * sizeof(Cx<R>);
-      const long long blocks = ((long long)n + SPB - 1) / SPB;
-      prop_pp_rows_kernel<R, CA, CB, SPB><<<(unsigned)blocks, 12 * SPB, smem, st>>>(p);
     } else {
-      // F3: bulk-copy pipeline, tiles of 8 sites, 96 consumer threads + one
-      // producer warp per block, three stages (57 KB): four blocks per SM at
-      // up to 128 registers.  Measured on B200 (131,072 sites): 90 us, where
-      // two stages took 92 us and five or six blocks per SM at 80-96
+      // bulk-copy pipeline, tiles of 8 sites, 96 consumer threads + one
+      // producer warp per block.  F3: three stages (57 KB), four blocks per
+      // SM at up to 128 registers; measured on B200 (131,072 sites) 90 us,
+      // where two stages took 92 us and five or six blocks per SM at 80-96
       // registers 95-98 us (fewer registers cost more than the extra warps
-      // gain).
+      // gain).  D3: two stages (75 KB), three blocks per SM.
       constexpr int SPB = 8;
-      p.stages = 3;
+      constexpr bool F32 = sizeof(R) == 4;
+      constexpr int MINB = F32 ? 4 : 3;
+      p.stages = F32 ? 3 : 2;
       p.err = device_error_word();
-      const size_t smem = pp_tma_smem(SPB, p.stages);
+      const size_t smem = pp_tma_smem<R>(SPB, p.stages);
       const long long ntiles = ((long long)n + SPB - 1) / SPB;
-      constexpr int MINB = 4;
-      const void* fn = reinterpret_cast<const void*>(&prop_pp_tma_kernel<CA, CB, SPB, MINB>);
+      const void* fn = reinterpret_cast<const void*>(&prop_pp_tma_kernel<R, CA, CB, SPB, MINB>);
       long long blocks = (long long)prop_blocks_per_sm(fn, 12 * SPB + 32, smem) * device_sm_count();
       if (blocks > ntiles) blocks = ntiles;
-      prop_pp_tma_kernel<CA, CB, SPB, MINB><<<(unsigned)blocks, 12 * SPB + 32, smem, st>>>(p, ntiles);
+      prop_pp_tma_kernel<R, CA, CB, SPB, MINB><<<(unsigned)blocks, 12 * SPB + 32, smem, st>>>(p, ntiles);
     }
   }
   check_launch(kid);
