@@ -41,85 +41,86 @@ struct PropParams {
   long long n;
   int eqop;
   int vec_a, vec_b, vec_out;  // 16-B vector access allowed (contiguous, aligned)
-  float negzero;              // -0.0f, passed at run time (see mul_rn_x2)
+  float negzero;              // -0.0f, passed at run time (see f2_mul)
   unsigned* err;              // device error word (bounded waits of the bulk-copy P * P)
   int stages;                 // stage ring depth of the bulk-copy P * P
 };
 
 // ---------------------------------------------------------------------------
 // Packed FP32x2 arithmetic with per-lane rounding identical to the scalar
-// __fmul_rn / __fadd_rn / __fsub_rn.  The packed add and sub are used as
-// they are.  A packed product followed by a packed add is fused into one
-// multiply-add by the compiler even with explicit .rn rounding (measured on
-// sm_100a: every result equal to fmaf, none to the separately rounded pair),
-// so the product is written as fma(a, b, z) with z = -0: a*b + (-0) rounds
-// exactly as a*b alone, signed zeros included, and because z is a kernel
+// __fmul_rn / __fadd_rn / __fsub_rn.  A pair of floats lives in one 64-bit
+// register (F2: low lane first), so that a chain of packed operations needs
+// no packing between them.  The packed add and sub are used as they are.  A
+// packed product followed by a packed add is fused into one multiply-add by
+// the compiler even with explicit .rn rounding (measured on sm_100a: every
+// result equal to fmaf, none to the separately rounded pair), so the product
+// is written as fma(a, b, z) with z = (-0, -0): a*b + (-0) rounds exactly as
+// a*b alone, signed zeros included, and because z comes from a kernel
 // argument the compiler cannot fold it into a plain product again.
-__device__ __forceinline__ float2 mul_rn_x2(float2 a, float2 b, float z) {
-  float2 r;
-  asm("{.reg .b64 pa, pb, pc, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\t"
-      "mov.b64 pb, {%4, %5};\n\t"
-      "mov.b64 pc, {%6, %6};\n\t"
-      "fma.rn.f32x2 pd, pa, pb, pc;\n\t"
-      "mov.b64 {%0, %1}, pd;}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(z));
+using F2 = unsigned long long;
+__device__ __forceinline__ F2 f2_pack(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
   return r;
 }
-__device__ __forceinline__ float2 add_rn_x2(float2 a, float2 b) {
-  float2 r;
-  asm("{.reg .b64 pa, pb, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\t"
-      "mov.b64 pb, {%4, %5};\n\t"
-      "add.rn.f32x2 pd, pa, pb;\n\t"
-      "mov.b64 {%0, %1}, pd;}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+__device__ __forceinline__ float f2_lo(F2 v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float f2_hi(F2 v) { return __uint_as_float((unsigned)(v >> 32)); }
+__device__ __forceinline__ F2 f2_neg(F2 v) { return v ^ 0x8000000080000000ull; }  // both lanes, exactly
+__device__ __forceinline__ F2 f2_mul(F2 a, F2 b, F2 z) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(z));
   return r;
 }
-__device__ __forceinline__ float2 sub_rn_x2(float2 a, float2 b) {
-  float2 r;
-  asm("{.reg .b64 pa, pb, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\t"
-      "mov.b64 pb, {%4, %5};\n\t"
-      "sub.rn.f32x2 pd, pa, pb;\n\t"
-      "mov.b64 {%0, %1}, pd;}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+__device__ __forceinline__ F2 f2_add(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ F2 f2_sub(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
 
 // x (+|-)= a * b for two output columns at once: lanes hold columns j0, j1
-// (b's real parts bre, imaginary parts bim), a is broadcast.  Per lane the
-// operations and their order are cmac<CA, CB>'s.
+// (b's real parts bre, imaginary parts bim), a is broadcast (ar = (a.re,
+// a.re), ai = (a.im, a.im)).  Per lane the operations and their order are
+// cmac<CA, CB>'s.
+template <bool CA, bool CB>
+__device__ __forceinline__ void cmac_f2(F2& xre, F2& xim, bool minus, F2 ar, F2 ai, F2 bre, F2 bim, F2 z) {
+  const F2 p1 = f2_mul(ar, bre, z), p2 = f2_mul(ai, bim, z);
+  const F2 p3 = f2_mul(ar, bim, z), p4 = f2_mul(ai, bre, z);
+  F2 re, im;
+  if constexpr (!CA && !CB) {
+    re = f2_sub(p1, p2);
+    im = f2_add(p3, p4);
+  } else if constexpr (CA && !CB) {
+    re = f2_add(p1, p2);
+    im = f2_sub(p3, p4);
+  } else if constexpr (!CA && CB) {
+    re = f2_add(p1, p2);
+    im = f2_sub(p4, p3);
+  } else {
+    re = f2_sub(p1, p2);
+    im = f2_sub(f2_neg(p3), p4);  // (-a.re) b.im = -(a.re b.im) exactly
+  }
+  if (minus) {
+    xre = f2_sub(xre, re);
+    xim = f2_sub(xim, im);
+  } else {
+    xre = f2_add(xre, re);
+    xim = f2_add(xim, im);
+  }
+}
+// the same on float2 values (one complex a)
 template <bool CA, bool CB>
 __device__ __forceinline__ void cmac_x2(float2& xre, float2& xim, bool minus, Cx<float> a, float2 bre, float2 bim,
                                         float z) {
-  const float2 ar = make_float2(a.re, a.re), ai = make_float2(a.im, a.im);
-  const float2 p1 = mul_rn_x2(ar, bre, z), p2 = mul_rn_x2(ai, bim, z);
-  const float2 p3 = mul_rn_x2(ar, bim, z), p4 = mul_rn_x2(ai, bre, z);
-  float2 re, im;
-  if constexpr (!CA && !CB) {
-    re = sub_rn_x2(p1, p2);
-    im = add_rn_x2(p3, p4);
-  } else if constexpr (CA && !CB) {
-    re = add_rn_x2(p1, p2);
-    im = sub_rn_x2(p3, p4);
-  } else if constexpr (!CA && CB) {
-    re = add_rn_x2(p1, p2);
-    im = sub_rn_x2(p4, p3);
-  } else {
-    re = sub_rn_x2(p1, p2);
-    im = sub_rn_x2(make_float2(-p3.x, -p3.y), p4);  // (-a.re) b.im = -(a.re b.im) exactly
-  }
-  if (minus) {
-    xre = sub_rn_x2(xre, re);
-    xim = sub_rn_x2(xim, im);
-  } else {
-    xre = add_rn_x2(xre, re);
-    xim = add_rn_x2(xim, im);
-  }
+  F2 r = f2_pack(xre.x, xre.y), i = f2_pack(xim.x, xim.y);
+  cmac_f2<CA, CB>(r, i, minus, f2_pack(a.re, a.re), f2_pack(a.im, a.im), f2_pack(bre.x, bre.y),
+                  f2_pack(bim.x, bim.y), f2_pack(z, z));
+  xre = make_float2(f2_lo(r), f2_hi(r));
+  xim = make_float2(f2_lo(i), f2_hi(i));
 }
 
 template <typename R>
@@ -498,7 +499,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
     const int ls = tid / 12, t12 = tid - ls * 12, rg = t12 >> 1, cg = t12 & 1;
     const bool minus = (p.eqop == MEQ || p.eqop == EQM);
     const bool load = (p.eqop == PEQ || p.eqop == MEQ);
-    const float z = p.negzero;  // (F3 products)
+    const F2 z2 = f2_pack(p.negzero, p.negzero);  // (F3 products)
     int st = 0;
     uint32_t par = 0;
     for (long long k = 0; k < my; k++) {
@@ -513,49 +514,54 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
         const float* A = reinterpret_cast<const float*>(stg + ls * SA);
         const float* B = reinterpret_cast<const float*>(stg + SPB * SA + ls * SB);
         const Cx<float>* og = static_cast<const Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
-        float2 xr[2][3], xi[2][3];  // [row 2rg + i][q]: lanes = columns 2(cg + 2q), +1
+        F2 xr[2][3], xi[2][3];  // [row 2rg + i][q]: lanes = columns 2(cg + 2q), +1
 #pragma unroll
         for (int i = 0; i < 2; i++)
 #pragma unroll
           for (int q = 0; q < 3; q++) {
             if (load && active) {
               const float4 v = *reinterpret_cast<const float4*>(og + (2 * rg + i) * 12 + 4 * q);
-              xr[i][q] = make_float2(v.x, v.z);
-              xi[i][q] = make_float2(v.y, v.w);
+              xr[i][q] = f2_pack(v.x, v.z);
+              xi[i][q] = f2_pack(v.y, v.w);
             } else {
-              xr[i][q] = make_float2(0.f, 0.f);
-              xi[i][q] = make_float2(0.f, 0.f);
+              xr[i][q] = 0ull;  // (+0, +0)
+              xi[i][q] = 0ull;
             }
           }
         if (active) {
 #pragma unroll
           for (int kk = 0; kk < 12; kk += 2) {
-            Cx<float> a[2][2];  // element (row 2rg + i, kk + h) before conjugation
+            // element (row 2rg + i, kk + h) before conjugation, broadcast to both lanes
+            F2 ar[2][2], ai[2][2];
             if constexpr (!CA) {
 #pragma unroll
               for (int i = 0; i < 2; i++) {
                 const float4 v = *reinterpret_cast<const float4*>(A + ((2 * rg + i) * 12 + kk) * 2);
-                a[i][0] = Cx<float>{v.x, v.y};
-                a[i][1] = Cx<float>{v.z, v.w};
+                ar[i][0] = f2_pack(v.x, v.x);
+                ai[i][0] = f2_pack(v.y, v.y);
+                ar[i][1] = f2_pack(v.z, v.z);
+                ai[i][1] = f2_pack(v.w, v.w);
               }
             } else {  // P^+[r][kk] = conj P[kk][r]: elements (kk + h, 2rg), (kk + h, 2rg + 1) are adjacent
 #pragma unroll
               for (int h = 0; h < 2; h++) {
                 const float4 v = *reinterpret_cast<const float4*>(A + ((kk + h) * 12 + 2 * rg) * 2);
-                a[0][h] = Cx<float>{v.x, v.y};
-                a[1][h] = Cx<float>{v.z, v.w};
+                ar[0][h] = f2_pack(v.x, v.x);
+                ai[0][h] = f2_pack(v.y, v.y);
+                ar[1][h] = f2_pack(v.z, v.z);
+                ai[1][h] = f2_pack(v.w, v.w);
               }
             }
             // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before conjugation
-            float2 bre[2][3], bim[2][3];
+            F2 bre[2][3], bim[2][3];
             if constexpr (!CB) {
 #pragma unroll
               for (int h = 0; h < 2; h++)
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                   const float4 v = *reinterpret_cast<const float4*>(B + (kk + h) * 24 + 4 * (cg + 2 * q));
-                  bre[h][q] = make_float2(v.x, v.z);
-                  bim[h][q] = make_float2(v.y, v.w);
+                  bre[h][q] = f2_pack(v.x, v.z);
+                  bim[h][q] = f2_pack(v.y, v.w);
                 }
             } else {  // P^+[kk][j] = conj P[j][kk]: elements (j, kk), (j, kk + 1) are adjacent
 #pragma unroll
@@ -563,10 +569,10 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
                 const int j = 2 * (cg + 2 * q);
                 const float4 v0 = *reinterpret_cast<const float4*>(B + j * 24 + 2 * kk);
                 const float4 v1 = *reinterpret_cast<const float4*>(B + (j + 1) * 24 + 2 * kk);
-                bre[0][q] = make_float2(v0.x, v1.x);
-                bim[0][q] = make_float2(v0.y, v1.y);
-                bre[1][q] = make_float2(v0.z, v1.z);
-                bim[1][q] = make_float2(v0.w, v1.w);
+                bre[0][q] = f2_pack(v0.x, v1.x);
+                bim[0][q] = f2_pack(v0.y, v1.y);
+                bre[1][q] = f2_pack(v0.z, v1.z);
+                bim[1][q] = f2_pack(v0.w, v1.w);
               }
             }
 #pragma unroll
@@ -575,7 +581,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
               for (int i = 0; i < 2; i++)
 #pragma unroll
                 for (int q = 0; q < 3; q++)
-                  cmac_x2<CA, CB>(xr[i][q], xi[i][q], minus, a[i][h], bre[h][q], bim[h][q], z);
+                  cmac_f2<CA, CB>(xr[i][q], xi[i][q], minus, ar[i][h], ai[i][h], bre[h][q], bim[h][q], z2);
           }
         }
         release_stage(&empty[st], lane);  // this warp is done with the stage
@@ -590,7 +596,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
 #pragma unroll
             for (int q = 0; q < 3; q++)
               *reinterpret_cast<float4*>(o + (2 * rg + i) * 12 + 4 * q) =
-                  make_float4(xr[i][q].x, xi[i][q].x, xr[i][q].y, xi[i][q].y);
+                  make_float4(f2_lo(xr[i][q]), f2_lo(xi[i][q]), f2_hi(xr[i][q]), f2_hi(xi[i][q]));
         }
       } else {
         // D3: thread (rg, cg) accumulates rows 2rg, 2rg+1 at columns cg + 2q,
