@@ -100,6 +100,13 @@ struct BatchPlan {
   size_t smem;
 };
 
+// The field of tile g given the previous answer f (or -1): tiles come in
+// runs, so a range check usually settles it without the search.
+__device__ __forceinline__ int find_field(const long long* tile0, int nf, long long g);
+__device__ __forceinline__ int field_of(const long long* tile0, int nf, long long g, int f) {
+  if (f >= 0 && tile0[f] <= g && (f + 1 == nf || g < tile0[f + 1])) return f;
+  return find_field(tile0, nf, g);
+}
 __device__ __forceinline__ int find_field(const long long* tile0, int nf, long long g) {
   int lo = 0, hi = nf - 1;  // last field with tile0 <= g
   while (lo < hi) {
@@ -635,7 +642,7 @@ __global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) 
           break;
         }
         const long long g = tile_of(k);
-        const BField& F = cached_field_1(p, find_field(tile0, p.nfields, g), cached, desc);
+        const BField& F = cached_field_1(p, field_of(tile0, p.nfields, g, cached), cached, desc);
         const long long site0 = (g - F.tile0) * T;
         unsigned char* st = stages + (size_t)s * p.stage_bytes;
         if (!F.direct && site0 + T <= F.n) {
@@ -670,7 +677,7 @@ __global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) 
         break;
       }
       const long long g = tile_of(k);
-      const BField& F = cached_field(p, find_field(tile0, p.nfields, g), cached, desc, lane);
+      const BField& F = cached_field(p, field_of(tile0, p.nfields, g, cached), cached, desc, lane);
       const long long site0 = (g - F.tile0) * T;
       const int t = warp * 32 + lane;
       const long long i = site0 + t;
