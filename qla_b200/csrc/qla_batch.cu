@@ -428,6 +428,18 @@ struct Shape {
 };
 struct GenericShape {};
 
+// The operand of a compiled shape's first step that is gathered (1: a, 2: b,
+// 0: none) and its record length in complex numbers.
+template <class SH>
+struct LeadGather {
+  static constexpr int which = 0, n = 0;
+};
+template <class S0, class... R>
+struct LeadGather<Shape<S0, R...>> {
+  static constexpr int which = S0::sb == SRC_GATHER ? 2 : S0::sa == SRC_GATHER ? 1 : 0;
+  static constexpr int n = which == 2 ? kncplx(S0::kb) : which == 1 ? kncplx(S0::ka) : 0;
+};
+
 // r = u * u2[nbr], w = r * v                          (config 4)
 using ShapeConfig4 = Shape<StepShape<BOP_LMULT, BK_M, BK_M, 0, 0, SRC_CONTIG, SRC_GATHER, EQ>,
                            StepShape<BOP_LMULT, BK_M, BK_V, 0, 0, SRC_PREV, SRC_CONTIG, EQ>>;
@@ -684,6 +696,16 @@ __global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) 
       // staged: a full tile of a 16-B aligned field, in the stage; else the
       // same program with plain loads and stores (partial / unaligned tiles)
       const bool staged = !F.direct && site0 + T <= F.n;
+      // a compiled shape that starts with a gather: when the block's next tile
+      // is the next tile of this field, load this lane's index of it now and
+      // prefetch its gathered record into L2 after this tile's arithmetic
+      int pf_j = -1;
+      if constexpr (LeadGather<SH>::which != 0) {
+        if (k + 1 < my && tile_of(k + 1) == g + 1 && i + T < F.n) {
+          const BStream& G = F.s[LeadGather<SH>::which == 2 ? F.st[0].b : F.st[0].a];
+          pf_j = __ldg(G.idx + i + T);
+        }
+      }
       unsigned char* ob = myout;
       if (staged) {
         if (lane == 0) bulk_wait_read<0>();  // the slice is no longer read by this warp's previous store
@@ -694,6 +716,15 @@ __global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) 
       if (staged || i < F.n)  // one call site: the program is inlined once
         run_program<MC, SH>(F, SiteSrc{staged ? stages + (size_t)s * p.stage_bytes : nullptr, t, i, p.err, regs, T},
                             staged ? ob : nullptr, lane);
+      if constexpr (LeadGather<SH>::which != 0) {
+        const BStream& G = F.s[LeadGather<SH>::which == 2 ? F.st[0].b : F.st[0].a];
+        if (pf_j >= 0 && (G.nsrc <= 0 || pf_j < G.nsrc)) {  // only an index the gather would dereference
+          constexpr long long RBG = LeadGather<SH>::n * 8;
+          const char* q = G.base + (long long)pf_j * RBG;
+          prefetch_l2(q);
+          prefetch_l2(q + RBG - 8);
+        }
+      }
       if (staged) {
         // every lane orders its reads of the stage and its writes of the
         // slice before the async proxy: the slice's bulk stores below, and

@@ -326,6 +326,9 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Prefetch the L2 line holding a global address (no register result).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // L2 eviction policies for streamed data (read once / written once).
 __device__ __forceinline__ uint64_t policy_evict_first() {
   uint64_t p;
