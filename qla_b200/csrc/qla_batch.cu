@@ -596,7 +596,11 @@ constexpr int kBatchThreadsMax = 160;
 template <int MC, class SH>
 constexpr int batch_min_blocks() {
   constexpr bool compiled = !std::is_same<SH, GenericShape>::value && !std::is_same<SH, MultiShape>::value;
-  return MC == 9 ? (compiled ? 4 : 3) : (compiled ? 3 : 2);
+  // (the multi-shape kernel at 12 complex numbers: three blocks with spills
+  // measured 0.39 of HBM on a config-4 / hop mix, two 0.38, one at 254
+  // registers 0.32)
+  constexpr bool multi = std::is_same<SH, MultiShape>::value;
+  return MC == 9 ? (compiled ? 4 : 3) : (compiled || multi ? 3 : 2);
 }
 template <int MC, class SH>
 __global__ void __launch_bounds__(kBatchThreadsMax, batch_min_blocks<MC, SH>()) batch_program_kernel(
