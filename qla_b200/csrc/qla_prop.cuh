@@ -17,7 +17,7 @@
 //           P[ic][is][kc][js..js+1] serves all three output colours jc;
 //   P * P   contiguous operands through a bulk-copy (TMA) pipeline of
 //           8-site tiles, 12 threads per site, 2 output rows x 6 columns per
-//           thread (F3 in packed FP32x2 arithmetic; prop_pp_tma_kernel);
+//           thread (F3 in packed FP32x2 arithmetic; prop_tma_kernel);
 //           gang, pointer or unaligned operands 6 (F3) / 12 (D3) threads per
 //           site, a column block of the second operand in registers
 //           (prop_pp_kernel).
@@ -121,6 +121,48 @@ __device__ __forceinline__ void cmac_x2(float2& xre, float2& xim, bool minus, Cx
                   f2_pack(bim.x, bim.y), f2_pack(z, z));
   xre = make_float2(f2_lo(r), f2_hi(r));
   xim = make_float2(f2_lo(i), f2_hi(i));
+}
+
+// one complex number as a single 8-B (F3) / 16-B (D3) access (the address
+// is aligned to the complex number's size)
+template <typename R>
+__device__ __forceinline__ Cx<R> ldc(const Cx<R>* q) {
+  if constexpr (sizeof(R) == 4) {
+    const float2 v = *reinterpret_cast<const float2*>(q);
+    return Cx<R>{v.x, v.y};
+  } else {
+    const double2 v = *reinterpret_cast<const double2*>(q);
+    return Cx<R>{v.x, v.y};
+  }
+}
+// two consecutive complex numbers (16-B aligned): one 16-B access in F3
+template <typename R>
+__device__ __forceinline__ void ldc2(const Cx<R>* q, Cx<R>& u, Cx<R>& v) {
+  if constexpr (sizeof(R) == 4) {
+    const float4 w = *reinterpret_cast<const float4*>(q);
+    u = Cx<R>{w.x, w.y};
+    v = Cx<R>{w.z, w.w};
+  } else {
+    const double2 a = reinterpret_cast<const double2*>(q)[0], b = reinterpret_cast<const double2*>(q)[1];
+    u = Cx<R>{a.x, a.y};
+    v = Cx<R>{b.x, b.y};
+  }
+}
+template <typename R>
+__device__ __forceinline__ void stc2(Cx<R>* q, Cx<R> u, Cx<R> v) {
+  if constexpr (sizeof(R) == 4) {
+    *reinterpret_cast<float4*>(q) = make_float4(u.re, u.im, v.re, v.im);
+  } else {
+    reinterpret_cast<double2*>(q)[0] = make_double2(u.re, u.im);
+    reinterpret_cast<double2*>(q)[1] = make_double2(v.re, v.im);
+  }
+}
+template <typename R>
+__device__ __forceinline__ void stc(Cx<R>* q, Cx<R> v) {
+  if constexpr (sizeof(R) == 4)
+    *reinterpret_cast<float2*>(q) = make_float2(v.re, v.im);
+  else
+    *reinterpret_cast<double2*>(q) = make_double2(v.re, v.im);
 }
 
 template <typename R>
@@ -423,26 +465,38 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
 //
 // Dynamic shared memory: [full[8] | empty[8] | abort flag | pad to 256 B |
 //                         stages x (SPB x SA + SPB x SB floats)].
-template <typename R>
-struct PPStride;  // bytes per site of the first / second operand in a stage
-template <>
-struct PPStride<float> {
-  static constexpr unsigned A = 1168, B = 1184;
-};
-template <>
-struct PPStride<double> {
-  static constexpr unsigned A = 2336, B = 2336;
+// Stage slots of the bulk-copy kernel per operand: record bytes and slot
+// stride (bytes), chosen so that the sites one warp covers spread over the
+// shared-memory banks.  P records, one bulk copy per site into padded slots:
+// F3 1168 (first operand of P * P, M * P and P * M) / 1184 (second operand of
+// P * P), D3 2336.  M records (72 / 144 B, not a multiple of 16), one bulk
+// copy per full tile into consecutive slots: three sites 72 / 144 B apart
+// read distinct banks.
+template <typename R, int KIND>
+struct PTSlots {
+  static constexpr unsigned PREC = 144 * sizeof(Cx<R>), MREC = 9 * sizeof(Cx<R>);
+  static constexpr unsigned PSLOT_A = sizeof(R) == 4 ? 1168 : 2336, PSLOT_B = sizeof(R) == 4 ? 1184 : 2336;
+  static constexpr unsigned MSLOT = MREC;
+  static constexpr unsigned RA = KIND == PK_MP ? MREC : PREC;  // first operand
+  static constexpr unsigned RB = KIND == PK_PM ? MREC : PREC;  // second operand
+  static constexpr unsigned A = KIND == PK_MP ? MSLOT : PSLOT_A;
+  static constexpr unsigned B = KIND == PK_PM ? MSLOT : (KIND == PK_PP ? PSLOT_B : PSLOT_A);
 };
 
-template <typename R, bool CA, bool CB, int SPB, int MINB>
-__global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const PropParams p, long long ntiles) {
+template <typename R, int KIND, bool CA, bool CB, int SPB, int MINB>
+__global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const PropParams p, long long ntiles) {
   extern __shared__ __align__(128) unsigned char ptm[];
   constexpr int NCT = 12 * SPB;  // consumer threads
   constexpr int NCW = NCT / 32;  // consumer warps
-  constexpr unsigned RB = 144 * sizeof(Cx<R>);  // bytes per record
-  constexpr unsigned SA = PPStride<R>::A, SB = PPStride<R>::B;
+  using SL = PTSlots<R, KIND>;
+  constexpr unsigned RA = SL::RA, RB = SL::RB;  // bytes per record of each operand
+  constexpr unsigned SA = SL::A, SB = SL::B;
   constexpr unsigned STAGE = SPB * (SA + SB);
-  static_assert(SA % 16 == 0 && SB % 16 == 0 && SA >= RB && SB >= RB, "stage slots keep 16-B alignment");
+  // per-site (P) slots start on 16 B; the M slots of a tile form one region
+  // whose size keeps the next region on 16 B
+  static_assert((KIND == PK_MP ? (SPB * SA) % 16 : SA % 16) == 0 &&
+                    (KIND == PK_PM ? (SPB * SB) % 16 : SB % 16) == 0 && SA >= RA && SB >= RB,
+                "stage slots keep 16-B alignment");
   static_assert(NCT % 32 == 0, "consumer threads fill whole warps");
   static_assert(2 * SPB <= 32, "one producer lane per site and operand");
   const int S = p.stages;
@@ -482,12 +536,27 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
       const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
       unsigned char* sa = stages + (size_t)st * STAGE;
       unsigned char* sb = sa + SPB * SA;
-      if (lane == 0) mbar_arrive_expect_tx(&full[st], (uint32_t)nloc * 2u * RB);
+      if (lane == 0) mbar_arrive_expect_tx(&full[st], (uint32_t)nloc * (RA + RB));
       __syncwarp();
-      if (lane < nloc)
-        bulk_g2s(sa + lane * SA, Ag + (site0 + lane) * RB, RB, &full[st], pol);
-      else if (lane >= SPB && lane - SPB < nloc)
-        bulk_g2s(sb + (lane - SPB) * SB, Bg + (site0 + lane - SPB) * RB, RB, &full[st], pol);
+      if constexpr (KIND == PK_PP) {
+        if (lane < nloc)
+          bulk_g2s(sa + lane * SA, Ag + (site0 + lane) * RA, RA, &full[st], pol);
+        else if (lane >= SPB && lane - SPB < nloc)
+          bulk_g2s(sb + (lane - SPB) * SB, Bg + (site0 + lane - SPB) * RB, RB, &full[st], pol);
+      } else {
+        // P records one per site; the M records of the tile (always a full
+        // tile here: SPB x 72 / 144 B from a 16-B aligned start) in one copy
+        constexpr bool MP = KIND == PK_MP;
+        constexpr unsigned PREC = SL::PREC, MREC = SL::MREC, PS = MP ? SB : SA;
+        unsigned char* pslots = MP ? sb : sa;
+        unsigned char* mslots = MP ? sa : sb;
+        const char* Pg = MP ? Bg : Ag;
+        const char* Mg = MP ? Ag : Bg;
+        if (lane < nloc)
+          bulk_g2s(pslots + lane * PS, Pg + (site0 + lane) * PREC, PREC, &full[st], pol);
+        else if (lane == 31)
+          bulk_g2s(mslots, Mg + site0 * MREC, (unsigned)nloc * MREC, &full[st], pol);
+      }
       if (++st == S) {
         st = 0;
         round++;
@@ -510,7 +579,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
       const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
       const bool active = ok && ls < nloc;
       const unsigned char* stg = stages + (size_t)st * STAGE;
-      if constexpr (sizeof(R) == 4) {
+      if constexpr (KIND == PK_PP && sizeof(R) == 4) {
         const float* A = reinterpret_cast<const float*>(stg + ls * SA);
         const float* B = reinterpret_cast<const float*>(stg + SPB * SA + ls * SB);
         const Cx<float>* og = static_cast<const Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
@@ -598,7 +667,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
               *reinterpret_cast<float4*>(o + (2 * rg + i) * 12 + 4 * q) =
                   make_float4(f2_lo(xr[i][q]), f2_lo(xi[i][q]), f2_hi(xr[i][q]), f2_hi(xi[i][q]));
         }
-      } else {
+      } else if constexpr (KIND == PK_PP) {
         // D3: thread (rg, cg) accumulates rows 2rg, 2rg+1 at columns cg + 2q,
         // q = 0..5, with cmac<CA, CB>
         const Cx<double>* A = reinterpret_cast<const Cx<double>*>(stg + ls * SA);
@@ -648,6 +717,71 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
             for (int q = 0; q < 6; q++)
               *reinterpret_cast<double2*>(o + (2 * rg + i) * 12 + 2 * q) = make_double2(x[i][q].re, x[i][q].im);
         }
+      } else {
+        // M * P: thread (is, jc) of a site accumulates outputs (ic, is, jc, js),
+        // ic = 0..2, js = 0..3; P * M: thread (ic, is) accumulates outputs
+        // (ic, is, jc, js), jc = 0..2, js = 0..3.  Scalar cmac<CA, CB> (these
+        // products have a quarter of P * P's arithmetic), k in order.
+        constexpr bool MP = KIND == PK_MP;
+        const Cx<R>* A = reinterpret_cast<const Cx<R>*>(stg + ls * SA);
+        const Cx<R>* B = reinterpret_cast<const Cx<R>*>(stg + SPB * SA + ls * SB);
+        const int u = MP ? t12 / 3 : t12 / 4, v = MP ? t12 % 3 : t12 % 4;  // (is, jc) or (ic, is)
+        Cx<R>* o = static_cast<Cx<R>*>(p.out) + (site0 + ls) * 144;
+        // output (w, js) of this thread: w = ic (M * P) or jc (P * M)
+        auto oidx = [&](int w) { return MP ? p_idx(w, u, v, 0, false) : p_idx(u, v, w, 0, false); };
+        Cx<R> x[3][4];
+#pragma unroll
+        for (int w = 0; w < 3; w++)
+#pragma unroll
+          for (int js = 0; js < 4; js += 2) {
+            if (load && active) {
+              ldc2(o + oidx(w) + js, x[w][js], x[w][js + 1]);
+            } else {
+              x[w][js] = Cx<R>{R(0), R(0)};
+              x[w][js + 1] = Cx<R>{R(0), R(0)};
+            }
+          }
+        if (active) {
+#pragma unroll
+          for (int kc = 0; kc < 3; kc++) {
+            Cx<R> pv[4], mv[3];  // the P operand's four elements, the M operand's three
+            // M * P: P'[kc][is][jc][js]; P * M: P'[ic][is][kc][js] (P^+ read
+            // transposed, element by element; else four consecutive elements)
+            const Cx<R>* P = MP ? B : A;
+            constexpr bool adj = MP ? CB : CA;
+            if constexpr (!adj) {
+              const Cx<R>* q = P + (MP ? p_idx(kc, u, v, 0, false) : p_idx(u, v, kc, 0, false));
+              ldc2(q, pv[0], pv[1]);
+              ldc2(q + 2, pv[2], pv[3]);
+            } else {
+#pragma unroll
+              for (int js = 0; js < 4; js++)
+                pv[js] = ldc(P + (MP ? p_idx(kc, u, v, js, true) : p_idx(u, v, kc, js, true)));
+            }
+#pragma unroll
+            for (int w = 0; w < 3; w++) mv[w] = MP ? ldc(A + m_idx(w, kc, CA)) : ldc(B + m_idx(kc, w, CB));
+#pragma unroll
+            for (int w = 0; w < 3; w++)
+#pragma unroll
+              for (int js = 0; js < 4; js++) {
+                if constexpr (MP)
+                  cmac<CA, CB>(x[w][js], minus, mv[w], pv[js]);
+                else
+                  cmac<CA, CB>(x[w][js], minus, pv[js], mv[w]);
+              }
+          }
+        }
+        release_stage(&empty[st], lane);  // this warp is done with the stage
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+        if (ls < nloc) {
+#pragma unroll
+          for (int w = 0; w < 3; w++)
+#pragma unroll
+            for (int js = 0; js < 4; js += 2) stc2(o + oidx(w) + js, x[w][js], x[w][js + 1]);
+        }
       }
       if (++st == S) {
         st = 0;
@@ -665,10 +799,10 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_pp_tma_kernel(const 
   }
 }
 
-// shared-memory bytes of prop_pp_tma_kernel<.., SPB> with `stages` stages
-template <typename R>
-constexpr size_t pp_tma_smem(int spb, int stages) {
-  return 256 + (size_t)stages * spb * (PPStride<R>::A + PPStride<R>::B);
+// shared-memory bytes of prop_tma_kernel<R, KIND, .., SPB> with `stages` stages
+template <typename R, int KIND>
+constexpr size_t prop_tma_smem(int spb, int stages) {
+  return 256 + (size_t)stages * spb * (PTSlots<R, KIND>::A + PTSlots<R, KIND>::B);
 }
 
 // blocks per SM of a kernel at (threads, smem), raising its dynamic
@@ -744,35 +878,62 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
   if (grid > cap) grid = cap;
   const unsigned gr = (unsigned)(grid < 1 ? 1 : grid);
   cudaStream_t st = current_stream();
-  if constexpr (KIND == PK_TRACE)
+  const bool contig =
+      gang == nullptr && a.mode == OM_CONTIG && b.mode == OM_CONTIG && p.vec_a && p.vec_b && p.vec_out;
+  if constexpr (KIND == PK_TRACE) {
     prop_trace_kernel<R><<<gr, 256, 0, st>>>(p);
-  else if constexpr (KIND == PK_MP)
-    prop_mp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
-  else if constexpr (KIND == PK_PM)
-    prop_pm_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
-  else {
-    const bool contig = gang == nullptr && a.mode == OM_CONTIG && b.mode == OM_CONTIG && p.vec_a && p.vec_b &&
-                        p.vec_out;
-    if (!contig) {
+  } else if (!contig) {
+    // gang, pointer or unaligned operands: the direct kernels
+    if constexpr (KIND == PK_MP)
+      prop_mp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+    else if constexpr (KIND == PK_PM)
+      prop_pm_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
+    else
       prop_pp_kernel<R, CA, CB><<<gr, 256, 0, st>>>(p);
-    } else {
-      // bulk-copy pipeline, tiles of 8 sites, 96 consumer threads + one
-      // producer warp per block.  F3: three stages (57 KB), four blocks per
-      // SM at up to 128 registers; measured on B200 (131,072 sites) 90 us,
-      // where two stages took 92 us and five or six blocks per SM at 80-96
-      // registers 95-98 us (fewer registers cost more than the extra warps
-      // gain).  D3: two stages (75 KB), three blocks per SM.
-      constexpr int SPB = 8;
-      constexpr bool F32 = sizeof(R) == 4;
-      constexpr int MINB = F32 ? 4 : 3;
-      p.stages = F32 ? 3 : 2;
-      p.err = device_error_word();
-      const size_t smem = pp_tma_smem<R>(SPB, p.stages);
-      const long long ntiles = ((long long)n + SPB - 1) / SPB;
-      const void* fn = reinterpret_cast<const void*>(&prop_pp_tma_kernel<R, CA, CB, SPB, MINB>);
-      long long blocks = (long long)prop_blocks_per_sm(fn, 12 * SPB + 32, smem) * device_sm_count();
+  } else {
+    // bulk-copy pipeline, tiles of 8 sites, 96 consumer threads + one
+    // producer warp per block.  P * P: F3 three stages (57 KB), four blocks
+    // per SM at up to 128 registers; measured on B200 (131,072 sites) 90 us,
+    // where two stages took 92 us and five or six blocks per SM at 80-96
+    // registers 95-98 us (fewer registers cost more than the extra warps
+    // gain); D3 two stages (75 KB), three blocks per SM.  M * P and P * M,
+    // where fewer requests in flight measured faster (131,072 sites, M * P /
+    // P * M): F3 three stages and three blocks per SM 53.7 / 55.0 us = 0.88 /
+    // 0.87 of HBM peak (four stages and five blocks 57.0 / 61.8 us); D3 two
+    // stages and two blocks per SM 106.7 / 124.8 us (three stages and three
+    // blocks 113.0 / 137.6 us).
+    constexpr int SPB = 8;
+    constexpr bool F32 = sizeof(R) == 4;
+    constexpr bool PP = KIND == PK_PP;
+    constexpr int MINB = PP ? (F32 ? 4 : 3) : 3;
+    constexpr int CAP = PP ? 32 : (F32 ? 3 : 2);  // blocks per SM at most
+    p.stages = PP ? (F32 ? 3 : 2) : (F32 ? 3 : 2);
+    p.err = device_error_word();
+    const size_t smem = prop_tma_smem<R, KIND>(SPB, p.stages);
+    // M * P and P * M: full tiles in the pipeline (the M records of a tile go
+    // in one bulk copy), the last n % SPB sites by the direct kernel
+    const long long ntiles = PP ? ((long long)n + SPB - 1) / SPB : (long long)n / SPB;
+    if (ntiles > 0) {
+      const void* fn = reinterpret_cast<const void*>(&prop_tma_kernel<R, KIND, CA, CB, SPB, MINB>);
+      const int nb = prop_blocks_per_sm(fn, 12 * SPB + 32, smem);
+      long long blocks = (long long)(nb < CAP ? nb : CAP) * device_sm_count();
       if (blocks > ntiles) blocks = ntiles;
-      prop_pp_tma_kernel<R, CA, CB, SPB, MINB><<<(unsigned)blocks, 12 * SPB + 32, smem, st>>>(p, ntiles);
+      prop_tma_kernel<R, KIND, CA, CB, SPB, MINB><<<(unsigned)blocks, 12 * SPB + 32, smem, st>>>(p, ntiles);
+    }
+    if constexpr (!PP) {
+      const long long done = ntiles * SPB;
+      if (done < n) {
+        using SL = PTSlots<R, KIND>;
+        PropParams t = p;
+        t.a.base = static_cast<const char*>(a.base) + done * SL::RA;
+        t.b.base = static_cast<const char*>(b.base) + done * SL::RB;
+        t.out = static_cast<Cx<R>*>(r) + done * 144;
+        t.n = n - done;
+        if constexpr (KIND == PK_MP)
+          prop_mp_kernel<R, CA, CB><<<1, 256, 0, st>>>(t);
+        else
+          prop_pm_kernel<R, CA, CB><<<1, 256, 0, st>>>(t);
+      }
     }
   }
   check_launch(kid);

@@ -61,21 +61,26 @@ def test_all_propagator_entry_points(qla, pc, dt):
 @pytest.mark.parametrize("pc,dt", [("F3", np.float32), ("D3", np.float64)])
 @pytest.mark.parametrize("n", [1, 7, 20011])
 def test_propagator_products_many_tiles_and_tiny_fields(qla, pc, dt, n):
-    """The contiguous P*P kernels at sizes where persistent blocks walk many
-    tiles (software pipeline refilled many times; 20,011 sites is a partial
-    last tile) and at fewer sites than one tile, every eqop and adjoint."""
+    """The contiguous P*P, M*P and P*M kernels (bulk-copy pipeline) at sizes
+    where persistent blocks walk many tiles (stage ring refilled many times;
+    20,011 sites ends in a partial tile, which M*P and P*M hand to the direct
+    kernel) and at fewer sites than one tile, every eqop and adjoint."""
     rng = np.random.default_rng(124 + n)
     p1 = T.gaussian_field(rng, n, 144, dt)
     p2 = T.gaussian_field(rng, n, 144, dt)
+    m = T.gaussian_field(rng, n, 9, dt)
     r0 = T.gaussian_field(rng, n, 144, dt)
-    d1, d2 = T.to_dev(p1), T.to_dev(p2)
-    for eq in ("eq", "peq", "meq", "eqm"):
-        for ca in ("", "a"):
-            for cb in ("", "a"):
-                name = f"P_v{eq}_P{ca}_times_P{cb}"
-                r_d = T.to_dev(r0)
-                getattr(getattr(qla, pc), name)(r_d, d1, d2, n)
-                want = r0.copy()
-                T.ora_prop("PP", want, p1, p2, n, eq, ca=int(bool(ca)), cb=int(bool(cb)))
-                assert T.bits_equal(T.to_host(r_d), want), (name, n)
+    d1, d2, dm = T.to_dev(p1), T.to_dev(p2), T.to_dev(m)
+    for ta, tb in (("P", "P"), ("M", "P"), ("P", "M")):
+        for eq in ("eq", "peq", "meq", "eqm"):
+            for ca in ("", "a"):
+                for cb in ("", "a"):
+                    name = f"P_v{eq}_{ta}{ca}_times_{tb}{cb}"
+                    xa, xb = (m if ta == "M" else p1), (m if tb == "M" else p2)
+                    da, db = (dm if ta == "M" else d1), (dm if tb == "M" else d2)
+                    r_d = T.to_dev(r0)
+                    getattr(getattr(qla, pc), name)(r_d, da, db, n)
+                    want = r0.copy()
+                    T.ora_prop(ta + tb, want, xa, xb, n, eq, ca=int(bool(ca)), cb=int(bool(cb)))
+                    assert T.bits_equal(T.to_host(r_d), want), (name, n)
     assert qla.device_error() == 0
