@@ -8,22 +8,27 @@
 // multiplication, expressions_tensor.pl:766; spin trace build_qla.pl:942-968).
 //
 // A P record does not fit in one thread's registers, so several threads share
-// a site, and the work is split so that every thread reads each operand
-// element it needs once, in 16-B (F3) / 32-B (D3) runs of two consecutive
-// complex numbers, and consecutive threads touch consecutive runs:
+// a site.  Contiguous, 16-B aligned operands without a gang index go through
+// one bulk-copy (TMA) pipeline of 8-site tiles (prop_tma_kernel: a producer
+// warp stages the tile's records, 12 consumer threads per site compute from
+// shared memory):
+//   M * P   thread (is, jc) accumulates outputs (ic, is, jc, js) over ic, js;
+//   P * M   thread (ic, is) accumulates outputs (ic, is, jc, js) over jc, js;
+//   P * P   2 output rows x 6 columns per thread (F3 in packed FP32x2
+//           arithmetic).
+// Gang, pointer or unaligned operands (and the last n mod 8 sites of M * P
+// and P * M) run direct kernels that read every operand element once, in
+// 16-B (F3) / 32-B (D3) runs of two consecutive complex numbers, consecutive
+// threads touching consecutive runs:
 //   M * P   24 threads per site, thread (is, jc, js pair): the P run
 //           P[kc][is][jc][js..js+1] serves all three output colours ic;
 //   P * M   24 threads per site, thread (ic, is, js pair): the P run
 //           P[ic][is][kc][js..js+1] serves all three output colours jc;
-//   P * P   contiguous operands through a bulk-copy (TMA) pipeline of
-//           8-site tiles, 12 threads per site, 2 output rows x 6 columns per
-//           thread (F3 in packed FP32x2 arithmetic; prop_tma_kernel);
-//           gang, pointer or unaligned operands 6 (F3) / 12 (D3) threads per
-//           site, a column block of the second operand in registers
-//           (prop_pp_kernel).
-// The 9 matrix elements come from L1 (shared by a site's threads).  Adjoint
-// or pointer operands read element by element.  Every output element is
-// accumulated exactly as the reference does (x = 0 or r, then
+//   P * P   6 (F3) / 12 (D3) threads per site, a column block of the second
+//           operand in registers (prop_pp_kernel);
+// there the 9 matrix elements come from L1 (shared by a site's threads), and
+// adjoint or pointer operands are read element by element.  Every output
+// element is accumulated exactly as the reference does (x = 0 or r, then
 // x (+|-)= a*b over k in order), so results are bit-identical.  The spin
 // trace keeps one thread per output element (9 per site).
 #pragma once
