@@ -1048,10 +1048,9 @@ static BatchPlan* make_plan(const char* who, const qlagpu_F3_batch_program* fiel
   plan->grid = (int)(grid < 1 ? 1 : grid);
   // Tile groups, measured on B200 (64 uneven fields, fraction of HBM peak by
   // group size 1 / 4 / 8 / 16 / one contiguous run per block): config 4's
-  // shape 0.80 / 0.82 / 0.83 / 0.85 / 0.86-0.89, where each tile's work is
-  // short and a descriptor reload per tile shows; the hop shape 0.68 / 0.70 /
-  // 0.70 / 0.67 / 0.62 and a config-4 / hop mix 0.35 / 0.36 / 0.37 / 0.37 /
-  // 0.35, where the grid walking the fields together reads memory in order.
+  // shape 0.78 / 0.83 / 0.86 / 0.88 / 0.91, where each tile's work is short
+  // and a descriptor reload per tile shows; the hop shape 0.67 / 0.72 / 0.73 /
+  // 0.72 / 0.74 and a config-4 / hop mix 0.37 / 0.38 / 0.39 / 0.38 / 0.39.
   plan->chunk = shape == SH_CONFIG4 ? (tiles + plan->grid - 1) / plan->grid : 8;
   return plan;
 }
