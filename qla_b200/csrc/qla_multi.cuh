@@ -233,6 +233,14 @@ inline void api_multi(const char* kid, void* r, const void* a, bool pa, const vo
       p.b[d] = pb ? op_ptr(static_cast<const void* const*>(bd)) : op_contig(bd);
       direct = direct || !aligned16(ad) || !aligned16(bd);
     }
+    // pointer (gathered) operands whose staged bytes per site leave tiles of
+    // fewer than 128 sites run the direct kernel: with few sites staged per
+    // block the gathers' latency is exposed.  Measured on B200, D3
+    // V_vpeq_nM_times_npV at nd = 4 (656 B staged per site, 64-site tiles),
+    // 32^3 x 64 sites: staged 345 us, direct 264 us; F3 (344 B, 128-site
+    // tiles) stays staged at 0.98 of HBM peak.
+    const unsigned staged_bps = (unsigned)p.nd * ((pa ? 8u : RM) + (pb ? 8u : RV)) + (p.out_read ? RV : 0u);
+    if ((pa || pb) && default_shape(staged_bps, RV).threads < 128) direct = true;
     if (direct) {
       long long grid = ((long long)n + 255) / 256;
       if (grid > (long long)sms * 8) grid = (long long)sms * 8;
