@@ -508,13 +508,19 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
   uint64_t* full = reinterpret_cast<uint64_t*>(ptm);
   uint64_t* empty = full + 8;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(ptm + 8 * 16);
+  uint64_t* ready = reinterpret_cast<uint64_t*>(ptm + 8 * 24);  // F3 P * P: second operand rewritten
   unsigned char* stages = ptm + 256;
+  // F3 P * P: the producer warp rewrites each landed second-operand record
+  // in place into per-column-pair real / imaginary planes, so that the
+  // consumers load ready FP32x2 operand pairs; consumers wait on `ready`
+  constexpr bool XF = KIND == PK_PP && sizeof(R) == 4;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long my = ((long long)blockIdx.x < ntiles) ? (ntiles - 1 - (long long)blockIdx.x) / gridDim.x + 1 : 0;
   if (tid == 0) {
     for (int i = 0; i < S; i++) {
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], (unsigned)NCW);
+      mbar_init(&ready[i], 1);
     }
     *abort_flag = 0;
     mbar_init_fence();
@@ -526,6 +532,56 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
     const uint64_t pol = policy_evict_first();
     const char* Ag = static_cast<const char*>(p.a.base);
     const char* Bg = static_cast<const char*>(p.b.base);
+    // F3 P * P: once tile kt's copies have landed, rewrite its second-operand
+    // records in place.  Element (kk, j) (of P, or of P^+ read transposed)
+    // goes to floats kk*24 + cg*12 + 2q + (j & 1) (real) and 6 later
+    // (imaginary), with j / 2 = cg + 2q: per k and column half cg, the real
+    // parts of the three column pairs, then their imaginary parts.
+    auto transform = [&](long long kt) -> bool {
+      const int sst = (int)(kt % S);
+      const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded_idle(&full[sst], (uint32_t)((kt / S) & 1), p.err,
+                                                                      2000000000ull, abort_flag));
+      if (!ok) return false;
+      const long long s0 = ((long long)blockIdx.x + kt * gridDim.x) * SPB;
+      const int nl = (int)((p.n - s0) < SPB ? (p.n - s0) : SPB);
+      float* sbase = reinterpret_cast<float*>(stages + (size_t)sst * STAGE + SPB * SA);
+      for (int site = 0; site < nl; site++) {
+        float* b = sbase + site * (SB / 4);
+        float4 v[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          const int w = lane + 32 * i;  // 16-B word of the record: elements (r, c), (r, c + 1), c even
+          if (w < 72) v[i] = reinterpret_cast<const float4*>(b)[w];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          const int w = lane + 32 * i;
+          if (w < 72) {
+            const int r = w / 6, c = 2 * (w - r * 6);
+            if constexpr (!CB) {  // (kk, j) = (r, c), (r, c + 1): one pair of each plane
+              const int jp = c >> 1, o = r * 24 + (jp & 1) * 12 + 2 * (jp >> 1);
+              *reinterpret_cast<float2*>(b + o) = make_float2(v[i].x, v[i].z);
+              *reinterpret_cast<float2*>(b + o + 6) = make_float2(v[i].y, v[i].w);
+            } else {  // P^+: (kk, j) = (c, r), (c + 1, r)
+              const int jp = r >> 1, o = c * 24 + (jp & 1) * 12 + 2 * (jp >> 1) + (r & 1);
+              b[o] = v[i].x;
+              b[o + 6] = v[i].y;
+              b[o + 24] = v[i].z;
+              b[o + 30] = v[i].w;
+            }
+          }
+        }
+        __syncwarp();
+      }
+      // the rewritten slots: visible to the consumers through `ready`, and
+      // ordered before the async proxy's next copy into the stage
+      __threadfence_block();
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ready[sst]);
+      return true;
+    };
     int st = 0;
     long long round = 0, k = 0;
     for (; k < my; k++) {
@@ -562,12 +618,22 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
         else if (lane == 31)
           bulk_g2s(mslots, Mg + site0 * MREC, (unsigned)nloc * MREC, &full[st], pol);
       }
+      if constexpr (XF) {
+        if (k >= 1 && !transform(k - 1)) {  // the previous tile, while this one's copies fly
+          if (lane == 0) *abort_flag = 1;
+          k++;  // tile k's copies were issued
+          break;
+        }
+      }
       if (++st == S) {
         st = 0;
         round++;
       }
     }
     issued = k;
+    if constexpr (XF) {
+      if (issued == my && my >= 1 && !transform(my - 1) && lane == 0) *abort_flag = 1;
+    }
   } else {
     // ------------------------------------------------------------ consumers
     const int ls = tid / 12, t12 = tid - ls * 12, rg = t12 >> 1, cg = t12 & 1;
@@ -578,8 +644,8 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
     uint32_t par = 0;
     for (long long k = 0; k < my; k++) {
       // warp-uniform, so that the warp leaves the loop as a whole
-      const bool ok =
-          __all_sync(0xffffffffu, mbar_wait_bounded_idle(&full[st], par, p.err, 2000000000ull, abort_flag));
+      const bool ok = __all_sync(
+          0xffffffffu, mbar_wait_bounded_idle(XF ? &ready[st] : &full[st], par, p.err, 2000000000ull, abort_flag));
       const long long site0 = ((long long)blockIdx.x + k * gridDim.x) * SPB;
       const int nloc = (int)((p.n - site0) < SPB ? (p.n - site0) : SPB);
       const bool active = ok && ls < nloc;
@@ -626,28 +692,20 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
                 ai[1][h] = f2_pack(v.w, v.w);
               }
             }
-            // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before conjugation
+            // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before
+            // conjugation, from the planes the producer wrote: per (k, cg) the
+            // real pairs of q = 0, 1, 2 then the imaginary pairs
             F2 bre[2][3], bim[2][3];
-            if constexpr (!CB) {
 #pragma unroll
-              for (int h = 0; h < 2; h++)
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                  const float4 v = *reinterpret_cast<const float4*>(B + (kk + h) * 24 + 4 * (cg + 2 * q));
-                  bre[h][q] = f2_pack(v.x, v.z);
-                  bim[h][q] = f2_pack(v.y, v.w);
-                }
-            } else {  // P^+[kk][j] = conj P[j][kk]: elements (j, kk), (j, kk + 1) are adjacent
-#pragma unroll
-              for (int q = 0; q < 3; q++) {
-                const int j = 2 * (cg + 2 * q);
-                const float4 v0 = *reinterpret_cast<const float4*>(B + j * 24 + 2 * kk);
-                const float4 v1 = *reinterpret_cast<const float4*>(B + (j + 1) * 24 + 2 * kk);
-                bre[0][q] = f2_pack(v0.x, v1.x);
-                bim[0][q] = f2_pack(v0.y, v1.y);
-                bre[1][q] = f2_pack(v0.z, v1.z);
-                bim[1][q] = f2_pack(v0.w, v1.w);
-              }
+            for (int h = 0; h < 2; h++) {
+              const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(B + (kk + h) * 24 + cg * 12);
+              const ulonglong2 w0 = q2[0], w1 = q2[1], w2 = q2[2];
+              bre[h][0] = w0.x;
+              bre[h][1] = w0.y;
+              bre[h][2] = w1.x;
+              bim[h][0] = w1.y;
+              bim[h][1] = w2.x;
+              bim[h][2] = w2.y;
             }
 #pragma unroll
             for (int h = 0; h < 2; h++)
@@ -898,10 +956,11 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
   } else {
     // bulk-copy pipeline, tiles of 8 sites, 96 consumer threads + one
     // producer warp per block.  P * P: F3 three stages (57 KB), four blocks
-    // per SM at up to 128 registers; measured on B200 (131,072 sites) 90 us,
-    // where two stages took 92 us and five or six blocks per SM at 80-96
-    // registers 95-98 us (fewer registers cost more than the extra warps
-    // gain); D3 two stages (75 KB), three blocks per SM.  M * P and P * M,
+    // per SM at up to 128 registers; measured on B200 (131,072 sites) 86 us
+    // with the producer's rewrite of the second operand into planes, where
+    // two stages took 109 us and four stages at three blocks per SM 99 us
+    // (before the rewrite: 90 us; five or six blocks per SM at 80-96
+    // registers 95-98 us); D3 two stages (75 KB), three blocks per SM.  M * P and P * M,
     // where fewer requests in flight measured faster (131,072 sites, M * P /
     // P * M): F3 three stages and three blocks per SM 53.7 / 55.0 us = 0.88 /
     // 0.87 of HBM peak (four stages and five blocks 57.0 / 61.8 us); D3 two
