@@ -1,13 +1,14 @@
 """Autotuner of the bulk-copy pipeline's launch shape.
 
-    python -m qla_b200.tune [--out qla_b200/tune_b200.txt] [--reps 20]
+    python -m qla_b200.tune [--out qla_b200/tune_b200.txt] [--reps 20] [--keys KEY ...]
 
 For each hot kernel (identified by the key the launcher uses:
 "<pc>_<family>:<operand modes>[r]", modes c = contiguous, p = pointer array,
 i = int32 index stream, r = destination read by peq/meq) it times every
 (consumer threads = sites per tile in {64,128,256}) x (pipeline stages in
 {2,3,4}) shape with CUDA events on fields larger than L2 and writes the
-fastest per key.  libqla_b200.so reads the table at its first launch (the
+fastest per key; the batched program launch (key F3_batch_program, config 4's
+64 uneven fields) over sites per tile in {64,128} x stages {2,3,4}.  libqla_b200.so reads the table at its first launch (the
 file beside the package, or $QLA_B200_TUNE); keys missing from it use the
 built-in heuristic.
 """
@@ -80,17 +81,77 @@ def _workloads(torch, L):
                lambda: getattr(L, f"QLA_{pc}_M_veq_M_times_M")(V(Mo), V(U), V(U2), m))
         del U, U2, Mo, D, H, H2, Vv, Vo, pH, pV, pM, idx, Dout
         torch.cuda.empty_cache()
+    yield _batch_workload(torch)
 
 
-def tune(out=DEFAULT_OUT, reps=20, verbose=True):
+class _Batch:
+    """Config 4's batched launch: 64 F3 fields with extents drawn from
+    {8,12,16,20,24,32}^4, each running r = u * u2[nbr], w = r * v.  The tile
+    shape is fixed when a plan is built, so prepare() rebuilds the plan after
+    each tuned shape is set."""
+    SHAPES = list(itertools.product([64, 128], [2, 3, 4]))  # the batch kernel's launch bounds allow 64 / 128
+
+    def __init__(self, torch):
+        import numpy as np
+        rng = np.random.default_rng(4)
+        choices = [8, 12, 16, 20, 24, 32]
+        self.fields = []
+        for k in range(64):
+            dims = [int(x) for x in rng.choice(choices, 4)]
+            n = int(np.prod(dims))
+            nbr = torch.empty(n, dtype=torch.int32, device="cuda")
+            qla.shift_index(nbr, dims, k % 4, 1)
+            self.fields.append({"r": torch.empty(n, 18, device="cuda"), "u": torch.randn(n, 18, device="cuda"),
+                                "u2": torch.randn(n, 18, device="cuda"), "nbr": nbr,
+                                "w": torch.empty(n, 6, device="cuda"), "v": torch.randn(n, 6, device="cuda"),
+                                "n": n})
+        self.nbytes = sum(f["n"] for f in self.fields) * (72 * 3 + 24 * 2 + 4)
+        self.plan = None
+
+    def prepare(self):
+        if self.plan is not None:
+            self.plan.close()
+        self.plan = qla.BatchPlan(self.fields)
+
+    def __call__(self):
+        self.plan.run()
+
+
+def _batch_workload(torch):
+    b = _Batch(torch)
+    return ("F3_batch_program", b.nbytes, b, _Batch.SHAPES, b.prepare)
+
+
+def _read_table(path):
+    rows = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            for line in f:
+                parts = line.split("#")[0].split()
+                if len(parts) == 3:
+                    g = line.split("#")[1].strip() if "#" in line else "0"
+                    rows[parts[0]] = (int(parts[1]), int(parts[2]), float(g or 0))
+    return rows
+
+
+def tune(out=DEFAULT_OUT, reps=20, verbose=True, keys=None):
+    """Tune every workload (or those whose key contains one of `keys`, the
+    other rows of an existing table kept) and write the table."""
     import torch
     L = qla.lib()
     L.qlagpu_tune_clear()
     rows = []
-    for key, nbytes, fn in _workloads(torch, L):
+    for wl in _workloads(torch, L):
+        key, nbytes, fn = wl[:3]
+        shapes = wl[3] if len(wl) > 3 else SHAPES
+        prepare = wl[4] if len(wl) > 4 else None
+        if keys and not any(k in key for k in keys):
+            continue
         best = None
-        for t, s in SHAPES:
+        for t, s in shapes:
             L.qlagpu_tune_set(key.encode(), t, s)
+            if prepare is not None:
+                prepare()
             for _ in range(3):
                 fn()
             torch.cuda.synchronize()
@@ -111,11 +172,14 @@ def tune(out=DEFAULT_OUT, reps=20, verbose=True):
     L.qlagpu_tune_clear()
     if qla.device_error():
         raise qla.QLAError("a kernel reported an error during tuning")
+    table = _read_table(out) if keys else {}
+    for key, t, s, g in rows:
+        table[key] = (t, s, g)
     with open(out, "w") as f:
         f.write("# qla_b200 launch shapes measured on %s by python -m qla_b200.tune\n"
                 % torch.cuda.get_device_name())
         f.write("# key threads stages  (GB/s of algorithmic traffic at the tuning size)\n")
-        for key, t, s, g in rows:
+        for key, (t, s, g) in table.items():
             f.write(f"{key} {t} {s}  # {g:.0f}\n")
     return rows
 
@@ -124,5 +188,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--keys", nargs="*", default=None,
+                    help="tune only the keys containing one of these strings; keep the table's other rows")
     a = ap.parse_args()
-    tune(a.out, a.reps)
+    tune(a.out, a.reps, keys=a.keys)
