@@ -447,29 +447,34 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
   }
 }
 
-// P * P (F3 and D3) for contiguous, 16-B aligned operands without a gang
-// index: bulk-copy (TMA) pipeline, persistent, warp-specialised like the site
-// engine.
+// Propagator products (P * P, M * P, P * M; F3 and D3) for contiguous, 16-B
+// aligned operands without a gang index: bulk-copy (TMA) pipeline,
+// persistent, warp-specialised like the site engine.
 // Block = 12 * SPB consumer threads (12 per site of a tile of SPB sites) + one
 // producer warp.  Per stage of the ring there is a `full` mbarrier (completed
 // by the copies' transaction bytes) and an `empty` mbarrier (one arrival per
-// consumer warp).  The producer issues one 1152-B bulk copy per site and
-// operand into the stage (sites SA / SB floats apart, so that the sites one
-// warp covers spread over the banks); consumers wait on `full`, compute from
-// the stage, release it and store their results with 16-B stores.  No block
-// barrier sits in the tile loop.
+// consumer warp).  The producer issues one bulk copy per P record and one per
+// tile for the M records into the stage (slots padded so that the sites one
+// warp covers spread over the banks, PTSlots); consumers wait on `full`,
+// compute from the stage, release it and store their results with 16-B
+// stores.  No block barrier sits in the tile loop.  F3 P * P: the producer
+// then rewrites each landed second-operand record in place into
+// per-column-pair real / imaginary planes and arrives on a third mbarrier,
+// `ready`, which the consumers wait on instead of `full`.
 //
-// Thread (rg, cg) of a site accumulates the 12 output elements of rows 2rg,
-// 2rg+1: in F3 at the column pairs {2(cg + 2q), 2(cg + 2q) + 1}, q = 0..2, two
-// columns per FP32x2 register (cmac_x2: per-lane rounding as cmac<CA, CB>),
-// in D3 at the columns cg + 2q, q = 0..5, with cmac<CA, CB>; every element is
-// accumulated over k in order as the reference does, so results are
-// bit-identical.  Every wait is time-bounded; a failed wait raises the
-// block's abort flag, which ends every other wait of the block at once, and
-// loads still in flight are drained (bounded) before the block exits.
+// P * P: thread (rg, cg) of a site accumulates the 12 output elements of rows
+// 2rg, 2rg+1: in F3 at the column pairs {2(cg + 2q), 2(cg + 2q) + 1}, q = 0..2,
+// two columns per FP32x2 register (cmac_f2: per-lane rounding as cmac<CA,
+// CB>), in D3 at the columns cg + 2q, q = 0..5, with cmac<CA, CB>.  M * P and
+// P * M: see the consumer branch.  Every element is accumulated over k in
+// order as the reference does, so results are bit-identical.  Every wait is
+// time-bounded; a failed wait raises the block's abort flag, which ends every
+// other wait of the block at once, and loads still in flight are drained
+// (bounded) before the block exits.
 //
-// Dynamic shared memory: [full[8] | empty[8] | abort flag | pad to 256 B |
-//                         stages x (SPB x SA + SPB x SB floats)].
+// Dynamic shared memory: [full[8] | empty[8] | abort flag | ready[8] at
+//                         192 B | pad to 256 B | stages x (SPB x (SA + SB)
+//                         bytes)].
 // Stage slots of the bulk-copy kernel per operand: record bytes and slot
 // stride (bytes), chosen so that the sites one warp covers spread over the
 // shared-memory banks.  P records, one bulk copy per site into padded slots:
