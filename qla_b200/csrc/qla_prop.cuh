@@ -462,10 +462,11 @@ __global__ void __launch_bounds__(256) prop_pp_kernel(const PropParams p) {
 // per-column-pair real / imaginary planes and arrives on a third mbarrier,
 // `ready`, which the consumers wait on instead of `full`.
 //
-// P * P: thread (rg, cg) of a site accumulates the 12 output elements of rows
-// 2rg, 2rg+1: in F3 at the column pairs {2(cg + 2q), 2(cg + 2q) + 1}, q = 0..2,
-// two columns per FP32x2 register (cmac_f2: per-lane rounding as cmac<CA,
-// CB>), in D3 at the columns cg + 2q, q = 0..5, with cmac<CA, CB>.  M * P and
+// P * P: in F3 thread (rg, cg) of a site (12 per site) accumulates the 12
+// output elements of rows 2rg, 2rg+1 at the column pairs {2(cg + 2q),
+// 2(cg + 2q) + 1}, q = 0..2, two columns per FP32x2 register (cmac_f2:
+// per-lane rounding as cmac<CA, CB>); in D3 thread (r, cg) (24 per site)
+// accumulates row r at the columns cg + 2q, q = 0..5, with cmac<CA, CB>.  M * P and
 // P * M: see the consumer branch.  Every element is accumulated over k in
 // order as the reference does, so results are bit-identical.  Every wait is
 // time-bounded; a failed wait raises the block's abort flag, which ends every
@@ -493,10 +494,19 @@ struct PTSlots {
   static constexpr unsigned B = KIND == PK_PM ? MSLOT : (KIND == PK_PP ? PSLOT_B : PSLOT_A);
 };
 
+// consumer threads per site: 24 for D3 P * P (one output row each: twice the
+// warps in the same shared memory for its FP64 dependency chains), else 12
+template <typename R, int KIND>
+constexpr int prop_tma_tps() {
+  return (KIND == PK_PP && sizeof(R) == 8) ? 24 : 12;
+}
+
 template <typename R, int KIND, bool CA, bool CB, int SPB, int MINB>
-__global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const PropParams p, long long ntiles) {
+__global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
+    prop_tma_kernel(const PropParams p, long long ntiles) {
   extern __shared__ __align__(128) unsigned char ptm[];
-  constexpr int NCT = 12 * SPB;  // consumer threads
+  constexpr int TPS = prop_tma_tps<R, KIND>();
+  constexpr int NCT = TPS * SPB;  // consumer threads
   constexpr int NCW = NCT / 32;  // consumer warps
   using SL = PTSlots<R, KIND>;
   constexpr unsigned RA = SL::RA, RB = SL::RB;  // bytes per record of each operand
@@ -641,7 +651,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
     }
   } else {
     // ------------------------------------------------------------ consumers
-    const int ls = tid / 12, t12 = tid - ls * 12, rg = t12 >> 1, cg = t12 & 1;
+    const int ls = tid / TPS, t12 = tid - ls * TPS, rg = t12 >> 1, cg = t12 & 1;  // (t12: 0 .. TPS-1)
     const bool minus = (p.eqop == MEQ || p.eqop == EQM);
     const bool load = (p.eqop == PEQ || p.eqop == MEQ);
     const F2 z2 = f2_pack(p.negzero, p.negzero);  // (F3 products)
@@ -736,40 +746,24 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
                   make_float4(f2_lo(xr[i][q]), f2_lo(xi[i][q]), f2_hi(xr[i][q]), f2_hi(xi[i][q]));
         }
       } else if constexpr (KIND == PK_PP) {
-        // D3: thread (rg, cg) accumulates rows 2rg, 2rg+1 at columns cg + 2q,
-        // q = 0..5, with cmac<CA, CB>
+        // D3 (24 threads per site): thread (r, cg) = (rg, cg) accumulates row r
+        // at columns cg + 2q, q = 0..5, with cmac<CA, CB>
+        const int r = rg;
         const Cx<double>* A = reinterpret_cast<const Cx<double>*>(stg + ls * SA);
         const Cx<double>* B = reinterpret_cast<const Cx<double>*>(stg + SPB * SA + ls * SB);
-        Cx<double>* o = static_cast<Cx<double>*>(p.out) + (site0 + ls) * 144 + cg;
-        Cx<double> x[2][6];
+        Cx<double>* o = static_cast<Cx<double>*>(p.out) + (site0 + ls) * 144 + r * 12 + cg;
+        Cx<double> x[6];
 #pragma unroll
-        for (int i = 0; i < 2; i++)
-#pragma unroll
-          for (int q = 0; q < 6; q++) {
-            if (load && active) {
-              const double2 v = *reinterpret_cast<const double2*>(o + (2 * rg + i) * 12 + 2 * q);
-              x[i][q] = Cx<double>{v.x, v.y};
-            } else {
-              x[i][q] = Cx<double>{0.0, 0.0};
-            }
-          }
+        for (int q = 0; q < 6; q++) x[q] = (load && active) ? ldc(o + 2 * q) : Cx<double>{0.0, 0.0};
         if (active) {
-#pragma unroll 2
+#pragma unroll 4
           for (int kk = 0; kk < 12; kk++) {
-            Cx<double> a[2];  // element (row 2rg + i, kk) before conjugation (P^+[r][kk] = conj P[kk][r])
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-              const double2 v =
-                  *reinterpret_cast<const double2*>(A + (CA ? kk * 12 + 2 * rg + i : (2 * rg + i) * 12 + kk));
-              a[i] = Cx<double>{v.x, v.y};
-            }
+            // element (r, kk) before conjugation (P^+[r][kk] = conj P[kk][r])
+            const Cx<double> a = ldc(A + (CA ? kk * 12 + r : r * 12 + kk));
 #pragma unroll
             for (int q = 0; q < 6; q++) {
               const int j = cg + 2 * q;  // P^+[kk][j] = conj P[j][kk]
-              const double2 v = *reinterpret_cast<const double2*>(B + (CB ? j * 12 + kk : kk * 12 + j));
-              const Cx<double> bv{v.x, v.y};
-#pragma unroll
-              for (int i = 0; i < 2; i++) cmac<CA, CB>(x[i][q], minus, a[i], bv);
+              cmac<CA, CB>(x[q], minus, a, ldc(B + (CB ? j * 12 + kk : kk * 12 + j)));
             }
           }
         }
@@ -780,10 +774,7 @@ __global__ void __launch_bounds__(12 * SPB + 32, MINB) prop_tma_kernel(const Pro
         }
         if (ls < nloc) {
 #pragma unroll
-          for (int i = 0; i < 2; i++)
-#pragma unroll
-            for (int q = 0; q < 6; q++)
-              *reinterpret_cast<double2*>(o + (2 * rg + i) * 12 + 2 * q) = make_double2(x[i][q].re, x[i][q].im);
+          for (int q = 0; q < 6; q++) stc(o + 2 * q, x[q]);
         }
       } else {
         // M * P: thread (is, jc) of a site accumulates outputs (ic, is, jc, js),
@@ -984,10 +975,11 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
     const long long ntiles = PP ? ((long long)n + SPB - 1) / SPB : (long long)n / SPB;
     if (ntiles > 0) {
       const void* fn = reinterpret_cast<const void*>(&prop_tma_kernel<R, KIND, CA, CB, SPB, MINB>);
-      const int nb = prop_blocks_per_sm(fn, 12 * SPB + 32, smem);
+      constexpr int NT = prop_tma_tps<R, KIND>() * SPB + 32;
+      const int nb = prop_blocks_per_sm(fn, NT, smem);
       long long blocks = (long long)(nb < CAP ? nb : CAP) * device_sm_count();
       if (blocks > ntiles) blocks = ntiles;
-      prop_tma_kernel<R, KIND, CA, CB, SPB, MINB><<<(unsigned)blocks, 12 * SPB + 32, smem, st>>>(p, ntiles);
+      prop_tma_kernel<R, KIND, CA, CB, SPB, MINB><<<(unsigned)blocks, NT, smem, st>>>(p, ntiles);
     }
     if constexpr (!PP) {
       const long long done = ntiles * SPB;
