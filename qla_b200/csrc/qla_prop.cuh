@@ -10,12 +10,14 @@
 // A P record does not fit in one thread's registers, so several threads share
 // a site.  Contiguous, 16-B aligned operands without a gang index go through
 // one bulk-copy (TMA) pipeline of 8-site tiles (prop_tma_kernel: a producer
-// warp stages the tile's records, 12 consumer threads per site compute from
-// shared memory):
-//   M * P   thread (is, jc) accumulates outputs (ic, is, jc, js) over ic, js;
-//   P * M   thread (ic, is) accumulates outputs (ic, is, jc, js) over jc, js;
-//   P * P   2 output rows x 6 columns per thread (F3 in packed FP32x2
-//           arithmetic).
+// warp stages the tile's records, the consumer threads compute from shared
+// memory):
+//   M * P   24 threads per site, thread (is, jc, jh) accumulates outputs
+//           (ic, is, jc, 2jh..2jh+1) over ic;
+//   P * M   24 threads per site, thread (ic, is, jh) accumulates outputs
+//           (ic, is, jc, 2jh..2jh+1) over jc;
+//   P * P   F3 12 threads per site, 2 output rows x 6 columns each in packed
+//           FP32x2 arithmetic; D3 24 threads per site, one row x 6 columns.
 // Gang, pointer or unaligned operands (and the last n mod 8 sites of M * P
 // and P * M) run direct kernels that read every operand element once, in
 // 16-B (F3) / 32-B (D3) runs of two consecutive complex numbers, consecutive
@@ -495,10 +497,12 @@ struct PTSlots {
 };
 
 // consumer threads per site: 24 for D3 P * P (one output row each: twice the
-// warps in the same shared memory for its FP64 dependency chains), else 12
+// warps in the same shared memory for its FP64 dependency chains) and for
+// M * P and P * M (a thread's outputs are two consecutive elements of three
+// rows, so that adjacent lanes write adjacent 16-B / 32-B runs), else 12
 template <typename R, int KIND>
 constexpr int prop_tma_tps() {
-  return (KIND == PK_PP && sizeof(R) == 8) ? 24 : 12;
+  return (KIND == PK_MP || KIND == PK_PM || sizeof(R) == 8) ? 24 : 12;
 }
 
 template <typename R, int KIND, bool CA, bool CB, int SPB, int MINB>
@@ -777,56 +781,53 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
           for (int q = 0; q < 6; q++) stc(o + 2 * q, x[q]);
         }
       } else {
-        // M * P: thread (is, jc) of a site accumulates outputs (ic, is, jc, js),
-        // ic = 0..2, js = 0..3; P * M: thread (ic, is) accumulates outputs
-        // (ic, is, jc, js), jc = 0..2, js = 0..3.  Scalar cmac<CA, CB> (these
-        // products have a quarter of P * P's arithmetic), k in order.
+        static_assert(KIND != PK_PP && TPS == 24, "M * P and P * M run 24 threads per site");
+        // 24 threads per site, scalar cmac<CA, CB>, k in order.  M * P:
+        // thread (is, jc, jh) accumulates outputs (ic, is, jc, 2jh + j),
+        // ic = 0..2, from P'[kc][is][jc][2jh + j] and M'[ic][kc]; P * M: thread
+        // (ic, is, jh) accumulates outputs (ic, is, jc, 2jh + j), jc = 0..2,
+        // from P'[ic][is][kc][2jh + j] and M'[kc][jc] (P^+ read transposed)
         constexpr bool MP = KIND == PK_MP;
+        const int g = t12 >> 1, jh = t12 & 1;  // g = is * 3 + jc (M * P) or ic * 4 + is (P * M)
+        const int u = MP ? g / 3 : g >> 2, v = MP ? g - (g / 3) * 3 : g & 3;
         const Cx<R>* A = reinterpret_cast<const Cx<R>*>(stg + ls * SA);
         const Cx<R>* B = reinterpret_cast<const Cx<R>*>(stg + SPB * SA + ls * SB);
-        const int u = MP ? t12 / 3 : t12 / 4, v = MP ? t12 % 3 : t12 % 4;  // (is, jc) or (ic, is)
+        const Cx<R>* P = MP ? B : A;
         Cx<R>* o = static_cast<Cx<R>*>(p.out) + (site0 + ls) * 144;
-        // output (w, js) of this thread: w = ic (M * P) or jc (P * M)
-        auto oidx = [&](int w) { return MP ? p_idx(w, u, v, 0, false) : p_idx(u, v, w, 0, false); };
-        Cx<R> x[3][4];
+        // output w (ic for M * P, jc for P * M), elements 2jh, 2jh + 1
+        auto oidx = [&](int w) { return (MP ? p_idx(w, u, v, 0, false) : p_idx(u, v, w, 0, false)) + 2 * jh; };
+        Cx<R> x[3][2];
 #pragma unroll
-        for (int w = 0; w < 3; w++)
-#pragma unroll
-          for (int js = 0; js < 4; js += 2) {
-            if (load && active) {
-              ldc2(o + oidx(w) + js, x[w][js], x[w][js + 1]);
-            } else {
-              x[w][js] = Cx<R>{R(0), R(0)};
-              x[w][js + 1] = Cx<R>{R(0), R(0)};
-            }
+        for (int w = 0; w < 3; w++) {
+          if (load && active) {
+            ldc2(o + oidx(w), x[w][0], x[w][1]);
+          } else {
+            x[w][0] = Cx<R>{R(0), R(0)};
+            x[w][1] = Cx<R>{R(0), R(0)};
           }
+        }
         if (active) {
 #pragma unroll
           for (int kc = 0; kc < 3; kc++) {
-            Cx<R> pv[4], mv[3];  // the P operand's four elements, the M operand's three
-            // M * P: P'[kc][is][jc][js]; P * M: P'[ic][is][kc][js] (P^+ read
-            // transposed, element by element; else four consecutive elements)
-            const Cx<R>* P = MP ? B : A;
+            Cx<R> pv[2], mv[3];
             constexpr bool adj = MP ? CB : CA;
             if constexpr (!adj) {
-              const Cx<R>* q = P + (MP ? p_idx(kc, u, v, 0, false) : p_idx(u, v, kc, 0, false));
-              ldc2(q, pv[0], pv[1]);
-              ldc2(q + 2, pv[2], pv[3]);
+              ldc2(P + (MP ? p_idx(kc, u, v, 2 * jh, false) : p_idx(u, v, kc, 2 * jh, false)), pv[0], pv[1]);
             } else {
 #pragma unroll
-              for (int js = 0; js < 4; js++)
-                pv[js] = ldc(P + (MP ? p_idx(kc, u, v, js, true) : p_idx(u, v, kc, js, true)));
+              for (int j = 0; j < 2; j++)
+                pv[j] = ldc(P + (MP ? p_idx(kc, u, v, 2 * jh + j, true) : p_idx(u, v, kc, 2 * jh + j, true)));
             }
 #pragma unroll
             for (int w = 0; w < 3; w++) mv[w] = MP ? ldc(A + m_idx(w, kc, CA)) : ldc(B + m_idx(kc, w, CB));
 #pragma unroll
             for (int w = 0; w < 3; w++)
 #pragma unroll
-              for (int js = 0; js < 4; js++) {
+              for (int j = 0; j < 2; j++) {
                 if constexpr (MP)
-                  cmac<CA, CB>(x[w][js], minus, mv[w], pv[js]);
+                  cmac<CA, CB>(x[w][j], minus, mv[w], pv[j]);
                 else
-                  cmac<CA, CB>(x[w][js], minus, pv[js], mv[w]);
+                  cmac<CA, CB>(x[w][j], minus, pv[j], mv[w]);
               }
           }
         }
@@ -837,9 +838,7 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
         }
         if (ls < nloc) {
 #pragma unroll
-          for (int w = 0; w < 3; w++)
-#pragma unroll
-            for (int js = 0; js < 4; js += 2) stc2(o + oidx(w) + js, x[w][js], x[w][js + 1]);
+          for (int w = 0; w < 3; w++) stc2(o + oidx(w), x[w][0], x[w][1]);
         }
       }
       if (++st == S) {
@@ -956,18 +955,18 @@ inline void api_prop(const char* kid, void* r, Opnd a, Opnd b, const int* gang, 
     // with the producer's rewrite of the second operand into planes, where
     // two stages took 109 us and four stages at three blocks per SM 99 us
     // (before the rewrite: 90 us; five or six blocks per SM at 80-96
-    // registers 95-98 us); D3 two stages (75 KB), three blocks per SM.  M * P and P * M,
-    // where fewer requests in flight measured faster (131,072 sites, M * P /
-    // P * M): F3 three stages and three blocks per SM 53.7 / 55.0 us = 0.88 /
-    // 0.87 of HBM peak (four stages and five blocks 57.0 / 61.8 us); D3 two
-    // stages and two blocks per SM 106.7 / 124.8 us (three stages and three
-    // blocks 113.0 / 137.6 us).
+    // registers 95-98 us); D3 two stages (75 KB), three blocks per SM.  M * P
+    // and P * M (24 threads per site), where fewer requests in flight
+    // measured faster (131,072 sites, M * P / P * M): F3 two stages and four
+    // blocks per SM 52.5 / 52.6 us = 0.91 of HBM peak (three stages and three
+    // blocks 53.3 / 53.4 us); D3 two stages and two blocks per SM 99.4 / 101.5
+    // us = 0.96 / 0.94 (three stages and three blocks 107.4 / 114.8 us).
     constexpr int SPB = 8;
     constexpr bool F32 = sizeof(R) == 4;
     constexpr bool PP = KIND == PK_PP;
     constexpr int MINB = PP ? (F32 ? 4 : 3) : 3;
-    constexpr int CAP = PP ? 32 : (F32 ? 3 : 2);  // blocks per SM at most
-    p.stages = PP ? (F32 ? 3 : 2) : (F32 ? 3 : 2);
+    constexpr int CAP = PP ? 32 : (F32 ? 4 : 2);  // blocks per SM at most
+    p.stages = PP ? (F32 ? 3 : 2) : 2;
     p.err = device_error_word();
     const size_t smem = prop_tma_smem<R, KIND>(SPB, p.stages);
     // M * P and P * M: full tiles in the pipeline (the M records of a tile go
