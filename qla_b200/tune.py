@@ -175,13 +175,18 @@ def tune(out=DEFAULT_OUT, reps=20, verbose=True, keys=None):
     table = _read_table(out) if keys else {}
     for key, t, s, g in rows:
         table[key] = (t, s, g)
-    with open(out, "w") as f:
-        f.write("# qla_b200 launch shapes measured on %s by python -m qla_b200.tune\n"
-                % torch.cuda.get_device_name())
+    _write_table(out, table, torch.cuda.get_device_name())
+    return rows
+
+
+def _write_table(path, table, device):
+    """Write {key: (threads, stages, GB/s)} in the format the library reads
+    (`key threads stages`, `#` comments)."""
+    with open(path, "w") as f:
+        f.write("# qla_b200 launch shapes measured on %s by python -m qla_b200.tune\n" % device)
         f.write("# key threads stages  (GB/s of algorithmic traffic at the tuning size)\n")
         for key, (t, s, g) in table.items():
             f.write(f"{key} {t} {s}  # {g:.0f}\n")
-    return rows
 
 
 if __name__ == "__main__":
