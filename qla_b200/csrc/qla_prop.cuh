@@ -502,6 +502,8 @@ struct PTSlots {
 // rows, so that adjacent lanes write adjacent 16-B / 32-B runs), else 12
 template <typename R, int KIND>
 constexpr int prop_tma_tps() {
+  // (F3 P * P at 24 threads per site, one row each, measured slower: 98 us
+  // against 87 us at 12)
   return (KIND == PK_MP || KIND == PK_PM || sizeof(R) == 8) ? 24 : 12;
 }
 
@@ -670,16 +672,18 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
       const bool active = ok && ls < nloc;
       const unsigned char* stg = stages + (size_t)st * STAGE;
       if constexpr (KIND == PK_PP && sizeof(R) == 4) {
+        // rows RPT * rg + i of this thread (RPT = 1 with 24 threads per site)
+        constexpr int RPT = TPS == 24 ? 1 : 2;
         const float* A = reinterpret_cast<const float*>(stg + ls * SA);
         const float* B = reinterpret_cast<const float*>(stg + SPB * SA + ls * SB);
         const Cx<float>* og = static_cast<const Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
-        F2 xr[2][3], xi[2][3];  // [row 2rg + i][q]: lanes = columns 2(cg + 2q), +1
+        F2 xr[RPT][3], xi[RPT][3];  // [row RPT * rg + i][q]: lanes = columns 2(cg + 2q), +1
 #pragma unroll
-        for (int i = 0; i < 2; i++)
+        for (int i = 0; i < RPT; i++)
 #pragma unroll
           for (int q = 0; q < 3; q++) {
             if (load && active) {
-              const float4 v = *reinterpret_cast<const float4*>(og + (2 * rg + i) * 12 + 4 * q);
+              const float4 v = *reinterpret_cast<const float4*>(og + (RPT * rg + i) * 12 + 4 * q);
               xr[i][q] = f2_pack(v.x, v.z);
               xi[i][q] = f2_pack(v.y, v.w);
             } else {
@@ -690,18 +694,19 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
         if (active) {
 #pragma unroll
           for (int kk = 0; kk < 12; kk += 2) {
-            // element (row 2rg + i, kk + h) before conjugation, broadcast to both lanes
-            F2 ar[2][2], ai[2][2];
+            // element (row RPT * rg + i, kk + h) before conjugation, broadcast to both lanes
+            F2 ar[RPT][2], ai[RPT][2];
             if constexpr (!CA) {
 #pragma unroll
-              for (int i = 0; i < 2; i++) {
-                const float4 v = *reinterpret_cast<const float4*>(A + ((2 * rg + i) * 12 + kk) * 2);
+              for (int i = 0; i < RPT; i++) {
+                const float4 v = *reinterpret_cast<const float4*>(A + ((RPT * rg + i) * 12 + kk) * 2);
                 ar[i][0] = f2_pack(v.x, v.x);
                 ai[i][0] = f2_pack(v.y, v.y);
                 ar[i][1] = f2_pack(v.z, v.z);
                 ai[i][1] = f2_pack(v.w, v.w);
               }
-            } else {  // P^+[r][kk] = conj P[kk][r]: elements (kk + h, 2rg), (kk + h, 2rg + 1) are adjacent
+            } else if constexpr (RPT == 2) {
+              // P^+[r][kk] = conj P[kk][r]: elements (kk + h, 2rg), (kk + h, 2rg + 1) are adjacent
 #pragma unroll
               for (int h = 0; h < 2; h++) {
                 const float4 v = *reinterpret_cast<const float4*>(A + ((kk + h) * 12 + 2 * rg) * 2);
@@ -709,6 +714,13 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
                 ai[0][h] = f2_pack(v.y, v.y);
                 ar[1][h] = f2_pack(v.z, v.z);
                 ai[1][h] = f2_pack(v.w, v.w);
+              }
+            } else {  // P^+[r][kk] = conj P[kk][r], one row
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const float2 v = *reinterpret_cast<const float2*>(A + ((kk + h) * 12 + rg) * 2);
+                ar[0][h] = f2_pack(v.x, v.x);
+                ai[0][h] = f2_pack(v.y, v.y);
               }
             }
             // second-operand elements (kk + h, j), j = 2(cg + 2q) + {0, 1}, before
@@ -729,7 +741,7 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
 #pragma unroll
             for (int h = 0; h < 2; h++)
 #pragma unroll
-              for (int i = 0; i < 2; i++)
+              for (int i = 0; i < RPT; i++)
 #pragma unroll
                 for (int q = 0; q < 3; q++)
                   cmac_f2<CA, CB>(xr[i][q], xi[i][q], minus, ar[i][h], ai[i][h], bre[h][q], bim[h][q], z2);
@@ -743,10 +755,10 @@ __global__ void __launch_bounds__(prop_tma_tps<R, KIND>() * SPB + 32, MINB)
         if (ls < nloc) {
           Cx<float>* o = static_cast<Cx<float>*>(p.out) + (site0 + ls) * 144 + 2 * cg;
 #pragma unroll
-          for (int i = 0; i < 2; i++)
+          for (int i = 0; i < RPT; i++)
 #pragma unroll
             for (int q = 0; q < 3; q++)
-              *reinterpret_cast<float4*>(o + (2 * rg + i) * 12 + 4 * q) =
+              *reinterpret_cast<float4*>(o + (RPT * rg + i) * 12 + 4 * q) =
                   make_float4(f2_lo(xr[i][q]), f2_lo(xi[i][q]), f2_hi(xr[i][q]), f2_hi(xi[i][q]));
         }
       } else if constexpr (KIND == PK_PP) {
